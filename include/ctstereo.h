@@ -1,0 +1,291 @@
+/*
+ * ctstereo.h — C ABI of the ctstereo B200 stereo block-matching library.
+ *
+ * This boundary replaces the operator API of CluTec.Cuda's MultiView stereo
+ * drivers. Each reference driver object
+ *     CDriver::Configure(const CDevice&, const SImageFormat&, const SParameter&)
+ *     CDriver::Process(output, left, right, ...)
+ * becomes a handle with ct_<algo>_configure / ct_<algo>_process. Images are
+ * caller-owned device buffers described by ct_image (the role of
+ * _CDeviceSurface); parameters are plain structs passed to configure and used
+ * as kernel arguments (the reference copies them into __constant__ symbols,
+ * BlockMatcherNCC.cu:1393-1420); errors are int status codes instead of C++
+ * exceptions (CLU_EXCEPTION / CLU_CUDA_ENSURE_OK, Api.cpp:86-95).
+ *
+ * Conventions
+ *  - All process calls are asynchronous on the given stream and do no host
+ *    synchronisation, except where stated (ct_crosscheck_range).
+ *  - A handle may own device scratch (allocated in configure, freed by
+ *    ct_destroy). It is not thread-safe: use one handle per host thread or
+ *    lock externally; calls on one handle must not overlap on the GPU.
+ *  - Disparity d in [0, D) maps a base pixel x to x - d in the other view for
+ *    left-to-right matching and to x + d for right-to-left (the reference
+ *    hides this in _SDisparityConfig::MapPixelPos, whose arithmetic is not
+ *    available; this mapping is the library's definition).
+ *  - Disparity map encodings:
+ *      CT_PIX_U8 : d itself, 255 = not a disparity (invalid/inconsistent);
+ *                  requires D <= 255.
+ *      CT_PIX_U16: EDisparityId encoding (DisparityId.h:35-47): d + 1 for a
+ *                  disparity (First = 1 .. Last = 0xFFEF), 0xFFFF
+ *                  CannotEvaluate (window outside the image), 0xFFFA
+ *                  Inconsistent (failed cross-check).
+ *      CT_PIX_F32: sub-pixel disparity, -1.0f = invalid.
+ */
+#ifndef CTSTEREO_H
+#define CTSTEREO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* cudaStream_t without including the CUDA headers. */
+typedef struct CUstream_st* ct_stream;
+
+/* ---- status codes ------------------------------------------------------ */
+#define CT_OK 0
+#define CT_EINVAL 1   /* bad argument: null pointer, size or parameter out of range */
+#define CT_ETYPE 2    /* pixel type not supported ("Pixel types of given images not supported") */
+#define CT_EFORMAT 3  /* image sizes disagree ("... do not have the same format") */
+#define CT_ECUDA 4    /* a CUDA runtime call or kernel launch failed */
+#define CT_ETIMEOUT 5 /* a bounded device-side wait gave up (status read back later) */
+#define CT_ESTATE 6   /* handle of the wrong kind, or process before configure */
+#define CT_ENOMEM 7   /* device allocation failed */
+
+/* ---- pixel types (TPixel_Lum_UInt8 etc.) -------------------------------- */
+#define CT_PIX_U8 1
+#define CT_PIX_U16 2
+#define CT_PIX_U64 3
+#define CT_PIX_F32 4
+
+/* EDisparityId codes used in CT_PIX_U16 maps (DisparityId.h:35-47). */
+#define CT_DISP_FIRST 0x0001
+#define CT_DISP_LAST 0xFFEF
+#define CT_DISP_UNKNOWN 0x0000
+#define CT_DISP_CANNOT_EVALUATE 0xFFFF
+#define CT_DISP_SATURATED 0xFFFE
+#define CT_DISP_NOT_FOUND 0xFFFD
+#define CT_DISP_NOT_SPECIFIC 0xFFFC
+#define CT_DISP_NOT_UNIQUE 0xFFFB
+#define CT_DISP_INCONSISTENT 0xFFFA
+#define CT_DISP_U8_INVALID 0xFF
+
+/* A device image: the role of _CDeviceSurface (DeviceSurface.h:43-264), as a
+ * pitched linear buffer instead of a cudaArray + surface object. */
+typedef struct ct_image {
+    void* ptr;            /* device pointer to row 0 */
+    size_t pitch_bytes;   /* bytes between rows; >= width * element size */
+    int32_t width;
+    int32_t height;
+    int32_t type;         /* CT_PIX_* */
+    int32_t reserved;     /* must be 0 */
+} ct_image;
+
+/* Image format handed to configure: SImageFormat (width, height, pixel type). */
+typedef struct ct_format {
+    int32_t width;
+    int32_t height;
+    int32_t type;         /* pixel type of the input images: CT_PIX_U8 */
+} ct_format;
+
+typedef struct ct_handle ct_handle;
+
+/* ---- common ------------------------------------------------------------ */
+
+/* Message of the last failing call on this host thread ("" if none). */
+const char* ct_last_error_string(void);
+/* Library version, e.g. "ctstereo 0.1.0 sm_100a". */
+const char* ct_version(void);
+/* Release a handle of any kind and its device scratch. NULL is a no-op. */
+int ct_destroy(ct_handle* h);
+/* Device status word of the handle's last launches: 0 = fine, otherwise a
+ * CT_E* code written by a kernel (a bounded wait gave up). Synchronises the
+ * stream the handle last used, then clears the word. */
+int ct_handle_device_status(ct_handle* h, int32_t* status);
+
+/* ---- census transform: CensusTransform::CDriver -------------------------
+ * Replaces CensusTransform.h:44-70 / CensusTransform.cu:60-157.
+ *   CT_CENSUS_9X7: U8 -> U64. Window dx in [-4,4], dy in [-3,3]; the 63
+ *     positions in raster order including the centre go to bits 62..0 (MSB
+ *     first), bit 63 = 0; a bit is set iff neighbour > centre. Pixels within
+ *     4 columns / 3 rows of the border get 0.
+ *   CT_CENSUS_3X3: U8 -> U8, the reference transform exactly: 8 neighbours
+ *     in raster order to bits 7..0, strict '>', 1-px border NOT written.
+ */
+#define CT_CENSUS_9X7 0
+#define CT_CENSUS_3X3 1
+typedef struct ct_census_params {
+    int32_t window;       /* CT_CENSUS_9X7 or CT_CENSUS_3X3 */
+} ct_census_params;
+
+int ct_census_create(ct_handle** out);
+/* CDriver::Configure(device, format) (CensusTransform.cu:125-135). */
+int ct_census_configure(ct_handle* h, int32_t device, const ct_format* fmt, const ct_census_params* p);
+/* CDriver::Process(trg, src) (CensusTransform.cu:138-157): src U8, dst U64
+ * (9x7) or U8 (3x3), same width/height as configured. */
+int ct_census_process(ct_handle* h, const ct_image* dst, const ct_image* src, ct_stream stream);
+
+/* ---- census block matcher -----------------------------------------------
+ * 9x7 census of both images + Hamming cost (CensusDifference,
+ * BlockMatcherNCC.cu:153-158, on 64-bit descriptors) + (2r+1)^2 box
+ * aggregation + winner-take-all with the lowest d winning ties. A pixel is
+ * valid iff its aggregation window is inside the image; disparity d is
+ * searched iff the matched window is inside too. The handle owns the census
+ * descriptor scratch (2 * W * H * 8 bytes) and a key buffer (W * H * 4).
+ */
+typedef struct ct_census_match_params {
+    int32_t disp_count;     /* D, 1..256 */
+    int32_t agg_radius;     /* r: 2 gives the 5x5 box (only 2 is built) */
+    int32_t left_to_right;  /* 1: base = left image; 0: base = right image */
+    int32_t reserved;       /* must be 0 */
+} ct_census_match_params;
+
+int ct_bm_census_create(ct_handle** out);
+int ct_bm_census_configure(ct_handle* h, int32_t device, const ct_format* fmt,
+                           const ct_census_match_params* p);
+/* disp: U8 or U16 W x H. left/right: U8 W x H. */
+int ct_bm_census_process(ct_handle* h, const ct_image* disp, const ct_image* left,
+                         const ct_image* right, ct_stream stream);
+/* Both directions and the cross-check in one call: disp_lr / disp_rl (either
+ * may be NULL when not wanted) receive the left-to-right and right-to-left
+ * maps; disp_checked (may be NULL) the left map after the cross-check with
+ * tolerance tol (CrossCheckDisparityMaps semantics). The left_to_right field
+ * of the configured params is ignored here. */
+int ct_bm_census_process_lr(ct_handle* h, const ct_image* disp_lr, const ct_image* disp_rl,
+                            const ct_image* disp_checked, int32_t tol,
+                            const ct_image* left, const ct_image* right, ct_stream stream);
+/* Matching only, on census descriptors the caller computed with
+ * ct_census_process (U64, CT_CENSUS_9X7): desc_base is the base view's
+ * descriptors, desc_match the other view's; left_to_right selects x - d
+ * (1) or x + d (0). Same output rules as ct_bm_census_process. */
+int ct_bm_census_match_desc(ct_handle* h, const ct_image* disp, const ct_image* desc_base,
+                            const ct_image* desc_match, int32_t left_to_right, ct_stream stream);
+
+/* ---- SAD block matcher: BlockMatcherSAD1::CDriver ------------------------
+ * Replaces BlockMatcherSAD1.h:42-127 / BlockMatcherSAD1.cu:493-596 for the
+ * exhaustive mode: per-pixel |L - R| (EvalSAD, BlockMatcherSAD1.cu:151-153),
+ * (2r+1)^2 box sum, winner-take-all over all D with lowest-d ties. (The
+ * reference's coarse/fine search, gradient gate and SAD threshold are not
+ * built; SAD1 is excluded from the reference's own build.)
+ */
+typedef struct ct_sad_params {
+    int32_t disp_count;     /* iDispRange: D, 1..256 */
+    int32_t radius;         /* EConfig patch: r = 4 gives 9x9; 1..7 */
+    int32_t left_to_right;  /* 1: base = left image */
+    int32_t reserved;
+} ct_sad_params;
+
+int ct_bm_sad_create(ct_handle** out);
+int ct_bm_sad_configure(ct_handle* h, int32_t device, const ct_format* fmt, const ct_sad_params* p);
+/* CDriver::Process(disp, left, right): disp U8 or U16. */
+int ct_bm_sad_process(ct_handle* h, const ct_image* disp, const ct_image* left,
+                      const ct_image* right, ct_stream stream);
+
+/* ---- NCC block matcher: BlockMatcherNCC::CDriver -------------------------
+ * Replaces BlockMatcherNCC.h:41-144 / BlockMatcherNCC.cu:1270-1420.
+ * Exact integer window sums (Sx, Sxx, Sy, Syy, Sxy) and FP32 normalisation:
+ * ncc = float(n Sxy - Sx Sy) / sqrtf(float(n Sxx - Sx^2) * float(n Syy - Sy^2))
+ * and 0 when sigma_x sigma_y < 1 (BlockMatcherNCC.cu:255-262). Argmax over d
+ * with lowest-d ties. Left-to-right only. The score is not quantised.
+ */
+typedef struct ct_ncc_params {
+    int32_t disp_count;     /* D, 1..256 */
+    int32_t radius;         /* EConfig: 5 = Patch_11x11, 4 = Patch_9x9, 2 = Patch_5x5 */
+    int32_t left_to_right;  /* must be 1 */
+    int32_t reserved;
+} ct_ncc_params;
+
+int ct_bm_ncc_create(ct_handle** out);
+int ct_bm_ncc_configure(ct_handle* h, int32_t device, const ct_format* fmt, const ct_ncc_params* p);
+/* disp U8/U16; score (nullable) F32 = NCC at the chosen d (0 for invalid
+ * pixels); disp_init must be NULL (the guided MatcherUseDisparity mode is not
+ * built). */
+int ct_bm_ncc_process(ct_handle* h, const ct_image* disp, const ct_image* score,
+                      const ct_image* left, const ct_image* right, const ct_image* disp_init,
+                      ct_stream stream);
+
+/* ---- adaptive-window block matcher: BlockMatcherAW1 / AW2 ----------------
+ * Replaces BlockMatcherAW1.h:41-157 and BlockMatcherAW2.h:41-135 with the
+ * "best of 5 shifted windows" cost: A = min of the 7x7 SAD of the centred
+ * window and of the windows shifted by +-3 px in x and in y; winner-take-all
+ * (lowest d on ties) and FP32 parabolic sub-pixel refinement
+ * d + (c- - c+) / (2 (c- - 2 c0 + c+)), skipped at d = 0, d = D-1 or when
+ * d + 1 is not searchable. Left-to-right. Pixel valid iff 6 <= x < W-6 and
+ * 6 <= y < H-6; d searched iff x - d - 6 >= 0.
+ */
+typedef struct ct_aw_params {
+    int32_t disp_count;     /* D, 1..256 */
+    int32_t left_to_right;  /* must be 1 */
+    int32_t reserved0;
+    int32_t reserved1;
+} ct_aw_params;
+
+int ct_bm_aw_create(ct_handle** out);
+int ct_bm_aw_configure(ct_handle* h, int32_t device, const ct_format* fmt, const ct_aw_params* p);
+/* disp: F32 (sub-pixel, -1 invalid) or U8/U16 (integer WTA). */
+int ct_bm_aw_process(ct_handle* h, const ct_image* disp, const ct_image* left,
+                     const ct_image* right, ct_stream stream);
+
+/* ---- cross-check: CrossCheckDisparityMaps::CDriver ------------------------
+ * Replaces CrossCheckDisparityMaps.h:38-117 / .cu:63-190. For each pixel of
+ * disp_base holding a disparity d: x' = x - d (left_to_right = 1) or x + d;
+ * if x' is outside the image, or disp_other(x') is not a disparity, or
+ * |disp_other(x') - d| > disp_delta_thresh, the result is Inconsistent;
+ * otherwise d is kept. Non-disparity inputs are copied through. The min / max
+ * of the kept disparities is reduced on the device (the reference does a
+ * per-thread atomic range plus two blocking copies and a host reduction).
+ */
+typedef struct ct_crosscheck_params {
+    int32_t disp_delta_thresh;  /* iDispDeltaThresh */
+    int32_t left_to_right;      /* iIsLeftToRight */
+    int32_t reserved0;
+    int32_t reserved1;
+} ct_crosscheck_params;
+
+int ct_crosscheck_create(ct_handle** out);
+int ct_crosscheck_configure(ct_handle* h, int32_t device, const ct_format* fmt,
+                            const ct_crosscheck_params* p);
+/* result, disp_base, disp_other: same size and type (U8 or U16). */
+int ct_crosscheck_process(ct_handle* h, const ct_image* result, const ct_image* disp_base,
+                          const ct_image* disp_other, ct_stream stream);
+/* CDriver::DispMin() / DispMax(): synchronises the last process stream and
+ * returns the kept range in disparity units (min > max when none kept). */
+int ct_crosscheck_range(ct_handle* h, int32_t* disp_min, int32_t* disp_max);
+
+/* ---- synthetic stereo pairs -----------------------------------------------
+ * Seeded generator of rectified stereo pairs with ground truth (host memory).
+ *   kind 1: fractal value noise (4 octaves) left image; disparity = 4
+ *           background + 8 fronto-parallel rectangles in [0, dmax]; right =
+ *           forward warp with occlusion handling + N(0, 2^2); disoccluded
+ *           right pixels get fresh noise.
+ *   kind 2: 24 slanted planes (|grad d| <= 0.1 px/px, rounded), noise 3.
+ *   kind 3: 6 smooth Gaussians scaled to [0, dmax] + 12 sharp rectangles,
+ *           right-image gain in [0.9, 1.1], noise 2.
+ * gt: int16 left-view ground truth disparity; occ: 1 where the left pixel is
+ * occluded in the right view (or maps outside it). Any output may be NULL.
+ */
+int ct_synth_pair(int32_t kind, uint64_t seed, int32_t width, int32_t height, int32_t dmax,
+                  uint8_t* left, uint8_t* right, int16_t* gt, uint8_t* occ);
+
+/* ---- pipe-rate probe ---------------------------------------------------------
+ * Measures the issue rate of the integer operations the matchers are built
+ * from on the given device (a few ms of GPU time), as operations per SM per
+ * clock, plus the SM clock seen. Used for the integer-pipe roofline. */
+typedef struct ct_pipe_rates {
+    double popc_per_clk_sm;     /* 32-bit POPC */
+    double iadd3_per_clk_sm;    /* IADD3 */
+    double lop3_per_clk_sm;     /* LOP3 (xor) */
+    double vimnmx_per_clk_sm;   /* packed u16x2 3-way min */
+    double imad_per_clk_sm;     /* IMAD */
+    double sm_clock_mhz;        /* clock measured during the probe */
+    int32_t sm_count;
+    int32_t reserved;
+} ct_pipe_rates;
+int ct_probe_pipe_rates(int32_t device, ct_pipe_rates* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CTSTEREO_H */

@@ -1,0 +1,407 @@
+// census.cu — CensusTransform::CDriver and the census block matcher.
+//
+// Census transform (CensusTransform.cu:60-157): the 9x7 / 64-bit transform
+// stages an image tile into shared memory with one 2D TMA load and builds
+// each descriptor bit with a subtract + funnel shift (the sign of
+// centre - neighbour is the "neighbour > centre" bit). The 3x3 / 8-bit
+// reference transform is kept for parity with the reference.
+#include "ct_internal.h"
+#include "ct_device.cuh"
+#include "census_match.cuh"
+
+namespace ct {
+
+// ---------------------------------------------------------------------------
+// 9x7 census transform kernel
+// ---------------------------------------------------------------------------
+namespace census {
+
+constexpr int kTX = 64;   // tile columns
+constexpr int kTY = 32;   // tile rows
+constexpr int kPY = 8;    // rows per thread
+constexpr int kNT = kTX * (kTY / kPY);  // 256 threads
+constexpr int kBoxW = kTX + 32;         // 16 halo bytes each side (TMA x alignment)
+constexpr int kBoxH = kTY + 6;
+
+__global__ void __launch_bounds__(kNT) census9x7_kernel(const __grid_constant__ CUtensorMap tm_img, int W, int H,
+                                                         uint64_t* out, size_t out_pitch_elems,
+                                                         int32_t* status) {
+    __shared__ __align__(128) uint8_t tile[kBoxH * kBoxW];
+    __shared__ __align__(8) uint64_t bar;
+    const int tid = threadIdx.x;
+    const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
+    if (tid == 0) {
+        dev::mbar_init(&bar, 1);
+        dev::fence_barrier_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        dev::mbar_arrive_expect_tx(&bar, kBoxW * kBoxH);
+        dev::tma_load_2d(tile, &tm_img, x0 - 16, y0 - 3, &bar);
+    }
+    const bool got = dev::mbar_wait_bounded(&bar, 0);
+    if (__syncthreads_or(!got)) {
+        if (tid == 0) dev::report(status, CT_ETIMEOUT);
+        return;
+    }
+    const int tx = tid % kTX, ty = tid / kTX;
+    const int x = x0 + tx;
+    if (x >= W) return;
+    // sliding 7 x 9 window (values as int), rows advance one per pixel
+    int w[7][9];
+    const uint8_t* base = tile + (ty * kPY) * kBoxW + (16 + tx - 4);
+#pragma unroll
+    for (int r = 0; r < 6; ++r)
+#pragma unroll
+        for (int c = 0; c < 9; ++c) w[r + 1][c] = base[r * kBoxW + c];
+#pragma unroll
+    for (int p = 0; p < kPY; ++p) {
+#pragma unroll
+        for (int r = 0; r < 6; ++r)
+#pragma unroll
+            for (int c = 0; c < 9; ++c) w[r][c] = w[r + 1][c];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) w[6][c] = base[(p + 6) * kBoxW + c];
+        const int y = y0 + ty * kPY + p;
+        if (y >= H) break;
+        const int ctr = w[3][4];
+        uint32_t hi = 0, lo = 0;
+        int k = 0;
+#pragma unroll
+        for (int r = 0; r < 7; ++r)
+#pragma unroll
+            for (int c = 0; c < 9; ++c, ++k) {
+                const uint32_t t = uint32_t(ctr - w[r][c]);  // sign bit = neighbour > centre
+                if (k < 31) hi = __funnelshift_l(t, hi, 1);
+                else lo = __funnelshift_l(t, lo, 1);
+            }
+        const bool inside = x >= 4 && x < W - 4 && y >= 3 && y < H - 3;
+        const uint64_t d = inside ? ((uint64_t(hi) << 32) | lo) : 0ull;
+        out[(size_t)y * out_pitch_elems + x] = d;
+    }
+}
+
+// 3x3 / 8-bit reference transform (CensusTransform.cu:60-120): bits 7..0 =
+// (-1,-1),(0,-1),(+1,-1),(-1,0),(+1,0),(-1,+1),(0,+1),(+1,+1), strict '>',
+// 1-px border not written.
+__global__ void census3x3_kernel(const uint8_t* img, size_t pitch, int W, int H, uint8_t* out,
+                                 size_t out_pitch) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x < 1 || y < 1 || x >= W - 1 || y >= H - 1) return;
+    auto P = [&](int dx, int dy) { return img[(size_t)(y + dy) * pitch + x + dx]; };
+    const uint8_t c = P(0, 0);
+    uint32_t v = 0;
+    v |= 0x80u * (P(-1, -1) > c);
+    v |= 0x40u * (P(0, -1) > c);
+    v |= 0x20u * (P(1, -1) > c);
+    v |= 0x10u * (P(-1, 0) > c);
+    v |= 0x08u * (P(1, 0) > c);
+    v |= 0x04u * (P(-1, 1) > c);
+    v |= 0x02u * (P(0, 1) > c);
+    v |= 0x01u * (P(1, 1) > c);
+    out[(size_t)y * out_pitch + x] = uint8_t(v);
+}
+
+int launch9x7(const ct_image* src, uint64_t* dst, size_t dst_pitch_elems, int32_t* status, cudaStream_t s) {
+    CUtensorMap tm;
+    if (int rc = make_tmap_2d(&tm, src->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, src->width, src->height,
+                              src->pitch_bytes, kBoxW, kBoxH))
+        return rc;
+    dim3 grid((src->width + kTX - 1) / kTX, (src->height + kTY - 1) / kTY);
+    census9x7_kernel<<<grid, kNT, 0, s>>>(tm, src->width, src->height, dst, dst_pitch_elems, status);
+    CT_LAUNCH_CHECK();
+    return CT_OK;
+}
+
+}  // namespace census
+
+// ---------------------------------------------------------------------------
+// CensusTransform::CDriver
+// ---------------------------------------------------------------------------
+struct CensusHandle : ct_handle {
+    CensusHandle() : ct_handle(Kind::Census) {}
+    ct_format fmt{};
+    ct_census_params par{};
+};
+
+// ---------------------------------------------------------------------------
+// Census block matcher
+// ---------------------------------------------------------------------------
+struct BmCensusHandle : ct_handle {
+    BmCensusHandle() : ct_handle(Kind::BmCensus) {}
+    ~BmCensusHandle() override {
+        if (device >= 0) cudaSetDevice(device);
+        cudaFree(desc);
+        cudaFree(keys);
+        cudaFree(tmp_lr);
+        cudaFree(tmp_rl);
+    }
+    ct_format fmt{};
+    ct_census_match_params par{};
+    uint64_t* desc = nullptr;      // [2][H][pitch] census descriptors of left, right
+    size_t desc_pitch = 0;         // elements
+    uint32_t* keys = nullptr;      // W*H merge keys (0xFFFFFFFF between calls)
+    uint16_t* tmp_lr = nullptr;    // U16 maps for process_lr when the caller wants only one
+    uint16_t* tmp_rl = nullptr;
+    size_t tmp_pitch = 0;
+    CUtensorMap tm_lb, tm_rb, tm_lm, tm_rm;  // left/right as base (box 128) / match (box 192)
+    int th = 36;
+    uint64_t* left_desc() const { return desc; }
+    uint64_t* right_desc() const { return desc + (size_t)fmt.height * desc_pitch; }
+};
+
+int crosscheck_launch(const ct_image* result, const ct_image* base, const ct_image* other, int tol, int lr,
+                      int32_t* range, cudaStream_t s);  // crosscheck.cu
+
+namespace {
+
+template <typename H>
+H* as(ct_handle* h, Kind k) {
+    return (h && h->kind == k) ? static_cast<H*>(h) : nullptr;
+}
+
+int census_match_pass_maps(BmCensusHandle* h, int dir, const ct_image* disp, const CUtensorMap& tb,
+                           const CUtensorMap& tm, cudaStream_t s) {
+    using namespace cm;
+    const int W = h->fmt.width, H = h->fmt.height, D = h->par.disp_count;
+    MatchArgs a{};
+    a.W = W; a.H = H; a.D = D;
+    a.th = h->th;
+    a.nbatch = (a.th + 2 * kAR) / kRB;
+    a.keys = h->keys;
+    a.out = disp->ptr; a.out_pitch = disp->pitch_bytes; a.out_type = disp->type;
+    a.status = h->d_status;
+    dim3 grid((W + kTWO - 1) / kTWO, (H + a.th - 1) / a.th, (D + kDPC - 1) / kDPC);
+    const size_t smem = smem_bytes(a.th);
+    if (dir == 0) {
+        census_match_kernel<0><<<grid, kNT, smem, s>>>(tb, tm, a);
+    } else {
+        census_match_kernel<1><<<grid, kNT, smem, s>>>(tb, tm, a);
+    }
+    CT_LAUNCH_CHECK();
+    if (grid.z > 1) {
+        keys_finalize_kernel<<<dim3((W + 255) / 256, H), 256, 0, s>>>(h->keys, W, H, kAR, disp->ptr,
+                                                                      disp->pitch_bytes, disp->type);
+        CT_LAUNCH_CHECK();
+    }
+    return CT_OK;
+}
+
+int census_match_pass(BmCensusHandle* h, int dir, const ct_image* disp, cudaStream_t s) {
+    return dir == 0 ? census_match_pass_maps(h, 0, disp, h->tm_lb, h->tm_rm, s)
+                    : census_match_pass_maps(h, 1, disp, h->tm_rb, h->tm_lm, s);
+}
+
+int census_both(BmCensusHandle* h, const ct_image* left, const ct_image* right, cudaStream_t s) {
+    if (int rc = census::launch9x7(left, h->left_desc(), h->desc_pitch, h->d_status, s)) return rc;
+    if (int rc = census::launch9x7(right, h->right_desc(), h->desc_pitch, h->d_status, s)) return rc;
+    return CT_OK;
+}
+
+}  // namespace
+
+static int set_smem_attrs() {
+    static bool done = false;
+    if (done) return CT_OK;
+    const int smem = (int)cm::smem_bytes(96);
+    CT_CUDA_TRY(cudaFuncSetAttribute(cm::census_match_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CT_CUDA_TRY(cudaFuncSetAttribute(cm::census_match_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    done = true;
+    return CT_OK;
+}
+
+}  // namespace ct
+
+using namespace ct;
+
+extern "C" {
+
+int ct_census_create(ct_handle** out) {
+    clear_error();
+    if (!out) return fail(CT_EINVAL, "null output handle pointer");
+    *out = new CensusHandle();
+    return CT_OK;
+}
+
+int ct_census_configure(ct_handle* hh, int32_t device, const ct_format* fmt, const ct_census_params* p) {
+    clear_error();
+    auto* h = as<CensusHandle>(hh, Kind::Census);
+    if (!h) return fail(CT_ESTATE, "not a census handle");
+    if (!fmt || !p) return fail(CT_EINVAL, "null format or parameters");
+    if (fmt->type != CT_PIX_U8) return fail(CT_ETYPE, "census input must be U8 (TPixel_Lum_UInt8)");
+    if (fmt->width < 1 || fmt->height < 1) return fail(CT_EINVAL, "bad size");
+    if (p->window != CT_CENSUS_9X7 && p->window != CT_CENSUS_3X3) return fail(CT_EINVAL, "unknown census window");
+    if (int rc = use_device(device)) return rc;
+    h->device = device;
+    if (int rc = h->init_status()) return rc;
+    h->fmt = *fmt;
+    h->par = *p;
+    h->configured = true;
+    return CT_OK;
+}
+
+int ct_census_process(ct_handle* hh, const ct_image* dst, const ct_image* src, ct_stream stream) {
+    clear_error();
+    auto* h = as<CensusHandle>(hh, Kind::Census);
+    if (!h) return fail(CT_ESTATE, "not a census handle");
+    if (!h->configured) return fail(CT_ESTATE, "process before configure");
+    if (int rc = check_image(src, "src", 1u << CT_PIX_U8)) return rc;
+    const uint32_t dt = h->par.window == CT_CENSUS_9X7 ? (1u << CT_PIX_U64) : (1u << CT_PIX_U8);
+    if (int rc = check_image(dst, "dst", dt)) return rc;
+    if (int rc = check_same_size(dst, src, "dst", "src")) return rc;
+    if (src->width != h->fmt.width || src->height != h->fmt.height)
+        return fail(CT_EFORMAT, "image size differs from the configured format");
+    if (int rc = use_device(h->device)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    h->last_stream = s;
+    if (h->par.window == CT_CENSUS_9X7) {
+        return census::launch9x7(src, static_cast<uint64_t*>(dst->ptr), dst->pitch_bytes / 8, h->d_status, s);
+    }
+    dim3 blk(32, 8), grid((src->width + 31) / 32, (src->height + 7) / 8);
+    census::census3x3_kernel<<<grid, blk, 0, s>>>(static_cast<const uint8_t*>(src->ptr), src->pitch_bytes,
+                                                  src->width, src->height, static_cast<uint8_t*>(dst->ptr),
+                                                  dst->pitch_bytes);
+    CT_LAUNCH_CHECK();
+    return CT_OK;
+}
+
+int ct_bm_census_create(ct_handle** out) {
+    clear_error();
+    if (!out) return fail(CT_EINVAL, "null output handle pointer");
+    *out = new BmCensusHandle();
+    return CT_OK;
+}
+
+int ct_bm_census_configure(ct_handle* hh, int32_t device, const ct_format* fmt, const ct_census_match_params* p) {
+    clear_error();
+    auto* h = as<BmCensusHandle>(hh, Kind::BmCensus);
+    if (!h) return fail(CT_ESTATE, "not a census matcher handle");
+    if (!fmt || !p) return fail(CT_EINVAL, "null format or parameters");
+    if (fmt->type != CT_PIX_U8) return fail(CT_ETYPE, "matcher input must be U8 (TPixel_Lum_UInt8)");
+    if (fmt->width < 8 || fmt->height < 8 || fmt->width > 32768 || fmt->height > 32768)
+        return fail(CT_EINVAL, "image size %dx%d out of range (8..32768)", fmt->width, fmt->height);
+    if (p->disp_count < 1 || p->disp_count > 256) return fail(CT_EINVAL, "disp_count must be 1..256");
+    if (p->agg_radius != cm::kAR) return fail(CT_EINVAL, "only agg_radius 2 (5x5) is built");
+    if (p->reserved != 0) return fail(CT_EINVAL, "reserved must be 0");
+    if (int rc = use_device(device)) return rc;
+    if (int rc = set_smem_attrs()) return rc;
+    // release a previous configuration
+    cudaFree(h->desc); cudaFree(h->keys); cudaFree(h->tmp_lr); cudaFree(h->tmp_rl);
+    h->desc = nullptr; h->keys = nullptr; h->tmp_lr = nullptr; h->tmp_rl = nullptr;
+    h->device = device;
+    if (int rc = h->init_status()) return rc;
+    const int W = fmt->width, H = fmt->height;
+    h->desc_pitch = ((size_t)W + 31) / 32 * 32;
+    if (cudaMalloc(&h->desc, 2 * h->desc_pitch * H * 8) != cudaSuccess) return fail(CT_ENOMEM, "descriptor scratch");
+    if (cudaMalloc(&h->keys, (size_t)W * H * 4) != cudaSuccess) return fail(CT_ENOMEM, "key scratch");
+    CT_CUDA_TRY(cudaMemset(h->keys, 0xFF, (size_t)W * H * 4));
+    h->tmp_pitch = ((size_t)W * 2 + 255) / 256 * 256;
+    if (cudaMalloc(&h->tmp_lr, h->tmp_pitch * H) != cudaSuccess) return fail(CT_ENOMEM, "map scratch");
+    if (cudaMalloc(&h->tmp_rl, h->tmp_pitch * H) != cudaSuccess) return fail(CT_ENOMEM, "map scratch");
+    const uint64_t pb = h->desc_pitch * 8;
+    using namespace cm;
+    if (int rc = make_tmap_2d(&h->tm_lb, h->left_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kTWV, kRB)) return rc;
+    if (int rc = make_tmap_2d(&h->tm_rb, h->right_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kTWV, kRB)) return rc;
+    if (int rc = make_tmap_2d(&h->tm_lm, h->left_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kMW, kRB)) return rc;
+    if (int rc = make_tmap_2d(&h->tm_rm, h->right_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kMW, kRB)) return rc;
+    h->fmt = *fmt;
+    h->par = *p;
+    h->configured = true;
+    return CT_OK;
+}
+
+static int check_match_io(BmCensusHandle* h, const ct_image* left, const ct_image* right) {
+    if (!h->configured) return fail(CT_ESTATE, "process before configure");
+    if (int rc = check_image(left, "left", 1u << CT_PIX_U8)) return rc;
+    if (int rc = check_image(right, "right", 1u << CT_PIX_U8)) return rc;
+    if (int rc = check_same_size(left, right, "left", "right")) return rc;
+    if (left->width != h->fmt.width || left->height != h->fmt.height)
+        return fail(CT_EFORMAT, "image size differs from the configured format");
+    return CT_OK;
+}
+
+static int check_disp_out(BmCensusHandle* h, const ct_image* d, const char* name) {
+    if (int rc = check_image(d, name, (1u << CT_PIX_U8) | (1u << CT_PIX_U16))) return rc;
+    if (d->width != h->fmt.width || d->height != h->fmt.height)
+        return fail(CT_EFORMAT, "%s size differs from the configured format", name);
+    if (d->type == CT_PIX_U8 && h->par.disp_count > 255) return fail(CT_ETYPE, "U8 maps need disp_count <= 255");
+    return CT_OK;
+}
+
+int ct_bm_census_process(ct_handle* hh, const ct_image* disp, const ct_image* left, const ct_image* right,
+                         ct_stream stream) {
+    clear_error();
+    auto* h = as<BmCensusHandle>(hh, Kind::BmCensus);
+    if (!h) return fail(CT_ESTATE, "not a census matcher handle");
+    if (int rc = check_match_io(h, left, right)) return rc;
+    if (int rc = check_disp_out(h, disp, "disp")) return rc;
+    if (int rc = use_device(h->device)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    h->last_stream = s;
+    if (int rc = census_both(h, left, right, s)) return rc;
+    return census_match_pass(h, h->par.left_to_right ? 0 : 1, disp, s);
+}
+
+int ct_bm_census_process_lr(ct_handle* hh, const ct_image* disp_lr, const ct_image* disp_rl,
+                            const ct_image* disp_checked, int32_t tol, const ct_image* left,
+                            const ct_image* right, ct_stream stream) {
+    clear_error();
+    auto* h = as<BmCensusHandle>(hh, Kind::BmCensus);
+    if (!h) return fail(CT_ESTATE, "not a census matcher handle");
+    if (int rc = check_match_io(h, left, right)) return rc;
+    if (!disp_lr && !disp_rl && !disp_checked) return fail(CT_EINVAL, "no output requested");
+    if (tol < 0) return fail(CT_EINVAL, "tol must be >= 0");
+    int32_t t = -1;
+    for (const ct_image* d : {disp_lr, disp_rl, disp_checked}) {
+        if (!d) continue;
+        if (int rc = check_disp_out(h, d, "disp")) return rc;
+        if (t >= 0 && d->type != t) return fail(CT_ETYPE, "all output maps must have the same type");
+        t = d->type;
+    }
+    if (int rc = use_device(h->device)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    h->last_stream = s;
+    if (int rc = census_both(h, left, right, s)) return rc;
+    const int W = h->fmt.width, H = h->fmt.height;
+    ct_image tlr{h->tmp_lr, h->tmp_pitch, W, H, t, 0};
+    ct_image trl{h->tmp_rl, h->tmp_pitch, W, H, t, 0};
+    if (t == CT_PIX_U8) { tlr.pitch_bytes = trl.pitch_bytes = h->tmp_pitch; }
+    const ct_image* lr = disp_lr ? disp_lr : &tlr;
+    const ct_image* rl = disp_rl ? disp_rl : &trl;
+    const bool need_lr = disp_lr || disp_checked, need_rl = disp_rl || disp_checked;
+    if (need_lr)
+        if (int rc = census_match_pass(h, 0, lr, s)) return rc;
+    if (need_rl)
+        if (int rc = census_match_pass(h, 1, rl, s)) return rc;
+    if (disp_checked) return crosscheck_launch(disp_checked, lr, rl, tol, 1, nullptr, s);
+    return CT_OK;
+}
+
+int ct_bm_census_match_desc(ct_handle* hh, const ct_image* disp, const ct_image* desc_base,
+                            const ct_image* desc_match, int32_t left_to_right, ct_stream stream) {
+    clear_error();
+    auto* h = as<BmCensusHandle>(hh, Kind::BmCensus);
+    if (!h) return fail(CT_ESTATE, "not a census matcher handle");
+    if (!h->configured) return fail(CT_ESTATE, "process before configure");
+    if (int rc = check_image(desc_base, "desc_base", 1u << CT_PIX_U64)) return rc;
+    if (int rc = check_image(desc_match, "desc_match", 1u << CT_PIX_U64)) return rc;
+    if (int rc = check_same_size(desc_base, desc_match, "desc_base", "desc_match")) return rc;
+    if (desc_base->width != h->fmt.width || desc_base->height != h->fmt.height)
+        return fail(CT_EFORMAT, "descriptor size differs from the configured format");
+    if (int rc = check_disp_out(h, disp, "disp")) return rc;
+    if (int rc = use_device(h->device)) return rc;
+    const int W = h->fmt.width, H = h->fmt.height;
+    CUtensorMap tb, tm;
+    if (int rc = make_tmap_2d(&tb, desc_base->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, desc_base->pitch_bytes,
+                              cm::kTWV, cm::kRB))
+        return rc;
+    if (int rc = make_tmap_2d(&tm, desc_match->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H,
+                              desc_match->pitch_bytes, cm::kMW, cm::kRB))
+        return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    h->last_stream = s;
+    return census_match_pass_maps(h, left_to_right ? 0 : 1, disp, tb, tm, s);
+}
+
+}  // extern "C"

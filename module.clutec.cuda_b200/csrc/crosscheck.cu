@@ -1,0 +1,173 @@
+// crosscheck.cu — CrossCheckDisparityMaps::CDriver.
+//
+// Per pixel (CrossCheckDisparityMaps.cu:63-110): a base pixel holding a
+// disparity d is kept iff the other map at x -/+ d holds a disparity within
+// disp_delta_thresh of d; otherwise it becomes Inconsistent. Non-disparity
+// codes are copied through. The kept range is reduced on the device with one
+// warp reduction and one atomic per warp, into a word pair that a memset
+// clears (min is stored as INT_MAX - d so that both halves reduce with max).
+#include "ct_internal.h"
+#include "ct_device.cuh"
+
+namespace ct {
+
+namespace {
+
+template <typename T>
+__device__ __forceinline__ bool decode(T v, int& d);
+
+template <>
+__device__ __forceinline__ bool decode<uint8_t>(uint8_t v, int& d) {
+    d = v;
+    return v != 0xFF;
+}
+template <>
+__device__ __forceinline__ bool decode<uint16_t>(uint16_t v, int& d) {
+    d = int(v) - 1;
+    return v >= CT_DISP_FIRST && v <= CT_DISP_LAST;
+}
+
+template <typename T>
+__device__ __forceinline__ T inconsistent();
+template <>
+__device__ __forceinline__ uint8_t inconsistent<uint8_t>() { return 0xFF; }
+template <>
+__device__ __forceinline__ uint16_t inconsistent<uint16_t>() { return CT_DISP_INCONSISTENT; }
+
+template <typename T>
+__global__ void crosscheck_kernel(T* out, size_t po, const T* base, size_t pb, const T* other, size_t pt, int W,
+                                  int H, int tol, int lr, int32_t* range) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    int kept = -1;
+    if (x < W) {
+        const T v = reinterpret_cast<const T*>(reinterpret_cast<const char*>(base) + (size_t)y * pb)[x];
+        T r = v;
+        int d;
+        if (decode<T>(v, d)) {
+            const int xo = lr ? x - d : x + d;
+            r = inconsistent<T>();
+            if (xo >= 0 && xo < W) {
+                const T vo = reinterpret_cast<const T*>(reinterpret_cast<const char*>(other) + (size_t)y * pt)[xo];
+                int dd;
+                if (decode<T>(vo, dd) && abs(dd - d) <= tol) {
+                    r = v;
+                    kept = d;
+                }
+            }
+        }
+        reinterpret_cast<T*>(reinterpret_cast<char*>(out) + (size_t)y * po)[x] = r;
+    }
+    if (range) {
+        const unsigned mn = __reduce_max_sync(0xffffffffu, kept >= 0 ? unsigned(0x7FFFFFFF - kept) : 0u);
+        const unsigned mx = __reduce_max_sync(0xffffffffu, unsigned(kept + 1));
+        if ((threadIdx.x & 31) == 0) {
+            if (mn) atomicMax(reinterpret_cast<unsigned*>(&range[0]), mn);
+            if (mx) atomicMax(reinterpret_cast<unsigned*>(&range[1]), mx);
+        }
+    }
+}
+
+struct CrossCheckHandle : ct_handle {
+    CrossCheckHandle() : ct_handle(Kind::CrossCheck) {}
+    ~CrossCheckHandle() override {
+        if (device >= 0) cudaSetDevice(device);
+        cudaFree(range);
+    }
+    ct_format fmt{};
+    ct_crosscheck_params par{};
+    int32_t* range = nullptr;  // [2] encoded min / max
+};
+
+}  // namespace
+
+int crosscheck_launch(const ct_image* result, const ct_image* base, const ct_image* other, int tol, int lr,
+                      int32_t* range, cudaStream_t s) {
+    const int W = base->width, H = base->height;
+    dim3 grid((W + 127) / 128, H);
+    if (range) CT_CUDA_TRY(cudaMemsetAsync(range, 0, 2 * sizeof(int32_t), s));
+    if (base->type == CT_PIX_U8) {
+        crosscheck_kernel<uint8_t><<<grid, 128, 0, s>>>(
+            static_cast<uint8_t*>(result->ptr), result->pitch_bytes, static_cast<const uint8_t*>(base->ptr),
+            base->pitch_bytes, static_cast<const uint8_t*>(other->ptr), other->pitch_bytes, W, H, tol, lr, range);
+    } else {
+        crosscheck_kernel<uint16_t><<<grid, 128, 0, s>>>(
+            static_cast<uint16_t*>(result->ptr), result->pitch_bytes, static_cast<const uint16_t*>(base->ptr),
+            base->pitch_bytes, static_cast<const uint16_t*>(other->ptr), other->pitch_bytes, W, H, tol, lr, range);
+    }
+    CT_LAUNCH_CHECK();
+    return CT_OK;
+}
+
+}  // namespace ct
+
+using namespace ct;
+
+extern "C" {
+
+int ct_crosscheck_create(ct_handle** out) {
+    clear_error();
+    if (!out) return fail(CT_EINVAL, "null output handle pointer");
+    *out = new CrossCheckHandle();
+    return CT_OK;
+}
+
+int ct_crosscheck_configure(ct_handle* hh, int32_t device, const ct_format* fmt, const ct_crosscheck_params* p) {
+    clear_error();
+    auto* h = (hh && hh->kind == Kind::CrossCheck) ? static_cast<CrossCheckHandle*>(hh) : nullptr;
+    if (!h) return fail(CT_ESTATE, "not a cross-check handle");
+    if (!fmt || !p) return fail(CT_EINVAL, "null format or parameters");
+    if (fmt->type != CT_PIX_U8 && fmt->type != CT_PIX_U16)
+        return fail(CT_ETYPE, "disparity maps must be U8 or U16");
+    if (fmt->width < 1 || fmt->height < 1) return fail(CT_EINVAL, "bad size");
+    if (p->disp_delta_thresh < 0) return fail(CT_EINVAL, "disp_delta_thresh must be >= 0");
+    if (int rc = use_device(device)) return rc;
+    h->device = device;
+    if (int rc = h->init_status()) return rc;
+    if (!h->range && cudaMalloc(&h->range, 2 * sizeof(int32_t)) != cudaSuccess)
+        return fail(CT_ENOMEM, "range buffer");
+    CT_CUDA_TRY(cudaMemset(h->range, 0, 2 * sizeof(int32_t)));
+    h->fmt = *fmt;
+    h->par = *p;
+    h->configured = true;
+    return CT_OK;
+}
+
+int ct_crosscheck_process(ct_handle* hh, const ct_image* result, const ct_image* disp_base,
+                          const ct_image* disp_other, ct_stream stream) {
+    clear_error();
+    auto* h = (hh && hh->kind == Kind::CrossCheck) ? static_cast<CrossCheckHandle*>(hh) : nullptr;
+    if (!h) return fail(CT_ESTATE, "not a cross-check handle");
+    if (!h->configured) return fail(CT_ESTATE, "process before configure");
+    const uint32_t t = 1u << h->fmt.type;
+    if (int rc = check_image(disp_base, "disp_base", t)) return rc;
+    if (int rc = check_image(disp_other, "disp_other", t)) return rc;
+    if (int rc = check_image(result, "result", t)) return rc;
+    if (int rc = check_same_size(disp_base, disp_other, "disp_base", "disp_other")) return rc;
+    if (int rc = check_same_size(disp_base, result, "disp_base", "result")) return rc;
+    if (disp_base->width != h->fmt.width || disp_base->height != h->fmt.height)
+        return fail(CT_EFORMAT, "map size differs from the configured format");
+    if (int rc = use_device(h->device)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    h->last_stream = s;
+    return crosscheck_launch(result, disp_base, disp_other, h->par.disp_delta_thresh, h->par.left_to_right ? 1 : 0,
+                             h->range, s);
+}
+
+int ct_crosscheck_range(ct_handle* hh, int32_t* disp_min, int32_t* disp_max) {
+    clear_error();
+    auto* h = (hh && hh->kind == Kind::CrossCheck) ? static_cast<CrossCheckHandle*>(hh) : nullptr;
+    if (!h) return fail(CT_ESTATE, "not a cross-check handle");
+    if (!disp_min || !disp_max) return fail(CT_EINVAL, "null output");
+    if (!h->configured) return fail(CT_ESTATE, "range before configure");
+    if (int rc = use_device(h->device)) return rc;
+    if (h->last_stream) CT_CUDA_TRY(cudaStreamSynchronize(h->last_stream));
+    else CT_CUDA_TRY(cudaDeviceSynchronize());
+    uint32_t r[2];
+    CT_CUDA_TRY(cudaMemcpy(r, h->range, sizeof r, cudaMemcpyDeviceToHost));
+    *disp_min = r[0] ? int32_t(0x7FFFFFFF - r[0]) : INT32_MAX;
+    *disp_max = int32_t(r[1]) - 1;
+    return CT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,341 @@
+"""ctstereo — Python mirror of the CluTec.Cuda MultiView driver API over the
+libctstereo C ABI (include/ctstereo.h).
+
+Each reference driver (``BlockMatcherNCC::CDriver`` etc.) is a class with
+``configure(device, fmt, params)`` and ``process(...)``; images are torch CUDA
+tensors (uint8 / int16-as-uint16 / int64-as-uint64 / float32, 2-D, row-major,
+rows 16-byte aligned). Errors raise :class:`CtError`, the counterpart of the
+reference's ``CLU_EXCEPTION``. All calls are asynchronous on the given CUDA
+stream (default: torch's current stream).
+
+The native library must be built (``python module.clutec.cuda_b200/build.py``);
+there is no fallback path: loading fails loudly if the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libctstereo.so"
+
+# status codes (ctstereo.h)
+CT_OK, CT_EINVAL, CT_ETYPE, CT_EFORMAT, CT_ECUDA, CT_ETIMEOUT, CT_ESTATE, CT_ENOMEM = range(8)
+# pixel types
+CT_PIX_U8, CT_PIX_U16, CT_PIX_U64, CT_PIX_F32 = 1, 2, 3, 4
+# EDisparityId codes
+DISP_FIRST, DISP_LAST = 0x0001, 0xFFEF
+DISP_CANNOT_EVALUATE, DISP_INCONSISTENT, DISP_U8_INVALID = 0xFFFF, 0xFFFA, 0xFF
+CENSUS_9X7, CENSUS_3X3 = 0, 1
+
+_STATUS_NAMES = {0: "CT_OK", 1: "CT_EINVAL", 2: "CT_ETYPE", 3: "CT_EFORMAT", 4: "CT_ECUDA",
+                 5: "CT_ETIMEOUT", 6: "CT_ESTATE", 7: "CT_ENOMEM"}
+
+
+class CtError(RuntimeError):
+    """A non-zero status from the C ABI, with ct_last_error_string()."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class ct_image(C.Structure):
+    _fields_ = [("ptr", C.c_void_p), ("pitch_bytes", C.c_size_t), ("width", C.c_int32),
+                ("height", C.c_int32), ("type", C.c_int32), ("reserved", C.c_int32)]
+
+
+class ct_format(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("type", C.c_int32)]
+
+
+class ct_census_params(C.Structure):
+    _fields_ = [("window", C.c_int32)]
+
+
+class ct_census_match_params(C.Structure):
+    _fields_ = [("disp_count", C.c_int32), ("agg_radius", C.c_int32), ("left_to_right", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class ct_sad_params(C.Structure):
+    _fields_ = [("disp_count", C.c_int32), ("radius", C.c_int32), ("left_to_right", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class ct_ncc_params(C.Structure):
+    _fields_ = [("disp_count", C.c_int32), ("radius", C.c_int32), ("left_to_right", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class ct_aw_params(C.Structure):
+    _fields_ = [("disp_count", C.c_int32), ("left_to_right", C.c_int32), ("reserved0", C.c_int32),
+                ("reserved1", C.c_int32)]
+
+
+class ct_crosscheck_params(C.Structure):
+    _fields_ = [("disp_delta_thresh", C.c_int32), ("left_to_right", C.c_int32), ("reserved0", C.c_int32),
+                ("reserved1", C.c_int32)]
+
+
+class ct_pipe_rates(C.Structure):
+    _fields_ = [("popc_per_clk_sm", C.c_double), ("iadd3_per_clk_sm", C.c_double),
+                ("lop3_per_clk_sm", C.c_double), ("vimnmx_per_clk_sm", C.c_double),
+                ("imad_per_clk_sm", C.c_double), ("sm_clock_mhz", C.c_double), ("sm_count", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libctstereo.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} not built: run python module.clutec.cuda_b200/build.py")
+        _lib = C.CDLL(str(LIB_PATH))
+        _declare(_lib)
+    return _lib
+
+
+def _declare(L: C.CDLL) -> None:
+    H = C.c_void_p
+    P = C.POINTER
+    img = P(ct_image)
+    fmt = P(ct_format)
+    L.ct_last_error_string.restype = C.c_char_p
+    L.ct_version.restype = C.c_char_p
+    sigs = {
+        "ct_destroy": [H],
+        "ct_handle_device_status": [H, P(C.c_int32)],
+        "ct_census_create": [P(H)],
+        "ct_census_configure": [H, C.c_int32, fmt, P(ct_census_params)],
+        "ct_census_process": [H, img, img, C.c_void_p],
+        "ct_bm_census_create": [P(H)],
+        "ct_bm_census_configure": [H, C.c_int32, fmt, P(ct_census_match_params)],
+        "ct_bm_census_process": [H, img, img, img, C.c_void_p],
+        "ct_bm_census_process_lr": [H, img, img, img, C.c_int32, img, img, C.c_void_p],
+        "ct_bm_census_match_desc": [H, img, img, img, C.c_int32, C.c_void_p],
+        "ct_bm_sad_create": [P(H)],
+        "ct_bm_sad_configure": [H, C.c_int32, fmt, P(ct_sad_params)],
+        "ct_bm_sad_process": [H, img, img, img, C.c_void_p],
+        "ct_bm_ncc_create": [P(H)],
+        "ct_bm_ncc_configure": [H, C.c_int32, fmt, P(ct_ncc_params)],
+        "ct_bm_ncc_process": [H, img, img, img, img, img, C.c_void_p],
+        "ct_bm_aw_create": [P(H)],
+        "ct_bm_aw_configure": [H, C.c_int32, fmt, P(ct_aw_params)],
+        "ct_bm_aw_process": [H, img, img, img, C.c_void_p],
+        "ct_crosscheck_create": [P(H)],
+        "ct_crosscheck_configure": [H, C.c_int32, fmt, P(ct_crosscheck_params)],
+        "ct_crosscheck_process": [H, img, img, img, C.c_void_p],
+        "ct_crosscheck_range": [H, P(C.c_int32), P(C.c_int32)],
+        "ct_synth_pair": [C.c_int32, C.c_uint64, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                          C.c_void_p, C.c_void_p],
+        "ct_probe_pipe_rates": [C.c_int32, P(ct_pipe_rates)],
+    }
+    for name, args in sigs.items():
+        f = getattr(L, name, None)
+        if f is None:
+            continue
+        f.argtypes = args
+        f.restype = C.c_int
+
+
+def exported_symbols():
+    """Names of the ct_* entry points declared in include/ctstereo.h."""
+    hdr = (_PKG.parent / "include" / "ctstereo.h").read_text()
+    return sorted(set(re.findall(r"\b(ct_[a-z0-9_]+)\s*\(", hdr)))
+
+
+def check(rc: int) -> None:
+    if rc != CT_OK:
+        raise CtError(rc, lib().ct_last_error_string().decode())
+
+
+def version() -> str:
+    return lib().ct_version().decode()
+
+
+# ---------------------------------------------------------------------------
+# tensors <-> ct_image
+# ---------------------------------------------------------------------------
+
+def _pix_type(t) -> int:
+    import torch
+    m = {torch.uint8: CT_PIX_U8, torch.int16: CT_PIX_U16, torch.uint16: CT_PIX_U16,
+         torch.int64: CT_PIX_U64, torch.uint64: CT_PIX_U64, torch.float32: CT_PIX_F32}
+    if t.dtype not in m:
+        raise CtError(CT_ETYPE, f"tensor dtype {t.dtype} has no ctstereo pixel type")
+    return m[t.dtype]
+
+
+def image(t) -> ct_image:
+    """Describes a 2-D CUDA tensor (row stride may exceed the width) as a ct_image."""
+    if t.dim() != 2 or t.stride(1) != 1:
+        raise CtError(CT_EINVAL, "images must be 2-D tensors with unit column stride")
+    return ct_image(t.data_ptr(), t.stride(0) * t.element_size(), t.shape[1], t.shape[0], _pix_type(t), 0)
+
+
+def _img_ref(t):
+    return None if t is None else C.byref(image(t))
+
+
+def _stream(stream):
+    import torch
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+
+def alloc_image(height: int, width: int, dtype, device="cuda"):
+    """A 2-D tensor whose row pitch is a multiple of 256 bytes (TMA-friendly)."""
+    import torch
+    esz = torch.empty(0, dtype=dtype).element_size()
+    pitch = -(-width * esz // 256) * 256 // esz
+    return torch.empty((height, pitch), dtype=dtype, device=device)[:, :width]
+
+
+class _Driver:
+    _create = None
+
+    def __init__(self):
+        h = C.c_void_p()
+        check(getattr(lib(), self._create)(C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().ct_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def device_status(self) -> int:
+        v = C.c_int32()
+        check(lib().ct_handle_device_status(self._h, C.byref(v)))
+        return v.value
+
+
+def _fmt(width, height, type_=CT_PIX_U8):
+    return ct_format(width, height, type_)
+
+
+class CensusTransform(_Driver):
+    """CensusTransform::CDriver (CensusTransform.h:44-70)."""
+    _create = "ct_census_create"
+
+    def configure(self, device: int, width: int, height: int, window: int = CENSUS_9X7):
+        check(lib().ct_census_configure(self._h, device, C.byref(_fmt(width, height)),
+                                        C.byref(ct_census_params(window))))
+
+    def process(self, dst, src, stream=None):
+        check(lib().ct_census_process(self._h, _img_ref(dst), _img_ref(src), _stream(stream)))
+
+
+class BlockMatcherCensus(_Driver):
+    """Census (9x7 / 64-bit) + Hamming + 5x5 box + WTA matcher."""
+    _create = "ct_bm_census_create"
+
+    def configure(self, device: int, width: int, height: int, disp_count: int, left_to_right: bool = True,
+                  agg_radius: int = 2):
+        check(lib().ct_bm_census_configure(self._h, device, C.byref(_fmt(width, height)), C.byref(
+            ct_census_match_params(disp_count, agg_radius, int(left_to_right), 0))))
+
+    def process(self, disp, left, right, stream=None):
+        check(lib().ct_bm_census_process(self._h, _img_ref(disp), _img_ref(left), _img_ref(right),
+                                         _stream(stream)))
+
+    def match_desc(self, disp, desc_base, desc_match, left_to_right=True, stream=None):
+        """Matching on precomputed 9x7 census descriptors (int64 tensors)."""
+        check(lib().ct_bm_census_match_desc(self._h, _img_ref(disp), _img_ref(desc_base), _img_ref(desc_match),
+                                            int(left_to_right), _stream(stream)))
+
+    def process_lr(self, left, right, disp_lr=None, disp_rl=None, disp_checked=None, tol=1, stream=None):
+        check(lib().ct_bm_census_process_lr(self._h, _img_ref(disp_lr), _img_ref(disp_rl),
+                                            _img_ref(disp_checked), tol, _img_ref(left), _img_ref(right),
+                                            _stream(stream)))
+
+
+class BlockMatcherSAD1(_Driver):
+    """BlockMatcherSAD1::CDriver, exhaustive (2r+1)^2 SAD + WTA."""
+    _create = "ct_bm_sad_create"
+
+    def configure(self, device: int, width: int, height: int, disp_count: int, radius: int = 4,
+                  left_to_right: bool = True):
+        check(lib().ct_bm_sad_configure(self._h, device, C.byref(_fmt(width, height)),
+                                        C.byref(ct_sad_params(disp_count, radius, int(left_to_right), 0))))
+
+    def process(self, disp, left, right, stream=None):
+        check(lib().ct_bm_sad_process(self._h, _img_ref(disp), _img_ref(left), _img_ref(right),
+                                      _stream(stream)))
+
+
+class BlockMatcherNCC(_Driver):
+    """BlockMatcherNCC::CDriver with an FP32 (unquantised) score."""
+    _create = "ct_bm_ncc_create"
+
+    def configure(self, device: int, width: int, height: int, disp_count: int, radius: int = 5):
+        check(lib().ct_bm_ncc_configure(self._h, device, C.byref(_fmt(width, height)),
+                                        C.byref(ct_ncc_params(disp_count, radius, 1, 0))))
+
+    def process(self, disp, left, right, score=None, disp_init=None, stream=None):
+        check(lib().ct_bm_ncc_process(self._h, _img_ref(disp), _img_ref(score), _img_ref(left),
+                                      _img_ref(right), _img_ref(disp_init), _stream(stream)))
+
+
+class BlockMatcherAW(_Driver):
+    """BlockMatcherAW1/AW2: best of 5 shifted 7x7 SAD windows + sub-pixel."""
+    _create = "ct_bm_aw_create"
+
+    def configure(self, device: int, width: int, height: int, disp_count: int):
+        check(lib().ct_bm_aw_configure(self._h, device, C.byref(_fmt(width, height)),
+                                       C.byref(ct_aw_params(disp_count, 1, 0, 0))))
+
+    def process(self, disp, left, right, stream=None):
+        check(lib().ct_bm_aw_process(self._h, _img_ref(disp), _img_ref(left), _img_ref(right),
+                                     _stream(stream)))
+
+
+class CrossCheckDisparityMaps(_Driver):
+    """CrossCheckDisparityMaps::CDriver."""
+    _create = "ct_crosscheck_create"
+
+    def configure(self, device: int, width: int, height: int, type_: int = CT_PIX_U8,
+                  disp_delta_thresh: int = 1, left_to_right: bool = True):
+        check(lib().ct_crosscheck_configure(self._h, device, C.byref(_fmt(width, height, type_)),
+                                            C.byref(ct_crosscheck_params(disp_delta_thresh,
+                                                                         int(left_to_right), 0, 0))))
+
+    def process(self, result, disp_base, disp_other, stream=None):
+        check(lib().ct_crosscheck_process(self._h, _img_ref(result), _img_ref(disp_base),
+                                          _img_ref(disp_other), _stream(stream)))
+
+    def disp_range(self):
+        lo, hi = C.c_int32(), C.c_int32()
+        check(lib().ct_crosscheck_range(self._h, C.byref(lo), C.byref(hi)))
+        return lo.value, hi.value
+
+
+def synth_pair(kind: int, seed: int, width: int, height: int, dmax: int):
+    """Seeded synthetic pair -> (left u8, right u8, gt int16, occ u8) numpy arrays."""
+    import numpy as np
+    L = np.empty((height, width), np.uint8)
+    R = np.empty((height, width), np.uint8)
+    G = np.empty((height, width), np.int16)
+    O = np.empty((height, width), np.uint8)
+    check(lib().ct_synth_pair(kind, seed, width, height, dmax, L.ctypes.data, R.ctypes.data, G.ctypes.data,
+                              O.ctypes.data))
+    return L, R, G, O
+
+
+def probe_pipe_rates(device: int = 0) -> dict:
+    r = ct_pipe_rates()
+    check(lib().ct_probe_pipe_rates(device, C.byref(r)))
+    return {k: getattr(r, k) for k, _ in ct_pipe_rates._fields_ if k != "reserved"}

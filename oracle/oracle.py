@@ -1,0 +1,165 @@
+"""ctypes loader for the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline / reference legs of bench.py as the checker. The product code
+never imports this module.
+
+Every function takes and returns numpy arrays; disparities are int16 with -1
+for invalid pixels (and -2 for cross-check failures).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+_DIR = Path(__file__).resolve().parent
+LIB_PATH = _DIR / "liboracle.so"
+_lib = None
+
+
+def build() -> Path:
+    """Builds liboracle.so with the Makefile next to this file."""
+    subprocess.run(["make", "-s", "-C", str(_DIR)], check=True)
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        _lib = C.CDLL(str(LIB_PATH))
+        vp, i = C.c_void_p, C.c_int
+        _lib.or_num_threads.restype = i
+        _lib.or_set_threads.argtypes = [i]
+        _lib.or_census3x3.argtypes = [vp, i, i, i, vp, i]
+        _lib.or_census9x7.argtypes = [vp, i, i, i, vp, i]
+        _lib.or_match_census_desc.argtypes = [vp, vp, i, i, i, i, i, vp, vp, vp, i]
+        _lib.or_match_census.argtypes = [vp, vp, i, i, i, i, i, i, vp, vp, vp, i]
+        _lib.or_match_sad.argtypes = [vp, vp, i, i, i, i, i, i, vp, vp]
+        _lib.or_match_aw.argtypes = [vp, vp, i, i, i, i, vp, vp, vp, vp]
+        _lib.or_match_ncc.argtypes = [vp, vp, i, i, i, i, i, vp, vp, vp]
+        _lib.or_crosscheck.argtypes = [vp, vp, i, i, i, i, vp, vp]
+    return _lib
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+def _u8(a):
+    a = np.ascontiguousarray(a, dtype=np.uint8)
+    assert a.ndim == 2
+    return a
+
+
+def num_threads() -> int:
+    return lib().or_num_threads()
+
+
+def set_threads(n: int) -> None:
+    lib().or_set_threads(n)
+
+
+def census9x7(img):
+    img = _u8(img)
+    H, W = img.shape
+    out = np.empty((H, W), np.uint64)
+    lib().or_census9x7(_p(img), W, H, W, _p(out), W)
+    return out
+
+
+def census3x3(img, fill=0):
+    img = _u8(img)
+    H, W = img.shape
+    out = np.full((H, W), fill, np.uint8)
+    lib().or_census3x3(_p(img), W, H, W, _p(out), W)
+    return out
+
+
+def match_census(L, R, D, r=2, left_to_right=True, curve_shift=None):
+    """-> (disp int16, best cost int32[, curve uint8 HxWxD])"""
+    L, R = _u8(L), _u8(R)
+    H, W = L.shape
+    disp = np.empty((H, W), np.int16)
+    cost = np.empty((H, W), np.int32)
+    curve = None
+    if curve_shift is not None:
+        curve = np.full((H, W, D), 255, np.uint8)
+    lib().or_match_census(_p(L), _p(R), W, H, W, D, r, 0 if left_to_right else 1, _p(disp), _p(cost),
+                          _p(curve) if curve is not None else None, curve_shift or 0)
+    return (disp, cost) if curve is None else (disp, cost, curve)
+
+
+def match_census_desc(cb, cm, D, r=2, left_to_right=True):
+    cb = np.ascontiguousarray(cb, np.uint64)
+    cm = np.ascontiguousarray(cm, np.uint64)
+    H, W = cb.shape
+    disp = np.empty((H, W), np.int16)
+    cost = np.empty((H, W), np.int32)
+    lib().or_match_census_desc(_p(cb), _p(cm), W, H, D, r, 0 if left_to_right else 1, _p(disp), _p(cost),
+                               None, 0)
+    return disp, cost
+
+
+def match_sad(L, R, D, r=4, left_to_right=True):
+    L, R = _u8(L), _u8(R)
+    H, W = L.shape
+    disp = np.empty((H, W), np.int16)
+    cost = np.empty((H, W), np.int32)
+    lib().or_match_sad(_p(L), _p(R), W, H, W, D, r, 0 if left_to_right else 1, _p(disp), _p(cost))
+    return disp, cost
+
+
+def match_aw(L, R, D):
+    """-> (disp int16, cost int32, sub32 float32, sub64 float64)"""
+    L, R = _u8(L), _u8(R)
+    H, W = L.shape
+    disp = np.empty((H, W), np.int16)
+    cost = np.empty((H, W), np.int32)
+    s32 = np.empty((H, W), np.float32)
+    s64 = np.empty((H, W), np.float64)
+    lib().or_match_aw(_p(L), _p(R), W, H, W, D, _p(disp), _p(cost), _p(s32), _p(s64))
+    return disp, cost, s32, s64
+
+
+def match_ncc(L, R, D, r=5):
+    """-> (disp int16, score32 float32, score64 float64)"""
+    L, R = _u8(L), _u8(R)
+    H, W = L.shape
+    disp = np.empty((H, W), np.int16)
+    s32 = np.empty((H, W), np.float32)
+    s64 = np.empty((H, W), np.float64)
+    lib().or_match_ncc(_p(L), _p(R), W, H, W, D, r, _p(disp), _p(s32), _p(s64))
+    return disp, s32, s64
+
+
+def crosscheck(base, other, tol=1, left_to_right=True):
+    """-> (out int16 with -2 = inconsistent, (min, max))"""
+    base = np.ascontiguousarray(base, np.int16)
+    other = np.ascontiguousarray(other, np.int16)
+    H, W = base.shape
+    out = np.empty((H, W), np.int16)
+    rng = np.zeros(2, np.int32)
+    lib().or_crosscheck(_p(base), _p(other), W, H, tol, 1 if left_to_right else 0, _p(out), _p(rng))
+    return out, (int(rng[0]), int(rng[1]))
+
+
+# ---- encodings of the library's output maps --------------------------------
+
+def to_u8(disp):
+    """int16 oracle map -> the library's U8 encoding (255 = not a disparity)."""
+    d = np.asarray(disp)
+    return np.where(d >= 0, d, 255).astype(np.uint8)
+
+
+def to_u16(disp):
+    """int16 oracle map -> EDisparityId U16 encoding (d+1; 0xFFFF cannot
+    evaluate; 0xFFFA inconsistent)."""
+    d = np.asarray(disp).astype(np.int32)
+    out = np.where(d >= 0, d + 1, 0xFFFF)
+    out = np.where(d == -2, 0xFFFA, out)
+    return out.astype(np.uint16)

@@ -1,0 +1,60 @@
+"""C ABI checks that need no GPU: the library loads, exports every entry
+point include/ctstereo.h declares, and rejects bad arguments with status codes
+(never exceptions across the ABI, never a device call)."""
+import ctypes as C
+
+import pytest
+
+
+def test_library_loads_and_versions(ct):
+    assert "sm_100a" in ct.version()
+
+
+def test_every_declared_symbol_is_exported(ct):
+    names = ct.exported_symbols()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(ct.lib(), n)]
+    assert not missing, missing
+
+
+def test_create_destroy_each_kind(ct):
+    for cls in (ct.CensusTransform, ct.BlockMatcherCensus, ct.BlockMatcherSAD1, ct.BlockMatcherNCC,
+                ct.BlockMatcherAW, ct.CrossCheckDisparityMaps):
+        d = cls()
+        d.close()
+        d.close()  # idempotent
+
+
+def test_null_arguments_are_rejected(ct):
+    L = ct.lib()
+    assert L.ct_census_create(None) == ct.CT_EINVAL
+    h = C.c_void_p()
+    assert L.ct_census_create(C.byref(h)) == ct.CT_OK
+    assert L.ct_census_configure(h, 0, None, None) == ct.CT_EINVAL
+    assert b"null" in L.ct_last_error_string()
+    # wrong handle kind
+    assert L.ct_bm_census_process(h, None, None, None, None) == ct.CT_ESTATE
+    assert L.ct_destroy(h) == ct.CT_OK
+    assert L.ct_destroy(None) == ct.CT_OK
+
+
+def test_parameter_validation_before_any_device_call(ct):
+    m = ct.BlockMatcherCensus()
+    with pytest.raises(ct.CtError) as e:
+        m.configure(0, 640, 480, disp_count=0)
+    assert e.value.code == ct.CT_EINVAL
+    with pytest.raises(ct.CtError) as e:
+        m.configure(0, 640, 480, disp_count=64, agg_radius=3)
+    assert e.value.code == ct.CT_EINVAL
+    with pytest.raises(ct.CtError) as e:
+        m.configure(0, 4, 4, disp_count=64)
+    assert e.value.code == ct.CT_EINVAL
+    # process before configure
+    L = ct.lib()
+    img = ct.ct_image(1 << 20, 640, 640, 480, ct.CT_PIX_U8, 0)
+    rc = L.ct_bm_census_process(m._h, C.byref(img), C.byref(img), C.byref(img), None)
+    assert rc == ct.CT_ESTATE
+
+
+def test_synth_rejects_bad_kind(ct):
+    assert ct.lib().ct_synth_pair(9, 1, 16, 16, 8, None, None, None, None) == ct.CT_EINVAL

@@ -1,0 +1,147 @@
+"""Census path on the GPU against the CPU oracle: bit-exact descriptors,
+disparity maps (both directions, U8 and U16 encodings) and cross-check."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import to_dev
+
+pytestmark = pytest.mark.gpu
+
+
+def pair(ct, kind, seed, W, H, dmax):
+    L, R, G, O = ct.synth_pair(kind, seed, W, H, dmax)
+    return L, R
+
+
+@pytest.mark.parametrize("W,H", [(67, 43), (640, 480), (1920, 1080)])
+def test_census9x7_bit_exact(ct, oracle, cuda, W, H):
+    L, _ = pair(ct, 2, 3, W, H, 64)
+    ctr = ct.CensusTransform()
+    ctr.configure(0, W, H, ct.CENSUS_9X7)
+    src = to_dev(L, cuda)
+    dst = ct.alloc_image(H, W, torch.int64, cuda)
+    ctr.process(dst, src)
+    torch.cuda.synchronize()
+    got = dst.cpu().numpy().view(np.uint64)
+    np.testing.assert_array_equal(got, oracle.census9x7(L))
+    assert ctr.device_status() == 0
+
+
+def test_census3x3_reference_semantics(ct, oracle, cuda):
+    W, H = 95, 61
+    L, _ = pair(ct, 1, 4, W, H, 30)
+    ctr = ct.CensusTransform()
+    ctr.configure(0, W, H, ct.CENSUS_3X3)
+    src = to_dev(L, cuda)
+    dst = ct.alloc_image(H, W, torch.uint8, cuda)
+    dst.fill_(0xAB)
+    ctr.process(dst, src)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(dst.cpu().numpy(), oracle.census3x3(L, fill=0xAB))
+
+
+CASES = [
+    # W, H, D, generator kind
+    (67, 43, 13, 1),
+    (130, 37, 64, 1),     # exactly one CTA of disparities
+    (333, 111, 128, 2),   # two disparity CTAs merged through global keys
+    (257, 90, 200, 2),    # partial last warp group
+    (96, 64, 1, 1),       # D = 1
+    (640, 480, 64, 1),
+]
+
+
+@pytest.mark.parametrize("W,H,D,kind", CASES)
+@pytest.mark.parametrize("lr", [True, False])
+def test_census_match_bit_exact(ct, oracle, cuda, W, H, D, kind, lr):
+    L, R = pair(ct, kind, W * 7 + D, W, H, max(1, D - 1))
+    m = ct.BlockMatcherCensus()
+    m.configure(0, W, H, D, left_to_right=lr)
+    dl, dr = to_dev(L, cuda), to_dev(R, cuda)
+    want, _ = oracle.match_census(L, R, D, 2, lr)
+    for dtype, enc in ((torch.uint8, oracle.to_u8), (torch.int16, oracle.to_u16)):
+        if dtype == torch.uint8 and D > 255:
+            continue
+        out = ct.alloc_image(H, W, dtype, cuda)
+        out.fill_(0x5A)
+        m.process(out, dl, dr)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        if dtype == torch.int16:
+            got = got.view(np.uint16)
+        np.testing.assert_array_equal(got, enc(want))
+    assert m.device_status() == 0
+
+
+def test_census_match_full_size_1080p_d128(ct, oracle, cuda):
+    W, H, D = 1920, 1080, 128
+    L, R = pair(ct, 2, 2024, W, H, D - 1)
+    m = ct.BlockMatcherCensus()
+    m.configure(0, W, H, D)
+    out = ct.alloc_image(H, W, torch.uint8, cuda)
+    m.process(out, to_dev(L, cuda), to_dev(R, cuda))
+    torch.cuda.synchronize()
+    want, _ = oracle.match_census(L, R, D)
+    np.testing.assert_array_equal(out.cpu().numpy(), oracle.to_u8(want))
+
+
+def test_process_lr_and_crosscheck(ct, oracle, cuda):
+    W, H, D = 400, 150, 96
+    L, R = pair(ct, 2, 77, W, H, D - 1)
+    m = ct.BlockMatcherCensus()
+    m.configure(0, W, H, D)
+    dl, dr = to_dev(L, cuda), to_dev(R, cuda)
+    lr = ct.alloc_image(H, W, torch.int16, cuda)
+    rl = ct.alloc_image(H, W, torch.int16, cuda)
+    ck = ct.alloc_image(H, W, torch.int16, cuda)
+    m.process_lr(dl, dr, disp_lr=lr, disp_rl=rl, disp_checked=ck, tol=1)
+    torch.cuda.synchronize()
+    wl, _ = oracle.match_census(L, R, D, 2, True)
+    wr, _ = oracle.match_census(L, R, D, 2, False)
+    wc, _ = oracle.crosscheck(wl, wr, 1, True)
+    np.testing.assert_array_equal(lr.cpu().numpy().view(np.uint16), oracle.to_u16(wl))
+    np.testing.assert_array_equal(rl.cpu().numpy().view(np.uint16), oracle.to_u16(wr))
+    np.testing.assert_array_equal(ck.cpu().numpy().view(np.uint16), oracle.to_u16(wc))
+    # checked map only (internal scratch maps), U8
+    ck8 = ct.alloc_image(H, W, torch.uint8, cuda)
+    m.process_lr(dl, dr, disp_checked=ck8, tol=1)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(ck8.cpu().numpy(), oracle.to_u8(np.where(wc == -2, -1, wc)))
+
+
+@pytest.mark.parametrize("dtype", [torch.uint8, torch.int16])
+def test_crosscheck_driver_and_range(ct, oracle, cuda, dtype):
+    W, H, D = 300, 120, 48
+    L, R = pair(ct, 1, 5, W, H, D - 1)
+    wl, _ = oracle.match_census(L, R, D, 2, True)
+    wr, _ = oracle.match_census(L, R, D, 2, False)
+    enc = oracle.to_u8 if dtype == torch.uint8 else oracle.to_u16
+    base, other = to_dev(enc(wl).view(np.int16) if dtype == torch.int16 else enc(wl), cuda), \
+        to_dev(enc(wr).view(np.int16) if dtype == torch.int16 else enc(wr), cuda)
+    cc = ct.CrossCheckDisparityMaps()
+    cc.configure(0, W, H, ct.CT_PIX_U8 if dtype == torch.uint8 else ct.CT_PIX_U16, disp_delta_thresh=1)
+    res = ct.alloc_image(H, W, dtype, cuda)
+    cc.process(res, base, other)
+    lo, hi = cc.disp_range()
+    want, (wlo, whi) = oracle.crosscheck(wl, wr, 1, True)
+    got = res.cpu().numpy()
+    if dtype == torch.int16:
+        np.testing.assert_array_equal(got.view(np.uint16), oracle.to_u16(want))
+    else:
+        np.testing.assert_array_equal(got, oracle.to_u8(np.where(want == -2, -1, want)))
+    assert (lo, hi) == (wlo, whi)
+
+
+def test_format_mismatch_is_an_error(ct, cuda):
+    m = ct.BlockMatcherCensus()
+    m.configure(0, 64, 32, 16)
+    a = ct.alloc_image(32, 64, torch.uint8, cuda)
+    b = ct.alloc_image(31, 64, torch.uint8, cuda)
+    with pytest.raises(ct.CtError) as e:
+        m.process(a, a, b)
+    assert e.value.code == ct.CT_EFORMAT
+    f = ct.alloc_image(32, 64, torch.float32, cuda)
+    with pytest.raises(ct.CtError) as e:
+        m.process(f, a, a)
+    assert e.value.code == ct.CT_ETYPE

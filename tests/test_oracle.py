@@ -1,0 +1,135 @@
+"""The CPU oracle against the golden fixtures and hand-computed answers.
+
+The fixtures come from an independent brute-force restatement
+(tests/golden/make_golden.py); agreement pins the oracle before it is used as
+the checker of the CUDA kernels.
+"""
+import json
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+
+def load(name):
+    return np.load(GOLDEN / name)
+
+
+def test_census3x3_golden(oracle):
+    g = load("census3x3.npz")
+    out = oracle.census3x3(g["img"])
+    H, W = g["img"].shape
+    np.testing.assert_array_equal(out[1:H - 1, 1:W - 1], g["out"][1:H - 1, 1:W - 1])
+
+
+def test_census3x3_leaves_border_unwritten(oracle):
+    img = np.random.default_rng(0).integers(0, 256, (9, 11), dtype=np.uint8)
+    out = oracle.census3x3(img, fill=0xAB)
+    assert (out[0] == 0xAB).all() and (out[-1] == 0xAB).all()
+    assert (out[:, 0] == 0xAB).all() and (out[:, -1] == 0xAB).all()
+
+
+def test_census9x7_golden(oracle):
+    g = load("census9x7.npz")
+    np.testing.assert_array_equal(oracle.census9x7(g["img"]), g["out"])
+
+
+def test_census9x7_known_patch(oracle):
+    k = json.loads((GOLDEN / "known.json").read_text())["census9x7_patch"]
+    img = np.array(k["patch"], np.uint8)
+    out = oracle.census9x7(img)
+    assert int(out[3, 4]) == int(k["descriptor"])
+    # bit 63 and the centre bit (31) are never set
+    assert int(out[3, 4]) >> 63 == 0 and (int(out[3, 4]) >> 31) & 1 == 0
+
+
+@pytest.mark.parametrize("lr", [True, False])
+def test_census_match_golden(oracle, lr):
+    g = load("census_match.npz")
+    d, c = oracle.match_census(g["L"], g["R"], int(g["D"]), 2, lr)
+    tag = "lr" if lr else "rl"
+    np.testing.assert_array_equal(d, g["disp_" + tag])
+    valid = g["disp_" + tag] >= 0
+    np.testing.assert_array_equal(c[valid], g["cost_" + tag][valid])
+
+
+def test_census_match_on_descriptors_equals_image_path(oracle):
+    g = load("census_match.npz")
+    cl, cr = oracle.census9x7(g["L"]), oracle.census9x7(g["R"])
+    d1, _ = oracle.match_census_desc(cl, cr, int(g["D"]))
+    d2, _ = oracle.match_census(g["L"], g["R"], int(g["D"]))
+    np.testing.assert_array_equal(d1, d2)
+
+
+def test_sad_golden(oracle):
+    g = load("sad.npz")
+    d, c = oracle.match_sad(g["L"], g["R"], int(g["D"]), 4)
+    np.testing.assert_array_equal(d, g["disp"])
+    valid = g["disp"] >= 0
+    np.testing.assert_array_equal(c[valid], g["cost"][valid])
+
+
+def test_aw_golden(oracle):
+    g = load("aw.npz")
+    d, c, s32, s64 = oracle.match_aw(g["L"], g["R"], int(g["D"]))
+    np.testing.assert_array_equal(d, g["disp"])
+    valid = g["disp"] >= 0
+    np.testing.assert_array_equal(c[valid], g["cost"][valid])
+    np.testing.assert_allclose(s64[valid], g["sub"][valid], rtol=0, atol=1e-12)
+    assert np.abs(s32[valid] - s64[valid]).max() <= 1e-4
+
+
+def test_ncc_golden(oracle):
+    g = load("ncc.npz")
+    d, s32, s64 = oracle.match_ncc(g["L"], g["R"], int(g["D"]), 5)
+    np.testing.assert_array_equal(d, g["disp"])
+    valid = g["disp"] >= 0
+    np.testing.assert_allclose(s64[valid], g["score"][valid], rtol=0, atol=1e-12)
+    assert np.abs(s32[valid] - s64[valid]).max() <= 1e-4
+    # the flat patch hits the sigma < 1 rule: score 0 at its interior pixels
+    assert (s64[6, 6:9] == 0).all() and (s32[6, 6:9] == 0).all()
+
+
+def test_crosscheck_golden(oracle):
+    g = load("crosscheck.npz")
+    out, (lo, hi) = oracle.crosscheck(g["base"], g["other"], 1)
+    np.testing.assert_array_equal(out, g["out"])
+    kept = g["out"][g["out"] >= 0]
+    assert (lo, hi) == (int(kept.min()), int(kept.max()))
+
+
+def test_constant_image_gives_lowest_d(oracle):
+    img = np.full((30, 40), 91, np.uint8)
+    d, _ = oracle.match_census(img, img, 8)
+    assert (d[d >= 0] == 0).all()
+    d, _ = oracle.match_sad(img, img, 8, 4)
+    assert (d[d >= 0] == 0).all()
+
+
+def test_pure_shift_recovered(oracle):
+    k = json.loads((GOLDEN / "known.json").read_text())["shift"]["k"]
+    rng = np.random.default_rng(5)
+    L = rng.integers(0, 256, (40, 64)).astype(np.uint8)
+    R = np.roll(L, -k, axis=1)  # R(x) = L(x + k): left pixel x matches right x - k
+    d, _ = oracle.match_census(L, R, 12)
+    inner = d[8:-8, 24:-8]
+    assert (inner == k).mean() > 0.98
+    d, _ = oracle.match_sad(L, R, 12, 4)
+    assert (d[8:-8, 24:-8] == k).mean() > 0.98
+
+
+def test_validity_rules(oracle):
+    rng = np.random.default_rng(2)
+    L = rng.integers(0, 256, (20, 30)).astype(np.uint8)
+    R = rng.integers(0, 256, (20, 30)).astype(np.uint8)
+    d, _ = oracle.match_census(L, R, 16)
+    H, W = L.shape
+    assert (d[:2] == -1).all() and (d[H - 2:] == -1).all()
+    assert (d[:, :2] == -1).all() and (d[:, W - 2:] == -1).all()
+    xs = np.arange(W)[None, :].repeat(H, 0)
+    v = d >= 0
+    assert (d[v] <= xs[v] - 2).all()  # matched window stays inside
+    d, _ = oracle.match_census(L, R, 16, left_to_right=False)
+    v = d >= 0
+    assert (d[v] <= (W - 1 - 2) - xs[v]).all()
