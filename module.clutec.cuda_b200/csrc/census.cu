@@ -300,13 +300,13 @@ int ct_bm_census_configure(ct_handle* hh, int32_t device, const ct_format* fmt, 
     if (cudaMalloc(&h->tmp_lr, h->tmp_pitch * H) != cudaSuccess) return fail(CT_ENOMEM, "map scratch");
     if (cudaMalloc(&h->tmp_rl, h->tmp_pitch * H) != cudaSuccess) return fail(CT_ENOMEM, "map scratch");
     const uint64_t pb = h->desc_pitch * 8;
+    h->fmt = *fmt;  // left_desc() / right_desc() below depend on the height
+    h->par = *p;
     using namespace cm;
     if (int rc = make_tmap_2d(&h->tm_lb, h->left_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kTWV, kRB)) return rc;
     if (int rc = make_tmap_2d(&h->tm_rb, h->right_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kTWV, kRB)) return rc;
     if (int rc = make_tmap_2d(&h->tm_lm, h->left_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kMW, kRB)) return rc;
     if (int rc = make_tmap_2d(&h->tm_rm, h->right_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kMW, kRB)) return rc;
-    h->fmt = *fmt;
-    h->par = *p;
     h->configured = true;
     return CT_OK;
 }

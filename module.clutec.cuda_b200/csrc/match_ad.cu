@@ -1,0 +1,516 @@
+// match_ad.cu — absolute-difference block matchers:
+//   BlockMatcherSAD1::CDriver (exhaustive (2r+1)^2 SAD + WTA) and
+//   BlockMatcherAW1/AW2 (best of 5 shifted 7x7 SAD windows + WTA + FP32
+//   parabolic sub-pixel refinement).
+//
+// Layout (same decomposition as the census matcher): a CTA owns 128 "V
+// columns" x th output rows x 64 disparities; warp w owns 8 disparities and
+// lane L the 4 adjacent columns 4L..4L+3. The uint8 image strips the CTA needs
+// (th + 2*ext rows of the base view, 128 + 16 columns; of the match view,
+// 192 + 16 columns) are staged in shared memory by two 2D TMA loads. Each
+// thread walks the strip downwards keeping vertical running sums of |B - M|
+// for 4 columns x 8 disparities packed as 16-bit pairs; the row leaving the
+// window is recomputed from the staged pixels (cheaper than a register ring
+// for a 1-byte cost). The horizontal pass takes r halo columns from the
+// neighbouring lanes by shuffles (AlgoArraySum_W32H16::SumCache's two passes,
+// Kernel.Algo.ArraySum_W32H16.h:163-200).
+// The AW variant stores each row of 7x7 box sums S in a 7-row shared-memory
+// ring and takes A = min(S(x,y), S(x-3,y), S(x+3,y), S(x,y-3), S(x,y+3)) with
+// two packed 3-way mins (the min-variant of AlgoAdaptWnd3D's neighbourhood
+// evaluation, Kernel.Algo.AdaptWnd3D.h:244-300, with the 5-window layout).
+// Winner-take-all keys are (cost << 16 | d): the lowest cost wins, then the
+// lowest d; warps merge through shared-memory atomicMin, CTAs that split D
+// through a global key buffer.
+#include "ct_internal.h"
+#include "ct_device.cuh"
+
+namespace ct {
+namespace ad {
+
+constexpr int kCPT = 4, kTWV = 128, kDPW = 8, kNW = 8, kNT = kNW * 32, kDPC = kDPW * kNW;
+constexpr int kBW = kTWV + 16;        // staged base columns
+constexpr int kMWs = kTWV + kDPC + 16; // staged match columns (208)
+constexpr int kRing = 7;              // AW: rows of S kept
+constexpr int kRingW = kTWV + 8;      // AW: padded ring row (4 words each side)
+
+__host__ __device__ constexpr int ext_of(int R, bool aw) { return aw ? 2 * R : R; }
+__host__ __device__ constexpr int two_of(int R, bool aw) { return kTWV - 2 * ext_of(R, aw); }
+
+struct Args {
+    int W, H, D, th;
+    uint32_t* keys;      // global keys when gridDim.z > 1 (or always for AW)
+    void* out;
+    size_t out_pitch;
+    int out_type;
+    int32_t* status;
+};
+
+__host__ __device__ constexpr size_t strip_bytes(int th, int R, bool aw) {
+    return (size_t(kBW) * (th + 2 * ext_of(R, aw)) + 127) / 128 * 128 +
+           (size_t(kMWs) * (th + 2 * ext_of(R, aw)) + 127) / 128 * 128;
+}
+__host__ __device__ constexpr size_t smem_bytes(int th, int R, bool aw) {
+    return strip_bytes(th, R, aw) + (aw ? size_t(kRing) * kNW * 4 * kRingW * 4 : 0) +
+           size_t(th) * two_of(R, aw) * 4 + 16;
+}
+
+__device__ __forceinline__ int floor16(int v) { return v & ~15; }
+
+// U8 / U16 disparity store from a (cost << 16 | d) key; 0xFFFF cost = none.
+__device__ __forceinline__ void store_key(void* out, size_t pitch, int type, int x, int y, bool valid,
+                                          uint32_t key) {
+    const bool ok = valid && (key >> 16) != 0xFFFFu;
+    const uint32_t d = key & 0xFFFFu;
+    char* row = static_cast<char*>(out) + (size_t)y * pitch;
+    if (type == CT_PIX_U8) reinterpret_cast<uint8_t*>(row)[x] = ok ? uint8_t(d) : uint8_t(0xFF);
+    else if (type == CT_PIX_U16) reinterpret_cast<uint16_t*>(row)[x] = ok ? uint16_t(d + 1) : uint16_t(0xFFFF);
+    else reinterpret_cast<float*>(row)[x] = ok ? float(d) : -1.0f;
+}
+
+// Horizontal (2R+1)-wide sums of the packed column sums V of this lane's 4
+// columns, halo columns taken from the neighbouring lanes.
+template <int R>
+__device__ __forceinline__ void hsum(const uint32_t (&V)[kCPT], uint32_t (&C)[kCPT]) {
+    uint32_t win[kCPT + 2 * R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {  // column j - R < 0
+        const int i = R - 1 - j;    // halo index: column -(i+1)
+        win[j] = __shfl_up_sync(0xffffffffu, V[3 - (i % 4)], i / 4 + 1);
+    }
+#pragma unroll
+    for (int c = 0; c < kCPT; ++c) win[R + c] = V[c];
+#pragma unroll
+    for (int i = 0; i < R; ++i) win[R + kCPT + i] = __shfl_down_sync(0xffffffffu, V[i % 4], i / 4 + 1);
+    uint32_t s = 0;
+#pragma unroll
+    for (int j = 0; j <= 2 * R; ++j) s += win[j];
+    C[0] = s;
+#pragma unroll
+    for (int c = 1; c < kCPT; ++c) {
+        s = s + win[c + 2 * R] - win[c - 1];
+        C[c] = s;
+    }
+}
+
+template <int R, bool AW, int DIR>
+__global__ void __launch_bounds__(kNT, 1)
+    ad_match_kernel(const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmM, Args a) {
+    constexpr int EXT = ext_of(R, AW);
+    constexpr int TWO = two_of(R, AW);
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int NR = a.th + 2 * EXT;
+    uint8_t* sB = smem;
+    uint8_t* sM = smem + (size_t(kBW) * NR + 127) / 128 * 128;
+    unsigned char* after = smem + strip_bytes(a.th, R, AW);
+    uint32_t* ring = reinterpret_cast<uint32_t*>(after);  // AW only
+    uint32_t* sKey = reinterpret_cast<uint32_t*>(after + (AW ? size_t(kRing) * kNW * 4 * kRingW * 4 : 0));
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sKey + a.th * TWO);
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int xs = blockIdx.x * TWO - EXT;
+    const int y0 = blockIdx.y * a.th;
+    const int dz0 = blockIdx.z * kDPC;
+    const int dw = dz0 + warp * kDPW;
+    const bool warp_active = dw < a.D;
+    const int ab = floor16(xs);
+    const int am = DIR == 0 ? floor16(xs - dz0 - (kDPC - 1)) : floor16(xs + dz0);
+    // AW windows reach EXT = 6 columns; SAD ones r columns.
+    const bool interior = (dz0 + kDPC <= a.D) &&
+                          (DIR == 0 ? (xs + EXT - EXT >= dz0 + kDPC - 1)
+                                    : (xs + kTWV - 1 - EXT + dz0 + kDPC - 1 + EXT <= a.W - 1));
+
+    if (tid == 0) {
+        dev::prefetch_tmap(&tmB);
+        dev::prefetch_tmap(&tmM);
+        dev::mbar_init(bar, 1);
+        dev::fence_barrier_init();
+    }
+    for (int i = tid; i < a.th * TWO; i += kNT) sKey[i] = 0xFFFFFFFFu;
+    __syncthreads();
+    if (tid == 0) {
+        dev::mbar_arrive_expect_tx(bar, uint32_t(kBW * NR + kMWs * NR));
+        dev::tma_load_2d(sB, &tmB, ab, y0 - EXT, bar);
+        dev::tma_load_2d(sM, &tmM, am, y0 - EXT, bar);
+    }
+    const bool got = dev::mbar_wait_bounded(bar, 0);
+    if (__syncthreads_or(!got)) {
+        if (tid == 0) dev::report(a.status, CT_ETIMEOUT);
+        return;
+    }
+
+    const int bo = xs - ab + 4 * lane;                                        // base column 0 in strip
+    const int mo = DIR == 0 ? (xs - dz0 - am) + 4 * lane - kDPW * warp - 7   // match column for (c=0, j=7)
+                            : (xs + dz0 - am) + 4 * lane + kDPW * warp;      // match column for (c=0, j=0)
+    uint32_t dlo[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) dlo[p] = uint32_t(dw + 2 * p);
+
+    auto row_pairs = [&](int i, uint32_t (&P)[kCPT][4]) {
+        const uint8_t* rb = sB + i * kBW + bo;
+        const uint8_t* rm = sM + i * kMWs + mo;
+        int b[kCPT], m[11];
+#pragma unroll
+        for (int c = 0; c < kCPT; ++c) b[c] = rb[c];
+#pragma unroll
+        for (int k = 0; k < 11; ++k) m[k] = rm[k];
+#pragma unroll
+        for (int c = 0; c < kCPT; ++c)
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                const int j0 = 2 * p, j1 = 2 * p + 1;
+                const int k0 = DIR == 0 ? c - j0 + 7 : c + j0;
+                const int k1 = DIR == 0 ? c - j1 + 7 : c + j1;
+                const uint32_t e0 = uint32_t(abs(b[c] - m[k0]));
+                const uint32_t e1 = uint32_t(abs(b[c] - m[k1]));
+                P[c][p] = e0 | (e1 << 16);
+            }
+    };
+
+    uint32_t V[4][kCPT];  // [pair][column]
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int c = 0; c < kCPT; ++c) V[p][c] = 0;
+
+    if (warp_active) {
+        for (int i = 0; i < NR; ++i) {
+            uint32_t Pn[kCPT][4];
+            row_pairs(i, Pn);
+            if (i >= 2 * R + 1) {
+                uint32_t Po[kCPT][4];
+                row_pairs(i - 2 * R - 1, Po);
+#pragma unroll
+                for (int c = 0; c < kCPT; ++c)
+#pragma unroll
+                    for (int p = 0; p < 4; ++p) V[p][c] = V[p][c] + Pn[c][p] - Po[c][p];
+            } else {
+#pragma unroll
+                for (int c = 0; c < kCPT; ++c)
+#pragma unroll
+                    for (int p = 0; p < 4; ++p) V[p][c] += Pn[c][p];
+            }
+            if (i < 2 * R) continue;
+            // S (box sums) of strip row i - R, all 4 pairs
+            uint32_t S[4][kCPT];
+#pragma unroll
+            for (int p = 0; p < 4; ++p) hsum<R>(V[p], S[p]);
+            int oy;
+            uint32_t A[4][kCPT];
+            if (!AW) {
+                oy = i - 2 * R;
+#pragma unroll
+                for (int p = 0; p < 4; ++p)
+#pragma unroll
+                    for (int c = 0; c < kCPT; ++c) A[p][c] = S[p][c];
+            } else {
+                // S row index since the first S row: s = i - 2R; ring slot s % 7
+                const int s = i - 2 * R;
+                uint32_t* slot = ring + size_t(s % kRing) * kNW * 4 * kRingW;
+#pragma unroll
+                for (int p = 0; p < 4; ++p)
+                    *reinterpret_cast<uint4*>(slot + (warp * 4 + p) * kRingW + 4 + 4 * lane) =
+                        make_uint4(S[p][0], S[p][1], S[p][2], S[p][3]);
+                __syncwarp();
+                if (s < 2 * R) continue;  // need S rows s - 3 and s - 6
+                oy = s - 2 * R;
+                const uint32_t* mid = ring + size_t((s - R) % kRing) * kNW * 4 * kRingW;
+                const uint32_t* top = ring + size_t((s - 2 * R) % kRing) * kNW * 4 * kRingW;
+#pragma unroll
+                for (int p = 0; p < 4; ++p) {
+                    const uint32_t* rm = mid + (warp * 4 + p) * kRingW + 4 * lane;  // padded index of col 4L-4
+                    const uint4 q0 = *reinterpret_cast<const uint4*>(rm);
+                    const uint4 q1 = *reinterpret_cast<const uint4*>(rm + 4);
+                    const uint4 q2 = *reinterpret_cast<const uint4*>(rm + 8);
+                    const uint32_t w12[12] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w,
+                                              q2.x, q2.y, q2.z, q2.w};  // cols 4L-4 .. 4L+7
+                    const uint4 t = *reinterpret_cast<const uint4*>(top + (warp * 4 + p) * kRingW + 4 + 4 * lane);
+                    const uint32_t tw[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+                    for (int c = 0; c < kCPT; ++c) {
+                        const uint32_t m3 = dev::min3_u16x2(w12[4 + c], w12[4 + c - R], w12[4 + c + R]);
+                        A[p][c] = dev::min3_u16x2(m3, tw[c], S[p][c]);
+                    }
+                }
+            }
+            if (oy < 0 || oy >= a.th) continue;
+#pragma unroll
+            for (int c = 0; c < kCPT; ++c) {
+                const int v = 4 * lane + c;
+                if (v < EXT || v >= kTWV - EXT) continue;
+                uint32_t best = 0xFFFFFFFFu;
+                const int x = xs + v;
+                int lim = DIR == 0 ? x - EXT : a.W - 1 - EXT - x;
+                lim = min(lim, a.D - 1);
+#pragma unroll
+                for (int p = 0; p < 4; ++p) {
+                    uint32_t klo = __byte_perm(A[p][c], dlo[p], 0x1054);        // cost_lo << 16 | d
+                    uint32_t khi = (A[p][c] & 0xFFFF0000u) | (dlo[p] + 1);       // cost_hi << 16 | d+1
+                    if (!interior) {
+                        if (int(dlo[p]) > lim) klo |= 0xFFFF0000u;
+                        if (int(dlo[p]) + 1 > lim) khi |= 0xFFFF0000u;
+                    }
+                    best = min(best, min(klo, khi));
+                }
+                atomicMin(&sKey[oy * TWO + v - EXT], best);
+            }
+        }
+    } else if (AW) {
+        // inactive warps still own ring slices nobody reads; nothing to do
+    }
+    __syncthreads();
+    const bool direct = !AW && gridDim.z == 1;
+    for (int idx = tid; idx < a.th * TWO; idx += kNT) {
+        const int oy = idx / TWO, ox = idx - oy * TWO;
+        const int x = xs + EXT + ox, y = y0 + oy;
+        if (x >= a.W || y >= a.H) continue;
+        const uint32_t key = sKey[idx];
+        if (direct) {
+            const bool valid = x >= EXT && x < a.W - EXT && y >= EXT && y < a.H - EXT;
+            store_key(a.out, a.out_pitch, a.out_type, x, y, valid, key);
+        } else {
+            atomicMin(&a.keys[(size_t)y * a.W + x], key);
+        }
+    }
+}
+
+__global__ void ad_finalize_kernel(uint32_t* keys, int W, int H, int ext, void* out, size_t pitch, int type) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W) return;
+    uint32_t* kp = &keys[(size_t)y * W + x];
+    const uint32_t key = *kp;
+    *kp = 0xFFFFFFFFu;
+    const bool valid = x >= ext && x < W - ext && y >= ext && y < H - ext;
+    store_key(out, pitch, type, x, y, valid, key);
+}
+
+// AW cost A(x, y, d) directly from the images (7x7 windows, shifts of 3).
+// Column sums of 7 rows around y over columns x-6..x+6 give the three
+// horizontally shifted windows; the two vertical shifts are summed directly.
+__device__ int aw_cost_at(const uint8_t* L, size_t pl, const uint8_t* Rm, size_t pr, int x, int y, int d) {
+    int col[13];
+#pragma unroll
+    for (int k = 0; k < 13; ++k) {
+        const int xx = x - 6 + k;
+        int s = 0;
+#pragma unroll
+        for (int dy = -3; dy <= 3; ++dy)
+            s += abs(int(L[(size_t)(y + dy) * pl + xx]) - int(Rm[(size_t)(y + dy) * pr + xx - d]));
+        col[k] = s;
+    }
+    int sc = 0, sl = 0, sr = 0;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) { sl += col[k]; sc += col[k + 3]; sr += col[k + 6]; }
+    int su = 0, sd = 0;
+#pragma unroll
+    for (int dy = -3; dy <= 3; ++dy)
+#pragma unroll
+        for (int dx = -3; dx <= 3; ++dx) {
+            const int xx = x + dx;
+            su += abs(int(L[(size_t)(y - 3 + dy) * pl + xx]) - int(Rm[(size_t)(y - 3 + dy) * pr + xx - d]));
+            sd += abs(int(L[(size_t)(y + 3 + dy) * pl + xx]) - int(Rm[(size_t)(y + 3 + dy) * pr + xx - d]));
+        }
+    return min(min(min(sc, sl), min(sr, su)), sd);
+}
+
+// Sub-pixel refinement from the merged AW keys: d* = d + (c- - c+) /
+// (2 (c- - 2 c0 + c+)) in IEEE FP32, skipped at d = 0, d = D-1 or when d+1 is
+// not searchable (x - (d+1) - 6 < 0). Resets the keys.
+__global__ void aw_subpixel_kernel(uint32_t* keys, int W, int H, int D, const uint8_t* L, size_t pl,
+                                   const uint8_t* Rm, size_t pr, void* out, size_t pitch, int type) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W) return;
+    uint32_t* kp = &keys[(size_t)y * W + x];
+    const uint32_t key = *kp;
+    *kp = 0xFFFFFFFFu;
+    const bool valid = x >= 6 && x < W - 6 && y >= 6 && y < H - 6 && (key >> 16) != 0xFFFFu;
+    if (type != CT_PIX_F32 || !valid) {
+        store_key(out, pitch, type, x, y, valid, key);
+        return;
+    }
+    const int d = int(key & 0xFFFFu);
+    const int c0 = int(key >> 16);
+    float s = float(d);
+    if (d > 0 && d < D - 1 && x - (d + 1) - 6 >= 0) {
+        const int cm = aw_cost_at(L, pl, Rm, pr, x, y, d - 1);
+        const int cp = aw_cost_at(L, pl, Rm, pr, x, y, d + 1);
+        const int den = cm - 2 * c0 + cp;
+        if (den > 0) s = __fadd_rn(float(d), __fdiv_rn(float(cm - cp), float(2 * den)));
+    }
+    reinterpret_cast<float*>(static_cast<char*>(out) + (size_t)y * pitch)[x] = s;
+}
+
+}  // namespace ad
+
+// ---------------------------------------------------------------------------
+// Handles and C ABI
+// ---------------------------------------------------------------------------
+namespace {
+
+struct AdHandle : ct_handle {
+    explicit AdHandle(Kind k) : ct_handle(k) {}
+    ~AdHandle() override {
+        if (device >= 0) cudaSetDevice(device);
+        cudaFree(keys);
+    }
+    ct_format fmt{};
+    int D = 0, R = 4, dir = 0;
+    uint32_t* keys = nullptr;
+    int th = 32;
+};
+
+template <int R, bool AW, int DIR>
+int set_attr() {
+    static bool done = false;
+    if (!done) {
+        CT_CUDA_TRY(cudaFuncSetAttribute(ad::ad_match_kernel<R, AW, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)ad::smem_bytes(64, R, AW)));
+        done = true;
+    }
+    return CT_OK;
+}
+
+template <int R, bool AW, int DIR>
+int launch_ad(AdHandle* h, const ct_image* disp, const ct_image* L, const ct_image* Rimg, cudaStream_t s) {
+    using namespace ad;
+    if (int rc = set_attr<R, AW, DIR>()) return rc;
+    const int W = h->fmt.width, H = h->fmt.height;
+    constexpr int EXT = ext_of(R, AW), TWO = two_of(R, AW);
+    Args a{};
+    a.W = W; a.H = H; a.D = h->D; a.th = h->th;
+    a.keys = h->keys;
+    a.out = disp->ptr; a.out_pitch = disp->pitch_bytes; a.out_type = disp->type;
+    a.status = h->d_status;
+    const int NR = a.th + 2 * EXT;
+    const ct_image* B = DIR == 0 ? L : Rimg;
+    const ct_image* M = DIR == 0 ? Rimg : L;
+    CUtensorMap tb, tm;
+    if (int rc = make_tmap_2d(&tb, B->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, W, H, B->pitch_bytes, kBW, NR)) return rc;
+    if (int rc = make_tmap_2d(&tm, M->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, W, H, M->pitch_bytes, kMWs, NR)) return rc;
+    dim3 grid((W + TWO - 1) / TWO, (H + a.th - 1) / a.th, (h->D + kDPC - 1) / kDPC);
+    ad_match_kernel<R, AW, DIR><<<grid, kNT, smem_bytes(a.th, R, AW), s>>>(tb, tm, a);
+    CT_LAUNCH_CHECK();
+    if (AW) {
+        aw_subpixel_kernel<<<dim3((W + 127) / 128, H), 128, 0, s>>>(
+            h->keys, W, H, h->D, static_cast<const uint8_t*>(L->ptr), L->pitch_bytes,
+            static_cast<const uint8_t*>(Rimg->ptr), Rimg->pitch_bytes, disp->ptr, disp->pitch_bytes, disp->type);
+        CT_LAUNCH_CHECK();
+    } else if (grid.z > 1) {
+        ad_finalize_kernel<<<dim3((W + 255) / 256, H), 256, 0, s>>>(h->keys, W, H, EXT, disp->ptr,
+                                                                    disp->pitch_bytes, disp->type);
+        CT_LAUNCH_CHECK();
+    }
+    return CT_OK;
+}
+
+int configure_ad(AdHandle* h, int32_t device, const ct_format* fmt, int D, int R, int dir) {
+    if (fmt->type != CT_PIX_U8) return fail(CT_ETYPE, "matcher input must be U8 (TPixel_Lum_UInt8)");
+    if (fmt->width < 16 || fmt->height < 16 || fmt->width > 32768 || fmt->height > 32768)
+        return fail(CT_EINVAL, "image size %dx%d out of range (16..32768)", fmt->width, fmt->height);
+    if (D < 1 || D > 256) return fail(CT_EINVAL, "disp_count must be 1..256");
+    if (int rc = use_device(device)) return rc;
+    cudaFree(h->keys);
+    h->keys = nullptr;
+    h->device = device;
+    if (int rc = h->init_status()) return rc;
+    if (cudaMalloc(&h->keys, (size_t)fmt->width * fmt->height * 4) != cudaSuccess)
+        return fail(CT_ENOMEM, "key scratch");
+    CT_CUDA_TRY(cudaMemset(h->keys, 0xFF, (size_t)fmt->width * fmt->height * 4));
+    h->fmt = *fmt;
+    h->D = D;
+    h->R = R;
+    h->dir = dir;
+    h->configured = true;
+    return CT_OK;
+}
+
+int check_io(AdHandle* h, const ct_image* disp, const ct_image* L, const ct_image* R, uint32_t disp_types) {
+    if (!h->configured) return fail(CT_ESTATE, "process before configure");
+    if (int rc = check_image(L, "left", 1u << CT_PIX_U8)) return rc;
+    if (int rc = check_image(R, "right", 1u << CT_PIX_U8)) return rc;
+    if (int rc = check_same_size(L, R, "left", "right")) return rc;
+    if (L->width != h->fmt.width || L->height != h->fmt.height)
+        return fail(CT_EFORMAT, "image size differs from the configured format");
+    if (int rc = check_image(disp, "disp", disp_types)) return rc;
+    if (int rc = check_same_size(disp, L, "disp", "left")) return rc;
+    if (disp->type == CT_PIX_U8 && h->D > 255) return fail(CT_ETYPE, "U8 maps need disp_count <= 255");
+    return CT_OK;
+}
+
+}  // namespace
+}  // namespace ct
+
+using namespace ct;
+
+extern "C" {
+
+int ct_bm_sad_create(ct_handle** out) {
+    clear_error();
+    if (!out) return fail(CT_EINVAL, "null output handle pointer");
+    *out = new AdHandle(Kind::BmSad);
+    return CT_OK;
+}
+
+int ct_bm_sad_configure(ct_handle* hh, int32_t device, const ct_format* fmt, const ct_sad_params* p) {
+    clear_error();
+    auto* h = (hh && hh->kind == Kind::BmSad) ? static_cast<AdHandle*>(hh) : nullptr;
+    if (!h) return fail(CT_ESTATE, "not a SAD matcher handle");
+    if (!fmt || !p) return fail(CT_EINVAL, "null format or parameters");
+    if (p->radius < 1 || p->radius > 4) return fail(CT_EINVAL, "radius must be 1..4 (3x3 .. 9x9)");
+    if (p->reserved != 0) return fail(CT_EINVAL, "reserved must be 0");
+    return configure_ad(h, device, fmt, p->disp_count, p->radius, p->left_to_right ? 0 : 1);
+}
+
+int ct_bm_sad_process(ct_handle* hh, const ct_image* disp, const ct_image* left, const ct_image* right,
+                      ct_stream stream) {
+    clear_error();
+    auto* h = (hh && hh->kind == Kind::BmSad) ? static_cast<AdHandle*>(hh) : nullptr;
+    if (!h) return fail(CT_ESTATE, "not a SAD matcher handle");
+    if (int rc = check_io(h, disp, left, right, (1u << CT_PIX_U8) | (1u << CT_PIX_U16))) return rc;
+    if (int rc = use_device(h->device)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    h->last_stream = s;
+    const int k = h->R * 2 + h->dir;
+    switch (k) {
+        case 2: return launch_ad<1, false, 0>(h, disp, left, right, s);
+        case 3: return launch_ad<1, false, 1>(h, disp, left, right, s);
+        case 4: return launch_ad<2, false, 0>(h, disp, left, right, s);
+        case 5: return launch_ad<2, false, 1>(h, disp, left, right, s);
+        case 6: return launch_ad<3, false, 0>(h, disp, left, right, s);
+        case 7: return launch_ad<3, false, 1>(h, disp, left, right, s);
+        case 8: return launch_ad<4, false, 0>(h, disp, left, right, s);
+        case 9: return launch_ad<4, false, 1>(h, disp, left, right, s);
+        default: return fail(CT_EINVAL, "unsupported radius");
+    }
+}
+
+int ct_bm_aw_create(ct_handle** out) {
+    clear_error();
+    if (!out) return fail(CT_EINVAL, "null output handle pointer");
+    *out = new AdHandle(Kind::BmAw);
+    return CT_OK;
+}
+
+int ct_bm_aw_configure(ct_handle* hh, int32_t device, const ct_format* fmt, const ct_aw_params* p) {
+    clear_error();
+    auto* h = (hh && hh->kind == Kind::BmAw) ? static_cast<AdHandle*>(hh) : nullptr;
+    if (!h) return fail(CT_ESTATE, "not an AW matcher handle");
+    if (!fmt || !p) return fail(CT_EINVAL, "null format or parameters");
+    if (p->left_to_right != 1) return fail(CT_EINVAL, "the AW matcher is left-to-right only");
+    if (p->reserved0 || p->reserved1) return fail(CT_EINVAL, "reserved fields must be 0");
+    return configure_ad(h, device, fmt, p->disp_count, 3, 0);
+}
+
+int ct_bm_aw_process(ct_handle* hh, const ct_image* disp, const ct_image* left, const ct_image* right,
+                     ct_stream stream) {
+    clear_error();
+    auto* h = (hh && hh->kind == Kind::BmAw) ? static_cast<AdHandle*>(hh) : nullptr;
+    if (!h) return fail(CT_ESTATE, "not an AW matcher handle");
+    if (int rc = check_io(h, disp, left, right, (1u << CT_PIX_U8) | (1u << CT_PIX_U16) | (1u << CT_PIX_F32)))
+        return rc;
+    if (int rc = use_device(h->device)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    h->last_stream = s;
+    return launch_ad<3, true, 0>(h, disp, left, right, s);
+}
+
+}  // extern "C"

@@ -1,0 +1,376 @@
+// match_ncc.cu — BlockMatcherNCC::CDriver with an unquantised FP32 score.
+//
+// The reference forms NCC from integer window sums and normalises in FP32
+// through means and standard deviations (BlockMatcherNCC.cu:182-262), which
+// cancels badly. Here every window sum is an exact int32 (11x11 x 255^2 fits)
+// and only the last step is FP32, with IEEE-rounded operations:
+//   num = n Sxy - Sx Sy,  vx = n Sxx - Sx^2,  vy = n Syy - Sy^2   (exact ints)
+//   ncc = 0 if vx * vy < n^4 (sigma_x sigma_y < 1, NCC.cu:255-262)
+//   ncc = float(num) / sqrt(float(vx) * float(vy)) otherwise.
+// Per-pixel (Sx, vx) of both images come from a box-statistics pass; the
+// matching kernel keeps vertical running sums of L(x) R(x-d) for 4 columns x
+// 8 disparities per thread (same CTA decomposition as the other matchers) and
+// merges the argmax through 64-bit keys (ordered score << 32 | ~d): the
+// highest score wins, then the lowest d.
+#include "ct_internal.h"
+#include "ct_device.cuh"
+
+namespace ct {
+namespace ncc {
+
+constexpr int kCPT = 4, kTWV = 128, kDPW = 8, kNW = 8, kNT = kNW * 32, kDPC = kDPW * kNW;
+constexpr int kBW = kTWV + 16, kMWs = kTWV + kDPC + 16;
+
+__host__ __device__ constexpr int two_of(int R) { return kTWV - 2 * R; }
+__host__ __device__ constexpr size_t strip_bytes(int th, int R) {
+    return (size_t(kBW) * (th + 2 * R) + 127) / 128 * 128 + (size_t(kMWs) * (th + 2 * R) + 127) / 128 * 128;
+}
+__host__ __device__ constexpr size_t smem_bytes(int th, int R) {
+    return strip_bytes(th, R) + size_t(th) * two_of(R) * 8 + 16;
+}
+
+// Box sum S and n*Q - S^2 for every pixel whose window is inside the image.
+template <int R>
+__global__ void box_stats_kernel(const uint8_t* img, size_t pitch, int W, int H, int32_t* S, int32_t* V) {
+    constexpr int TX = 32, TY = 8, SW = TX + 2 * R, SH = TY + 2 * R;
+    __shared__ uint8_t t[SH][SW];
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    for (int i = threadIdx.y * TX + threadIdx.x; i < SW * SH; i += TX * TY) {
+        const int yy = y0 - R + i / SW, xx = x0 - R + i % SW;
+        t[i / SW][i % SW] = (xx >= 0 && xx < W && yy >= 0 && yy < H) ? img[(size_t)yy * pitch + xx] : 0;
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+    if (x >= W || y >= H) return;
+    int s = 0, q = 0;
+#pragma unroll
+    for (int dy = 0; dy <= 2 * R; ++dy)
+#pragma unroll
+        for (int dx = 0; dx <= 2 * R; ++dx) {
+            const int v = t[threadIdx.y + dy][threadIdx.x + dx];
+            s += v;
+            q += v * v;
+        }
+    constexpr int n = (2 * R + 1) * (2 * R + 1);
+    S[(size_t)y * W + x] = s;
+    V[(size_t)y * W + x] = n * q - s * s;
+}
+
+__device__ __forceinline__ uint32_t ordered(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float unordered(uint32_t o) {
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
+}
+
+struct Args {
+    int W, H, D, th;
+    const int32_t *Sx, *Vx, *Sy, *Vy;   // stats of the left / right image (W*H)
+    unsigned long long* keys;          // global keys when gridDim.z > 1
+    void* out;
+    size_t out_pitch;
+    int out_type;
+    float* score;
+    size_t score_pitch;
+    int32_t* status;
+};
+
+__device__ __forceinline__ void store_ncc(const Args& a, int x, int y, bool valid, unsigned long long key) {
+    const bool ok = valid && key != 0ull;
+    const uint32_t d = ok ? 0xFFFFFFFFu - uint32_t(key & 0xFFFFFFFFull) : 0u;
+    char* row = static_cast<char*>(a.out) + (size_t)y * a.out_pitch;
+    if (a.out_type == CT_PIX_U8) reinterpret_cast<uint8_t*>(row)[x] = ok ? uint8_t(d) : uint8_t(0xFF);
+    else reinterpret_cast<uint16_t*>(row)[x] = ok ? uint16_t(d + 1) : uint16_t(0xFFFF);
+    if (a.score)
+        reinterpret_cast<float*>(reinterpret_cast<char*>(a.score) + (size_t)y * a.score_pitch)[x] =
+            ok ? unordered(uint32_t(key >> 32)) : 0.0f;
+}
+
+template <int R>
+__global__ void __launch_bounds__(kNT, 1)
+    ncc_match_kernel(const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmM, Args a) {
+    constexpr int TWO = two_of(R);
+    constexpr int n = (2 * R + 1) * (2 * R + 1);
+    constexpr long long n4 = (long long)n * n * n * n;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int NR = a.th + 2 * R;
+    uint8_t* sB = smem;
+    uint8_t* sM = smem + (size_t(kBW) * NR + 127) / 128 * 128;
+    unsigned long long* sKey = reinterpret_cast<unsigned long long*>(smem + strip_bytes(a.th, R));
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sKey + a.th * TWO);
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int xs = blockIdx.x * TWO - R;
+    const int y0 = blockIdx.y * a.th;
+    const int dz0 = blockIdx.z * kDPC;
+    const int dw = dz0 + warp * kDPW;
+    const bool warp_active = dw < a.D;
+    const int ab = xs & ~15;
+    const int am = (xs - dz0 - (kDPC - 1)) & ~15;
+
+    if (tid == 0) {
+        dev::prefetch_tmap(&tmB);
+        dev::prefetch_tmap(&tmM);
+        dev::mbar_init(bar, 1);
+        dev::fence_barrier_init();
+    }
+    for (int i = tid; i < a.th * TWO; i += kNT) sKey[i] = 0ull;
+    __syncthreads();
+    if (tid == 0) {
+        dev::mbar_arrive_expect_tx(bar, uint32_t(kBW * NR + kMWs * NR));
+        dev::tma_load_2d(sB, &tmB, ab, y0 - R, bar);
+        dev::tma_load_2d(sM, &tmM, am, y0 - R, bar);
+    }
+    const bool got = dev::mbar_wait_bounded(bar, 0);
+    if (__syncthreads_or(!got)) {
+        if (tid == 0) dev::report(a.status, CT_ETIMEOUT);
+        return;
+    }
+    const int bo = xs - ab + 4 * lane;
+    const int mo = (xs - dz0 - am) + 4 * lane - kDPW * warp - 7;
+
+    int V[kDPW][kCPT];
+#pragma unroll
+    for (int j = 0; j < kDPW; ++j)
+#pragma unroll
+        for (int c = 0; c < kCPT; ++c) V[j][c] = 0;
+
+    if (warp_active) {
+        for (int i = 0; i < NR; ++i) {
+            {
+                const uint8_t* rb = sB + i * kBW + bo;
+                const uint8_t* rm = sM + i * kMWs + mo;
+                int b[kCPT], m[11];
+#pragma unroll
+                for (int c = 0; c < kCPT; ++c) b[c] = rb[c];
+#pragma unroll
+                for (int k = 0; k < 11; ++k) m[k] = rm[k];
+                if (i >= 2 * R + 1) {
+                    const uint8_t* ob = sB + (i - 2 * R - 1) * kBW + bo;
+                    const uint8_t* om = sM + (i - 2 * R - 1) * kMWs + mo;
+                    int bb[kCPT], mm[11];
+#pragma unroll
+                    for (int c = 0; c < kCPT; ++c) bb[c] = ob[c];
+#pragma unroll
+                    for (int k = 0; k < 11; ++k) mm[k] = om[k];
+#pragma unroll
+                    for (int j = 0; j < kDPW; ++j)
+#pragma unroll
+                        for (int c = 0; c < kCPT; ++c)
+                            V[j][c] += b[c] * m[c - j + 7] - bb[c] * mm[c - j + 7];
+                } else {
+#pragma unroll
+                    for (int j = 0; j < kDPW; ++j)
+#pragma unroll
+                        for (int c = 0; c < kCPT; ++c) V[j][c] += b[c] * m[c - j + 7];
+                }
+            }
+            if (i < 2 * R) continue;
+            const int oy = i - 2 * R;
+            const int y = y0 + oy;
+            int C[kDPW][kCPT];
+#pragma unroll
+            for (int j = 0; j < kDPW; ++j) {
+                int win[kCPT + 2 * R];
+#pragma unroll
+                for (int q = 0; q < R; ++q) {
+                    const int h = R - 1 - q;
+                    win[q] = __shfl_up_sync(0xffffffffu, V[j][3 - (h % 4)], h / 4 + 1);
+                }
+#pragma unroll
+                for (int c = 0; c < kCPT; ++c) win[R + c] = V[j][c];
+#pragma unroll
+                for (int h = 0; h < R; ++h) win[R + kCPT + h] = __shfl_down_sync(0xffffffffu, V[j][h % 4], h / 4 + 1);
+                int s = 0;
+#pragma unroll
+                for (int q = 0; q <= 2 * R; ++q) s += win[q];
+                C[j][0] = s;
+#pragma unroll
+                for (int c = 1; c < kCPT; ++c) { s = s + win[c + 2 * R] - win[c - 1]; C[j][c] = s; }
+            }
+            if (y >= a.H) continue;
+#pragma unroll
+            for (int c = 0; c < kCPT; ++c) {
+                const int v = 4 * lane + c;
+                if (v < R || v >= kTWV - R) continue;
+                const int x = xs + v;
+                if (x < R || x >= a.W - R || y < R || y >= a.H - R) continue;
+                const size_t o = (size_t)y * a.W + x;
+                const int sx = a.Sx[o], vx = a.Vx[o];
+                const float fvx = __int2float_rn(vx);
+                unsigned long long best = 0ull;
+#pragma unroll
+                for (int j = 0; j < kDPW; ++j) {
+                    const int d = dw + j;
+                    if (d >= a.D || x - d - R < 0) continue;
+                    const int sy = a.Sy[o - d], vy = a.Vy[o - d];
+                    const int num = n * C[j][c] - sx * sy;
+                    float sc = 0.0f;
+                    if ((long long)vx * (long long)vy >= n4)
+                        sc = __fdiv_rn(__int2float_rn(num), __fsqrt_rn(__fmul_rn(fvx, __int2float_rn(vy))));
+                    const unsigned long long key =
+                        ((unsigned long long)ordered(sc) << 32) | (0xFFFFFFFFu - uint32_t(d));
+                    best = key > best ? key : best;
+                }
+                if (best) atomicMax(&sKey[oy * TWO + v - R], best);
+            }
+        }
+    }
+    __syncthreads();
+    const bool direct = gridDim.z == 1;
+    for (int idx = tid; idx < a.th * TWO; idx += kNT) {
+        const int oy = idx / TWO, ox = idx - oy * TWO;
+        const int x = xs + R + ox, y = y0 + oy;
+        if (x >= a.W || y >= a.H) continue;
+        const unsigned long long key = sKey[idx];
+        if (direct) {
+            const bool valid = x >= R && x < a.W - R && y >= R && y < a.H - R;
+            store_ncc(a, x, y, valid, key);
+        } else if (key) {
+            atomicMax(&a.keys[(size_t)y * a.W + x], key);
+        }
+    }
+}
+
+__global__ void ncc_finalize_kernel(Args a, int R) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= a.W) return;
+    unsigned long long* kp = &a.keys[(size_t)y * a.W + x];
+    const unsigned long long key = *kp;
+    *kp = 0ull;
+    const bool valid = x >= R && x < a.W - R && y >= R && y < a.H - R;
+    store_ncc(a, x, y, valid, key);
+}
+
+}  // namespace ncc
+
+namespace {
+
+struct NccHandle : ct_handle {
+    NccHandle() : ct_handle(Kind::BmNcc) {}
+    ~NccHandle() override {
+        if (device >= 0) cudaSetDevice(device);
+        cudaFree(stats);
+        cudaFree(keys);
+    }
+    ct_format fmt{};
+    ct_ncc_params par{};
+    int32_t* stats = nullptr;  // Sx, Vx, Sy, Vy
+    unsigned long long* keys = nullptr;
+    int th = 32;
+};
+
+template <int R>
+int launch_ncc(NccHandle* h, const ct_image* disp, const ct_image* score, const ct_image* L, const ct_image* Rr,
+               cudaStream_t s) {
+    using namespace ncc;
+    static bool attr = false;
+    if (!attr) {
+        CT_CUDA_TRY(cudaFuncSetAttribute(ncc_match_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem_bytes(64, R)));
+        attr = true;
+    }
+    const int W = h->fmt.width, H = h->fmt.height;
+    const size_t N = (size_t)W * H;
+    Args a{};
+    a.W = W; a.H = H; a.D = h->par.disp_count; a.th = h->th;
+    a.Sx = h->stats; a.Vx = h->stats + N; a.Sy = h->stats + 2 * N; a.Vy = h->stats + 3 * N;
+    a.keys = h->keys;
+    a.out = disp->ptr; a.out_pitch = disp->pitch_bytes; a.out_type = disp->type;
+    a.score = score ? static_cast<float*>(score->ptr) : nullptr;
+    a.score_pitch = score ? score->pitch_bytes : 0;
+    a.status = h->d_status;
+    dim3 sb(32, 8), sg((W + 31) / 32, (H + 7) / 8);
+    box_stats_kernel<R><<<sg, sb, 0, s>>>(static_cast<const uint8_t*>(L->ptr), L->pitch_bytes, W, H, h->stats,
+                                          h->stats + N);
+    box_stats_kernel<R><<<sg, sb, 0, s>>>(static_cast<const uint8_t*>(Rr->ptr), Rr->pitch_bytes, W, H,
+                                          h->stats + 2 * N, h->stats + 3 * N);
+    CT_LAUNCH_CHECK();
+    const int NR = a.th + 2 * R;
+    CUtensorMap tb, tm;
+    if (int rc = make_tmap_2d(&tb, L->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, W, H, L->pitch_bytes, kBW, NR)) return rc;
+    if (int rc = make_tmap_2d(&tm, Rr->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, W, H, Rr->pitch_bytes, kMWs, NR))
+        return rc;
+    dim3 grid((W + two_of(R) - 1) / two_of(R), (H + a.th - 1) / a.th, (a.D + kDPC - 1) / kDPC);
+    ncc_match_kernel<R><<<grid, kNT, smem_bytes(a.th, R), s>>>(tb, tm, a);
+    CT_LAUNCH_CHECK();
+    if (grid.z > 1) {
+        ncc_finalize_kernel<<<dim3((W + 255) / 256, H), 256, 0, s>>>(a, R);
+        CT_LAUNCH_CHECK();
+    }
+    return CT_OK;
+}
+
+}  // namespace
+}  // namespace ct
+
+using namespace ct;
+
+extern "C" {
+
+int ct_bm_ncc_create(ct_handle** out) {
+    clear_error();
+    if (!out) return fail(CT_EINVAL, "null output handle pointer");
+    *out = new NccHandle();
+    return CT_OK;
+}
+
+int ct_bm_ncc_configure(ct_handle* hh, int32_t device, const ct_format* fmt, const ct_ncc_params* p) {
+    clear_error();
+    auto* h = (hh && hh->kind == Kind::BmNcc) ? static_cast<NccHandle*>(hh) : nullptr;
+    if (!h) return fail(CT_ESTATE, "not an NCC matcher handle");
+    if (!fmt || !p) return fail(CT_EINVAL, "null format or parameters");
+    if (fmt->type != CT_PIX_U8) return fail(CT_ETYPE, "matcher input must be U8 (TPixel_Lum_UInt8)");
+    if (fmt->width < 16 || fmt->height < 16 || fmt->width > 32768 || fmt->height > 32768)
+        return fail(CT_EINVAL, "image size out of range (16..32768)");
+    if (p->disp_count < 1 || p->disp_count > 256) return fail(CT_EINVAL, "disp_count must be 1..256");
+    if (p->radius != 2 && p->radius != 4 && p->radius != 5)
+        return fail(CT_EINVAL, "radius must be 5 (Patch_11x11), 4 (Patch_9x9) or 2 (Patch_5x5)");
+    if (p->left_to_right != 1) return fail(CT_EINVAL, "the NCC matcher is left-to-right only");
+    if (p->reserved != 0) return fail(CT_EINVAL, "reserved must be 0");
+    if (int rc = use_device(device)) return rc;
+    cudaFree(h->stats); cudaFree(h->keys);
+    h->stats = nullptr; h->keys = nullptr;
+    h->device = device;
+    if (int rc = h->init_status()) return rc;
+    const size_t N = (size_t)fmt->width * fmt->height;
+    if (cudaMalloc(&h->stats, 4 * N * sizeof(int32_t)) != cudaSuccess) return fail(CT_ENOMEM, "stats scratch");
+    if (cudaMalloc(&h->keys, N * sizeof(unsigned long long)) != cudaSuccess) return fail(CT_ENOMEM, "key scratch");
+    CT_CUDA_TRY(cudaMemset(h->keys, 0, N * sizeof(unsigned long long)));
+    h->fmt = *fmt;
+    h->par = *p;
+    h->configured = true;
+    return CT_OK;
+}
+
+int ct_bm_ncc_process(ct_handle* hh, const ct_image* disp, const ct_image* score, const ct_image* left,
+                      const ct_image* right, const ct_image* disp_init, ct_stream stream) {
+    clear_error();
+    auto* h = (hh && hh->kind == Kind::BmNcc) ? static_cast<NccHandle*>(hh) : nullptr;
+    if (!h) return fail(CT_ESTATE, "not an NCC matcher handle");
+    if (!h->configured) return fail(CT_ESTATE, "process before configure");
+    if (disp_init) return fail(CT_EINVAL, "disp_init (guided MatcherUseDisparity mode) is not built");
+    if (int rc = check_image(left, "left", 1u << CT_PIX_U8)) return rc;
+    if (int rc = check_image(right, "right", 1u << CT_PIX_U8)) return rc;
+    if (int rc = check_same_size(left, right, "left", "right")) return rc;
+    if (left->width != h->fmt.width || left->height != h->fmt.height)
+        return fail(CT_EFORMAT, "image size differs from the configured format");
+    if (int rc = check_image(disp, "disp", (1u << CT_PIX_U8) | (1u << CT_PIX_U16))) return rc;
+    if (int rc = check_same_size(disp, left, "disp", "left")) return rc;
+    if (disp->type == CT_PIX_U8 && h->par.disp_count > 255) return fail(CT_ETYPE, "U8 maps need disp_count <= 255");
+    if (score) {
+        if (int rc = check_image(score, "score", 1u << CT_PIX_F32)) return rc;
+        if (int rc = check_same_size(score, left, "score", "left")) return rc;
+    }
+    if (int rc = use_device(h->device)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    h->last_stream = s;
+    switch (h->par.radius) {
+        case 2: return launch_ncc<2>(h, disp, score, left, right, s);
+        case 4: return launch_ncc<4>(h, disp, score, left, right, s);
+        default: return launch_ncc<5>(h, disp, score, left, right, s);
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,139 @@
+"""SAD, adaptive-window (+ sub-pixel) and NCC matchers on the GPU against the
+CPU oracle. Integer disparities are bit-exact; FP32 scores and sub-pixel
+disparities are compared with the FP64 oracle at an absolute tolerance of
+1e-4 (the maximum error seen is printed), and with the FP32 restatement
+bit-exactly (same IEEE operations)."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import to_dev
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-4
+
+
+def run_sad(ct, cuda, L, R, D, r, lr, dtype):
+    H, W = L.shape
+    m = ct.BlockMatcherSAD1()
+    m.configure(0, W, H, D, radius=r, left_to_right=lr)
+    out = ct.alloc_image(H, W, dtype, cuda)
+    out.fill_(0x5A)
+    m.process(out, to_dev(L, cuda), to_dev(R, cuda))
+    torch.cuda.synchronize()
+    assert m.device_status() == 0
+    got = out.cpu().numpy()
+    return got.view(np.uint16) if dtype == torch.int16 else got
+
+
+@pytest.mark.parametrize("W,H,D,r", [(67, 43, 13, 4), (640, 480, 64, 4), (300, 100, 100, 4), (129, 70, 64, 1),
+                                     (129, 70, 65, 2), (200, 50, 30, 3)])
+@pytest.mark.parametrize("lr", [True, False])
+def test_sad_bit_exact(ct, oracle, cuda, W, H, D, r, lr):
+    L, R, _, _ = ct.synth_pair(1, W + D, W, H, D - 1)
+    want, _ = oracle.match_sad(L, R, D, r, lr)
+    np.testing.assert_array_equal(run_sad(ct, cuda, L, R, D, r, lr, torch.uint8), oracle.to_u8(want))
+    np.testing.assert_array_equal(run_sad(ct, cuda, L, R, D, r, lr, torch.int16), oracle.to_u16(want))
+
+
+def test_sad_config1_accuracy(ct, oracle, cuda):
+    """640x480, D = 64, 9x9: bit-exact and mostly right against ground truth."""
+    L, R, G, O = ct.synth_pair(1, 1, 640, 480, 63)
+    got = run_sad(ct, cuda, L, R, 64, 4, True, torch.uint8)
+    want, _ = oracle.match_sad(L, R, 64, 4, True)
+    np.testing.assert_array_equal(got, oracle.to_u8(want))
+    v = (got != 255) & (O == 0)
+    assert (np.abs(got[v].astype(int) - G[v]) <= 1).mean() > 0.8
+
+
+def run_aw(ct, cuda, L, R, D, dtype):
+    H, W = L.shape
+    m = ct.BlockMatcherAW()
+    m.configure(0, W, H, D)
+    out = ct.alloc_image(H, W, dtype, cuda)
+    out.fill_(0)
+    m.process(out, to_dev(L, cuda), to_dev(R, cuda))
+    torch.cuda.synchronize()
+    assert m.device_status() == 0
+    got = out.cpu().numpy()
+    return got.view(np.uint16) if dtype == torch.int16 else got
+
+
+@pytest.mark.parametrize("W,H,D", [(67, 43, 13), (300, 120, 100), (640, 200, 256)])
+def test_aw_integer_and_subpixel(ct, oracle, cuda, W, H, D):
+    L, R, _, _ = ct.synth_pair(3, W * 3 + D, W, H, D - 1)
+    d, c, s32, s64 = oracle.match_aw(L, R, D)
+    if D <= 255:
+        np.testing.assert_array_equal(run_aw(ct, cuda, L, R, D, torch.uint8), oracle.to_u8(d))
+    np.testing.assert_array_equal(run_aw(ct, cuda, L, R, D, torch.int16), oracle.to_u16(d))
+    sub = run_aw(ct, cuda, L, R, D, torch.float32)
+    np.testing.assert_array_equal(sub, s32)  # same IEEE operations
+    v = d >= 0
+    err = np.abs(sub[v].astype(np.float64) - s64[v]).max()
+    print(f"AW {W}x{H} D={D}: max |sub32 - sub64| = {err:.3g}")
+    assert err <= TOL
+
+
+@pytest.mark.slow
+def test_aw_config3_full_size(ct, oracle, cuda):
+    W, H, D = 2560, 1440, 256
+    L, R, G, O = ct.synth_pair(3, 33, W, H, D - 1)
+    d, c, s32, s64 = oracle.match_aw(L, R, D)
+    sub = run_aw(ct, cuda, L, R, D, torch.float32)
+    v = d >= 0
+    np.testing.assert_array_equal(sub, s32)
+    err = np.abs(sub[v].astype(np.float64) - s64[v]).max()
+    print(f"AW 2560x1440 D=256: max |sub32 - sub64| = {err:.3g}")
+    assert err <= TOL
+
+
+def run_ncc(ct, cuda, L, R, D, r, dtype=torch.uint8):
+    H, W = L.shape
+    m = ct.BlockMatcherNCC()
+    m.configure(0, W, H, D, radius=r)
+    out = ct.alloc_image(H, W, dtype, cuda)
+    score = ct.alloc_image(H, W, torch.float32, cuda)
+    m.process(out, to_dev(L, cuda), to_dev(R, cuda), score=score)
+    torch.cuda.synchronize()
+    assert m.device_status() == 0
+    got = out.cpu().numpy()
+    return (got.view(np.uint16) if dtype == torch.int16 else got), score.cpu().numpy()
+
+
+@pytest.mark.parametrize("W,H,D,r", [(67, 43, 13, 5), (400, 150, 96, 5), (150, 60, 40, 4), (150, 60, 70, 2)])
+def test_ncc(ct, oracle, cuda, W, H, D, r):
+    L, R, _, _ = ct.synth_pair(2, W + 5 * D, W, H, D - 1)
+    L[5:25, 5:30] = 128  # flat patch: the sigma < 1 rule
+    d, s32, s64 = oracle.match_ncc(L, R, D, r)
+    got, score = run_ncc(ct, cuda, L, R, D, r)
+    np.testing.assert_array_equal(got, oracle.to_u8(d))
+    v = d >= 0
+    np.testing.assert_array_equal(score[v], s32[v])
+    err = np.abs(score[v].astype(np.float64) - s64[v]).max()
+    print(f"NCC {W}x{H} D={D} r={r}: max |score32 - score64| = {err:.3g}")
+    assert err <= TOL
+    got16, _ = run_ncc(ct, cuda, L, R, D, r, torch.int16)
+    np.testing.assert_array_equal(got16, oracle.to_u16(d))
+
+
+@pytest.mark.slow
+def test_ncc_config2_full_size(ct, oracle, cuda):
+    W, H, D = 1920, 1080, 128
+    L, R, _, _ = ct.synth_pair(2, 2024, W, H, D - 1)
+    d, s32, s64 = oracle.match_ncc(L, R, D, 5)
+    got, score = run_ncc(ct, cuda, L, R, D, 5)
+    np.testing.assert_array_equal(got, oracle.to_u8(d))
+    v = d >= 0
+    err = np.abs(score[v].astype(np.float64) - s64[v]).max()
+    print(f"NCC 1920x1080 D=128: max |score32 - score64| = {err:.3g}")
+    assert err <= TOL
+
+
+def test_ncc_rejects_guided_mode(ct, cuda):
+    m = ct.BlockMatcherNCC()
+    m.configure(0, 64, 32, 16)
+    a = ct.alloc_image(32, 64, torch.uint8, cuda)
+    with pytest.raises(ct.CtError) as e:
+        m.process(a, a, a, disp_init=a)
+    assert e.value.code == ct.CT_EINVAL
