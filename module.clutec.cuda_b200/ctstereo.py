@@ -147,7 +147,7 @@ def _declare(L: C.CDLL) -> None:
 def exported_symbols():
     """Names of the ct_* entry points declared in include/ctstereo.h."""
     hdr = (_PKG.parent / "include" / "ctstereo.h").read_text()
-    return sorted(set(re.findall(r"\b(ct_[a-z0-9_]+)\s*\(", hdr)))
+    return sorted(set(re.findall(r"^(?:int|const char\s*\*)\s+(ct_[a-z0-9_]+)\s*\(", hdr, re.M)))
 
 
 def check(rc: int) -> None:
