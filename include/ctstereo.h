@@ -163,6 +163,23 @@ int ct_bm_census_process_lr(ct_handle* h, const ct_image* disp_lr, const ct_imag
 int ct_bm_census_match_desc(ct_handle* h, const ct_image* disp, const ct_image* desc_base,
                             const ct_image* desc_match, int32_t left_to_right, ct_stream stream);
 
+/* Census matching that allocates nothing. No counterpart in the reference:
+ * it exists for callers that cannot call cudaMalloc (a stream being captured
+ * into a CUDA graph, a real-time loop with a frozen allocator, a host whose
+ * device memory belongs to another framework's pool). Same kernels and
+ * results as ct_bm_census_process with {disp_count, agg_radius 2,
+ * left_to_right}, no handle; its scratch is a fixed static device array of
+ * 40 MiB per GPU that loads the library, so images are limited to 2,097,152
+ * pixels with rows rounded up to 32 (1920 x 1080 fits; larger -> CT_EINVAL).
+ * Runs on the current device. Its first call on a device looks up the array
+ * addresses: make it before any stream capture. Calls share the array, so
+ * calls that overlap on the GPU race; serialise them. device_status
+ * (nullable, caller-owned device int32) receives CT_ETIMEOUT if a bounded
+ * wait gives up. */
+int ct_bm_census_process_static(const ct_image* disp, const ct_image* left, const ct_image* right,
+                                int32_t disp_count, int32_t left_to_right, int32_t* device_status,
+                                ct_stream stream);
+
 /* ---- SAD block matcher: BlockMatcherSAD1::CDriver ------------------------
  * Replaces BlockMatcherSAD1.h:42-127 / BlockMatcherSAD1.cu:493-596 for the
  * exhaustive mode: per-pixel |L - R| (EvalSAD, BlockMatcherSAD1.cu:151-153),

@@ -248,7 +248,8 @@ __global__ void __launch_bounds__(kNT, 1)
 }
 
 // Converts merged keys to disparities and resets the keys for the next call.
-__global__ void keys_finalize_kernel(uint32_t* keys, int W, int H, int r, void* out, size_t out_pitch,
+// (static: each translation unit that launches it has its own copy.)
+static __global__ void keys_finalize_kernel(uint32_t* keys, int W, int H, int r, void* out, size_t out_pitch,
                                      int out_type) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;

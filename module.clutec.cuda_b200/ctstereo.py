@@ -119,6 +119,7 @@ def _declare(L: C.CDLL) -> None:
         "ct_bm_census_process": [H, img, img, img, C.c_void_p],
         "ct_bm_census_process_lr": [H, img, img, img, C.c_int32, img, img, C.c_void_p],
         "ct_bm_census_match_desc": [H, img, img, img, C.c_int32, C.c_void_p],
+        "ct_bm_census_process_static": [img, img, img, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p],
         "ct_bm_sad_create": [P(H)],
         "ct_bm_sad_configure": [H, C.c_int32, fmt, P(ct_sad_params)],
         "ct_bm_sad_process": [H, img, img, img, C.c_void_p],
@@ -321,6 +322,15 @@ class CrossCheckDisparityMaps(_Driver):
         lo, hi = C.c_int32(), C.c_int32()
         check(lib().ct_crosscheck_range(self._h, C.byref(lo), C.byref(hi)))
         return lo.value, hi.value
+
+
+def census_match_static(disp, left, right, disp_count: int, left_to_right: bool = True, device_status=None,
+                        stream=None):
+    """ct_bm_census_process_static: census matching with no device allocation
+    (static scratch; images up to 2,097,152 pixels with rows rounded to 32)."""
+    st = None if device_status is None else C.c_void_p(device_status.data_ptr())
+    check(lib().ct_bm_census_process_static(_img_ref(disp), _img_ref(left), _img_ref(right), disp_count,
+                                            int(left_to_right), st, _stream(stream)))
 
 
 def synth_pair(kind: int, seed: int, width: int, height: int, dmax: int):
