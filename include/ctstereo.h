@@ -163,6 +163,20 @@ int ct_bm_census_process_lr(ct_handle* h, const ct_image* disp_lr, const ct_imag
 int ct_bm_census_match_desc(ct_handle* h, const ct_image* disp, const ct_image* desc_base,
                             const ct_image* desc_match, int32_t left_to_right, ct_stream stream);
 
+/* Autotuner: times the kernel variants (4 or 8 disparities per warp) and
+ * strip heights for this handle's (W, H, D, direction) on the given images,
+ * keeps the fastest in the handle for later process calls. Synchronises
+ * `stream`. (No counterpart in the reference, whose launch shapes are
+ * compile-time SConfig constants, BlockMatcherNCC.h:43-79.) */
+int ct_bm_census_autotune(ct_handle* h, const ct_image* left, const ct_image* right, ct_stream stream);
+/* The handle's current launch shape (strip height in rows, disparities per
+ * warp); either pointer may be NULL. */
+int ct_bm_census_tuning(ct_handle* h, int32_t* strip_height, int32_t* disp_per_warp);
+/* Sets the launch shape (e.g. from a saved tuning table): strip_height with
+ * strip_height + 4 a multiple of 5 (11..511), disp_per_warp 4 or 8. Results do
+ * not depend on it. */
+int ct_bm_census_set_tuning(ct_handle* h, int32_t strip_height, int32_t disp_per_warp);
+
 /* Census matching that allocates nothing. No counterpart in the reference:
  * it exists for callers that cannot call cudaMalloc (a stream being captured
  * into a CUDA graph, a real-time loop with a frozen allocator, a host whose

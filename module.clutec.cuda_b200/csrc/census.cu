@@ -146,7 +146,8 @@ struct BmCensusHandle : ct_handle {
     uint16_t* tmp_rl = nullptr;
     size_t tmp_pitch = 0;
     CUtensorMap tm_lb, tm_rb, tm_lm, tm_rm;  // left/right as base (box 128) / match (box 192)
-    int th = 36;
+    int th = 36;   // strip height, chosen in configure or by the autotuner
+    int dpw = 4;   // disparities per warp (kernel variant)
     uint64_t* left_desc() const { return desc; }
     uint64_t* right_desc() const { return desc + (size_t)fmt.height * desc_pitch; }
 };
@@ -164,27 +165,15 @@ H* as(ct_handle* h, Kind k) {
 int census_match_pass_maps(BmCensusHandle* h, int dir, const ct_image* disp, const CUtensorMap& tb,
                            const CUtensorMap& tm, cudaStream_t s) {
     using namespace cm;
-    const int W = h->fmt.width, H = h->fmt.height, D = h->par.disp_count;
     MatchArgs a{};
-    a.W = W; a.H = H; a.D = D;
+    a.W = h->fmt.width; a.H = h->fmt.height; a.D = h->par.disp_count;
     a.th = h->th;
-    a.nbatch = (a.th + 2 * kAR) / kRB;
     a.keys = h->keys;
     a.out = disp->ptr; a.out_pitch = disp->pitch_bytes; a.out_type = disp->type;
     a.status = h->d_status;
-    dim3 grid((W + kTWO - 1) / kTWO, (H + a.th - 1) / a.th, (D + kDPC - 1) / kDPC);
-    const size_t smem = smem_bytes(a.th);
-    if (dir == 0) {
-        census_match_kernel<0><<<grid, kNT, smem, s>>>(tb, tm, a);
-    } else {
-        census_match_kernel<1><<<grid, kNT, smem, s>>>(tb, tm, a);
-    }
-    CT_LAUNCH_CHECK();
-    if (grid.z > 1) {
-        keys_finalize_kernel<<<dim3((W + 255) / 256, H), 256, 0, s>>>(h->keys, W, H, kAR, disp->ptr,
-                                                                      disp->pitch_bytes, disp->type);
-        CT_LAUNCH_CHECK();
-    }
+    const cudaError_t e = dir == 0 ? launch_census_match<0>(tb, tm, a, s, h->dpw)
+                                   : launch_census_match<1>(tb, tm, a, s, h->dpw);
+    if (e != cudaSuccess) return fail(CT_ECUDA, "census match launch failed: %s", cudaGetErrorString(e));
     return CT_OK;
 }
 
@@ -200,16 +189,6 @@ int census_both(BmCensusHandle* h, const ct_image* left, const ct_image* right, 
 }
 
 }  // namespace
-
-static int set_smem_attrs() {
-    static bool done = false;
-    if (done) return CT_OK;
-    const int smem = (int)cm::smem_bytes(96);
-    CT_CUDA_TRY(cudaFuncSetAttribute(cm::census_match_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CT_CUDA_TRY(cudaFuncSetAttribute(cm::census_match_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    done = true;
-    return CT_OK;
-}
 
 }  // namespace ct
 
@@ -285,7 +264,6 @@ int ct_bm_census_configure(ct_handle* hh, int32_t device, const ct_format* fmt, 
     if (p->agg_radius != cm::kAR) return fail(CT_EINVAL, "only agg_radius 2 (5x5) is built");
     if (p->reserved != 0) return fail(CT_EINVAL, "reserved must be 0");
     if (int rc = use_device(device)) return rc;
-    if (int rc = set_smem_attrs()) return rc;
     // release a previous configuration
     cudaFree(h->desc); cudaFree(h->keys); cudaFree(h->tmp_lr); cudaFree(h->tmp_rl);
     h->desc = nullptr; h->keys = nullptr; h->tmp_lr = nullptr; h->tmp_rl = nullptr;
@@ -301,6 +279,7 @@ int ct_bm_census_configure(ct_handle* hh, int32_t device, const ct_format* fmt, 
     if (cudaMalloc(&h->tmp_rl, h->tmp_pitch * H) != cudaSuccess) return fail(CT_ENOMEM, "map scratch");
     const uint64_t pb = h->desc_pitch * 8;
     h->fmt = *fmt;  // left_desc() / right_desc() below depend on the height
+    h->th = cm::pick_strip_height(W, H, p->disp_count, sm_count(device));
     h->par = *p;
     using namespace cm;
     if (int rc = make_tmap_2d(&h->tm_lb, h->left_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kTWV, kRB)) return rc;
@@ -375,6 +354,77 @@ int ct_bm_census_process_lr(ct_handle* hh, const ct_image* disp_lr, const ct_ima
     if (need_rl)
         if (int rc = census_match_pass(h, 1, rl, s)) return rc;
     if (disp_checked) return crosscheck_launch(disp_checked, lr, rl, tol, 1, nullptr, s);
+    return CT_OK;
+}
+
+int ct_bm_census_autotune(ct_handle* hh, const ct_image* left, const ct_image* right, ct_stream stream) {
+    clear_error();
+    auto* h = as<BmCensusHandle>(hh, Kind::BmCensus);
+    if (!h) return fail(CT_ESTATE, "not a census matcher handle");
+    if (int rc = check_match_io(h, left, right)) return rc;
+    if (int rc = use_device(h->device)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    h->last_stream = s;
+    if (int rc = census_both(h, left, right, s)) return rc;
+    const int W = h->fmt.width, H = h->fmt.height, D = h->par.disp_count;
+    const int dir = h->par.left_to_right ? 0 : 1;
+    // candidates: both variants x the model's strip height and its neighbours
+    const int th0 = cm::pick_strip_height(W, H, D, sm_count(h->device));
+    int ths[6] = {th0, th0 - 10, th0 + 10, th0 - 40, 36, 61};
+    ct_image out{h->tmp_lr, h->tmp_pitch, W, H, CT_PIX_U16, 0};
+    cudaEvent_t e0, e1;
+    CT_CUDA_TRY(cudaEventCreate(&e0));
+    CT_CUDA_TRY(cudaEventCreate(&e1));
+    float best_ms = 1e30f;
+    int best_th = th0, best_dpw = 4;
+    int rc = CT_OK;
+    for (int dpw : {4, 8}) {
+        for (int th : ths) {
+            if (th < 11 || (th + 2 * cm::kAR) % cm::kRB != 0) continue;
+            h->dpw = dpw;
+            h->th = th;
+            if ((rc = census_match_pass(h, dir, &out, s))) break;  // warm-up
+            float t = 1e30f;
+            for (int rep = 0; rep < 3 && rc == CT_OK; ++rep) {
+                cudaEventRecord(e0, s);
+                rc = census_match_pass(h, dir, &out, s);
+                cudaEventRecord(e1, s);
+                if (cudaEventSynchronize(e1) != cudaSuccess) { rc = fail(CT_ECUDA, "autotune timing failed"); break; }
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                t = ms < t ? ms : t;
+            }
+            if (rc) break;
+            if (t < best_ms) { best_ms = t; best_th = th; best_dpw = dpw; }
+        }
+        if (rc) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    h->th = best_th;
+    h->dpw = best_dpw;
+    return rc;
+}
+
+int ct_bm_census_tuning(ct_handle* hh, int32_t* strip_height, int32_t* disp_per_warp) {
+    clear_error();
+    auto* h = as<BmCensusHandle>(hh, Kind::BmCensus);
+    if (!h) return fail(CT_ESTATE, "not a census matcher handle");
+    if (!h->configured) return fail(CT_ESTATE, "tuning before configure");
+    if (strip_height) *strip_height = h->th;
+    if (disp_per_warp) *disp_per_warp = h->dpw;
+    return CT_OK;
+}
+
+int ct_bm_census_set_tuning(ct_handle* hh, int32_t strip_height, int32_t disp_per_warp) {
+    clear_error();
+    auto* h = as<BmCensusHandle>(hh, Kind::BmCensus);
+    if (!h) return fail(CT_ESTATE, "not a census matcher handle");
+    if (strip_height < 11 || strip_height > 511 || (strip_height + 2 * cm::kAR) % cm::kRB != 0)
+        return fail(CT_EINVAL, "strip_height must be 11..511 with strip_height + 4 a multiple of 5");
+    if (disp_per_warp != 4 && disp_per_warp != 8) return fail(CT_EINVAL, "disp_per_warp must be 4 or 8");
+    h->th = strip_height;
+    h->dpw = disp_per_warp;
     return CT_OK;
 }
 

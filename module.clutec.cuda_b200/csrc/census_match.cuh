@@ -1,14 +1,15 @@
-// census_match.cuh — census transform and the fused census matcher kernel:
-// Hamming cost (popcount of XOR of 64-bit descriptors) + 5x5 box aggregation
-// + winner-take-all, one launch per direction.
+// census_match.cuh — the fused census matcher kernel: Hamming cost (popcount
+// of XOR of 64-bit descriptors) + 5x5 box aggregation + winner-take-all, one
+// launch per direction.
 //
 // Mapping to B200:
 //  * A CTA owns a tile of 128 "V columns" (124 output columns plus 2 halo
-//    columns on each side) x th output rows x 64 disparities. Its 8 warps share
-//    the same columns and rows; warp w owns disparities dz0 + 8w .. +7 and
-//    lane L owns the 4 adjacent columns 4L..4L+3.
+//    columns on each side) x th output rows x 64 disparities. Its warps share
+//    the same columns and rows; warp w owns disparities dz0 + DPW w .. + DPW-1
+//    (DPW = 4: 16 warps of <= 128 registers; DPW = 8: 8 warps) and lane L owns
+//    the 4 adjacent columns 4L..4L+3.
 //  * Descriptor rows are staged in shared memory by 2D TMA tile loads (one box
-//    of 5 rows of the base image and one of the match image per batch), two
+//    of 5 rows of the base view and one of the match view per batch), two
 //    batches in flight, completion tracked by mbarriers with bounded waits.
 //  * Each thread keeps, in registers, the vertical running sums V of its 4
 //    columns x 8 disparities and a 5-deep ring of the per-row Hamming costs
@@ -19,12 +20,19 @@
 //  * The horizontal pass (ArraySum_W32H16.h:186-200) takes the 2 halo columns
 //    from the neighbouring lanes with warp shuffles and runs a 5-wide running
 //    sum over the thread's columns.
+//  * Rows are software-pipelined: the aggregation and winner-take-all of the
+//    window ending at row i-1 are issued next to the popcounts of row i, so
+//    the POPC pipe (16 lanes / clock / SM, the bound) is kept busy while the
+//    integer pipes do the rest.
 //  * Winner-take-all folds the disparity into the low 5 bits of each 16-bit
-//    lane (key = C << 5 | d mod 32, C <= 25 * 63 = 1575 so it fits), so the min
-//    over 8 disparities is two packed 3-way mins, and the lowest d wins ties
-//    by construction (the reference's strict '<' scanning d upward). Warps
-//    merge per pixel through a shared-memory atomicMin on (C << 16 | d); CTAs
-//    that split D merge through a global atomicMin.
+//    lane (key = C << 5 | d mod 32, C <= 25 * 63 = 1575 so it fits): the min
+//    over a thread's disparities is one or two packed mins plus a half swap, and the
+//    lowest d wins ties by construction (the reference's strict '<' scanning
+//    d upward). Warps of one 32-disparity group merge with a shared-memory
+//    atomicMin; the two groups of a CTA are merged, converted to
+//    (C << 16 | d) and flushed after every batch of 5 rows, directly into the
+//    disparity map when the CTA saw all D, else through a global atomicMin
+//    whose keys a finalize kernel turns into disparities.
 #pragma once
 
 #include <cstdint>
@@ -38,20 +46,25 @@ constexpr int kCPT = 4;                 // columns per thread
 constexpr int kTWV = 32 * kCPT;         // 128 V columns per tile
 constexpr int kAR = 2;                  // aggregation radius (5x5)
 constexpr int kTWO = kTWV - 2 * kAR;    // 124 output columns per tile
-constexpr int kDPW = 8;                 // disparities per warp
-constexpr int kNW = 8;                  // warps per CTA
-constexpr int kNT = kNW * 32;           // threads per CTA
-constexpr int kDPC = kDPW * kNW;        // 64 disparities per CTA
+constexpr int kDPC = 64;                // disparities per CTA
+constexpr int kGroups = kDPC / 32;      // key groups of 32 disparities
+// Variant: disparities per warp (8 = 8 warps of 255 registers, one CTA of 8
+// warps per SM; 4 = 16 warps of at most 128 registers, 16 warps per SM).
+template <int DPW>
+struct Var {
+    static constexpr int kDPW = DPW;
+    static constexpr int kNP = DPW / 2;           // packed pairs per thread
+    static constexpr int kNW = kDPC / DPW;        // warps per CTA
+    static constexpr int kNT = kNW * 32;          // threads per CTA
+    static constexpr int kWords = DPW + 4;        // match descriptors a thread reads per row
+    static constexpr int kWarpsPerGroup = 32 / DPW;
+};
 constexpr int kRB = 2 * kAR + 1;        // rows per TMA batch = ring depth = 5
 constexpr int kMW = kTWV + kDPC;        // 192 match columns staged per row
 
-// Output rows per CTA: th + 2*kAR must be a multiple of kRB.
-__host__ __device__ constexpr bool valid_th(int th) { return th > 0 && (th + 2 * kAR) % kRB == 0; }
-
 struct MatchArgs {
     int W, H, D;
-    int th;             // output rows per CTA
-    int nbatch;         // (th + 2*kAR) / kRB
+    int th;             // output rows per CTA (strip height)
     uint32_t* keys;     // W*H keys merged by atomicMin when gridDim.z > 1
     void* out;          // direct disparity output when gridDim.z == 1
     size_t out_pitch;
@@ -59,11 +72,13 @@ struct MatchArgs {
     int32_t* status;
 };
 
-__host__ __device__ constexpr size_t smem_bytes(int th) {
-    return size_t(2) * kRB * kTWV * 8 + size_t(2) * kRB * kMW * 8 + size_t(th) * kTWO * 4 + 2 * 8;
+// Shared memory: 2 stages of base (5 x 128) and match (5 x 192) descriptor
+// rows, 2 buffers x 2 groups x 5 rows x 128 key slots, 2 mbarriers. 35.6 KB.
+__host__ __device__ constexpr size_t smem_bytes() {
+    return size_t(2) * kRB * kTWV * 8 + size_t(2) * kRB * kMW * 8 + size_t(2) * kGroups * kRB * kTWV * 4 + 2 * 8;
 }
 
-// Disparity code for an output pixel from its merged key.
+// Disparity code for an output pixel from its merged key (C << 16 | d).
 __device__ __forceinline__ void store_disp(void* out, size_t pitch, int type, int x, int y, bool valid,
                                            uint32_t key) {
     const uint32_t d = key & 0xFFFFu;
@@ -76,30 +91,202 @@ __device__ __forceinline__ void store_disp(void* out, size_t pitch, int type, in
     }
 }
 
-template <int DIR>
-__global__ void __launch_bounds__(kNT, 1)
+template <int DIR, bool EDGE, int DPW>
+__device__ __forceinline__ void match_body(const CUtensorMap* tmB, const CUtensorMap* tmM, const MatchArgs& a,
+                                           uint64_t* sB, uint64_t* sM, uint32_t* sKey, uint64_t* bars, int nb,
+                                           int rows_here, int xs, int y0, int ye0, int dz0, int ms) {
+    using VT = Var<DPW>;
+    constexpr int NP = VT::kNP, NT = VT::kNT, NWD = VT::kWords;
+    constexpr uint32_t kBytes = kRB * kTWV * 8 + kRB * kMW * 8;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int dw = dz0 + warp * DPW;
+    const bool warp_active = dw < a.D;
+    const int grp = warp / VT::kWarpsPerGroup;
+
+    uint32_t V[kCPT][NP];
+    uint32_t ring[kRB][kCPT][NP];
+#pragma unroll
+    for (int c = 0; c < kCPT; ++c)
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            V[c][p] = 0;
+#pragma unroll
+            for (int r = 0; r < kRB; ++r) ring[r][c][p] = 0;
+        }
+    uint32_t dconst[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p)
+        dconst[p] = uint32_t((dw + 2 * p) & 31) | (uint32_t((dw + 2 * p + 1) & 31) << 16);
+    int lim[kCPT];  // largest searchable d per column (EDGE tiles only)
+#pragma unroll
+    for (int c = 0; c < kCPT; ++c) {
+        const int x = xs + 4 * lane + c;
+        lim[c] = min(DIR == 0 ? x - kAR : a.W - 1 - kAR - x, a.D - 1);
+    }
+    // first match descriptor this thread reads per row (an even index)
+    const int mstart = DIR == 0 ? 4 * lane + kDPC - DPW - DPW * warp : 4 * lane + DPW * warp;
+
+    // Adds cost row r of stage s to the running sums.
+    auto accum = [&](int s, int r) {
+        const uint64_t* rowB = sB + (s * kRB + r) * kTWV;
+        const uint64_t* rowM = sM + (s * kRB + r) * kMW;
+        uint2 bw[kCPT], mw[NWD];
+        const uint4* pb = reinterpret_cast<const uint4*>(rowB + 4 * lane);
+        const uint4 q0 = pb[0], q1 = pb[1];
+        bw[0] = make_uint2(q0.x, q0.y); bw[1] = make_uint2(q0.z, q0.w);
+        bw[2] = make_uint2(q1.x, q1.y); bw[3] = make_uint2(q1.z, q1.w);
+        const uint4* pm = reinterpret_cast<const uint4*>(rowM + mstart);
+#pragma unroll
+        for (int k = 0; k < NWD / 2; ++k) {
+            const uint4 q = pm[k];
+            mw[2 * k] = make_uint2(q.x, q.y);
+            mw[2 * k + 1] = make_uint2(q.z, q.w);
+        }
+#pragma unroll
+        for (int c = 0; c < kCPT; ++c)
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                // left-to-right: column x - d sits at mw[c - j + DPW]; right-to-left: x + d at mw[c + j]
+                const int k0 = DIR == 0 ? c - 2 * p + DPW : c + 2 * p;
+                const int k1 = DIR == 0 ? c - 2 * p - 1 + DPW : c + 2 * p + 1;
+                const uint32_t e0 = __popc(bw[c].x ^ mw[k0].x) + __popc(bw[c].y ^ mw[k0].y);
+                const uint32_t e1 = __popc(bw[c].x ^ mw[k1].x) + __popc(bw[c].y ^ mw[k1].y);
+                const uint32_t P = e0 + (e1 << 16);
+                V[c][p] = V[c][p] + P - ring[r][c][p];
+                ring[r][c][p] = P;
+            }
+    };
+
+    // Horizontal 5-wide sums of V and winner-take-all of this thread's
+    // disparities for its 4 columns, merged into key buffer `buf`, row r.
+    // Keys are stored column-interleaved (index c * 32 + lane) so the 32 lanes'
+    // atomics hit 32 different banks.
+    auto emit = [&](int buf, int r) {
+        uint32_t C[kCPT][NP];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            const uint32_t h0 = __shfl_up_sync(0xffffffffu, V[2][p], 1);
+            const uint32_t h1 = __shfl_up_sync(0xffffffffu, V[3][p], 1);
+            const uint32_t h4 = __shfl_down_sync(0xffffffffu, V[0][p], 1);
+            const uint32_t h5 = __shfl_down_sync(0xffffffffu, V[1][p], 1);
+            C[0][p] = h0 + h1 + V[0][p] + V[1][p] + V[2][p];
+            C[1][p] = C[0][p] + V[3][p] - h0;
+            C[2][p] = C[1][p] + h4 - h1;
+            C[3][p] = C[2][p] + h5 - V[0][p];
+        }
+        uint32_t* krow = sKey + ((buf * kGroups + grp) * kRB + r) * kTWV + lane;
+#pragma unroll
+        for (int c = 0; c < kCPT; ++c) {
+            uint32_t k[NP];
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                k[p] = (C[c][p] << 5) + dconst[p];
+                if (EDGE) {
+                    const int dlo = dw + 2 * p;
+                    k[p] |= (dlo > lim[c] ? 0x0000FFFFu : 0u) | (dlo + 1 > lim[c] ? 0xFFFF0000u : 0u);
+                }
+            }
+            uint32_t m;
+            if (NP == 4) {
+                m = dev::min3_u16x2(k[0], k[1], k[NP > 2 ? 2 : 0]);
+                m = dev::min_u16x2(m, k[NP > 3 ? 3 : 0]);
+            } else {
+                m = dev::min_u16x2(k[0], k[NP > 1 ? 1 : 0]);
+            }
+            m = dev::min_u16x2(m, __byte_perm(m, 0u, 0x1032));  // both halves = the minimum
+            const int v = 4 * lane + c;
+            if (v >= kAR && v < kTWV - kAR) atomicMin(&krow[c * 32], m);
+        }
+    };
+
+    // Merges the groups of key buffer `buf` (rows oy0 .. oy0 + n - 1), writes
+    // or forwards the result, and resets the buffer.
+    auto flush = [&](int buf, int oy0, int n) {
+        for (int idx = tid; idx < n * kTWO; idx += NT) {
+            const int r = idx / kTWO, ox = idx - r * kTWO;
+            const int v = ox + kAR;                      // V column
+            const int slot = (v & 3) * 32 + (v >> 2);    // column-interleaved key index
+            uint32_t best = 0xFFFFFFFFu;
+#pragma unroll
+            for (int g = 0; g < kGroups; ++g) {
+                uint32_t* kp = sKey + ((buf * kGroups + g) * kRB + r) * kTWV + slot;
+                const uint32_t k16 = *kp & 0xFFFFu;
+                *kp = 0xFFFFFFFFu;
+                const uint32_t key = ((k16 & 0xFFE0u) << 11) | ((k16 & 31u) + uint32_t(dz0 + 32 * g));
+                best = min(best, key);
+            }
+            const int oy = oy0 + r, x = xs + v, y = y0 + oy;
+            if (oy < rows_here && x < a.W) {
+                if (gridDim.z == 1) {
+                    const bool valid = x >= kAR && x < a.W - kAR && y >= kAR && y < a.H - kAR;
+                    store_disp(a.out, a.out_pitch, a.out_type, x, y, valid, best);
+                } else {
+                    atomicMin(&a.keys[(size_t)y * a.W + x], best);
+                }
+            }
+        }
+    };
+
+    for (int b = 0; b < nb; ++b) {
+        const int s = b & 1;
+        const bool got = dev::mbar_wait_bounded(&bars[s], (b >> 1) & 1);
+        if (__syncthreads_or(!got)) {
+            if (tid == 0) {
+                dev::report(a.status, CT_ETIMEOUT);
+                // let the other stage's copy (if any) land before leaving
+                if (b + 1 < nb) dev::mbar_wait_bounded(&bars[s ^ 1], ((b + 1) >> 1) & 1);
+            }
+            return;
+        }
+        if (warp_active) {
+            if (b == 0) {
+#pragma unroll
+                for (int r = 0; r < kRB; ++r) accum(s, r);
+            } else {
+#pragma unroll
+                for (int r = 0; r < kRB; ++r) {
+                    emit(b & 1, r);  // output row 5b + r - 5: the window ending at row 5b + r - 1
+                    accum(s, r);
+                }
+            }
+        }
+        __syncthreads();  // stage s consumed; key buffer b & 1 complete
+        if (tid == 0 && b + 2 < nb) {
+            dev::fence_proxy_async();
+            dev::mbar_arrive_expect_tx(&bars[s], kBytes);
+            dev::tma_load_2d(sB + s * kRB * kTWV, tmB, xs, ye0 + (b + 2) * kRB, &bars[s]);
+            dev::tma_load_2d(sM + s * kRB * kMW, tmM, ms, ye0 + (b + 2) * kRB, &bars[s]);
+        }
+        if (b >= 1) flush(b & 1, kRB * b - kRB, kRB);
+    }
+    // the window ending at the last staged row
+    if (warp_active) emit(nb & 1, 0);
+    __syncthreads();
+    flush(nb & 1, kRB * nb - kRB, 1);
+}
+
+template <int DIR, int DPW>
+__global__ void __launch_bounds__(Var<DPW>::kNT, 1)
     census_match_kernel(const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmM,
                         MatchArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     uint64_t* sB = reinterpret_cast<uint64_t*>(smem_raw);   // [2][kRB][kTWV]
     uint64_t* sM = sB + 2 * kRB * kTWV;                      // [2][kRB][kMW]
-    uint32_t* sKey = reinterpret_cast<uint32_t*>(sM + 2 * kRB * kMW);  // [th][kTWO]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sKey + a.th * kTWO);  // [2]
+    uint32_t* sKey = reinterpret_cast<uint32_t*>(sM + 2 * kRB * kMW);  // [2][kGroups][kRB][kTWV]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sKey + 2 * kGroups * kRB * kTWV);  // [2]
 
     const int tid = threadIdx.x;
-    const int lane = tid & 31;
-    const int warp = tid >> 5;
     const int xs = blockIdx.x * kTWO - kAR;       // first V column
     const int y0 = blockIdx.y * a.th;             // first output row
     const int ye0 = y0 - kAR;                     // first cost row
     const int dz0 = blockIdx.z * kDPC;
-    const int dw = dz0 + warp * kDPW;
     const int ms = DIR == 0 ? xs - dz0 - kDPC : xs + dz0;  // first staged match column
-    const bool warp_active = dw < a.D;
+    const int rows_here = min(a.th, a.H - y0);
+    const int nb = (rows_here + 2 * kAR + kRB - 1) / kRB;   // batches of 5 cost rows
     const bool interior = (dz0 + kDPC <= a.D) &&
                           (DIR == 0 ? (xs >= dz0 + kDPC - 1) : (xs + dz0 + kDPC - 1 + kTWV <= a.W));
-
-    constexpr uint32_t kBytesB = kRB * kTWV * 8, kBytesM = kRB * kMW * 8;
 
     if (tid == 0) {
         dev::prefetch_tmap(&tmB);
@@ -108,149 +295,25 @@ __global__ void __launch_bounds__(kNT, 1)
         dev::mbar_init(&bars[1], 1);
         dev::fence_barrier_init();
     }
-    for (int i = tid; i < a.th * kTWO; i += kNT) sKey[i] = 0xFFFFFFFFu;
+    for (int i = tid; i < 2 * kGroups * kRB * kTWV; i += Var<DPW>::kNT) sKey[i] = 0xFFFFFFFFu;
     __syncthreads();
     if (tid == 0) {
-        for (int b = 0; b < 2 && b < a.nbatch; ++b) {
-            dev::mbar_arrive_expect_tx(&bars[b], kBytesB + kBytesM);
+        for (int b = 0; b < 2 && b < nb; ++b) {
+            dev::mbar_arrive_expect_tx(&bars[b], kRB * kTWV * 8 + kRB * kMW * 8);
             dev::tma_load_2d(sB + b * kRB * kTWV, &tmB, xs, ye0 + b * kRB, &bars[b]);
             dev::tma_load_2d(sM + b * kRB * kMW, &tmM, ms, ye0 + b * kRB, &bars[b]);
         }
     }
-
-    // Per-thread state: running vertical sums and the ring of packed costs.
-    uint32_t V[kCPT][4];
-    uint32_t ring[kRB][kCPT][4];
-#pragma unroll
-    for (int c = 0; c < kCPT; ++c)
-#pragma unroll
-        for (int p = 0; p < 4; ++p) {
-            V[c][p] = 0;
-#pragma unroll
-            for (int r = 0; r < kRB; ++r) ring[r][c][p] = 0;
-        }
-    // d mod 32 of the two disparities of each pair, packed.
-    uint32_t dconst[4];
-#pragma unroll
-    for (int p = 0; p < 4; ++p)
-        dconst[p] = uint32_t((dw + 2 * p) & 31) | (uint32_t((dw + 2 * p + 1) & 31) << 16);
-    const uint32_t dgroup = uint32_t(dw & ~31);
-    const int mstart = DIR == 0 ? 4 * lane + kDPC - 8 - kDPW * warp : 4 * lane + kDPW * warp;
-
-    for (int b = 0; b < a.nbatch; ++b) {
-        const int s = b & 1;
-        const bool got = dev::mbar_wait_bounded(&bars[s], (b >> 1) & 1);
-        if (__syncthreads_or(!got)) {
-            if (tid == 0) {
-                dev::report(a.status, CT_ETIMEOUT);
-                // let the other stage's copy (if any) land before leaving
-                if (b + 1 < a.nbatch) dev::mbar_wait_bounded(&bars[s ^ 1], ((b + 1) >> 1) & 1);
-            }
-            return;
-        }
-        if (warp_active) {
-#pragma unroll
-            for (int r = 0; r < kRB; ++r) {
-                const uint64_t* rowB = sB + (s * kRB + r) * kTWV;
-                const uint64_t* rowM = sM + (s * kRB + r) * kMW;
-                uint2 bw[kCPT], mw[12];
-                {
-                    const uint4* pb = reinterpret_cast<const uint4*>(rowB + 4 * lane);
-                    const uint4 q0 = pb[0], q1 = pb[1];
-                    bw[0] = make_uint2(q0.x, q0.y); bw[1] = make_uint2(q0.z, q0.w);
-                    bw[2] = make_uint2(q1.x, q1.y); bw[3] = make_uint2(q1.z, q1.w);
-                    const uint4* pm = reinterpret_cast<const uint4*>(rowM + mstart);
-#pragma unroll
-                    for (int k = 0; k < 6; ++k) {
-                        const uint4 q = pm[k];
-                        mw[2 * k] = make_uint2(q.x, q.y);
-                        mw[2 * k + 1] = make_uint2(q.z, q.w);
-                    }
-                }
-#pragma unroll
-                for (int c = 0; c < kCPT; ++c) {
-#pragma unroll
-                    for (int p = 0; p < 4; ++p) {
-                        const int j0 = 2 * p, j1 = 2 * p + 1;
-                        const int k0 = DIR == 0 ? c - j0 + 8 : c + j0;
-                        const int k1 = DIR == 0 ? c - j1 + 8 : c + j1;
-                        const uint32_t e0 = __popc(bw[c].x ^ mw[k0].x) + __popc(bw[c].y ^ mw[k0].y);
-                        const uint32_t e1 = __popc(bw[c].x ^ mw[k1].x) + __popc(bw[c].y ^ mw[k1].y);
-                        const uint32_t P = e0 | (e1 << 16);
-                        V[c][p] = V[c][p] + P - ring[r][c][p];
-                        ring[r][c][p] = P;
-                    }
-                }
-                const int i = b * kRB + r;  // cost row index since ye0
-                const int oy = i - 2 * kAR;
-                if (oy >= 0 && oy < a.th) {
-                    uint32_t C[kCPT][4];
-#pragma unroll
-                    for (int p = 0; p < 4; ++p) {
-                        const uint32_t h0 = __shfl_up_sync(0xffffffffu, V[2][p], 1);
-                        const uint32_t h1 = __shfl_up_sync(0xffffffffu, V[3][p], 1);
-                        const uint32_t h4 = __shfl_down_sync(0xffffffffu, V[0][p], 1);
-                        const uint32_t h5 = __shfl_down_sync(0xffffffffu, V[1][p], 1);
-                        C[0][p] = h0 + h1 + V[0][p] + V[1][p] + V[2][p];
-                        C[1][p] = C[0][p] + V[3][p] - h0;
-                        C[2][p] = C[1][p] + h4 - h1;
-                        C[3][p] = C[2][p] + h5 - V[0][p];
-                    }
-#pragma unroll
-                    for (int c = 0; c < kCPT; ++c) {
-                        const int v = 4 * lane + c;
-                        if (v < kAR || v >= kTWV - kAR) continue;
-                        uint32_t k[4];
-#pragma unroll
-                        for (int p = 0; p < 4; ++p) k[p] = (C[c][p] << 5) + dconst[p];
-                        if (!interior) {
-                            const int x = xs + v;
-                            int lim = DIR == 0 ? x - kAR : a.W - 1 - kAR - x;
-                            lim = min(lim, a.D - 1);
-#pragma unroll
-                            for (int p = 0; p < 4; ++p) {
-                                const int dlo = dw + 2 * p;
-                                k[p] |= (dlo > lim ? 0x0000FFFFu : 0u) | (dlo + 1 > lim ? 0xFFFF0000u : 0u);
-                            }
-                        }
-                        uint32_t m = dev::min3_u16x2(k[0], k[1], k[2]);
-                        m = dev::min_u16x2(m, k[3]);
-                        const uint32_t k16 = min(m & 0xFFFFu, m >> 16);
-                        const uint32_t key = ((k16 & 0xFFE0u) << 11) | ((k16 & 31u) + dgroup);
-                        atomicMin(&sKey[oy * kTWO + v - kAR], key);
-                    }
-                }
-            }
-        }
-        __syncthreads();  // every warp is done with stage s
-        if (tid == 0 && b + 2 < a.nbatch) {
-            dev::fence_proxy_async();
-            dev::mbar_arrive_expect_tx(&bars[s], kBytesB + kBytesM);
-            dev::tma_load_2d(sB + s * kRB * kTWV, &tmB, xs, ye0 + (b + 2) * kRB, &bars[s]);
-            dev::tma_load_2d(sM + s * kRB * kMW, &tmM, ms, ye0 + (b + 2) * kRB, &bars[s]);
-        }
-    }
-
-    // Output: direct when this CTA saw every disparity, else global merge.
-    const bool direct = gridDim.z == 1;
-    for (int idx = tid; idx < a.th * kTWO; idx += kNT) {
-        const int oy = idx / kTWO, ox = idx - oy * kTWO;
-        const int x = xs + kAR + ox, y = y0 + oy;
-        if (x >= a.W || y >= a.H) continue;
-        const uint32_t key = sKey[idx];
-        if (direct) {
-            const bool valid = x >= kAR && x < a.W - kAR && y >= kAR && y < a.H - kAR;
-            store_disp(a.out, a.out_pitch, a.out_type, x, y, valid, key);
-        } else {
-            atomicMin(&a.keys[(size_t)y * a.W + x], key);
-        }
-    }
+    if (interior)
+        match_body<DIR, false, DPW>(&tmB, &tmM, a, sB, sM, sKey, bars, nb, rows_here, xs, y0, ye0, dz0, ms);
+    else
+        match_body<DIR, true, DPW>(&tmB, &tmM, a, sB, sM, sKey, bars, nb, rows_here, xs, y0, ye0, dz0, ms);
 }
 
 // Converts merged keys to disparities and resets the keys for the next call.
 // (static: each translation unit that launches it has its own copy.)
 static __global__ void keys_finalize_kernel(uint32_t* keys, int W, int H, int r, void* out, size_t out_pitch,
-                                     int out_type) {
+                                            int out_type) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (x >= W) return;
@@ -259,6 +322,42 @@ static __global__ void keys_finalize_kernel(uint32_t* keys, int W, int H, int r,
     *kp = 0xFFFFFFFFu;
     const bool valid = x >= r && x < W - r && y >= r && y < H - r;
     store_disp(out, out_pitch, out_type, x, y, valid, key);
+}
+
+// Strip height: th + 4 must be a multiple of 5. Picks the height that
+// minimises (waves of CTAs over the SMs) x (cost rows per CTA), i.e. the
+// trade-off between the 4 halo rows every strip recomputes and the tail of
+// the last wave (one CTA per SM).
+inline int pick_strip_height(int W, int H, int D, int sms) {
+    const int tiles = ((W + kTWO - 1) / kTWO) * ((D + kDPC - 1) / kDPC);
+    int best = 36;
+    long best_cost = -1;
+    for (int th = 11; th <= 511; th += kRB) {
+        const int strips = (H + th - 1) / th;
+        const long ctas = long(strips) * tiles;
+        const long waves = (ctas + sms - 1) / sms;
+        const int rows = min(th, H);
+        const long cost = waves * long((rows + 2 * kAR + kRB - 1) / kRB * kRB);
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = th;
+        }
+    }
+    return best;
+}
+
+// Launches one matching pass (+ the key finalize when D is split over CTAs).
+template <int DIR>
+inline cudaError_t launch_census_match(const CUtensorMap& tb, const CUtensorMap& tm, const MatchArgs& a,
+                                       cudaStream_t s, int dpw = 4) {
+    dim3 grid((a.W + kTWO - 1) / kTWO, (a.H + a.th - 1) / a.th, (a.D + kDPC - 1) / kDPC);
+    if (dpw == 8) census_match_kernel<DIR, 8><<<grid, Var<8>::kNT, smem_bytes(), s>>>(tb, tm, a);
+    else census_match_kernel<DIR, 4><<<grid, Var<4>::kNT, smem_bytes(), s>>>(tb, tm, a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || grid.z == 1) return e;
+    keys_finalize_kernel<<<dim3((a.W + 255) / 256, a.H), 256, 0, s>>>(a.keys, a.W, a.H, kAR, a.out, a.out_pitch,
+                                                                      a.out_type);
+    return cudaGetLastError();
 }
 
 }  // namespace cm

@@ -115,20 +115,12 @@ extern "C" int ct_bm_census_process_static(const ct_image* disp, const ct_image*
         return rc;
     MatchArgs a{};
     a.W = W; a.H = H; a.D = disp_count;
-    a.th = 36;
-    a.nbatch = (a.th + 2 * kAR) / kRB;
+    a.th = pick_strip_height(W, H, disp_count, sm_count(device));
     a.keys = sc.keys;
     a.out = disp->ptr; a.out_pitch = disp->pitch_bytes; a.out_type = disp->type;
     a.status = status;
-    dim3 grid((W + kTWO - 1) / kTWO, (H + a.th - 1) / a.th, (disp_count + kDPC - 1) / kDPC);
-    const size_t smem = smem_bytes(a.th);  // below the 48 KiB default: no attribute call needed
-    if (dir == 0) census_match_kernel<0><<<grid, kNT, smem, s>>>(tb, tm, a);
-    else census_match_kernel<1><<<grid, kNT, smem, s>>>(tb, tm, a);
-    CT_LAUNCH_CHECK();
-    if (grid.z > 1) {
-        keys_finalize_kernel<<<dim3((W + 255) / 256, H), 256, 0, s>>>(sc.keys, W, H, kAR, disp->ptr,
-                                                                      disp->pitch_bytes, disp->type);
-        CT_LAUNCH_CHECK();
-    }
+    // 35.5 KB of dynamic shared memory: below the 48 KiB default, no attribute call
+    const cudaError_t e = dir == 0 ? launch_census_match<0>(tb, tm, a, s) : launch_census_match<1>(tb, tm, a, s);
+    if (e != cudaSuccess) return fail(CT_ECUDA, "census match launch failed: %s", cudaGetErrorString(e));
     return CT_OK;
 }

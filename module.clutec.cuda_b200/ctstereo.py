@@ -119,6 +119,9 @@ def _declare(L: C.CDLL) -> None:
         "ct_bm_census_process": [H, img, img, img, C.c_void_p],
         "ct_bm_census_process_lr": [H, img, img, img, C.c_int32, img, img, C.c_void_p],
         "ct_bm_census_match_desc": [H, img, img, img, C.c_int32, C.c_void_p],
+        "ct_bm_census_autotune": [H, img, img, C.c_void_p],
+        "ct_bm_census_tuning": [H, P(C.c_int32), P(C.c_int32)],
+        "ct_bm_census_set_tuning": [H, C.c_int32, C.c_int32],
         "ct_bm_census_process_static": [img, img, img, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p],
         "ct_bm_sad_create": [P(H)],
         "ct_bm_sad_configure": [H, C.c_int32, fmt, P(ct_sad_params)],
@@ -252,6 +255,19 @@ class BlockMatcherCensus(_Driver):
     def process(self, disp, left, right, stream=None):
         check(lib().ct_bm_census_process(self._h, _img_ref(disp), _img_ref(left), _img_ref(right),
                                          _stream(stream)))
+
+    def autotune(self, left, right, stream=None):
+        """Times the launch-shape candidates on these images; keeps the fastest."""
+        check(lib().ct_bm_census_autotune(self._h, _img_ref(left), _img_ref(right), _stream(stream)))
+        return self.tuning()
+
+    def set_tuning(self, strip_height: int, disp_per_warp: int):
+        check(lib().ct_bm_census_set_tuning(self._h, strip_height, disp_per_warp))
+
+    def tuning(self):
+        th, dpw = C.c_int32(), C.c_int32()
+        check(lib().ct_bm_census_tuning(self._h, C.byref(th), C.byref(dpw)))
+        return {"strip_height": th.value, "disp_per_warp": dpw.value}
 
     def match_desc(self, disp, desc_base, desc_match, left_to_right=True, stream=None):
         """Matching on precomputed 9x7 census descriptors (int64 tensors)."""

@@ -145,3 +145,40 @@ def test_format_mismatch_is_an_error(ct, cuda):
     with pytest.raises(ct.CtError) as e:
         m.process(f, a, a)
     assert e.value.code == ct.CT_ETYPE
+
+
+@pytest.mark.parametrize("dpw", [4, 8])
+@pytest.mark.parametrize("th", [11, 36, 121, 511])
+def test_every_launch_shape_is_bit_exact(ct, oracle, cuda, dpw, th):
+    """Results do not depend on the kernel variant or strip height."""
+    W, H, D = 301, 157, 100
+    L, R = pair(ct, 2, 9, W, H, D - 1)
+    want, _ = oracle.match_census(L, R, D, 2, True)
+    wrl, _ = oracle.match_census(L, R, D, 2, False)
+    m = ct.BlockMatcherCensus()
+    m.configure(0, W, H, D)
+    m.set_tuning(th, dpw)
+    assert m.tuning() == {"strip_height": th, "disp_per_warp": dpw}
+    lr = ct.alloc_image(H, W, torch.uint8, cuda)
+    rl = ct.alloc_image(H, W, torch.uint8, cuda)
+    m.process_lr(to_dev(L, cuda), to_dev(R, cuda), disp_lr=lr, disp_rl=rl)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(lr.cpu().numpy(), oracle.to_u8(want))
+    np.testing.assert_array_equal(rl.cpu().numpy(), oracle.to_u8(wrl))
+
+
+def test_autotune_keeps_results(ct, oracle, cuda):
+    W, H, D = 640, 480, 64
+    L, R = pair(ct, 1, 21, W, H, D - 1)
+    m = ct.BlockMatcherCensus()
+    m.configure(0, W, H, D)
+    dl, dr = to_dev(L, cuda), to_dev(R, cuda)
+    t = m.autotune(dl, dr)
+    assert t["disp_per_warp"] in (4, 8) and (t["strip_height"] + 4) % 5 == 0
+    out = ct.alloc_image(H, W, torch.uint8, cuda)
+    m.process(out, dl, dr)
+    torch.cuda.synchronize()
+    want, _ = oracle.match_census(L, R, D)
+    np.testing.assert_array_equal(out.cpu().numpy(), oracle.to_u8(want))
+    with pytest.raises(ct.CtError):
+        m.set_tuning(12, 4)
