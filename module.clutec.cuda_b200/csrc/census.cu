@@ -280,12 +280,13 @@ int ct_bm_census_configure(ct_handle* hh, int32_t device, const ct_format* fmt, 
     const uint64_t pb = h->desc_pitch * 8;
     h->fmt = *fmt;  // left_desc() / right_desc() below depend on the height
     h->th = cm::pick_strip_height(W, H, p->disp_count, sm_count(device));
+    CT_CUDA_TRY(cm::prepare_census_match());
     h->par = *p;
     using namespace cm;
-    if (int rc = make_tmap_2d(&h->tm_lb, h->left_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kTWV, kRB)) return rc;
-    if (int rc = make_tmap_2d(&h->tm_rb, h->right_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kTWV, kRB)) return rc;
-    if (int rc = make_tmap_2d(&h->tm_lm, h->left_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kMW, kRB)) return rc;
-    if (int rc = make_tmap_2d(&h->tm_rm, h->right_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kMW, kRB)) return rc;
+    if (int rc = make_tmap_2d(&h->tm_lb, h->left_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kTWV, kBR)) return rc;
+    if (int rc = make_tmap_2d(&h->tm_rb, h->right_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kTWV, kBR)) return rc;
+    if (int rc = make_tmap_2d(&h->tm_lm, h->left_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kMW, kBR)) return rc;
+    if (int rc = make_tmap_2d(&h->tm_rm, h->right_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kMW, kBR)) return rc;
     h->configured = true;
     return CT_OK;
 }
@@ -444,10 +445,10 @@ int ct_bm_census_match_desc(ct_handle* hh, const ct_image* disp, const ct_image*
     const int W = h->fmt.width, H = h->fmt.height;
     CUtensorMap tb, tm;
     if (int rc = make_tmap_2d(&tb, desc_base->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, desc_base->pitch_bytes,
-                              cm::kTWV, cm::kRB))
+                              cm::kTWV, cm::kBR))
         return rc;
     if (int rc = make_tmap_2d(&tm, desc_match->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H,
-                              desc_match->pitch_bytes, cm::kMW, cm::kRB))
+                              desc_match->pitch_bytes, cm::kMW, cm::kBR))
         return rc;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     h->last_stream = s;

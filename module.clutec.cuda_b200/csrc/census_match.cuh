@@ -9,10 +9,11 @@
 //    (DPW = 4: 16 warps of <= 128 registers; DPW = 8: 8 warps) and lane L owns
 //    the 4 adjacent columns 4L..4L+3.
 //  * Descriptor rows are staged in shared memory by 2D TMA tile loads (one box
-//    of 5 rows of the base view and one of the match view per batch), two
-//    batches in flight, completion tracked by mbarriers with bounded waits.
+//    of 10 rows of the base view and one of the match view per batch), two
+//    batches in flight, completion tracked by mbarriers with bounded waits;
+//    one CTA barrier per batch.
 //  * Each thread keeps, in registers, the vertical running sums V of its 4
-//    columns x 8 disparities and a 5-deep ring of the per-row Hamming costs
+//    columns x DPW disparities and a 5-deep ring of the per-row Hamming costs
 //    (the role of AlgoArraySum_W32H16::SumCache's vertical pass,
 //    Kernel.Algo.ArraySum_W32H16.h:163-182). Costs for two disparities are
 //    packed in the two 16-bit halves of one register, so every add/sub of the
@@ -26,13 +27,13 @@
 //    integer pipes do the rest.
 //  * Winner-take-all folds the disparity into the low 5 bits of each 16-bit
 //    lane (key = C << 5 | d mod 32, C <= 25 * 63 = 1575 so it fits): the min
-//    over a thread's disparities is one or two packed mins plus a half swap, and the
-//    lowest d wins ties by construction (the reference's strict '<' scanning
-//    d upward). Warps of one 32-disparity group merge with a shared-memory
-//    atomicMin; the two groups of a CTA are merged, converted to
-//    (C << 16 | d) and flushed after every batch of 5 rows, directly into the
-//    disparity map when the CTA saw all D, else through a global atomicMin
-//    whose keys a finalize kernel turns into disparities.
+//    over a thread's disparities is one or two packed mins plus a half swap,
+//    and the lowest d wins ties by construction (the reference's strict '<'
+//    scanning d upward). Warps of one 32-disparity group merge with a
+//    shared-memory atomicMin; the two groups of a CTA are merged, converted to
+//    (C << 16 | d) and flushed after every batch, directly into the disparity
+//    map when the CTA saw all D, else through a global atomicMin whose keys a
+//    finalize kernel turns into disparities.
 #pragma once
 
 #include <cstdint>
@@ -48,19 +49,20 @@ constexpr int kAR = 2;                  // aggregation radius (5x5)
 constexpr int kTWO = kTWV - 2 * kAR;    // 124 output columns per tile
 constexpr int kDPC = 64;                // disparities per CTA
 constexpr int kGroups = kDPC / 32;      // key groups of 32 disparities
+constexpr int kRB = 2 * kAR + 1;        // ring depth = vertical window = 5
+constexpr int kBR = 2 * kRB;            // cost rows per TMA batch = 10
+constexpr int kMW = kTWV + kDPC;        // 192 match columns staged per row
+
 // Variant: disparities per warp (8 = 8 warps of 255 registers, one CTA of 8
 // warps per SM; 4 = 16 warps of at most 128 registers, 16 warps per SM).
 template <int DPW>
 struct Var {
-    static constexpr int kDPW = DPW;
     static constexpr int kNP = DPW / 2;           // packed pairs per thread
     static constexpr int kNW = kDPC / DPW;        // warps per CTA
     static constexpr int kNT = kNW * 32;          // threads per CTA
     static constexpr int kWords = DPW + 4;        // match descriptors a thread reads per row
     static constexpr int kWarpsPerGroup = 32 / DPW;
 };
-constexpr int kRB = 2 * kAR + 1;        // rows per TMA batch = ring depth = 5
-constexpr int kMW = kTWV + kDPC;        // 192 match columns staged per row
 
 struct MatchArgs {
     int W, H, D;
@@ -72,10 +74,12 @@ struct MatchArgs {
     int32_t* status;
 };
 
-// Shared memory: 2 stages of base (5 x 128) and match (5 x 192) descriptor
-// rows, 2 buffers x 2 groups x 5 rows x 128 key slots, 2 mbarriers. 35.6 KB.
+// Shared memory: 2 stages of base (10 x 128) and match (10 x 192) descriptor
+// rows, 2 buffers x 2 groups x 10 rows x 128 key slots, 2 mbarriers and a
+// flag. 70 KB.
 __host__ __device__ constexpr size_t smem_bytes() {
-    return size_t(2) * kRB * kTWV * 8 + size_t(2) * kRB * kMW * 8 + size_t(2) * kGroups * kRB * kTWV * 4 + 2 * 8;
+    return size_t(2) * kBR * kTWV * 8 + size_t(2) * kBR * kMW * 8 + size_t(2) * kGroups * kBR * kTWV * 4 + 2 * 8 +
+           16;
 }
 
 // Disparity code for an output pixel from its merged key (C << 16 | d).
@@ -93,11 +97,12 @@ __device__ __forceinline__ void store_disp(void* out, size_t pitch, int type, in
 
 template <int DIR, bool EDGE, int DPW>
 __device__ __forceinline__ void match_body(const CUtensorMap* tmB, const CUtensorMap* tmM, const MatchArgs& a,
-                                           uint64_t* sB, uint64_t* sM, uint32_t* sKey, uint64_t* bars, int nb,
-                                           int rows_here, int xs, int y0, int ye0, int dz0, int ms) {
+                                           uint64_t* sB, uint64_t* sM, uint32_t* sKey, uint64_t* bars,
+                                           int* sflag, int nb, int rows_here, int xs, int y0, int ye0, int dz0,
+                                           int ms) {
     using VT = Var<DPW>;
     constexpr int NP = VT::kNP, NT = VT::kNT, NWD = VT::kWords;
-    constexpr uint32_t kBytes = kRB * kTWV * 8 + kRB * kMW * 8;
+    constexpr uint32_t kBytes = kBR * kTWV * 8 + kBR * kMW * 8;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -128,10 +133,10 @@ __device__ __forceinline__ void match_body(const CUtensorMap* tmB, const CUtenso
     // first match descriptor this thread reads per row (an even index)
     const int mstart = DIR == 0 ? 4 * lane + kDPC - DPW - DPW * warp : 4 * lane + DPW * warp;
 
-    // Adds cost row r of stage s to the running sums.
+    // Adds cost row r of stage s to the running sums (ring slot r mod 5).
     auto accum = [&](int s, int r) {
-        const uint64_t* rowB = sB + (s * kRB + r) * kTWV;
-        const uint64_t* rowM = sM + (s * kRB + r) * kMW;
+        const uint64_t* rowB = sB + (s * kBR + r) * kTWV;
+        const uint64_t* rowM = sM + (s * kBR + r) * kMW;
         uint2 bw[kCPT], mw[NWD];
         const uint4* pb = reinterpret_cast<const uint4*>(rowB + 4 * lane);
         const uint4 q0 = pb[0], q1 = pb[1];
@@ -144,6 +149,7 @@ __device__ __forceinline__ void match_body(const CUtensorMap* tmB, const CUtenso
             mw[2 * k] = make_uint2(q.x, q.y);
             mw[2 * k + 1] = make_uint2(q.z, q.w);
         }
+        const int slot = r % kRB;
 #pragma unroll
         for (int c = 0; c < kCPT; ++c)
 #pragma unroll
@@ -154,15 +160,16 @@ __device__ __forceinline__ void match_body(const CUtensorMap* tmB, const CUtenso
                 const uint32_t e0 = __popc(bw[c].x ^ mw[k0].x) + __popc(bw[c].y ^ mw[k0].y);
                 const uint32_t e1 = __popc(bw[c].x ^ mw[k1].x) + __popc(bw[c].y ^ mw[k1].y);
                 const uint32_t P = e0 + (e1 << 16);
-                V[c][p] = V[c][p] + P - ring[r][c][p];
-                ring[r][c][p] = P;
+                V[c][p] = V[c][p] + P - ring[slot][c][p];
+                ring[slot][c][p] = P;
             }
     };
 
     // Horizontal 5-wide sums of V and winner-take-all of this thread's
-    // disparities for its 4 columns, merged into key buffer `buf`, row r.
+    // disparities for its 4 columns, merged into key buffer `buf`, slot r.
     // Keys are stored column-interleaved (index c * 32 + lane) so the 32 lanes'
-    // atomics hit 32 different banks.
+    // atomics hit 32 different banks; the halo columns' slots (V columns 0, 1,
+    // 126, 127) receive values nobody reads.
     auto emit = [&](int buf, int r) {
         uint32_t C[kCPT][NP];
 #pragma unroll
@@ -176,7 +183,7 @@ __device__ __forceinline__ void match_body(const CUtensorMap* tmB, const CUtenso
             C[2][p] = C[1][p] + h4 - h1;
             C[3][p] = C[2][p] + h5 - V[0][p];
         }
-        uint32_t* krow = sKey + ((buf * kGroups + grp) * kRB + r) * kTWV + lane;
+        uint32_t* krow = sKey + ((buf * kGroups + grp) * kBR + r) * kTWV + lane;
 #pragma unroll
         for (int c = 0; c < kCPT; ++c) {
             uint32_t k[NP];
@@ -196,29 +203,28 @@ __device__ __forceinline__ void match_body(const CUtensorMap* tmB, const CUtenso
                 m = dev::min_u16x2(k[0], k[NP > 1 ? 1 : 0]);
             }
             m = dev::min_u16x2(m, __byte_perm(m, 0u, 0x1032));  // both halves = the minimum
-            const int v = 4 * lane + c;
-            if (v >= kAR && v < kTWV - kAR) atomicMin(&krow[c * 32], m);
+            atomicMin(&krow[c * 32], m);
         }
     };
 
-    // Merges the groups of key buffer `buf` (rows oy0 .. oy0 + n - 1), writes
-    // or forwards the result, and resets the buffer.
-    auto flush = [&](int buf, int oy0, int n) {
-        for (int idx = tid; idx < n * kTWO; idx += NT) {
-            const int r = idx / kTWO, ox = idx - r * kTWO;
+    // Merges the groups of key buffer `buf`, slots r0 .. r1-1 (output row
+    // oy0 + slot), writes or forwards the result, and resets the slots.
+    auto flush = [&](int buf, int oy0, int r0, int r1) {
+        for (int idx = tid; idx < (r1 - r0) * kTWO; idx += NT) {
+            const int r = r0 + idx / kTWO, ox = idx % kTWO;
             const int v = ox + kAR;                      // V column
             const int slot = (v & 3) * 32 + (v >> 2);    // column-interleaved key index
             uint32_t best = 0xFFFFFFFFu;
 #pragma unroll
             for (int g = 0; g < kGroups; ++g) {
-                uint32_t* kp = sKey + ((buf * kGroups + g) * kRB + r) * kTWV + slot;
+                uint32_t* kp = sKey + ((buf * kGroups + g) * kBR + r) * kTWV + slot;
                 const uint32_t k16 = *kp & 0xFFFFu;
                 *kp = 0xFFFFFFFFu;
                 const uint32_t key = ((k16 & 0xFFE0u) << 11) | ((k16 & 31u) + uint32_t(dz0 + 32 * g));
                 best = min(best, key);
             }
             const int oy = oy0 + r, x = xs + v, y = y0 + oy;
-            if (oy < rows_here && x < a.W) {
+            if (oy >= 0 && oy < rows_here && x < a.W) {
                 if (gridDim.z == 1) {
                     const bool valid = x >= kAR && x < a.W - kAR && y >= kAR && y < a.H - kAR;
                     store_disp(a.out, a.out_pitch, a.out_type, x, y, valid, best);
@@ -229,42 +235,46 @@ __device__ __forceinline__ void match_body(const CUtensorMap* tmB, const CUtenso
         }
     };
 
+    // Cost row i = kBR * b + r. Before row i is added, V holds rows i-5..i-1:
+    // the window of output row i - 5, whose keys go to buffer b & 1, slot r.
     for (int b = 0; b < nb; ++b) {
         const int s = b & 1;
-        const bool got = dev::mbar_wait_bounded(&bars[s], (b >> 1) & 1);
-        if (__syncthreads_or(!got)) {
-            if (tid == 0) {
-                dev::report(a.status, CT_ETIMEOUT);
-                // let the other stage's copy (if any) land before leaving
-                if (b + 1 < nb) dev::mbar_wait_bounded(&bars[s ^ 1], ((b + 1) >> 1) & 1);
-            }
-            return;
-        }
+        if (!dev::mbar_wait_bounded(&bars[s], (b >> 1) & 1)) *sflag = 1;
         if (warp_active) {
             if (b == 0) {
 #pragma unroll
-                for (int r = 0; r < kRB; ++r) accum(s, r);
+                for (int r = 0; r < kBR; ++r) {
+                    if (r >= kRB) emit(0, r);
+                    accum(s, r);
+                }
             } else {
 #pragma unroll
-                for (int r = 0; r < kRB; ++r) {
-                    emit(b & 1, r);  // output row 5b + r - 5: the window ending at row 5b + r - 1
+                for (int r = 0; r < kBR; ++r) {
+                    emit(b & 1, r);
                     accum(s, r);
                 }
             }
         }
         __syncthreads();  // stage s consumed; key buffer b & 1 complete
+        if (*sflag) {     // a tile load never arrived: report and leave together
+            if (tid == 0) {
+                dev::report(a.status, CT_ETIMEOUT);
+                if (b + 1 < nb) dev::mbar_wait_bounded(&bars[s ^ 1], ((b + 1) >> 1) & 1);
+            }
+            return;
+        }
         if (tid == 0 && b + 2 < nb) {
             dev::fence_proxy_async();
             dev::mbar_arrive_expect_tx(&bars[s], kBytes);
-            dev::tma_load_2d(sB + s * kRB * kTWV, tmB, xs, ye0 + (b + 2) * kRB, &bars[s]);
-            dev::tma_load_2d(sM + s * kRB * kMW, tmM, ms, ye0 + (b + 2) * kRB, &bars[s]);
+            dev::tma_load_2d(sB + s * kBR * kTWV, tmB, xs, ye0 + (b + 2) * kBR, &bars[s]);
+            dev::tma_load_2d(sM + s * kBR * kMW, tmM, ms, ye0 + (b + 2) * kBR, &bars[s]);
         }
-        if (b >= 1) flush(b & 1, kRB * b - kRB, kRB);
+        flush(b & 1, kBR * b - kRB, b == 0 ? kRB : 0, kBR);
     }
-    // the window ending at the last staged row
+    // the window ending at the last staged row: output kBR * nb - 5, buffer nb & 1, slot 0
     if (warp_active) emit(nb & 1, 0);
     __syncthreads();
-    flush(nb & 1, kRB * nb - kRB, 1);
+    flush(nb & 1, kBR * nb - kRB, 0, 1);
 }
 
 template <int DIR, int DPW>
@@ -272,10 +282,11 @@ __global__ void __launch_bounds__(Var<DPW>::kNT, 1)
     census_match_kernel(const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmM,
                         MatchArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    uint64_t* sB = reinterpret_cast<uint64_t*>(smem_raw);   // [2][kRB][kTWV]
-    uint64_t* sM = sB + 2 * kRB * kTWV;                      // [2][kRB][kMW]
-    uint32_t* sKey = reinterpret_cast<uint32_t*>(sM + 2 * kRB * kMW);  // [2][kGroups][kRB][kTWV]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sKey + 2 * kGroups * kRB * kTWV);  // [2]
+    uint64_t* sB = reinterpret_cast<uint64_t*>(smem_raw);   // [2][kBR][kTWV]
+    uint64_t* sM = sB + 2 * kBR * kTWV;                      // [2][kBR][kMW]
+    uint32_t* sKey = reinterpret_cast<uint32_t*>(sM + 2 * kBR * kMW);  // [2][kGroups][kBR][kTWV]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sKey + 2 * kGroups * kBR * kTWV);  // [2]
+    int* sflag = reinterpret_cast<int*>(bars + 2);
 
     const int tid = threadIdx.x;
     const int xs = blockIdx.x * kTWO - kAR;       // first V column
@@ -284,7 +295,7 @@ __global__ void __launch_bounds__(Var<DPW>::kNT, 1)
     const int dz0 = blockIdx.z * kDPC;
     const int ms = DIR == 0 ? xs - dz0 - kDPC : xs + dz0;  // first staged match column
     const int rows_here = min(a.th, a.H - y0);
-    const int nb = (rows_here + 2 * kAR + kRB - 1) / kRB;   // batches of 5 cost rows
+    const int nb = (rows_here + 2 * kAR + kBR - 1) / kBR;   // batches of 10 cost rows
     const bool interior = (dz0 + kDPC <= a.D) &&
                           (DIR == 0 ? (xs >= dz0 + kDPC - 1) : (xs + dz0 + kDPC - 1 + kTWV <= a.W));
 
@@ -294,20 +305,21 @@ __global__ void __launch_bounds__(Var<DPW>::kNT, 1)
         dev::mbar_init(&bars[0], 1);
         dev::mbar_init(&bars[1], 1);
         dev::fence_barrier_init();
+        *sflag = 0;
     }
-    for (int i = tid; i < 2 * kGroups * kRB * kTWV; i += Var<DPW>::kNT) sKey[i] = 0xFFFFFFFFu;
+    for (int i = tid; i < 2 * kGroups * kBR * kTWV; i += Var<DPW>::kNT) sKey[i] = 0xFFFFFFFFu;
     __syncthreads();
     if (tid == 0) {
         for (int b = 0; b < 2 && b < nb; ++b) {
-            dev::mbar_arrive_expect_tx(&bars[b], kRB * kTWV * 8 + kRB * kMW * 8);
-            dev::tma_load_2d(sB + b * kRB * kTWV, &tmB, xs, ye0 + b * kRB, &bars[b]);
-            dev::tma_load_2d(sM + b * kRB * kMW, &tmM, ms, ye0 + b * kRB, &bars[b]);
+            dev::mbar_arrive_expect_tx(&bars[b], kBR * kTWV * 8 + kBR * kMW * 8);
+            dev::tma_load_2d(sB + b * kBR * kTWV, &tmB, xs, ye0 + b * kBR, &bars[b]);
+            dev::tma_load_2d(sM + b * kBR * kMW, &tmM, ms, ye0 + b * kBR, &bars[b]);
         }
     }
     if (interior)
-        match_body<DIR, false, DPW>(&tmB, &tmM, a, sB, sM, sKey, bars, nb, rows_here, xs, y0, ye0, dz0, ms);
+        match_body<DIR, false, DPW>(&tmB, &tmM, a, sB, sM, sKey, bars, sflag, nb, rows_here, xs, y0, ye0, dz0, ms);
     else
-        match_body<DIR, true, DPW>(&tmB, &tmM, a, sB, sM, sKey, bars, nb, rows_here, xs, y0, ye0, dz0, ms);
+        match_body<DIR, true, DPW>(&tmB, &tmM, a, sB, sM, sKey, bars, sflag, nb, rows_here, xs, y0, ye0, dz0, ms);
 }
 
 // Converts merged keys to disparities and resets the keys for the next call.
@@ -324,26 +336,40 @@ static __global__ void keys_finalize_kernel(uint32_t* keys, int W, int H, int r,
     store_disp(out, out_pitch, out_type, x, y, valid, key);
 }
 
-// Strip height: th + 4 must be a multiple of 5. Picks the height that
-// minimises (waves of CTAs over the SMs) x (cost rows per CTA), i.e. the
-// trade-off between the 4 halo rows every strip recomputes and the tail of
-// the last wave (one CTA per SM).
+// Strip height: picks the height that minimises (waves of CTAs over the SMs)
+// x (cost rows per CTA), i.e. the trade-off between the 4 halo rows every
+// strip recomputes and the tail of the last wave (one CTA per SM). Heights
+// with th + 4 a multiple of 10 waste no staged rows.
 inline int pick_strip_height(int W, int H, int D, int sms) {
     const int tiles = ((W + kTWO - 1) / kTWO) * ((D + kDPC - 1) / kDPC);
     int best = 36;
     long best_cost = -1;
-    for (int th = 11; th <= 511; th += kRB) {
+    for (int th = 16; th <= 506; th += kBR) {
         const int strips = (H + th - 1) / th;
         const long ctas = long(strips) * tiles;
         const long waves = (ctas + sms - 1) / sms;
         const int rows = min(th, H);
-        const long cost = waves * long((rows + 2 * kAR + kRB - 1) / kRB * kRB);
+        const long cost = waves * long((rows + 2 * kAR + kBR - 1) / kBR * kBR);
         if (best_cost < 0 || cost < best_cost) {
             best_cost = cost;
             best = th;
         }
     }
     return best;
+}
+
+// Allows the 70 KB of dynamic shared memory on the current device for every
+// kernel instantiation. Sets function attributes only (no allocation).
+inline cudaError_t prepare_census_match() {
+    const int smem = int(smem_bytes());
+    cudaError_t e = cudaFuncSetAttribute(census_match_kernel<0, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(census_match_kernel<0, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(census_match_kernel<1, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(census_match_kernel<1, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    return e;
 }
 
 // Launches one matching pass (+ the key finalize when D is split over CTAs).

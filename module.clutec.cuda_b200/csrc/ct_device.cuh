@@ -12,7 +12,7 @@ namespace dev {
 // if a phase has not completed after this many polls (each try_wait may
 // suspend the thread for a while), the wait gives up and the kernel reports
 // CT_ETIMEOUT through its status word instead of hanging the GPU.
-constexpr uint32_t kWaitLimit = 1u << 22;
+constexpr uint32_t kWaitLimit = 1u << 20;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));

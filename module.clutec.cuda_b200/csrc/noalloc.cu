@@ -64,6 +64,7 @@ int static_scratch(int device, StaticScratch* out) {
         CT_CUDA_TRY(cudaGetSymbolAddress(reinterpret_cast<void**>(&t.desc), g_static_desc));
         CT_CUDA_TRY(cudaGetSymbolAddress(reinterpret_cast<void**>(&t.keys), g_static_keys));
         CT_CUDA_TRY(cudaGetSymbolAddress(reinterpret_cast<void**>(&t.status), g_static_status));
+        CT_CUDA_TRY(cm::prepare_census_match());  // function attributes only
         s = t;
     }
     *out = s;
@@ -109,9 +110,9 @@ extern "C" int ct_bm_census_process_static(const ct_image* disp, const ct_image*
     if (int rc = census::launch9x7(right, dr, pitch, status, s)) return rc;
     const int dir = left_to_right ? 0 : 1;
     CUtensorMap tb, tm;
-    if (int rc = make_tmap_2d(&tb, dir == 0 ? dl : dr, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pitch * 8, kTWV, kRB))
+    if (int rc = make_tmap_2d(&tb, dir == 0 ? dl : dr, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pitch * 8, kTWV, kBR))
         return rc;
-    if (int rc = make_tmap_2d(&tm, dir == 0 ? dr : dl, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pitch * 8, kMW, kRB))
+    if (int rc = make_tmap_2d(&tm, dir == 0 ? dr : dl, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pitch * 8, kMW, kBR))
         return rc;
     MatchArgs a{};
     a.W = W; a.H = H; a.D = disp_count;
@@ -119,7 +120,6 @@ extern "C" int ct_bm_census_process_static(const ct_image* disp, const ct_image*
     a.keys = sc.keys;
     a.out = disp->ptr; a.out_pitch = disp->pitch_bytes; a.out_type = disp->type;
     a.status = status;
-    // 35.5 KB of dynamic shared memory: below the 48 KiB default, no attribute call
     const cudaError_t e = dir == 0 ? launch_census_match<0>(tb, tm, a, s) : launch_census_match<1>(tb, tm, a, s);
     if (e != cudaSuccess) return fail(CT_ECUDA, "census match launch failed: %s", cudaGetErrorString(e));
     return CT_OK;
