@@ -236,15 +236,14 @@ def run_ours(args):
         step_ms = [a.elapsed_time(b) for a, b in ev]
         total_ms = max_over_ranks(sum(step_ms))
 
-        # dominant kernel alone: one direction on precomputed descriptors
+        # dominant kernel: one left-to-right pass (census of both images +
+        # census_match_kernel) minus the two census transforms, both timed
+        # here with events on the launching stream
         desc_l = ct.alloc_image(H_, W_, torch.int64, dev)
-        desc_r = ct.alloc_image(H_, W_, torch.int64, dev)
         cen = ct.CensusTransform()
         cen.configure(local, W_, H_)
-        cen.process(desc_l, dL, stream=stream)
-        cen.process(desc_r, dR, stream=stream)
         for _ in range(3):
-            m.match_desc(lr, desc_l, desc_r, True, stream=stream)
+            m.process(lr, dL, dR, stream=stream)
         kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                for _ in range(args.steps)]
         cev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -253,16 +252,16 @@ def run_ours(args):
         for k in range(args.steps):
             flush()
             kev[k][0].record(stream)
-            m.match_desc(lr, desc_l, desc_r, True, stream=stream)
+            m.process(lr, dL, dR, stream=stream)
             kev[k][1].record(stream)
             flush()
             cev[k][0].record(stream)
             cen.process(desc_l, dL, stream=stream)
-            cen.process(desc_r, dR, stream=stream)
+            cen.process(desc_l, dR, stream=stream)
             cev[k][1].record(stream)
         barrier()
-        match_ms = sum(a.elapsed_time(b) for a, b in kev) / args.steps
         census_ms = sum(a.elapsed_time(b) for a, b in cev) / args.steps
+        match_ms = sum(a.elapsed_time(b) for a, b in kev) / args.steps - census_ms
 
         # end-to-end through the public API with host buffers
         hL = torch.from_numpy(L).pin_memory()
@@ -311,7 +310,7 @@ def run_ours(args):
     units_launch = W_ * H_ * D_
     achieved_popc = 2.0 * units_launch / (match_ms * 1e-3)          # 2 POPC per unit
     int_peak = rates["iadd3_per_clk_sm"] * sms * clock_hz
-    launches = 7  # census x2, match x2 (+ key finalize x2 since D > 64), cross-check
+    launches = 5  # census x2, census_match_kernel x2 (D halves merged in-kernel), cross-check
 
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -327,7 +326,7 @@ def run_ours(args):
                      "peak": round(popc_peak / 1e12, 4), "unit": "Tpopc/s",
                      "frac": round(achieved_popc / popc_peak, 4),
                      "traffic": traffic_from_profile(),
-                     "kernel": "census_match_kernel<0> (one direction, 1920x1080x128)",
+                     "kernel": "census_match_kernel<0> (one direction, 1920x1080x128; timed as process() minus the two census transforms)",
                      "kernel_ms": round(match_ms, 4), "census_transform_ms": round(census_ms, 4),
                      "algorithmic_per_unit": "2 POPC + ~9 INT per pixel x disparity",
                      "int_frac_at_9_ops": round(9.0 * units_launch / (match_ms * 1e-3) / int_peak, 4),

@@ -184,7 +184,8 @@ int ct_bm_census_set_tuning(ct_handle* h, int32_t strip_height, int32_t disp_per
  * results as ct_bm_census_process with {disp_count, agg_radius 2,
  * left_to_right}, no handle; its scratch is a fixed static device array of
  * 40 MiB per GPU that loads the library, so images are limited to 2,097,152
- * pixels with rows rounded up to 32 (1920 x 1080 fits; larger -> CT_EINVAL).
+ * pixels with rows rounded up to a multiple of 4 (1920 x 1080 fits; larger
+ * -> CT_EINVAL).
  * Runs on the current device. Its first call on a device looks up the array
  * addresses: make it before any stream capture. Calls share the array, so
  * calls that overlap on the GPU race; serialise them. device_status

@@ -25,7 +25,7 @@ constexpr int kBoxH = kTY + 6;
 
 __global__ void __launch_bounds__(kNT) census9x7_kernel(const __grid_constant__ CUtensorMap tm_img, int W, int H,
                                                          uint64_t* out, size_t out_pitch_elems,
-                                                         int32_t* status) {
+                                                         int32_t* status, int planar) {
     __shared__ __align__(128) uint8_t tile[kBoxH * kBoxW];
     __shared__ __align__(8) uint64_t bar;
     const int tid = threadIdx.x;
@@ -77,7 +77,8 @@ __global__ void __launch_bounds__(kNT) census9x7_kernel(const __grid_constant__ 
             }
         const bool inside = x >= 4 && x < W - 4 && y >= 3 && y < H - 3;
         const uint64_t d = inside ? ((uint64_t(hi) << 32) | lo) : 0ull;
-        out[(size_t)y * out_pitch_elems + x] = d;
+        // planar: the matcher's pair-planar scratch layout (cm::planar_index)
+        out[planar ? cm::planar_index(x, y, W) : (size_t)y * out_pitch_elems + x] = d;
     }
 }
 
@@ -103,18 +104,27 @@ __global__ void census3x3_kernel(const uint8_t* img, size_t pitch, int W, int H,
     out[(size_t)y * out_pitch + x] = uint8_t(v);
 }
 
-int launch9x7(const ct_image* src, uint64_t* dst, size_t dst_pitch_elems, int32_t* status, cudaStream_t s) {
+// Natural layout (dst row pitch in elements) or, with planar = 1, the
+// matcher's pair-planar scratch layout (pitch ignored).
+int launch9x7(const ct_image* src, uint64_t* dst, size_t dst_pitch_elems, int32_t* status, cudaStream_t s,
+              int planar) {
     CUtensorMap tm;
     if (int rc = make_tmap_2d(&tm, src->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, src->width, src->height,
                               src->pitch_bytes, kBoxW, kBoxH))
         return rc;
     dim3 grid((src->width + kTX - 1) / kTX, (src->height + kTY - 1) / kTY);
-    census9x7_kernel<<<grid, kNT, 0, s>>>(tm, src->width, src->height, dst, dst_pitch_elems, status);
+    census9x7_kernel<<<grid, kNT, 0, s>>>(tm, src->width, src->height, dst, dst_pitch_elems, status, planar);
     CT_LAUNCH_CHECK();
     return CT_OK;
 }
 
 }  // namespace census
+
+// Natural-layout descriptors (row pitch in elements) -> pair-planar scratch.
+__global__ void to_planar_kernel(const uint64_t* src, size_t src_pitch, uint64_t* dst, int W, int H) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x < W && y < H) dst[cm::planar_index(x, y, W)] = src[(size_t)y * src_pitch + x];
+}
 
 // ---------------------------------------------------------------------------
 // CensusTransform::CDriver
@@ -134,6 +144,7 @@ struct BmCensusHandle : ct_handle {
         if (device >= 0) cudaSetDevice(device);
         cudaFree(desc);
         cudaFree(keys);
+        cudaFree(counters);
         cudaFree(tmp_lr);
         cudaFree(tmp_rl);
     }
@@ -141,7 +152,8 @@ struct BmCensusHandle : ct_handle {
     ct_census_match_params par{};
     uint64_t* desc = nullptr;      // [2][H][pitch] census descriptors of left, right
     size_t desc_pitch = 0;         // elements
-    uint32_t* keys = nullptr;      // W*H merge keys (0xFFFFFFFF between calls)
+    uint32_t* keys = nullptr;      // ceil(D/64) planes of W*H merge keys
+    uint32_t* counters = nullptr;  // one per (strip, column tile); 0 between calls
     uint16_t* tmp_lr = nullptr;    // U16 maps for process_lr when the caller wants only one
     uint16_t* tmp_rl = nullptr;
     size_t tmp_pitch = 0;
@@ -169,6 +181,8 @@ int census_match_pass_maps(BmCensusHandle* h, int dir, const ct_image* disp, con
     a.W = h->fmt.width; a.H = h->fmt.height; a.D = h->par.disp_count;
     a.th = h->th;
     a.keys = h->keys;
+    a.counters = h->counters;
+    a.merge_last = 1;
     a.out = disp->ptr; a.out_pitch = disp->pitch_bytes; a.out_type = disp->type;
     a.status = h->d_status;
     const cudaError_t e = dir == 0 ? launch_census_match<0>(tb, tm, a, s, h->dpw)
@@ -183,8 +197,8 @@ int census_match_pass(BmCensusHandle* h, int dir, const ct_image* disp, cudaStre
 }
 
 int census_both(BmCensusHandle* h, const ct_image* left, const ct_image* right, cudaStream_t s) {
-    if (int rc = census::launch9x7(left, h->left_desc(), h->desc_pitch, h->d_status, s)) return rc;
-    if (int rc = census::launch9x7(right, h->right_desc(), h->desc_pitch, h->d_status, s)) return rc;
+    if (int rc = census::launch9x7(left, h->left_desc(), h->desc_pitch, h->d_status, s, 1)) return rc;
+    if (int rc = census::launch9x7(right, h->right_desc(), h->desc_pitch, h->d_status, s, 1)) return rc;
     return CT_OK;
 }
 
@@ -235,7 +249,7 @@ int ct_census_process(ct_handle* hh, const ct_image* dst, const ct_image* src, c
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     h->last_stream = s;
     if (h->par.window == CT_CENSUS_9X7) {
-        return census::launch9x7(src, static_cast<uint64_t*>(dst->ptr), dst->pitch_bytes / 8, h->d_status, s);
+        return census::launch9x7(src, static_cast<uint64_t*>(dst->ptr), dst->pitch_bytes / 8, h->d_status, s, 0);
     }
     dim3 blk(32, 8), grid((src->width + 31) / 32, (src->height + 7) / 8);
     census::census3x3_kernel<<<grid, blk, 0, s>>>(static_cast<const uint8_t*>(src->ptr), src->pitch_bytes,
@@ -265,28 +279,29 @@ int ct_bm_census_configure(ct_handle* hh, int32_t device, const ct_format* fmt, 
     if (p->reserved != 0) return fail(CT_EINVAL, "reserved must be 0");
     if (int rc = use_device(device)) return rc;
     // release a previous configuration
-    cudaFree(h->desc); cudaFree(h->keys); cudaFree(h->tmp_lr); cudaFree(h->tmp_rl);
-    h->desc = nullptr; h->keys = nullptr; h->tmp_lr = nullptr; h->tmp_rl = nullptr;
+    cudaFree(h->desc); cudaFree(h->keys); cudaFree(h->counters); cudaFree(h->tmp_lr); cudaFree(h->tmp_rl);
+    h->desc = nullptr; h->keys = nullptr; h->counters = nullptr; h->tmp_lr = nullptr; h->tmp_rl = nullptr;
     h->device = device;
     if (int rc = h->init_status()) return rc;
     const int W = fmt->width, H = fmt->height;
-    h->desc_pitch = ((size_t)W + 31) / 32 * 32;
+    h->desc_pitch = cm::planar_pitch(W);  // pair-planar layout
     if (cudaMalloc(&h->desc, 2 * h->desc_pitch * H * 8) != cudaSuccess) return fail(CT_ENOMEM, "descriptor scratch");
-    if (cudaMalloc(&h->keys, (size_t)W * H * 4) != cudaSuccess) return fail(CT_ENOMEM, "key scratch");
-    CT_CUDA_TRY(cudaMemset(h->keys, 0xFF, (size_t)W * H * 4));
+    const size_t zplanes = (p->disp_count + cm::kDPC - 1) / cm::kDPC;
+    if (cudaMalloc(&h->keys, zplanes * W * H * 4) != cudaSuccess) return fail(CT_ENOMEM, "key scratch");
+    // counters for the shortest strips any launch shape uses (11 rows)
+    const size_t ngroups = size_t((H + 10) / 11) * ((W + cm::kTWO - 1) / cm::kTWO);
+    if (cudaMalloc(&h->counters, ngroups * 4) != cudaSuccess) return fail(CT_ENOMEM, "counter scratch");
+    CT_CUDA_TRY(cudaMemset(h->counters, 0, ngroups * 4));
     h->tmp_pitch = ((size_t)W * 2 + 255) / 256 * 256;
     if (cudaMalloc(&h->tmp_lr, h->tmp_pitch * H) != cudaSuccess) return fail(CT_ENOMEM, "map scratch");
     if (cudaMalloc(&h->tmp_rl, h->tmp_pitch * H) != cudaSuccess) return fail(CT_ENOMEM, "map scratch");
-    const uint64_t pb = h->desc_pitch * 8;
     h->fmt = *fmt;  // left_desc() / right_desc() below depend on the height
     h->th = cm::pick_strip_height(W, H, p->disp_count, sm_count(device));
     CT_CUDA_TRY(cm::prepare_census_match());
     h->par = *p;
     using namespace cm;
-    if (int rc = make_tmap_2d(&h->tm_lb, h->left_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kTWV, kBR)) return rc;
-    if (int rc = make_tmap_2d(&h->tm_rb, h->right_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kTWV, kBR)) return rc;
-    if (int rc = make_tmap_2d(&h->tm_lm, h->left_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kMW, kBR)) return rc;
-    if (int rc = make_tmap_2d(&h->tm_rm, h->right_desc(), CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pb, kMW, kBR)) return rc;
+    if (int rc = make_planar_maps(&h->tm_lb, &h->tm_rm, h->left_desc(), h->right_desc(), W, H)) return rc;
+    if (int rc = make_planar_maps(&h->tm_rb, &h->tm_lm, h->right_desc(), h->left_desc(), W, H)) return rc;
     h->configured = true;
     return CT_OK;
 }
@@ -443,16 +458,19 @@ int ct_bm_census_match_desc(ct_handle* hh, const ct_image* disp, const ct_image*
     if (int rc = check_disp_out(h, disp, "disp")) return rc;
     if (int rc = use_device(h->device)) return rc;
     const int W = h->fmt.width, H = h->fmt.height;
-    CUtensorMap tb, tm;
-    if (int rc = make_tmap_2d(&tb, desc_base->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, desc_base->pitch_bytes,
-                              cm::kTWV, cm::kBR))
-        return rc;
-    if (int rc = make_tmap_2d(&tm, desc_match->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H,
-                              desc_match->pitch_bytes, cm::kMW, cm::kBR))
-        return rc;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     h->last_stream = s;
-    return census_match_pass_maps(h, left_to_right ? 0 : 1, disp, tb, tm, s);
+    // the caller's natural-layout descriptors -> the handle's pair-planar scratch
+    const int dir = left_to_right ? 0 : 1;
+    uint64_t* base_dst = dir == 0 ? h->left_desc() : h->right_desc();
+    uint64_t* match_dst = dir == 0 ? h->right_desc() : h->left_desc();
+    dim3 cb(256), cg((W + 255) / 256, H);
+    to_planar_kernel<<<cg, cb, 0, s>>>(static_cast<const uint64_t*>(desc_base->ptr), desc_base->pitch_bytes / 8,
+                                       base_dst, W, H);
+    to_planar_kernel<<<cg, cb, 0, s>>>(static_cast<const uint64_t*>(desc_match->ptr), desc_match->pitch_bytes / 8,
+                                       match_dst, W, H);
+    CT_LAUNCH_CHECK();
+    return census_match_pass(h, dir, disp, s);
 }
 
 }  // extern "C"

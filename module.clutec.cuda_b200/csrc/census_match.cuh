@@ -53,6 +53,28 @@ constexpr int kRB = 2 * kAR + 1;        // ring depth = vertical window = 5
 constexpr int kBR = 2 * kRB;            // cost rows per TMA batch = 10
 constexpr int kMW = kTWV + kDPC;        // 192 match columns staged per row
 
+// Descriptor scratch layout ("pair-planar"): each row holds the 16-byte pairs
+// of adjacent columns (x & ~1, x | 1), even pairs in plane 0, odd pairs in
+// plane 1: word (x, y) lives at y * pitch + ((x >> 1) & 1) * 2 * NI +
+// (x >> 2) * 2 + (x & 1), NI = ceil(W / 4), pitch = 4 * NI. A lane's 4
+// adjacent columns are then two 16-byte elements at consecutive indices of
+// the two planes, so a warp's 16-byte shared loads are contiguous (no bank
+// conflicts). Staged boxes: [row][plane][kPB or kPM][2] words.
+constexpr int kPB = kTWV / 4 + 1;       // 33 pair indices per plane (base rows)
+constexpr int kPM = kMW / 4 + 1;        // 49 (match rows)
+constexpr int kRowB = 2 * kPB * 2;      // words per staged base row
+constexpr int kRowM = 2 * kPM * 2;      // words per staged match row
+constexpr int kStageB = (kBR * kRowB * 8 + 127) / 128 * 128;  // bytes per stage (128-aligned)
+constexpr int kStageM = (kBR * kRowM * 8 + 127) / 128 * 128;
+constexpr uint32_t kTxB = kBR * kRowB * 8;  // bytes a base box delivers
+constexpr uint32_t kTxM = kBR * kRowM * 8;
+
+__host__ __device__ constexpr int planar_ni(int W) { return (W + 3) / 4; }
+__host__ __device__ constexpr size_t planar_pitch(int W) { return size_t(4) * planar_ni(W); }
+__host__ __device__ constexpr size_t planar_index(int x, int y, int W) {
+    return size_t(y) * planar_pitch(W) + size_t((x >> 1) & 1) * 2 * planar_ni(W) + size_t(x >> 2) * 2 + (x & 1);
+}
+
 // Variant: disparities per warp (8 = 8 warps of 255 registers, one CTA of 8
 // warps per SM; 4 = 16 warps of at most 128 registers, 16 warps per SM).
 template <int DPW>
@@ -64,22 +86,28 @@ struct Var {
     static constexpr int kWarpsPerGroup = 32 / DPW;
 };
 
+// When D spans several CTAs (gridDim.z > 1) their winners are merged either
+// (merge_last = 1) through per-z key planes keys[z][y][x] written with plain
+// stores, merged by whichever CTA of the (strip, column tile) group finishes
+// last (one atomic counter per group, reset by that CTA), or (merge_last = 0)
+// by atomicMin into one key plane that keys_finalize_kernel converts.
 struct MatchArgs {
     int W, H, D;
     int th;             // output rows per CTA (strip height)
-    uint32_t* keys;     // W*H keys merged by atomicMin when gridDim.z > 1
-    void* out;          // direct disparity output when gridDim.z == 1
+    uint32_t* keys;     // key plane(s), see above
+    uint32_t* counters; // merge_last: one counter per (strip, column tile), 0 between calls
+    int merge_last;
+    void* out;          // disparity output
     size_t out_pitch;
     int out_type;       // CT_PIX_U8 / CT_PIX_U16
     int32_t* status;
 };
 
-// Shared memory: 2 stages of base (10 x 128) and match (10 x 192) descriptor
-// rows, 2 buffers x 2 groups x 10 rows x 128 key slots, 2 mbarriers and a
-// flag. 70 KB.
+// Shared memory: 2 stages of base (10 rows x 66 pairs) and match (10 x 98
+// pairs) descriptors, 2 buffers x 2 groups x 10 rows x 128 key slots, 2
+// mbarriers and a flag. 71.3 KB.
 __host__ __device__ constexpr size_t smem_bytes() {
-    return size_t(2) * kBR * kTWV * 8 + size_t(2) * kBR * kMW * 8 + size_t(2) * kGroups * kBR * kTWV * 4 + 2 * 8 +
-           16;
+    return size_t(2) * (kStageB + kStageM) + size_t(2) * kGroups * kBR * kTWV * 4 + 2 * 8 + 16;
 }
 
 // Disparity code for an output pixel from its merged key (C << 16 | d).
@@ -102,7 +130,7 @@ __device__ __forceinline__ void match_body(const CUtensorMap* tmB, const CUtenso
                                            int ms) {
     using VT = Var<DPW>;
     constexpr int NP = VT::kNP, NT = VT::kNT, NWD = VT::kWords;
-    constexpr uint32_t kBytes = kBR * kTWV * 8 + kBR * kMW * 8;
+    constexpr uint32_t kBytes = kTxB + kTxM;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -130,22 +158,34 @@ __device__ __forceinline__ void match_body(const CUtensorMap* tmB, const CUtenso
         const int x = xs + 4 * lane + c;
         lim[c] = min(DIR == 0 ? x - kAR : a.W - 1 - kAR - x, a.D - 1);
     }
-    // first match descriptor this thread reads per row (an even index)
+    // First match column this thread reads per row, as an (even) offset from
+    // ms: its words are the pairs (ms + mstart) / 2 + u, u < NWD / 2.
     const int mstart = DIR == 0 ? 4 * lane + kDPC - DPW - DPW * warp : 4 * lane + DPW * warp;
+    // Word offsets, within a staged row, of this thread's two base pairs and
+    // its NWD / 2 match pairs (pair-planar layout; see kPB).
+    const int P0 = xs >> 1, i0 = P0 >> 1;          // first base pair, first staged pair index
+    const int Q0 = ms >> 1, j0 = Q0 >> 1;          // same for the match rows
+    int boff[2], moff[NWD / 2];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) boff[t] = (((P0 + t) & 1) * kPB + ((P0 + t) >> 1) - i0 + lane) * 2;
+    {
+        const int g0 = Q0 + ((mstart - 4 * lane) >> 1);  // pair of u = 0, minus 2 * lane
+#pragma unroll
+        for (int u = 0; u < NWD / 2; ++u) moff[u] = (((g0 + u) & 1) * kPM + ((g0 + u) >> 1) - j0 + lane) * 2;
+    }
 
     // Adds cost row r of stage s to the running sums (ring slot r mod 5).
     auto accum = [&](int s, int r) {
-        const uint64_t* rowB = sB + (s * kBR + r) * kTWV;
-        const uint64_t* rowM = sM + (s * kBR + r) * kMW;
+        const uint64_t* rowB = sB + s * (kStageB / 8) + r * kRowB;
+        const uint64_t* rowM = sM + s * (kStageM / 8) + r * kRowM;
         uint2 bw[kCPT], mw[NWD];
-        const uint4* pb = reinterpret_cast<const uint4*>(rowB + 4 * lane);
-        const uint4 q0 = pb[0], q1 = pb[1];
+        const uint4 q0 = *reinterpret_cast<const uint4*>(rowB + boff[0]);
+        const uint4 q1 = *reinterpret_cast<const uint4*>(rowB + boff[1]);
         bw[0] = make_uint2(q0.x, q0.y); bw[1] = make_uint2(q0.z, q0.w);
         bw[2] = make_uint2(q1.x, q1.y); bw[3] = make_uint2(q1.z, q1.w);
-        const uint4* pm = reinterpret_cast<const uint4*>(rowM + mstart);
 #pragma unroll
         for (int k = 0; k < NWD / 2; ++k) {
-            const uint4 q = pm[k];
+            const uint4 q = *reinterpret_cast<const uint4*>(rowM + moff[k]);
             mw[2 * k] = make_uint2(q.x, q.y);
             mw[2 * k + 1] = make_uint2(q.z, q.w);
         }
@@ -228,6 +268,8 @@ __device__ __forceinline__ void match_body(const CUtensorMap* tmB, const CUtenso
                 if (gridDim.z == 1) {
                     const bool valid = x >= kAR && x < a.W - kAR && y >= kAR && y < a.H - kAR;
                     store_disp(a.out, a.out_pitch, a.out_type, x, y, valid, best);
+                } else if (a.merge_last) {
+                    a.keys[(size_t)blockIdx.z * a.W * a.H + (size_t)y * a.W + x] = best;
                 } else {
                     atomicMin(&a.keys[(size_t)y * a.W + x], best);
                 }
@@ -260,14 +302,18 @@ __device__ __forceinline__ void match_body(const CUtensorMap* tmB, const CUtenso
             if (tid == 0) {
                 dev::report(a.status, CT_ETIMEOUT);
                 if (b + 1 < nb) dev::mbar_wait_bounded(&bars[s ^ 1], ((b + 1) >> 1) & 1);
+                if (gridDim.z > 1 && a.merge_last) {  // keep the group counter consistent
+                    unsigned* cnt = reinterpret_cast<unsigned*>(&a.counters[blockIdx.y * gridDim.x + blockIdx.x]);
+                    if (atomicAdd(cnt, 1u) == gridDim.z - 1) *cnt = 0u;
+                }
             }
             return;
         }
         if (tid == 0 && b + 2 < nb) {
             dev::fence_proxy_async();
             dev::mbar_arrive_expect_tx(&bars[s], kBytes);
-            dev::tma_load_2d(sB + s * kBR * kTWV, tmB, xs, ye0 + (b + 2) * kBR, &bars[s]);
-            dev::tma_load_2d(sM + s * kBR * kMW, tmM, ms, ye0 + (b + 2) * kBR, &bars[s]);
+            dev::tma_load_4d(sB + s * (kStageB / 8), tmB, 0, i0, 0, ye0 + (b + 2) * kBR, &bars[s]);
+            dev::tma_load_4d(sM + s * (kStageM / 8), tmM, 0, j0, 0, ye0 + (b + 2) * kBR, &bars[s]);
         }
         flush(b & 1, kBR * b - kRB, b == 0 ? kRB : 0, kBR);
     }
@@ -275,6 +321,33 @@ __device__ __forceinline__ void match_body(const CUtensorMap* tmB, const CUtenso
     if (warp_active) emit(nb & 1, 0);
     __syncthreads();
     flush(nb & 1, kBR * nb - kRB, 0, 1);
+
+    if (gridDim.z > 1 && a.merge_last) {
+        // The last CTA of this (strip, column tile) group merges the groups'
+        // key planes. Writers fence before counting; the merger fences after.
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            unsigned* cnt = reinterpret_cast<unsigned*>(&a.counters[blockIdx.y * gridDim.x + blockIdx.x]);
+            const unsigned prev = atomicAdd(cnt, 1u);
+            sflag[1] = prev == gridDim.z - 1;
+            if (sflag[1]) *cnt = 0u;  // ready for the next call
+        }
+        __syncthreads();
+        if (sflag[1]) {
+            __threadfence();
+            const size_t plane = (size_t)a.W * a.H;
+            for (int idx = tid; idx < rows_here * kTWO; idx += NT) {
+                const int oy = idx / kTWO, x = xs + kAR + idx % kTWO, y = y0 + oy;
+                if (x >= a.W) continue;
+                const uint32_t* kp = a.keys + (size_t)y * a.W + x;
+                uint32_t best = 0xFFFFFFFFu;
+                for (unsigned z = 0; z < gridDim.z; ++z) best = min(best, __ldcg(kp + z * plane));
+                const bool valid = x >= kAR && x < a.W - kAR && y >= kAR && y < a.H - kAR;
+                store_disp(a.out, a.out_pitch, a.out_type, x, y, valid, best);
+            }
+        }
+    }
 }
 
 template <int DIR, int DPW>
@@ -282,9 +355,9 @@ __global__ void __launch_bounds__(Var<DPW>::kNT, 1)
     census_match_kernel(const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmM,
                         MatchArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    uint64_t* sB = reinterpret_cast<uint64_t*>(smem_raw);   // [2][kBR][kTWV]
-    uint64_t* sM = sB + 2 * kBR * kTWV;                      // [2][kBR][kMW]
-    uint32_t* sKey = reinterpret_cast<uint32_t*>(sM + 2 * kBR * kMW);  // [2][kGroups][kBR][kTWV]
+    uint64_t* sB = reinterpret_cast<uint64_t*>(smem_raw);                 // [2 stages][kBR][2][kPB][2]
+    uint64_t* sM = reinterpret_cast<uint64_t*>(smem_raw + 2 * kStageB);   // [2 stages][kBR][2][kPM][2]
+    uint32_t* sKey = reinterpret_cast<uint32_t*>(smem_raw + 2 * (kStageB + kStageM));  // [2][kGroups][kBR][kTWV]
     uint64_t* bars = reinterpret_cast<uint64_t*>(sKey + 2 * kGroups * kBR * kTWV);  // [2]
     int* sflag = reinterpret_cast<int*>(bars + 2);
 
@@ -311,9 +384,9 @@ __global__ void __launch_bounds__(Var<DPW>::kNT, 1)
     __syncthreads();
     if (tid == 0) {
         for (int b = 0; b < 2 && b < nb; ++b) {
-            dev::mbar_arrive_expect_tx(&bars[b], kBR * kTWV * 8 + kBR * kMW * 8);
-            dev::tma_load_2d(sB + b * kBR * kTWV, &tmB, xs, ye0 + b * kBR, &bars[b]);
-            dev::tma_load_2d(sM + b * kBR * kMW, &tmM, ms, ye0 + b * kBR, &bars[b]);
+            dev::mbar_arrive_expect_tx(&bars[b], kTxB + kTxM);
+            dev::tma_load_4d(sB + b * (kStageB / 8), &tmB, 0, (xs >> 1) >> 1, 0, ye0 + b * kBR, &bars[b]);
+            dev::tma_load_4d(sM + b * (kStageM / 8), &tmM, 0, (ms >> 1) >> 1, 0, ye0 + b * kBR, &bars[b]);
         }
     }
     if (interior)
@@ -358,7 +431,20 @@ inline int pick_strip_height(int W, int H, int D, int sms) {
     return best;
 }
 
-// Allows the 70 KB of dynamic shared memory on the current device for every
+// 4D TMA maps over pair-planar descriptor buffers (dims: word in pair, pair
+// index, plane, row): `tb` stages base rows (kPB pairs per plane), `tm` match
+// rows (kPM), kBR rows per box.
+inline int make_planar_maps(CUtensorMap* tb, CUtensorMap* tm, const uint64_t* base, const uint64_t* match, int W,
+                            int H) {
+    const uint64_t ni = uint64_t(planar_ni(W));
+    const uint64_t dims[4] = {2, ni, 2, uint64_t(H)};
+    const uint64_t strides[3] = {16, ni * 16, ni * 32};
+    const uint32_t box_b[4] = {2, kPB, 2, kBR}, box_m[4] = {2, kPM, 2, kBR};
+    if (int rc = ct::make_tmap_nd(tb, base, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, 4, dims, strides, box_b)) return rc;
+    return ct::make_tmap_nd(tm, match, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, 4, dims, strides, box_m);
+}
+
+// Allows the 71 KB of dynamic shared memory on the current device for every
 // kernel instantiation. Sets function attributes only (no allocation).
 inline cudaError_t prepare_census_match() {
     const int smem = int(smem_bytes());
@@ -380,7 +466,7 @@ inline cudaError_t launch_census_match(const CUtensorMap& tb, const CUtensorMap&
     if (dpw == 8) census_match_kernel<DIR, 8><<<grid, Var<8>::kNT, smem_bytes(), s>>>(tb, tm, a);
     else census_match_kernel<DIR, 4><<<grid, Var<4>::kNT, smem_bytes(), s>>>(tb, tm, a);
     cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess || grid.z == 1) return e;
+    if (e != cudaSuccess || grid.z == 1 || a.merge_last) return e;
     keys_finalize_kernel<<<dim3((a.W + 255) / 256, a.H), 256, 0, s>>>(a.keys, a.W, a.H, kAR, a.out, a.out_pitch,
                                                                       a.out_type);
     return cudaGetLastError();

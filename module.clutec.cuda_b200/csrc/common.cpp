@@ -108,6 +108,37 @@ int make_tmap_2d(CUtensorMap* map, const void* base, CUtensorMapDataType dtype, 
     return CT_OK;
 }
 
+int make_tmap_nd(CUtensorMap* map, const void* base, CUtensorMapDataType dtype, size_t elem_bytes, int rank,
+                 const uint64_t* dims, const uint64_t* strides_bytes, const uint32_t* box) {
+    std::call_once(g_encode_once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    });
+    if (!g_encode) return fail(CT_ECUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    if (rank < 1 || rank > 5) return fail(CT_EINVAL, "tensor rank %d", rank);
+    if ((reinterpret_cast<uintptr_t>(base) & 15) || ((box[0] * elem_bytes) & 15))
+        return fail(CT_EINVAL, "TMA alignment: base and box row must be multiples of 16 bytes");
+    cuuint64_t d[5], st[4];
+    cuuint32_t b[5], es[5];
+    for (int i = 0; i < rank; ++i) {
+        d[i] = dims[i];
+        b[i] = box[i];
+        es[i] = 1;
+        if (i + 1 < rank) {
+            st[i] = strides_bytes[i];
+            if (st[i] & 15) return fail(CT_EINVAL, "TMA stride %d not a multiple of 16 bytes", i);
+        }
+    }
+    CUresult r = g_encode(map, dtype, cuuint32_t(rank), const_cast<void*>(base), d, st, b, es,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(CT_ECUDA, "cuTensorMapEncodeTiled (rank %d) failed (%d)", rank, (int)r);
+    return CT_OK;
+}
+
 int sm_count(int device) {
     static std::mutex mu;
     static std::vector<int> cache;

@@ -82,6 +82,12 @@ int use_device(int device);
 int make_tmap_2d(CUtensorMap* map, const void* base, CUtensorMapDataType dtype, size_t elem_bytes,
                  uint64_t width, uint64_t height, uint64_t pitch_bytes, uint32_t box_w, uint32_t box_h);
 
+// Rank-N TMA descriptor (N <= 5): dims[0] innermost, strides_bytes[i] = byte
+// stride of dimension i + 1, box[i] elements per dimension. Out-of-bounds
+// elements read as zero.
+int make_tmap_nd(CUtensorMap* map, const void* base, CUtensorMapDataType dtype, size_t elem_bytes, int rank,
+                 const uint64_t* dims, const uint64_t* strides_bytes, const uint32_t* box);
+
 // Device properties cached per device.
 int sm_count(int device);
 

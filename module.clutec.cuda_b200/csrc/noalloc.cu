@@ -11,7 +11,7 @@
 //
 // Limits and rules:
 //  * Images up to kStaticMaxPixels = 2,097,152 pixels counted with the row
-//    rounded up to a multiple of 32 (1920 x 1080 fits); larger images are
+//    rounded up to a multiple of 4 (1920 x 1080 fits); larger images are
 //    rejected with CT_EINVAL. The arrays take 40 MiB + 256 B of device memory
 //    on every GPU that loads this library's module, until the process exits.
 //  * The first call on a device looks up the arrays' device addresses
@@ -32,7 +32,8 @@
 
 namespace ct {
 namespace census {
-int launch9x7(const ct_image* src, uint64_t* dst, size_t dst_pitch_elems, int32_t* status, cudaStream_t s);
+int launch9x7(const ct_image* src, uint64_t* dst, size_t dst_pitch_elems, int32_t* status, cudaStream_t s,
+              int planar);
 }
 
 namespace {
@@ -89,11 +90,11 @@ extern "C" int ct_bm_census_process_static(const ct_image* disp, const ct_image*
     if (W < 8 || H < 8) return fail(CT_EINVAL, "image size %dx%d below 8x8", W, H);
     if (disp_count < 1 || disp_count > 256) return fail(CT_EINVAL, "disp_count must be 1..256");
     if (disp->type == CT_PIX_U8 && disp_count > 255) return fail(CT_ETYPE, "U8 maps need disp_count <= 255");
-    const size_t pitch = ((size_t)W + 31) / 32 * 32;  // descriptor row, elements
+    const size_t pitch = cm::planar_pitch(W);  // descriptor row (pair-planar layout), elements
     if (pitch * (size_t)H > kStaticMaxPixels)
         return fail(CT_EINVAL,
                     "image %dx%d exceeds the static scratch of ct_bm_census_process_static "
-                    "(%zu pixels with rows rounded up to 32; 1920x1080 fits)",
+                    "(%zu pixels with rows rounded up to a multiple of 4; 1920x1080 fits)",
                     W, H, kStaticMaxPixels);
     int device = 0;
     CT_CUDA_TRY(cudaGetDevice(&device));
@@ -106,18 +107,16 @@ extern "C" int ct_bm_census_process_static(const ct_image* disp, const ct_image*
     uint64_t* dl = sc.desc;
     uint64_t* dr = sc.desc + pitch * H;
     CT_CUDA_TRY(cudaMemsetAsync(sc.keys, 0xFF, (size_t)W * H * sizeof(uint32_t), s));
-    if (int rc = census::launch9x7(left, dl, pitch, status, s)) return rc;
-    if (int rc = census::launch9x7(right, dr, pitch, status, s)) return rc;
+    if (int rc = census::launch9x7(left, dl, pitch, status, s, 1)) return rc;
+    if (int rc = census::launch9x7(right, dr, pitch, status, s, 1)) return rc;
     const int dir = left_to_right ? 0 : 1;
     CUtensorMap tb, tm;
-    if (int rc = make_tmap_2d(&tb, dir == 0 ? dl : dr, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pitch * 8, kTWV, kBR))
-        return rc;
-    if (int rc = make_tmap_2d(&tm, dir == 0 ? dr : dl, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, W, H, pitch * 8, kMW, kBR))
-        return rc;
+    if (int rc = make_planar_maps(&tb, &tm, dir == 0 ? dl : dr, dir == 0 ? dr : dl, W, H)) return rc;
     MatchArgs a{};
     a.W = W; a.H = H; a.D = disp_count;
     a.th = pick_strip_height(W, H, disp_count, sm_count(device));
     a.keys = sc.keys;
+    a.merge_last = 0;  // one key plane merged by atomicMin (keeps the static scratch at 40 MiB)
     a.out = disp->ptr; a.out_pitch = disp->pitch_bytes; a.out_type = disp->type;
     a.status = status;
     const cudaError_t e = dir == 0 ? launch_census_match<0>(tb, tm, a, s) : launch_census_match<1>(tb, tm, a, s);
