@@ -286,6 +286,46 @@ int ct_crosscheck_process(ct_handle* h, const ct_image* result, const ct_image* 
  * returns the kept range in disparity units (min > max when none kept). */
 int ct_crosscheck_range(ct_handle* h, int32_t* disp_min, int32_t* disp_max);
 
+/* ---- batched census stereo ------------------------------------------------
+ * Many pairs of mixed size and disparity range per call: 9x7 census of both
+ * images, census matching left-to-right and right-to-left, cross-check with
+ * tolerance tol, for every pair. One batched census launch and one
+ * persistent, work-queue-scheduled matching launch (one CTA per SM) whose
+ * last CTAs per strip run the cross-check. Each pair's result equals
+ * ct_bm_census_process_lr(disp_checked) run on that pair alone. No
+ * counterpart in the reference (its drivers process one image per call).
+ * The handle owns all scratch; pair shapes are fixed at configure. */
+typedef struct ct_batch_shape {
+    int32_t width;
+    int32_t height;
+    int32_t disp_count;   /* 1..256 */
+    int32_t reserved;
+} ct_batch_shape;
+
+typedef struct ct_batch_item {
+    ct_image left;        /* U8 */
+    ct_image right;       /* U8 */
+    ct_image disp;        /* U8 (disp_count <= 255) or U16: the cross-checked left map */
+} ct_batch_item;
+
+int ct_batch_create(ct_handle** out);
+/* Up to 256 pairs; strip heights start from a cost model per (W, H, D). */
+int ct_batch_configure(ct_handle* h, int32_t device, const ct_batch_shape* shapes, int32_t n, int32_t tol);
+/* items[i] must match shapes[i]. Asynchronous on stream, except that it
+ * first waits for this handle's previous call (its pinned staging buffer is
+ * reused). */
+int ct_batch_process(ct_handle* h, const ct_batch_item* items, int32_t n, ct_stream stream);
+/* Autotuner: times the whole batch on these items for candidate strip heights
+ * of each distinct (W, H, D) and keeps the fastest. Synchronises stream. */
+int ct_batch_autotune(ct_handle* h, const ct_batch_item* items, int32_t n, ct_stream stream);
+/* Strip height chosen for pair `pair` (index into the configured shapes). */
+int ct_batch_strip_height(ct_handle* h, int32_t pair, int32_t* strip_height);
+/* Captures one process call on these items into a CUDA graph held by the
+ * handle (the items' buffers must stay valid); ct_batch_graph_launch replays
+ * it on any stream without host work. Re-configure or autotune drops it. */
+int ct_batch_graph_create(ct_handle* h, const ct_batch_item* items, int32_t n);
+int ct_batch_graph_launch(ct_handle* h, ct_stream stream);
+
 /* ---- synthetic stereo pairs -----------------------------------------------
  * Seeded generator of rectified stereo pairs with ground truth (host memory).
  *   kind 1: fractal value noise (4 octaves) left image; disparity = 4

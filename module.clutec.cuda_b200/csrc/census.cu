@@ -1,13 +1,12 @@
 // census.cu — CensusTransform::CDriver and the census block matcher.
 //
-// Census transform (CensusTransform.cu:60-157): the 9x7 / 64-bit transform
-// stages an image tile into shared memory with one 2D TMA load and builds
-// each descriptor bit with a subtract + funnel shift (the sign of
-// centre - neighbour is the "neighbour > centre" bit). The 3x3 / 8-bit
-// reference transform is kept for parity with the reference.
+// Census transform (CensusTransform.cu:60-157): the 9x7 / 64-bit transform is
+// census_tile.cuh; the 3x3 / 8-bit reference transform is kept for parity
+// with the reference.
 #include "ct_internal.h"
 #include "ct_device.cuh"
 #include "census_match.cuh"
+#include "census_tile.cuh"
 
 namespace ct {
 
@@ -16,70 +15,11 @@ namespace ct {
 // ---------------------------------------------------------------------------
 namespace census {
 
-constexpr int kTX = 64;   // tile columns
-constexpr int kTY = 32;   // tile rows
-constexpr int kPY = 8;    // rows per thread
-constexpr int kNT = kTX * (kTY / kPY);  // 256 threads
-constexpr int kBoxW = kTX + 32;         // 16 halo bytes each side (TMA x alignment)
-constexpr int kBoxH = kTY + 6;
-
 __global__ void __launch_bounds__(kNT) census9x7_kernel(const __grid_constant__ CUtensorMap tm_img, int W, int H,
                                                          uint64_t* out, size_t out_pitch_elems,
                                                          int32_t* status, int planar) {
-    __shared__ __align__(128) uint8_t tile[kBoxH * kBoxW];
-    __shared__ __align__(8) uint64_t bar;
-    const int tid = threadIdx.x;
-    const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
-    if (tid == 0) {
-        dev::mbar_init(&bar, 1);
-        dev::fence_barrier_init();
-    }
-    __syncthreads();
-    if (tid == 0) {
-        dev::mbar_arrive_expect_tx(&bar, kBoxW * kBoxH);
-        dev::tma_load_2d(tile, &tm_img, x0 - 16, y0 - 3, &bar);
-    }
-    const bool got = dev::mbar_wait_bounded(&bar, 0);
-    if (__syncthreads_or(!got)) {
-        if (tid == 0) dev::report(status, CT_ETIMEOUT);
-        return;
-    }
-    const int tx = tid % kTX, ty = tid / kTX;
-    const int x = x0 + tx;
-    if (x >= W) return;
-    // sliding 7 x 9 window (values as int), rows advance one per pixel
-    int w[7][9];
-    const uint8_t* base = tile + (ty * kPY) * kBoxW + (16 + tx - 4);
-#pragma unroll
-    for (int r = 0; r < 6; ++r)
-#pragma unroll
-        for (int c = 0; c < 9; ++c) w[r + 1][c] = base[r * kBoxW + c];
-#pragma unroll
-    for (int p = 0; p < kPY; ++p) {
-#pragma unroll
-        for (int r = 0; r < 6; ++r)
-#pragma unroll
-            for (int c = 0; c < 9; ++c) w[r][c] = w[r + 1][c];
-#pragma unroll
-        for (int c = 0; c < 9; ++c) w[6][c] = base[(p + 6) * kBoxW + c];
-        const int y = y0 + ty * kPY + p;
-        if (y >= H) break;
-        const int ctr = w[3][4];
-        uint32_t hi = 0, lo = 0;
-        int k = 0;
-#pragma unroll
-        for (int r = 0; r < 7; ++r)
-#pragma unroll
-            for (int c = 0; c < 9; ++c, ++k) {
-                const uint32_t t = uint32_t(ctr - w[r][c]);  // sign bit = neighbour > centre
-                if (k < 31) hi = __funnelshift_l(t, hi, 1);
-                else lo = __funnelshift_l(t, lo, 1);
-            }
-        const bool inside = x >= 4 && x < W - 4 && y >= 3 && y < H - 3;
-        const uint64_t d = inside ? ((uint64_t(hi) << 32) | lo) : 0ull;
-        // planar: the matcher's pair-planar scratch layout (cm::planar_index)
-        out[planar ? cm::planar_index(x, y, W) : (size_t)y * out_pitch_elems + x] = d;
-    }
+    __shared__ __align__(128) TileSmem sm;
+    census_tile(&tm_img, W, H, blockIdx.x * kTX, blockIdx.y * kTY, out, out_pitch_elems, planar, status, sm);
 }
 
 // 3x3 / 8-bit reference transform (CensusTransform.cu:60-120): bits 7..0 =

@@ -123,11 +123,26 @@ __device__ __forceinline__ void store_disp(void* out, size_t pitch, int type, in
     }
 }
 
+// A CTA's piece of work: column tile bx of nbx, strip by, disparity block bz
+// of nbz. The single-image kernel takes it from blockIdx / gridDim; the
+// batched persistent kernel from its work queue.
+struct Tile {
+    int bx, by, bz, nbx, nbz;
+};
+
+// Result of one tile: whether this CTA wrote final disparities for its
+// (strip, column tile) group (always when nbz == 1; the last arriver
+// otherwise), and whether a tile load timed out.
+struct TileResult {
+    bool group_done;
+    bool aborted;
+};
+
 template <int DIR, bool EDGE, int DPW>
-__device__ __forceinline__ void match_body(const CUtensorMap* tmB, const CUtensorMap* tmM, const MatchArgs& a,
-                                           uint64_t* sB, uint64_t* sM, uint32_t* sKey, uint64_t* bars,
-                                           int* sflag, int nb, int rows_here, int xs, int y0, int ye0, int dz0,
-                                           int ms) {
+__device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const CUtensorMap* tmM,
+                                                 const MatchArgs& a, const Tile& t, uint64_t* sB, uint64_t* sM,
+                                                 uint32_t* sKey, uint64_t* bars, int* sflag, const uint32_t* par,
+                                                 int nb, int rows_here, int xs, int y0, int ye0, int dz0, int ms) {
     using VT = Var<DPW>;
     constexpr int NP = VT::kNP, NT = VT::kNT, NWD = VT::kWords;
     constexpr uint32_t kBytes = kTxB + kTxM;
@@ -265,23 +280,26 @@ __device__ __forceinline__ void match_body(const CUtensorMap* tmB, const CUtenso
             }
             const int oy = oy0 + r, x = xs + v, y = y0 + oy;
             if (oy >= 0 && oy < rows_here && x < a.W) {
-                if (gridDim.z == 1) {
+                if (t.nbz == 1) {
                     const bool valid = x >= kAR && x < a.W - kAR && y >= kAR && y < a.H - kAR;
                     store_disp(a.out, a.out_pitch, a.out_type, x, y, valid, best);
                 } else if (a.merge_last) {
-                    a.keys[(size_t)blockIdx.z * a.W * a.H + (size_t)y * a.W + x] = best;
+                    a.keys[(size_t)t.bz * a.W * a.H + (size_t)y * a.W + x] = best;
                 } else {
                     atomicMin(&a.keys[(size_t)y * a.W + x], best);
                 }
             }
         }
     };
+    unsigned* group_counter = reinterpret_cast<unsigned*>(a.counters ? &a.counters[t.by * t.nbx + t.bx] : nullptr);
 
     // Cost row i = kBR * b + r. Before row i is added, V holds rows i-5..i-1:
     // the window of output row i - 5, whose keys go to buffer b & 1, slot r.
+    // Stage s is used by batches s, s + 2, ...: its (b >> 1)-th use in this
+    // tile completes phase par[s] + (b >> 1) of its mbarrier.
     for (int b = 0; b < nb; ++b) {
         const int s = b & 1;
-        if (!dev::mbar_wait_bounded(&bars[s], (b >> 1) & 1)) *sflag = 1;
+        if (!dev::mbar_wait_bounded(&bars[s], (par[s] + (b >> 1)) & 1)) *sflag = 1;
         if (warp_active) {
             if (b == 0) {
 #pragma unroll
@@ -301,13 +319,12 @@ __device__ __forceinline__ void match_body(const CUtensorMap* tmB, const CUtenso
         if (*sflag) {     // a tile load never arrived: report and leave together
             if (tid == 0) {
                 dev::report(a.status, CT_ETIMEOUT);
-                if (b + 1 < nb) dev::mbar_wait_bounded(&bars[s ^ 1], ((b + 1) >> 1) & 1);
-                if (gridDim.z > 1 && a.merge_last) {  // keep the group counter consistent
-                    unsigned* cnt = reinterpret_cast<unsigned*>(&a.counters[blockIdx.y * gridDim.x + blockIdx.x]);
-                    if (atomicAdd(cnt, 1u) == gridDim.z - 1) *cnt = 0u;
+                if (b + 1 < nb) dev::mbar_wait_bounded(&bars[s ^ 1], (par[s ^ 1] + ((b + 1) >> 1)) & 1);
+                if (t.nbz > 1 && a.merge_last) {  // keep the group counter consistent
+                    if (atomicAdd(group_counter, 1u) == unsigned(t.nbz) - 1) *group_counter = 0u;
                 }
             }
-            return;
+            return TileResult{false, true};
         }
         if (tid == 0 && b + 2 < nb) {
             dev::fence_proxy_async();
@@ -322,50 +339,60 @@ __device__ __forceinline__ void match_body(const CUtensorMap* tmB, const CUtenso
     __syncthreads();
     flush(nb & 1, kBR * nb - kRB, 0, 1);
 
-    if (gridDim.z > 1 && a.merge_last) {
-        // The last CTA of this (strip, column tile) group merges the groups'
-        // key planes. Writers fence before counting; the merger fences after.
-        __syncthreads();
-        if (tid == 0) {
-            __threadfence();
-            unsigned* cnt = reinterpret_cast<unsigned*>(&a.counters[blockIdx.y * gridDim.x + blockIdx.x]);
-            const unsigned prev = atomicAdd(cnt, 1u);
-            sflag[1] = prev == gridDim.z - 1;
-            if (sflag[1]) *cnt = 0u;  // ready for the next call
-        }
-        __syncthreads();
-        if (sflag[1]) {
-            __threadfence();
-            const size_t plane = (size_t)a.W * a.H;
-            for (int idx = tid; idx < rows_here * kTWO; idx += NT) {
-                const int oy = idx / kTWO, x = xs + kAR + idx % kTWO, y = y0 + oy;
-                if (x >= a.W) continue;
-                const uint32_t* kp = a.keys + (size_t)y * a.W + x;
-                uint32_t best = 0xFFFFFFFFu;
-                for (unsigned z = 0; z < gridDim.z; ++z) best = min(best, __ldcg(kp + z * plane));
-                const bool valid = x >= kAR && x < a.W - kAR && y >= kAR && y < a.H - kAR;
-                store_disp(a.out, a.out_pitch, a.out_type, x, y, valid, best);
-            }
+    if (t.nbz == 1) return TileResult{true, false};
+    if (!a.merge_last) return TileResult{false, false};
+    // The last CTA of this (strip, column tile) group merges the groups' key
+    // planes. Writers fence before counting; the merger fences after.
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(group_counter, 1u);
+        sflag[1] = prev == unsigned(t.nbz) - 1;
+        if (sflag[1]) *group_counter = 0u;  // ready for the next call
+    }
+    __syncthreads();
+    const bool last = sflag[1] != 0;
+    if (last) {
+        __threadfence();
+        const size_t plane = (size_t)a.W * a.H;
+        for (int idx = tid; idx < rows_here * kTWO; idx += NT) {
+            const int oy = idx / kTWO, x = xs + kAR + idx % kTWO, y = y0 + oy;
+            if (x >= a.W) continue;
+            const uint32_t* kp = a.keys + (size_t)y * a.W + x;
+            uint32_t best = 0xFFFFFFFFu;
+            for (int z = 0; z < t.nbz; ++z) best = min(best, __ldcg(kp + z * plane));
+            const bool valid = x >= kAR && x < a.W - kAR && y >= kAR && y < a.H - kAR;
+            store_disp(a.out, a.out_pitch, a.out_type, x, y, valid, best);
         }
     }
+    return TileResult{last, false};
 }
 
-template <int DIR, int DPW>
-__global__ void __launch_bounds__(Var<DPW>::kNT, 1)
-    census_match_kernel(const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmM,
-                        MatchArgs a) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    uint64_t* sB = reinterpret_cast<uint64_t*>(smem_raw);                 // [2 stages][kBR][2][kPB][2]
-    uint64_t* sM = reinterpret_cast<uint64_t*>(smem_raw + 2 * kStageB);   // [2 stages][kBR][2][kPM][2]
-    uint32_t* sKey = reinterpret_cast<uint32_t*>(smem_raw + 2 * (kStageB + kStageM));  // [2][kGroups][kBR][kTWV]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sKey + 2 * kGroups * kBR * kTWV);  // [2]
-    int* sflag = reinterpret_cast<int*>(bars + 2);
+// Shared-memory carve-up common to the single-image and the batched kernels.
+struct Smem {
+    uint64_t* sB;     // [2 stages][kBR][2][kPB][2]
+    uint64_t* sM;     // [2 stages][kBR][2][kPM][2]
+    uint32_t* sKey;   // [2][kGroups][kBR][kTWV]
+    uint64_t* bars;   // [2]
+    int* sflag;       // [4]
+    __device__ explicit Smem(unsigned char* raw)
+        : sB(reinterpret_cast<uint64_t*>(raw)),
+          sM(reinterpret_cast<uint64_t*>(raw + 2 * kStageB)),
+          sKey(reinterpret_cast<uint32_t*>(raw + 2 * (kStageB + kStageM))),
+          bars(reinterpret_cast<uint64_t*>(raw + 2 * (kStageB + kStageM) + size_t(2) * kGroups * kBR * kTWV * 4)),
+          sflag(reinterpret_cast<int*>(bars + 2)) {}
+};
 
+// Runs one tile. The mbarriers must be initialised; par[s] counts the phases
+// stage s has completed so far in this CTA and is advanced here.
+template <int DIR, int DPW>
+__device__ TileResult run_tile(const CUtensorMap* tmB, const CUtensorMap* tmM, const MatchArgs& a, const Tile& t,
+                               const Smem& sm, uint32_t* par) {
     const int tid = threadIdx.x;
-    const int xs = blockIdx.x * kTWO - kAR;       // first V column
-    const int y0 = blockIdx.y * a.th;             // first output row
+    const int xs = t.bx * kTWO - kAR;             // first V column
+    const int y0 = t.by * a.th;                   // first output row
     const int ye0 = y0 - kAR;                     // first cost row
-    const int dz0 = blockIdx.z * kDPC;
+    const int dz0 = t.bz * kDPC;
     const int ms = DIR == 0 ? xs - dz0 - kDPC : xs + dz0;  // first staged match column
     const int rows_here = min(a.th, a.H - y0);
     const int nb = (rows_here + 2 * kAR + kBR - 1) / kBR;   // batches of 10 cost rows
@@ -373,26 +400,50 @@ __global__ void __launch_bounds__(Var<DPW>::kNT, 1)
                           (DIR == 0 ? (xs >= dz0 + kDPC - 1) : (xs + dz0 + kDPC - 1 + kTWV <= a.W));
 
     if (tid == 0) {
-        dev::prefetch_tmap(&tmB);
-        dev::prefetch_tmap(&tmM);
-        dev::mbar_init(&bars[0], 1);
-        dev::mbar_init(&bars[1], 1);
-        dev::fence_barrier_init();
-        *sflag = 0;
+        dev::prefetch_tmap(tmB);
+        dev::prefetch_tmap(tmM);
+        sm.sflag[0] = 0;
     }
-    for (int i = tid; i < 2 * kGroups * kBR * kTWV; i += Var<DPW>::kNT) sKey[i] = 0xFFFFFFFFu;
+    for (int i = tid; i < 2 * kGroups * kBR * kTWV; i += Var<DPW>::kNT) sm.sKey[i] = 0xFFFFFFFFu;
     __syncthreads();
     if (tid == 0) {
         for (int b = 0; b < 2 && b < nb; ++b) {
-            dev::mbar_arrive_expect_tx(&bars[b], kTxB + kTxM);
-            dev::tma_load_4d(sB + b * (kStageB / 8), &tmB, 0, (xs >> 1) >> 1, 0, ye0 + b * kBR, &bars[b]);
-            dev::tma_load_4d(sM + b * (kStageM / 8), &tmM, 0, (ms >> 1) >> 1, 0, ye0 + b * kBR, &bars[b]);
+            dev::fence_proxy_async();
+            dev::mbar_arrive_expect_tx(&sm.bars[b], kTxB + kTxM);
+            dev::tma_load_4d(sm.sB + b * (kStageB / 8), tmB, 0, (xs >> 1) >> 1, 0, ye0 + b * kBR, &sm.bars[b]);
+            dev::tma_load_4d(sm.sM + b * (kStageM / 8), tmM, 0, (ms >> 1) >> 1, 0, ye0 + b * kBR, &sm.bars[b]);
         }
     }
-    if (interior)
-        match_body<DIR, false, DPW>(&tmB, &tmM, a, sB, sM, sKey, bars, sflag, nb, rows_here, xs, y0, ye0, dz0, ms);
-    else
-        match_body<DIR, true, DPW>(&tmB, &tmM, a, sB, sM, sKey, bars, sflag, nb, rows_here, xs, y0, ye0, dz0, ms);
+    const TileResult res =
+        interior ? match_body<DIR, false, DPW>(tmB, tmM, a, t, sm.sB, sm.sM, sm.sKey, sm.bars, sm.sflag, par, nb,
+                                               rows_here, xs, y0, ye0, dz0, ms)
+                 : match_body<DIR, true, DPW>(tmB, tmM, a, t, sm.sB, sm.sM, sm.sKey, sm.bars, sm.sflag, par, nb,
+                                              rows_here, xs, y0, ye0, dz0, ms);
+    par[0] += (nb + 1) / 2;
+    par[1] += nb / 2;
+    __syncthreads();  // the next tile reuses the shared memory
+    return res;
+}
+
+__device__ __forceinline__ void init_barriers(const Smem& sm) {
+    if (threadIdx.x == 0) {
+        dev::mbar_init(&sm.bars[0], 1);
+        dev::mbar_init(&sm.bars[1], 1);
+        dev::fence_barrier_init();
+    }
+    __syncthreads();
+}
+
+template <int DIR, int DPW>
+__global__ void __launch_bounds__(Var<DPW>::kNT, 1)
+    census_match_kernel(const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmM,
+                        MatchArgs a) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const Smem sm(smem_raw);
+    init_barriers(sm);
+    uint32_t par[2] = {0, 0};
+    const Tile t{int(blockIdx.x), int(blockIdx.y), int(blockIdx.z), int(gridDim.x), int(gridDim.z)};
+    run_tile<DIR, DPW>(&tmB, &tmM, a, t, sm, par);
 }
 
 // Converts merged keys to disparities and resets the keys for the next call.

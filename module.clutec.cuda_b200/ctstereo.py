@@ -80,6 +80,14 @@ class ct_crosscheck_params(C.Structure):
                 ("reserved1", C.c_int32)]
 
 
+class ct_batch_shape(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("disp_count", C.c_int32), ("reserved", C.c_int32)]
+
+
+class ct_batch_item(C.Structure):
+    _fields_ = [("left", ct_image), ("right", ct_image), ("disp", ct_image)]
+
+
 class ct_pipe_rates(C.Structure):
     _fields_ = [("popc_per_clk_sm", C.c_double), ("iadd3_per_clk_sm", C.c_double),
                 ("lop3_per_clk_sm", C.c_double), ("vimnmx_per_clk_sm", C.c_double),
@@ -136,6 +144,13 @@ def _declare(L: C.CDLL) -> None:
         "ct_crosscheck_configure": [H, C.c_int32, fmt, P(ct_crosscheck_params)],
         "ct_crosscheck_process": [H, img, img, img, C.c_void_p],
         "ct_crosscheck_range": [H, P(C.c_int32), P(C.c_int32)],
+        "ct_batch_create": [P(H)],
+        "ct_batch_configure": [H, C.c_int32, P(ct_batch_shape), C.c_int32, C.c_int32],
+        "ct_batch_process": [H, P(ct_batch_item), C.c_int32, C.c_void_p],
+        "ct_batch_autotune": [H, P(ct_batch_item), C.c_int32, C.c_void_p],
+        "ct_batch_strip_height": [H, C.c_int32, P(C.c_int32)],
+        "ct_batch_graph_create": [H, P(ct_batch_item), C.c_int32],
+        "ct_batch_graph_launch": [H, C.c_void_p],
         "ct_synth_pair": [C.c_int32, C.c_uint64, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
                           C.c_void_p, C.c_void_p],
         "ct_probe_pipe_rates": [C.c_int32, P(ct_pipe_rates)],
@@ -338,6 +353,47 @@ class CrossCheckDisparityMaps(_Driver):
         lo, hi = C.c_int32(), C.c_int32()
         check(lib().ct_crosscheck_range(self._h, C.byref(lo), C.byref(hi)))
         return lo.value, hi.value
+
+
+class BatchStereo(_Driver):
+    """Batched census stereo (both directions + cross-check) over many pairs:
+    one census launch and one persistent matching launch per call."""
+    _create = "ct_batch_create"
+
+    def configure(self, device: int, shapes, tol: int = 1):
+        """shapes: list of (width, height, disp_count)."""
+        arr = (ct_batch_shape * len(shapes))(*[ct_batch_shape(w, h, d, 0) for w, h, d in shapes])
+        check(lib().ct_batch_configure(self._h, device, arr, len(shapes), tol))
+        self.n = len(shapes)
+
+    @staticmethod
+    def _items(pairs):
+        """pairs: list of (left, right, disp) tensors."""
+        return (ct_batch_item * len(pairs))(*[ct_batch_item(image(l), image(r), image(d)) for l, r, d in pairs])
+
+    def process(self, pairs, stream=None):
+        items = self._items(pairs)
+        check(lib().ct_batch_process(self._h, items, len(pairs), _stream(stream)))
+
+    def autotune(self, pairs, stream=None):
+        items = self._items(pairs)
+        check(lib().ct_batch_autotune(self._h, items, len(pairs), _stream(stream)))
+        return self.strip_heights()
+
+    def strip_heights(self):
+        out = []
+        for i in range(self.n):
+            v = C.c_int32()
+            check(lib().ct_batch_strip_height(self._h, i, C.byref(v)))
+            out.append(v.value)
+        return out
+
+    def graph_create(self, pairs):
+        self._graph_items = self._items(pairs)  # keep the descriptors alive
+        check(lib().ct_batch_graph_create(self._h, self._graph_items, len(pairs)))
+
+    def graph_launch(self, stream=None):
+        check(lib().ct_batch_graph_launch(self._h, _stream(stream)))
 
 
 def census_match_static(disp, left, right, disp_count: int, left_to_right: bool = True, device_status=None,
