@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="census1080",
+                    choices=["census1080", "sad640", "ncc1080", "aw1440", "batch64"],
+                    help="census1080 (default, the headline) or another configuration, one JSON line each")
     ap.add_argument("--profile", default=None, choices=["census_match"],
                     help="run the named kernel twice on the 1080p D=128 pair and exit (for ncu captures)")
     return ap.parse_args()
@@ -376,12 +379,163 @@ def run_profile(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Other configurations (--workload): one JSON line each, same timing rules
+# ---------------------------------------------------------------------------
+
+BATCH_SIZES = [(320, 240), (640, 480), (1280, 720), (1920, 1080)]
+BATCH_DISPS = [32, 64, 128, 256]
+
+
+def batch_shapes(n=64, seed=4):
+    """64 pairs: sizes and D drawn uniformly (seeded) from the two lists."""
+    import numpy as np
+    r = np.random.default_rng(seed)
+    return [(*BATCH_SIZES[int(r.integers(4))], BATCH_DISPS[int(r.integers(4))]) for _ in range(n)]
+
+
+def run_workload(args):
+    import numpy as np
+    import torch
+    import ctstereo as ct
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle  # CPU baseline leg only
+
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    stream = torch.cuda.current_stream(dev)
+    flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    wl = args.workload
+
+    def up(a):
+        t = ct.alloc_image(a.shape[0], a.shape[1], torch.from_numpy(a).dtype, dev)
+        t.copy_(torch.from_numpy(a))
+        return t
+
+    if wl == "batch64":
+        shapes = batch_shapes()
+        pairs, host = [], []
+        for i, (W, H, D) in enumerate(shapes):
+            L, R, _, _ = ct.synth_pair(1, 1000 + 97 * rank + i, W, H, D - 1)
+            pairs.append((up(L), up(R), ct.alloc_image(H, W, torch.int16, dev)))
+            host.append((L, R, D))
+        b = ct.BatchStereo()
+        b.configure(local, shapes, tol=1)
+        ths = b.autotune(pairs, stream=stream)
+        b.graph_create(pairs)
+        step = lambda: b.graph_launch(stream=stream)
+        units = sum(2 * W * H * D for W, H, D in shapes)
+        metric = "Mpix*disp/s batched census + L-R check, 64 mixed pairs, one graph"
+        cfg = {"workload": "batch64_census_lrcheck_mixed", "pairs": 64, "sizes": BATCH_SIZES, "disps": BATCH_DISPS,
+               "strip_heights": sorted(set(ths))}
+        check_fn = lambda: all(np.array_equal(  # each pair vs the oracle, first 4 pairs
+            pairs[i][2].cpu().numpy().view(np.uint16),
+            oracle.to_u16(oracle.crosscheck(oracle.match_census(host[i][0], host[i][1], host[i][2])[0],
+                                            oracle.match_census(host[i][0], host[i][1], host[i][2], 2, False)[0],
+                                            1, True)[0])) for i in range(4))
+
+        def cpu_sample():
+            L, R, D = host[0]
+            t0 = time.perf_counter()
+            dl, _ = oracle.match_census(L, R, D, 2, True)
+            dr, _ = oracle.match_census(L, R, D, 2, False)
+            oracle.crosscheck(dl, dr, 1, True)
+            return 2 * L.shape[0] * L.shape[1] * D / (time.perf_counter() - t0) / 1e6, f"pair 0 alone ({L.shape[1]}x{L.shape[0]}, D={D})"
+        launches = 2
+    else:
+        W, H, D, kind = {"sad640": (640, 480, 64, 1), "ncc1080": (1920, 1080, 128, 2),
+                         "aw1440": (2560, 1440, 256, 3)}[wl]
+        L, R, G, O = ct.synth_pair(kind, SEED + rank, W, H, D - 1)
+        dL, dR = up(L), up(R)
+        if wl == "sad640":
+            m = ct.BlockMatcherSAD1()
+            m.configure(local, W, H, D, radius=4)
+            out = ct.alloc_image(H, W, torch.uint8, dev)
+            step = lambda: m.process(out, dL, dR, stream=stream)
+            check_fn = lambda: np.array_equal(out.cpu().numpy(), oracle.to_u8(oracle.match_sad(L, R, D, 4)[0]))
+            cpu_fn = lambda: oracle.match_sad(L, R, D, 4)
+            metric, launches = "Mpix*disp/s SAD 9x9 WTA, 640x480 D=64", 1
+        elif wl == "ncc1080":
+            m = ct.BlockMatcherNCC()
+            m.configure(local, W, H, D, radius=5)
+            out = ct.alloc_image(H, W, torch.uint8, dev)
+            score = ct.alloc_image(H, W, torch.float32, dev)
+            step = lambda: m.process(out, dL, dR, score=score, stream=stream)
+            check_fn = lambda: np.array_equal(out.cpu().numpy(), oracle.to_u8(oracle.match_ncc(L, R, D, 5)[0]))
+            cpu_fn = lambda: oracle.match_ncc(L, R, D, 5)
+            metric, launches = "Mpix*disp/s NCC 11x11 FP32, 1920x1080 D=128", 4
+        else:
+            m = ct.BlockMatcherAW()
+            m.configure(local, W, H, D)
+            out = ct.alloc_image(H, W, torch.float32, dev)
+            step = lambda: m.process(out, dL, dR, stream=stream)
+            check_fn = lambda: np.array_equal(out.cpu().numpy(), oracle.match_aw(L, R, D)[2])
+            cpu_fn = lambda: oracle.match_aw(L, R, D)
+            metric, launches = "Mpix*disp/s adaptive window (5 x 7x7) + sub-pixel, 2560x1440 D=256", 2
+        units = W * H * D
+        cfg = {"workload": f"{wl}", "width": W, "height": H, "D": D}
+
+        def cpu_sample():
+            t0 = time.perf_counter()
+            cpu_fn()
+            return units / (time.perf_counter() - t0) / 1e6, f"one full frame {W}x{H} D={D}"
+
+    for _ in range(max(3, args.warmup)):
+        flush_buf.zero_()
+        step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        for k in range(args.steps):
+            flush_buf.zero_()
+            ev[k][0].record(stream)
+            step()
+            ev[k][1].record(stream)
+        torch.cuda.synchronize(dev)
+    clocks = clk.summary()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * units / (ms * 1e-3) / 1e6
+    out_line = {
+        "metric": metric, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8 pixels / integer costs" + (" / fp32 score" if wl == "ncc1080" else ""),
+        "data": "synthetic (seeded generator)", "config": dict(cfg, l2="flushed before every timed step"),
+        "gpu_launches": launches * args.steps, "clocks": clocks,
+    }
+    if rank == 0:
+        out_line["parity_rank0"] = bool(check_fn())
+        v, sample = cpu_sample()
+        out_line["cpu_baseline"] = {"value": round(v, 1), "unit": UNIT, "cores": oracle.num_threads(),
+                                    "kind": "port", "sample": sample}
+        print(json.dumps(out_line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.profile:
         return run_profile(args)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "census1080":
+        return run_workload(args)
     return run_ours(args)
 
 

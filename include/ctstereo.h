@@ -53,6 +53,7 @@ typedef struct CUstream_st* ct_stream;
 #define CT_ETIMEOUT 5 /* a bounded device-side wait gave up (status read back later) */
 #define CT_ESTATE 6   /* handle of the wrong kind, or process before configure */
 #define CT_ENOMEM 7   /* device allocation failed */
+#define CT_EINTERNAL 8 /* a device-side consistency check failed (status read back later) */
 
 /* ---- pixel types (TPixel_Lum_UInt8 etc.) -------------------------------- */
 #define CT_PIX_U8 1

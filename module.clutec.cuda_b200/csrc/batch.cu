@@ -80,6 +80,10 @@ __global__ void __launch_bounds__(census::kNT) census_batch_kernel(const PairDev
     const PairDev& P = pairs[p];
     const int local = item - P.census_item0;
     const int per_img = P.census_tx * P.census_ty;
+    if (local < 0 || local >= 2 * per_img) {  // table inconsistent with the grid
+        if (threadIdx.x == 0) dev::report(status, CT_EINTERNAL);
+        return;
+    }
     const int img = local / per_img, t = local % per_img;
     const CUtensorMap* tm = &maps[p].img[img];
     if (threadIdx.x == 0) tmap_acquire(tm);
@@ -136,6 +140,10 @@ __global__ void __launch_bounds__(cm::Var<4>::kNT, 1)
         const PairDev& P = pairs[p];
         int local = item - P.match_item0;
         const int per_dir = P.strips * P.tiles_x * P.zc;
+        if (local < 0 || local >= P.match_items || P.match_items != 2 * per_dir) {  // table inconsistent
+            if (tid == 0) dev::report(status, CT_EINTERNAL);
+            break;
+        }
         const int dir = local / per_dir;
         local %= per_dir;
         // disparity blocks of one group are consecutive items, so the group's
@@ -179,16 +187,54 @@ __global__ void __launch_bounds__(cm::Var<4>::kNT, 1)
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
+// Pinned host staging of one call's pair table and image tensor maps. The
+// host rewrites a slot only after the copies that read it have run (event
+// `copied`, recorded behind them): cuTensorMapEncodeTiled does not write a
+// descriptor in one store, so a copy racing a rewrite could deliver a torn
+// tensor map even when the new bytes equal the old ones.
+struct Staging {
+    PairDev* pairs = nullptr;
+    CallMaps* maps = nullptr;
+    cudaEvent_t copied = nullptr;
+    bool pending = false;  // `copied` recorded and not yet waited for
+    int wait() {
+        if (pending) CT_CUDA_TRY(cudaEventSynchronize(copied));
+        pending = false;
+        return CT_OK;
+    }
+    int alloc(int n) {
+        if (!copied) CT_CUDA_TRY(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
+        release_host();
+        CT_CUDA_TRY(cudaMallocHost(&pairs, sizeof(PairDev) * n));
+        CT_CUDA_TRY(cudaMallocHost(&maps, sizeof(CallMaps) * n));
+        return CT_OK;
+    }
+    void release_host() {
+        wait();
+        cudaFreeHost(pairs);
+        cudaFreeHost(maps);
+        pairs = nullptr;
+        maps = nullptr;
+    }
+    void release() {
+        release_host();
+        if (copied) cudaEventDestroy(copied);
+        copied = nullptr;
+    }
+};
+
+// Staging slots used in turn by process calls, so the host fills call k + 1
+// while the copies of call k are still queued behind earlier work.
+constexpr int kSlots = 3;
+
 struct BatchHandle : ct_handle {
     BatchHandle() : ct_handle(Kind::Batch) {}
     ~BatchHandle() override {
         if (device >= 0) cudaSetDevice(device);
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        for (Staging& st : stage) st.release();
+        graph_stage.release();
         cudaFree(arena);
-        cudaFreeHost(host_pairs);
-        cudaFreeHost(host_maps);
-        cudaFreeHost(graph_pairs);
-        cudaFreeHost(graph_maps);
     }
     int n = 0;
     int tol = 1;
@@ -201,10 +247,10 @@ struct BatchHandle : ct_handle {
     CallMaps* d_maps = nullptr;
     CUtensorMap* d_match_maps = nullptr;
     unsigned* d_queue = nullptr;
-    PairDev* host_pairs = nullptr;       // pinned staging
-    CallMaps* host_maps = nullptr;
-    PairDev* graph_pairs = nullptr;      // pinned snapshot used by the graph
-    CallMaps* graph_maps = nullptr;
+    Staging stage[kSlots];               // process calls
+    int next_slot = 0;
+    Staging graph_stage;                 // snapshot read by every graph launch; `copied`
+                                         // is recorded behind each launch
     cudaGraphExec_t graph_exec = nullptr;
     int sms = 148;
 };
@@ -237,9 +283,16 @@ int fill_call(BatchHandle* h, const ct_batch_item* items, int n, PairDev* pd, Ca
     return CT_OK;
 }
 
-int enqueue(BatchHandle* h, const PairDev* pd, const CallMaps* cmaps, cudaStream_t s) {
-    CT_CUDA_TRY(cudaMemcpyAsync(h->d_pairs, pd, sizeof(PairDev) * h->n, cudaMemcpyHostToDevice, s));
-    CT_CUDA_TRY(cudaMemcpyAsync(h->d_maps, cmaps, sizeof(CallMaps) * h->n, cudaMemcpyHostToDevice, s));
+// Enqueues one call: table copies from `st` (its event recorded behind them
+// unless `record` is false, as inside a stream capture), queue reset, census
+// launch, matching launch.
+int enqueue(BatchHandle* h, Staging& st, bool record, cudaStream_t s) {
+    CT_CUDA_TRY(cudaMemcpyAsync(h->d_pairs, st.pairs, sizeof(PairDev) * h->n, cudaMemcpyHostToDevice, s));
+    CT_CUDA_TRY(cudaMemcpyAsync(h->d_maps, st.maps, sizeof(CallMaps) * h->n, cudaMemcpyHostToDevice, s));
+    if (record) {
+        CT_CUDA_TRY(cudaEventRecord(st.copied, s));
+        st.pending = true;
+    }
     CT_CUDA_TRY(cudaMemsetAsync(h->d_queue, 0, sizeof(unsigned), s));
     census_batch_kernel<<<h->total_census, census::kNT, 0, s>>>(h->d_pairs, h->n, h->d_maps, h->d_status);
     CT_LAUNCH_CHECK();
@@ -375,12 +428,8 @@ int ct_batch_configure(ct_handle* hh, int32_t device, const ct_batch_shape* shap
     for (int i = 0; i < n; ++i)
         th[i] = cm::pick_strip_height(shapes[i].width, shapes[i].height, shapes[i].disp_count, h->sms);
     if (int rc = layout(h, th)) return rc;
-    cudaFreeHost(h->host_pairs);
-    cudaFreeHost(h->host_maps);
-    h->host_pairs = nullptr;
-    h->host_maps = nullptr;
-    CT_CUDA_TRY(cudaMallocHost(&h->host_pairs, sizeof(PairDev) * n));
-    CT_CUDA_TRY(cudaMallocHost(&h->host_maps, sizeof(CallMaps) * n));
+    for (Staging& st : h->stage)
+        if (int rc = st.alloc(n)) return rc;
     h->configured = true;
     return CT_OK;
 }
@@ -393,11 +442,12 @@ int ct_batch_process(ct_handle* hh, const ct_batch_item* items, int32_t n, ct_st
     if (!items) return fail(CT_EINVAL, "null items");
     if (int rc = use_device(h->device)) return rc;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    // the staging buffers may still feed a copy of the previous call
-    if (h->last_stream) CT_CUDA_TRY(cudaStreamSynchronize(h->last_stream));
     h->last_stream = s;
-    if (int rc = fill_call(h, items, n, h->host_pairs, h->host_maps)) return rc;
-    return enqueue(h, h->host_pairs, h->host_maps, s);
+    Staging& st = h->stage[h->next_slot];
+    if (int rc = st.wait()) return rc;  // the slot may still feed a copy of an earlier call
+    if (int rc = fill_call(h, items, n, st.pairs, st.maps)) return rc;
+    h->next_slot = (h->next_slot + 1) % kSlots;
+    return enqueue(h, st, true, s);
 }
 
 int ct_batch_autotune(ct_handle* hh, const ct_batch_item* items, int32_t n, ct_stream stream) {
@@ -425,7 +475,8 @@ int ct_batch_autotune(ct_handle* hh, const ct_batch_item* items, int32_t n, ct_s
             cudaEventRecord(e0, s);
             if (int rc = ct_batch_process(hh, items, n, stream)) return rc;
             cudaEventRecord(e1, s);
-            if (cudaEventSynchronize(e1) != cudaSuccess) return fail(CT_ECUDA, "autotune timing failed");
+            const cudaError_t e = cudaEventSynchronize(e1);
+            if (e != cudaSuccess) return fail(CT_ECUDA, "autotune timing failed: %s", cudaGetErrorString(e));
             float ms = 0.f;
             cudaEventElapsedTime(&ms, e0, e1);
             best = std::min(best, ms);
@@ -477,11 +528,11 @@ int ct_batch_graph_create(ct_handle* hh, const ct_batch_item* items, int32_t n) 
         cudaGraphExecDestroy(h->graph_exec);
         h->graph_exec = nullptr;
     }
-    if (!h->graph_pairs) {
-        CT_CUDA_TRY(cudaMallocHost(&h->graph_pairs, sizeof(PairDev) * kMaxPairs));
-        CT_CUDA_TRY(cudaMallocHost(&h->graph_maps, sizeof(CallMaps) * kMaxPairs));
+    if (!h->graph_stage.pairs) {
+        if (int rc = h->graph_stage.alloc(kMaxPairs)) return rc;
     }
-    if (int rc = fill_call(h, items, n, h->graph_pairs, h->graph_maps)) return rc;
+    if (int rc = h->graph_stage.wait()) return rc;  // earlier launches read the snapshot
+    if (int rc = fill_call(h, items, n, h->graph_stage.pairs, h->graph_stage.maps)) return rc;
     cudaStream_t cs;
     CT_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     cudaGraph_t g = nullptr;
@@ -489,7 +540,7 @@ int ct_batch_graph_create(ct_handle* hh, const ct_batch_item* items, int32_t n) 
     if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         rc = fail(CT_ECUDA, "stream capture failed to begin");
     } else {
-        rc = enqueue(h, h->graph_pairs, h->graph_maps, cs);
+        rc = enqueue(h, h->graph_stage, false, cs);
         const cudaError_t e = cudaStreamEndCapture(cs, &g);
         if (!rc && e != cudaSuccess) rc = fail(CT_ECUDA, "stream capture failed: %s", cudaGetErrorString(e));
     }
@@ -507,6 +558,8 @@ int ct_batch_graph_launch(ct_handle* hh, ct_stream stream) {
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     h->last_stream = s;
     CT_CUDA_TRY(cudaGraphLaunch(h->graph_exec, s));
+    CT_CUDA_TRY(cudaEventRecord(h->graph_stage.copied, s));
+    h->graph_stage.pending = true;
     return CT_OK;
 }
 

@@ -345,7 +345,8 @@ int ct_bm_census_autotune(ct_handle* hh, const ct_image* left, const ct_image* r
                 cudaEventRecord(e0, s);
                 rc = census_match_pass(h, dir, &out, s);
                 cudaEventRecord(e1, s);
-                if (cudaEventSynchronize(e1) != cudaSuccess) { rc = fail(CT_ECUDA, "autotune timing failed"); break; }
+                const cudaError_t e = cudaEventSynchronize(e1);
+                if (e != cudaSuccess) { rc = fail(CT_ECUDA, "autotune timing failed: %s", cudaGetErrorString(e)); break; }
                 float ms = 0.f;
                 cudaEventElapsedTime(&ms, e0, e1);
                 t = ms < t ? ms : t;

@@ -22,7 +22,7 @@ _PKG = Path(__file__).resolve().parent
 LIB_PATH = _PKG / "libctstereo.so"
 
 # status codes (ctstereo.h)
-CT_OK, CT_EINVAL, CT_ETYPE, CT_EFORMAT, CT_ECUDA, CT_ETIMEOUT, CT_ESTATE, CT_ENOMEM = range(8)
+CT_OK, CT_EINVAL, CT_ETYPE, CT_EFORMAT, CT_ECUDA, CT_ETIMEOUT, CT_ESTATE, CT_ENOMEM, CT_EINTERNAL = range(9)
 # pixel types
 CT_PIX_U8, CT_PIX_U16, CT_PIX_U64, CT_PIX_F32 = 1, 2, 3, 4
 # EDisparityId codes
@@ -31,7 +31,7 @@ DISP_CANNOT_EVALUATE, DISP_INCONSISTENT, DISP_U8_INVALID = 0xFFFF, 0xFFFA, 0xFF
 CENSUS_9X7, CENSUS_3X3 = 0, 1
 
 _STATUS_NAMES = {0: "CT_OK", 1: "CT_EINVAL", 2: "CT_ETYPE", 3: "CT_EFORMAT", 4: "CT_ECUDA",
-                 5: "CT_ETIMEOUT", 6: "CT_ESTATE", 7: "CT_ENOMEM"}
+                 5: "CT_ETIMEOUT", 6: "CT_ESTATE", 7: "CT_ENOMEM", 8: "CT_EINTERNAL"}
 
 
 class CtError(RuntimeError):

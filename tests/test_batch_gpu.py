@@ -74,3 +74,22 @@ def test_batch_rejects_mismatched_items(ct, cuda):
     with pytest.raises(ct.CtError) as e:
         b.process(pairs)
     assert e.value.code == ct.CT_EFORMAT
+
+
+def test_batch_back_to_back_default_stream(ct, cuda):
+    """Calls queued back to back on the legacy default stream (handle 0) with
+    no host synchronisation: each call's staged pair table and tensor maps
+    must reach the device intact while the host fills the next call."""
+    shapes = [(96 + 32 * (i % 5), 48 + 16 * (i % 3), 16 * (1 + i % 4)) for i in range(48)]
+    b = ct.BatchStereo()
+    b.configure(0, shapes, tol=1)
+    pairs, host = make_batch(ct, cuda, shapes)
+    want = [alone(ct, cuda, L, R, D, torch.int16) for (W, H, D), (L, R) in zip(shapes, host)]
+    default = torch.cuda.default_stream(cuda)
+    assert default.cuda_stream == 0
+    for _ in range(6):
+        b.process(pairs, stream=default)
+    torch.cuda.synchronize()
+    assert b.device_status() == 0
+    for (W, H, D), (l, r, out), w in zip(shapes, pairs, want):
+        np.testing.assert_array_equal(out.cpu().numpy(), w, err_msg=f"{W}x{H} D={D}")
