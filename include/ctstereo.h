@@ -164,6 +164,35 @@ int ct_bm_census_process_lr(ct_handle* h, const ct_image* disp_lr, const ct_imag
 int ct_bm_census_match_desc(ct_handle* h, const ct_image* disp, const ct_image* desc_base,
                             const ct_image* desc_match, int32_t left_to_right, ct_stream stream);
 
+/* Cost-curve volume: the matcher's aggregated cost of every (pixel,
+ * disparity), one byte each, the input of the learned confidence net
+ * (ct_confnet_*). Code = min(255, 5x5 Hamming sum >> 2); 255 for a disparity
+ * whose match window leaves the image and for all disparities of a border
+ * pixel (within 2 of the image edge). Layout: groups g = 0 .. ceil(D/4) - 1
+ * of 4 disparities; row (y, g) starts at ptr + (y * ceil(D/4) + g) *
+ * pitch_bytes and holds one 32-bit word per pixel, word x + 2 for column x,
+ * whose byte k (little-endian) is the code of disparity 4g + k. pitch_bytes
+ * must be a multiple of 16 and at least 4 * (width + 2); ct_curves_pitch
+ * gives the packed choice. No counterpart in the reference: its matchers
+ * keep only the winning cost (BlockMatcherNCC.cu:491-592 WriteDisparity). */
+typedef struct ct_curves {
+    void* ptr;            /* device memory, 16-byte aligned, caller-owned */
+    size_t pitch_bytes;
+    int32_t width;
+    int32_t height;
+    int32_t disp_count;
+    int32_t reserved;
+} ct_curves;
+
+/* Row pitch (bytes, a multiple of 256) of a curve volume of this width. */
+int ct_curves_pitch(int32_t width, size_t* pitch_bytes);
+
+/* ct_bm_census_process that also writes the cost-curve volume of the
+ * configured direction (curves sized width x height x disp_count as
+ * configured). The disparity map is identical to ct_bm_census_process. */
+int ct_bm_census_process_curves(ct_handle* h, const ct_image* disp, const ct_curves* curves,
+                                const ct_image* left, const ct_image* right, ct_stream stream);
+
 /* Autotuner: times the kernel variants (4 or 8 disparities per warp) and
  * strip heights for this handle's (W, H, D, direction) on the given images,
  * keeps the fastest in the handle for later process calls. Synchronises
@@ -341,6 +370,54 @@ int ct_batch_graph_launch(ct_handle* h, ct_stream stream);
  */
 int ct_synth_pair(int32_t kind, uint64_t seed, int32_t width, int32_t height, int32_t dmax,
                   uint8_t* left, uint8_t* right, int16_t* gt, uint8_t* occ);
+
+/* ---- learned confidence ------------------------------------------------------
+ * A small network that scores, per pixel, how likely the census matcher's
+ * winner-take-all disparity is correct, from the pixel's cost curve
+ * (ct_curves, D = 128). It stands in for the right-to-left pass of the
+ * left-right check (CrossCheckDisparityMaps.cu:63-110), which stays the
+ * fallback and the judge of its error. No counterpart in the reference.
+ *
+ * Network: conv1 1->32 (k=5, stride 4, pad 2) -> max-pool 4 -> ReLU ->
+ * conv2 32->32 (k=5, stride 2, pad 2) -> ReLU -> conv3 32->32 (k=5, pad 1, one
+ * output) -> ReLU -> fc1 32->64 -> ReLU -> fc2 64->1 -> sigmoid. Weights bf16
+ * (fp32 master copies during training), biases fp32, accumulation fp32, conv
+ * activations rounded to bf16. Flat parameter order (CT_CONFNET_PARAMS
+ * floats): w1[32][5], b1[32], w2[32][32][5] ([out][in][tap]), b2[32],
+ * w3[32][32][5], b3[32], w4[64][32], b4[64], w5[64], b5.
+ *
+ * Training runs on the GPU with the library's own forward/backward kernels
+ * (CUDA cores, fp32 accumulation) and Adam; inference over a whole curve
+ * volume runs on the tensor cores (tcgen05, fp32 accumulation in TMEM).
+ * Device pointers below (samples, labels, xy, grad, loss, scores) are device
+ * memory. */
+#define CT_CONFNET_PARAMS 12673
+
+int ct_confnet_create(ct_handle** out);
+/* Allocates training scratch for up to max_batch samples per step and
+ * initialises the weights (ct_confnet_init with seed 1). */
+int ct_confnet_configure(ct_handle* h, int32_t device, int32_t max_batch);
+/* He-style random initialisation from a seed; resets the optimiser. */
+int ct_confnet_init(ct_handle* h, uint64_t seed);
+/* Host fp32 parameter vectors (save / load); set resets the optimiser. */
+int ct_confnet_set_params(ct_handle* h, const float* params, int32_t n);
+int ct_confnet_get_params(ct_handle* h, float* params, int32_t n);
+/* samples[n][128] (bytes) = curves at pixels xy[n] = (x, y) pairs. */
+int ct_confnet_gather(ct_handle* h, uint8_t* samples, const ct_curves* curves, const int32_t* xy, int32_t n,
+                      ct_stream stream);
+/* Mean binary cross-entropy of n samples (labels: 1 = disparity correct)
+ * and its gradient (CT_CONFNET_PARAMS floats); either output may be NULL. */
+int ct_confnet_loss_grad(ct_handle* h, const uint8_t* samples, const uint8_t* labels, int32_t n, float* grad,
+                         float* loss, ct_stream stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on n samples; loss may be NULL. */
+int ct_confnet_train_step(ct_handle* h, const uint8_t* samples, const uint8_t* labels, int32_t n, float lr,
+                          float* loss, ct_stream stream);
+/* Scores (sigmoid) of n samples through the training forward. */
+int ct_confnet_scores(ct_handle* h, float* scores, const uint8_t* samples, int32_t n, ct_stream stream);
+/* Score map (F32, P(disparity correct)) of a whole curve volume on the
+ * tensor cores. The first call after new weights packs them (synchronises
+ * the previous stream). */
+int ct_confnet_infer(ct_handle* h, const ct_image* score, const ct_curves* curves, ct_stream stream);
 
 /* ---- pipe-rate probe ---------------------------------------------------------
  * Measures the issue rate of the integer operations the matchers are built

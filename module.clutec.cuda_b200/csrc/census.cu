@@ -115,7 +115,7 @@ H* as(ct_handle* h, Kind k) {
 }
 
 int census_match_pass_maps(BmCensusHandle* h, int dir, const ct_image* disp, const CUtensorMap& tb,
-                           const CUtensorMap& tm, cudaStream_t s) {
+                           const CUtensorMap& tm, cudaStream_t s, const ct_curves* curves = nullptr) {
     using namespace cm;
     MatchArgs a{};
     a.W = h->fmt.width; a.H = h->fmt.height; a.D = h->par.disp_count;
@@ -125,15 +125,21 @@ int census_match_pass_maps(BmCensusHandle* h, int dir, const ct_image* disp, con
     a.merge_last = 1;
     a.out = disp->ptr; a.out_pitch = disp->pitch_bytes; a.out_type = disp->type;
     a.status = h->d_status;
+    if (curves) {
+        a.curve = static_cast<uint32_t*>(curves->ptr);
+        a.curve_pitch = curves->pitch_bytes / 4;
+        a.curve_groups = (a.D + 3) / 4;
+    }
     const cudaError_t e = dir == 0 ? launch_census_match<0>(tb, tm, a, s, h->dpw)
                                    : launch_census_match<1>(tb, tm, a, s, h->dpw);
     if (e != cudaSuccess) return fail(CT_ECUDA, "census match launch failed: %s", cudaGetErrorString(e));
     return CT_OK;
 }
 
-int census_match_pass(BmCensusHandle* h, int dir, const ct_image* disp, cudaStream_t s) {
-    return dir == 0 ? census_match_pass_maps(h, 0, disp, h->tm_lb, h->tm_rm, s)
-                    : census_match_pass_maps(h, 1, disp, h->tm_rb, h->tm_lm, s);
+int census_match_pass(BmCensusHandle* h, int dir, const ct_image* disp, cudaStream_t s,
+                      const ct_curves* curves = nullptr) {
+    return dir == 0 ? census_match_pass_maps(h, 0, disp, h->tm_lb, h->tm_rm, s, curves)
+                    : census_match_pass_maps(h, 1, disp, h->tm_rb, h->tm_lm, s, curves);
 }
 
 int census_both(BmCensusHandle* h, const ct_image* left, const ct_image* right, cudaStream_t s) {
@@ -276,6 +282,34 @@ int ct_bm_census_process(ct_handle* hh, const ct_image* disp, const ct_image* le
     h->last_stream = s;
     if (int rc = census_both(h, left, right, s)) return rc;
     return census_match_pass(h, h->par.left_to_right ? 0 : 1, disp, s);
+}
+
+int ct_curves_pitch(int32_t width, size_t* pitch_bytes) {
+    clear_error();
+    if (!pitch_bytes || width < 1) return fail(CT_EINVAL, "bad width or null output");
+    *pitch_bytes = cm::curve_pitch_words(width) * 4;
+    return CT_OK;
+}
+
+int ct_bm_census_process_curves(ct_handle* hh, const ct_image* disp, const ct_curves* curves,
+                                const ct_image* left, const ct_image* right, ct_stream stream) {
+    clear_error();
+    auto* h = as<BmCensusHandle>(hh, Kind::BmCensus);
+    if (!h) return fail(CT_ESTATE, "not a census matcher handle");
+    if (int rc = check_match_io(h, left, right)) return rc;
+    if (int rc = check_disp_out(h, disp, "disp")) return rc;
+    if (!curves || !curves->ptr) return fail(CT_EINVAL, "null curve volume");
+    if (curves->width != h->fmt.width || curves->height != h->fmt.height ||
+        curves->disp_count != h->par.disp_count)
+        return fail(CT_EFORMAT, "curve volume size differs from the configured format");
+    if (reinterpret_cast<uintptr_t>(curves->ptr) % 16 || curves->pitch_bytes % 16 ||
+        curves->pitch_bytes < 4 * (size_t(h->fmt.width) + 2))
+        return fail(CT_EINVAL, "curve volume needs a 16-byte aligned pointer and pitch >= 4 * (width + 2)");
+    if (int rc = use_device(h->device)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    h->last_stream = s;
+    if (int rc = census_both(h, left, right, s)) return rc;
+    return census_match_pass(h, h->par.left_to_right ? 0 : 1, disp, s, curves);
 }
 
 int ct_bm_census_process_lr(ct_handle* hh, const ct_image* disp_lr, const ct_image* disp_rl,

@@ -101,7 +101,20 @@ struct MatchArgs {
     size_t out_pitch;
     int out_type;       // CT_PIX_U8 / CT_PIX_U16
     int32_t* status;
+    // Optional cost-curve volume (kernels instantiated with CURVE = true):
+    // row (y, g) at curve + (y * curve_groups + g) * curve_pitch holds one
+    // 32-bit word per pixel, word x + 2 for column x, whose bytes are the
+    // codes of disparities 4g .. 4g + 3 (byte k = disparity 4g + k).
+    // Code = min(255, aggregated cost >> 2); 255 for a disparity whose match
+    // window leaves the image and for every disparity of a border pixel.
+    uint32_t* curve;
+    size_t curve_pitch;  // 32-bit words per row, a multiple of 4
+    int curve_groups;    // ceil(D / 4)
 };
+
+// Curve word pitch for width W: words 0 .. W + 1 used, rounded up to 64
+// words (256 bytes) so every row starts 16-byte aligned.
+__host__ __device__ constexpr size_t curve_pitch_words(int W) { return (size_t(W) + 2 + 63) / 64 * 64; }
 
 // Shared memory: 2 stages of base (10 rows x 66 pairs) and match (10 x 98
 // pairs) descriptors, 2 buffers x 2 groups x 10 rows x 128 key slots, 2
@@ -138,7 +151,7 @@ struct TileResult {
     bool aborted;
 };
 
-template <int DIR, bool EDGE, int DPW>
+template <int DIR, bool EDGE, int DPW, bool CURVE>
 __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const CUtensorMap* tmM,
                                                  const MatchArgs& a, const Tile& t, uint64_t* sB, uint64_t* sM,
                                                  uint32_t* sKey, uint64_t* bars, int* sflag, const uint32_t* par,
@@ -220,12 +233,63 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
             }
     };
 
+    // Writes this thread's curve codes of output row oy (see MatchArgs): one
+    // 32-bit word (4 disparities) per column and disparity group, the 4
+    // columns of a lane as one 16-byte store (word index xs + 4 lane + 2 is a
+    // multiple of 4); lanes 0 and 31 skip their halo columns.
+    auto store_curve = [&](const uint32_t (&C)[kCPT][NP], int oy) {
+        const int y = y0 + oy;
+        const bool rowv = y >= kAR && y < a.H - kAR;
+        constexpr int NG = DPW / 4;
+        uint32_t wv[kCPT][NG];
+#pragma unroll
+        for (int c = 0; c < kCPT; ++c) {
+            const int x = xs + 4 * lane + c;
+            const bool pv = rowv && x >= kAR && x < a.W - kAR;
+            uint32_t v[NP];
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                uint32_t t = dev::min_u16x2((C[c][p] >> 2) & 0x3FFF3FFFu, 0x00FF00FFu);
+                if (EDGE) {
+                    const int dlo = dw + 2 * p;
+                    t |= (dlo > lim[c] ? 0x000000FFu : 0u) | (dlo + 1 > lim[c] ? 0x00FF0000u : 0u);
+                }
+                v[p] = pv ? t : 0x00FF00FFu;
+            }
+#pragma unroll
+            for (int q = 0; q < NG; ++q) wv[c][q] = __byte_perm(v[2 * q], v[2 * q + 1], 0x6420);
+        }
+#pragma unroll
+        for (int q = 0; q < NG; ++q) {
+            const int g = (dw >> 2) + q;
+            if (g >= a.curve_groups) break;
+            uint32_t* dst = a.curve + ((size_t)y * a.curve_groups + g) * a.curve_pitch + (xs + 4 * lane + 2);
+            if (xs + kTWV - kAR <= a.W) {  // warp-uniform: every own column is inside the image
+                // lanes 1..30 store 4 columns; lane 0 its columns 2, 3; lane 31 its columns 0, 1
+                if (lane > 0 && lane < 31) {
+                    *reinterpret_cast<uint4*>(dst) = make_uint4(wv[0][q], wv[1][q], wv[2][q], wv[3][q]);
+                } else {
+                    const bool l0 = lane == 0;
+                    *reinterpret_cast<uint2*>(dst + (l0 ? 2 : 0)) =
+                        l0 ? make_uint2(wv[2][q], wv[3][q]) : make_uint2(wv[0][q], wv[1][q]);
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < kCPT; ++c) {
+                    const int v = 4 * lane + c;
+                    if (v >= kAR && v < kAR + kTWO && xs + v < a.W) dst[c] = wv[c][q];
+                }
+            }
+        }
+    };
+
     // Horizontal 5-wide sums of V and winner-take-all of this thread's
-    // disparities for its 4 columns, merged into key buffer `buf`, slot r.
+    // disparities for its 4 columns, merged into key buffer `buf`, slot r
+    // (output row oy of the strip).
     // Keys are stored column-interleaved (index c * 32 + lane) so the 32 lanes'
     // atomics hit 32 different banks; the halo columns' slots (V columns 0, 1,
     // 126, 127) receive values nobody reads.
-    auto emit = [&](int buf, int r) {
+    auto emit = [&](int buf, int r, int oy) {
         uint32_t C[kCPT][NP];
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
@@ -237,6 +301,9 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
             C[1][p] = C[0][p] + V[3][p] - h0;
             C[2][p] = C[1][p] + h4 - h1;
             C[3][p] = C[2][p] + h5 - V[0][p];
+        }
+        if constexpr (CURVE) {
+            if (oy >= 0 && oy < rows_here) store_curve(C, oy);
         }
         uint32_t* krow = sKey + ((buf * kGroups + grp) * kBR + r) * kTWV + lane;
 #pragma unroll
@@ -304,13 +371,13 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
             if (b == 0) {
 #pragma unroll
                 for (int r = 0; r < kBR; ++r) {
-                    if (r >= kRB) emit(0, r);
+                    if (r >= kRB) emit(0, r, r - kRB);
                     accum(s, r);
                 }
             } else {
 #pragma unroll
                 for (int r = 0; r < kBR; ++r) {
-                    emit(b & 1, r);
+                    emit(b & 1, r, kBR * b - kRB + r);
                     accum(s, r);
                 }
             }
@@ -335,7 +402,7 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
         flush(b & 1, kBR * b - kRB, b == 0 ? kRB : 0, kBR);
     }
     // the window ending at the last staged row: output kBR * nb - 5, buffer nb & 1, slot 0
-    if (warp_active) emit(nb & 1, 0);
+    if (warp_active) emit(nb & 1, 0, kBR * nb - kRB);
     __syncthreads();
     flush(nb & 1, kBR * nb - kRB, 0, 1);
 
@@ -385,7 +452,7 @@ struct Smem {
 
 // Runs one tile. The mbarriers must be initialised; par[s] counts the phases
 // stage s has completed so far in this CTA and is advanced here.
-template <int DIR, int DPW>
+template <int DIR, int DPW, bool CURVE = false>
 __device__ TileResult run_tile(const CUtensorMap* tmB, const CUtensorMap* tmM, const MatchArgs& a, const Tile& t,
                                const Smem& sm, uint32_t* par) {
     const int tid = threadIdx.x;
@@ -415,10 +482,10 @@ __device__ TileResult run_tile(const CUtensorMap* tmB, const CUtensorMap* tmM, c
         }
     }
     const TileResult res =
-        interior ? match_body<DIR, false, DPW>(tmB, tmM, a, t, sm.sB, sm.sM, sm.sKey, sm.bars, sm.sflag, par, nb,
-                                               rows_here, xs, y0, ye0, dz0, ms)
-                 : match_body<DIR, true, DPW>(tmB, tmM, a, t, sm.sB, sm.sM, sm.sKey, sm.bars, sm.sflag, par, nb,
-                                              rows_here, xs, y0, ye0, dz0, ms);
+        interior ? match_body<DIR, false, DPW, CURVE>(tmB, tmM, a, t, sm.sB, sm.sM, sm.sKey, sm.bars, sm.sflag, par,
+                                                      nb, rows_here, xs, y0, ye0, dz0, ms)
+                 : match_body<DIR, true, DPW, CURVE>(tmB, tmM, a, t, sm.sB, sm.sM, sm.sKey, sm.bars, sm.sflag, par,
+                                                     nb, rows_here, xs, y0, ye0, dz0, ms);
     par[0] += (nb + 1) / 2;
     par[1] += nb / 2;
     __syncthreads();  // the next tile reuses the shared memory
@@ -434,7 +501,7 @@ __device__ __forceinline__ void init_barriers(const Smem& sm) {
     __syncthreads();
 }
 
-template <int DIR, int DPW>
+template <int DIR, int DPW, bool CURVE = false>
 __global__ void __launch_bounds__(Var<DPW>::kNT, 1)
     census_match_kernel(const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmM,
                         MatchArgs a) {
@@ -443,7 +510,7 @@ __global__ void __launch_bounds__(Var<DPW>::kNT, 1)
     init_barriers(sm);
     uint32_t par[2] = {0, 0};
     const Tile t{int(blockIdx.x), int(blockIdx.y), int(blockIdx.z), int(gridDim.x), int(gridDim.z)};
-    run_tile<DIR, DPW>(&tmB, &tmM, a, t, sm, par);
+    run_tile<DIR, DPW, CURVE>(&tmB, &tmM, a, t, sm, par);
 }
 
 // Converts merged keys to disparities and resets the keys for the next call.
@@ -499,14 +566,18 @@ inline int make_planar_maps(CUtensorMap* tb, CUtensorMap* tm, const uint64_t* ba
 // kernel instantiation. Sets function attributes only (no allocation).
 inline cudaError_t prepare_census_match() {
     const int smem = int(smem_bytes());
-    cudaError_t e = cudaFuncSetAttribute(census_match_kernel<0, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(census_match_kernel<0, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(census_match_kernel<1, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(census_match_kernel<1, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    return e;
+    const void* kernels[] = {
+        reinterpret_cast<const void*>(census_match_kernel<0, 4>), reinterpret_cast<const void*>(census_match_kernel<0, 8>),
+        reinterpret_cast<const void*>(census_match_kernel<1, 4>), reinterpret_cast<const void*>(census_match_kernel<1, 8>),
+        reinterpret_cast<const void*>(census_match_kernel<0, 4, true>),
+        reinterpret_cast<const void*>(census_match_kernel<0, 8, true>),
+        reinterpret_cast<const void*>(census_match_kernel<1, 4, true>),
+        reinterpret_cast<const void*>(census_match_kernel<1, 8, true>)};
+    for (const void* k : kernels) {
+        const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 // Launches one matching pass (+ the key finalize when D is split over CTAs).
@@ -514,8 +585,13 @@ template <int DIR>
 inline cudaError_t launch_census_match(const CUtensorMap& tb, const CUtensorMap& tm, const MatchArgs& a,
                                        cudaStream_t s, int dpw = 4) {
     dim3 grid((a.W + kTWO - 1) / kTWO, (a.H + a.th - 1) / a.th, (a.D + kDPC - 1) / kDPC);
-    if (dpw == 8) census_match_kernel<DIR, 8><<<grid, Var<8>::kNT, smem_bytes(), s>>>(tb, tm, a);
-    else census_match_kernel<DIR, 4><<<grid, Var<4>::kNT, smem_bytes(), s>>>(tb, tm, a);
+    if (a.curve) {
+        if (dpw == 8) census_match_kernel<DIR, 8, true><<<grid, Var<8>::kNT, smem_bytes(), s>>>(tb, tm, a);
+        else census_match_kernel<DIR, 4, true><<<grid, Var<4>::kNT, smem_bytes(), s>>>(tb, tm, a);
+    } else {
+        if (dpw == 8) census_match_kernel<DIR, 8><<<grid, Var<8>::kNT, smem_bytes(), s>>>(tb, tm, a);
+        else census_match_kernel<DIR, 4><<<grid, Var<4>::kNT, smem_bytes(), s>>>(tb, tm, a);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || grid.z == 1 || a.merge_last) return e;
     keys_finalize_kernel<<<dim3((a.W + 255) / 256, a.H), 256, 0, s>>>(a.keys, a.W, a.H, kAR, a.out, a.out_pitch,

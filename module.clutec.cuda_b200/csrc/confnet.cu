@@ -1,0 +1,1154 @@
+// confnet.cu — learned confidence for census disparities: a small 1D-conv +
+// MLP network that reads a pixel's census cost curve (128 disparities, one
+// byte each, from ct_bm_census_process_curves) and scores how likely the
+// winner-take-all disparity is correct. It stands in for the right-to-left
+// matching pass of the left-right check (CrossCheckDisparityMaps.cu:63-110),
+// which stays as the fallback and as the judge of its error.
+//
+// Network (weights bf16, biases fp32, accumulation fp32):
+//   conv1  1 -> 32, k=5, stride 4, pad 2 -> 32 positions (no bias); sum over
+//          4 positions + bias; ReLU; rounded to bf16 -> a1[8][32]
+//   conv2 32 -> 32, k=5, stride 2, pad 2 -> 4 positions; ReLU; bf16 -> a2[4][32]
+//   conv3 32 -> 32, k=5, pad 1, one output; ReLU; bf16 -> a3[32]
+//   fc1   32 -> 64, ReLU (fp32) -> a4[64]
+//   fc2   64 -> 1, logit; score = sigmoid(logit)
+// Flat parameter order: w1[32][5], b1[32], w2[32][32][5] ([out][in][tap]),
+// b2[32], w3[32][32][5], b3[32], w4[64][32], b4[64], w5[64], b5[1].
+//
+// Training (CUDA cores): layer kernels with one thread per (sample, channel)
+// keep the activations each backward step needs; weight gradients are
+// reduced per chunk of samples into partial sums that the Adam kernel adds
+// in a fixed order (deterministic). Adam keeps fp32 master weights and
+// writes their bf16 roundings for the next forward.
+//
+// Inference (tensor cores, tcgen05): a persistent kernel, one CTA of 8 warps
+// per SM, 128 pixels (one row segment) per tile. Each layer is a set of
+// M=128 tcgen05.mma into TMEM (fp32): conv1 as 16 windows of K=16 inputs x
+// N=64 (2 positions x 32 channels, f16 operands: curve codes are integers,
+// exact in f16, and the bf16 weights are exact in f16), conv2/conv3 per
+// output position as K=16 slices (channel halves) of each tap (bf16), fc1
+// K=32 x N=64. Biases are written into the accumulator columns with
+// tcgen05.st before each layer. Epilogue warps read the accumulators with
+// tcgen05.ld, pool / ReLU / round to bf16 and write the next layer's A
+// operand to shared memory; conv1 runs in 8 chunks of 2 windows into two
+// TMEM buffers so the MMAs of chunk k+1 overlap the epilogue of chunk k.
+#include "ct_internal.h"
+#include "ct_device.cuh"
+#include "census_match.cuh"
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+namespace ct {
+namespace cn {
+
+// ---------------------------------------------------------------------------
+// Parameter layout
+// ---------------------------------------------------------------------------
+constexpr int kOffW1 = 0, kOffB1 = 160, kOffW2 = 192, kOffB2 = 5312, kOffW3 = 5344, kOffB3 = 10464,
+              kOffW4 = 10496, kOffB4 = 12544, kOffW5 = 12608, kOffB5 = 12672;
+constexpr int kParams = 12673;
+static_assert(kParams == CT_CONFNET_PARAMS, "parameter count");
+constexpr int kLen = 128;  // curve length (disparities)
+
+__host__ __device__ inline bool is_weight(int p) {
+    return p < kOffB1 || (p >= kOffW2 && p < kOffB2) || (p >= kOffW3 && p < kOffB3) || (p >= kOffW4 && p < kOffB4) ||
+           (p >= kOffW5 && p < kOffB5);
+}
+
+__device__ __forceinline__ float bf16r(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
+
+// ---------------------------------------------------------------------------
+// Gather: samples[n][128] from a curve volume at pixel list xy[n][2]
+// ---------------------------------------------------------------------------
+// Pixels outside the volume read as all-255 curves and set CT_EINVAL.
+__global__ void gather_kernel(uint8_t* samples, const uint32_t* curve, size_t pitch_words, int groups, int W,
+                              int H, const int32_t* xy, int n, int32_t* status) {
+    const int s = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int g = threadIdx.x & 31;
+    if (s >= n) return;
+    const int x = xy[2 * s], y = xy[2 * s + 1];
+    const bool inside = x >= 0 && x < W && y >= 0 && y < H;
+    if (!inside && g == 0) dev::report(status, CT_EINVAL);
+    const uint32_t w = (inside && g < groups) ? curve[((size_t)y * groups + g) * pitch_words + x + 2] : 0xFFFFFFFFu;
+    reinterpret_cast<uint32_t*>(samples + (size_t)s * kLen)[g] = w;
+}
+
+// ---------------------------------------------------------------------------
+// Training kernels (block (32, 16): threadIdx.x = channel, threadIdx.y = sample)
+// ---------------------------------------------------------------------------
+struct Act {  // per-sample activations and gradient signals, [n][...]
+    float* a1;      // [8][32] bf16 values
+    float* a2;      // [4][32]
+    float* a3;      // [32]
+    float* a4;      // [64]
+    float* logit;   // [1]
+    float* dl;      // dloss/dlogit
+    float* loss;    // per-sample loss
+    float* dz4;     // [64]
+    float* dz3;     // [32]
+    float* dz2;     // [4][32]
+    float* dm1;     // [8][32]
+};
+
+constexpr int kSY = 16;  // samples per CTA
+
+__global__ void __launch_bounds__(32 * kSY) fwd1_kernel(const uint8_t* x, const float* wq, Act A, int n) {
+    __shared__ float xs[kSY][kLen];
+    const int o = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * kSY + sl;
+    for (int k = threadIdx.x; k < kLen; k += 32) xs[sl][k] = s < n ? float(x[(size_t)s * kLen + k]) : 0.f;
+    __syncthreads();
+    if (s >= n) return;
+    float w[5];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) w[j] = wq[kOffW1 + o * 5 + j];
+    const float b = wq[kOffB1 + o];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        float z = b;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int p = 4 * q + k;
+#pragma unroll
+            for (int j = 0; j < 5; ++j) {
+                const int i = 4 * p + j - 2;
+                if (i >= 0 && i < kLen) z = fmaf(w[j], xs[sl][i], z);
+            }
+        }
+        A.a1[(size_t)s * 256 + q * 32 + o] = bf16r(fmaxf(z, 0.f));
+    }
+}
+
+__global__ void __launch_bounds__(32 * kSY) fwd2_kernel(const float* wq, Act A, int n) {
+    __shared__ float wt[32][5][32];  // [in][tap][out]
+    __shared__ float as[kSY][8][32];
+    const int o = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * kSY + sl;
+    const int tid = sl * 32 + o;
+    for (int k = tid; k < 5120; k += 32 * kSY) {
+        const int oo = k / 160, i = (k / 5) % 32, j = k % 5;
+        wt[i][j][oo] = wq[kOffW2 + k];
+    }
+    for (int k = o; k < 256; k += 32) as[sl][k / 32][k % 32] = s < n ? A.a1[(size_t)s * 256 + k] : 0.f;
+    __syncthreads();
+    if (s >= n) return;
+    float z[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) z[r] = wq[kOffB2 + o];
+    for (int i = 0; i < 32; ++i) {
+#pragma unroll
+        for (int j = 0; j < 5; ++j) {
+            const float w = wt[i][j][o];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int q = 2 * r + j - 2;
+                if (q >= 0 && q < 8) z[r] = fmaf(w, as[sl][q][i], z[r]);
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) A.a2[(size_t)s * 128 + r * 32 + o] = bf16r(fmaxf(z[r], 0.f));
+}
+
+__global__ void __launch_bounds__(32 * kSY) fwd3_kernel(const float* wq, Act A, int n) {
+    __shared__ float wt[32][5][32];
+    __shared__ float as[kSY][4][32];
+    const int o = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * kSY + sl;
+    const int tid = sl * 32 + o;
+    for (int k = tid; k < 5120; k += 32 * kSY) {
+        const int oo = k / 160, i = (k / 5) % 32, j = k % 5;
+        wt[i][j][oo] = wq[kOffW3 + k];
+    }
+    for (int k = o; k < 128; k += 32) as[sl][k / 32][k % 32] = s < n ? A.a2[(size_t)s * 128 + k] : 0.f;
+    __syncthreads();
+    if (s >= n) return;
+    float z = wq[kOffB3 + o];
+    for (int i = 0; i < 32; ++i) {
+#pragma unroll
+        for (int j = 1; j < 5; ++j) z = fmaf(wt[i][j][o], as[sl][j - 1][i], z);
+    }
+    A.a3[(size_t)s * 32 + o] = bf16r(fmaxf(z, 0.f));
+}
+
+// block (64, 8)
+__global__ void __launch_bounds__(512) fwd4_kernel(const float* wq, Act A, int n) {
+    __shared__ float wt[32][64];  // [in][hidden]
+    __shared__ float as[8][32];
+    const int h = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * 8 + sl;
+    const int tid = sl * 64 + h;
+    for (int k = tid; k < 2048; k += 512) wt[k % 32][k / 32] = wq[kOffW4 + k];
+    if (h < 32) as[sl][h] = s < n ? A.a3[(size_t)s * 32 + h] : 0.f;
+    __syncthreads();
+    if (s >= n) return;
+    float z = wq[kOffB4 + h];
+#pragma unroll 8
+    for (int i = 0; i < 32; ++i) z = fmaf(wt[i][h], as[sl][i], z);
+    A.a4[(size_t)s * 64 + h] = fmaxf(z, 0.f);
+}
+
+// one thread per sample: logit, loss, dloss/dlogit (labels may be null: scores only)
+__global__ void head_kernel(const float* wq, Act A, const uint8_t* labels, float inv_n, float* scores, int n) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    float z = wq[kOffB5];
+    for (int h = 0; h < 64; ++h) z = fmaf(wq[kOffW5 + h], A.a4[(size_t)s * 64 + h], z);
+    A.logit[s] = z;
+    const float p = 1.f / (1.f + expf(-z));
+    if (scores) scores[s] = p;
+    if (labels) {
+        const float y = labels[s] ? 1.f : 0.f;
+        A.dl[s] = (p - y) * inv_n;
+        A.loss[s] = fmaxf(z, 0.f) + log1pf(expf(-fabsf(z))) - y * z;
+    }
+}
+
+// block (64, 8): dz4 = dl * w5 * (a4 > 0)
+__global__ void bwd4_kernel(const float* wq, Act A, int n) {
+    const int h = threadIdx.x, s = blockIdx.x * 8 + threadIdx.y;
+    if (s >= n) return;
+    const float a = A.a4[(size_t)s * 64 + h];
+    A.dz4[(size_t)s * 64 + h] = a > 0.f ? A.dl[s] * wq[kOffW5 + h] : 0.f;
+}
+
+// block (32, 16): dz3 = (W4^T dz4) * (a3 > 0)
+__global__ void __launch_bounds__(32 * kSY) bwd3_kernel(const float* wq, Act A, int n) {
+    __shared__ float w4[64][33];
+    const int o = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * kSY + sl;
+    for (int k = sl * 32 + o; k < 2048; k += 32 * kSY) w4[k / 32][k % 32] = wq[kOffW4 + k];
+    __syncthreads();
+    if (s >= n) return;
+    float g = 0.f;
+    for (int h = 0; h < 64; ++h) g = fmaf(A.dz4[(size_t)s * 64 + h], w4[h][o], g);
+    A.dz3[(size_t)s * 32 + o] = A.a3[(size_t)s * 32 + o] > 0.f ? g : 0.f;
+}
+
+// block (32, 16), thread = input channel i: dz2[pos][i] = sum_o dz3[o] w3[o][i][pos+1], masked
+__global__ void __launch_bounds__(32 * kSY) bwd2_kernel(const float* wq, Act A, int n) {
+    __shared__ float w3[32][32][6];  // [out][in][tap], padded
+    __shared__ float g3[kSY][32];
+    const int i = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * kSY + sl;
+    for (int k = sl * 32 + i; k < 5120; k += 32 * kSY) w3[k / 160][(k / 5) % 32][k % 5] = wq[kOffW3 + k];
+    g3[sl][i] = s < n ? A.dz3[(size_t)s * 32 + i] : 0.f;
+    __syncthreads();
+    if (s >= n) return;
+#pragma unroll
+    for (int pos = 0; pos < 4; ++pos) {
+        float g = 0.f;
+        for (int o = 0; o < 32; ++o) g = fmaf(g3[sl][o], w3[o][i][pos + 1], g);
+        const size_t k = (size_t)s * 128 + pos * 32 + i;
+        A.dz2[k] = A.a2[k] > 0.f ? g : 0.f;
+    }
+}
+
+// block (32, 16), thread = input channel i: dm1[q][i] = sum_{r,j: 2r+j-2=q} sum_o dz2[r][o] w2[o][i][j], masked
+__global__ void __launch_bounds__(32 * kSY) bwd1_kernel(const float* wq, Act A, int n) {
+    __shared__ float w2[32][32][6];
+    __shared__ float g2[kSY][4][32];
+    const int i = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * kSY + sl;
+    for (int k = sl * 32 + i; k < 5120; k += 32 * kSY) w2[k / 160][(k / 5) % 32][k % 5] = wq[kOffW2 + k];
+    for (int k = i; k < 128; k += 32) g2[sl][k / 32][k % 32] = s < n ? A.dz2[(size_t)s * 128 + k] : 0.f;
+    __syncthreads();
+    if (s >= n) return;
+    float da[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) da[q] = 0.f;
+    for (int o = 0; o < 32; ++o) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const float g = g2[sl][r][o];
+#pragma unroll
+            for (int j = 0; j < 5; ++j) {
+                const int q = 2 * r + j - 2;
+                if (q >= 0 && q < 8) da[q] = fmaf(g, w2[o][i][j], da[q]);
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const size_t k = (size_t)s * 256 + q * 32 + i;
+        A.dm1[k] = A.a1[k] > 0.f ? da[q] : 0.f;
+    }
+}
+
+// Weight gradients of one layer (blockIdx.y) over one chunk of samples
+// (blockIdx.x), written to part[chunk][param]. 256 threads.
+constexpr int kChunk = 256;
+
+__global__ void __launch_bounds__(256) wgrad_kernel(const uint8_t* x, Act A, int n, float* part) {
+    const int t = threadIdx.x;
+    const int s0 = blockIdx.x * kChunk, s1 = min(n, s0 + kChunk);
+    float* P = part + (size_t)blockIdx.x * kParams;
+    switch (blockIdx.y) {
+        case 0: {  // w1 (o, j) for t < 160, b1 for 160 <= t < 192
+            if (t >= 192) return;
+            const bool bias = t >= 160;
+            const int o = bias ? t - 160 : t / 5, j = t % 5;
+            float acc = 0.f;
+            for (int s = s0; s < s1; ++s) {
+                for (int q = 0; q < 8; ++q) {
+                    const float g = A.dm1[(size_t)s * 256 + q * 32 + o];
+                    if (g == 0.f) continue;
+                    if (bias) { acc += g; continue; }
+                    float xsum = 0.f;  // inputs of tap j over the 4 pooled positions
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int i = 4 * (4 * q + k) + j - 2;
+                        if (i >= 0 && i < kLen) xsum += float(x[(size_t)s * kLen + i]);
+                    }
+                    acc = fmaf(g, xsum, acc);
+                }
+            }
+            P[bias ? kOffB1 + o : kOffW1 + t] = acc;
+            break;
+        }
+        case 1: {  // w2: pairs (o, i) = t + 256 k, k < 4; b2 for t < 32
+            float acc[4][5] = {};
+            float bacc = 0.f;
+            for (int s = s0; s < s1; ++s) {
+                const float* a1 = A.a1 + (size_t)s * 256;
+                const float* g2 = A.dz2 + (size_t)s * 128;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int pi = t + 256 * k, o = pi / 32, i = pi % 32;
+                    float g[4], av[8];
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) g[r] = g2[r * 32 + o];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) av[q] = a1[q * 32 + i];
+#pragma unroll
+                    for (int j = 0; j < 5; ++j)
+#pragma unroll
+                        for (int r = 0; r < 4; ++r) {
+                            const int q = 2 * r + j - 2;
+                            if (q >= 0 && q < 8) acc[k][j] = fmaf(g[r], av[q], acc[k][j]);
+                        }
+                }
+                if (t < 32)
+                    for (int r = 0; r < 4; ++r) bacc += g2[r * 32 + t];
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int pi = t + 256 * k, o = pi / 32, i = pi % 32;
+#pragma unroll
+                for (int j = 0; j < 5; ++j) P[kOffW2 + o * 160 + i * 5 + j] = acc[k][j];
+            }
+            if (t < 32) P[kOffB2 + t] = bacc;
+            break;
+        }
+        case 2: {  // w3: pairs (o, i); tap 0 always meets padding; b3 for t < 32
+            float acc[4][5] = {};
+            float bacc = 0.f;
+            for (int s = s0; s < s1; ++s) {
+                const float* a2 = A.a2 + (size_t)s * 128;
+                const float* g3 = A.dz3 + (size_t)s * 32;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int pi = t + 256 * k, o = pi / 32, i = pi % 32;
+                    const float g = g3[o];
+#pragma unroll
+                    for (int j = 1; j < 5; ++j) acc[k][j] = fmaf(g, a2[(j - 1) * 32 + i], acc[k][j]);
+                }
+                if (t < 32) bacc += g3[t];
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int pi = t + 256 * k, o = pi / 32, i = pi % 32;
+#pragma unroll
+                for (int j = 0; j < 5; ++j) P[kOffW3 + o * 160 + i * 5 + j] = acc[k][j];
+            }
+            if (t < 32) P[kOffB3 + t] = bacc;
+            break;
+        }
+        case 3: {  // w4: pairs (h, i) = t + 256 k, k < 8; b4 for t < 64
+            float acc[8] = {};
+            float bacc = 0.f;
+            for (int s = s0; s < s1; ++s) {
+                const float* a3 = A.a3 + (size_t)s * 32;
+                const float* g4 = A.dz4 + (size_t)s * 64;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int pi = t + 256 * k;
+                    acc[k] = fmaf(g4[pi / 32], a3[pi % 32], acc[k]);
+                }
+                if (t < 64) bacc += g4[t];
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) P[kOffW4 + t + 256 * k] = acc[k];
+            if (t < 64) P[kOffB4 + t] = bacc;
+            break;
+        }
+        default: {  // w5 for t < 64, b5 for t == 64
+            if (t > 64) return;
+            float acc = 0.f;
+            for (int s = s0; s < s1; ++s) acc += t < 64 ? A.dl[s] * A.a4[(size_t)s * 64 + t] : A.dl[s];
+            P[t < 64 ? kOffW5 + t : kOffB5] = acc;
+            break;
+        }
+    }
+}
+
+// Sums the chunk partials (fixed order) into grad; with adam != 0 also
+// applies one Adam step to the fp32 master weights and refreshes wq.
+struct AdamArgs {
+    int adam;
+    float lr, beta1, beta2, eps, c1, c2;  // c1 = 1 - beta1^t, c2 = 1 - beta2^t
+};
+
+__global__ void reduce_adam_kernel(const float* part, int chunks, float* grad, float* master, float* m, float* v,
+                                   float* wq, AdamArgs aa) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= kParams) return;
+    float g = 0.f;
+    for (int c = 0; c < chunks; ++c) g += part[(size_t)c * kParams + p];
+    if (grad) grad[p] = g;
+    if (!aa.adam) return;
+    const float mm = aa.beta1 * m[p] + (1.f - aa.beta1) * g;
+    const float vv = aa.beta2 * v[p] + (1.f - aa.beta2) * g * g;
+    m[p] = mm;
+    v[p] = vv;
+    const float w = master[p] - aa.lr * (mm / aa.c1) / (sqrtf(vv / aa.c2) + aa.eps);
+    master[p] = w;
+    wq[p] = is_weight(p) ? bf16r(w) : w;
+}
+
+// Deterministic mean of the per-sample losses (one CTA).
+__global__ void loss_mean_kernel(const float* loss, int n, float* out) {
+    __shared__ float red[256];
+    float acc = 0.f;
+    for (int s = threadIdx.x; s < n; s += 256) acc += loss[s];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int k = 128; k > 0; k >>= 1) {
+        if (threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = red[0] / float(n);
+}
+
+// ---------------------------------------------------------------------------
+// Inference kernel (tcgen05)
+// ---------------------------------------------------------------------------
+namespace inf {
+
+constexpr int kNT = 256;  // 2 warpgroups; each runs its own stream of tiles
+constexpr int kM = 128;   // pixels per tile = TMEM lanes = MMA M
+constexpr int kChunkBytes = kM * 16;  // one K-chunk (8 elements) of a 128-row operand
+
+// Shared-memory image. Operands are K-major without swizzle, stored as
+// K-chunk panels: element (row r, k) at (k / 8) * rows * 16 + r * 16 +
+// (k % 8) * 2, so a descriptor's leading byte offset (next K-chunk) is
+// rows * 16 and its stride byte offset (next 8 rows) is 128.
+// Per warpgroup:
+//   region X: A1 = curve codes (f16), 18 chunks = inputs -8 .. 135; later A3
+//             = conv2 output a2[r][ch] (bf16), chunk r * 4 + ch / 8
+//   region Y: A2 = pooled conv1 output a1[q][ch] (bf16), chunk q * 4 + ch / 8;
+//             later A4 = conv3 output a3[ch], chunk ch / 8
+// (A3 is written after the conv1 MMAs that read A1 have completed, A4 after
+// the conv2 MMAs that read A2.)
+constexpr int kRegX = 18 * kChunkBytes;
+constexpr int kRegY = 32 * kChunkBytes;
+constexpr int kWG = kRegX + kRegY;
+constexpr int kWImg = 2 * kWG;
+// packed weight image (also the device buffer layout written by the host)
+constexpr int kB1e = 0;                   // conv1, even positions: N=32 x K=16 f16, taps at k = 6..10 (LBO 512)
+constexpr int kB1o = kB1e + 2 * 32 * 16;  // conv1, odd positions: taps at k = 2..6
+constexpr int kB2 = kB1o + 2 * 32 * 16;   // N=32 x K=160 bf16: chunks tap * 4 + in / 8 (LBO 512)
+constexpr int kB3 = kB2 + 20 * 32 * 16;
+constexpr int kB4 = kB3 + 20 * 32 * 16;   // N=64 x K=32 bf16: 4 chunks of 64 rows (LBO 1024)
+constexpr int kBias = kB4 + 4 * 64 * 16;  // fp32: b1[32] b2[32] b3[32] b4[64] w5[64] b5
+constexpr int kWBytes = kBias + (32 + 32 + 32 + 64 + 64 + 4) * 4;
+constexpr int kBar = kWImg + kWBytes;     // 2 mbarriers per warpgroup
+constexpr int kTmemSlot = kBar + 4 * 8;
+constexpr int kSmem = kTmemSlot + 16;
+static_assert(kWBytes % 16 == 0, "weight image must be a whole number of 16-byte words");
+static_assert(kSmem <= 232448, "shared memory");
+
+// TMEM: 512 columns, 256 per warpgroup: conv1 accumulators (8 pooled
+// positions x 32) at 0..255; conv2 (4 x 32) at 0..127 once conv1's are read;
+// conv3 at 128..159; fc1 at 160..223.
+constexpr uint32_t kTmemCols = 512;
+constexpr uint32_t kColC2 = 0, kColC3 = 128, kColF1 = 160;
+
+// Instruction descriptors (kind::f16): D fp32 (bit 4), A/B format at bits
+// 7 / 10 (0 = f16, 1 = bf16), both K-major, N >> 3 at bit 17, M >> 4 at 24.
+constexpr uint32_t idesc(int fmt, int N) {
+    return (1u << 4) | (uint32_t(fmt) << 7) | (uint32_t(fmt) << 10) | (uint32_t(N >> 3) << 17) |
+           (uint32_t(kM >> 4) << 24);
+}
+constexpr uint32_t kIdC1 = idesc(0, 32), kIdC2 = idesc(1, 32), kIdF1 = idesc(1, 64);
+
+// Shared-memory matrix descriptor: start, leading byte offset (next K chunk),
+// stride byte offset 128 (next 8 rows), version 1, no swizzle.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo) {
+    return uint64_t((saddr >> 4) & 0x3FFF) | (uint64_t((lbo >> 4) & 0x3FFF) << 16) | (uint64_t(128 >> 4) << 32) |
+           (uint64_t(1) << 46);
+}
+
+__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t id) {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, 1, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(id)
+        : "memory");
+}
+__device__ __forceinline__ void commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     dev::smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// Barrier of one warpgroup (named barrier id, 128 threads).
+__device__ __forceinline__ void wg_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+// Same, returning whether any of the 128 threads passed a non-zero flag.
+__device__ __forceinline__ bool wg_sync_or(int id, bool flag) {
+    uint32_t r;
+    asm volatile(
+        "{\n.reg .pred p, q;\nsetp.ne.u32 q, %1, 0;\nbar.red.or.pred p, %2, 128, q;\nselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(r)
+        : "r"(uint32_t(flag)), "r"(id)
+        : "memory");
+    return r != 0;
+}
+
+// 32 consecutive TMEM columns of this thread's lane, with the load's wait in
+// the same asm statement (the registers are defined only after completion).
+__device__ __forceinline__ void ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "{\n"
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        "tcgen05.wait::ld.sync.aligned;\n"
+        "}\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int k = 0; k < 32; ++k) v[k] = __uint_as_float(r[k]);
+}
+__device__ __forceinline__ void st32(uint32_t taddr, const float (&v)[32]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])),
+        "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])),
+        "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])),
+        "r"(__float_as_uint(v[11])), "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])),
+        "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15])), "r"(__float_as_uint(v[16])),
+        "r"(__float_as_uint(v[17])), "r"(__float_as_uint(v[18])), "r"(__float_as_uint(v[19])),
+        "r"(__float_as_uint(v[20])), "r"(__float_as_uint(v[21])), "r"(__float_as_uint(v[22])),
+        "r"(__float_as_uint(v[23])), "r"(__float_as_uint(v[24])), "r"(__float_as_uint(v[25])),
+        "r"(__float_as_uint(v[26])), "r"(__float_as_uint(v[27])), "r"(__float_as_uint(v[28])),
+        "r"(__float_as_uint(v[29])), "r"(__float_as_uint(v[30])), "r"(__float_as_uint(v[31]))
+        : "memory");
+}
+
+// bf16x2 with relu: low half = a, high half = b
+__device__ __forceinline__ uint32_t pack_relu(float a, float b) {
+    uint32_t d;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(b), "f"(a));
+    return d;
+}
+// Two curve codes (bytes sel of w) -> f16x2 of their integer values: the
+// bytes become the low mantissa of 1024.0 (0x6400), then 1024 is subtracted.
+__device__ __forceinline__ uint32_t codes_f16x2(uint32_t w, uint32_t sel) {
+    const uint32_t h = __byte_perm(w, 0x64646464u, sel);
+    uint32_t d;
+    asm("sub.rn.f16x2 %0, %1, %2;" : "=r"(d) : "r"(h), "r"(0x64006400u));
+    return d;
+}
+// 32 channels (fp32 accumulators) -> ReLU -> bf16 -> 4 chunks of an operand
+__device__ __forceinline__ void store_bf16_row(unsigned char* chunk0, int m, const float (&v)[32]) {
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc)
+        *reinterpret_cast<uint4*>(chunk0 + cc * kChunkBytes + m * 16) =
+            make_uint4(pack_relu(v[8 * cc], v[8 * cc + 1]), pack_relu(v[8 * cc + 2], v[8 * cc + 3]),
+                       pack_relu(v[8 * cc + 4], v[8 * cc + 5]), pack_relu(v[8 * cc + 6], v[8 * cc + 7]));
+}
+
+struct InferArgs {
+    const uint32_t* curve;
+    size_t curve_pitch;  // words
+    int groups;          // 32
+    int W, H;
+    float* score;
+    size_t score_pitch;  // bytes
+    const uint4* wimg;   // packed weight image (kWBytes)
+    int32_t* status;
+};
+
+__global__ void __launch_bounds__(kNT, 1) infer_kernel(InferArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int wg = tid >> 7;               // warpgroup
+    const int m = tid & 127;               // pixel of the tile = TMEM lane
+    const int bar_id = 1 + wg;             // named barrier of this warpgroup
+    const bool issuer = m == 0;            // issues this warpgroup's MMAs
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kBar) + 2 * wg;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kTmemSlot);
+    unsigned char* X = smem + wg * kWG;    // A1 / A3
+    unsigned char* Y = X + kRegX;          // A2 / A4
+    const uint32_t sX = dev::smem_u32(X), sY = dev::smem_u32(Y), sW = dev::smem_u32(smem + kWImg);
+
+    for (int k = tid; k < kWBytes / 16; k += kNT) reinterpret_cast<uint4*>(smem + kWImg)[k] = a.wimg[k];
+    if (tid == 0) {
+        for (int b = 0; b < 4; ++b) dev::mbar_init(reinterpret_cast<uint64_t*>(smem + kBar) + b, 1);
+        dev::fence_barrier_init();
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dev::smem_u32(tslot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tm = *tslot + 256u * wg;                      // this warpgroup's columns
+    const uint32_t tl = tm + (uint32_t((warp & 3) * 32) << 16);  // + this warp's lane quarter
+
+    const float* bias = reinterpret_cast<const float*>(smem + kWImg + kBias);
+    const float* w5 = bias + 160;
+    const float b5 = bias[224];
+
+    const int tiles_x = (a.W + kM - 1) / kM;
+    const int tiles = tiles_x * a.H;
+    const int stride = 2 * gridDim.x;
+    uint32_t ph[2] = {0, 0};  // phases waited for, per mbarrier of this warpgroup
+    uint32_t cm[2] = {0, 0};  // commits issued (issuer thread)
+    bool failed = false;
+    auto commit_to = [&](int b) {
+        commit(&bars[b]);
+        ++cm[b];
+    };
+    auto wait_bar = [&](int b) {  // a phase that timed out stays pending in ph
+        const bool ok = dev::mbar_wait_bounded(&bars[b], ph[b] & 1);
+        if (ok) ++ph[b];
+        return ok;
+    };
+
+    // this thread's curve words (pixel m, 32 groups of 4 disparities)
+    uint32_t cw[32];
+    auto load_curve = [&](int t) {
+        const int y = t / tiles_x, x = (t % tiles_x) * kM + m;
+#pragma unroll
+        for (int g = 0; g < 32; ++g)
+            cw[g] = x < a.W ? __ldg(a.curve + ((size_t)y * a.groups + g) * a.curve_pitch + x + 2) : 0xFFFFFFFFu;
+    };
+
+    int t = 2 * blockIdx.x + wg;
+    if (t < tiles) load_curve(t);
+    for (; t < tiles; t += stride) {
+        const int y = t / tiles_x, x0 = (t % tiles_x) * kM;
+        // ---- A1: padding chunks 0 and 17, codes of inputs 0..127 in chunks 1..16
+        *reinterpret_cast<uint4*>(X + m * 16) = make_uint4(0, 0, 0, 0);
+        *reinterpret_cast<uint4*>(X + 17 * kChunkBytes + m * 16) = make_uint4(0, 0, 0, 0);
+#pragma unroll
+        for (int c = 0; c < 16; ++c)
+            *reinterpret_cast<uint4*>(X + (1 + c) * kChunkBytes + m * 16) =
+                make_uint4(codes_f16x2(cw[2 * c], 0x4140), codes_f16x2(cw[2 * c], 0x4342),
+                           codes_f16x2(cw[2 * c + 1], 0x4140), codes_f16x2(cw[2 * c + 1], 0x4342));
+        {
+            float bv[32];
+#pragma unroll
+            for (int c = 0; c < 32; ++c) bv[c] = bias[c];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) st32(tl + q * 32, bv);
+        }
+        wait_st();
+        dev::fence_proxy_async();
+        fence_before();
+        wg_sync(bar_id);
+        // ---- conv1 + sum-pool: position p = 4q + k accumulates into columns q * 32
+        if (issuer) {
+            fence_after();
+            for (int p = 0; p < 32; ++p) {
+                const bool odd = p & 1;
+                const int chunk = odd ? (p + 1) / 2 : p / 2;
+                mma(tm + (p >> 2) * 32, sdesc(sX + chunk * kChunkBytes, kChunkBytes),
+                    sdesc(sW + (odd ? kB1o : kB1e), 512), kIdC1);
+            }
+            commit_to(0);
+        }
+        if (t + stride < tiles) load_curve(t + stride);  // next tile, behind the MMAs
+        if (wg_sync_or(bar_id, !wait_bar(0))) { failed = true; break; }
+        fence_after();
+        // ---- conv1 epilogue -> A2
+#pragma unroll 1
+        for (int q = 0; q < 8; ++q) {
+            float v[32];
+            ld32(tl + q * 32, v);
+            store_bf16_row(Y + q * 4 * kChunkBytes, m, v);
+        }
+        {
+            float bv[32];
+#pragma unroll
+            for (int c = 0; c < 32; ++c) bv[c] = bias[32 + c];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) st32(tl + kColC2 + r * 32, bv);
+        }
+        wait_st();
+        dev::fence_proxy_async();
+        fence_before();
+        wg_sync(bar_id);
+        // ---- conv2: position r, taps j with input q = 2r + j - 2 in 0..7
+        if (issuer) {
+            fence_after();
+            for (int r = 0; r < 4; ++r)
+                for (int j = 0; j < 5; ++j) {
+                    const int q = 2 * r + j - 2;
+                    if (q < 0 || q >= 8) continue;
+#pragma unroll
+                    for (int h2 = 0; h2 < 2; ++h2)
+                        mma(tm + kColC2 + r * 32, sdesc(sY + (q * 4 + 2 * h2) * kChunkBytes, kChunkBytes),
+                            sdesc(sW + kB2 + (j * 4 + 2 * h2) * 512, 512), kIdC2);
+                }
+            commit_to(1);
+        }
+        if (wg_sync_or(bar_id, !wait_bar(1))) { failed = true; break; }
+        fence_after();
+        // ---- conv2 epilogue -> A3 (region X)
+#pragma unroll 1
+        for (int r = 0; r < 4; ++r) {
+            float v[32];
+            ld32(tl + kColC2 + r * 32, v);
+            store_bf16_row(X + r * 4 * kChunkBytes, m, v);
+        }
+        {
+            float bv[32];
+#pragma unroll
+            for (int c = 0; c < 32; ++c) bv[c] = bias[64 + c];
+            st32(tl + kColC3, bv);
+        }
+        wait_st();
+        dev::fence_proxy_async();
+        fence_before();
+        wg_sync(bar_id);
+        // ---- conv3: taps 1..4 on positions 0..3 (tap 0 meets the padding)
+        if (issuer) {
+            fence_after();
+            for (int j = 1; j < 5; ++j)
+#pragma unroll
+                for (int h2 = 0; h2 < 2; ++h2)
+                    mma(tm + kColC3, sdesc(sX + ((j - 1) * 4 + 2 * h2) * kChunkBytes, kChunkBytes),
+                        sdesc(sW + kB3 + (j * 4 + 2 * h2) * 512, 512), kIdC2);
+            commit_to(0);
+        }
+        if (wg_sync_or(bar_id, !wait_bar(0))) { failed = true; break; }
+        fence_after();
+        {
+            float v[32];
+            ld32(tl + kColC3, v);
+            store_bf16_row(Y, m, v);  // A4 (region Y)
+            float bv[32];
+#pragma unroll
+            for (int c = 0; c < 32; ++c) bv[c] = bias[96 + c];
+            st32(tl + kColF1, bv);
+#pragma unroll
+            for (int c = 0; c < 32; ++c) bv[c] = bias[128 + c];
+            st32(tl + kColF1 + 32, bv);
+        }
+        wait_st();
+        dev::fence_proxy_async();
+        fence_before();
+        wg_sync(bar_id);
+        // ---- fc1: K = 32 (2 MMAs), N = 64
+        if (issuer) {
+            fence_after();
+#pragma unroll
+            for (int h2 = 0; h2 < 2; ++h2)
+                mma(tm + kColF1, sdesc(sY + 2 * h2 * kChunkBytes, kChunkBytes),
+                    sdesc(sW + kB4 + 2 * h2 * 1024, 1024), kIdF1);
+            commit_to(1);
+        }
+        if (wg_sync_or(bar_id, !wait_bar(1))) { failed = true; break; }
+        fence_after();
+        // ---- fc1 epilogue + fc2
+        {
+            float v0[32], v1[32];
+            ld32(tl + kColF1, v0);
+            ld32(tl + kColF1 + 32, v1);
+            float z0 = b5, z1 = 0.f;
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                z0 = fmaf(w5[c], fmaxf(v0[c], 0.f), z0);
+                z1 = fmaf(w5[32 + c], fmaxf(v1[c], 0.f), z1);
+            }
+            if (x0 + m < a.W)
+                reinterpret_cast<float*>(reinterpret_cast<char*>(a.score) + (size_t)y * a.score_pitch)[x0 + m] =
+                    1.f / (1.f + __expf(-(z0 + z1)));
+        }
+        fence_before();  // this tile's TMEM reads before the next tile's MMAs
+    }
+    // After a timeout, MMAs may still be in flight: wait (bounded) for every
+    // commit not yet waited for before giving the TMEM back.
+    if (failed && issuer) {
+        dev::report(a.status, CT_ETIMEOUT);
+        for (int b = 0; b < 2; ++b)
+            for (uint32_t k = ph[b]; k < cm[b]; ++k) dev::mbar_wait_bounded(&bars[b], k & 1);
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tslot), "r"(kTmemCols)
+                     : "memory");
+}
+
+}  // namespace inf
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+uint16_t f32_to_bf16_bits(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7FFFFFFFu) > 0x7F800000u) return uint16_t((u >> 16) | 0x40);  // NaN
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return uint16_t(u >> 16);
+}
+float bf16_bits_to_f32(uint16_t b) {
+    const uint32_t u = uint32_t(b) << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+// Exact conversion of a bf16 value to f16 bits; returns false if the value
+// is not representable in f16 (outside its range or below its precision).
+bool bf16_to_f16_exact(float v, uint16_t* out) {
+    const __half h = __float2half_rn(v);
+    *out = __half_as_ushort(h);
+    return __half2float(h) == v;
+}
+
+struct ConfNetHandle : ct_handle {
+    ConfNetHandle() : ct_handle(Kind::ConfNet) {}
+    ~ConfNetHandle() override {
+        if (device >= 0) cudaSetDevice(device);
+        cudaFree(arena);
+    }
+    int max_batch = 0;
+    unsigned char* arena = nullptr;
+    float *master = nullptr, *m = nullptr, *v = nullptr, *wq = nullptr, *grad = nullptr, *part = nullptr;
+    float* loss_out = nullptr;
+    unsigned char* wimg = nullptr;  // packed inference weights
+    Act act{};
+    int steps = 0;
+    bool wimg_dirty = true;
+    int sms = 148;
+};
+
+ConfNetHandle* as_net(ct_handle* h) {
+    return (h && h->kind == Kind::ConfNet) ? static_cast<ConfNetHandle*>(h) : nullptr;
+}
+
+int chunks_for(int n) { return (n + kChunk - 1) / kChunk; }
+
+// forward (+ backward when labels are given) of n samples on stream s
+int run_train_graph(ConfNetHandle* h, const uint8_t* x, const uint8_t* labels, int n, float* scores,
+                    cudaStream_t s) {
+    const Act& A = h->act;
+    const dim3 b32(32, kSY), b64(64, 8);
+    const int g32 = (n + kSY - 1) / kSY, g64 = (n + 7) / 8;
+    fwd1_kernel<<<g32, b32, 0, s>>>(x, h->wq, A, n);
+    fwd2_kernel<<<g32, b32, 0, s>>>(h->wq, A, n);
+    fwd3_kernel<<<g32, b32, 0, s>>>(h->wq, A, n);
+    fwd4_kernel<<<g64, b64, 0, s>>>(h->wq, A, n);
+    head_kernel<<<(n + 255) / 256, 256, 0, s>>>(h->wq, A, labels, 1.f / float(n), scores, n);
+    CT_LAUNCH_CHECK();
+    if (!labels) return CT_OK;
+    bwd4_kernel<<<g64, b64, 0, s>>>(h->wq, A, n);
+    bwd3_kernel<<<g32, b32, 0, s>>>(h->wq, A, n);
+    bwd2_kernel<<<g32, b32, 0, s>>>(h->wq, A, n);
+    bwd1_kernel<<<g32, b32, 0, s>>>(h->wq, A, n);
+    wgrad_kernel<<<dim3(chunks_for(n), 5), 256, 0, s>>>(x, A, n, h->part);
+    CT_LAUNCH_CHECK();
+    return CT_OK;
+}
+
+// Packs master weights into the inference image (host side).
+int pack_weights(ConfNetHandle* h) {
+    using namespace inf;
+    std::vector<float> p(kParams);
+    CT_CUDA_TRY(cudaMemcpy(p.data(), h->master, sizeof(float) * kParams, cudaMemcpyDeviceToHost));
+    std::vector<unsigned char> img(kWBytes, 0);
+    auto put16 = [&](int off, uint16_t v) { std::memcpy(&img[off], &v, 2); };
+    auto bf = [&](int idx) { return bf16_bits_to_f32(f32_to_bf16_bits(p[idx])); };
+    // B1e / B1o: rows = channel, K = window offset of tap j: j + 6 (even
+    // positions) / j + 2 (odd positions); 2 chunks of 32 rows each
+    for (int odd = 0; odd < 2; ++odd)
+        for (int ch = 0; ch < 32; ++ch)
+            for (int j = 0; j < 5; ++j) {
+                const int k = j + (odd ? 2 : 6);
+                uint16_t hb;
+                if (!bf16_to_f16_exact(bf(kOffW1 + ch * 5 + j), &hb))
+                    return fail(CT_EINVAL, "conv1 weight %d (%g) is not exact in f16", ch * 5 + j,
+                                double(bf(kOffW1 + ch * 5 + j)));
+                put16((odd ? kB1o : kB1e) + (k / 8) * 32 * 16 + ch * 16 + (k % 8) * 2, hb);
+            }
+    // B2 / B3: rows o, K = tap * 32 + in
+    for (int layer = 0; layer < 2; ++layer) {
+        const int base = layer == 0 ? kB2 : kB3, off = layer == 0 ? kOffW2 : kOffW3;
+        for (int o = 0; o < 32; ++o)
+            for (int i = 0; i < 32; ++i)
+                for (int j = 0; j < 5; ++j) {
+                    const int k = j * 32 + i;
+                    put16(base + (k / 8) * 32 * 16 + o * 16 + (k % 8) * 2, f32_to_bf16_bits(p[off + o * 160 + i * 5 + j]));
+                }
+    }
+    // B4: rows h, K = in
+    for (int hh = 0; hh < 64; ++hh)
+        for (int i = 0; i < 32; ++i)
+            put16(kB4 + (i / 8) * 64 * 16 + hh * 16 + (i % 8) * 2, f32_to_bf16_bits(p[kOffW4 + hh * 32 + i]));
+    float* bias = reinterpret_cast<float*>(&img[kBias]);
+    for (int k = 0; k < 32; ++k) bias[k] = p[kOffB1 + k];
+    for (int k = 0; k < 32; ++k) bias[32 + k] = p[kOffB2 + k];
+    for (int k = 0; k < 32; ++k) bias[64 + k] = p[kOffB3 + k];
+    for (int k = 0; k < 64; ++k) bias[96 + k] = p[kOffB4 + k];
+    for (int k = 0; k < 64; ++k) bias[160 + k] = bf(kOffW5 + k);
+    bias[224] = p[kOffB5];
+    CT_CUDA_TRY(cudaMemcpy(h->wimg, img.data(), kWBytes, cudaMemcpyHostToDevice));
+    h->wimg_dirty = false;
+    return CT_OK;
+}
+
+int upload_params(ConfNetHandle* h, const float* host) {
+    std::vector<float> q(host, host + kParams);
+    for (int p = 0; p < kParams; ++p)
+        if (is_weight(p)) q[p] = bf16_bits_to_f32(f32_to_bf16_bits(q[p]));
+    CT_CUDA_TRY(cudaMemcpy(h->master, host, sizeof(float) * kParams, cudaMemcpyHostToDevice));
+    CT_CUDA_TRY(cudaMemcpy(h->wq, q.data(), sizeof(float) * kParams, cudaMemcpyHostToDevice));
+    CT_CUDA_TRY(cudaMemset(h->m, 0, sizeof(float) * kParams));
+    CT_CUDA_TRY(cudaMemset(h->v, 0, sizeof(float) * kParams));
+    h->steps = 0;
+    h->wimg_dirty = true;
+    return CT_OK;
+}
+
+}  // namespace cn
+}  // namespace ct
+
+using namespace ct;
+using namespace ct::cn;
+
+extern "C" {
+
+int ct_confnet_create(ct_handle** out) {
+    clear_error();
+    if (!out) return fail(CT_EINVAL, "null output handle pointer");
+    *out = new ConfNetHandle();
+    return CT_OK;
+}
+
+int ct_confnet_configure(ct_handle* hh, int32_t device, int32_t max_batch) {
+    clear_error();
+    auto* h = as_net(hh);
+    if (!h) return fail(CT_ESTATE, "not a confidence-net handle");
+    if (max_batch < 1 || max_batch > (1 << 22)) return fail(CT_EINVAL, "max_batch must be 1..4194304");
+    if (int rc = use_device(device)) return rc;
+    h->device = device;
+    if (int rc = h->init_status()) return rc;
+    CT_CUDA_TRY(cudaFuncSetAttribute(inf::infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, inf::kSmem));
+    h->sms = sm_count(device);
+    const size_t n = size_t(max_batch);
+    size_t bytes = 0;
+    auto take = [&](size_t b) { const size_t o = bytes; bytes += (b + 255) / 256 * 256; return o; };
+    const size_t o_master = take(4 * kParams), o_m = take(4 * kParams), o_v = take(4 * kParams),
+                 o_wq = take(4 * kParams), o_grad = take(4 * kParams),
+                 o_part = take(4 * size_t(kParams) * chunks_for(max_batch)), o_loss = take(16),
+                 o_wimg = take(inf::kWBytes), o_a1 = take(4 * 256 * n), o_a2 = take(4 * 128 * n),
+                 o_a3 = take(4 * 32 * n), o_a4 = take(4 * 64 * n), o_logit = take(4 * n), o_dl = take(4 * n),
+                 o_ls = take(4 * n), o_dz4 = take(4 * 64 * n), o_dz3 = take(4 * 32 * n), o_dz2 = take(4 * 128 * n),
+                 o_dm1 = take(4 * 256 * n);
+    cudaFree(h->arena);
+    h->arena = nullptr;
+    if (cudaMalloc(&h->arena, bytes) != cudaSuccess) return fail(CT_ENOMEM, "confidence-net scratch (%zu bytes)", bytes);
+    CT_CUDA_TRY(cudaMemset(h->arena, 0, bytes));
+    unsigned char* A = h->arena;
+    h->master = reinterpret_cast<float*>(A + o_master);
+    h->m = reinterpret_cast<float*>(A + o_m);
+    h->v = reinterpret_cast<float*>(A + o_v);
+    h->wq = reinterpret_cast<float*>(A + o_wq);
+    h->grad = reinterpret_cast<float*>(A + o_grad);
+    h->part = reinterpret_cast<float*>(A + o_part);
+    h->loss_out = reinterpret_cast<float*>(A + o_loss);
+    h->wimg = A + o_wimg;
+    h->act.a1 = reinterpret_cast<float*>(A + o_a1);
+    h->act.a2 = reinterpret_cast<float*>(A + o_a2);
+    h->act.a3 = reinterpret_cast<float*>(A + o_a3);
+    h->act.a4 = reinterpret_cast<float*>(A + o_a4);
+    h->act.logit = reinterpret_cast<float*>(A + o_logit);
+    h->act.dl = reinterpret_cast<float*>(A + o_dl);
+    h->act.loss = reinterpret_cast<float*>(A + o_ls);
+    h->act.dz4 = reinterpret_cast<float*>(A + o_dz4);
+    h->act.dz3 = reinterpret_cast<float*>(A + o_dz3);
+    h->act.dz2 = reinterpret_cast<float*>(A + o_dz2);
+    h->act.dm1 = reinterpret_cast<float*>(A + o_dm1);
+    h->max_batch = max_batch;
+    h->configured = true;
+    return ct_confnet_init(hh, 1);
+}
+
+int ct_confnet_init(ct_handle* hh, uint64_t seed) {
+    clear_error();
+    auto* h = as_net(hh);
+    if (!h || !h->configured) return fail(CT_ESTATE, "not a configured confidence-net handle");
+    if (int rc = use_device(h->device)) return rc;
+    // SplitMix64 + Box-Muller, He-style scales (conv1 scaled for inputs 0..255)
+    uint64_t st = seed * 0x9E3779B97F4A7C15ull + 0x2545F4914F6CDD1Dull;
+    auto u01 = [&]() {
+        st += 0x9E3779B97F4A7C15ull;
+        uint64_t z = st;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return (double(z >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+    };
+    auto normal = [&]() { return std::sqrt(-2.0 * std::log(u01())) * std::cos(6.283185307179586 * u01()); };
+    std::vector<float> p(kParams, 0.f);
+    auto fill = [&](int off, int count, double sd) {
+        for (int k = 0; k < count; ++k) p[off + k] = float(sd * normal());
+    };
+    fill(kOffW1, 160, 1.0 / (std::sqrt(5.0) * 128.0));
+    fill(kOffW2, 5120, std::sqrt(2.0 / 160));
+    fill(kOffW3, 5120, std::sqrt(2.0 / 128));
+    fill(kOffW4, 2048, std::sqrt(2.0 / 32));
+    fill(kOffW5, 64, std::sqrt(1.0 / 64));
+    return upload_params(h, p.data());
+}
+
+int ct_confnet_set_params(ct_handle* hh, const float* params, int32_t n) {
+    clear_error();
+    auto* h = as_net(hh);
+    if (!h || !h->configured) return fail(CT_ESTATE, "not a configured confidence-net handle");
+    if (!params || n != kParams) return fail(CT_EINVAL, "need %d parameters", kParams);
+    if (int rc = use_device(h->device)) return rc;
+    return upload_params(h, params);
+}
+
+int ct_confnet_get_params(ct_handle* hh, float* params, int32_t n) {
+    clear_error();
+    auto* h = as_net(hh);
+    if (!h || !h->configured) return fail(CT_ESTATE, "not a configured confidence-net handle");
+    if (!params || n != kParams) return fail(CT_EINVAL, "need %d parameters", kParams);
+    if (int rc = use_device(h->device)) return rc;
+    CT_CUDA_TRY(cudaDeviceSynchronize());
+    CT_CUDA_TRY(cudaMemcpy(params, h->master, sizeof(float) * kParams, cudaMemcpyDeviceToHost));
+    return CT_OK;
+}
+
+int ct_confnet_gather(ct_handle* hh, uint8_t* samples, const ct_curves* curves, const int32_t* xy, int32_t n,
+                      ct_stream stream) {
+    clear_error();
+    auto* h = as_net(hh);
+    if (!h || !h->configured) return fail(CT_ESTATE, "not a configured confidence-net handle");
+    if (!samples || !curves || !curves->ptr || !xy || n < 0) return fail(CT_EINVAL, "null argument");
+    if (curves->disp_count != kLen) return fail(CT_EFORMAT, "the confidence net reads curves of 128 disparities");
+    if (n == 0) return CT_OK;
+    if (int rc = use_device(h->device)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    h->last_stream = s;
+    gather_kernel<<<(n + 7) / 8, 256, 0, s>>>(samples, static_cast<const uint32_t*>(curves->ptr),
+                                              curves->pitch_bytes / 4, kLen / 4, curves->width, curves->height, xy,
+                                              n, h->d_status);
+    CT_LAUNCH_CHECK();
+    return CT_OK;
+}
+
+int ct_confnet_loss_grad(ct_handle* hh, const uint8_t* samples, const uint8_t* labels, int32_t n, float* grad,
+                         float* loss, ct_stream stream) {
+    clear_error();
+    auto* h = as_net(hh);
+    if (!h || !h->configured) return fail(CT_ESTATE, "not a configured confidence-net handle");
+    if (!samples || !labels || n < 1 || n > h->max_batch) return fail(CT_EINVAL, "bad samples/labels or n");
+    if (int rc = use_device(h->device)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    h->last_stream = s;
+    if (int rc = run_train_graph(h, samples, labels, n, nullptr, s)) return rc;
+    reduce_adam_kernel<<<(kParams + 255) / 256, 256, 0, s>>>(h->part, chunks_for(n), grad ? grad : h->grad, h->master,
+                                                            h->m, h->v, h->wq, AdamArgs{0, 0, 0, 0, 0, 1, 1});
+    if (loss) loss_mean_kernel<<<1, 256, 0, s>>>(h->act.loss, n, loss);
+    CT_LAUNCH_CHECK();
+    return CT_OK;
+}
+
+int ct_confnet_train_step(ct_handle* hh, const uint8_t* samples, const uint8_t* labels, int32_t n, float lr,
+                          float* loss, ct_stream stream) {
+    clear_error();
+    auto* h = as_net(hh);
+    if (!h || !h->configured) return fail(CT_ESTATE, "not a configured confidence-net handle");
+    if (!samples || !labels || n < 1 || n > h->max_batch) return fail(CT_EINVAL, "bad samples/labels or n");
+    if (!(lr > 0.f)) return fail(CT_EINVAL, "lr must be > 0");
+    if (int rc = use_device(h->device)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    h->last_stream = s;
+    if (int rc = run_train_graph(h, samples, labels, n, nullptr, s)) return rc;
+    ++h->steps;
+    const float b1 = 0.9f, b2 = 0.999f;
+    AdamArgs aa{1, lr, b1, b2, 1e-8f, float(1.0 - std::pow(double(b1), h->steps)),
+                float(1.0 - std::pow(double(b2), h->steps))};
+    reduce_adam_kernel<<<(kParams + 255) / 256, 256, 0, s>>>(h->part, chunks_for(n), h->grad, h->master, h->m, h->v,
+                                                            h->wq, aa);
+    if (loss) loss_mean_kernel<<<1, 256, 0, s>>>(h->act.loss, n, loss);
+    CT_LAUNCH_CHECK();
+    h->wimg_dirty = true;
+    return CT_OK;
+}
+
+int ct_confnet_scores(ct_handle* hh, float* scores, const uint8_t* samples, int32_t n, ct_stream stream) {
+    clear_error();
+    auto* h = as_net(hh);
+    if (!h || !h->configured) return fail(CT_ESTATE, "not a configured confidence-net handle");
+    if (!scores || !samples || n < 1 || n > h->max_batch) return fail(CT_EINVAL, "bad arguments");
+    if (int rc = use_device(h->device)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    h->last_stream = s;
+    return run_train_graph(h, samples, nullptr, n, scores, s);
+}
+
+int ct_confnet_infer(ct_handle* hh, const ct_image* score, const ct_curves* curves, ct_stream stream) {
+    clear_error();
+    auto* h = as_net(hh);
+    if (!h || !h->configured) return fail(CT_ESTATE, "not a configured confidence-net handle");
+    if (int rc = check_image(score, "score", 1u << CT_PIX_F32)) return rc;
+    if (!curves || !curves->ptr) return fail(CT_EINVAL, "null curve volume");
+    if (curves->disp_count != kLen) return fail(CT_EFORMAT, "the confidence net reads curves of 128 disparities");
+    if (curves->width != score->width || curves->height != score->height)
+        return fail(CT_EFORMAT, "score map and curve volume differ in size");
+    if (reinterpret_cast<uintptr_t>(curves->ptr) % 16 || curves->pitch_bytes % 16 ||
+        curves->pitch_bytes < 4 * (size_t(curves->width) + 2))
+        return fail(CT_EINVAL, "curve volume needs a 16-byte aligned pointer and pitch >= 4 * (width + 2)");
+    if (int rc = use_device(h->device)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (h->wimg_dirty) {
+        if (h->last_stream) CT_CUDA_TRY(cudaStreamSynchronize(h->last_stream));
+        if (int rc = pack_weights(h)) return rc;
+    }
+    h->last_stream = s;
+    inf::InferArgs a{};
+    a.curve = static_cast<const uint32_t*>(curves->ptr);
+    a.curve_pitch = curves->pitch_bytes / 4;
+    a.groups = kLen / 4;
+    a.W = score->width;
+    a.H = score->height;
+    a.score = static_cast<float*>(score->ptr);
+    a.score_pitch = score->pitch_bytes;
+    a.wimg = reinterpret_cast<const uint4*>(h->wimg);
+    a.status = h->d_status;
+    const int tiles = ((a.W + inf::kM - 1) / inf::kM) * a.H;
+    const int grid = (tiles + 1) / 2 < h->sms ? (tiles + 1) / 2 : h->sms;  // 2 tile streams per CTA
+    inf::infer_kernel<<<grid, inf::kNT, inf::kSmem, s>>>(a);
+    CT_LAUNCH_CHECK();
+    return CT_OK;
+}
+
+}  // extern "C"

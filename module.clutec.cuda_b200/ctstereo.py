@@ -88,6 +88,14 @@ class ct_batch_item(C.Structure):
     _fields_ = [("left", ct_image), ("right", ct_image), ("disp", ct_image)]
 
 
+class ct_curves(C.Structure):
+    _fields_ = [("ptr", C.c_void_p), ("pitch_bytes", C.c_size_t), ("width", C.c_int32), ("height", C.c_int32),
+                ("disp_count", C.c_int32), ("reserved", C.c_int32)]
+
+
+CT_CONFNET_PARAMS = 12673
+
+
 class ct_pipe_rates(C.Structure):
     _fields_ = [("popc_per_clk_sm", C.c_double), ("iadd3_per_clk_sm", C.c_double),
                 ("lop3_per_clk_sm", C.c_double), ("vimnmx_per_clk_sm", C.c_double),
@@ -131,6 +139,18 @@ def _declare(L: C.CDLL) -> None:
         "ct_bm_census_tuning": [H, P(C.c_int32), P(C.c_int32)],
         "ct_bm_census_set_tuning": [H, C.c_int32, C.c_int32],
         "ct_bm_census_process_static": [img, img, img, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p],
+        "ct_curves_pitch": [C.c_int32, P(C.c_size_t)],
+        "ct_bm_census_process_curves": [H, img, P(ct_curves), img, img, C.c_void_p],
+        "ct_confnet_create": [P(H)],
+        "ct_confnet_configure": [H, C.c_int32, C.c_int32],
+        "ct_confnet_init": [H, C.c_uint64],
+        "ct_confnet_set_params": [H, C.c_void_p, C.c_int32],
+        "ct_confnet_get_params": [H, C.c_void_p, C.c_int32],
+        "ct_confnet_gather": [H, C.c_void_p, P(ct_curves), C.c_void_p, C.c_int32, C.c_void_p],
+        "ct_confnet_loss_grad": [H, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p],
+        "ct_confnet_train_step": [H, C.c_void_p, C.c_void_p, C.c_int32, C.c_float, C.c_void_p, C.c_void_p],
+        "ct_confnet_scores": [H, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p],
+        "ct_confnet_infer": [H, img, P(ct_curves), C.c_void_p],
         "ct_bm_sad_create": [P(H)],
         "ct_bm_sad_configure": [H, C.c_int32, fmt, P(ct_sad_params)],
         "ct_bm_sad_process": [H, img, img, img, C.c_void_p],
@@ -294,6 +314,36 @@ class BlockMatcherCensus(_Driver):
                                             _img_ref(disp_checked), tol, _img_ref(left), _img_ref(right),
                                             _stream(stream)))
 
+    def process_curves(self, disp, curves, left, right, stream=None):
+        """process() that also writes the cost-curve volume (see CurveVolume)."""
+        check(lib().ct_bm_census_process_curves(self._h, _img_ref(disp), C.byref(curves.desc()), _img_ref(left),
+                                                _img_ref(right), _stream(stream)))
+
+
+class CurveVolume:
+    """Device cost-curve volume (ct_curves): rows (y, g) of 32-bit words, word
+    x + 2 of row (y, g) = codes of disparities 4g .. 4g + 3 at column x."""
+
+    def __init__(self, width: int, height: int, disp_count: int, device="cuda"):
+        import torch
+        pitch = C.c_size_t()
+        check(lib().ct_curves_pitch(width, C.byref(pitch)))
+        self.width, self.height, self.disp_count = width, height, disp_count
+        self.groups = (disp_count + 3) // 4
+        self.pitch_words = pitch.value // 4
+        self.words = torch.full((height * self.groups, self.pitch_words), -1, dtype=torch.int32, device=device)
+
+    def desc(self) -> ct_curves:
+        return ct_curves(self.words.data_ptr(), self.pitch_words * 4, self.width, self.height, self.disp_count, 0)
+
+    def to_hwd(self):
+        """(H, W, D) uint8 numpy array of the codes."""
+        import numpy as np
+        w = self.words.cpu().numpy().view(np.uint32).reshape(self.height, self.groups, self.pitch_words)
+        b = w[:, :, 2:2 + self.width].view(np.uint8).reshape(self.height, self.groups, self.width, 4)
+        return np.ascontiguousarray(b.transpose(0, 2, 1, 3).reshape(self.height, self.width, 4 * self.groups)
+                                    [:, :, :self.disp_count])
+
 
 class BlockMatcherSAD1(_Driver):
     """BlockMatcherSAD1::CDriver, exhaustive (2r+1)^2 SAD + WTA."""
@@ -394,6 +444,49 @@ class BatchStereo(_Driver):
 
     def graph_launch(self, stream=None):
         check(lib().ct_batch_graph_launch(self._h, _stream(stream)))
+
+
+class ConfNet(_Driver):
+    """Learned confidence net over census cost curves (ct_confnet_*)."""
+    _create = "ct_confnet_create"
+
+    def configure(self, device: int, max_batch: int):
+        check(lib().ct_confnet_configure(self._h, device, max_batch))
+
+    def init(self, seed: int):
+        check(lib().ct_confnet_init(self._h, seed))
+
+    def set_params(self, params):
+        import numpy as np
+        p = np.ascontiguousarray(params, np.float32)
+        check(lib().ct_confnet_set_params(self._h, p.ctypes.data, p.size))
+
+    def get_params(self):
+        import numpy as np
+        p = np.empty(CT_CONFNET_PARAMS, np.float32)
+        check(lib().ct_confnet_get_params(self._h, p.ctypes.data, p.size))
+        return p
+
+    def gather(self, samples, curves: "CurveVolume", xy, stream=None):
+        """samples: (n, 128) uint8 CUDA tensor; xy: (n, 2) int32 CUDA tensor."""
+        check(lib().ct_confnet_gather(self._h, samples.data_ptr(), C.byref(curves.desc()), xy.data_ptr(),
+                                      xy.shape[0], _stream(stream)))
+
+    def loss_grad(self, samples, labels, grad=None, loss=None, stream=None):
+        check(lib().ct_confnet_loss_grad(self._h, samples.data_ptr(), labels.data_ptr(), samples.shape[0],
+                                         None if grad is None else grad.data_ptr(),
+                                         None if loss is None else loss.data_ptr(), _stream(stream)))
+
+    def train_step(self, samples, labels, lr: float, loss=None, stream=None):
+        check(lib().ct_confnet_train_step(self._h, samples.data_ptr(), labels.data_ptr(), samples.shape[0], lr,
+                                          None if loss is None else loss.data_ptr(), _stream(stream)))
+
+    def scores(self, out, samples, stream=None):
+        check(lib().ct_confnet_scores(self._h, out.data_ptr(), samples.data_ptr(), samples.shape[0],
+                                      _stream(stream)))
+
+    def infer(self, score, curves: "CurveVolume", stream=None):
+        check(lib().ct_confnet_infer(self._h, _img_ref(score), C.byref(curves.desc()), _stream(stream)))
 
 
 def census_match_static(disp, left, right, disp_count: int, left_to_right: bool = True, device_status=None,
