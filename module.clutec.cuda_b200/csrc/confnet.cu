@@ -82,8 +82,8 @@ __global__ void gather_kernel(uint8_t* samples, const uint32_t* curve, size_t pi
 // Training kernels (block (32, 16): threadIdx.x = channel, threadIdx.y = sample)
 // ---------------------------------------------------------------------------
 struct Act {  // per-sample activations and gradient signals, [n][...]
-    float* a1;      // [8][32] bf16 values
-    float* a2;      // [4][32]
+    float* a1;      // [7][32] bf16 values
+    float* a2;      // [2][32]
     float* a3;      // [32]
     float* a4;      // [64]
     float* logit;   // [1]
@@ -91,12 +91,15 @@ struct Act {  // per-sample activations and gradient signals, [n][...]
     float* loss;    // per-sample loss
     float* dz4;     // [64]
     float* dz3;     // [32]
-    float* dz2;     // [4][32]
-    float* dm1;     // [8][32]
+    float* dz2;     // [2][32]
+    float* dm1;     // [7][32]
 };
+constexpr int kQ = 7;   // pooled conv1 positions
+constexpr int kR = 2;   // conv2 positions
 
 constexpr int kSY = 16;  // samples per CTA
 
+// conv1 (k=5, stride 5, pad 2) + sum over 4 positions + bias, ReLU, bf16
 __global__ void __launch_bounds__(32 * kSY) fwd1_kernel(const uint8_t* x, const float* wq, Act A, int n) {
     __shared__ float xs[kSY][kLen];
     const int o = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * kSY + sl;
@@ -108,67 +111,65 @@ __global__ void __launch_bounds__(32 * kSY) fwd1_kernel(const uint8_t* x, const 
     for (int j = 0; j < 5; ++j) w[j] = wq[kOffW1 + o * 5 + j];
     const float b = wq[kOffB1 + o];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < kQ; ++q) {
         float z = b;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int p = 4 * q + k;
-#pragma unroll
-            for (int j = 0; j < 5; ++j) {
-                const int i = 4 * p + j - 2;
-                if (i >= 0 && i < kLen) z = fmaf(w[j], xs[sl][i], z);
-            }
+        for (int t = 0; t < 20; ++t) {  // position 4q + t / 5, tap t % 5
+            const int i = 20 * q + t - 2;
+            if (i >= 0 && i < kLen) z = fmaf(w[t % 5], xs[sl][i], z);
         }
-        A.a1[(size_t)s * 256 + q * 32 + o] = bf16r(fmaxf(z, 0.f));
+        A.a1[(size_t)s * 224 + q * 32 + o] = bf16r(fmaxf(z, 0.f));
     }
 }
 
+// conv2 (k=5, stride 3, pad 1): 2 positions
 __global__ void __launch_bounds__(32 * kSY) fwd2_kernel(const float* wq, Act A, int n) {
     __shared__ float wt[32][5][32];  // [in][tap][out]
-    __shared__ float as[kSY][8][32];
+    __shared__ float as[kSY][kQ][32];
     const int o = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * kSY + sl;
     const int tid = sl * 32 + o;
     for (int k = tid; k < 5120; k += 32 * kSY) {
         const int oo = k / 160, i = (k / 5) % 32, j = k % 5;
         wt[i][j][oo] = wq[kOffW2 + k];
     }
-    for (int k = o; k < 256; k += 32) as[sl][k / 32][k % 32] = s < n ? A.a1[(size_t)s * 256 + k] : 0.f;
+    for (int k = o; k < 224; k += 32) as[sl][k / 32][k % 32] = s < n ? A.a1[(size_t)s * 224 + k] : 0.f;
     __syncthreads();
     if (s >= n) return;
-    float z[4];
+    float z[kR];
 #pragma unroll
-    for (int r = 0; r < 4; ++r) z[r] = wq[kOffB2 + o];
+    for (int r = 0; r < kR; ++r) z[r] = wq[kOffB2 + o];
     for (int i = 0; i < 32; ++i) {
 #pragma unroll
         for (int j = 0; j < 5; ++j) {
             const float w = wt[i][j][o];
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const int q = 2 * r + j - 2;
-                if (q >= 0 && q < 8) z[r] = fmaf(w, as[sl][q][i], z[r]);
+            for (int r = 0; r < kR; ++r) {
+                const int q = 3 * r + j - 1;
+                if (q >= 0 && q < kQ) z[r] = fmaf(w, as[sl][q][i], z[r]);
             }
         }
     }
 #pragma unroll
-    for (int r = 0; r < 4; ++r) A.a2[(size_t)s * 128 + r * 32 + o] = bf16r(fmaxf(z[r], 0.f));
+    for (int r = 0; r < kR; ++r) A.a2[(size_t)s * 64 + r * 32 + o] = bf16r(fmaxf(z[r], 0.f));
 }
 
+// conv3 (k=5, pad 2, one output): taps 2, 3 on positions 0, 1
 __global__ void __launch_bounds__(32 * kSY) fwd3_kernel(const float* wq, Act A, int n) {
-    __shared__ float wt[32][5][32];
-    __shared__ float as[kSY][4][32];
+    __shared__ float wt[32][2][32];  // [in][tap - 2][out]
+    __shared__ float as[kSY][kR][32];
     const int o = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * kSY + sl;
     const int tid = sl * 32 + o;
-    for (int k = tid; k < 5120; k += 32 * kSY) {
-        const int oo = k / 160, i = (k / 5) % 32, j = k % 5;
-        wt[i][j][oo] = wq[kOffW3 + k];
+    for (int k = tid; k < 2048; k += 32 * kSY) {
+        const int oo = k / 64, i = (k / 2) % 32, j = k % 2;
+        wt[i][j][oo] = wq[kOffW3 + oo * 160 + i * 5 + 2 + j];
     }
-    for (int k = o; k < 128; k += 32) as[sl][k / 32][k % 32] = s < n ? A.a2[(size_t)s * 128 + k] : 0.f;
+    for (int k = o; k < 64; k += 32) as[sl][k / 32][k % 32] = s < n ? A.a2[(size_t)s * 64 + k] : 0.f;
     __syncthreads();
     if (s >= n) return;
     float z = wq[kOffB3 + o];
     for (int i = 0; i < 32; ++i) {
 #pragma unroll
-        for (int j = 1; j < 5; ++j) z = fmaf(wt[i][j][o], as[sl][j - 1][i], z);
+        for (int j = 0; j < 2; ++j) z = fmaf(wt[i][j][o], as[sl][j][i], z);
     }
     A.a3[(size_t)s * 32 + o] = bf16r(fmaxf(z, 0.f));
 }
@@ -225,50 +226,53 @@ __global__ void __launch_bounds__(32 * kSY) bwd3_kernel(const float* wq, Act A, 
     A.dz3[(size_t)s * 32 + o] = A.a3[(size_t)s * 32 + o] > 0.f ? g : 0.f;
 }
 
-// block (32, 16), thread = input channel i: dz2[pos][i] = sum_o dz3[o] w3[o][i][pos+1], masked
+// block (32, 16), thread = input channel i: dz2[pos][i] = sum_o dz3[o] w3[o][i][pos+2], masked
 __global__ void __launch_bounds__(32 * kSY) bwd2_kernel(const float* wq, Act A, int n) {
-    __shared__ float w3[32][32][6];  // [out][in][tap], padded
+    __shared__ float w3[32][32][3];  // [out][in][tap - 2], padded
     __shared__ float g3[kSY][32];
     const int i = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * kSY + sl;
-    for (int k = sl * 32 + i; k < 5120; k += 32 * kSY) w3[k / 160][(k / 5) % 32][k % 5] = wq[kOffW3 + k];
+    for (int k = sl * 32 + i; k < 2048; k += 32 * kSY) {
+        const int o = k / 64, ii = (k / 2) % 32, j = k % 2;
+        w3[o][ii][j] = wq[kOffW3 + o * 160 + ii * 5 + 2 + j];
+    }
     g3[sl][i] = s < n ? A.dz3[(size_t)s * 32 + i] : 0.f;
     __syncthreads();
     if (s >= n) return;
 #pragma unroll
-    for (int pos = 0; pos < 4; ++pos) {
+    for (int pos = 0; pos < kR; ++pos) {
         float g = 0.f;
-        for (int o = 0; o < 32; ++o) g = fmaf(g3[sl][o], w3[o][i][pos + 1], g);
-        const size_t k = (size_t)s * 128 + pos * 32 + i;
+        for (int o = 0; o < 32; ++o) g = fmaf(g3[sl][o], w3[o][i][pos], g);
+        const size_t k = (size_t)s * 64 + pos * 32 + i;
         A.dz2[k] = A.a2[k] > 0.f ? g : 0.f;
     }
 }
 
-// block (32, 16), thread = input channel i: dm1[q][i] = sum_{r,j: 2r+j-2=q} sum_o dz2[r][o] w2[o][i][j], masked
+// block (32, 16), thread = input channel i: dm1[q][i] = sum_{r,j: 3r+j-1=q} sum_o dz2[r][o] w2[o][i][j], masked
 __global__ void __launch_bounds__(32 * kSY) bwd1_kernel(const float* wq, Act A, int n) {
     __shared__ float w2[32][32][6];
-    __shared__ float g2[kSY][4][32];
+    __shared__ float g2[kSY][kR][32];
     const int i = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * kSY + sl;
     for (int k = sl * 32 + i; k < 5120; k += 32 * kSY) w2[k / 160][(k / 5) % 32][k % 5] = wq[kOffW2 + k];
-    for (int k = i; k < 128; k += 32) g2[sl][k / 32][k % 32] = s < n ? A.dz2[(size_t)s * 128 + k] : 0.f;
+    for (int k = i; k < 64; k += 32) g2[sl][k / 32][k % 32] = s < n ? A.dz2[(size_t)s * 64 + k] : 0.f;
     __syncthreads();
     if (s >= n) return;
-    float da[8];
+    float da[kQ];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) da[q] = 0.f;
+    for (int q = 0; q < kQ; ++q) da[q] = 0.f;
     for (int o = 0; o < 32; ++o) {
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
+        for (int r = 0; r < kR; ++r) {
             const float g = g2[sl][r][o];
 #pragma unroll
             for (int j = 0; j < 5; ++j) {
-                const int q = 2 * r + j - 2;
-                if (q >= 0 && q < 8) da[q] = fmaf(g, w2[o][i][j], da[q]);
+                const int q = 3 * r + j - 1;
+                if (q >= 0 && q < kQ) da[q] = fmaf(g, w2[o][i][j], da[q]);
             }
         }
     }
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const size_t k = (size_t)s * 256 + q * 32 + i;
+    for (int q = 0; q < kQ; ++q) {
+        const size_t k = (size_t)s * 224 + q * 32 + i;
         A.dm1[k] = A.a1[k] > 0.f ? da[q] : 0.f;
     }
 }
@@ -288,14 +292,14 @@ __global__ void __launch_bounds__(256) wgrad_kernel(const uint8_t* x, Act A, int
             const int o = bias ? t - 160 : t / 5, j = t % 5;
             float acc = 0.f;
             for (int s = s0; s < s1; ++s) {
-                for (int q = 0; q < 8; ++q) {
-                    const float g = A.dm1[(size_t)s * 256 + q * 32 + o];
+                for (int q = 0; q < kQ; ++q) {
+                    const float g = A.dm1[(size_t)s * 224 + q * 32 + o];
                     if (g == 0.f) continue;
                     if (bias) { acc += g; continue; }
                     float xsum = 0.f;  // inputs of tap j over the 4 pooled positions
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
-                        const int i = 4 * (4 * q + k) + j - 2;
+                        const int i = 20 * q + 5 * k + j - 2;
                         if (i >= 0 && i < kLen) xsum += float(x[(size_t)s * kLen + i]);
                     }
                     acc = fmaf(g, xsum, acc);
@@ -308,26 +312,26 @@ __global__ void __launch_bounds__(256) wgrad_kernel(const uint8_t* x, Act A, int
             float acc[4][5] = {};
             float bacc = 0.f;
             for (int s = s0; s < s1; ++s) {
-                const float* a1 = A.a1 + (size_t)s * 256;
-                const float* g2 = A.dz2 + (size_t)s * 128;
+                const float* a1 = A.a1 + (size_t)s * 224;
+                const float* g2 = A.dz2 + (size_t)s * 64;
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     const int pi = t + 256 * k, o = pi / 32, i = pi % 32;
-                    float g[4], av[8];
+                    float g[kR], av[kQ];
 #pragma unroll
-                    for (int r = 0; r < 4; ++r) g[r] = g2[r * 32 + o];
+                    for (int r = 0; r < kR; ++r) g[r] = g2[r * 32 + o];
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) av[q] = a1[q * 32 + i];
+                    for (int q = 0; q < kQ; ++q) av[q] = a1[q * 32 + i];
 #pragma unroll
                     for (int j = 0; j < 5; ++j)
 #pragma unroll
-                        for (int r = 0; r < 4; ++r) {
-                            const int q = 2 * r + j - 2;
-                            if (q >= 0 && q < 8) acc[k][j] = fmaf(g[r], av[q], acc[k][j]);
+                        for (int r = 0; r < kR; ++r) {
+                            const int q = 3 * r + j - 1;
+                            if (q >= 0 && q < kQ) acc[k][j] = fmaf(g[r], av[q], acc[k][j]);
                         }
                 }
                 if (t < 32)
-                    for (int r = 0; r < 4; ++r) bacc += g2[r * 32 + t];
+                    for (int r = 0; r < kR; ++r) bacc += g2[r * 32 + t];
             }
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
@@ -338,18 +342,18 @@ __global__ void __launch_bounds__(256) wgrad_kernel(const uint8_t* x, Act A, int
             if (t < 32) P[kOffB2 + t] = bacc;
             break;
         }
-        case 2: {  // w3: pairs (o, i); tap 0 always meets padding; b3 for t < 32
-            float acc[4][5] = {};
+        case 2: {  // w3: pairs (o, i); only taps 2, 3 meet data; b3 for t < 32
+            float acc[4][2] = {};
             float bacc = 0.f;
             for (int s = s0; s < s1; ++s) {
-                const float* a2 = A.a2 + (size_t)s * 128;
+                const float* a2 = A.a2 + (size_t)s * 64;
                 const float* g3 = A.dz3 + (size_t)s * 32;
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     const int pi = t + 256 * k, o = pi / 32, i = pi % 32;
                     const float g = g3[o];
 #pragma unroll
-                    for (int j = 1; j < 5; ++j) acc[k][j] = fmaf(g, a2[(j - 1) * 32 + i], acc[k][j]);
+                    for (int j = 0; j < 2; ++j) acc[k][j] = fmaf(g, a2[j * 32 + i], acc[k][j]);
                 }
                 if (t < 32) bacc += g3[t];
             }
@@ -357,7 +361,7 @@ __global__ void __launch_bounds__(256) wgrad_kernel(const uint8_t* x, Act A, int
             for (int k = 0; k < 4; ++k) {
                 const int pi = t + 256 * k, o = pi / 32, i = pi % 32;
 #pragma unroll
-                for (int j = 0; j < 5; ++j) P[kOffW3 + o * 160 + i * 5 + j] = acc[k][j];
+                for (int j = 0; j < 5; ++j) P[kOffW3 + o * 160 + i * 5 + j] = (j == 2 || j == 3) ? acc[k][j - 2] : 0.f;
             }
             if (t < 32) P[kOffB3 + t] = bacc;
             break;
@@ -433,44 +437,43 @@ __global__ void loss_mean_kernel(const float* loss, int n, float* out) {
 // ---------------------------------------------------------------------------
 namespace inf {
 
-constexpr int kNT = 256;  // 2 warpgroups; each runs its own stream of tiles
-constexpr int kM = 128;   // pixels per tile = TMEM lanes = MMA M
-constexpr int kChunkBytes = kM * 16;  // one K-chunk (8 elements) of a 128-row operand
+constexpr int kNT = 128;  // one warpgroup: thread = pixel of the tile = TMEM lane
+constexpr int kM = 128;   // pixels per tile = MMA M
+constexpr int kChunkBytes = kM * 16;  // one K-chunk (8 elements) of the 128-row A1 operand
 
-// Shared-memory image. Operands are K-major without swizzle, stored as
-// K-chunk panels: element (row r, k) at (k / 8) * rows * 16 + r * 16 +
-// (k % 8) * 2, so a descriptor's leading byte offset (next K-chunk) is
-// rows * 16 and its stride byte offset (next 8 rows) is 128.
-// Per warpgroup:
-//   region X: A1 = curve codes (f16), 18 chunks = inputs -8 .. 135; later A3
-//             = conv2 output a2[r][ch] (bf16), chunk r * 4 + ch / 8
-//   region Y: A2 = pooled conv1 output a1[q][ch] (bf16), chunk q * 4 + ch / 8;
-//             later A4 = conv3 output a3[ch], chunk ch / 8
-// (A3 is written after the conv1 MMAs that read A1 have completed, A4 after
-// the conv2 MMAs that read A2.)
-constexpr int kRegX = 18 * kChunkBytes;
-constexpr int kRegY = 32 * kChunkBytes;
-constexpr int kWG = kRegX + kRegY;
-constexpr int kWImg = 2 * kWG;
-// packed weight image (also the device buffer layout written by the host)
-constexpr int kB1e = 0;                   // conv1, even positions: N=32 x K=16 f16, taps at k = 6..10 (LBO 512)
-constexpr int kB1o = kB1e + 2 * 32 * 16;  // conv1, odd positions: taps at k = 2..6
-constexpr int kB2 = kB1o + 2 * 32 * 16;   // N=32 x K=160 bf16: chunks tap * 4 + in / 8 (LBO 512)
-constexpr int kB3 = kB2 + 20 * 32 * 16;
-constexpr int kB4 = kB3 + 20 * 32 * 16;   // N=64 x K=32 bf16: 4 chunks of 64 rows (LBO 1024)
-constexpr int kBias = kB4 + 4 * 64 * 16;  // fp32: b1[32] b2[32] b3[32] b4[64] w5[64] b5
+// Shared memory: A1 = the tile's curve codes as f16, K-major without
+// swizzle in K-chunk panels (element (pixel r, input i) at chunk (i + 8) / 8,
+// offset r * 16 + ((i + 8) % 8) * 2; 19 chunks = inputs -8 .. 143, zero
+// outside 0 .. 127), then the packed weights (B operands in the same panel
+// form with rows = output channels, and fp32 biases).
+constexpr int kA1Chunks = 19;
+constexpr int kA1 = 0;
+constexpr int kWImg = kA1Chunks * kChunkBytes;
+constexpr int kB1e = 0;                 // conv1, even groups: N=32 x K=32 f16, 20 taps at k = 6..25 (LBO 512)
+constexpr int kB1o = kB1e + 4 * 512;    // conv1, odd groups: taps at k = 2..21
+constexpr int kB2 = kB1o + 4 * 512;     // conv2: N=32 x K=160 bf16, chunk = tap * 4 + in / 8 (LBO 512)
+constexpr int kB3 = kB2 + 20 * 512;     // conv3 taps 2, 3: N=32 x K=64, chunk = (tap - 2) * 4 + in / 8
+constexpr int kB4 = kB3 + 8 * 512;      // fc1: N=64 x K=32 bf16 (LBO 1024)
+constexpr int kBias = kB4 + 4 * 1024;   // fp32: b1[32] b2[32] b3[32] b4[64] w5[64] b5
 constexpr int kWBytes = kBias + (32 + 32 + 32 + 64 + 64 + 4) * 4;
-constexpr int kBar = kWImg + kWBytes;     // 2 mbarriers per warpgroup
-constexpr int kTmemSlot = kBar + 4 * 8;
+constexpr int kBar = kWImg + kWBytes;   // 2 mbarriers
+constexpr int kTmemSlot = kBar + 2 * 8;
 constexpr int kSmem = kTmemSlot + 16;
 static_assert(kWBytes % 16 == 0, "weight image must be a whole number of 16-byte words");
-static_assert(kSmem <= 232448, "shared memory");
+static_assert(2 * kSmem <= 228 * 1024, "two CTAs per SM");
 
-// TMEM: 512 columns, 256 per warpgroup: conv1 accumulators (8 pooled
-// positions x 32) at 0..255; conv2 (4 x 32) at 0..127 once conv1's are read;
-// conv3 at 128..159; fc1 at 160..223.
-constexpr uint32_t kTmemCols = 512;
-constexpr uint32_t kColC2 = 0, kColC3 = 128, kColF1 = 160;
+// TMEM (256 columns per CTA, two CTAs per SM). Accumulators are fp32, one
+// column per output; A operands held in TMEM are bf16 pairs, a K=16 slice =
+// 8 columns. Regions are reused as soon as what they held has been read:
+//   C1 conv1 accumulators, group q at 32 q                     0 .. 223
+//   A2 pooled conv1 output (bf16), position q at 16 q         0 .. 111
+//   C2 conv2 accumulators, position r at 128 + 32 r          128 .. 191
+//   A3 conv2 output, position r at 192 + 16 r                192 .. 223
+//   C3 conv3 accumulators                                      0 .. 31
+//   A4 conv3 output                                           32 .. 47
+//   C4 fc1 accumulators                                       64 .. 127
+constexpr uint32_t kTmemCols = 256;
+constexpr uint32_t kC2 = 128, kA3 = 192, kC3 = 0, kA4 = 32, kC4 = 64;
 
 // Instruction descriptors (kind::f16): D fp32 (bit 4), A/B format at bits
 // 7 / 10 (0 = f16, 1 = bf16), both K-major, N >> 3 at bit 17, M >> 4 at 24.
@@ -487,11 +490,20 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo) {
            (uint64_t(1) << 46);
 }
 
-__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t id) {
+// D (TMEM) += A (shared memory) x B (shared memory)
+__device__ __forceinline__ void mma_ss(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t id) {
     asm volatile(
         "{\n.reg .pred p;\nsetp.ne.b32 p, 1, 0;\n"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
         "l"(a), "l"(b), "r"(id)
+        : "memory");
+}
+// D (TMEM) += A (TMEM, lane = row, K packed in pairs per column) x B (shared memory)
+__device__ __forceinline__ void mma_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t b, uint32_t id) {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, 1, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(b), "r"(id)
         : "memory");
 }
 __device__ __forceinline__ void commit(uint64_t* bar) {
@@ -502,19 +514,6 @@ __device__ __forceinline__ void commit(uint64_t* bar) {
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
-
-// Barrier of one warpgroup (named barrier id, 128 threads).
-__device__ __forceinline__ void wg_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
-// Same, returning whether any of the 128 threads passed a non-zero flag.
-__device__ __forceinline__ bool wg_sync_or(int id, bool flag) {
-    uint32_t r;
-    asm volatile(
-        "{\n.reg .pred p, q;\nsetp.ne.u32 q, %1, 0;\nbar.red.or.pred p, %2, 128, q;\nselp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(r)
-        : "r"(uint32_t(flag)), "r"(id)
-        : "memory");
-    return r != 0;
-}
 
 // 32 consecutive TMEM columns of this thread's lane, with the load's wait in
 // the same asm statement (the registers are defined only after completion).
@@ -551,6 +550,14 @@ __device__ __forceinline__ void st32(uint32_t taddr, const float (&v)[32]) {
         "r"(__float_as_uint(v[29])), "r"(__float_as_uint(v[30])), "r"(__float_as_uint(v[31]))
         : "memory");
 }
+__device__ __forceinline__ void st16(uint32_t taddr, const uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+            taddr),
+        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+        "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
+        : "memory");
+}
 
 // bf16x2 with relu: low half = a, high half = b
 __device__ __forceinline__ uint32_t pack_relu(float a, float b) {
@@ -566,14 +573,20 @@ __device__ __forceinline__ uint32_t codes_f16x2(uint32_t w, uint32_t sel) {
     asm("sub.rn.f16x2 %0, %1, %2;" : "=r"(d) : "r"(h), "r"(0x64006400u));
     return d;
 }
-// 32 channels (fp32 accumulators) -> ReLU -> bf16 -> 4 chunks of an operand
-__device__ __forceinline__ void store_bf16_row(unsigned char* chunk0, int m, const float (&v)[32]) {
+// 32 accumulators -> ReLU -> bf16 pairs -> 16 TMEM columns (an A operand row)
+__device__ __forceinline__ void relu_bf16_to_tmem(uint32_t dst, const float (&v)[32]) {
+    uint32_t o[16];
 #pragma unroll
-    for (int cc = 0; cc < 4; ++cc)
-        *reinterpret_cast<uint4*>(chunk0 + cc * kChunkBytes + m * 16) =
-            make_uint4(pack_relu(v[8 * cc], v[8 * cc + 1]), pack_relu(v[8 * cc + 2], v[8 * cc + 3]),
-                       pack_relu(v[8 * cc + 4], v[8 * cc + 5]), pack_relu(v[8 * cc + 6], v[8 * cc + 7]));
+    for (int c = 0; c < 16; ++c) o[c] = pack_relu(v[2 * c], v[2 * c + 1]);
+    st16(dst, o);
 }
+
+// A1 chunk of the first input of conv1 group q: the K=32 window starting at
+// input 8 * floor((20 q - 2) / 8), which holds the group's 20 inputs at
+// offset 6 (q even) or 2 (q odd).
+__host__ __device__ constexpr int c1_chunk(int q) { return (20 * q + 6) / 8; }  // floor((20q - 2) / 8) + 1
+static_assert(c1_chunk(0) == 0 && c1_chunk(1) == 3 && c1_chunk(6) == 15 && c1_chunk(6) + 3 < kA1Chunks,
+              "conv1 windows lie inside A1");
 
 struct InferArgs {
     const uint32_t* curve;
@@ -586,22 +599,19 @@ struct InferArgs {
     int32_t* status;
 };
 
-__global__ void __launch_bounds__(kNT, 1) infer_kernel(InferArgs a) {
+__global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int tid = threadIdx.x, warp = tid >> 5;
-    const int wg = tid >> 7;               // warpgroup
-    const int m = tid & 127;               // pixel of the tile = TMEM lane
-    const int bar_id = 1 + wg;             // named barrier of this warpgroup
-    const bool issuer = m == 0;            // issues this warpgroup's MMAs
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kBar) + 2 * wg;
+    const int m = tid;  // pixel of the tile / TMEM lane
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kBar);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kTmemSlot);
-    unsigned char* X = smem + wg * kWG;    // A1 / A3
-    unsigned char* Y = X + kRegX;          // A2 / A4
-    const uint32_t sX = dev::smem_u32(X), sY = dev::smem_u32(Y), sW = dev::smem_u32(smem + kWImg);
+    unsigned char* A1 = smem + kA1;
+    const uint32_t sA1 = dev::smem_u32(A1), sW = dev::smem_u32(smem + kWImg);
 
     for (int k = tid; k < kWBytes / 16; k += kNT) reinterpret_cast<uint4*>(smem + kWImg)[k] = a.wimg[k];
     if (tid == 0) {
-        for (int b = 0; b < 4; ++b) dev::mbar_init(reinterpret_cast<uint64_t*>(smem + kBar) + b, 1);
+        dev::mbar_init(&bars[0], 1);
+        dev::mbar_init(&bars[1], 1);
         dev::fence_barrier_init();
     }
     if (warp == 0) {
@@ -613,8 +623,8 @@ __global__ void __launch_bounds__(kNT, 1) infer_kernel(InferArgs a) {
     fence_before();
     __syncthreads();
     fence_after();
-    const uint32_t tm = *tslot + 256u * wg;                      // this warpgroup's columns
-    const uint32_t tl = tm + (uint32_t((warp & 3) * 32) << 16);  // + this warp's lane quarter
+    const uint32_t tm = *tslot;
+    const uint32_t tl = tm + (uint32_t(warp * 32) << 16);  // this warp's lane quarter
 
     const float* bias = reinterpret_cast<const float*>(smem + kWImg + kBias);
     const float* w5 = bias + 160;
@@ -622,9 +632,8 @@ __global__ void __launch_bounds__(kNT, 1) infer_kernel(InferArgs a) {
 
     const int tiles_x = (a.W + kM - 1) / kM;
     const int tiles = tiles_x * a.H;
-    const int stride = 2 * gridDim.x;
-    uint32_t ph[2] = {0, 0};  // phases waited for, per mbarrier of this warpgroup
-    uint32_t cm[2] = {0, 0};  // commits issued (issuer thread)
+    uint32_t ph[2] = {0, 0};  // phases waited for, per mbarrier
+    uint32_t cm[2] = {0, 0};  // commits issued (thread 0)
     bool failed = false;
     auto commit_to = [&](int b) {
         commit(&bars[b]);
@@ -635,9 +644,22 @@ __global__ void __launch_bounds__(kNT, 1) infer_kernel(InferArgs a) {
         if (ok) ++ph[b];
         return ok;
     };
+    auto bias_to_tmem = [&](uint32_t col, const float* src) {
+        float bv[32];
+#pragma unroll
+        for (int c = 0; c < 32; ++c) bv[c] = src[c];
+        st32(tl + col, bv);
+    };
+    // all threads: make this thread's TMEM / shared writes visible, then let
+    // thread 0 issue the next MMAs
+    auto hand_to_issuer = [&](bool smem_written) {
+        wait_st();
+        if (smem_written) dev::fence_proxy_async();
+        fence_before();
+        __syncthreads();
+    };
 
-    // this thread's curve words (pixel m, 32 groups of 4 disparities)
-    uint32_t cw[32];
+    uint32_t cw[32];  // this thread's curve words (32 groups of 4 disparities)
     auto load_curve = [&](int t) {
         const int y = t / tiles_x, x = (t % tiles_x) * kM + m;
 #pragma unroll
@@ -645,16 +667,17 @@ __global__ void __launch_bounds__(kNT, 1) infer_kernel(InferArgs a) {
             cw[g] = x < a.W ? __ldg(a.curve + ((size_t)y * a.groups + g) * a.curve_pitch + x + 2) : 0xFFFFFFFFu;
     };
 
-    int t = 2 * blockIdx.x + wg;
+    // the zero chunks of A1 never change
+    for (int c : {0, 17, 18}) *reinterpret_cast<uint4*>(A1 + c * kChunkBytes + m * 16) = make_uint4(0, 0, 0, 0);
+
+    int t = blockIdx.x;
     if (t < tiles) load_curve(t);
-    for (; t < tiles; t += stride) {
+    for (; t < tiles; t += gridDim.x) {
         const int y = t / tiles_x, x0 = (t % tiles_x) * kM;
-        // ---- A1: padding chunks 0 and 17, codes of inputs 0..127 in chunks 1..16
-        *reinterpret_cast<uint4*>(X + m * 16) = make_uint4(0, 0, 0, 0);
-        *reinterpret_cast<uint4*>(X + 17 * kChunkBytes + m * 16) = make_uint4(0, 0, 0, 0);
+        // ---- A1 chunks 1..16 = inputs 0..127; conv1 biases into C1
 #pragma unroll
         for (int c = 0; c < 16; ++c)
-            *reinterpret_cast<uint4*>(X + (1 + c) * kChunkBytes + m * 16) =
+            *reinterpret_cast<uint4*>(A1 + (1 + c) * kChunkBytes + m * 16) =
                 make_uint4(codes_f16x2(cw[2 * c], 0x4140), codes_f16x2(cw[2 * c], 0x4342),
                            codes_f16x2(cw[2 * c + 1], 0x4140), codes_f16x2(cw[2 * c + 1], 0x4342));
         {
@@ -662,121 +685,92 @@ __global__ void __launch_bounds__(kNT, 1) infer_kernel(InferArgs a) {
 #pragma unroll
             for (int c = 0; c < 32; ++c) bv[c] = bias[c];
 #pragma unroll
-            for (int q = 0; q < 8; ++q) st32(tl + q * 32, bv);
+            for (int q = 0; q < 7; ++q) st32(tl + 32 * q, bv);
         }
-        wait_st();
-        dev::fence_proxy_async();
-        fence_before();
-        wg_sync(bar_id);
-        // ---- conv1 + sum-pool: position p = 4q + k accumulates into columns q * 32
-        if (issuer) {
+        hand_to_issuer(true);
+        // ---- conv1 (+ 4-wide sum pooling): group q = one K=32 window, 2 MMAs
+        if (tid == 0) {
             fence_after();
-            for (int p = 0; p < 32; ++p) {
-                const bool odd = p & 1;
-                const int chunk = odd ? (p + 1) / 2 : p / 2;
-                mma(tm + (p >> 2) * 32, sdesc(sX + chunk * kChunkBytes, kChunkBytes),
-                    sdesc(sW + (odd ? kB1o : kB1e), 512), kIdC1);
+            for (int q = 0; q < 7; ++q) {
+                const uint32_t bb = sW + ((q & 1) ? kB1o : kB1e);
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                    mma_ss(tm + 32 * q, sdesc(sA1 + (c1_chunk(q) + 2 * h) * kChunkBytes, kChunkBytes),
+                           sdesc(bb + 2 * h * 512, 512), kIdC1);
             }
             commit_to(0);
         }
-        if (t + stride < tiles) load_curve(t + stride);  // next tile, behind the MMAs
-        if (wg_sync_or(bar_id, !wait_bar(0))) { failed = true; break; }
+        if (t + (int)gridDim.x < tiles) load_curve(t + gridDim.x);  // next tile, behind the MMAs
+        if (__syncthreads_or(!wait_bar(0))) { failed = true; break; }
         fence_after();
-        // ---- conv1 epilogue -> A2
+        // ---- conv1 epilogue: A2 position q (bf16) over the consumed C1 columns
 #pragma unroll 1
-        for (int q = 0; q < 8; ++q) {
+        for (int q = 0; q < 7; ++q) {
             float v[32];
-            ld32(tl + q * 32, v);
-            store_bf16_row(Y + q * 4 * kChunkBytes, m, v);
+            ld32(tl + 32 * q, v);
+            relu_bf16_to_tmem(tl + 16 * q, v);
         }
-        {
-            float bv[32];
-#pragma unroll
-            for (int c = 0; c < 32; ++c) bv[c] = bias[32 + c];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) st32(tl + kColC2 + r * 32, bv);
-        }
-        wait_st();
-        dev::fence_proxy_async();
-        fence_before();
-        wg_sync(bar_id);
-        // ---- conv2: position r, taps j with input q = 2r + j - 2 in 0..7
-        if (issuer) {
+        bias_to_tmem(kC2, bias + 32);
+        bias_to_tmem(kC2 + 32, bias + 32);
+        hand_to_issuer(false);
+        // ---- conv2 (A2 in TMEM): position r, taps j with input q = 3r + j - 1 in 0..6
+        if (tid == 0) {
             fence_after();
-            for (int r = 0; r < 4; ++r)
+            for (int r = 0; r < 2; ++r)
                 for (int j = 0; j < 5; ++j) {
-                    const int q = 2 * r + j - 2;
-                    if (q < 0 || q >= 8) continue;
+                    const int q = 3 * r + j - 1;
+                    if (q < 0 || q >= 7) continue;
 #pragma unroll
-                    for (int h2 = 0; h2 < 2; ++h2)
-                        mma(tm + kColC2 + r * 32, sdesc(sY + (q * 4 + 2 * h2) * kChunkBytes, kChunkBytes),
-                            sdesc(sW + kB2 + (j * 4 + 2 * h2) * 512, 512), kIdC2);
+                    for (int h = 0; h < 2; ++h)
+                        mma_ts(tm + kC2 + 32 * r, tm + 16 * q + 8 * h, sdesc(sW + kB2 + (j * 4 + 2 * h) * 512, 512),
+                               kIdC2);
                 }
             commit_to(1);
         }
-        if (wg_sync_or(bar_id, !wait_bar(1))) { failed = true; break; }
+        if (__syncthreads_or(!wait_bar(1))) { failed = true; break; }
         fence_after();
-        // ---- conv2 epilogue -> A3 (region X)
 #pragma unroll 1
-        for (int r = 0; r < 4; ++r) {
+        for (int r = 0; r < 2; ++r) {
             float v[32];
-            ld32(tl + kColC2 + r * 32, v);
-            store_bf16_row(X + r * 4 * kChunkBytes, m, v);
+            ld32(tl + kC2 + 32 * r, v);
+            relu_bf16_to_tmem(tl + kA3 + 16 * r, v);
         }
-        {
-            float bv[32];
-#pragma unroll
-            for (int c = 0; c < 32; ++c) bv[c] = bias[64 + c];
-            st32(tl + kColC3, bv);
-        }
-        wait_st();
-        dev::fence_proxy_async();
-        fence_before();
-        wg_sync(bar_id);
-        // ---- conv3: taps 1..4 on positions 0..3 (tap 0 meets the padding)
-        if (issuer) {
+        bias_to_tmem(kC3, bias + 64);
+        hand_to_issuer(false);
+        // ---- conv3 (A3 in TMEM): taps 2, 3 on positions 0, 1
+        if (tid == 0) {
             fence_after();
-            for (int j = 1; j < 5; ++j)
+            for (int j = 0; j < 2; ++j)
 #pragma unroll
-                for (int h2 = 0; h2 < 2; ++h2)
-                    mma(tm + kColC3, sdesc(sX + ((j - 1) * 4 + 2 * h2) * kChunkBytes, kChunkBytes),
-                        sdesc(sW + kB3 + (j * 4 + 2 * h2) * 512, 512), kIdC2);
+                for (int h = 0; h < 2; ++h)
+                    mma_ts(tm + kC3, tm + kA3 + 16 * j + 8 * h, sdesc(sW + kB3 + (j * 4 + 2 * h) * 512, 512), kIdC2);
             commit_to(0);
         }
-        if (wg_sync_or(bar_id, !wait_bar(0))) { failed = true; break; }
+        if (__syncthreads_or(!wait_bar(0))) { failed = true; break; }
         fence_after();
         {
             float v[32];
-            ld32(tl + kColC3, v);
-            store_bf16_row(Y, m, v);  // A4 (region Y)
-            float bv[32];
-#pragma unroll
-            for (int c = 0; c < 32; ++c) bv[c] = bias[96 + c];
-            st32(tl + kColF1, bv);
-#pragma unroll
-            for (int c = 0; c < 32; ++c) bv[c] = bias[128 + c];
-            st32(tl + kColF1 + 32, bv);
+            ld32(tl + kC3, v);
+            relu_bf16_to_tmem(tl + kA4, v);
         }
-        wait_st();
-        dev::fence_proxy_async();
-        fence_before();
-        wg_sync(bar_id);
-        // ---- fc1: K = 32 (2 MMAs), N = 64
-        if (issuer) {
+        bias_to_tmem(kC4, bias + 96);
+        bias_to_tmem(kC4 + 32, bias + 128);
+        hand_to_issuer(false);
+        // ---- fc1 (A4 in TMEM): K = 32 (2 MMAs), N = 64
+        if (tid == 0) {
             fence_after();
 #pragma unroll
-            for (int h2 = 0; h2 < 2; ++h2)
-                mma(tm + kColF1, sdesc(sY + 2 * h2 * kChunkBytes, kChunkBytes),
-                    sdesc(sW + kB4 + 2 * h2 * 1024, 1024), kIdF1);
+            for (int h = 0; h < 2; ++h)
+                mma_ts(tm + kC4, tm + kA4 + 8 * h, sdesc(sW + kB4 + 2 * h * 1024, 1024), kIdF1);
             commit_to(1);
         }
-        if (wg_sync_or(bar_id, !wait_bar(1))) { failed = true; break; }
+        if (__syncthreads_or(!wait_bar(1))) { failed = true; break; }
         fence_after();
         // ---- fc1 epilogue + fc2
         {
             float v0[32], v1[32];
-            ld32(tl + kColF1, v0);
-            ld32(tl + kColF1 + 32, v1);
+            ld32(tl + kC4, v0);
+            ld32(tl + kC4 + 32, v1);
             float z0 = b5, z1 = 0.f;
 #pragma unroll
             for (int c = 0; c < 32; ++c) {
@@ -787,11 +781,11 @@ __global__ void __launch_bounds__(kNT, 1) infer_kernel(InferArgs a) {
                 reinterpret_cast<float*>(reinterpret_cast<char*>(a.score) + (size_t)y * a.score_pitch)[x0 + m] =
                     1.f / (1.f + __expf(-(z0 + z1)));
         }
-        fence_before();  // this tile's TMEM reads before the next tile's MMAs
+        fence_before();  // this tile's TMEM reads before the next tile's writes
     }
     // After a timeout, MMAs may still be in flight: wait (bounded) for every
     // commit not yet waited for before giving the TMEM back.
-    if (failed && issuer) {
+    if (failed && tid == 0) {
         dev::report(a.status, CT_ETIMEOUT);
         for (int b = 0; b < 2; ++b)
             for (uint32_t k = ph[b]; k < cm[b]; ++k) dev::mbar_wait_bounded(&bars[b], k & 1);
@@ -800,8 +794,7 @@ __global__ void __launch_bounds__(kNT, 1) infer_kernel(InferArgs a) {
     __syncthreads();
     fence_after();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tslot), "r"(kTmemCols)
-                     : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm), "r"(kTmemCols) : "memory");
 }
 
 }  // namespace inf
@@ -883,32 +876,35 @@ int pack_weights(ConfNetHandle* h) {
     std::vector<unsigned char> img(kWBytes, 0);
     auto put16 = [&](int off, uint16_t v) { std::memcpy(&img[off], &v, 2); };
     auto bf = [&](int idx) { return bf16_bits_to_f32(f32_to_bf16_bits(p[idx])); };
-    // B1e / B1o: rows = channel, K = window offset of tap j: j + 6 (even
-    // positions) / j + 2 (odd positions); 2 chunks of 32 rows each
+    // B1e / B1o: rows = channel, K = 32-wide window of a conv1 group: the
+    // group's 20 inputs (4 positions x 5 taps, no overlap at stride 5) at
+    // offset 6 (even groups) or 2 (odd groups), tap t % 5 at offset + t
     for (int odd = 0; odd < 2; ++odd)
         for (int ch = 0; ch < 32; ++ch)
-            for (int j = 0; j < 5; ++j) {
-                const int k = j + (odd ? 2 : 6);
+            for (int t = 0; t < 20; ++t) {
+                const int k = t + (odd ? 2 : 6), j = t % 5;
                 uint16_t hb;
                 if (!bf16_to_f16_exact(bf(kOffW1 + ch * 5 + j), &hb))
                     return fail(CT_EINVAL, "conv1 weight %d (%g) is not exact in f16", ch * 5 + j,
                                 double(bf(kOffW1 + ch * 5 + j)));
-                put16((odd ? kB1o : kB1e) + (k / 8) * 32 * 16 + ch * 16 + (k % 8) * 2, hb);
+                put16((odd ? kB1o : kB1e) + (k / 8) * 512 + ch * 16 + (k % 8) * 2, hb);
             }
-    // B2 / B3: rows o, K = tap * 32 + in
-    for (int layer = 0; layer < 2; ++layer) {
-        const int base = layer == 0 ? kB2 : kB3, off = layer == 0 ? kOffW2 : kOffW3;
-        for (int o = 0; o < 32; ++o)
-            for (int i = 0; i < 32; ++i)
-                for (int j = 0; j < 5; ++j) {
-                    const int k = j * 32 + i;
-                    put16(base + (k / 8) * 32 * 16 + o * 16 + (k % 8) * 2, f32_to_bf16_bits(p[off + o * 160 + i * 5 + j]));
-                }
-    }
+    // B2: rows o, K = tap * 32 + in; B3: rows o, K = (tap - 2) * 32 + in, taps 2, 3
+    for (int o = 0; o < 32; ++o)
+        for (int i = 0; i < 32; ++i) {
+            for (int j = 0; j < 5; ++j) {
+                const int k = j * 32 + i;
+                put16(kB2 + (k / 8) * 512 + o * 16 + (k % 8) * 2, f32_to_bf16_bits(p[kOffW2 + o * 160 + i * 5 + j]));
+            }
+            for (int j = 2; j < 4; ++j) {
+                const int k = (j - 2) * 32 + i;
+                put16(kB3 + (k / 8) * 512 + o * 16 + (k % 8) * 2, f32_to_bf16_bits(p[kOffW3 + o * 160 + i * 5 + j]));
+            }
+        }
     // B4: rows h, K = in
     for (int hh = 0; hh < 64; ++hh)
         for (int i = 0; i < 32; ++i)
-            put16(kB4 + (i / 8) * 64 * 16 + hh * 16 + (i % 8) * 2, f32_to_bf16_bits(p[kOffW4 + hh * 32 + i]));
+            put16(kB4 + (i / 8) * 1024 + hh * 16 + (i % 8) * 2, f32_to_bf16_bits(p[kOffW4 + hh * 32 + i]));
     float* bias = reinterpret_cast<float*>(&img[kBias]);
     for (int k = 0; k < 32; ++k) bias[k] = p[kOffB1 + k];
     for (int k = 0; k < 32; ++k) bias[32 + k] = p[kOffB2 + k];
@@ -965,10 +961,10 @@ int ct_confnet_configure(ct_handle* hh, int32_t device, int32_t max_batch) {
     const size_t o_master = take(4 * kParams), o_m = take(4 * kParams), o_v = take(4 * kParams),
                  o_wq = take(4 * kParams), o_grad = take(4 * kParams),
                  o_part = take(4 * size_t(kParams) * chunks_for(max_batch)), o_loss = take(16),
-                 o_wimg = take(inf::kWBytes), o_a1 = take(4 * 256 * n), o_a2 = take(4 * 128 * n),
+                 o_wimg = take(inf::kWBytes), o_a1 = take(4 * 224 * n), o_a2 = take(4 * 64 * n),
                  o_a3 = take(4 * 32 * n), o_a4 = take(4 * 64 * n), o_logit = take(4 * n), o_dl = take(4 * n),
-                 o_ls = take(4 * n), o_dz4 = take(4 * 64 * n), o_dz3 = take(4 * 32 * n), o_dz2 = take(4 * 128 * n),
-                 o_dm1 = take(4 * 256 * n);
+                 o_ls = take(4 * n), o_dz4 = take(4 * 64 * n), o_dz3 = take(4 * 32 * n), o_dz2 = take(4 * 64 * n),
+                 o_dm1 = take(4 * 224 * n);
     cudaFree(h->arena);
     h->arena = nullptr;
     if (cudaMalloc(&h->arena, bytes) != cudaSuccess) return fail(CT_ENOMEM, "confidence-net scratch (%zu bytes)", bytes);
@@ -1145,7 +1141,7 @@ int ct_confnet_infer(ct_handle* hh, const ct_image* score, const ct_curves* curv
     a.wimg = reinterpret_cast<const uint4*>(h->wimg);
     a.status = h->d_status;
     const int tiles = ((a.W + inf::kM - 1) / inf::kM) * a.H;
-    const int grid = (tiles + 1) / 2 < h->sms ? (tiles + 1) / 2 : h->sms;  // 2 tile streams per CTA
+    const int grid = tiles < 2 * h->sms ? tiles : 2 * h->sms;  // two CTAs per SM
     inf::infer_kernel<<<grid, inf::kNT, inf::kSmem, s>>>(a);
     CT_LAUNCH_CHECK();
     return CT_OK;

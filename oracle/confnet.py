@@ -9,13 +9,14 @@ The network reads a pixel's uint8 census cost curve c[0..127] (aggregated
 and returns a validity logit. Its numerics are defined exactly as the GPU
 runs them:
 
-  conv1  1 -> 32, k=5, stride 4, pad 2 : z1[p,o] = sum_j w1[o,j] c[4p+j-2]          p = 0..31
-  pool   sum over 4 positions, plus bias: m1[q,o] = b1[o] + sum_{k<4} z1[4q+k,o]
-         ReLU, rounded to bf16 -> a1[8,32]
-  conv2 32 -> 32, k=5, stride 2, pad 2 : z2[r,o] = b2[o] + sum_{j,i} w2[o,i,j] a1[2r+j-2,i]  r = 0..3
-         ReLU, rounded to bf16 -> a2[4,32]
-  conv3 32 -> 32, k=5, pad 1 (one output): z3[o] = b3[o] + sum_{j,i} w3[o,i,j] a2[j-1,i]
-         ReLU, rounded to bf16 -> a3[32]
+  conv1  1 -> 32, k=5, stride 5, pad 2 : z1[p,o] = sum_j w1[o,j] c[5p+j-2]          p = 0..27
+         (positions 26, 27 lie wholly in the padding and are 0)
+  pool   sum over 4 positions, plus bias: m1[q,o] = b1[o] + sum_{k<4} z1[4q+k,o]  q = 0..6
+         ReLU, rounded to bf16 -> a1[7,32]
+  conv2 32 -> 32, k=5, stride 3, pad 1 : z2[r,o] = b2[o] + sum_{j,i} w2[o,i,j] a1[3r+j-1,i]  r = 0, 1
+         ReLU, rounded to bf16 -> a2[2,32]
+  conv3 32 -> 32, k=5, pad 2 (one output): z3[o] = b3[o] + sum_{j,i} w3[o,i,j] a2[j-2,i]
+         (taps 0, 1, 4 meet the padding) ReLU, rounded to bf16 -> a3[32]
   fc1   32 -> 64 : z4 = b4 + W4 a3, a4 = ReLU(z4) (fp32)
   fc2   64 -> 1  : logit = b5 + w5 . a4, score = sigmoid(logit) = P(disparity correct)
 
@@ -83,16 +84,16 @@ def forward(curves, flat, emulate=True):
     w = {k: (rw(v) if k in WEIGHTS else np.asarray(v, np.float64)) for k, v in p.items()}
     x = np.asarray(curves, np.float64)
     n = x.shape[0]
-    i1, ok1 = _conv_idx(32, 4, 2, 128)
-    X1 = x[:, i1] * ok1                                       # (n, 32, 5)
-    z1 = np.einsum("npj,oj->npo", X1, w["w1"])                # (n, 32, 32)
-    m1 = z1.reshape(n, 8, 4, 32).sum(axis=2) + w["b1"]        # (n, 8, 32)
+    i1, ok1 = _conv_idx(28, 5, 2, 128)
+    X1 = x[:, i1] * ok1                                       # (n, 28, 5)
+    z1 = np.einsum("npj,oj->npo", X1, w["w1"])                # (n, 28, 32)
+    m1 = z1.reshape(n, 7, 4, 32).sum(axis=2) + w["b1"]        # (n, 7, 32)
     a1 = rw(np.maximum(m1, 0.0))
-    i2, ok2 = _conv_idx(4, 2, 2, 8)
-    A1 = a1[:, i2, :] * ok2[None, :, :, None]                 # (n, 4, 5, 32)
-    z2 = np.einsum("nrji,oij->nro", A1, w["w2"]) + w["b2"]    # (n, 4, 32)
+    i2, ok2 = _conv_idx(2, 3, 1, 7)
+    A1 = a1[:, i2, :] * ok2[None, :, :, None]                 # (n, 2, 5, 32)
+    z2 = np.einsum("nrji,oij->nro", A1, w["w2"]) + w["b2"]    # (n, 2, 32)
     a2 = rw(np.maximum(z2, 0.0))
-    i3, ok3 = _conv_idx(1, 1, 1, 4)
+    i3, ok3 = _conv_idx(1, 1, 2, 2)
     A2 = a2[:, i3[0], :] * ok3[0][None, :, None]              # (n, 5, 32)
     z3 = np.einsum("nji,oij->no", A2, w["w3"]) + w["b3"]      # (n, 32)
     a3 = rw(np.maximum(z3, 0.0))
@@ -122,7 +123,7 @@ def loss_and_grad(curves, labels, flat, emulate=True):
     g["b3"] = dz3.sum(0)
     g["w3"] = np.einsum("no,nji->oij", dz3, c["A2"])
     dA2 = np.einsum("no,oij->nji", dz3, w["w3"]) * c["ok3"][0][None, :, None]
-    da2 = np.zeros((n, 4, 32))
+    da2 = np.zeros((n, 2, 32))
     for j in range(5):
         if c["ok3"][0][j]:
             da2[:, c["i3"][0][j], :] += dA2[:, j, :]
@@ -130,13 +131,13 @@ def loss_and_grad(curves, labels, flat, emulate=True):
     g["b2"] = dz2.sum((0, 1))
     g["w2"] = np.einsum("nro,nrji->oij", dz2, c["A1"])
     dA1 = np.einsum("nro,oij->nrji", dz2, w["w2"]) * c["ok2"][None, :, :, None]
-    da1 = np.zeros((n, 8, 32))
-    for r in range(4):
+    da1 = np.zeros((n, 7, 32))
+    for r in range(2):
         for j in range(5):
             if c["ok2"][r, j]:
                 da1[:, c["i2"][r, j], :] += dA1[:, r, j, :]
     dm1 = da1 * (c["m1"] > 0)
-    dz1 = np.repeat(dm1, 4, axis=1)                           # every pooled position
+    dz1 = np.repeat(dm1, 4, axis=1)                           # every pooled position (n, 28, 32)
     g["b1"] = dm1.sum((0, 1))
     g["w1"] = np.einsum("npo,npj->oj", dz1, c["X1"])
     return loss, flatten(g)
