@@ -166,7 +166,7 @@ int ct_bm_census_match_desc(ct_handle* h, const ct_image* disp, const ct_image* 
 
 /* Cost-curve volume: the matcher's aggregated cost of every (pixel,
  * disparity), one byte each, the input of the learned confidence net
- * (ct_confnet_*). Code = min(255, 5x5 Hamming sum >> 2); 255 for a disparity
+ * (ct_confnet_*). Code = 5x5 Hamming sum >> 3 (0..196); 255 for a disparity
  * whose match window leaves the image and for all disparities of a border
  * pixel (within 2 of the image edge). Layout: groups g = 0 .. ceil(D/4) - 1
  * of 4 disparities; row (y, g) starts at ptr + (y * ceil(D/4) + g) *

@@ -105,8 +105,9 @@ struct MatchArgs {
     // row (y, g) at curve + (y * curve_groups + g) * curve_pitch holds one
     // 32-bit word per pixel, word x + 2 for column x, whose bytes are the
     // codes of disparities 4g .. 4g + 3 (byte k = disparity 4g + k).
-    // Code = min(255, aggregated cost >> 2); 255 for a disparity whose match
-    // window leaves the image and for every disparity of a border pixel.
+    // Code = aggregated cost >> 3 (at most 1575 >> 3 = 196); 255 for a
+    // disparity whose match window leaves the image and for every disparity of
+    // a border pixel.
     uint32_t* curve;
     size_t curve_pitch;  // 32-bit words per row, a multiple of 4
     int curve_groups;    // ceil(D / 4)
@@ -246,18 +247,18 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
         for (int c = 0; c < kCPT; ++c) {
             const int x = xs + 4 * lane + c;
             const bool pv = rowv && x >= kAR && x < a.W - kAR;
-            uint32_t v[NP];
 #pragma unroll
-            for (int p = 0; p < NP; ++p) {
-                uint32_t t = dev::min_u16x2((C[c][p] >> 2) & 0x3FFF3FFFu, 0x00FF00FFu);
-                if (EDGE) {
-                    const int dlo = dw + 2 * p;
-                    t |= (dlo > lim[c] ? 0x000000FFu : 0u) | (dlo + 1 > lim[c] ? 0x00FF0000u : 0u);
+            for (int q = 0; q < NG; ++q) {
+                // C < 2048 per 16-bit half, so byte 0 and byte 2 of C >> 3 are
+                // the two codes (bits of the high half shifted into byte 1 are
+                // never selected)
+                uint32_t w = __byte_perm(C[c][2 * q] >> 3, C[c][2 * q + 1] >> 3, 0x6420);
+                if (EDGE) {  // disparities above lim[c] read 255
+                    const int nvalid = min(max(lim[c] - (dw + 4 * q) + 1, 0), 4);
+                    w |= nvalid >= 4 ? 0u : (0xFFFFFFFFu << (8 * nvalid));
                 }
-                v[p] = pv ? t : 0x00FF00FFu;
+                wv[c][q] = pv ? w : 0xFFFFFFFFu;
             }
-#pragma unroll
-            for (int q = 0; q < NG; ++q) wv[c][q] = __byte_perm(v[2 * q], v[2 * q + 1], 0x6420);
         }
 #pragma unroll
         for (int q = 0; q < NG; ++q) {

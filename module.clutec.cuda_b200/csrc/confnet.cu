@@ -490,26 +490,35 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo) {
            (uint64_t(1) << 46);
 }
 
+// A descriptor moved by `bytes` (a multiple of 16) along its start field.
+__device__ __forceinline__ uint64_t dplus(uint64_t d, uint32_t bytes) { return d + uint64_t(bytes >> 4); }
+
+// The MMA helpers are executed by a whole (converged) warp; one elected lane
+// issues. Warp-uniform operands stay in uniform registers, which makes the
+// issue of consecutive MMAs several times cheaper than from a lone thread.
 // D (TMEM) += A (shared memory) x B (shared memory)
 __device__ __forceinline__ void mma_ss(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t id) {
     asm volatile(
-        "{\n.reg .pred p;\nsetp.ne.b32 p, 1, 0;\n"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "{\n.reg .pred p, e;\nsetp.ne.b32 p, 1, 0;\nelect.sync _|e, 0xffffffff;\n"
+        "@e tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
         "l"(a), "l"(b), "r"(id)
         : "memory");
 }
 // D (TMEM) += A (TMEM, lane = row, K packed in pairs per column) x B (shared memory)
 __device__ __forceinline__ void mma_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t b, uint32_t id) {
     asm volatile(
-        "{\n.reg .pred p;\nsetp.ne.b32 p, 1, 0;\n"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "{\n.reg .pred p, e;\nsetp.ne.b32 p, 1, 0;\nelect.sync _|e, 0xffffffff;\n"
+        "@e tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n}\n" ::"r"(tmem_d),
         "r"(tmem_a), "l"(b), "r"(id)
         : "memory");
 }
+// Completion of this warp's MMAs so far -> one arrive on bar (elected lane).
 __device__ __forceinline__ void commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                     dev::smem_u32(bar))
-                 : "memory");
+    asm volatile(
+        "{\n.reg .pred e;\nelect.sync _|e, 0xffffffff;\n"
+        "@e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n}\n" ::"r"(
+            dev::smem_u32(bar))
+        : "memory");
 }
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -533,6 +542,24 @@ __device__ __forceinline__ void ld32(uint32_t taddr, float (&v)[32]) {
         : "memory");
 #pragma unroll
     for (int k = 0; k < 32; ++k) v[k] = __uint_as_float(r[k]);
+}
+// Two 32-column loads (columns taddr .. +31 and taddr2 .. +31), one wait.
+__device__ __forceinline__ void ld32x2(uint32_t taddr, uint32_t taddr2, float (&v)[32], float (&u)[32]) {
+    uint32_t r[64];
+    asm volatile(
+        "{\n"
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%64];\n"
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%65];\n"
+        "tcgen05.wait::ld.sync.aligned;\n"
+        "}\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+        : "r"(taddr), "r"(taddr2)
+        : "memory");
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+        v[k] = __uint_as_float(r[k]);
+        u[k] = __uint_as_float(r[32 + k]);
+    }
 }
 __device__ __forceinline__ void st32(uint32_t taddr, const float (&v)[32]) {
     asm volatile(
@@ -629,11 +656,18 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
     const float* bias = reinterpret_cast<const float*>(smem + kWImg + kBias);
     const float* w5 = bias + 160;
     const float b5 = bias[224];
+    float bias1[32];  // conv1 biases, stored into 7 accumulator groups per tile
+#pragma unroll
+    for (int c = 0; c < 32; ++c) bias1[c] = bias[c];
+    // base descriptors; every operand of a tile is a constant offset from one
+    const uint64_t dA1 = sdesc(sA1, kChunkBytes);
+    const uint64_t dB1e = sdesc(sW + kB1e, 512), dB1o = sdesc(sW + kB1o, 512);
+    const uint64_t dB2 = sdesc(sW + kB2, 512), dB3 = sdesc(sW + kB3, 512), dB4 = sdesc(sW + kB4, 1024);
 
     const int tiles_x = (a.W + kM - 1) / kM;
     const int tiles = tiles_x * a.H;
     uint32_t ph[2] = {0, 0};  // phases waited for, per mbarrier
-    uint32_t cm[2] = {0, 0};  // commits issued (thread 0)
+    uint32_t cm[2] = {0, 0};  // commits issued (counted by every lane of warp 0)
     bool failed = false;
     auto commit_to = [&](int b) {
         commit(&bars[b]);
@@ -680,70 +714,72 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
             *reinterpret_cast<uint4*>(A1 + (1 + c) * kChunkBytes + m * 16) =
                 make_uint4(codes_f16x2(cw[2 * c], 0x4140), codes_f16x2(cw[2 * c], 0x4342),
                            codes_f16x2(cw[2 * c + 1], 0x4140), codes_f16x2(cw[2 * c + 1], 0x4342));
-        {
-            float bv[32];
 #pragma unroll
-            for (int c = 0; c < 32; ++c) bv[c] = bias[c];
-#pragma unroll
-            for (int q = 0; q < 7; ++q) st32(tl + 32 * q, bv);
-        }
+        for (int q = 0; q < 7; ++q) st32(tl + 32 * q, bias1);
         hand_to_issuer(true);
         // ---- conv1 (+ 4-wide sum pooling): group q = one K=32 window, 2 MMAs
-        if (tid == 0) {
+        if (warp == 0) {  // MMA issue: whole warp, one elected lane
             fence_after();
-            for (int q = 0; q < 7; ++q) {
-                const uint32_t bb = sW + ((q & 1) ? kB1o : kB1e);
+#pragma unroll
+            for (int q = 0; q < 7; ++q)
 #pragma unroll
                 for (int h = 0; h < 2; ++h)
-                    mma_ss(tm + 32 * q, sdesc(sA1 + (c1_chunk(q) + 2 * h) * kChunkBytes, kChunkBytes),
-                           sdesc(bb + 2 * h * 512, 512), kIdC1);
-            }
+                    mma_ss(tm + 32 * q, dplus(dA1, (c1_chunk(q) + 2 * h) * kChunkBytes),
+                           dplus((q & 1) ? dB1o : dB1e, 2 * h * 512), kIdC1);
             commit_to(0);
         }
         if (t + (int)gridDim.x < tiles) load_curve(t + gridDim.x);  // next tile, behind the MMAs
         if (__syncthreads_or(!wait_bar(0))) { failed = true; break; }
         fence_after();
         // ---- conv1 epilogue: A2 position q (bf16) over the consumed C1 columns
-#pragma unroll 1
-        for (int q = 0; q < 7; ++q) {
-            float v[32];
-            ld32(tl + 32 * q, v);
+#pragma unroll
+        for (int q = 0; q < 6; q += 2) {
+            float v[32], u[32];
+            ld32x2(tl + 32 * q, tl + 32 * (q + 1), v, u);
             relu_bf16_to_tmem(tl + 16 * q, v);
+            relu_bf16_to_tmem(tl + 16 * (q + 1), u);
+        }
+        {
+            float v[32];
+            ld32(tl + 32 * 6, v);
+            relu_bf16_to_tmem(tl + 16 * 6, v);
         }
         bias_to_tmem(kC2, bias + 32);
         bias_to_tmem(kC2 + 32, bias + 32);
         hand_to_issuer(false);
         // ---- conv2 (A2 in TMEM): position r, taps j with input q = 3r + j - 1 in 0..6
-        if (tid == 0) {
+        if (warp == 0) {  // MMA issue: whole warp, one elected lane
             fence_after();
+#pragma unroll
             for (int r = 0; r < 2; ++r)
+#pragma unroll
                 for (int j = 0; j < 5; ++j) {
                     const int q = 3 * r + j - 1;
                     if (q < 0 || q >= 7) continue;
 #pragma unroll
                     for (int h = 0; h < 2; ++h)
-                        mma_ts(tm + kC2 + 32 * r, tm + 16 * q + 8 * h, sdesc(sW + kB2 + (j * 4 + 2 * h) * 512, 512),
-                               kIdC2);
+                        mma_ts(tm + kC2 + 32 * r, tm + 16 * q + 8 * h, dplus(dB2, (j * 4 + 2 * h) * 512), kIdC2);
                 }
             commit_to(1);
         }
         if (__syncthreads_or(!wait_bar(1))) { failed = true; break; }
         fence_after();
-#pragma unroll 1
-        for (int r = 0; r < 2; ++r) {
-            float v[32];
-            ld32(tl + kC2 + 32 * r, v);
-            relu_bf16_to_tmem(tl + kA3 + 16 * r, v);
+        {
+            float v[32], u[32];
+            ld32x2(tl + kC2, tl + kC2 + 32, v, u);
+            relu_bf16_to_tmem(tl + kA3, v);
+            relu_bf16_to_tmem(tl + kA3 + 16, u);
         }
         bias_to_tmem(kC3, bias + 64);
         hand_to_issuer(false);
         // ---- conv3 (A3 in TMEM): taps 2, 3 on positions 0, 1
-        if (tid == 0) {
+        if (warp == 0) {  // MMA issue: whole warp, one elected lane
             fence_after();
+#pragma unroll
             for (int j = 0; j < 2; ++j)
 #pragma unroll
                 for (int h = 0; h < 2; ++h)
-                    mma_ts(tm + kC3, tm + kA3 + 16 * j + 8 * h, sdesc(sW + kB3 + (j * 4 + 2 * h) * 512, 512), kIdC2);
+                    mma_ts(tm + kC3, tm + kA3 + 16 * j + 8 * h, dplus(dB3, (j * 4 + 2 * h) * 512), kIdC2);
             commit_to(0);
         }
         if (__syncthreads_or(!wait_bar(0))) { failed = true; break; }
@@ -757,11 +793,10 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
         bias_to_tmem(kC4 + 32, bias + 128);
         hand_to_issuer(false);
         // ---- fc1 (A4 in TMEM): K = 32 (2 MMAs), N = 64
-        if (tid == 0) {
+        if (warp == 0) {  // MMA issue: whole warp, one elected lane
             fence_after();
 #pragma unroll
-            for (int h = 0; h < 2; ++h)
-                mma_ts(tm + kC4, tm + kA4 + 8 * h, sdesc(sW + kB4 + 2 * h * 1024, 1024), kIdF1);
+            for (int h = 0; h < 2; ++h) mma_ts(tm + kC4, tm + kA4 + 8 * h, dplus(dB4, 2 * h * 1024), kIdF1);
             commit_to(1);
         }
         if (__syncthreads_or(!wait_bar(1))) { failed = true; break; }
@@ -769,17 +804,18 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
         // ---- fc1 epilogue + fc2
         {
             float v0[32], v1[32];
-            ld32(tl + kC4, v0);
-            ld32(tl + kC4 + 32, v1);
-            float z0 = b5, z1 = 0.f;
+            ld32x2(tl + kC4, tl + kC4 + 32, v0, v1);
+            float z[4] = {b5, 0.f, 0.f, 0.f};  // four independent chains
 #pragma unroll
-            for (int c = 0; c < 32; ++c) {
-                z0 = fmaf(w5[c], fmaxf(v0[c], 0.f), z0);
-                z1 = fmaf(w5[32 + c], fmaxf(v1[c], 0.f), z1);
+            for (int c = 0; c < 32; c += 2) {
+                z[0] = fmaf(w5[c], fmaxf(v0[c], 0.f), z[0]);
+                z[1] = fmaf(w5[c + 1], fmaxf(v0[c + 1], 0.f), z[1]);
+                z[2] = fmaf(w5[32 + c], fmaxf(v1[c], 0.f), z[2]);
+                z[3] = fmaf(w5[33 + c], fmaxf(v1[c + 1], 0.f), z[3]);
             }
             if (x0 + m < a.W)
                 reinterpret_cast<float*>(reinterpret_cast<char*>(a.score) + (size_t)y * a.score_pitch)[x0 + m] =
-                    1.f / (1.f + __expf(-(z0 + z1)));
+                    1.f / (1.f + __expf(-((z[0] + z[1]) + (z[2] + z[3]))));
         }
         fence_before();  // this tile's TMEM reads before the next tile's writes
     }

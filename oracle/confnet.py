@@ -5,7 +5,7 @@ kernels of the confidence net (csrc/confnet_*.cu). Only tests/ and the
 cpu_baseline leg of bench.py import it; the product never does.
 
 The network reads a pixel's uint8 census cost curve c[0..127] (aggregated
-5x5 Hamming cost >> 2, saturated at 255; 255 for unsearchable disparities)
+5x5 Hamming cost >> 3, 0..196; 255 for unsearchable disparities)
 and returns a validity logit. Its numerics are defined exactly as the GPU
 runs them:
 

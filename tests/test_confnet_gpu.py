@@ -35,7 +35,7 @@ def curves_of(ct, cuda, L, R, D, lr=True, tuning=None):
 def test_curves_bit_exact(ct, oracle, cuda, W, H, D, kind, lr, tuning):
     L, R, _, _ = ct.synth_pair(kind, 11 + W, W, H, D - 1)
     cv, disp = curves_of(ct, cuda, L, R, D, lr, tuning)
-    want_d, _, want_c = oracle.match_census(L, R, D, 2, lr, curve_shift=2)
+    want_d, _, want_c = oracle.match_census(L, R, D, 2, lr, curve_shift=3)
     np.testing.assert_array_equal(cv.to_hwd(), want_c)
     np.testing.assert_array_equal(disp.view(np.uint16), oracle.to_u16(want_d))
 
@@ -44,7 +44,7 @@ def test_gather(ct, oracle, cuda):
     W, H, D = 200, 64, 128
     L, R, _, _ = ct.synth_pair(1, 5, W, H, D - 1)
     cv, _ = curves_of(ct, cuda, L, R, D)
-    _, _, want_c = oracle.match_census(L, R, D, 2, True, curve_shift=2)
+    _, _, want_c = oracle.match_census(L, R, D, 2, True, curve_shift=3)
     r = np.random.default_rng(1)
     xy = np.stack([r.integers(0, W, 777), r.integers(0, H, 777)], 1).astype(np.int32)
     net = ct.ConfNet()
@@ -58,7 +58,7 @@ def test_gather(ct, oracle, cuda):
 def _real_samples(ct, oracle, n, seed):
     W, H, D = 333, 111, 128
     L, R, _, _ = ct.synth_pair(1, seed, W, H, D - 1)
-    _, _, curve = oracle.match_census(L, R, D, 2, True, curve_shift=2)
+    _, _, curve = oracle.match_census(L, R, D, 2, True, curve_shift=3)
     r = np.random.default_rng(seed)
     return curve[r.integers(0, H, n), r.integers(0, W, n)]
 
