@@ -378,9 +378,13 @@ int ct_synth_pair(int32_t kind, uint64_t seed, int32_t width, int32_t height, in
  * left-right check (CrossCheckDisparityMaps.cu:63-110), which stays the
  * fallback and the judge of its error. No counterpart in the reference.
  *
- * Network: conv1 1->32 (k=5, stride 4, pad 2) -> max-pool 4 -> ReLU ->
- * conv2 32->32 (k=5, stride 2, pad 2) -> ReLU -> conv3 32->32 (k=5, pad 1, one
- * output) -> ReLU -> fc1 32->64 -> ReLU -> fc2 64->1 -> sigmoid. Weights bf16
+ * Input: the pixel's curve re-centred on its winning disparity d (taken from
+ * the left-to-right disparity map): sample r[k] = c[d - 64 + k], 255 outside
+ * the curve; the convolutions read its 35 central codes r[52 .. 86] (the
+ * disparities d - 12 .. d + 22).
+ * Network: conv1 1->32 (k=5, stride 5) -> ReLU -> conv2 32->32 (k=5, stride
+ * 3, pad 1) -> ReLU -> conv3 32->32 (k=5, pad 2, one output) -> ReLU -> fc1
+ * 32->64 -> ReLU -> fc2 64->1 -> sigmoid. Weights bf16
  * (fp32 master copies during training), biases fp32, accumulation fp32, conv
  * activations rounded to bf16. Flat parameter order (CT_CONFNET_PARAMS
  * floats): w1[32][5], b1[32], w2[32][32][5] ([out][in][tap]), b2[32],
@@ -402,9 +406,10 @@ int ct_confnet_init(ct_handle* h, uint64_t seed);
 /* Host fp32 parameter vectors (save / load); set resets the optimiser. */
 int ct_confnet_set_params(ct_handle* h, const float* params, int32_t n);
 int ct_confnet_get_params(ct_handle* h, float* params, int32_t n);
-/* samples[n][128] (bytes) = curves at pixels xy[n] = (x, y) pairs. */
-int ct_confnet_gather(ct_handle* h, uint8_t* samples, const ct_curves* curves, const int32_t* xy, int32_t n,
-                      ct_stream stream);
+/* samples[n][128] (bytes) = re-centred curves at pixels xy[n] = (x, y)
+ * pairs; disp (U8 or U16, same size as the curves) holds the winners. */
+int ct_confnet_gather(ct_handle* h, uint8_t* samples, const ct_curves* curves, const ct_image* disp,
+                      const int32_t* xy, int32_t n, ct_stream stream);
 /* Mean binary cross-entropy of n samples (labels: 1 = disparity correct)
  * and its gradient (CT_CONFNET_PARAMS floats); either output may be NULL. */
 int ct_confnet_loss_grad(ct_handle* h, const uint8_t* samples, const uint8_t* labels, int32_t n, float* grad,
@@ -417,7 +422,8 @@ int ct_confnet_scores(ct_handle* h, float* scores, const uint8_t* samples, int32
 /* Score map (F32, P(disparity correct)) of a whole curve volume on the
  * tensor cores. The first call after new weights packs them (synchronises
  * the previous stream). */
-int ct_confnet_infer(ct_handle* h, const ct_image* score, const ct_curves* curves, ct_stream stream);
+int ct_confnet_infer(ct_handle* h, const ct_image* score, const ct_curves* curves, const ct_image* disp,
+                     ct_stream stream);
 
 /* ---- pipe-rate probe ---------------------------------------------------------
  * Measures the issue rate of the integer operations the matchers are built

@@ -6,10 +6,12 @@
 // which stays as the fallback and as the judge of its error.
 //
 // Network (weights bf16, biases fp32, accumulation fp32):
-//   conv1  1 -> 32, k=5, stride 4, pad 2 -> 32 positions (no bias); sum over
-//          4 positions + bias; ReLU; rounded to bf16 -> a1[8][32]
-//   conv2 32 -> 32, k=5, stride 2, pad 2 -> 4 positions; ReLU; bf16 -> a2[4][32]
-//   conv3 32 -> 32, k=5, pad 1, one output; ReLU; bf16 -> a3[32]
+//   input  the pixel's curve re-centred on its winning disparity d: sample
+//          r[k] = c[d - 64 + k] (255 outside); the convolutions read the 35
+//          codes x[k] = r[52 + k] (disparities d - 12 .. d + 22)
+//   conv1  1 -> 32, k=5, stride 5 -> 7 positions; ReLU; bf16 -> a1[7][32]
+//   conv2 32 -> 32, k=5, stride 3, pad 1 -> 2 positions; ReLU; bf16 -> a2[2][32]
+//   conv3 32 -> 32, k=5, pad 2, one output (taps 2, 3 meet data); ReLU; bf16 -> a3[32]
 //   fc1   32 -> 64, ReLU (fp32) -> a4[64]
 //   fc2   64 -> 1, logit; score = sigmoid(logit)
 // Flat parameter order: w1[32][5], b1[32], w2[32][32][5] ([out][in][tap]),
@@ -21,17 +23,15 @@
 // in a fixed order (deterministic). Adam keeps fp32 master weights and
 // writes their bf16 roundings for the next forward.
 //
-// Inference (tensor cores, tcgen05): a persistent kernel, one CTA of 8 warps
-// per SM, 128 pixels (one row segment) per tile. Each layer is a set of
-// M=128 tcgen05.mma into TMEM (fp32): conv1 as 16 windows of K=16 inputs x
-// N=64 (2 positions x 32 channels, f16 operands: curve codes are integers,
-// exact in f16, and the bf16 weights are exact in f16), conv2/conv3 per
-// output position as K=16 slices (channel halves) of each tap (bf16), fc1
-// K=32 x N=64. Biases are written into the accumulator columns with
-// tcgen05.st before each layer. Epilogue warps read the accumulators with
-// tcgen05.ld, pool / ReLU / round to bf16 and write the next layer's A
-// operand to shared memory; conv1 runs in 8 chunks of 2 windows into two
-// TMEM buffers so the MMAs of chunk k+1 overlap the epilogue of chunk k.
+// Inference (tensor cores, tcgen05): a persistent kernel of one warpgroup per
+// CTA, two CTAs per SM, 128 pixels (a row segment) per tile = the M of every
+// MMA. conv1 is three MMAs over an im2col of the 35 codes (15 per K=16
+// window, f16: the codes are integers and the bf16 weights are exact in
+// f16); conv2, conv3 and fc1 read their activations from tensor memory (the
+// A-from-TMEM form) and bf16 weights from shared memory. Biases are written
+// into the fp32 accumulator columns with tcgen05.st before each layer; the
+// epilogues read them with tcgen05.ld, apply ReLU, round to bf16 and store
+// the next layer's A operand back into the tensor memory they have consumed.
 #include "ct_internal.h"
 #include "ct_device.cuh"
 #include "census_match.cuh"
@@ -54,6 +54,7 @@ constexpr int kOffW1 = 0, kOffB1 = 160, kOffW2 = 192, kOffB2 = 5312, kOffW3 = 53
 constexpr int kParams = 12673;
 static_assert(kParams == CT_CONFNET_PARAMS, "parameter count");
 constexpr int kLen = 128;  // curve length (disparities)
+constexpr int kCropLo = 52, kCropLen = 35;  // codes of the re-centred sample the convolutions read
 
 __host__ __device__ inline bool is_weight(int p) {
     return p < kOffB1 || (p >= kOffW2 && p < kOffB2) || (p >= kOffW3 && p < kOffB3) || (p >= kOffW4 && p < kOffB4) ||
@@ -65,17 +66,40 @@ __device__ __forceinline__ float bf16r(float v) { return __bfloat162float(__floa
 // ---------------------------------------------------------------------------
 // Gather: samples[n][128] from a curve volume at pixel list xy[n][2]
 // ---------------------------------------------------------------------------
-// Pixels outside the volume read as all-255 curves and set CT_EINVAL.
-__global__ void gather_kernel(uint8_t* samples, const uint32_t* curve, size_t pitch_words, int groups, int W,
-                              int H, const int32_t* xy, int n, int32_t* status) {
+// Winning disparity of a map entry (U16 EDisparityId d + 1, U8 d; 0 when the
+// pixel has no disparity).
+__device__ __forceinline__ int winner(const void* disp, size_t pitch, int type, int x, int y) {
+    const char* row = static_cast<const char*>(disp) + (size_t)y * pitch;
+    if (type == CT_PIX_U8) {
+        const int v = reinterpret_cast<const uint8_t*>(row)[x];
+        return v < kLen ? v : 0;
+    }
+    const int v = reinterpret_cast<const uint16_t*>(row)[x];
+    return (v >= 1 && v <= kLen) ? v - 1 : 0;
+}
+
+// Re-centred samples: samples[s][k] = curve(x, y)[d - 64 + k] (255 outside),
+// d the pixel's winning disparity. One warp per sample, lane = output word.
+// Pixels outside the volume read as all-255 samples and set CT_EINVAL.
+__global__ void gather_kernel(uint8_t* samples, const uint32_t* curve, size_t pitch_words, int W, int H,
+                              const void* disp, size_t disp_pitch, int disp_type, const int32_t* xy, int n,
+                              int32_t* status) {
     const int s = blockIdx.x * 8 + (threadIdx.x >> 5);
-    const int g = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31;
     if (s >= n) return;
     const int x = xy[2 * s], y = xy[2 * s + 1];
     const bool inside = x >= 0 && x < W && y >= 0 && y < H;
-    if (!inside && g == 0) dev::report(status, CT_EINVAL);
-    const uint32_t w = (inside && g < groups) ? curve[((size_t)y * groups + g) * pitch_words + x + 2] : 0xFFFFFFFFu;
-    reinterpret_cast<uint32_t*>(samples + (size_t)s * kLen)[g] = w;
+    if (!inside && lane == 0) dev::report(status, CT_EINVAL);
+    uint32_t w = 0xFFFFFFFFu;
+    if (inside) {
+        const int b0 = winner(disp, disp_pitch, disp_type, x, y) - 64 + 4 * lane;  // first curve byte of this word
+        const int g0 = b0 >> 2, sh = (b0 & 3) * 8;                                 // arithmetic shift: floor
+        auto word = [&](int g) {
+            return (g >= 0 && g < kLen / 4) ? curve[((size_t)y * (kLen / 4) + g) * pitch_words + x + 2] : 0xFFFFFFFFu;
+        };
+        w = __funnelshift_r(word(g0), word(g0 + 1), sh);
+    }
+    reinterpret_cast<uint32_t*>(samples + (size_t)s * kLen)[lane] = w;
 }
 
 // ---------------------------------------------------------------------------
@@ -99,7 +123,7 @@ constexpr int kR = 2;   // conv2 positions
 
 constexpr int kSY = 16;  // samples per CTA
 
-// conv1 (k=5, stride 5, pad 2) + sum over 4 positions + bias, ReLU, bf16
+// conv1 (k=5, stride 5) over the 35 central codes, ReLU, bf16
 __global__ void __launch_bounds__(32 * kSY) fwd1_kernel(const uint8_t* x, const float* wq, Act A, int n) {
     __shared__ float xs[kSY][kLen];
     const int o = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * kSY + sl;
@@ -114,10 +138,7 @@ __global__ void __launch_bounds__(32 * kSY) fwd1_kernel(const uint8_t* x, const 
     for (int q = 0; q < kQ; ++q) {
         float z = b;
 #pragma unroll
-        for (int t = 0; t < 20; ++t) {  // position 4q + t / 5, tap t % 5
-            const int i = 20 * q + t - 2;
-            if (i >= 0 && i < kLen) z = fmaf(w[t % 5], xs[sl][i], z);
-        }
+        for (int j = 0; j < 5; ++j) z = fmaf(w[j], xs[sl][kCropLo + 5 * q + j], z);
         A.a1[(size_t)s * 224 + q * 32 + o] = bf16r(fmaxf(z, 0.f));
     }
 }
@@ -296,13 +317,7 @@ __global__ void __launch_bounds__(256) wgrad_kernel(const uint8_t* x, Act A, int
                     const float g = A.dm1[(size_t)s * 224 + q * 32 + o];
                     if (g == 0.f) continue;
                     if (bias) { acc += g; continue; }
-                    float xsum = 0.f;  // inputs of tap j over the 4 pooled positions
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const int i = 20 * q + 5 * k + j - 2;
-                        if (i >= 0 && i < kLen) xsum += float(x[(size_t)s * kLen + i]);
-                    }
-                    acc = fmaf(g, xsum, acc);
+                    acc = fmaf(g, float(x[(size_t)s * kLen + kCropLo + 5 * q + j]), acc);
                 }
             }
             P[bias ? kOffB1 + o : kOffW1 + t] = acc;
@@ -441,17 +456,25 @@ constexpr int kNT = 128;  // one warpgroup: thread = pixel of the tile = TMEM la
 constexpr int kM = 128;   // pixels per tile = MMA M
 constexpr int kChunkBytes = kM * 16;  // one K-chunk (8 elements) of the 128-row A1 operand
 
-// Shared memory: A1 = the tile's curve codes as f16, K-major without
-// swizzle in K-chunk panels (element (pixel r, input i) at chunk (i + 8) / 8,
-// offset r * 16 + ((i + 8) % 8) * 2; 19 chunks = inputs -8 .. 143, zero
-// outside 0 .. 127), then the packed weights (B operands in the same panel
-// form with rows = output channels, and fp32 biases).
-constexpr int kA1Chunks = 19;
-constexpr int kA1 = 0;
-constexpr int kWImg = kA1Chunks * kChunkBytes;
-constexpr int kB1e = 0;                 // conv1, even groups: N=32 x K=32 f16, 20 taps at k = 6..25 (LBO 512)
-constexpr int kB1o = kB1e + 4 * 512;    // conv1, odd groups: taps at k = 2..21
-constexpr int kB2 = kB1o + 4 * 512;     // conv2: N=32 x K=160 bf16, chunk = tap * 4 + in / 8 (LBO 512)
+// Shared memory:
+//   stage  each pixel's curve bytes in a row of kStageWords words: 3 words of
+//          255, the 32 curve words, 10 words of 255, so the 35 codes the
+//          convolutions read (curve bytes d - 12 .. d + 22) are row bytes
+//          d .. d + 34 (odd row stride: conflict-free column access)
+//   A1     conv1 operand, f16, K-major without swizzle in K-chunk panels
+//          (element (pixel r, k) at (k / 8) * 2048 + r * 16 + (k % 8) * 2):
+//          window t = chunks 2t, 2t + 1 holds codes 15t .. 15t + 14 (the
+//          16th element meets zero weights)
+//   then the packed weights (B operands in the same panel form with rows =
+//   output channels, and fp32 biases).
+constexpr int kStageWords = 45;
+constexpr int kStage = 0;
+constexpr int kA1 = kStage + kM * kStageWords * 4;
+constexpr int kA1Chunks = 6;
+constexpr int kWImg = kA1 + kA1Chunks * kChunkBytes;
+constexpr int kB1 = 0;                  // conv1: N=96 (position-in-window x 32) x K=16 f16, tap j of
+                                        // window position pp at k = 5 pp + j (LBO 96 * 16)
+constexpr int kB2 = kB1 + 2 * 1536;     // conv2: N=32 x K=160 bf16, chunk = tap * 4 + in / 8 (LBO 512)
 constexpr int kB3 = kB2 + 20 * 512;     // conv3 taps 2, 3: N=32 x K=64, chunk = (tap - 2) * 4 + in / 8
 constexpr int kB4 = kB3 + 8 * 512;      // fc1: N=64 x K=32 bf16 (LBO 1024)
 constexpr int kBias = kB4 + 4 * 1024;   // fp32: b1[32] b2[32] b3[32] b4[64] w5[64] b5
@@ -465,8 +488,8 @@ static_assert(2 * kSmem <= 228 * 1024, "two CTAs per SM");
 // TMEM (256 columns per CTA, two CTAs per SM). Accumulators are fp32, one
 // column per output; A operands held in TMEM are bf16 pairs, a K=16 slice =
 // 8 columns. Regions are reused as soon as what they held has been read:
-//   C1 conv1 accumulators, group q at 32 q                     0 .. 223
-//   A2 pooled conv1 output (bf16), position q at 16 q         0 .. 111
+//   C1 conv1 accumulators, position q at 32 q                  0 .. 223
+//   A2 conv1 output (bf16), position q at 16 q                0 .. 111
 //   C2 conv2 accumulators, position r at 128 + 32 r          128 .. 191
 //   A3 conv2 output, position r at 192 + 16 r                192 .. 223
 //   C3 conv3 accumulators                                      0 .. 31
@@ -481,7 +504,7 @@ constexpr uint32_t idesc(int fmt, int N) {
     return (1u << 4) | (uint32_t(fmt) << 7) | (uint32_t(fmt) << 10) | (uint32_t(N >> 3) << 17) |
            (uint32_t(kM >> 4) << 24);
 }
-constexpr uint32_t kIdC1 = idesc(0, 32), kIdC2 = idesc(1, 32), kIdF1 = idesc(1, 64);
+constexpr uint32_t kIdC1 = idesc(0, 96), kIdC1n = idesc(0, 32), kIdC2 = idesc(1, 32), kIdF1 = idesc(1, 64);
 
 // Shared-memory matrix descriptor: start, leading byte offset (next K chunk),
 // stride byte offset 128 (next 8 rows), version 1, no swizzle.
@@ -608,17 +631,13 @@ __device__ __forceinline__ void relu_bf16_to_tmem(uint32_t dst, const float (&v)
     st16(dst, o);
 }
 
-// A1 chunk of the first input of conv1 group q: the K=32 window starting at
-// input 8 * floor((20 q - 2) / 8), which holds the group's 20 inputs at
-// offset 6 (q even) or 2 (q odd).
-__host__ __device__ constexpr int c1_chunk(int q) { return (20 * q + 6) / 8; }  // floor((20q - 2) / 8) + 1
-static_assert(c1_chunk(0) == 0 && c1_chunk(1) == 3 && c1_chunk(6) == 15 && c1_chunk(6) + 3 < kA1Chunks,
-              "conv1 windows lie inside A1");
-
 struct InferArgs {
     const uint32_t* curve;
     size_t curve_pitch;  // words
     int groups;          // 32
+    const void* disp;    // winning disparities (U8 or U16 map)
+    size_t disp_pitch;
+    int disp_type;
     int W, H;
     float* score;
     size_t score_pitch;  // bytes
@@ -633,6 +652,7 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kBar);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kTmemSlot);
     unsigned char* A1 = smem + kA1;
+    uint32_t* stage = reinterpret_cast<uint32_t*>(smem + kStage) + m * kStageWords;  // this pixel's row
     const uint32_t sA1 = dev::smem_u32(A1), sW = dev::smem_u32(smem + kWImg);
 
     for (int k = tid; k < kWBytes / 16; k += kNT) reinterpret_cast<uint4*>(smem + kWImg)[k] = a.wimg[k];
@@ -661,7 +681,7 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
     for (int c = 0; c < 32; ++c) bias1[c] = bias[c];
     // base descriptors; every operand of a tile is a constant offset from one
     const uint64_t dA1 = sdesc(sA1, kChunkBytes);
-    const uint64_t dB1e = sdesc(sW + kB1e, 512), dB1o = sdesc(sW + kB1o, 512);
+    const uint64_t dB1 = sdesc(sW + kB1, 1536);
     const uint64_t dB2 = sdesc(sW + kB2, 512), dB3 = sdesc(sW + kB3, 512), dB4 = sdesc(sW + kB4, 1024);
 
     const int tiles_x = (a.W + kM - 1) / kM;
@@ -694,38 +714,50 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
     };
 
     uint32_t cw[32];  // this thread's curve words (32 groups of 4 disparities)
+    int dw = 0;       // and its winning disparity
     auto load_curve = [&](int t) {
         const int y = t / tiles_x, x = (t % tiles_x) * kM + m;
 #pragma unroll
         for (int g = 0; g < 32; ++g)
             cw[g] = x < a.W ? __ldg(a.curve + ((size_t)y * a.groups + g) * a.curve_pitch + x + 2) : 0xFFFFFFFFu;
+        dw = x < a.W ? winner(a.disp, a.disp_pitch, a.disp_type, x, y) : 0;
     };
 
-    // the zero chunks of A1 never change
-    for (int c : {0, 17, 18}) *reinterpret_cast<uint4*>(A1 + c * kChunkBytes + m * 16) = make_uint4(0, 0, 0, 0);
+    // the 255 padding of the staging row never changes
+    for (int k = 0; k < 3; ++k) stage[k] = 0xFFFFFFFFu;
+    for (int k = 35; k < kStageWords; ++k) stage[k] = 0xFFFFFFFFu;
 
     int t = blockIdx.x;
     if (t < tiles) load_curve(t);
     for (; t < tiles; t += gridDim.x) {
         const int y = t / tiles_x, x0 = (t % tiles_x) * kM;
-        // ---- A1 chunks 1..16 = inputs 0..127; conv1 biases into C1
+        // ---- A1: the 35 codes around the winner, 15 per K=16 window; conv1 biases into C1
 #pragma unroll
-        for (int c = 0; c < 16; ++c)
-            *reinterpret_cast<uint4*>(A1 + (1 + c) * kChunkBytes + m * 16) =
-                make_uint4(codes_f16x2(cw[2 * c], 0x4140), codes_f16x2(cw[2 * c], 0x4342),
-                           codes_f16x2(cw[2 * c + 1], 0x4140), codes_f16x2(cw[2 * c + 1], 0x4342));
+        for (int g = 0; g < 32; ++g) stage[3 + g] = cw[g];
+#pragma unroll
+        for (int t3 = 0; t3 < 3; ++t3) {
+            const int b0 = dw + 15 * t3, w0 = b0 >> 2, sh = (b0 & 3) * 8;  // row bytes b0 .. b0 + 15
+            uint32_t r[5], v[4];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) r[k] = stage[w0 + k];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) v[k] = __funnelshift_r(r[k], r[k + 1], sh);
+            unsigned char* c0 = A1 + 2 * t3 * kChunkBytes + m * 16;
+            *reinterpret_cast<uint4*>(c0) = make_uint4(codes_f16x2(v[0], 0x4140), codes_f16x2(v[0], 0x4342),
+                                                       codes_f16x2(v[1], 0x4140), codes_f16x2(v[1], 0x4342));
+            *reinterpret_cast<uint4*>(c0 + kChunkBytes) =
+                make_uint4(codes_f16x2(v[2], 0x4140), codes_f16x2(v[2], 0x4342), codes_f16x2(v[3], 0x4140),
+                           codes_f16x2(v[3], 0x4342));
+        }
 #pragma unroll
         for (int q = 0; q < 7; ++q) st32(tl + 32 * q, bias1);
         hand_to_issuer(true);
-        // ---- conv1 (+ 4-wide sum pooling): group q = one K=32 window, 2 MMAs
+        // ---- conv1: window t = positions 3t .. 3t + 2 (N = 96; the last window N = 32)
         if (warp == 0) {  // MMA issue: whole warp, one elected lane
             fence_after();
-#pragma unroll
-            for (int q = 0; q < 7; ++q)
-#pragma unroll
-                for (int h = 0; h < 2; ++h)
-                    mma_ss(tm + 32 * q, dplus(dA1, (c1_chunk(q) + 2 * h) * kChunkBytes),
-                           dplus((q & 1) ? dB1o : dB1e, 2 * h * 512), kIdC1);
+            mma_ss(tm, dA1, dB1, kIdC1);
+            mma_ss(tm + 96, dplus(dA1, 2 * kChunkBytes), dB1, kIdC1);
+            mma_ss(tm + 192, dplus(dA1, 4 * kChunkBytes), dB1, kIdC1n);
             commit_to(0);
         }
         if (t + (int)gridDim.x < tiles) load_curve(t + gridDim.x);  // next tile, behind the MMAs
@@ -912,18 +944,17 @@ int pack_weights(ConfNetHandle* h) {
     std::vector<unsigned char> img(kWBytes, 0);
     auto put16 = [&](int off, uint16_t v) { std::memcpy(&img[off], &v, 2); };
     auto bf = [&](int idx) { return bf16_bits_to_f32(f32_to_bf16_bits(p[idx])); };
-    // B1e / B1o: rows = channel, K = 32-wide window of a conv1 group: the
-    // group's 20 inputs (4 positions x 5 taps, no overlap at stride 5) at
-    // offset 6 (even groups) or 2 (odd groups), tap t % 5 at offset + t
-    for (int odd = 0; odd < 2; ++odd)
+    // B1: rows = pp * 32 + channel (pp = position in a conv1 window), tap j
+    // of position pp at K = 5 pp + j (K = 15 is zero); 2 chunks of 96 rows
+    for (int pp = 0; pp < 3; ++pp)
         for (int ch = 0; ch < 32; ++ch)
-            for (int t = 0; t < 20; ++t) {
-                const int k = t + (odd ? 2 : 6), j = t % 5;
+            for (int j = 0; j < 5; ++j) {
+                const int k = 5 * pp + j, n = pp * 32 + ch;
                 uint16_t hb;
                 if (!bf16_to_f16_exact(bf(kOffW1 + ch * 5 + j), &hb))
                     return fail(CT_EINVAL, "conv1 weight %d (%g) is not exact in f16", ch * 5 + j,
                                 double(bf(kOffW1 + ch * 5 + j)));
-                put16((odd ? kB1o : kB1e) + (k / 8) * 512 + ch * 16 + (k % 8) * 2, hb);
+                put16(kB1 + (k / 8) * 1536 + n * 16 + (k % 8) * 2, hb);
             }
     // B2: rows o, K = tap * 32 + in; B3: rows o, K = (tap - 2) * 32 + in, taps 2, 3
     for (int o = 0; o < 32; ++o)
@@ -1078,20 +1109,29 @@ int ct_confnet_get_params(ct_handle* hh, float* params, int32_t n) {
     return CT_OK;
 }
 
-int ct_confnet_gather(ct_handle* hh, uint8_t* samples, const ct_curves* curves, const int32_t* xy, int32_t n,
-                      ct_stream stream) {
+// The disparity map must match the curve volume's size; U8 or U16 encoding.
+static int check_disp_for(const ct_image* disp, const ct_curves* curves) {
+    if (int rc = check_image(disp, "disp", (1u << CT_PIX_U8) | (1u << CT_PIX_U16))) return rc;
+    if (disp->width != curves->width || disp->height != curves->height)
+        return fail(CT_EFORMAT, "disparity map and curve volume differ in size");
+    return CT_OK;
+}
+
+int ct_confnet_gather(ct_handle* hh, uint8_t* samples, const ct_curves* curves, const ct_image* disp,
+                      const int32_t* xy, int32_t n, ct_stream stream) {
     clear_error();
     auto* h = as_net(hh);
     if (!h || !h->configured) return fail(CT_ESTATE, "not a configured confidence-net handle");
     if (!samples || !curves || !curves->ptr || !xy || n < 0) return fail(CT_EINVAL, "null argument");
     if (curves->disp_count != kLen) return fail(CT_EFORMAT, "the confidence net reads curves of 128 disparities");
+    if (int rc = check_disp_for(disp, curves)) return rc;
     if (n == 0) return CT_OK;
     if (int rc = use_device(h->device)) return rc;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     h->last_stream = s;
     gather_kernel<<<(n + 7) / 8, 256, 0, s>>>(samples, static_cast<const uint32_t*>(curves->ptr),
-                                              curves->pitch_bytes / 4, kLen / 4, curves->width, curves->height, xy,
-                                              n, h->d_status);
+                                              curves->pitch_bytes / 4, curves->width, curves->height, disp->ptr,
+                                              disp->pitch_bytes, disp->type, xy, n, h->d_status);
     CT_LAUNCH_CHECK();
     return CT_OK;
 }
@@ -1147,7 +1187,8 @@ int ct_confnet_scores(ct_handle* hh, float* scores, const uint8_t* samples, int3
     return run_train_graph(h, samples, nullptr, n, scores, s);
 }
 
-int ct_confnet_infer(ct_handle* hh, const ct_image* score, const ct_curves* curves, ct_stream stream) {
+int ct_confnet_infer(ct_handle* hh, const ct_image* score, const ct_curves* curves, const ct_image* disp,
+                     ct_stream stream) {
     clear_error();
     auto* h = as_net(hh);
     if (!h || !h->configured) return fail(CT_ESTATE, "not a configured confidence-net handle");
@@ -1156,6 +1197,7 @@ int ct_confnet_infer(ct_handle* hh, const ct_image* score, const ct_curves* curv
     if (curves->disp_count != kLen) return fail(CT_EFORMAT, "the confidence net reads curves of 128 disparities");
     if (curves->width != score->width || curves->height != score->height)
         return fail(CT_EFORMAT, "score map and curve volume differ in size");
+    if (int rc = check_disp_for(disp, curves)) return rc;
     if (reinterpret_cast<uintptr_t>(curves->ptr) % 16 || curves->pitch_bytes % 16 ||
         curves->pitch_bytes < 4 * (size_t(curves->width) + 2))
         return fail(CT_EINVAL, "curve volume needs a 16-byte aligned pointer and pitch >= 4 * (width + 2)");
@@ -1170,6 +1212,9 @@ int ct_confnet_infer(ct_handle* hh, const ct_image* score, const ct_curves* curv
     a.curve = static_cast<const uint32_t*>(curves->ptr);
     a.curve_pitch = curves->pitch_bytes / 4;
     a.groups = kLen / 4;
+    a.disp = disp->ptr;
+    a.disp_pitch = disp->pitch_bytes;
+    a.disp_type = disp->type;
     a.W = score->width;
     a.H = score->height;
     a.score = static_cast<float*>(score->ptr);

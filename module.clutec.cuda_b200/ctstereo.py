@@ -146,11 +146,11 @@ def _declare(L: C.CDLL) -> None:
         "ct_confnet_init": [H, C.c_uint64],
         "ct_confnet_set_params": [H, C.c_void_p, C.c_int32],
         "ct_confnet_get_params": [H, C.c_void_p, C.c_int32],
-        "ct_confnet_gather": [H, C.c_void_p, P(ct_curves), C.c_void_p, C.c_int32, C.c_void_p],
+        "ct_confnet_gather": [H, C.c_void_p, P(ct_curves), img, C.c_void_p, C.c_int32, C.c_void_p],
         "ct_confnet_loss_grad": [H, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p],
         "ct_confnet_train_step": [H, C.c_void_p, C.c_void_p, C.c_int32, C.c_float, C.c_void_p, C.c_void_p],
         "ct_confnet_scores": [H, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p],
-        "ct_confnet_infer": [H, img, P(ct_curves), C.c_void_p],
+        "ct_confnet_infer": [H, img, P(ct_curves), img, C.c_void_p],
         "ct_bm_sad_create": [P(H)],
         "ct_bm_sad_configure": [H, C.c_int32, fmt, P(ct_sad_params)],
         "ct_bm_sad_process": [H, img, img, img, C.c_void_p],
@@ -467,10 +467,11 @@ class ConfNet(_Driver):
         check(lib().ct_confnet_get_params(self._h, p.ctypes.data, p.size))
         return p
 
-    def gather(self, samples, curves: "CurveVolume", xy, stream=None):
-        """samples: (n, 128) uint8 CUDA tensor; xy: (n, 2) int32 CUDA tensor."""
-        check(lib().ct_confnet_gather(self._h, samples.data_ptr(), C.byref(curves.desc()), xy.data_ptr(),
-                                      xy.shape[0], _stream(stream)))
+    def gather(self, samples, curves: "CurveVolume", disp, xy, stream=None):
+        """samples: (n, 128) uint8 CUDA tensor of re-centred curves; disp: the
+        winner map (uint8 / int16); xy: (n, 2) int32 CUDA tensor."""
+        check(lib().ct_confnet_gather(self._h, samples.data_ptr(), C.byref(curves.desc()), _img_ref(disp),
+                                      xy.data_ptr(), xy.shape[0], _stream(stream)))
 
     def loss_grad(self, samples, labels, grad=None, loss=None, stream=None):
         check(lib().ct_confnet_loss_grad(self._h, samples.data_ptr(), labels.data_ptr(), samples.shape[0],
@@ -485,8 +486,10 @@ class ConfNet(_Driver):
         check(lib().ct_confnet_scores(self._h, out.data_ptr(), samples.data_ptr(), samples.shape[0],
                                       _stream(stream)))
 
-    def infer(self, score, curves: "CurveVolume", stream=None):
-        check(lib().ct_confnet_infer(self._h, _img_ref(score), C.byref(curves.desc()), _stream(stream)))
+    def infer(self, score, curves: "CurveVolume", disp, stream=None):
+        """Score map (float32) of a curve volume; disp: its winner map."""
+        check(lib().ct_confnet_infer(self._h, _img_ref(score), C.byref(curves.desc()), _img_ref(disp),
+                                     _stream(stream)))
 
 
 def census_match_static(disp, left, right, disp_count: int, left_to_right: bool = True, device_status=None,

@@ -5,13 +5,14 @@ kernels of the confidence net (csrc/confnet_*.cu). Only tests/ and the
 cpu_baseline leg of bench.py import it; the product never does.
 
 The network reads a pixel's uint8 census cost curve c[0..127] (aggregated
-5x5 Hamming cost >> 3, 0..196; 255 for unsearchable disparities)
-and returns a validity logit. Its numerics are defined exactly as the GPU
-runs them:
+5x5 Hamming cost >> 3, 0..196; 255 for unsearchable disparities), re-centred
+on the pixel's winner-take-all disparity d: the sample is the 128-long
+r[k] = c[d - 64 + k] (255 outside 0..127), so r[64] is the winning cost. The
+convolution stack reads its 35 central codes x[k] = r[52 + k], i.e. the
+disparities d - 12 .. d + 22, and returns a validity logit. Its numerics are
+defined exactly as the GPU runs them:
 
-  conv1  1 -> 32, k=5, stride 5, pad 2 : z1[p,o] = sum_j w1[o,j] c[5p+j-2]          p = 0..27
-         (positions 26, 27 lie wholly in the padding and are 0)
-  pool   sum over 4 positions, plus bias: m1[q,o] = b1[o] + sum_{k<4} z1[4q+k,o]  q = 0..6
+  conv1  1 -> 32, k=5, stride 5        : z1[p,o] = b1[o] + sum_j w1[o,j] x[5p+j]     p = 0..6
          ReLU, rounded to bf16 -> a1[7,32]
   conv2 32 -> 32, k=5, stride 3, pad 1 : z2[r,o] = b2[o] + sum_{j,i} w2[o,i,j] a1[3r+j-1,i]  r = 0, 1
          ReLU, rounded to bf16 -> a2[2,32]
@@ -34,6 +35,17 @@ SHAPES = [("w1", (32, 5)), ("b1", (32,)), ("w2", (32, 32, 5)), ("b2", (32,)),
 WEIGHTS = {"w1", "w2", "w3", "w4", "w5"}
 N_PARAMS = sum(int(np.prod(s)) for _, s in SHAPES)  # 12673
 CURVE_LEN = 128
+CROP_LO = 52   # first code of r the convolutions read (disparity d - 12)
+CROP_LEN = 35
+
+
+def recenter(curve, d):
+    """(n, 128) curves and (n,) winning disparities -> (n, 128) samples
+    r[k] = curve[d - 64 + k], 255 outside the curve."""
+    curve = np.asarray(curve)
+    idx = np.asarray(d, np.int64)[:, None] - 64 + np.arange(128)[None, :]
+    ok = (idx >= 0) & (idx < 128)
+    return np.where(ok, np.take_along_axis(curve, np.clip(idx, 0, 127), 1), 255).astype(np.uint8)
 
 
 def unflatten(flat):
@@ -77,17 +89,17 @@ def _conv_idx(n_out, stride, pad, n_in, k=5):
 
 
 def forward(curves, flat, emulate=True):
-    """curves: (n, 128) uint8. Returns (logits, cache). emulate=False skips
-    the bf16 roundings (plain float64 network, for finite differences)."""
+    """curves: (n, 128) uint8 re-centred samples (see recenter). Returns
+    (logits, cache). emulate=False skips the bf16 roundings (plain float64
+    network, for finite differences)."""
     p = unflatten(np.asarray(flat, np.float64))
     rw = bf16 if emulate else (lambda a: np.asarray(a, np.float64))
     w = {k: (rw(v) if k in WEIGHTS else np.asarray(v, np.float64)) for k, v in p.items()}
     x = np.asarray(curves, np.float64)
     n = x.shape[0]
-    i1, ok1 = _conv_idx(28, 5, 2, 128)
-    X1 = x[:, i1] * ok1                                       # (n, 28, 5)
-    z1 = np.einsum("npj,oj->npo", X1, w["w1"])                # (n, 28, 32)
-    m1 = z1.reshape(n, 7, 4, 32).sum(axis=2) + w["b1"]        # (n, 7, 32)
+    i1 = CROP_LO + 5 * np.arange(7)[:, None] + np.arange(5)[None, :]
+    X1 = x[:, i1]                                             # (n, 7, 5)
+    m1 = np.einsum("npj,oj->npo", X1, w["w1"]) + w["b1"]      # (n, 7, 32)
     a1 = rw(np.maximum(m1, 0.0))
     i2, ok2 = _conv_idx(2, 3, 1, 7)
     A1 = a1[:, i2, :] * ok2[None, :, :, None]                 # (n, 2, 5, 32)
@@ -100,7 +112,7 @@ def forward(curves, flat, emulate=True):
     z4 = a3 @ w["w4"].T + w["b4"]                             # (n, 64)
     a4 = np.maximum(z4, 0.0)
     logit = a4 @ w["w5"] + w["b5"][0]
-    cache = dict(w=w, X1=X1, z1=z1, m1=m1, A1=A1, z2=z2, A2=A2, z3=z3, a3=a3, z4=z4, a4=a4,
+    cache = dict(w=w, X1=X1, m1=m1, A1=A1, z2=z2, A2=A2, z3=z3, a3=a3, z4=z4, a4=a4,
                  i2=i2, ok2=ok2, i3=i3, ok3=ok3, n=n)
     return logit, cache
 
@@ -137,9 +149,8 @@ def loss_and_grad(curves, labels, flat, emulate=True):
             if c["ok2"][r, j]:
                 da1[:, c["i2"][r, j], :] += dA1[:, r, j, :]
     dm1 = da1 * (c["m1"] > 0)
-    dz1 = np.repeat(dm1, 4, axis=1)                           # every pooled position (n, 28, 32)
     g["b1"] = dm1.sum((0, 1))
-    g["w1"] = np.einsum("npo,npj->oj", dz1, c["X1"])
+    g["w1"] = np.einsum("npo,npj->oj", dm1, c["X1"])
     return loss, flatten(g)
 
 

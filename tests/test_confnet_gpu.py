@@ -40,27 +40,40 @@ def test_curves_bit_exact(ct, oracle, cuda, W, H, D, kind, lr, tuning):
     np.testing.assert_array_equal(disp.view(np.uint16), oracle.to_u16(want_d))
 
 
-def test_gather(ct, oracle, cuda):
+def _winners(d):
+    return np.where(d >= 0, d, 0)
+
+
+@pytest.mark.parametrize("dtype", [torch.int16, torch.uint8])
+def test_gather_recentres(ct, oracle, cuda, dtype):
     W, H, D = 200, 64, 128
     L, R, _, _ = ct.synth_pair(1, 5, W, H, D - 1)
-    cv, _ = curves_of(ct, cuda, L, R, D)
-    _, _, want_c = oracle.match_census(L, R, D, 2, True, curve_shift=3)
+    m = ct.BlockMatcherCensus()
+    m.configure(0, W, H, D)
+    cv = ct.CurveVolume(W, H, D, cuda)
+    disp = ct.alloc_image(H, W, dtype, cuda)
+    m.process_curves(disp, cv, to_dev(L, cuda), to_dev(R, cuda))
+    want_d, _, want_c = oracle.match_census(L, R, D, 2, True, curve_shift=3)
     r = np.random.default_rng(1)
-    xy = np.stack([r.integers(0, W, 777), r.integers(0, H, 777)], 1).astype(np.int32)
+    xs, ys = r.integers(0, W, 777), r.integers(0, H, 777)
+    xy = np.stack([xs, ys], 1).astype(np.int32)
     net = ct.ConfNet()
     net.configure(0, 1024)
     samples = torch.empty((777, 128), dtype=torch.uint8, device=cuda)
-    net.gather(samples, cv, torch.from_numpy(xy).to(cuda))
+    net.gather(samples, cv, disp, torch.from_numpy(xy).to(cuda))
     torch.cuda.synchronize()
-    np.testing.assert_array_equal(samples.cpu().numpy(), want_c[xy[:, 1], xy[:, 0]])
+    assert net.device_status() == 0
+    want = cn.recenter(want_c[ys, xs], _winners(want_d[ys, xs]))
+    np.testing.assert_array_equal(samples.cpu().numpy(), want)
 
 
 def _real_samples(ct, oracle, n, seed):
     W, H, D = 333, 111, 128
     L, R, _, _ = ct.synth_pair(1, seed, W, H, D - 1)
-    _, _, curve = oracle.match_census(L, R, D, 2, True, curve_shift=3)
+    d, _, curve = oracle.match_census(L, R, D, 2, True, curve_shift=3)
     r = np.random.default_rng(seed)
-    return curve[r.integers(0, H, n), r.integers(0, W, n)]
+    ys, xs = r.integers(0, H, n), r.integers(0, W, n)
+    return cn.recenter(curve[ys, xs], _winners(d[ys, xs]))
 
 
 def _params(seed):
@@ -130,17 +143,21 @@ def test_tensor_core_inference_matches_training_forward(ct, oracle, cuda, W, H):
     D = 128
     L, R, _, _ = ct.synth_pair(2, 21 + W, W, max(H, 16), D - 1)
     L, R = np.ascontiguousarray(L[:H]), np.ascontiguousarray(R[:H])
-    cv, _ = curves_of(ct, cuda, L, R, D)
+    m = ct.BlockMatcherCensus()
+    m.configure(0, W, H, D)
+    cv = ct.CurveVolume(W, H, D, cuda)
+    disp = ct.alloc_image(H, W, torch.int16, cuda)
+    m.process_curves(disp, cv, to_dev(L, cuda), to_dev(R, cuda))
     net = ct.ConfNet()
     net.configure(0, W * H)
     p = _params(4)
     net.set_params(p)
     score = ct.alloc_image(H, W, torch.float32, cuda)
     score.fill_(-1.0)
-    net.infer(score, cv)
+    net.infer(score, cv, disp)
     xy = np.stack(np.meshgrid(np.arange(W), np.arange(H)), -1).reshape(-1, 2).astype(np.int32)
     samples = torch.empty((W * H, 128), dtype=torch.uint8, device=cuda)
-    net.gather(samples, cv, torch.from_numpy(xy).to(cuda))
+    net.gather(samples, cv, disp, torch.from_numpy(xy).to(cuda))
     ref = torch.empty(W * H, dtype=torch.float32, device=cuda)
     net.scores(ref, samples)
     torch.cuda.synchronize()

@@ -40,3 +40,11 @@ def test_auc_hand_cases():
     assert cn.auc([0, 0, 1, 1], [1, 1, 0, 0]) == 1.0
     assert cn.auc([1, 1, 1, 1], [1, 1, 0, 0]) == 0.5   # all ties
     assert cn.auc([0, 1, 0, 1], [1, 0, 0, 1]) == 0.5
+
+
+def test_recenter_places_the_winner_at_64():
+    c = np.arange(128, dtype=np.uint8)[None, :].repeat(3, 0)
+    r = cn.recenter(c, np.array([0, 64, 127]))
+    assert r[0, 64] == 0 and (r[0, :64] == 255).all() and r[0, 127] == 63
+    np.testing.assert_array_equal(r[1], np.arange(128))
+    assert r[2, 64] == 127 and (r[2, 65:] == 255).all() and r[2, 0] == 63
