@@ -167,8 +167,8 @@ int ct_bm_census_match_desc(ct_handle* h, const ct_image* disp, const ct_image* 
 /* Cost-curve volume: the matcher's aggregated cost of every (pixel,
  * disparity), one byte each, the input of the learned confidence net
  * (ct_confnet_*). Code = 5x5 Hamming sum >> 3 (0..196); 255 for a disparity
- * whose match window leaves the image and for all disparities of a border
- * pixel (within 2 of the image edge). Layout: groups g = 0 .. ceil(D/4) - 1
+ * whose match window leaves the image. Border pixels (within 2 of the image
+ * edge) have no disparity and unspecified codes. Layout: groups g = 0 .. ceil(D/4) - 1
  * of 4 disparities; row (y, g) starts at ptr + (y * ceil(D/4) + g) *
  * pitch_bytes and holds one 32-bit word per pixel, word x + 2 for column x,
  * whose byte k (little-endian) is the code of disparity 4g + k. pitch_bytes

@@ -106,8 +106,8 @@ struct MatchArgs {
     // 32-bit word per pixel, word x + 2 for column x, whose bytes are the
     // codes of disparities 4g .. 4g + 3 (byte k = disparity 4g + k).
     // Code = aggregated cost >> 3 (at most 1575 >> 3 = 196); 255 for a
-    // disparity whose match window leaves the image and for every disparity of
-    // a border pixel.
+    // disparity whose match window leaves the image. Border pixels (within 2
+    // of the image edge, which have no disparity) get unspecified codes.
     uint32_t* curve;
     size_t curve_pitch;  // 32-bit words per row, a multiple of 4
     int curve_groups;    // ceil(D / 4)
@@ -240,13 +240,10 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
     // multiple of 4); lanes 0 and 31 skip their halo columns.
     auto store_curve = [&](const uint32_t (&C)[kCPT][NP], int oy) {
         const int y = y0 + oy;
-        const bool rowv = y >= kAR && y < a.H - kAR;
         constexpr int NG = DPW / 4;
         uint32_t wv[kCPT][NG];
 #pragma unroll
         for (int c = 0; c < kCPT; ++c) {
-            const int x = xs + 4 * lane + c;
-            const bool pv = rowv && x >= kAR && x < a.W - kAR;
 #pragma unroll
             for (int q = 0; q < NG; ++q) {
                 // C < 2048 per 16-bit half, so byte 0 and byte 2 of C >> 3 are
@@ -257,7 +254,7 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
                     const int nvalid = min(max(lim[c] - (dw + 4 * q) + 1, 0), 4);
                     w |= nvalid >= 4 ? 0u : (0xFFFFFFFFu << (8 * nvalid));
                 }
-                wv[c][q] = pv ? w : 0xFFFFFFFFu;
+                wv[c][q] = w;
             }
         }
 #pragma unroll

@@ -457,17 +457,20 @@ constexpr int kM = 128;   // pixels per tile = MMA M
 constexpr int kChunkBytes = kM * 16;  // one K-chunk (8 elements) of the 128-row A1 operand
 
 // Shared memory:
-//   stage  each pixel's curve bytes in a row of kStageWords words: 3 words of
-//          255, the 32 curve words, 10 words of 255, so the 35 codes the
-//          convolutions read (curve bytes d - 12 .. d + 22) are row bytes
-//          d .. d + 34 (odd row stride: conflict-free column access)
+//   stage  each pixel's 10 curve words around its winner in a row of
+//          kStageWords words: words g0 .. g0 + 9 of the curve (g0 = floor((d -
+//          12) / 4); words outside the curve read 255), then 3 words of 255,
+//          so the 35 codes the convolutions read (curve bytes d - 12 .. d +
+//          22) start at row byte (d - 12) - 4 g0 (odd row stride:
+//          conflict-free column access)
 //   A1     conv1 operand, f16, K-major without swizzle in K-chunk panels
 //          (element (pixel r, k) at (k / 8) * 2048 + r * 16 + (k % 8) * 2):
 //          window t = chunks 2t, 2t + 1 holds codes 15t .. 15t + 14 (the
 //          16th element meets zero weights)
 //   then the packed weights (B operands in the same panel form with rows =
 //   output channels, and fp32 biases).
-constexpr int kStageWords = 45;
+constexpr int kCurveWords = 10;  // curve words loaded per pixel (40 bytes cover the 35 codes)
+constexpr int kStageWords = 13;
 constexpr int kStage = 0;
 constexpr int kA1 = kStage + kM * kStageWords * 4;
 constexpr int kA1Chunks = 6;
@@ -713,42 +716,65 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
         __syncthreads();
     };
 
-    uint32_t cw[32];  // this thread's curve words (32 groups of 4 disparities)
-    int dw = 0;       // and its winning disparity
-    auto load_curve = [&](int t) {
+    // this thread's curve words around its winner: groups g0 .. g0 + 9 of 4
+    // disparities; the lanes of a warp mostly share g0 (disparities are
+    // piecewise smooth), so the loads stay close to coalesced
+    // The winner of a tile is loaded one tile before its curve words, so the
+    // curve loads never wait on it.
+    uint32_t cw[kCurveWords];
+    int c0 = 0;  // byte of the first of the 35 codes within cw
+    auto load_winner = [&](int t) {
         const int y = t / tiles_x, x = (t % tiles_x) * kM + m;
+        return x < a.W ? winner(a.disp, a.disp_pitch, a.disp_type, x, y) : 0;
+    };
+    auto load_curve = [&](int t, int d) {
+        const int y = t / tiles_x, x = (t % tiles_x) * kM + m;
+        const int g0 = (d - 12) >> 2;  // floor
+        c0 = (d - 12) - 4 * g0;
 #pragma unroll
-        for (int g = 0; g < 32; ++g)
-            cw[g] = x < a.W ? __ldg(a.curve + ((size_t)y * a.groups + g) * a.curve_pitch + x + 2) : 0xFFFFFFFFu;
-        dw = x < a.W ? winner(a.disp, a.disp_pitch, a.disp_type, x, y) : 0;
+        for (int k = 0; k < kCurveWords; ++k) {
+            const int g = g0 + k;
+            cw[k] = (x < a.W && g >= 0 && g < a.groups)
+                        ? __ldg(a.curve + ((size_t)y * a.groups + g) * a.curve_pitch + x + 2)
+                        : 0xFFFFFFFFu;
+        }
     };
 
     // the 255 padding of the staging row never changes
-    for (int k = 0; k < 3; ++k) stage[k] = 0xFFFFFFFFu;
-    for (int k = 35; k < kStageWords; ++k) stage[k] = 0xFFFFFFFFu;
+    for (int k = kCurveWords; k < kStageWords; ++k) stage[k] = 0xFFFFFFFFu;
 
-    int t = blockIdx.x;
-    if (t < tiles) load_curve(t);
-    for (; t < tiles; t += gridDim.x) {
-        const int y = t / tiles_x, x0 = (t % tiles_x) * kM;
-        // ---- A1: the 35 codes around the winner, 15 per K=16 window; conv1 biases into C1
+    // A1 of the tile whose curve words are in cw: the 35 codes around the
+    // winner, 15 per K=16 window
+    auto build_a1 = [&]() {
 #pragma unroll
-        for (int g = 0; g < 32; ++g) stage[3 + g] = cw[g];
+        for (int k = 0; k < kCurveWords; ++k) stage[k] = cw[k];
 #pragma unroll
         for (int t3 = 0; t3 < 3; ++t3) {
-            const int b0 = dw + 15 * t3, w0 = b0 >> 2, sh = (b0 & 3) * 8;  // row bytes b0 .. b0 + 15
+            const int b0 = c0 + 15 * t3, w0 = b0 >> 2, sh = (b0 & 3) * 8;  // row bytes b0 .. b0 + 15
             uint32_t r[5], v[4];
 #pragma unroll
             for (int k = 0; k < 5; ++k) r[k] = stage[w0 + k];
 #pragma unroll
             for (int k = 0; k < 4; ++k) v[k] = __funnelshift_r(r[k], r[k + 1], sh);
-            unsigned char* c0 = A1 + 2 * t3 * kChunkBytes + m * 16;
-            *reinterpret_cast<uint4*>(c0) = make_uint4(codes_f16x2(v[0], 0x4140), codes_f16x2(v[0], 0x4342),
-                                                       codes_f16x2(v[1], 0x4140), codes_f16x2(v[1], 0x4342));
-            *reinterpret_cast<uint4*>(c0 + kChunkBytes) =
+            unsigned char* dst = A1 + 2 * t3 * kChunkBytes + m * 16;
+            *reinterpret_cast<uint4*>(dst) = make_uint4(codes_f16x2(v[0], 0x4140), codes_f16x2(v[0], 0x4342),
+                                                        codes_f16x2(v[1], 0x4140), codes_f16x2(v[1], 0x4342));
+            *reinterpret_cast<uint4*>(dst + kChunkBytes) =
                 make_uint4(codes_f16x2(v[2], 0x4140), codes_f16x2(v[2], 0x4342), codes_f16x2(v[3], 0x4140),
                            codes_f16x2(v[3], 0x4342));
         }
+    };
+
+    int t = blockIdx.x;
+    int d_next = 0;
+    if (t < tiles) {
+        load_curve(t, load_winner(t));
+        build_a1();
+    }
+    if (t + (int)gridDim.x < tiles) d_next = load_winner(t + gridDim.x);
+    for (; t < tiles; t += gridDim.x) {
+        const int y = t / tiles_x, x0 = (t % tiles_x) * kM;
+        // ---- conv1 biases into C1 (A1 was built while the previous tile's fc1 ran)
 #pragma unroll
         for (int q = 0; q < 7; ++q) st32(tl + 32 * q, bias1);
         hand_to_issuer(true);
@@ -760,7 +786,8 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
             mma_ss(tm + 192, dplus(dA1, 4 * kChunkBytes), dB1, kIdC1n);
             commit_to(0);
         }
-        if (t + (int)gridDim.x < tiles) load_curve(t + gridDim.x);  // next tile, behind the MMAs
+        if (t + (int)gridDim.x < tiles) load_curve(t + gridDim.x, d_next);  // next tile, behind the MMAs
+        if (t + 2 * (int)gridDim.x < tiles) d_next = load_winner(t + 2 * gridDim.x);
         if (__syncthreads_or(!wait_bar(0))) { failed = true; break; }
         fence_after();
         // ---- conv1 epilogue: A2 position q (bf16) over the consumed C1 columns
@@ -831,6 +858,9 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
             for (int h = 0; h < 2; ++h) mma_ts(tm + kC4, tm + kA4 + 8 * h, dplus(dB4, 2 * h * 1024), kIdF1);
             commit_to(1);
         }
+        // the next tile's A1 while fc1 runs (this tile's conv1 MMAs, the only
+        // readers of A1, completed before the conv1 epilogue)
+        if (t + (int)gridDim.x < tiles) build_a1();
         if (__syncthreads_or(!wait_bar(1))) { failed = true; break; }
         fence_after();
         // ---- fc1 epilogue + fc2
