@@ -52,10 +52,13 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="census1080",
-                    choices=["census1080", "sad640", "ncc1080", "aw1440", "batch64"],
+                    choices=["census1080", "sad640", "ncc1080", "aw1440", "batch64", "confnet1080"],
                     help="census1080 (default, the headline) or another configuration, one JSON line each")
-    ap.add_argument("--profile", default=None, choices=["census_match"],
-                    help="run the named kernel twice on the 1080p D=128 pair and exit (for ncu captures)")
+    ap.add_argument("--eval-pairs", type=int, default=None,
+                    help="held-out 1080p pairs for the confidence-net AUC (default 4 in the census line, 24 in confnet1080)")
+    ap.add_argument("--profile", default=None, choices=["census_match", "confnet_infer", "pipelines"],
+                    help="for ncu captures on the 1080p D=128 pair, then exit: census_match or confnet_infer = that "
+                         "kernel twice; pipelines = the plain L-R pipeline 3x, then the learned one 3x")
     return ap.parse_args()
 
 
@@ -175,6 +178,69 @@ def traffic_from_profile():
     return None
 
 
+def confnet_compare(ct, dev, stream, m, dL, dR, hL, hR, flush, steps, eval_pairs, device_index):
+    """The learned-confidence pipeline against the plain left-right pipeline
+    on the resident pair, both producing the same checked U8 map:
+      plain   ct_bm_census_process_lr (census x2, L->R, R->L, cross-check)
+      learned ct_bm_census_process_curves (census x2, L->R + cost curves) +
+              ct_confnet_infer (checked map = L->R with low scores marked)
+    Device time and end-to-end time (pinned H2D of both images + D2H of the
+    checked map in every step), and the invalid-pixel AUC of both methods
+    over held-out 1080p pairs with the committed weights."""
+    import torch
+    import confnet_train as T
+    net = ct.ConfNet()
+    net.configure(device_index, 16)
+    net.set_params(T.load_weights())
+    cv = ct.CurveVolume(W_, H_, D_, dev)
+    disp = ct.alloc_image(H_, W_, torch.uint8, dev)
+    ck_plain = ct.alloc_image(H_, W_, torch.uint8, dev)
+    ck_learned = ct.alloc_image(H_, W_, torch.uint8, dev)
+    hOut = torch.empty((H_, W_), dtype=torch.uint8).pin_memory()
+
+    def plain():
+        m.process_lr(dL, dR, disp_checked=ck_plain, tol=1, stream=stream)
+
+    def learned():
+        m.process_curves(disp, cv, dL, dR, stream=stream)
+        net.infer(None, cv, disp, checked=ck_learned, threshold=0.5, stream=stream)
+
+    def timed(fn, out=None):
+        for _ in range(3):
+            flush()
+            fn()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        torch.cuda.synchronize(dev)
+        for k in range(steps):
+            flush()
+            ev[k][0].record(stream)
+            if out is not None:
+                dL.copy_(hL, non_blocking=True)
+                dR.copy_(hR, non_blocking=True)
+            fn()
+            if out is not None:
+                hOut.copy_(out, non_blocking=True)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize(dev)
+        return sum(a.elapsed_time(b) for a, b in ev) / steps
+
+    res = {"plain_ms": timed(plain), "learned_ms": timed(learned),
+           "plain_e2e_ms": timed(plain, ck_plain), "learned_e2e_ms": timed(learned, ck_learned)}
+    if m.device_status() != 0 or net.device_status() != 0:
+        raise RuntimeError("device status set in the confidence-net comparison")
+    auc = T.evaluate({"net": net}, device_index, eval_pairs, W_, H_)
+    res = {k: round(v, 4) for k, v in res.items()}
+    res.update({"speedup": round(res["plain_ms"] / res["learned_ms"], 3),
+                "speedup_e2e": round(res["plain_e2e_ms"] / res["learned_e2e_ms"], 3),
+                "auc_net": round(auc["net"], 4), "auc_lr_check": round(auc["lr_check"], 4),
+                "lr_check_tpr": round(auc["lr_check_tpr"], 4), "lr_check_fpr": round(auc["lr_check_fpr"], 5),
+                "invalid_fraction": round(auc["invalid_fraction"], 4), "eval_pairs": auc["pairs"],
+                "eval_pixels": auc["pixels"], "threshold": 0.5,
+                "weights": "module.clutec.cuda_b200/confnet_census128.f32 (2000 seeded training pairs)",
+                "launches_learned": 4, "launches_plain": 5})
+    return res
+
+
 def run_ours(args):
     import torch
     import ctstereo as ct
@@ -288,6 +354,8 @@ def run_ours(args):
             eev[k][1].record(stream)
         barrier()
         e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in eev) / args.steps)
+        conf = confnet_compare(ct, dev, stream, m, dL, dR, hL, hR, flush, args.steps,
+                               args.eval_pairs or 4, local) if rank == 0 else None
     clocks = clk.summary()
 
     status = m.device_status()
@@ -339,6 +407,7 @@ def run_ours(args):
         "gpu_launches": launches * args.steps,
         "clocks": clocks,
         "parity_rank0": parity,
+        "confnet": conf,
     }
     if rank == 0:
         cpu_ms, cores = cpu_pipeline_time(L, R, 3)
@@ -353,10 +422,43 @@ def run_ours(args):
 
 
 def run_profile(args):
-    """Two launches of one kernel on the default workload, nothing else."""
+    """Two launches of one kernel on the default workload, nothing else (or
+    the two pipelines, three times each)."""
     import torch
     import ctstereo as ct
     dev = torch.device("cuda", 0)
+    if args.profile in ("confnet_infer", "pipelines"):
+        import confnet_train as T
+        L, R, _, _ = ct.synth_pair(1, SEED, W_, H_, D_ - 1)
+        dL = ct.alloc_image(H_, W_, torch.uint8, dev)
+        dR = ct.alloc_image(H_, W_, torch.uint8, dev)
+        dL.copy_(torch.from_numpy(L))
+        dR.copy_(torch.from_numpy(R))
+        m = ct.BlockMatcherCensus()
+        m.configure(0, W_, H_, D_)
+        m.set_tuning(126, 4)
+        net = ct.ConfNet()
+        net.configure(0, 16)
+        net.set_params(T.load_weights())
+        cv = ct.CurveVolume(W_, H_, D_, dev)
+        disp = ct.alloc_image(H_, W_, torch.uint8, dev)
+        ck = ct.alloc_image(H_, W_, torch.uint8, dev)
+        m.process_curves(disp, cv, dL, dR)
+        net.infer(None, cv, disp, checked=ck)  # packs the weights
+        torch.cuda.synchronize()
+        if args.profile == "confnet_infer":
+            for _ in range(2):
+                net.infer(None, cv, disp, checked=ck)
+        else:
+            for _ in range(3):
+                m.process_lr(dL, dR, disp_checked=ck, tol=1)
+            for _ in range(3):
+                m.process_curves(disp, cv, dL, dR)
+                net.infer(None, cv, disp, checked=ck)
+        torch.cuda.synchronize()
+        if m.device_status() != 0 or net.device_status() != 0:
+            raise RuntimeError("device status set")
+        return 0
     L, R, _, _ = ct.synth_pair(2, SEED, W_, H_, D_ - 1)
     dL = ct.alloc_image(H_, W_, torch.uint8, dev)
     dR = ct.alloc_image(H_, W_, torch.uint8, dev)
@@ -528,12 +630,53 @@ def run_workload(args):
     return 0
 
 
+def run_confnet(args):
+    """--workload confnet1080: the learned-confidence pipeline as its own line."""
+    import torch
+    import ctstereo as ct
+    rank, world, local = dist_info()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    L, R, _, _ = ct.synth_pair(1, SEED, W_, H_, D_ - 1)
+    hL, hR = torch.from_numpy(L).pin_memory(), torch.from_numpy(R).pin_memory()
+    dL = ct.alloc_image(H_, W_, torch.uint8, dev)
+    dR = ct.alloc_image(H_, W_, torch.uint8, dev)
+    dL.copy_(hL)
+    dR.copy_(hR)
+    m = ct.BlockMatcherCensus()
+    m.configure(local, W_, H_, D_)
+    tuning = m.autotune(dL, dR, stream=stream)
+    flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        c = confnet_compare(ct, dev, stream, m, dL, dR, hL, hR, flush_buf.zero_, args.steps,
+                            args.eval_pairs or 24, local)
+    fps = 1e3 / c["learned_ms"]
+    print(json.dumps({
+        "metric": "frames/s census 1080p D=128 + learned confidence (replaces the R->L pass and the L-R check)",
+        "value": round(fps, 1), "unit": "frames/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": c["learned_ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8 codes / bf16 weights / fp32 accumulate", "data": "synthetic (seeded generator kind 1)",
+        "config": {"workload": "confnet_1920x1080_d128", "width": W_, "height": H_, "D": D_, "seed": SEED,
+                   "l2": "flushed before every timed step (256 MiB memset)", "launch_shape": tuning},
+        "e2e": {"value": round(1e3 / c["learned_e2e_ms"], 1), "unit": "frames/s", "ms_per_step": c["learned_e2e_ms"],
+                "h2d_bytes_per_step": 2 * W_ * H_, "d2h_bytes_per_step": W_ * H_},
+        "plain_lr_pipeline": {"value": round(1e3 / c["plain_ms"], 1), "e2e": round(1e3 / c["plain_e2e_ms"], 1),
+                              "unit": "frames/s"},
+        "confnet": c, "gpu_launches": c["launches_learned"] * args.steps, "clocks": clk.summary()}), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.profile:
         return run_profile(args)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "confnet1080":
+        return run_confnet(args)
     if args.workload != "census1080":
         return run_workload(args)
     return run_ours(args)

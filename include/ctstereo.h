@@ -419,11 +419,16 @@ int ct_confnet_train_step(ct_handle* h, const uint8_t* samples, const uint8_t* l
                           float* loss, ct_stream stream);
 /* Scores (sigmoid) of n samples through the training forward. */
 int ct_confnet_scores(ct_handle* h, float* scores, const uint8_t* samples, int32_t n, ct_stream stream);
-/* Score map (F32, P(disparity correct)) of a whole curve volume on the
- * tensor cores. The first call after new weights packs them (synchronises
- * the previous stream). */
+/* Scores of a whole curve volume on the tensor cores. disp: the
+ * left-to-right winner map (U8 or U16) the curves came with. Outputs (either
+ * may be NULL, not both): score (F32, P(disparity correct) per pixel) and
+ * checked (same type as disp): disp with every disparity whose score is
+ * below threshold marked invalid, in the encoding the cross-check uses
+ * (U16 CT_DISP_INCONSISTENT, U8 255), so it replaces disp_checked of
+ * ct_bm_census_process_lr. The first call after new weights packs them
+ * (synchronises the previous stream). */
 int ct_confnet_infer(ct_handle* h, const ct_image* score, const ct_curves* curves, const ct_image* disp,
-                     ct_stream stream);
+                     const ct_image* checked, float threshold, ct_stream stream);
 
 /* ---- pipe-rate probe ---------------------------------------------------------
  * Measures the issue rate of the integer operations the matchers are built

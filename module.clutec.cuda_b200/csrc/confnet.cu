@@ -642,8 +642,11 @@ struct InferArgs {
     size_t disp_pitch;
     int disp_type;
     int W, H;
-    float* score;
+    float* score;        // may be null
     size_t score_pitch;  // bytes
+    void* checked;       // may be null: the winner map with rejected pixels marked
+    size_t checked_pitch;
+    float threshold;
     const uint4* wimg;   // packed weight image (kWBytes)
     int32_t* status;
 };
@@ -875,9 +878,24 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
                 z[2] = fmaf(w5[32 + c], fmaxf(v1[c], 0.f), z[2]);
                 z[3] = fmaf(w5[33 + c], fmaxf(v1[c + 1], 0.f), z[3]);
             }
-            if (x0 + m < a.W)
-                reinterpret_cast<float*>(reinterpret_cast<char*>(a.score) + (size_t)y * a.score_pitch)[x0 + m] =
-                    1.f / (1.f + __expf(-((z[0] + z[1]) + (z[2] + z[3]))));
+            const float p = 1.f / (1.f + __expf(-((z[0] + z[1]) + (z[2] + z[3]))));
+            const int x = x0 + m;
+            if (x < a.W) {
+                if (a.score) reinterpret_cast<float*>(reinterpret_cast<char*>(a.score) + (size_t)y * a.score_pitch)[x] = p;
+                if (a.checked) {  // same encoding as the cross-check's output map
+                    const char* drow = static_cast<const char*>(a.disp) + (size_t)y * a.disp_pitch;
+                    char* crow = static_cast<char*>(a.checked) + (size_t)y * a.checked_pitch;
+                    if (a.disp_type == CT_PIX_U8) {
+                        const uint8_t v = reinterpret_cast<const uint8_t*>(drow)[x];
+                        reinterpret_cast<uint8_t*>(crow)[x] = p >= a.threshold ? v : uint8_t(0xFF);
+                    } else {
+                        const uint16_t v = reinterpret_cast<const uint16_t*>(drow)[x];
+                        const bool disp = v >= CT_DISP_FIRST && v <= CT_DISP_LAST;
+                        reinterpret_cast<uint16_t*>(crow)[x] =
+                            (disp && p < a.threshold) ? uint16_t(CT_DISP_INCONSISTENT) : v;
+                    }
+                }
+            }
         }
         fence_before();  // this tile's TMEM reads before the next tile's writes
     }
@@ -1218,16 +1236,24 @@ int ct_confnet_scores(ct_handle* hh, float* scores, const uint8_t* samples, int3
 }
 
 int ct_confnet_infer(ct_handle* hh, const ct_image* score, const ct_curves* curves, const ct_image* disp,
-                     ct_stream stream) {
+                     const ct_image* checked, float threshold, ct_stream stream) {
     clear_error();
     auto* h = as_net(hh);
     if (!h || !h->configured) return fail(CT_ESTATE, "not a configured confidence-net handle");
-    if (int rc = check_image(score, "score", 1u << CT_PIX_F32)) return rc;
+    if (!score && !checked) return fail(CT_EINVAL, "no output requested");
     if (!curves || !curves->ptr) return fail(CT_EINVAL, "null curve volume");
     if (curves->disp_count != kLen) return fail(CT_EFORMAT, "the confidence net reads curves of 128 disparities");
-    if (curves->width != score->width || curves->height != score->height)
-        return fail(CT_EFORMAT, "score map and curve volume differ in size");
     if (int rc = check_disp_for(disp, curves)) return rc;
+    if (score) {
+        if (int rc = check_image(score, "score", 1u << CT_PIX_F32)) return rc;
+        if (curves->width != score->width || curves->height != score->height)
+            return fail(CT_EFORMAT, "score map and curve volume differ in size");
+    }
+    if (checked) {
+        if (int rc = check_image(checked, "checked", 1u << disp->type)) return rc;
+        if (checked->width != disp->width || checked->height != disp->height)
+            return fail(CT_EFORMAT, "checked map and disparity map differ in size");
+    }
     if (reinterpret_cast<uintptr_t>(curves->ptr) % 16 || curves->pitch_bytes % 16 ||
         curves->pitch_bytes < 4 * (size_t(curves->width) + 2))
         return fail(CT_EINVAL, "curve volume needs a 16-byte aligned pointer and pitch >= 4 * (width + 2)");
@@ -1245,10 +1271,13 @@ int ct_confnet_infer(ct_handle* hh, const ct_image* score, const ct_curves* curv
     a.disp = disp->ptr;
     a.disp_pitch = disp->pitch_bytes;
     a.disp_type = disp->type;
-    a.W = score->width;
-    a.H = score->height;
-    a.score = static_cast<float*>(score->ptr);
-    a.score_pitch = score->pitch_bytes;
+    a.W = curves->width;
+    a.H = curves->height;
+    a.score = score ? static_cast<float*>(score->ptr) : nullptr;
+    a.score_pitch = score ? score->pitch_bytes : 0;
+    a.checked = checked ? checked->ptr : nullptr;
+    a.checked_pitch = checked ? checked->pitch_bytes : 0;
+    a.threshold = threshold;
     a.wimg = reinterpret_cast<const uint4*>(h->wimg);
     a.status = h->d_status;
     const int tiles = ((a.W + inf::kM - 1) / inf::kM) * a.H;

@@ -150,7 +150,7 @@ def _declare(L: C.CDLL) -> None:
         "ct_confnet_loss_grad": [H, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p],
         "ct_confnet_train_step": [H, C.c_void_p, C.c_void_p, C.c_int32, C.c_float, C.c_void_p, C.c_void_p],
         "ct_confnet_scores": [H, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p],
-        "ct_confnet_infer": [H, img, P(ct_curves), img, C.c_void_p],
+        "ct_confnet_infer": [H, img, P(ct_curves), img, img, C.c_float, C.c_void_p],
         "ct_bm_sad_create": [P(H)],
         "ct_bm_sad_configure": [H, C.c_int32, fmt, P(ct_sad_params)],
         "ct_bm_sad_process": [H, img, img, img, C.c_void_p],
@@ -486,10 +486,12 @@ class ConfNet(_Driver):
         check(lib().ct_confnet_scores(self._h, out.data_ptr(), samples.data_ptr(), samples.shape[0],
                                       _stream(stream)))
 
-    def infer(self, score, curves: "CurveVolume", disp, stream=None):
-        """Score map (float32) of a curve volume; disp: its winner map."""
+    def infer(self, score, curves: "CurveVolume", disp, checked=None, threshold: float = 0.5, stream=None):
+        """Score map (float32, may be None) of a curve volume; disp: its winner
+        map; checked (optional, same dtype as disp): disp with disparities
+        scoring below threshold marked invalid, as the cross-check marks them."""
         check(lib().ct_confnet_infer(self._h, _img_ref(score), C.byref(curves.desc()), _img_ref(disp),
-                                     _stream(stream)))
+                                     _img_ref(checked), threshold, _stream(stream)))
 
 
 def census_match_static(disp, left, right, disp_count: int, left_to_right: bool = True, device_status=None,

@@ -174,3 +174,33 @@ def test_tensor_core_inference_matches_training_forward(ct, oracle, cuda, W, H):
     sub = np.random.default_rng(0).choice(W * H, min(500, W * H), replace=False)
     err_o = np.abs(got[sub] - cn.scores(samples.cpu().numpy()[sub], p)).max()
     assert err_o < 3e-3, err_o
+
+
+@pytest.mark.parametrize("dtype", [torch.int16, torch.uint8])
+def test_infer_checked_map_marks_low_scores(ct, cuda, dtype):
+    """The checked output is the winner map with every disparity scoring below
+    the threshold marked the way the cross-check marks it."""
+    import confnet_train as T
+    W, H, D = 257, 40, 128
+    L, R, _, _ = ct.synth_pair(1, 77, W, H, D - 1)
+    m = ct.BlockMatcherCensus()
+    m.configure(0, W, H, D)
+    cv = ct.CurveVolume(W, H, D, cuda)
+    disp = ct.alloc_image(H, W, dtype, cuda)
+    m.process_curves(disp, cv, to_dev(L, cuda), to_dev(R, cuda))
+    net = ct.ConfNet()
+    net.configure(0, 16)
+    net.set_params(T.load_weights())
+    score = ct.alloc_image(H, W, torch.float32, cuda)
+    checked = ct.alloc_image(H, W, dtype, cuda)
+    net.infer(score, cv, disp, checked=checked, threshold=0.6)
+    torch.cuda.synchronize()
+    assert net.device_status() == 0
+    s, d, c = score.cpu().numpy(), disp.cpu().numpy(), checked.cpu().numpy()
+    if dtype == torch.uint8:
+        want = np.where(s >= 0.6, d, 255).astype(np.uint8)
+    else:
+        du = d.view(np.uint16)
+        want = np.where((du >= 1) & (du <= 0xFFEF) & (s < 0.6), 0xFFFA, du).astype(np.uint16).view(np.int16)
+    np.testing.assert_array_equal(c, want)
+    assert 0.02 < (s < 0.6).mean() < 0.9
