@@ -234,7 +234,7 @@ int ct_bm_census_process_static(const ct_image* disp, const ct_image* left, cons
  */
 typedef struct ct_sad_params {
     int32_t disp_count;     /* iDispRange: D, 1..256 */
-    int32_t radius;         /* EConfig patch: r = 4 gives 9x9; 1..7 */
+    int32_t radius;         /* EConfig patch: r = 4 gives 9x9; 1..4 */
     int32_t left_to_right;  /* 1: base = left image */
     int32_t reserved;
 } ct_sad_params;
@@ -376,7 +376,7 @@ int ct_synth_pair(int32_t kind, uint64_t seed, int32_t width, int32_t height, in
  * winner-take-all disparity is correct, from the pixel's cost curve
  * (ct_curves, D = 128). It stands in for the right-to-left pass of the
  * left-right check (CrossCheckDisparityMaps.cu:63-110), which stays the
- * fallback and the judge of its error. No counterpart in the reference.
+ * fallback and the yardstick for its error. No counterpart in the reference.
  *
  * Input: the pixel's curve re-centred on its winning disparity d (taken from
  * the left-to-right disparity map): sample r[k] = c[d - 64 + k], 255 outside

@@ -1,0 +1,731 @@
+/* ctstereo.hpp — header-only C++ layer over the ctstereo C ABI that keeps the
+ * reference's driver shape, so code written against CluTec.Cuda's MultiView
+ * drivers switches by changing includes and a namespace:
+ *
+ *     Clu::Cuda::BlockMatcherNCC::CDriver xMatcher;         // reference
+ *     ctstereo::BlockMatcherNCC::CDriver xMatcher;          // this library
+ *
+ *     xMatcher.Configure(xDevice, xFormat, xPars);
+ *     double dMs = ProcessKernel(xMatcher, surfDisp, surfL, surfR, surfNone, surfNone);
+ *
+ * Mapping (reference file:line -> here):
+ *   Clu::Cuda::CDevice, Clu::SImageFormat       -> CDevice, SImageFormat
+ *   Clu::Cuda::_CDeviceSurface (DeviceSurface.h:43-264; cudaArray + surface)
+ *                                                -> _CDeviceSurface (pitched view)
+ *   Clu::Cuda::CDeviceSurface (Create / CopyFrom / CopyInto)
+ *                                                -> CDeviceSurface (owning)
+ *   Clu::Cuda::CKernelDriverBase (KernelDriverBase.h:46-177), ProcessKernel
+ *     (KernelDriverBase.h:180-199)              -> CKernelDriverBase, ProcessKernel
+ *   Clu::Cuda::EDisparityId (DisparityId.h:35-47) -> EDisparityId
+ *   CensusTransform::CDriver (CensusTransform.h:44-70)
+ *   BlockMatcherSAD1::{EConfig, SParameter, CDriver} (BlockMatcherSAD1.h:42-127)
+ *   BlockMatcherNCC::{EConfig, SParameter, CDriver} (BlockMatcherNCC.h:41-144)
+ *   BlockMatcherAW1::{EConfig, ESimType, SParameter, CDriver} (BlockMatcherAW1.h:41-157)
+ *   CrossCheckDisparityMaps::{SParameter, CDriver} (CrossCheckDisparityMaps.h:38-117)
+ * and, with no reference counterpart: BlockMatcherCensus (census pipeline in
+ * one call, with cost-curve export), BatchStereo (many pairs per launch) and
+ * ConfidenceNet (learned confidence over the cost curves).
+ *
+ * Errors: every failing C call becomes a CError exception carrying the CT_E*
+ * code and ct_last_error_string(), the role of CLU_EXCEPTION in the
+ * reference. The C ABI itself never throws.
+ *
+ * Differences a caller sees (the build's semantics, not the reference's):
+ *   - Disparities start at 0 (_SDisparityConfig::iMin must be 0) and U16
+ *     disparity maps hold d + EDisparityId::First or an ID, U8 maps hold d or
+ *     255; the 4 x uint16 TPixelEx output (cost and specificity channels) is
+ *     not produced.
+ *   - The reference's rejection gates (gradient threshold, SAD / NCC
+ *     thresholds, minimum-delta specificity) are not built. Configure throws
+ *     CError(CT_EINVAL) when a gate that would change the winner is switched
+ *     on (fGradThresh > 0); thresholds that only label the unbuilt cost
+ *     channels are accepted and ignored.
+ *   - Guided matching (iUseDispInput, xImageDispInit) is not built: a
+ *     non-empty xImageDispInit throws.
+ *   - BlockMatcherAW1 computes the "best of 5 shifted 7x7 windows" cost with
+ *     sub-pixel refinement (EConfig::Shifted5_7x7); the reference's 2-of-4
+ *     sub-window configurations throw.
+ *   - CrossCheckDisparityMaps::DispMin / DispMax return disparities (d, not
+ *     d + First) and synchronise the last Process stream.
+ *   - Process is asynchronous on the driver's stream (SetStream; default
+ *     stream 0); ProcessKernel records events around it and waits, like the
+ *     reference's Begin / End.
+ */
+#ifndef CTSTEREO_HPP
+#define CTSTEREO_HPP
+
+#include "ctstereo.h"
+
+#include <cuda_runtime_api.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace ctstereo {
+
+/* ---- errors --------------------------------------------------------------- */
+
+class CError : public std::runtime_error {
+public:
+    CError(int code, const std::string& what) : std::runtime_error(what), m_iCode(code) {}
+    int Code() const { return m_iCode; }
+
+private:
+    int m_iCode;
+};
+
+inline void Ensure(int rc, const char* what) {
+    if (rc != CT_OK) throw CError(rc, std::string(what) + ": " + ct_last_error_string());
+}
+
+inline void EnsureCuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CError(CT_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+/* ---- device, format, disparity IDs ----------------------------------------- */
+
+struct CDevice {
+    int iDevice = 0;
+    CDevice() = default;
+    explicit CDevice(int device) : iDevice(device) {}
+};
+
+enum class EDataType : int32_t {
+    UInt8 = CT_PIX_U8,
+    UInt16 = CT_PIX_U16,
+    UInt64 = CT_PIX_U64,
+    Single = CT_PIX_F32,
+};
+
+inline size_t BytesPerPixel(EDataType t) {
+    switch (t) {
+        case EDataType::UInt8: return 1;
+        case EDataType::UInt16: return 2;
+        case EDataType::UInt64: return 8;
+        case EDataType::Single: return 4;
+    }
+    return 0;
+}
+
+/* Luminance images only: the matchers take one channel (the reference
+ * requires TPixel_Lum_UInt8 inputs, BlockMatcherNCC.cu:1411-1419). */
+struct SImageFormat {
+    int iWidth = 0;
+    int iHeight = 0;
+    EDataType eDataType = EDataType::UInt8;
+
+    SImageFormat() = default;
+    SImageFormat(int w, int h, EDataType t = EDataType::UInt8) : iWidth(w), iHeight(h), eDataType(t) {}
+    bool operator==(const SImageFormat& o) const {
+        return iWidth == o.iWidth && iHeight == o.iHeight && eDataType == o.eDataType;
+    }
+    ct_format ToC() const { return ct_format{iWidth, iHeight, static_cast<int32_t>(eDataType)}; }
+};
+
+enum class EDisparityId : uint16_t {
+    First = CT_DISP_FIRST,
+    Last = CT_DISP_LAST,
+    Unknown = CT_DISP_UNKNOWN,
+    CannotEvaluate = CT_DISP_CANNOT_EVALUATE,
+    Saturated = CT_DISP_SATURATED,
+    NotFound = CT_DISP_NOT_FOUND,
+    NotSpecific = CT_DISP_NOT_SPECIFIC,
+    NotUnique = CT_DISP_NOT_UNIQUE,
+    Inconsistent = CT_DISP_INCONSISTENT,
+};
+
+/* Replaces _SDisparityConfig (CluTec.ImgProc/DisparityConfig.h, not in the
+ * reference tree): the searched disparities iMin .. iMin + iRange - 1. */
+struct _SDisparityConfig {
+    int iMin = 0;
+    int iRange = 0;
+    void Set(int _iMin, int _iRange) {
+        iMin = _iMin;
+        iRange = _iRange;
+    }
+};
+
+/* ---- device images --------------------------------------------------------- */
+
+/* A non-owning view of a pitched device image (trivially copyable, like the
+ * reference's _CDeviceSurface). An empty view (ptr null) stands for the
+ * reference's unused xImageDispInit / xImageDebug arguments. */
+class _CDeviceSurface {
+public:
+    _CDeviceSurface() = default;
+    _CDeviceSurface(void* ptr, size_t pitch_bytes, const SImageFormat& f) : m_xFormat(f) {
+        m_xImage = ct_image{ptr, pitch_bytes, f.iWidth, f.iHeight, static_cast<int32_t>(f.eDataType), 0};
+    }
+
+    bool IsValid() const { return m_xImage.ptr != nullptr; }
+    const SImageFormat& Format() const { return m_xFormat; }
+    void* DataPointer() const { return m_xImage.ptr; }
+    size_t Pitch() const { return m_xImage.pitch_bytes; }
+    const ct_image* C() const { return IsValid() ? &m_xImage : nullptr; }
+
+protected:
+    ct_image m_xImage{nullptr, 0, 0, 0, 0, 0};
+    SImageFormat m_xFormat;
+};
+
+/* An owning pitched device image (cudaMallocPitch), the role of the
+ * reference's CDeviceSurface::Create / CopyFrom / CopyInto. Caller memory:
+ * the library never allocates the images it is given. */
+class CDeviceSurface : public _CDeviceSurface {
+public:
+    CDeviceSurface() = default;
+    explicit CDeviceSurface(const SImageFormat& f) { Create(f); }
+    ~CDeviceSurface() { Destroy(); }
+    CDeviceSurface(const CDeviceSurface&) = delete;
+    CDeviceSurface& operator=(const CDeviceSurface&) = delete;
+    CDeviceSurface(CDeviceSurface&& o) noexcept { *this = std::move(o); }
+    CDeviceSurface& operator=(CDeviceSurface&& o) noexcept {
+        if (this != &o) {
+            Destroy();
+            m_xImage = o.m_xImage;
+            m_xFormat = o.m_xFormat;
+            o.m_xImage.ptr = nullptr;
+        }
+        return *this;
+    }
+
+    void Create(const SImageFormat& f) {
+        Destroy();
+        void* p = nullptr;
+        size_t pitch = 0;
+        EnsureCuda(cudaMallocPitch(&p, &pitch, size_t(f.iWidth) * BytesPerPixel(f.eDataType), size_t(f.iHeight)),
+                   "CDeviceSurface::Create");
+        m_xFormat = f;
+        m_xImage = ct_image{p, pitch, f.iWidth, f.iHeight, static_cast<int32_t>(f.eDataType), 0};
+    }
+
+    void Destroy() {
+        if (m_xImage.ptr) cudaFree(m_xImage.ptr);
+        m_xImage.ptr = nullptr;
+    }
+
+    /* Host rows of host_pitch bytes (0: tightly packed). Synchronous. */
+    void CopyFrom(const void* host, size_t host_pitch = 0) {
+        const size_t row = size_t(m_xFormat.iWidth) * BytesPerPixel(m_xFormat.eDataType);
+        EnsureCuda(cudaMemcpy2D(m_xImage.ptr, m_xImage.pitch_bytes, host, host_pitch ? host_pitch : row, row,
+                                size_t(m_xFormat.iHeight), cudaMemcpyHostToDevice),
+                   "CDeviceSurface::CopyFrom");
+    }
+
+    void CopyInto(void* host, size_t host_pitch = 0) const {
+        const size_t row = size_t(m_xFormat.iWidth) * BytesPerPixel(m_xFormat.eDataType);
+        EnsureCuda(cudaMemcpy2D(host, host_pitch ? host_pitch : row, m_xImage.ptr, m_xImage.pitch_bytes, row,
+                                size_t(m_xFormat.iHeight), cudaMemcpyDeviceToHost),
+                   "CDeviceSurface::CopyInto");
+    }
+
+    template <typename T>
+    std::vector<T> CopyInto() const {
+        std::vector<T> v(size_t(m_xFormat.iWidth) * size_t(m_xFormat.iHeight));
+        if (sizeof(T) != BytesPerPixel(m_xFormat.eDataType)) throw CError(CT_ETYPE, "CopyInto: element size");
+        CopyInto(v.data());
+        return v;
+    }
+};
+
+/* ---- driver base and ProcessKernel ----------------------------------------- */
+
+class CKernelDriverBase {
+public:
+    explicit CKernelDriverBase(const char* name) : m_sKernelName(name) {}
+    ~CKernelDriverBase() {
+        if (m_evStart) cudaEventDestroy(m_evStart);
+        if (m_evStop) cudaEventDestroy(m_evStop);
+        ct_destroy(m_pHandle);
+    }
+    CKernelDriverBase(const CKernelDriverBase&) = delete;
+    CKernelDriverBase& operator=(const CKernelDriverBase&) = delete;
+
+    const std::string& KernelName() const { return m_sKernelName; }
+    void SetStream(cudaStream_t s) { m_xStream = s; }
+    cudaStream_t Stream() const { return m_xStream; }
+    ct_handle* Handle() const { return m_pHandle; }
+    double LastProcessTime() const { return m_dLastProcessTime; }
+
+    /* Event before / after Process on the driver's stream; End waits and
+     * stores the elapsed milliseconds (KernelDriverBase.h:139-148). */
+    void Begin() {
+        if (!m_evStart) {
+            EnsureCuda(cudaEventCreate(&m_evStart), "cudaEventCreate");
+            EnsureCuda(cudaEventCreate(&m_evStop), "cudaEventCreate");
+        }
+        EnsureCuda(cudaEventRecord(m_evStart, m_xStream), "Begin");
+    }
+    void End() {
+        EnsureCuda(cudaEventRecord(m_evStop, m_xStream), "End");
+        EnsureCuda(cudaEventSynchronize(m_evStop), "End");
+        float ms = 0.f;
+        EnsureCuda(cudaEventElapsedTime(&ms, m_evStart, m_evStop), "End");
+        m_dLastProcessTime = ms;
+    }
+    /* Reads (and clears) the device status word of the handle's launches; a
+     * bounded device-side wait that gave up becomes CError(CT_ETIMEOUT). */
+    void EnsureDeviceStatus() {
+        int32_t st = 0;
+        Ensure(ct_handle_device_status(m_pHandle, &st), m_sKernelName.c_str());
+        if (st != 0) throw CError(st, m_sKernelName + ": device status " + std::to_string(st));
+    }
+
+protected:
+    ct_handle* EnsureHandle(int (*create)(ct_handle**)) {
+        if (!m_pHandle) Ensure(create(&m_pHandle), m_sKernelName.c_str());
+        return m_pHandle;
+    }
+    ct_stream S() const { return reinterpret_cast<ct_stream>(m_xStream); }
+
+    ct_handle* m_pHandle = nullptr;
+    cudaStream_t m_xStream = nullptr;
+    cudaEvent_t m_evStart = nullptr;
+    cudaEvent_t m_evStop = nullptr;
+    double m_dLastProcessTime = 0.0;
+    std::string m_sKernelName;
+};
+
+/* Runs xDriver.Process(args...) between Begin and End and returns the
+ * milliseconds it took on the device (KernelDriverBase.h:180-199). */
+template <typename TDriver, typename... TPars>
+double ProcessKernel(TDriver& xDriver, TPars&&... xPars) {
+    xDriver.Begin();
+    xDriver.Process(std::forward<TPars>(xPars)...);
+    xDriver.End();
+    xDriver.EnsureDeviceStatus();
+    return xDriver.LastProcessTime();
+}
+
+namespace detail {
+inline void RequireInputFormat(const SImageFormat& f, const char* who) {
+    if (f.eDataType != EDataType::UInt8)
+        throw CError(CT_ETYPE, std::string(who) + ": input images must be UInt8 luminance");
+}
+inline void RequireDispConfig(const _SDisparityConfig& c, const char* who) {
+    if (c.iMin != 0) throw CError(CT_EINVAL, std::string(who) + ": disparities start at 0 (iMin must be 0)");
+}
+inline void RequireNoGuide(const _CDeviceSurface& init, const char* who) {
+    if (init.IsValid()) throw CError(CT_EINVAL, std::string(who) + ": guided matching (xImageDispInit) is not built");
+}
+}  // namespace detail
+
+/* ---- CensusTransform (CensusTransform.h:44-70) ----------------------------- */
+namespace CensusTransform {
+
+enum class EWindow : int32_t { Census_9x7 = CT_CENSUS_9X7, Census_3x3 = CT_CENSUS_3X3 };
+
+class CDriver : public CKernelDriverBase {
+public:
+    CDriver() : CKernelDriverBase("Census Transform") {}
+
+    /* Census_9x7 (U8 -> U64, the matcher's descriptor) by default;
+     * Census_3x3 is the reference's transform exactly (U8 -> U8). */
+    void Configure(const CDevice& xDevice, const SImageFormat& xFormat, EWindow eWindow = EWindow::Census_9x7) {
+        detail::RequireInputFormat(xFormat, "CensusTransform");
+        EnsureHandle(ct_census_create);
+        const ct_format f = xFormat.ToC();
+        const ct_census_params p{static_cast<int32_t>(eWindow)};
+        Ensure(ct_census_configure(m_pHandle, xDevice.iDevice, &f, &p), "CensusTransform::Configure");
+    }
+
+    void Process(_CDeviceSurface& xImageTrg, const _CDeviceSurface& xImageSrc) {
+        Ensure(ct_census_process(m_pHandle, xImageTrg.C(), xImageSrc.C(), S()), "CensusTransform::Process");
+    }
+};
+
+}  // namespace CensusTransform
+
+/* ---- BlockMatcherSAD1 (BlockMatcherSAD1.h:42-127) -------------------------- */
+namespace BlockMatcherSAD1 {
+
+/* The reference's only configuration is Patch_16x16, an even window this
+ * build does not centre; the odd windows up to 9x9 are built. */
+enum class EConfig { Patch_16x16 = 0, Patch_3x3, Patch_5x5, Patch_7x7, Patch_9x9 };
+
+struct SParameter {
+    int iOffset = 0;
+    int iDispRange = 0;
+    float fSadThresh = 0.f;
+    int iMinDeltaThresh = 0;
+    float fGradThresh = 0.f;
+    EConfig eConfig = EConfig::Patch_9x9;
+    bool bLeftToRight = true;
+
+    void Set(int _iOffset, int _iDispRange, int _iMinDeltaThresh, float _fSadThresh, float _fGradThresh,
+             EConfig _eConfig) {
+        iOffset = _iOffset;
+        iDispRange = _iDispRange;
+        iMinDeltaThresh = _iMinDeltaThresh;
+        fSadThresh = _fSadThresh;
+        fGradThresh = _fGradThresh;
+        eConfig = _eConfig;
+    }
+};
+
+class CDriver : public CKernelDriverBase {
+public:
+    CDriver() : CKernelDriverBase("Block Matcher SAD 1") {}
+
+    void Configure(const CDevice& xDevice, const SImageFormat& xFormat, const SParameter& xPars) {
+        detail::RequireInputFormat(xFormat, "BlockMatcherSAD1");
+        if (xPars.iOffset != 0) throw CError(CT_EINVAL, "BlockMatcherSAD1: iOffset must be 0");
+        if (xPars.fGradThresh > 0.f) throw CError(CT_EINVAL, "BlockMatcherSAD1: the gradient gate is not built");
+        if (xPars.eConfig == EConfig::Patch_16x16)
+            throw CError(CT_EINVAL, "BlockMatcherSAD1: Patch_16x16 is not built (odd windows 3x3 .. 9x9)");
+        EnsureHandle(ct_bm_sad_create);
+        const ct_format f = xFormat.ToC();
+        const ct_sad_params p{xPars.iDispRange, static_cast<int32_t>(xPars.eConfig), xPars.bLeftToRight ? 1 : 0, 0};
+        Ensure(ct_bm_sad_configure(m_pHandle, xDevice.iDevice, &f, &p), "BlockMatcherSAD1::Configure");
+    }
+
+    /* xImageDisp: UInt8 or UInt16. */
+    void Process(_CDeviceSurface& xImageDisp, const _CDeviceSurface& xImageL, const _CDeviceSurface& xImageR) {
+        Ensure(ct_bm_sad_process(m_pHandle, xImageDisp.C(), xImageL.C(), xImageR.C(), S()),
+               "BlockMatcherSAD1::Process");
+    }
+};
+
+}  // namespace BlockMatcherSAD1
+
+/* ---- BlockMatcherNCC (BlockMatcherNCC.h:41-144) ---------------------------- */
+namespace BlockMatcherNCC {
+
+enum class EConfig { Patch_11x11 = 0, Patch_9x9, Patch_5x5 };
+
+struct SParameter {
+    _SDisparityConfig xDispConfig;
+    int iMinDeltaThresh = 0;
+    float fNccThresh = 0.f;
+    float fGradThresh = 0.f;
+    int iUseDispInput = 0;
+    EConfig eConfig = EConfig::Patch_11x11;
+    bool bLeftToRight = true;
+
+    void Set(const _SDisparityConfig& _xDispConfig, int _iMinDeltaThresh, float _fNccThresh, float _fGradThresh,
+             int _iUseDispInput, bool _bLeftToRight, EConfig _eConfig) {
+        xDispConfig = _xDispConfig;
+        iMinDeltaThresh = _iMinDeltaThresh;
+        fNccThresh = _fNccThresh;
+        fGradThresh = _fGradThresh;
+        iUseDispInput = _iUseDispInput;
+        bLeftToRight = _bLeftToRight;
+        eConfig = _eConfig;
+    }
+};
+
+class CDriver : public CKernelDriverBase {
+public:
+    CDriver() : CKernelDriverBase("Block Matcher NCC") {}
+
+    void Configure(const CDevice& xDevice, const SImageFormat& xFormat, const SParameter& xPars) {
+        detail::RequireInputFormat(xFormat, "BlockMatcherNCC");
+        detail::RequireDispConfig(xPars.xDispConfig, "BlockMatcherNCC");
+        if (xPars.fGradThresh > 0.f) throw CError(CT_EINVAL, "BlockMatcherNCC: the gradient gate is not built");
+        if (xPars.iUseDispInput) throw CError(CT_EINVAL, "BlockMatcherNCC: guided matching is not built");
+        static const int32_t radius[] = {5, 4, 2};
+        EnsureHandle(ct_bm_ncc_create);
+        const ct_format f = xFormat.ToC();
+        const ct_ncc_params p{xPars.xDispConfig.iRange, radius[static_cast<int>(xPars.eConfig)],
+                              xPars.bLeftToRight ? 1 : 0, 0};
+        Ensure(ct_bm_ncc_configure(m_pHandle, xDevice.iDevice, &f, &p), "BlockMatcherNCC::Configure");
+    }
+
+    /* xImageDisp: UInt8 or UInt16; xImageDebug, when valid, receives the
+     * Single NCC score at the chosen disparity (the build's score output);
+     * xImageDispInit must be empty. */
+    void Process(_CDeviceSurface& xImageDisp, const _CDeviceSurface& xImageL, const _CDeviceSurface& xImageR,
+                 const _CDeviceSurface& xImageDispInit, const _CDeviceSurface& xImageDebug) {
+        detail::RequireNoGuide(xImageDispInit, "BlockMatcherNCC");
+        Ensure(ct_bm_ncc_process(m_pHandle, xImageDisp.C(), xImageDebug.C(), xImageL.C(), xImageR.C(), nullptr, S()),
+               "BlockMatcherNCC::Process");
+    }
+    void Process(_CDeviceSurface& xImageDisp, const _CDeviceSurface& xImageL, const _CDeviceSurface& xImageR) {
+        Process(xImageDisp, xImageL, xImageR, _CDeviceSurface(), _CDeviceSurface());
+    }
+};
+
+}  // namespace BlockMatcherNCC
+
+/* ---- BlockMatcherAW1 (BlockMatcherAW1.h:41-157) ---------------------------- */
+namespace BlockMatcherAW1 {
+
+/* Patch_15x15 / Patch_9x9: the reference's 2-of-4 sub-window scores (not
+ * built). Shifted5_7x7: minimum of the 7x7 SAD over the centred window and
+ * the windows shifted by +-3 px in x and y, with FP32 sub-pixel refinement. */
+enum class EConfig { Patch_15x15 = 0, Patch_9x9, Shifted5_7x7 };
+enum class ESimType { AbsoluteDifference = 0, SignedProduct };
+
+struct SParameter {
+    _SDisparityConfig xDispConfig;
+    float fMinDeltaThresh = 0.f;
+    float fSimThresh = 0.f;
+    float fGradThresh = 0.f;
+    int iUseDispInput = 0;
+    EConfig eConfig = EConfig::Shifted5_7x7;
+    ESimType eSimType = ESimType::AbsoluteDifference;
+    bool bLeftToRight = true;
+
+    void Set(const _SDisparityConfig& _xDispConfig, float _fMinDeltaThresh, float _fSimThresh, float _fGradThresh,
+             int _iUseDispInput, bool _bLeftToRight, EConfig _eConfig, ESimType _eSimType) {
+        xDispConfig = _xDispConfig;
+        fMinDeltaThresh = _fMinDeltaThresh;
+        fSimThresh = _fSimThresh;
+        fGradThresh = _fGradThresh;
+        iUseDispInput = _iUseDispInput;
+        bLeftToRight = _bLeftToRight;
+        eConfig = _eConfig;
+        eSimType = _eSimType;
+    }
+};
+
+class CDriver : public CKernelDriverBase {
+public:
+    CDriver() : CKernelDriverBase("Block Matcher Adaptive Window 1") {}
+
+    void Configure(const CDevice& xDevice, const SImageFormat& xFormat, const SParameter& xPars) {
+        detail::RequireInputFormat(xFormat, "BlockMatcherAW1");
+        detail::RequireDispConfig(xPars.xDispConfig, "BlockMatcherAW1");
+        if (xPars.eConfig != EConfig::Shifted5_7x7)
+            throw CError(CT_EINVAL, "BlockMatcherAW1: only EConfig::Shifted5_7x7 is built");
+        if (xPars.eSimType != ESimType::AbsoluteDifference)
+            throw CError(CT_EINVAL, "BlockMatcherAW1: only ESimType::AbsoluteDifference is built");
+        if (xPars.fGradThresh > 0.f) throw CError(CT_EINVAL, "BlockMatcherAW1: the gradient gate is not built");
+        if (xPars.iUseDispInput) throw CError(CT_EINVAL, "BlockMatcherAW1: guided matching is not built");
+        EnsureHandle(ct_bm_aw_create);
+        const ct_format f = xFormat.ToC();
+        const ct_aw_params p{xPars.xDispConfig.iRange, xPars.bLeftToRight ? 1 : 0, 0, 0};
+        Ensure(ct_bm_aw_configure(m_pHandle, xDevice.iDevice, &f, &p), "BlockMatcherAW1::Configure");
+    }
+
+    /* xImageDisp: Single (sub-pixel, -1 invalid) or UInt8 / UInt16 (integer
+     * winner-take-all). xImageDispInit must be empty; xImageDebug is unused. */
+    void Process(_CDeviceSurface& xImageDisp, const _CDeviceSurface& xImageL, const _CDeviceSurface& xImageR,
+                 const _CDeviceSurface& xImageDispInit, const _CDeviceSurface& /*xImageDebug*/) {
+        detail::RequireNoGuide(xImageDispInit, "BlockMatcherAW1");
+        Ensure(ct_bm_aw_process(m_pHandle, xImageDisp.C(), xImageL.C(), xImageR.C(), S()),
+               "BlockMatcherAW1::Process");
+    }
+    void Process(_CDeviceSurface& xImageDisp, const _CDeviceSurface& xImageL, const _CDeviceSurface& xImageR) {
+        Process(xImageDisp, xImageL, xImageR, _CDeviceSurface(), _CDeviceSurface());
+    }
+};
+
+}  // namespace BlockMatcherAW1
+
+/* ---- CrossCheckDisparityMaps (CrossCheckDisparityMaps.h:38-117) ------------- */
+namespace CrossCheckDisparityMaps {
+
+struct SParameter {
+    _SDisparityConfig xDispConfig;
+    int iDispDeltaThresh = 1;
+    int iIsLeftToRight = 1;
+
+    void Set(const _SDisparityConfig& _xDispConfig, int _iDispDeltaThresh, int _iIsLeftToRight) {
+        xDispConfig = _xDispConfig;
+        iDispDeltaThresh = _iDispDeltaThresh;
+        iIsLeftToRight = _iIsLeftToRight;
+    }
+};
+
+class CDriver : public CKernelDriverBase {
+public:
+    CDriver() : CKernelDriverBase("Cross Check Disparity Maps") {}
+
+    /* xFormat: the disparity maps' format (UInt8 or UInt16). */
+    void Configure(const CDevice& xDevice, const SImageFormat& xFormat, const SParameter& xPars) {
+        detail::RequireDispConfig(xPars.xDispConfig, "CrossCheckDisparityMaps");
+        EnsureHandle(ct_crosscheck_create);
+        const ct_format f = xFormat.ToC();
+        const ct_crosscheck_params p{xPars.iDispDeltaThresh, xPars.iIsLeftToRight, 0, 0};
+        Ensure(ct_crosscheck_configure(m_pHandle, xDevice.iDevice, &f, &p), "CrossCheckDisparityMaps::Configure");
+    }
+
+    void Process(_CDeviceSurface& xDispResult, const _CDeviceSurface& xDispLR, const _CDeviceSurface& xDispRL) {
+        Ensure(ct_crosscheck_process(m_pHandle, xDispResult.C(), xDispLR.C(), xDispRL.C(), S()),
+               "CrossCheckDisparityMaps::Process");
+        m_bRangeRead = false;
+    }
+
+    /* Smallest / largest kept disparity of the last Process (min > max when
+     * none was kept). The first call after Process synchronises its stream. */
+    int DispMin() { return Range().first; }
+    int DispMax() { return Range().second; }
+
+private:
+    std::pair<int, int> Range() {
+        if (!m_bRangeRead) {
+            int32_t lo = 0, hi = 0;
+            Ensure(ct_crosscheck_range(m_pHandle, &lo, &hi), "CrossCheckDisparityMaps::DispMin/DispMax");
+            m_xRange = {lo, hi};
+            m_bRangeRead = true;
+        }
+        return m_xRange;
+    }
+    bool m_bRangeRead = false;
+    std::pair<int, int> m_xRange{0, -1};
+};
+
+}  // namespace CrossCheckDisparityMaps
+
+/* ---- no reference counterpart ----------------------------------------------- */
+
+/* Device cost-curve volume for BlockMatcherCensus::ProcessCurves and
+ * ConfidenceNet (layout: ct_curves). */
+class CCurveVolume {
+public:
+    CCurveVolume() = default;
+    CCurveVolume(int width, int height, int disp_count) { Create(width, height, disp_count); }
+    ~CCurveVolume() {
+        if (m_xCurves.ptr) cudaFree(m_xCurves.ptr);
+    }
+    CCurveVolume(const CCurveVolume&) = delete;
+    CCurveVolume& operator=(const CCurveVolume&) = delete;
+
+    void Create(int width, int height, int disp_count) {
+        if (m_xCurves.ptr) cudaFree(m_xCurves.ptr);
+        m_xCurves.ptr = nullptr;
+        size_t pitch = 0;
+        Ensure(ct_curves_pitch(width, &pitch), "CCurveVolume::Create");
+        const size_t rows = size_t(height) * size_t((disp_count + 3) / 4);
+        void* p = nullptr;
+        EnsureCuda(cudaMalloc(&p, rows * pitch), "CCurveVolume::Create");
+        m_xCurves = ct_curves{p, pitch, width, height, disp_count, 0};
+    }
+    const ct_curves* C() const { return &m_xCurves; }
+
+private:
+    ct_curves m_xCurves{nullptr, 0, 0, 0, 0, 0};
+};
+
+/* Census pipeline (9x7 census, 5x5 Hamming aggregation, winner-take-all)
+ * in one call per direction; ProcessLR adds the other direction and the
+ * cross-check, ProcessCurves the cost-curve export. */
+namespace BlockMatcherCensus {
+
+struct SParameter {
+    _SDisparityConfig xDispConfig;
+    int iAggRadius = 2;
+    bool bLeftToRight = true;
+};
+
+class CDriver : public CKernelDriverBase {
+public:
+    CDriver() : CKernelDriverBase("Block Matcher Census") {}
+
+    void Configure(const CDevice& xDevice, const SImageFormat& xFormat, const SParameter& xPars) {
+        detail::RequireInputFormat(xFormat, "BlockMatcherCensus");
+        detail::RequireDispConfig(xPars.xDispConfig, "BlockMatcherCensus");
+        EnsureHandle(ct_bm_census_create);
+        const ct_format f = xFormat.ToC();
+        const ct_census_match_params p{xPars.xDispConfig.iRange, xPars.iAggRadius, xPars.bLeftToRight ? 1 : 0, 0};
+        Ensure(ct_bm_census_configure(m_pHandle, xDevice.iDevice, &f, &p), "BlockMatcherCensus::Configure");
+    }
+
+    void Process(_CDeviceSurface& xImageDisp, const _CDeviceSurface& xImageL, const _CDeviceSurface& xImageR) {
+        Ensure(ct_bm_census_process(m_pHandle, xImageDisp.C(), xImageL.C(), xImageR.C(), S()),
+               "BlockMatcherCensus::Process");
+    }
+
+    /* Any of the three outputs may be an empty surface. */
+    void ProcessLR(_CDeviceSurface& xDispLR, _CDeviceSurface& xDispRL, _CDeviceSurface& xDispChecked,
+                   int iDispDeltaThresh, const _CDeviceSurface& xImageL, const _CDeviceSurface& xImageR) {
+        Ensure(ct_bm_census_process_lr(m_pHandle, xDispLR.C(), xDispRL.C(), xDispChecked.C(), iDispDeltaThresh,
+                                       xImageL.C(), xImageR.C(), S()),
+               "BlockMatcherCensus::ProcessLR");
+    }
+
+    void ProcessCurves(_CDeviceSurface& xImageDisp, CCurveVolume& xCurves, const _CDeviceSurface& xImageL,
+                       const _CDeviceSurface& xImageR) {
+        Ensure(ct_bm_census_process_curves(m_pHandle, xImageDisp.C(), xCurves.C(), xImageL.C(), xImageR.C(), S()),
+               "BlockMatcherCensus::ProcessCurves");
+    }
+};
+
+}  // namespace BlockMatcherCensus
+
+/* Many pairs of mixed size per call: census both ways + cross-check. */
+namespace BatchStereo {
+
+struct SPair {
+    _CDeviceSurface xImageL, xImageR, xDispChecked;
+};
+
+class CDriver : public CKernelDriverBase {
+public:
+    CDriver() : CKernelDriverBase("Batch Stereo") {}
+
+    /* xFormats[i] / iDispRanges[i]: the shape of pair i. */
+    void Configure(const CDevice& xDevice, const std::vector<SImageFormat>& xFormats,
+                   const std::vector<int>& iDispRanges, int iDispDeltaThresh) {
+        if (xFormats.size() != iDispRanges.size()) throw CError(CT_EINVAL, "BatchStereo: one range per format");
+        std::vector<ct_batch_shape> shapes;
+        for (size_t i = 0; i < xFormats.size(); ++i) {
+            detail::RequireInputFormat(xFormats[i], "BatchStereo");
+            shapes.push_back(ct_batch_shape{xFormats[i].iWidth, xFormats[i].iHeight, iDispRanges[i], 0});
+        }
+        EnsureHandle(ct_batch_create);
+        Ensure(ct_batch_configure(m_pHandle, xDevice.iDevice, shapes.data(), int32_t(shapes.size()), iDispDeltaThresh),
+               "BatchStereo::Configure");
+    }
+
+    void Process(const std::vector<SPair>& xPairs) {
+        std::vector<ct_batch_item> items;
+        for (const SPair& p : xPairs) {
+            if (!p.xImageL.IsValid() || !p.xImageR.IsValid() || !p.xDispChecked.IsValid())
+                throw CError(CT_EINVAL, "BatchStereo: empty surface in a pair");
+            items.push_back(ct_batch_item{*p.xImageL.C(), *p.xImageR.C(), *p.xDispChecked.C()});
+        }
+        Ensure(ct_batch_process(m_pHandle, items.data(), int32_t(items.size()), S()), "BatchStereo::Process");
+    }
+};
+
+}  // namespace BatchStereo
+
+/* Learned confidence over census cost curves (D = 128): replaces the
+ * right-to-left pass of the left-right check. */
+namespace ConfidenceNet {
+
+class CDriver : public CKernelDriverBase {
+public:
+    CDriver() : CKernelDriverBase("Confidence Net") {}
+
+    void Configure(const CDevice& xDevice, int iMaxTrainBatch = 16) {
+        EnsureHandle(ct_confnet_create);
+        Ensure(ct_confnet_configure(m_pHandle, xDevice.iDevice, iMaxTrainBatch), "ConfidenceNet::Configure");
+    }
+
+    void SetParams(const std::vector<float>& params) {
+        Ensure(ct_confnet_set_params(m_pHandle, params.data(), int32_t(params.size())), "ConfidenceNet::SetParams");
+    }
+
+    /* Raw little-endian fp32 weight file of CT_CONFNET_PARAMS floats. */
+    void LoadParams(const std::string& path) {
+        std::vector<float> p(CT_CONFNET_PARAMS);
+        FILE* f = std::fopen(path.c_str(), "rb");
+        if (!f) throw CError(CT_EINVAL, "ConfidenceNet::LoadParams: cannot open " + path);
+        const size_t n = std::fread(p.data(), sizeof(float), p.size() + 1, f);
+        std::fclose(f);
+        if (n != p.size()) throw CError(CT_EINVAL, "ConfidenceNet::LoadParams: " + path + " is not a weight file");
+        SetParams(p);
+    }
+
+    /* xScore (Single) and / or xDispChecked (the type of xDispLR): the
+     * per-pixel score, and xDispLR with every disparity scoring below
+     * fThreshold marked Inconsistent (UInt8: 255). */
+    void Process(_CDeviceSurface& xScore, _CDeviceSurface& xDispChecked, const CCurveVolume& xCurves,
+                 const _CDeviceSurface& xDispLR, float fThreshold) {
+        Ensure(ct_confnet_infer(m_pHandle, xScore.C(), xCurves.C(), xDispLR.C(), xDispChecked.C(), fThreshold, S()),
+               "ConfidenceNet::Process");
+    }
+};
+
+}  // namespace ConfidenceNet
+
+}  // namespace ctstereo
+
+#endif  // CTSTEREO_HPP

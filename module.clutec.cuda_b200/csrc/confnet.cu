@@ -3,7 +3,7 @@
 // byte each, from ct_bm_census_process_curves) and scores how likely the
 // winner-take-all disparity is correct. It stands in for the right-to-left
 // matching pass of the left-right check (CrossCheckDisparityMaps.cu:63-110),
-// which stays as the fallback and as the judge of its error.
+// which stays as the fallback and as the yardstick for its error.
 //
 // Network (weights bf16, biases fp32, accumulation fp32):
 //   input  the pixel's curve re-centred on its winning disparity d: sample

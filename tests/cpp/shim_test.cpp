@@ -1,0 +1,321 @@
+// Known-answer and error-path checks of the header-only C++ driver layer
+// (include/ctstereo.hpp), written the way a reference user drives
+// Clu::Cuda::*::CDriver: Configure -> ProcessKernel -> CopyInto.
+//
+//   shim_test cpu               argument checks that never reach a device
+//   shim_test gpu <weights.f32> every driver on a pair whose right image is
+//                               the left one shifted by a known disparity
+//
+// Exit status 0 = all checks passed; each failure prints one line.
+#include "ctstereo.hpp"
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <random>
+#include <string>
+#include <vector>
+
+using namespace ctstereo;
+
+static int g_failures = 0;
+
+#define CHECK(cond, ...)                                  \
+    do {                                                  \
+        if (!(cond)) {                                    \
+            std::printf("FAIL %s:%d: ", __FILE__, __LINE__); \
+            std::printf(__VA_ARGS__);                     \
+            std::printf("\n");                            \
+            ++g_failures;                                 \
+        }                                                 \
+    } while (0)
+
+// Runs f and returns the CError code it threw (0 if none, -1 for another exception).
+static int ThrownCode(const std::function<void()>& f) {
+    try {
+        f();
+    } catch (const CError& e) {
+        if (std::strlen(e.what()) == 0) return -2;
+        return e.Code();
+    } catch (...) {
+        return -1;
+    }
+    return 0;
+}
+
+static int RunCpu() {
+    const CDevice dev(0);
+    const SImageFormat f(320, 120);
+
+    BlockMatcherSAD1::SParameter sad;
+    sad.Set(0, 64, 0, 0.f, 0.f, BlockMatcherSAD1::EConfig::Patch_9x9);
+    CHECK(sad.iDispRange == 64 && sad.eConfig == BlockMatcherSAD1::EConfig::Patch_9x9, "SAD Set");
+    {
+        BlockMatcherSAD1::SParameter p = sad;
+        p.eConfig = BlockMatcherSAD1::EConfig::Patch_16x16;
+        BlockMatcherSAD1::CDriver d;
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "SAD Patch_16x16 must be rejected");
+        p = sad;
+        p.fGradThresh = 2.f;
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "SAD gradient gate must be rejected");
+        p = sad;
+        p.iOffset = 3;
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "SAD offset must be rejected");
+        CHECK(ThrownCode([&] { d.Configure(dev, SImageFormat(320, 120, EDataType::UInt16), sad); }) == CT_ETYPE,
+              "SAD UInt16 input must be rejected");
+        p = sad;
+        p.iDispRange = 0;  // reaches the C ABI, which checks before touching a device
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "SAD disp range 0 must be rejected");
+    }
+    {
+        _SDisparityConfig dc;
+        dc.Set(0, 128);
+        BlockMatcherNCC::SParameter p;
+        p.Set(dc, 0, 0.f, 0.f, 1, true, BlockMatcherNCC::EConfig::Patch_11x11);
+        BlockMatcherNCC::CDriver d;
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "NCC guided mode must be rejected");
+        p.iUseDispInput = 0;
+        p.xDispConfig.Set(5, 128);
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "NCC iMin != 0 must be rejected");
+        p.xDispConfig.Set(0, 128);
+        p.bLeftToRight = false;
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "NCC right-to-left must be rejected");
+    }
+    {
+        _SDisparityConfig dc;
+        dc.Set(0, 256);
+        BlockMatcherAW1::SParameter p;
+        p.Set(dc, 0.f, 0.f, 0.f, 0, true, BlockMatcherAW1::EConfig::Patch_15x15,
+              BlockMatcherAW1::ESimType::AbsoluteDifference);
+        BlockMatcherAW1::CDriver d;
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "AW1 2-of-4 must be rejected");
+        p.eConfig = BlockMatcherAW1::EConfig::Shifted5_7x7;
+        p.eSimType = BlockMatcherAW1::ESimType::SignedProduct;
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "AW1 signed product must be rejected");
+    }
+    {
+        CrossCheckDisparityMaps::SParameter p;
+        _SDisparityConfig dc;
+        dc.Set(0, 64);
+        p.Set(dc, 1, 1);
+        CrossCheckDisparityMaps::CDriver d;
+        CHECK(ThrownCode([&] { d.Configure(dev, SImageFormat(320, 120, EDataType::UInt64), p); }) == CT_ETYPE,
+              "cross-check on UInt64 maps must be rejected");
+        p.iDispDeltaThresh = -1;
+        CHECK(ThrownCode([&] { d.Configure(dev, SImageFormat(320, 120, EDataType::UInt16), p); }) == CT_EINVAL,
+              "negative tolerance must be rejected");
+    }
+    {
+        BatchStereo::CDriver d;
+        CHECK(ThrownCode([&] { d.Configure(dev, {f, f}, {64}, 1); }) == CT_EINVAL, "batch shape/range mismatch");
+    }
+    {
+        ConfidenceNet::CDriver d;
+        CHECK(ThrownCode([&] { d.LoadParams("/nonexistent/weights.f32"); }) == CT_EINVAL, "missing weight file");
+    }
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
+    if (n == 0) {
+        // a valid configuration reaches the device and fails as a CUDA error
+        BlockMatcherSAD1::CDriver d;
+        const int code = ThrownCode([&] { d.Configure(dev, f, sad); });
+        CHECK(code == CT_ECUDA, "configure without a device: code %d", code);
+    }
+    return g_failures;
+}
+
+// ---------------------------------------------------------------------------
+
+static uint64_t HostCensus9x7(const std::vector<uint8_t>& img, int W, int x, int y) {
+    uint64_t c = 0;
+    const uint8_t ctr = img[size_t(y) * W + x];
+    for (int dy = -3; dy <= 3; ++dy)
+        for (int dx = -4; dx <= 4; ++dx) c = (c << 1) | uint64_t(img[size_t(y + dy) * W + x + dx] > ctr);
+    return c;
+}
+
+static int RunGpu(const char* weights) {
+    const int W = 320, H = 120, K = 7;  // right image = left shifted by K: L(x) = R(x - K)
+    std::mt19937 rng(12345);
+    std::vector<uint8_t> L(size_t(W) * H), R(size_t(W) * H);
+    for (auto& v : L) v = uint8_t(rng() & 0xFF);
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) R[size_t(y) * W + x] = x + K < W ? L[size_t(y) * W + x + K] : uint8_t(rng() & 0xFF);
+
+    const CDevice dev(0);
+    const SImageFormat fin(W, H);
+    CDeviceSurface surfL(fin), surfR(fin);
+    surfL.CopyFrom(L.data());
+    surfR.CopyFrom(R.data());
+    const SImageFormat f16(W, H, EDataType::UInt16), f8(W, H, EDataType::UInt8), f32(W, H, EDataType::Single);
+    auto interior = [&](int x, int y, int r) { return y >= r && y < H - r && x >= K + r && x < W - r - K; };
+
+    {  // census transform
+        CensusTransform::CDriver d;
+        d.Configure(dev, fin);
+        CDeviceSurface desc(SImageFormat(W, H, EDataType::UInt64));
+        const double ms = ProcessKernel(d, desc, surfL);
+        CHECK(ms >= 0.0, "census time");
+        auto got = desc.CopyInto<uint64_t>();
+        int bad = 0;
+        for (int y = 3; y < H - 3; ++y)
+            for (int x = 4; x < W - 4; ++x) bad += got[size_t(y) * W + x] != HostCensus9x7(L, W, x, y);
+        CHECK(bad == 0, "census: %d descriptors differ", bad);
+    }
+    {  // SAD 9x9, UInt8
+        BlockMatcherSAD1::SParameter p;
+        p.Set(0, 64, 0, 0.f, 0.f, BlockMatcherSAD1::EConfig::Patch_9x9);
+        BlockMatcherSAD1::CDriver d;
+        d.Configure(dev, fin, p);
+        CDeviceSurface disp(f8);
+        ProcessKernel(d, disp, surfL, surfR);
+        auto v = disp.CopyInto<uint8_t>();
+        int bad = 0;
+        for (int y = 0; y < H; ++y)
+            for (int x = 0; x < W; ++x) bad += interior(x, y, 4) && v[size_t(y) * W + x] != K;
+        CHECK(bad == 0, "SAD: %d interior pixels not at d = %d", bad, K);
+    }
+    {  // NCC 11x11, UInt16 + score
+        _SDisparityConfig dc;
+        dc.Set(0, 128);
+        BlockMatcherNCC::SParameter p;
+        p.Set(dc, 0, 0.f, 0.f, 0, true, BlockMatcherNCC::EConfig::Patch_11x11);
+        BlockMatcherNCC::CDriver d;
+        d.Configure(dev, fin, p);
+        CDeviceSurface disp(f16), score(f32);
+        ProcessKernel(d, disp, surfL, surfR, _CDeviceSurface(), score);
+        auto v = disp.CopyInto<uint16_t>();
+        auto s = score.CopyInto<float>();
+        int bad = 0, low = 0;
+        for (int y = 0; y < H; ++y)
+            for (int x = 0; x < W; ++x)
+                if (interior(x, y, 5)) {
+                    bad += v[size_t(y) * W + x] != K + uint16_t(EDisparityId::First);
+                    low += s[size_t(y) * W + x] < 0.9999f;
+                }
+        CHECK(bad == 0 && low == 0, "NCC: %d interior pixels off, %d scores below 1", bad, low);
+    }
+    {  // AW1 shifted windows, sub-pixel
+        _SDisparityConfig dc;
+        dc.Set(0, 64);
+        BlockMatcherAW1::SParameter p;
+        p.Set(dc, 0.f, 0.f, 0.f, 0, true, BlockMatcherAW1::EConfig::Shifted5_7x7,
+              BlockMatcherAW1::ESimType::AbsoluteDifference);
+        BlockMatcherAW1::CDriver d;
+        d.Configure(dev, fin, p);
+        CDeviceSurface disp(f32);
+        ProcessKernel(d, disp, surfL, surfR, _CDeviceSurface(), _CDeviceSurface());
+        auto v = disp.CopyInto<float>();
+        int bad = 0;
+        for (int y = 0; y < H; ++y)
+            for (int x = 0; x < W; ++x) bad += interior(x, y, 6) && !(std::fabs(v[size_t(y) * W + x] - K) < 0.5f);
+        CHECK(bad == 0, "AW1: %d interior pixels not within 0.5 of %d", bad, K);
+    }
+    {  // census both ways + cross-check driver on the two maps
+        _SDisparityConfig dc;
+        dc.Set(0, 64);
+        BlockMatcherCensus::SParameter p;
+        p.xDispConfig = dc;
+        BlockMatcherCensus::CDriver m;
+        m.Configure(dev, fin, p);
+        CDeviceSurface lr(f16), rl(f16), chk(f16), res(f16);
+        _CDeviceSurface none;
+        m.ProcessLR(lr, rl, chk, 1, surfL, surfR);
+        CrossCheckDisparityMaps::SParameter cp;
+        cp.Set(dc, 1, 1);
+        CrossCheckDisparityMaps::CDriver cc;
+        cc.Configure(dev, f16, cp);
+        ProcessKernel(cc, res, lr, rl);
+        auto a = chk.CopyInto<uint16_t>();
+        auto b = res.CopyInto<uint16_t>();
+        int bad = 0, differ = 0;
+        for (int y = 0; y < H; ++y)
+            for (int x = 0; x < W; ++x) {
+                const size_t i = size_t(y) * W + x;
+                bad += interior(x, y, 6) && a[i] != K + 1;
+                differ += a[i] != b[i];
+            }
+        CHECK(bad == 0, "census L-R: %d interior pixels not kept at d = %d", bad, K);
+        CHECK(differ == 0, "ProcessLR and the cross-check driver disagree on %d pixels", differ);
+        CHECK(cc.DispMin() <= K && cc.DispMax() >= K, "range %d..%d", cc.DispMin(), cc.DispMax());
+        m.EnsureDeviceStatus();
+
+        // learned confidence on the same pair: checked = winner map with
+        // every pixel scoring below the threshold marked Inconsistent
+        ConfidenceNet::CDriver net;
+        net.Configure(dev);
+        net.LoadParams(weights);
+        BlockMatcherCensus::CDriver m128;
+        p.xDispConfig.Set(0, 128);
+        m128.Configure(dev, fin, p);
+        CCurveVolume cv(W, H, 128);
+        CDeviceSurface d128(f16), score(f32), checked(f16);
+        m128.ProcessCurves(d128, cv, surfL, surfR);
+        ProcessKernel(net, score, checked, cv, d128, 0.5f);
+        auto dv = d128.CopyInto<uint16_t>();
+        auto sv = score.CopyInto<float>();
+        auto cvv = checked.CopyInto<uint16_t>();
+        int wrong = 0, range = 0, kept = 0, n_in = 0;
+        for (size_t i = 0; i < dv.size(); ++i) {
+            const bool has = dv[i] >= CT_DISP_FIRST && dv[i] <= CT_DISP_LAST;
+            const uint16_t want = has && sv[i] < 0.5f ? uint16_t(EDisparityId::Inconsistent) : dv[i];
+            wrong += cvv[i] != want;
+            range += !(sv[i] >= 0.f && sv[i] <= 1.f) && has;
+            const int x = int(i % W), y = int(i / W);
+            if (interior(x, y, 6)) {
+                ++n_in;
+                kept += cvv[i] == K + 1;
+            }
+        }
+        CHECK(wrong == 0, "confidence: %d checked pixels disagree with the scores", wrong);
+        CHECK(range == 0, "confidence: %d scores outside [0, 1]", range);
+        std::printf("confidence net keeps %d of %d interior pixels of the exact shift\n", kept, n_in);
+    }
+    {  // batch: two pairs of different size in one call
+        const int W2 = 200, H2 = 64;
+        std::vector<uint8_t> L2(size_t(W2) * H2), R2(size_t(W2) * H2);
+        for (int y = 0; y < H2; ++y)
+            for (int x = 0; x < W2; ++x) {
+                L2[size_t(y) * W2 + x] = L[size_t(y) * W + x];
+                R2[size_t(y) * W2 + x] = R[size_t(y) * W + x];
+            }
+        CDeviceSurface sL2(SImageFormat(W2, H2)), sR2(SImageFormat(W2, H2));
+        sL2.CopyFrom(L2.data());
+        sR2.CopyFrom(R2.data());
+        BatchStereo::CDriver b;
+        b.Configure(dev, {fin, SImageFormat(W2, H2)}, {64, 32}, 1);
+        CDeviceSurface o1(f16), o2(SImageFormat(W2, H2, EDataType::UInt16));
+        ProcessKernel(b, std::vector<BatchStereo::SPair>{{surfL, surfR, o1}, {sL2, sR2, o2}});
+        auto v1 = o1.CopyInto<uint16_t>();
+        auto v2 = o2.CopyInto<uint16_t>();
+        int bad = 0;
+        for (int y = 6; y < H - 6; ++y)
+            for (int x = K + 6; x < W - 6 - K; ++x) bad += v1[size_t(y) * W + x] != K + 1;
+        for (int y = 6; y < H2 - 6; ++y)
+            for (int x = K + 6; x < W2 - 6 - K; ++x) bad += v2[size_t(y) * W2 + x] != K + 1;
+        CHECK(bad == 0, "batch: %d interior pixels not kept at d = %d", bad, K);
+    }
+    return g_failures;
+}
+
+int main(int argc, char** argv) {
+    const std::string mode = argc > 1 ? argv[1] : "cpu";
+    int rc = 0;
+    try {
+        if (mode == "cpu") {
+            rc = RunCpu();
+        } else if (mode == "gpu" && argc > 2) {
+            rc = RunGpu(argv[2]);
+        } else {
+            std::printf("usage: shim_test cpu | gpu <weights.f32>\n");
+            return 2;
+        }
+    } catch (const CError& e) {
+        std::printf("FAIL: uncaught CError %d: %s\n", e.Code(), e.what());
+        return 1;
+    }
+    std::printf("%s: %s (%d failures)\n", mode.c_str(), rc ? "FAILED" : "ok", rc);
+    return rc ? 1 : 0;
+}
