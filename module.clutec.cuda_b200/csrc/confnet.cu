@@ -66,16 +66,20 @@ __device__ __forceinline__ float bf16r(float v) { return __bfloat162float(__floa
 // ---------------------------------------------------------------------------
 // Gather: samples[n][128] from a curve volume at pixel list xy[n][2]
 // ---------------------------------------------------------------------------
+// A disparity map entry as stored (U8 or U16).
+__device__ __forceinline__ uint32_t disp_entry(const void* disp, size_t pitch, int type, int x, int y) {
+    const char* row = static_cast<const char*>(disp) + (size_t)y * pitch;
+    return type == CT_PIX_U8 ? uint32_t(reinterpret_cast<const uint8_t*>(row)[x])
+                             : uint32_t(reinterpret_cast<const uint16_t*>(row)[x]);
+}
 // Winning disparity of a map entry (U16 EDisparityId d + 1, U8 d; 0 when the
 // pixel has no disparity).
+__device__ __forceinline__ int entry_winner(uint32_t v, int type) {
+    if (type == CT_PIX_U8) return v < uint32_t(kLen) ? int(v) : 0;
+    return (v >= 1 && v <= uint32_t(kLen)) ? int(v) - 1 : 0;
+}
 __device__ __forceinline__ int winner(const void* disp, size_t pitch, int type, int x, int y) {
-    const char* row = static_cast<const char*>(disp) + (size_t)y * pitch;
-    if (type == CT_PIX_U8) {
-        const int v = reinterpret_cast<const uint8_t*>(row)[x];
-        return v < kLen ? v : 0;
-    }
-    const int v = reinterpret_cast<const uint16_t*>(row)[x];
-    return (v >= 1 && v <= kLen) ? v - 1 : 0;
+    return entry_winner(disp_entry(disp, pitch, type, x, y), type);
 }
 
 // Re-centred samples: samples[s][k] = curve(x, y)[d - 64 + k] (255 outside),
@@ -457,22 +461,22 @@ constexpr int kM = 128;   // pixels per tile = MMA M
 constexpr int kChunkBytes = kM * 16;  // one K-chunk (8 elements) of the 128-row A1 operand
 
 // Shared memory:
-//   stage  each pixel's 10 curve words around its winner in a row of
-//          kStageWords words: words g0 .. g0 + 9 of the curve (g0 = floor((d -
-//          12) / 4); words outside the curve read 255), then 3 words of 255,
-//          so the 35 codes the convolutions read (curve bytes d - 12 .. d +
-//          22) start at row byte (d - 12) - 4 g0 (odd row stride:
-//          conflict-free column access)
+//   box    the tile's curve block, brought in by one TMA load: all 32
+//          disparity groups x kBoxWords words starting at word x0 (the tile's
+//          first column x0 is word x0 + 2), group g at g * kBoxWords words;
+//          pixel m reads column m + 2 (lanes of a warp on distinct banks
+//          when they share the group)
 //   A1     conv1 operand, f16, K-major without swizzle in K-chunk panels
 //          (element (pixel r, k) at (k / 8) * 2048 + r * 16 + (k % 8) * 2):
-//          window t = chunks 2t, 2t + 1 holds codes 15t .. 15t + 14 (the
-//          16th element meets zero weights)
+//          window t = chunks 2t, 2t + 1 holds codes 15t .. 15t + 15 of the
+//          35 the convolutions read (codes past the 35th meet zero weights)
 //   then the packed weights (B operands in the same panel form with rows =
 //   output channels, and fp32 biases).
-constexpr int kCurveWords = 10;  // curve words loaded per pixel (40 bytes cover the 35 codes)
-constexpr int kStageWords = 13;
-constexpr int kStage = 0;
-constexpr int kA1 = kStage + kM * kStageWords * 4;
+constexpr int kGroups = 32;       // 128 disparities / 4 per word
+constexpr int kBoxWords = kM + 4; // 2 halo words + 128 columns, rounded to 16 bytes
+constexpr int kBoxBytes = kGroups * kBoxWords * 4;
+constexpr int kBox = 0;
+constexpr int kA1 = kBox + kBoxBytes;
 constexpr int kA1Chunks = 6;
 constexpr int kWImg = kA1 + kA1Chunks * kChunkBytes;
 constexpr int kB1 = 0;                  // conv1: N=96 (position-in-window x 32) x K=16 f16, tap j of
@@ -482,10 +486,11 @@ constexpr int kB3 = kB2 + 20 * 512;     // conv3 taps 2, 3: N=32 x K=64, chunk =
 constexpr int kB4 = kB3 + 8 * 512;      // fc1: N=64 x K=32 bf16 (LBO 1024)
 constexpr int kBias = kB4 + 4 * 1024;   // fp32: b1[32] b2[32] b3[32] b4[64] w5[64] b5
 constexpr int kWBytes = kBias + (32 + 32 + 32 + 64 + 64 + 4) * 4;
-constexpr int kBar = kWImg + kWBytes;   // 2 mbarriers
-constexpr int kTmemSlot = kBar + 2 * 8;
+constexpr int kBar = kWImg + kWBytes;   // 3 mbarriers: MMA commits (2), curve block
+constexpr int kTmemSlot = kBar + 3 * 8;
 constexpr int kSmem = kTmemSlot + 16;
 static_assert(kWBytes % 16 == 0, "weight image must be a whole number of 16-byte words");
+static_assert(kBoxWords * 4 % 16 == 0 && kA1 % 128 == 0, "TMA box rows and A1 panels 16-byte aligned");
 static_assert(2 * kSmem <= 228 * 1024, "two CTAs per SM");
 
 // TMEM (256 columns per CTA, two CTAs per SM). Accumulators are fp32, one
@@ -651,21 +656,23 @@ struct InferArgs {
     int32_t* status;
 };
 
-__global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
+__global__ void __launch_bounds__(kNT, 2) infer_kernel(const __grid_constant__ CUtensorMap tm_curve, InferArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int tid = threadIdx.x, warp = tid >> 5;
     const int m = tid;  // pixel of the tile / TMEM lane
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kBar);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kTmemSlot);
     unsigned char* A1 = smem + kA1;
-    uint32_t* stage = reinterpret_cast<uint32_t*>(smem + kStage) + m * kStageWords;  // this pixel's row
+    const uint32_t* box = reinterpret_cast<const uint32_t*>(smem + kBox) + m + 2;  // this pixel's column
     const uint32_t sA1 = dev::smem_u32(A1), sW = dev::smem_u32(smem + kWImg);
 
     for (int k = tid; k < kWBytes / 16; k += kNT) reinterpret_cast<uint4*>(smem + kWImg)[k] = a.wimg[k];
     if (tid == 0) {
         dev::mbar_init(&bars[0], 1);
         dev::mbar_init(&bars[1], 1);
+        dev::mbar_init(&bars[2], 1);
         dev::fence_barrier_init();
+        dev::prefetch_tmap(&tm_curve);
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dev::smem_u32(tslot)),
@@ -681,6 +688,7 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
 
     const float* bias = reinterpret_cast<const float*>(smem + kWImg + kBias);
     const float* w5 = bias + 160;
+    static_assert((kWImg + kBias + 160 * 4) % 16 == 0, "w5 is read as float4");
     const float b5 = bias[224];
     float bias1[32];  // conv1 biases, stored into 7 accumulator groups per tile
 #pragma unroll
@@ -692,8 +700,24 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
 
     const int tiles_x = (a.W + kM - 1) / kM;
     const int tiles = tiles_x * a.H;
-    uint32_t ph[2] = {0, 0};  // phases waited for, per mbarrier
-    uint32_t cm[2] = {0, 0};  // commits issued (counted by every lane of warp 0)
+    // Tile t = (row t / tiles_x, column tile t % tiles_x). A CTA visits tiles
+    // t, t + G, ... (G = gridDim.x) and tracks three of them ahead by adding
+    // (G / tiles_x, G % tiles_x) with a carry, never dividing in the loop.
+    struct TilePos {
+        int y, tx;
+    };
+    const int step_y = (int)gridDim.x / tiles_x, step_x = (int)gridDim.x % tiles_x;
+    auto advance = [&](TilePos q) {
+        q.y += step_y;
+        q.tx += step_x;
+        if (q.tx >= tiles_x) {
+            q.tx -= tiles_x;
+            ++q.y;
+        }
+        return q;
+    };
+    uint32_t ph[3] = {0, 0, 0};  // phases waited for, per mbarrier
+    uint32_t cm[3] = {0, 0, 0};  // commits / loads issued (counted by the issuing warp's lanes)
     bool failed = false;
     auto commit_to = [&](int b) {
         commit(&bars[b]);
@@ -719,44 +743,39 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
         __syncthreads();
     };
 
-    // this thread's curve words around its winner: groups g0 .. g0 + 9 of 4
-    // disparities; the lanes of a warp mostly share g0 (disparities are
-    // piecewise smooth), so the loads stay close to coalesced
-    // The winner of a tile is loaded one tile before its curve words, so the
-    // curve loads never wait on it.
-    uint32_t cw[kCurveWords];
-    int c0 = 0;  // byte of the first of the 35 codes within cw
-    auto load_winner = [&](int t) {
-        const int y = t / tiles_x, x = (t % tiles_x) * kM + m;
-        return x < a.W ? winner(a.disp, a.disp_pitch, a.disp_type, x, y) : 0;
+    // A tile's disparity entries are loaded two tiles ahead and kept as
+    // loaded (nothing consumes them before the next tile, so no thread waits
+    // on the load); they give the curve offsets of the next tile's A1 and the
+    // checked output without a second read of the map. The curve block of
+    // the next tile is one TMA load, issued by lane 0 of warp 1 while the
+    // conv1 MMAs run and waited for just before its A1 is built.
+    auto load_entry = [&](TilePos q) {
+        const int x = q.tx * kM + m;
+        return x < a.W ? disp_entry(a.disp, a.disp_pitch, a.disp_type, x, q.y) : 0u;
     };
-    auto load_curve = [&](int t, int d) {
-        const int y = t / tiles_x, x = (t % tiles_x) * kM + m;
-        const int g0 = (d - 12) >> 2;  // floor
-        c0 = (d - 12) - 4 * g0;
-#pragma unroll
-        for (int k = 0; k < kCurveWords; ++k) {
-            const int g = g0 + k;
-            cw[k] = (x < a.W && g >= 0 && g < a.groups)
-                        ? __ldg(a.curve + ((size_t)y * a.groups + g) * a.curve_pitch + x + 2)
-                        : 0xFFFFFFFFu;
+    auto load_box = [&](TilePos q) {  // warp 1, all lanes (they count the loads)
+        if ((tid & 31) == 0) {
+            dev::mbar_arrive_expect_tx(&bars[2], kBoxBytes);
+            dev::tma_load_3d(smem + kBox, &tm_curve, q.tx * kM, 0, q.y, &bars[2]);
         }
+        ++cm[2];
     };
 
-    // the 255 padding of the staging row never changes
-    for (int k = kCurveWords; k < kStageWords; ++k) stage[k] = 0xFFFFFFFFu;
-
-    // A1 of the tile whose curve words are in cw: the 35 codes around the
-    // winner, 15 per K=16 window
-    auto build_a1 = [&]() {
-#pragma unroll
-        for (int k = 0; k < kCurveWords; ++k) stage[k] = cw[k];
+    // A1 of the tile whose curve block is in the box: the 35 codes around
+    // the winner d (curve bytes d - 12 .. d + 22; 255 outside the curve),
+    // 15 per K=16 window
+    auto build_a1 = [&](int d) {
+        const int g0 = (d - 12) >> 2;  // floor: word of the first code
+        const int c0 = (d - 12) - 4 * g0;
 #pragma unroll
         for (int t3 = 0; t3 < 3; ++t3) {
-            const int b0 = c0 + 15 * t3, w0 = b0 >> 2, sh = (b0 & 3) * 8;  // row bytes b0 .. b0 + 15
+            const int b0 = c0 + 15 * t3, w0 = b0 >> 2, sh = (b0 & 3) * 8;  // codes b0 .. b0 + 15
             uint32_t r[5], v[4];
 #pragma unroll
-            for (int k = 0; k < 5; ++k) r[k] = stage[w0 + k];
+            for (int k = 0; k < 5; ++k) {
+                const int g = g0 + w0 + k;
+                r[k] = unsigned(g) < unsigned(kGroups) ? box[g * kBoxWords] : 0xFFFFFFFFu;
+            }
 #pragma unroll
             for (int k = 0; k < 4; ++k) v[k] = __funnelshift_r(r[k], r[k + 1], sh);
             unsigned char* dst = A1 + 2 * t3 * kChunkBytes + m * 16;
@@ -769,14 +788,18 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
     };
 
     int t = blockIdx.x;
-    int d_next = 0;
+    TilePos p_cur{t / tiles_x, t % tiles_x};  // tiles t, t + G, t + 2 G
+    TilePos p_next = advance(p_cur), p_next2 = advance(p_next);
+    uint32_t e_cur = 0, e_next = 0, e_next2 = 0;  // their disparity entries
     if (t < tiles) {
-        load_curve(t, load_winner(t));
-        build_a1();
+        e_cur = load_entry(p_cur);
+        if (warp == 1) load_box(p_cur);
+        if (__syncthreads_or(!wait_bar(2))) failed = true;
+        else build_a1(entry_winner(e_cur, a.disp_type));
     }
-    if (t + (int)gridDim.x < tiles) d_next = load_winner(t + gridDim.x);
-    for (; t < tiles; t += gridDim.x) {
-        const int y = t / tiles_x, x0 = (t % tiles_x) * kM;
+    if (t + (int)gridDim.x < tiles) e_next = load_entry(p_next);
+    for (; t < tiles && !failed; t += gridDim.x) {
+        const int y = p_cur.y, x0 = p_cur.tx * kM;
         // ---- conv1 biases into C1 (A1 was built while the previous tile's fc1 ran)
 #pragma unroll
         for (int q = 0; q < 7; ++q) st32(tl + 32 * q, bias1);
@@ -789,8 +812,9 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
             mma_ss(tm + 192, dplus(dA1, 4 * kChunkBytes), dB1, kIdC1n);
             commit_to(0);
         }
-        if (t + (int)gridDim.x < tiles) load_curve(t + gridDim.x, d_next);  // next tile, behind the MMAs
-        if (t + 2 * (int)gridDim.x < tiles) d_next = load_winner(t + 2 * gridDim.x);
+        // the next tile's curve block (the box was last read by this tile's A1 build)
+        if (warp == 1 && t + (int)gridDim.x < tiles) load_box(p_next);
+        if (t + 2 * (int)gridDim.x < tiles) e_next2 = load_entry(p_next2);
         if (__syncthreads_or(!wait_bar(0))) { failed = true; break; }
         fence_after();
         // ---- conv1 epilogue: A2 position q (bf16) over the consumed C1 columns
@@ -863,48 +887,65 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(InferArgs a) {
         }
         // the next tile's A1 while fc1 runs (this tile's conv1 MMAs, the only
         // readers of A1, completed before the conv1 epilogue)
-        if (t + (int)gridDim.x < tiles) build_a1();
-        if (__syncthreads_or(!wait_bar(1))) { failed = true; break; }
+        bool box_ok = true;
+        if (t + (int)gridDim.x < tiles) {
+            box_ok = wait_bar(2);
+            if (box_ok) build_a1(entry_winner(e_next, a.disp_type));
+        }
+        if (__syncthreads_or(!box_ok || !wait_bar(1))) { failed = true; break; }
         fence_after();
         // ---- fc1 epilogue + fc2
         {
             float v0[32], v1[32];
             ld32x2(tl + kC4, tl + kC4 + 32, v0, v1);
-            float z[4] = {b5, 0.f, 0.f, 0.f};  // four independent chains
+            float z[8] = {b5, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // eight independent chains
+            const float4* w5v = reinterpret_cast<const float4*>(w5);  // 16-byte aligned in the image
 #pragma unroll
-            for (int c = 0; c < 32; c += 2) {
-                z[0] = fmaf(w5[c], fmaxf(v0[c], 0.f), z[0]);
-                z[1] = fmaf(w5[c + 1], fmaxf(v0[c + 1], 0.f), z[1]);
-                z[2] = fmaf(w5[32 + c], fmaxf(v1[c], 0.f), z[2]);
-                z[3] = fmaf(w5[33 + c], fmaxf(v1[c + 1], 0.f), z[3]);
+            for (int c = 0; c < 8; ++c) {
+                const float4 wa = w5v[c], wb = w5v[8 + c];
+                z[0] = fmaf(wa.x, fmaxf(v0[4 * c], 0.f), z[0]);
+                z[1] = fmaf(wa.y, fmaxf(v0[4 * c + 1], 0.f), z[1]);
+                z[2] = fmaf(wa.z, fmaxf(v0[4 * c + 2], 0.f), z[2]);
+                z[3] = fmaf(wa.w, fmaxf(v0[4 * c + 3], 0.f), z[3]);
+                z[4] = fmaf(wb.x, fmaxf(v1[4 * c], 0.f), z[4]);
+                z[5] = fmaf(wb.y, fmaxf(v1[4 * c + 1], 0.f), z[5]);
+                z[6] = fmaf(wb.z, fmaxf(v1[4 * c + 2], 0.f), z[6]);
+                z[7] = fmaf(wb.w, fmaxf(v1[4 * c + 3], 0.f), z[7]);
             }
-            const float p = 1.f / (1.f + __expf(-((z[0] + z[1]) + (z[2] + z[3]))));
+            const float logit = ((z[0] + z[1]) + (z[2] + z[3])) + ((z[4] + z[5]) + (z[6] + z[7]));
+            const float p = __fdividef(1.f, 1.f + __expf(-logit));  // 0 once exp overflows
             const int x = x0 + m;
             if (x < a.W) {
                 if (a.score) reinterpret_cast<float*>(reinterpret_cast<char*>(a.score) + (size_t)y * a.score_pitch)[x] = p;
                 if (a.checked) {  // same encoding as the cross-check's output map
-                    const char* drow = static_cast<const char*>(a.disp) + (size_t)y * a.disp_pitch;
                     char* crow = static_cast<char*>(a.checked) + (size_t)y * a.checked_pitch;
                     if (a.disp_type == CT_PIX_U8) {
-                        const uint8_t v = reinterpret_cast<const uint8_t*>(drow)[x];
-                        reinterpret_cast<uint8_t*>(crow)[x] = p >= a.threshold ? v : uint8_t(0xFF);
+                        reinterpret_cast<uint8_t*>(crow)[x] = p >= a.threshold ? uint8_t(e_cur) : uint8_t(0xFF);
                     } else {
-                        const uint16_t v = reinterpret_cast<const uint16_t*>(drow)[x];
-                        const bool disp = v >= CT_DISP_FIRST && v <= CT_DISP_LAST;
+                        const bool disp = e_cur >= CT_DISP_FIRST && e_cur <= CT_DISP_LAST;
                         reinterpret_cast<uint16_t*>(crow)[x] =
-                            (disp && p < a.threshold) ? uint16_t(CT_DISP_INCONSISTENT) : v;
+                            (disp && p < a.threshold) ? uint16_t(CT_DISP_INCONSISTENT) : uint16_t(e_cur);
                     }
                 }
             }
         }
+        e_cur = e_next;
+        e_next = e_next2;
+        p_cur = p_next;
+        p_next = p_next2;
+        p_next2 = advance(p_next2);
         fence_before();  // this tile's TMEM reads before the next tile's writes
     }
     // After a timeout, MMAs may still be in flight: wait (bounded) for every
     // commit not yet waited for before giving the TMEM back.
-    if (failed && tid == 0) {
-        dev::report(a.status, CT_ETIMEOUT);
-        for (int b = 0; b < 2; ++b)
-            for (uint32_t k = ph[b]; k < cm[b]; ++k) dev::mbar_wait_bounded(&bars[b], k & 1);
+    if (failed && tid == 0) dev::report(a.status, CT_ETIMEOUT);
+    if (failed && (tid & 31) == 0) {  // warp 0 issued the MMAs, warp 1 the TMA loads
+        if (warp == 0) {
+            for (uint32_t k = ph[0]; k < cm[0]; ++k) dev::mbar_wait_bounded(&bars[0], k & 1);
+            for (uint32_t k = ph[1]; k < cm[1]; ++k) dev::mbar_wait_bounded(&bars[1], k & 1);
+        } else if (warp == 1) {
+            for (uint32_t k = ph[2]; k < cm[2]; ++k) dev::mbar_wait_bounded(&bars[2], k & 1);
+        }
     }
     fence_before();
     __syncthreads();
@@ -1282,7 +1323,15 @@ int ct_confnet_infer(ct_handle* hh, const ct_image* score, const ct_curves* curv
     a.status = h->d_status;
     const int tiles = ((a.W + inf::kM - 1) / inf::kM) * a.H;
     const int grid = tiles < 2 * h->sms ? tiles : 2 * h->sms;  // two CTAs per SM
-    inf::infer_kernel<<<grid, inf::kNT, inf::kSmem, s>>>(a);
+    // the curve volume as a 3D tensor (words along x, disparity group, row)
+    // for the kernel's per-tile block loads
+    CUtensorMap tm_curve;
+    const uint64_t dims[3] = {uint64_t(a.W) + 2, uint64_t(inf::kGroups), uint64_t(a.H)};
+    const uint64_t strides[2] = {curves->pitch_bytes, curves->pitch_bytes * inf::kGroups};
+    const uint32_t box[3] = {uint32_t(inf::kBoxWords), uint32_t(inf::kGroups), 1};
+    if (int rc = make_tmap_nd(&tm_curve, curves->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, 3, dims, strides, box))
+        return rc;
+    inf::infer_kernel<<<grid, inf::kNT, inf::kSmem, s>>>(tm_curve, a);
     CT_LAUNCH_CHECK();
     return CT_OK;
 }
