@@ -67,6 +67,49 @@ def dist_info():
         os.environ.get("LOCAL_RANK", 0))
 
 
+# Ranks are independent replicas (one pair per GPU, no collective on the data
+# path); the only collectives are barriers around the timed regions and the
+# max over ranks of the timings. NCCL on GPUs, gloo for CPU processes.
+def init_ranks(world, dev):
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        kw = {"device_id": dev} if dev.type == "cuda" else {}
+        dist.init_process_group("nccl" if dev.type == "cuda" else "gloo",
+                                timeout=datetime.timedelta(seconds=120), **kw)
+
+
+def rank_barrier(world, dev):
+    import torch
+    if dev.type == "cuda":
+        torch.cuda.synchronize(dev)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v, world, dev):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def close_ranks(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def replica_seed(rank):
+    """Each replica matches its own seeded pair."""
+    return SEED + rank
+
+
 def units_per_step():
     return 2 * W_ * H_ * D_
 
@@ -248,13 +291,10 @@ def run_ours(args):
     rank, world, local = dist_info()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    init_ranks(world, dev)
     stream = torch.cuda.current_stream(dev)
 
-    L, R, G, O = ct.synth_pair(2, SEED + rank, W_, H_, D_ - 1)
+    L, R, G, O = ct.synth_pair(2, replica_seed(rank), W_, H_, D_ - 1)
     dL = ct.alloc_image(H_, W_, torch.uint8, dev)
     dR = ct.alloc_image(H_, W_, torch.uint8, dev)
     dL.copy_(torch.from_numpy(L))
@@ -277,18 +317,7 @@ def run_ours(args):
     rates = ct.probe_pipe_rates(local)
 
     def barrier():
-        torch.cuda.synchronize(dev)
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
-
-    def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        import torch.distributed as dist
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        rank_barrier(world, dev)
 
     for _ in range(max(3, args.warmup)):
         flush()
@@ -303,7 +332,7 @@ def run_ours(args):
             ev[k][1].record(stream)
         barrier()
         step_ms = [a.elapsed_time(b) for a, b in ev]
-        total_ms = max_over_ranks(sum(step_ms))
+        total_ms = max_over_ranks(sum(step_ms), world, dev)
 
         # dominant kernel: one left-to-right pass (census of both images +
         # census_match_kernel) minus the two census transforms, both timed
@@ -353,7 +382,7 @@ def run_ours(args):
             hOut.copy_(ck, non_blocking=True)
             eev[k][1].record(stream)
         barrier()
-        e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in eev) / args.steps)
+        e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in eev) / args.steps, world, dev)
         conf = confnet_compare(ct, dev, stream, m, dL, dR, hL, hR, flush, args.steps,
                                args.eval_pairs or 4, local) if rank == 0 else None
     clocks = clk.summary()
@@ -414,10 +443,7 @@ def run_ours(args):
         out["cpu_baseline"] = {"value": round(units_per_step() / cpu_ms / 1e6, 1), "unit": UNIT, "cores": cores,
                                "kind": "port", "sample": "3 full pipelines (1920x1080, D=128, LR+RL+check)"}
         print(json.dumps(out), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-        dist.destroy_process_group()
+    close_ranks(world)
     return 0
 
 
@@ -506,10 +532,7 @@ def run_workload(args):
     rank, world, local = dist_info()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    init_ranks(world, dev)
     stream = torch.cuda.current_stream(dev)
     flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     wl = args.workload
@@ -590,10 +613,7 @@ def run_workload(args):
     for _ in range(max(3, args.warmup)):
         flush_buf.zero_()
         step()
-    torch.cuda.synchronize(dev)
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    rank_barrier(world, dev)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     with ClockSampler(torch.cuda.current_device()) as clk:
         for k in range(args.steps):
@@ -603,12 +623,7 @@ def run_workload(args):
             ev[k][1].record(stream)
         torch.cuda.synchronize(dev)
     clocks = clk.summary()
-    ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev) / args.steps, world, dev)
     value = world * units / (ms * 1e-3) / 1e6
     out_line = {
         "metric": metric, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -623,10 +638,7 @@ def run_workload(args):
         out_line["cpu_baseline"] = {"value": round(v, 1), "unit": UNIT, "cores": oracle.num_threads(),
                                     "kind": "port", "sample": sample}
         print(json.dumps(out_line), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-        dist.destroy_process_group()
+    close_ranks(world)
     return 0
 
 
