@@ -356,6 +356,35 @@ int ct_batch_strip_height(ct_handle* h, int32_t pair, int32_t* strip_height);
 int ct_batch_graph_create(ct_handle* h, const ct_batch_item* items, int32_t n);
 int ct_batch_graph_launch(ct_handle* h, ct_stream stream);
 
+/* ---- streamed census stereo ----------------------------------------------
+ * Frames in host memory in, cross-checked maps in host memory out, with the
+ * upload of one frame and the download of another overlapping the matching
+ * of a third (three device slots; copies and matching on three internal
+ * streams ordered by events). Each frame's map equals
+ * ct_bm_census_process_lr(disp_checked) on that pair. No counterpart in the
+ * reference (its CDeviceSurface::CopyFrom / CopyInto are synchronous copies
+ * around a blocking Process). Host images are rows of `pitch` bytes;
+ * page-locked memory (cudaHostAlloc / cudaHostRegister) lets the copies run
+ * behind the matching, pageable memory works but serialises frames. */
+int ct_census_stream_create(ct_handle** out);
+/* fmt: the pair's format (U8); p: the census matcher parameters (D, radius 2);
+ * tol: cross-check tolerance; out_type: CT_PIX_U8 or CT_PIX_U16 maps. */
+int ct_census_stream_configure(ct_handle* h, int32_t device, const ct_format* fmt,
+                               const ct_census_match_params* p, int32_t tol, int32_t out_type);
+/* Enqueues one frame and returns at once with its number in *frame. left,
+ * right and checked must stay valid, and left / right unchanged, until
+ * ct_census_stream_wait for that frame has returned. */
+int ct_census_stream_submit(ct_handle* h, const void* left, size_t left_pitch, const void* right,
+                            size_t right_pitch, void* checked, size_t checked_pitch, int64_t* frame);
+/* Blocks until the frame's map is in host memory (also reports a device
+ * status word set by the matching, as CT_ETIMEOUT / CT_EINTERNAL). */
+int ct_census_stream_wait(ct_handle* h, int64_t frame);
+/* Device time of a run of frames: start marks the point before the next
+ * frame's upload; stop waits for every submitted frame and returns the
+ * milliseconds from the mark to the end of the last download. */
+int ct_census_stream_timer_start(ct_handle* h);
+int ct_census_stream_timer_stop(ct_handle* h, float* ms);
+
 /* ---- synthetic stereo pairs -----------------------------------------------
  * Seeded generator of rectified stereo pairs with ground truth (host memory).
  *   kind 1: fractal value noise (4 octaves) left image; disparity = 4

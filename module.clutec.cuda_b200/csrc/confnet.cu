@@ -728,10 +728,16 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(const __grid_constant__ C
         if (ok) ++ph[b];
         return ok;
     };
-    auto bias_to_tmem = [&](uint32_t col, const float* src) {
+    auto bias_to_tmem = [&](uint32_t col, const float* src) {  // src 16-byte aligned
         float bv[32];
 #pragma unroll
-        for (int c = 0; c < 32; ++c) bv[c] = src[c];
+        for (int c = 0; c < 8; ++c) {
+            const float4 q = reinterpret_cast<const float4*>(src)[c];
+            bv[4 * c] = q.x;
+            bv[4 * c + 1] = q.y;
+            bv[4 * c + 2] = q.z;
+            bv[4 * c + 3] = q.w;
+        }
         st32(tl + col, bv);
     };
     // all threads: make this thread's TMEM / shared writes visible, then let
@@ -767,17 +773,28 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(const __grid_constant__ C
     auto build_a1 = [&](int d) {
         const int g0 = (d - 12) >> 2;  // floor: word of the first code
         const int c0 = (d - 12) - 4 * g0;
+        // words g0 .. g0 + 9 hold the 35 codes (bytes c0 .. c0 + 34); later
+        // words only feed codes that meet zero weights, so they read 255
+        uint32_t w[13];
+#pragma unroll
+        for (int k = 0; k < 10; ++k) {
+            const int g = g0 + k;
+            w[k] = unsigned(g) < unsigned(kGroups) ? box[g * kBoxWords] : 0xFFFFFFFFu;
+        }
+        w[10] = w[11] = w[12] = 0xFFFFFFFFu;
 #pragma unroll
         for (int t3 = 0; t3 < 3; ++t3) {
-            const int b0 = c0 + 15 * t3, w0 = b0 >> 2, sh = (b0 & 3) * 8;  // codes b0 .. b0 + 15
-            uint32_t r[5], v[4];
+            // codes b0 .. b0 + 15 start in word b0 / 4, one of two words per window
+            const int b0 = c0 + 15 * t3, sh = (b0 & 3) * 8;
+            const bool hi = t3 == 0 ? false : (t3 == 1 ? c0 >= 1 : c0 >= 2);
+            constexpr int kLo[3] = {0, 3, 7};
+            uint32_t v[4];
 #pragma unroll
-            for (int k = 0; k < 5; ++k) {
-                const int g = g0 + w0 + k;
-                r[k] = unsigned(g) < unsigned(kGroups) ? box[g * kBoxWords] : 0xFFFFFFFFu;
+            for (int k = 0; k < 4; ++k) {
+                const uint32_t r0 = hi ? w[kLo[t3] + k + 1] : w[kLo[t3] + k];
+                const uint32_t r1 = hi ? w[kLo[t3] + k + 2] : w[kLo[t3] + k + 1];
+                v[k] = __funnelshift_r(r0, r1, sh);
             }
-#pragma unroll
-            for (int k = 0; k < 4; ++k) v[k] = __funnelshift_r(r[k], r[k + 1], sh);
             unsigned char* dst = A1 + 2 * t3 * kChunkBytes + m * 16;
             *reinterpret_cast<uint4*>(dst) = make_uint4(codes_f16x2(v[0], 0x4140), codes_f16x2(v[0], 0x4342),
                                                         codes_f16x2(v[1], 0x4140), codes_f16x2(v[1], 0x4342));

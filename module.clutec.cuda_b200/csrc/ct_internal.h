@@ -26,6 +26,7 @@ enum class Kind : int32_t {
     CrossCheck = 6,
     Batch = 7,
     ConfNet = 8,
+    Stream = 9,
 };
 
 // Sets the thread-local message returned by ct_last_error_string and returns

@@ -171,6 +171,13 @@ def _declare(L: C.CDLL) -> None:
         "ct_batch_strip_height": [H, C.c_int32, P(C.c_int32)],
         "ct_batch_graph_create": [H, P(ct_batch_item), C.c_int32],
         "ct_batch_graph_launch": [H, C.c_void_p],
+        "ct_census_stream_create": [P(H)],
+        "ct_census_stream_configure": [H, C.c_int32, fmt, P(ct_census_match_params), C.c_int32, C.c_int32],
+        "ct_census_stream_submit": [H, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
+                                    P(C.c_int64)],
+        "ct_census_stream_wait": [H, C.c_int64],
+        "ct_census_stream_timer_start": [H],
+        "ct_census_stream_timer_stop": [H, P(C.c_float)],
         "ct_synth_pair": [C.c_int32, C.c_uint64, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
                           C.c_void_p, C.c_void_p],
         "ct_probe_pipe_rates": [C.c_int32, P(ct_pipe_rates)],
@@ -444,6 +451,49 @@ class BatchStereo(_Driver):
 
     def graph_launch(self, stream=None):
         check(lib().ct_batch_graph_launch(self._h, _stream(stream)))
+
+
+class CensusStream(_Driver):
+    """Streamed census stereo (ct_census_stream_*): host frames in, host
+    cross-checked maps out, copies of neighbouring frames overlapping the
+    matching. Host images are 2-D CPU tensors (pin_memory() ones overlap)."""
+    _create = "ct_census_stream_create"
+
+    def configure(self, device: int, width: int, height: int, disp_count: int, tol: int = 1, out_type=None):
+        import torch
+        self.out_dtype = torch.uint8 if out_type in (None, torch.uint8) else torch.int16
+        ot = CT_PIX_U8 if self.out_dtype == torch.uint8 else CT_PIX_U16
+        check(lib().ct_census_stream_configure(self._h, device, C.byref(_fmt(width, height)),
+                                               C.byref(ct_census_match_params(disp_count, 2, 1, 0)), tol, ot))
+        self._held = {}
+
+    @staticmethod
+    def _host(t):
+        if t.device.type != "cpu" or t.dim() != 2 or t.stride(1) != 1:
+            raise CtError(CT_EINVAL, "host images must be 2-D CPU tensors with unit column stride")
+        return C.c_void_p(t.data_ptr()), t.stride(0) * t.element_size()
+
+    def submit(self, left, right, checked) -> int:
+        """Enqueues a frame; returns its number. The tensors stay referenced
+        (and must stay unchanged) until wait() for that frame."""
+        (pl, sl), (pr, sr), (po, so) = self._host(left), self._host(right), self._host(checked)
+        k = C.c_int64()
+        check(lib().ct_census_stream_submit(self._h, pl, sl, pr, sr, po, so, C.byref(k)))
+        self._held[k.value] = (left, right, checked)
+        return k.value
+
+    def wait(self, frame: int):
+        check(lib().ct_census_stream_wait(self._h, frame))
+        for f in [f for f in self._held if f <= frame]:
+            del self._held[f]
+
+    def timer_start(self):
+        check(lib().ct_census_stream_timer_start(self._h))
+
+    def timer_stop(self) -> float:
+        ms = C.c_float()
+        check(lib().ct_census_stream_timer_stop(self._h, C.byref(ms)))
+        return ms.value
 
 
 class ConfNet(_Driver):

@@ -58,3 +58,23 @@ def test_parameter_validation_before_any_device_call(ct):
 
 def test_synth_rejects_bad_kind(ct):
     assert ct.lib().ct_synth_pair(9, 1, 16, 16, 8, None, None, None, None) == ct.CT_EINVAL
+
+
+def test_stream_argument_checks(ct):
+    """ct_census_stream_*: state and argument errors before any device call."""
+    L = ct.lib()
+    h = C.c_void_p()
+    assert L.ct_census_stream_create(C.byref(h)) == ct.CT_OK
+    k = C.c_int64()
+    buf = C.create_string_buffer(64)
+    assert L.ct_census_stream_submit(h, buf, 8, buf, 8, buf, 8, C.byref(k)) == ct.CT_ESTATE
+    assert L.ct_census_stream_wait(h, 0) == ct.CT_ESTATE
+    assert L.ct_census_stream_timer_start(h) == ct.CT_ESTATE
+    fmt = ct.ct_format(64, 32, ct.CT_PIX_U8)
+    p = ct.ct_census_match_params(64, 2, 1, 0)
+    assert L.ct_census_stream_configure(h, 0, C.byref(fmt), C.byref(p), -1, ct.CT_PIX_U8) == ct.CT_EINVAL
+    assert L.ct_census_stream_configure(h, 0, C.byref(fmt), C.byref(p), 1, ct.CT_PIX_F32) == ct.CT_ETYPE
+    p300 = ct.ct_census_match_params(256, 2, 1, 0)
+    assert L.ct_census_stream_configure(h, 0, C.byref(fmt), C.byref(p300), 1, ct.CT_PIX_U8) == ct.CT_ETYPE
+    assert L.ct_census_stream_configure(h, 0, None, C.byref(p), 1, ct.CT_PIX_U8) == ct.CT_EINVAL
+    assert L.ct_destroy(h) == ct.CT_OK
