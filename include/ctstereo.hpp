@@ -23,7 +23,8 @@
  *   BlockMatcherAW1::{EConfig, ESimType, SParameter, CDriver} (BlockMatcherAW1.h:41-157)
  *   CrossCheckDisparityMaps::{SParameter, CDriver} (CrossCheckDisparityMaps.h:38-117)
  * and, with no reference counterpart: BlockMatcherCensus (census pipeline in
- * one call, with cost-curve export), BatchStereo (many pairs per launch) and
+ * one call, with cost-curve export), CensusStream (host frames in, maps out,
+ * copies overlapping the matching), BatchStereo (many pairs per launch) and
  * ConfidenceNet (learned confidence over the cost curves).
  *
  * Errors: every failing C call becomes a CError exception carrying the CT_E*
@@ -647,6 +648,52 @@ public:
 };
 
 }  // namespace BlockMatcherCensus
+
+/* A stream of frames in host memory: census both ways + cross-check per
+ * frame, uploads and downloads of neighbouring frames overlapping the
+ * matching. Host buffers must stay valid (inputs unchanged) until Wait for
+ * their frame; page-locked memory lets the copies overlap. */
+namespace CensusStream {
+
+class CDriver : public CKernelDriverBase {
+public:
+    CDriver() : CKernelDriverBase("Census Stream") {}
+
+    void Configure(const CDevice& xDevice, const SImageFormat& xFormat, const BlockMatcherCensus::SParameter& xPars,
+                   int iDispDeltaThresh, EDataType eDispType = EDataType::UInt8) {
+        detail::RequireInputFormat(xFormat, "CensusStream");
+        detail::RequireDispConfig(xPars.xDispConfig, "CensusStream");
+        if (!xPars.bLeftToRight) throw CError(CT_EINVAL, "CensusStream: the checked map is the left view's");
+        EnsureHandle(ct_census_stream_create);
+        const ct_format f = xFormat.ToC();
+        const ct_census_match_params p{xPars.xDispConfig.iRange, xPars.iAggRadius, 1, 0};
+        Ensure(ct_census_stream_configure(m_pHandle, xDevice.iDevice, &f, &p, iDispDeltaThresh,
+                                          static_cast<int32_t>(eDispType)),
+               "CensusStream::Configure");
+    }
+
+    /* Returns the frame number to Wait for. */
+    int64_t Submit(const void* pLeft, size_t nLeftPitch, const void* pRight, size_t nRightPitch, void* pDisp,
+                   size_t nDispPitch) {
+        int64_t k = -1;
+        Ensure(ct_census_stream_submit(m_pHandle, pLeft, nLeftPitch, pRight, nRightPitch, pDisp, nDispPitch, &k),
+               "CensusStream::Submit");
+        return k;
+    }
+
+    void Wait(int64_t iFrame) { Ensure(ct_census_stream_wait(m_pHandle, iFrame), "CensusStream::Wait"); }
+
+    /* Device milliseconds from the next Submit's upload to the end of the
+     * last download (TimerStop waits for every submitted frame). */
+    void TimerStart() { Ensure(ct_census_stream_timer_start(m_pHandle), "CensusStream::TimerStart"); }
+    float TimerStop() {
+        float ms = 0.f;
+        Ensure(ct_census_stream_timer_stop(m_pHandle, &ms), "CensusStream::TimerStop");
+        return ms;
+    }
+};
+
+}  // namespace CensusStream
 
 /* Many pairs of mixed size per call: census both ways + cross-check. */
 namespace BatchStereo {

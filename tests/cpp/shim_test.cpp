@@ -115,6 +115,16 @@ static int RunCpu() {
         ConfidenceNet::CDriver d;
         CHECK(ThrownCode([&] { d.LoadParams("/nonexistent/weights.f32"); }) == CT_EINVAL, "missing weight file");
     }
+    {
+        CensusStream::CDriver d;
+        BlockMatcherCensus::SParameter p;
+        p.xDispConfig.Set(0, 64);
+        p.bLeftToRight = false;
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p, 1); }) == CT_EINVAL, "stream of right-view maps");
+        p.bLeftToRight = true;
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p, 1, EDataType::Single); }) == CT_ETYPE, "F32 stream maps");
+        CHECK(ThrownCode([&] { d.Submit(nullptr, 0, nullptr, 0, nullptr, 0); }) == CT_ESTATE, "unconfigured stream");
+    }
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
     if (n == 0) {
@@ -241,6 +251,18 @@ static int RunGpu(const char* weights) {
         CHECK(differ == 0, "ProcessLR and the cross-check driver disagree on %d pixels", differ);
         CHECK(cc.DispMin() <= K && cc.DispMax() >= K, "range %d..%d", cc.DispMin(), cc.DispMax());
         m.EnsureDeviceStatus();
+
+        // the same pair as a stream of frames from host memory
+        CensusStream::CDriver st;
+        st.Configure(dev, fin, p, 1, EDataType::UInt16);
+        std::vector<std::vector<uint16_t>> frames(4, std::vector<uint16_t>(size_t(W) * H));
+        int64_t last = -1;
+        for (auto& fr : frames) last = st.Submit(L.data(), W, R.data(), W, fr.data(), size_t(W) * 2);
+        st.Wait(last);
+        int sdiff = 0;
+        for (const auto& fr : frames)
+            for (size_t i = 0; i < fr.size(); ++i) sdiff += fr[i] != a[i];
+        CHECK(last == 3 && sdiff == 0, "stream: %d pixels differ from ProcessLR", sdiff);
 
         // learned confidence on the same pair: checked = winner map with
         // every pixel scoring below the threshold marked Inconsistent
