@@ -262,8 +262,14 @@ typedef struct ct_ncc_params {
 int ct_bm_ncc_create(ct_handle** out);
 int ct_bm_ncc_configure(ct_handle* h, int32_t device, const ct_format* fmt, const ct_ncc_params* p);
 /* disp U8/U16; score (nullable) F32 = NCC at the chosen d (0 for invalid
- * pixels); disp_init must be NULL (the guided MatcherUseDisparity mode is not
- * built). */
+ * pixels). disp_init (nullable) switches on the guided mode
+ * (MatcherUseDisparity, BlockMatcherNCC.cu:894-1255): a coarse disparity map
+ * (U8 or U16 encoding) whose width divides the image width, s = width /
+ * disp_init->width, with at least ceil(height / s) rows. Pixel (x, y) takes
+ * the coarse disparity at (x / s, y / s) scaled by s; the pixels of each
+ * 16 x 16 block (aligned to multiples of 16) search only
+ * [max(0, min - 4), max + 4] of their block's scaled coarse disparities, and
+ * get no disparity when none of them has one. */
 int ct_bm_ncc_process(ct_handle* h, const ct_image* disp, const ct_image* score,
                       const ct_image* left, const ct_image* right, const ct_image* disp_init,
                       ct_stream stream);

@@ -41,8 +41,9 @@
  *     CError(CT_EINVAL) when a gate that would change the winner is switched
  *     on (fGradThresh > 0); thresholds that only label the unbuilt cost
  *     channels are accepted and ignored.
- *   - Guided matching (iUseDispInput, xImageDispInit) is not built: a
- *     non-empty xImageDispInit throws.
+ *   - Guided matching (iUseDispInput + xImageDispInit) is built for
+ *     BlockMatcherNCC (search ranges per 16 x 16 block, see
+ *     ct_bm_ncc_process); BlockMatcherAW1 rejects it.
  *   - BlockMatcherAW1 computes the "best of 5 shifted 7x7 windows" cost with
  *     sub-pixel refinement (EConfig::Shifted5_7x7); the reference's 2-of-4
  *     sub-window configurations throw.
@@ -427,7 +428,7 @@ public:
         detail::RequireInputFormat(xFormat, "BlockMatcherNCC");
         detail::RequireDispConfig(xPars.xDispConfig, "BlockMatcherNCC");
         if (xPars.fGradThresh > 0.f) throw CError(CT_EINVAL, "BlockMatcherNCC: the gradient gate is not built");
-        if (xPars.iUseDispInput) throw CError(CT_EINVAL, "BlockMatcherNCC: guided matching is not built");
+        m_bUseDispInput = xPars.iUseDispInput != 0;
         static const int32_t radius[] = {5, 4, 2};
         EnsureHandle(ct_bm_ncc_create);
         const ct_format f = xFormat.ToC();
@@ -437,17 +438,24 @@ public:
     }
 
     /* xImageDisp: UInt8 or UInt16; xImageDebug, when valid, receives the
-     * Single NCC score at the chosen disparity (the build's score output);
-     * xImageDispInit must be empty. */
+     * Single NCC score at the chosen disparity (the build's score output).
+     * With iUseDispInput set, xImageDispInit is the coarse disparity map of
+     * the guided mode (MatcherUseDisparity; see ct_bm_ncc_process); without
+     * it, xImageDispInit is ignored. */
     void Process(_CDeviceSurface& xImageDisp, const _CDeviceSurface& xImageL, const _CDeviceSurface& xImageR,
                  const _CDeviceSurface& xImageDispInit, const _CDeviceSurface& xImageDebug) {
-        detail::RequireNoGuide(xImageDispInit, "BlockMatcherNCC");
-        Ensure(ct_bm_ncc_process(m_pHandle, xImageDisp.C(), xImageDebug.C(), xImageL.C(), xImageR.C(), nullptr, S()),
+        if (m_bUseDispInput && !xImageDispInit.IsValid())
+            throw CError(CT_EINVAL, "BlockMatcherNCC: iUseDispInput needs xImageDispInit");
+        Ensure(ct_bm_ncc_process(m_pHandle, xImageDisp.C(), xImageDebug.C(), xImageL.C(), xImageR.C(),
+                                 m_bUseDispInput ? xImageDispInit.C() : nullptr, S()),
                "BlockMatcherNCC::Process");
     }
     void Process(_CDeviceSurface& xImageDisp, const _CDeviceSurface& xImageL, const _CDeviceSurface& xImageR) {
         Process(xImageDisp, xImageL, xImageR, _CDeviceSurface(), _CDeviceSurface());
     }
+
+private:
+    bool m_bUseDispInput = false;
 };
 
 }  // namespace BlockMatcherNCC

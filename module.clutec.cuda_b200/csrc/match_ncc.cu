@@ -64,8 +64,46 @@ __device__ __forceinline__ float unordered(uint32_t o) {
     return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
 }
 
+// Guided mode (MatcherUseDisparity, BlockMatcherNCC.cu:980-1168): pixels
+// are grouped in 16 x 16 blocks; a block searches only
+// [max(0, min - 4), max + 4] of its pixels' coarse disparities scaled by s
+// (pixel (x, y) reads the coarse map at (x / s, y / s)), and nothing when
+// none of them has a coarse disparity. One thread per block; the range is
+// packed lo | hi << 16 (lo > hi: no search).
+constexpr int kGuideBlock = 16, kGuideMargin = 4;
+
+__global__ void guide_range_kernel(const void* coarse, size_t pitch, int type, int s, int W, int H, uint32_t* ranges,
+                                   int gw, int gh) {
+    const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y;
+    if (gx >= gw || gy >= gh) return;
+    const int x0 = gx * kGuideBlock, x1 = min(x0 + kGuideBlock, W) - 1;
+    const int y0 = gy * kGuideBlock, y1 = min(y0 + kGuideBlock, H) - 1;
+    int lo = 1 << 20, hi = -1;
+    for (int cy = y0 / s; cy <= y1 / s; ++cy) {
+        const char* row = static_cast<const char*>(coarse) + (size_t)cy * pitch;
+        for (int cx = x0 / s; cx <= x1 / s; ++cx) {
+            int d;
+            if (type == CT_PIX_U8) {
+                const int v = reinterpret_cast<const uint8_t*>(row)[cx];
+                d = v == 0xFF ? -1 : v;
+            } else {
+                const int v = reinterpret_cast<const uint16_t*>(row)[cx];
+                d = (v >= CT_DISP_FIRST && v <= CT_DISP_LAST) ? v - 1 : -1;
+            }
+            if (d >= 0) {
+                lo = min(lo, d * s);
+                hi = max(hi, d * s);
+            }
+        }
+    }
+    ranges[(size_t)gy * gw + gx] =
+        hi < 0 ? 0x0000FFFFu : (uint32_t(max(0, lo - kGuideMargin)) | (uint32_t(min(hi + kGuideMargin, 0xFFFF)) << 16));
+}
+
 struct Args {
     int W, H, D, th;
+    const uint32_t* guide;   // per 16 x 16 block search range, or null (search all D)
+    int guide_gw;
     const int32_t *Sx, *Vx, *Sy, *Vy;   // stats of the left / right image (W*H)
     unsigned long long* keys;          // global keys when gridDim.z > 1
     void* out;
@@ -122,6 +160,26 @@ __global__ void __launch_bounds__(kNT, 1)
         dev::tma_load_2d(sB, &tmB, ab, y0 - R, bar);
         dev::tma_load_2d(sM, &tmM, am, y0 - R, bar);
     }
+    // guided: skip the matching when no block of this tile searches this
+    // CTA's disparities (the outputs are still written below)
+    bool searches = true;
+    if (a.guide) {
+        int* uni = reinterpret_cast<int*>(bar + 1);  // 8 spare bytes after the mbarrier
+        if (tid == 0) { uni[0] = 1 << 20; uni[1] = -1; }
+        __syncthreads();
+        const int gx0 = max(xs + R, 0) / kGuideBlock, gx1 = (min(xs + R + TWO, a.W) - 1) / kGuideBlock;
+        const int gy0 = y0 / kGuideBlock, gy1 = (min(y0 + a.th, a.H) - 1) / kGuideBlock;
+        const int ngx = gx1 - gx0 + 1;
+        for (int i = tid; i < ngx * (gy1 - gy0 + 1); i += kNT) {
+            const uint32_t g = a.guide[(size_t)(gy0 + i / ngx) * a.guide_gw + gx0 + i % ngx];
+            if ((g & 0xFFFFu) <= (g >> 16)) {
+                atomicMin(&uni[0], int(g & 0xFFFFu));
+                atomicMax(&uni[1], int(g >> 16));
+            }
+        }
+        __syncthreads();
+        searches = uni[0] <= uni[1] && uni[1] >= dz0 && uni[0] < dz0 + kDPC;
+    }
     const bool got = dev::mbar_wait_bounded(bar, 0);
     if (__syncthreads_or(!got)) {
         if (tid == 0) dev::report(a.status, CT_ETIMEOUT);
@@ -136,7 +194,7 @@ __global__ void __launch_bounds__(kNT, 1)
 #pragma unroll
         for (int c = 0; c < kCPT; ++c) V[j][c] = 0;
 
-    if (warp_active) {
+    if (warp_active && searches) {
         for (int i = 0; i < NR; ++i) {
             {
                 const uint8_t* rb = sB + i * kBW + bo;
@@ -199,11 +257,17 @@ __global__ void __launch_bounds__(kNT, 1)
                 const size_t o = (size_t)y * a.W + x;
                 const int sx = a.Sx[o], vx = a.Vx[o];
                 const float fvx = __int2float_rn(vx);
+                int glo = 0, ghi = a.D - 1;
+                if (a.guide) {
+                    const uint32_t g = __ldg(&a.guide[(size_t)(y / kGuideBlock) * a.guide_gw + x / kGuideBlock]);
+                    glo = int(g & 0xFFFFu);
+                    ghi = min(int(g >> 16), a.D - 1);
+                }
                 unsigned long long best = 0ull;
 #pragma unroll
                 for (int j = 0; j < kDPW; ++j) {
                     const int d = dw + j;
-                    if (d >= a.D || x - d - R < 0) continue;
+                    if (d > ghi || d < glo || x - d - R < 0) continue;
                     const int sy = a.Sy[o - d], vy = a.Vy[o - d];
                     const int num = n * C[j][c] - sx * sy;
                     float sc = 0.0f;
@@ -253,17 +317,19 @@ struct NccHandle : ct_handle {
         if (device >= 0) cudaSetDevice(device);
         cudaFree(stats);
         cudaFree(keys);
+        cudaFree(guide);
     }
     ct_format fmt{};
     ct_ncc_params par{};
     int32_t* stats = nullptr;  // Sx, Vx, Sy, Vy
     unsigned long long* keys = nullptr;
+    uint32_t* guide = nullptr;  // guided mode: one search range per 16 x 16 block
     int th = 32;
 };
 
 template <int R>
 int launch_ncc(NccHandle* h, const ct_image* disp, const ct_image* score, const ct_image* L, const ct_image* Rr,
-               cudaStream_t s) {
+               const ct_image* init, cudaStream_t s) {
     using namespace ncc;
     static bool attr = false;
     if (!attr) {
@@ -281,6 +347,14 @@ int launch_ncc(NccHandle* h, const ct_image* disp, const ct_image* score, const 
     a.score = score ? static_cast<float*>(score->ptr) : nullptr;
     a.score_pitch = score ? score->pitch_bytes : 0;
     a.status = h->d_status;
+    if (init) {
+        const int gw = (W + kGuideBlock - 1) / kGuideBlock, gh = (H + kGuideBlock - 1) / kGuideBlock;
+        guide_range_kernel<<<dim3((gw + 127) / 128, gh), 128, 0, s>>>(init->ptr, init->pitch_bytes, init->type,
+                                                                      W / init->width, W, H, h->guide, gw, gh);
+        CT_LAUNCH_CHECK();
+        a.guide = h->guide;
+        a.guide_gw = gw;
+    }
     dim3 sb(32, 8), sg((W + 31) / 32, (H + 7) / 8);
     box_stats_kernel<R><<<sg, sb, 0, s>>>(static_cast<const uint8_t*>(L->ptr), L->pitch_bytes, W, H, h->stats,
                                           h->stats + N);
@@ -330,14 +404,17 @@ int ct_bm_ncc_configure(ct_handle* hh, int32_t device, const ct_format* fmt, con
     if (p->left_to_right != 1) return fail(CT_EINVAL, "the NCC matcher is left-to-right only");
     if (p->reserved != 0) return fail(CT_EINVAL, "reserved must be 0");
     if (int rc = use_device(device)) return rc;
-    cudaFree(h->stats); cudaFree(h->keys);
-    h->stats = nullptr; h->keys = nullptr;
+    cudaFree(h->stats); cudaFree(h->keys); cudaFree(h->guide);
+    h->stats = nullptr; h->keys = nullptr; h->guide = nullptr;
     h->device = device;
     if (int rc = h->init_status()) return rc;
     const size_t N = (size_t)fmt->width * fmt->height;
     if (cudaMalloc(&h->stats, 4 * N * sizeof(int32_t)) != cudaSuccess) return fail(CT_ENOMEM, "stats scratch");
     if (cudaMalloc(&h->keys, N * sizeof(unsigned long long)) != cudaSuccess) return fail(CT_ENOMEM, "key scratch");
     CT_CUDA_TRY(cudaMemset(h->keys, 0, N * sizeof(unsigned long long)));
+    const size_t G = size_t((fmt->width + ncc::kGuideBlock - 1) / ncc::kGuideBlock) *
+                     ((fmt->height + ncc::kGuideBlock - 1) / ncc::kGuideBlock);
+    if (cudaMalloc(&h->guide, G * sizeof(uint32_t)) != cudaSuccess) return fail(CT_ENOMEM, "guide ranges");
     h->fmt = *fmt;
     h->par = *p;
     h->configured = true;
@@ -350,7 +427,6 @@ int ct_bm_ncc_process(ct_handle* hh, const ct_image* disp, const ct_image* score
     auto* h = (hh && hh->kind == Kind::BmNcc) ? static_cast<NccHandle*>(hh) : nullptr;
     if (!h) return fail(CT_ESTATE, "not an NCC matcher handle");
     if (!h->configured) return fail(CT_ESTATE, "process before configure");
-    if (disp_init) return fail(CT_EINVAL, "disp_init (guided MatcherUseDisparity mode) is not built");
     if (int rc = check_image(left, "left", 1u << CT_PIX_U8)) return rc;
     if (int rc = check_image(right, "right", 1u << CT_PIX_U8)) return rc;
     if (int rc = check_same_size(left, right, "left", "right")) return rc;
@@ -363,13 +439,23 @@ int ct_bm_ncc_process(ct_handle* hh, const ct_image* disp, const ct_image* score
         if (int rc = check_image(score, "score", 1u << CT_PIX_F32)) return rc;
         if (int rc = check_same_size(score, left, "score", "left")) return rc;
     }
+    if (disp_init) {  // guided: coarse map at 1/s of the width, s a whole number
+        if (int rc = check_image(disp_init, "disp_init", (1u << CT_PIX_U8) | (1u << CT_PIX_U16))) return rc;
+        const int sc = disp_init->width > 0 ? left->width / disp_init->width : 0;
+        if (sc < 1 || sc * disp_init->width != left->width)
+            return fail(CT_EFORMAT, "disp_init width must divide the image width (scale %d / %d)", left->width,
+                        disp_init->width);
+        if (disp_init->height < (left->height + sc - 1) / sc)
+            return fail(CT_EFORMAT, "disp_init needs at least ceil(height / %d) = %d rows", sc,
+                        (left->height + sc - 1) / sc);
+    }
     if (int rc = use_device(h->device)) return rc;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     h->last_stream = s;
     switch (h->par.radius) {
-        case 2: return launch_ncc<2>(h, disp, score, left, right, s);
-        case 4: return launch_ncc<4>(h, disp, score, left, right, s);
-        default: return launch_ncc<5>(h, disp, score, left, right, s);
+        case 2: return launch_ncc<2>(h, disp, score, left, right, disp_init, s);
+        case 4: return launch_ncc<4>(h, disp, score, left, right, disp_init, s);
+        default: return launch_ncc<5>(h, disp, score, left, right, disp_init, s);
     }
 }
 

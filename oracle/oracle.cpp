@@ -342,8 +342,19 @@ void or_match_aw(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, in
 // Outputs: disp (int16, -1 invalid), best32 (FP32 score at the argmax),
 // best64 (FP64 score at that same d).
 // ---------------------------------------------------------------------------
+// Guided variant (MatcherUseDisparity, BlockMatcherNCC.cu:980-1168): pixel
+// (x, y) searches only d in [lo[y W + x], hi[y W + x]]; lo > hi means no
+// search (the pixel gets no disparity). or_match_ncc is the unguided case.
+void or_match_ncc_guided(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, int D, int r,
+                         const int32_t* lo, const int32_t* hi, int16_t* disp, float* best32, double* best64);
+
 void or_match_ncc(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, int D, int r,
                   int16_t* disp, float* best32, double* best64) {
+    or_match_ncc_guided(L, R, W, H, pitch, D, r, nullptr, nullptr, disp, best32, best64);
+}
+
+void or_match_ncc_guided(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, int D, int r,
+                         const int32_t* lo, const int32_t* hi, int16_t* disp, float* best32, double* best64) {
     const int n = (2 * r + 1) * (2 * r + 1), K = 2 * r + 1;
     const int64_t n4 = (int64_t)n * n * n * n;
     // per-pixel box sums of L, L^2, R, R^2 (independent of d)
@@ -397,7 +408,8 @@ void or_match_ncc(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, i
                         const size_t ro = (size_t)(y - y0) * W;
                         for (int x = r; x < W - r; ++x) {
                             acc += colsum[x + r];
-                            if (x - d - r >= 0) {
+                            if (x - d - r >= 0 &&
+                                (!lo || (d >= lo[(size_t)y * W + x] && d <= hi[(size_t)y * W + x]))) {
                                 const size_t o = (size_t)y * W + x, om = o - d;
                                 const int64_t sx = bl[o], sxx = bll[o], sy = br[om], syy = brr[om];
                                 const int64_t vx = n * sxx - sx * sx, vy = n * syy - sy * sy;

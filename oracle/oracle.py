@@ -42,6 +42,7 @@ def lib() -> C.CDLL:
         _lib.or_match_sad.argtypes = [vp, vp, i, i, i, i, i, i, vp, vp]
         _lib.or_match_aw.argtypes = [vp, vp, i, i, i, i, vp, vp, vp, vp]
         _lib.or_match_ncc.argtypes = [vp, vp, i, i, i, i, i, vp, vp, vp]
+        _lib.or_match_ncc_guided.argtypes = [vp, vp, i, i, i, i, i, vp, vp, vp, vp, vp]
         _lib.or_crosscheck.argtypes = [vp, vp, i, i, i, i, vp, vp]
     return _lib
 
@@ -134,6 +135,52 @@ def match_ncc(L, R, D, r=5):
     s32 = np.empty((H, W), np.float32)
     s64 = np.empty((H, W), np.float64)
     lib().or_match_ncc(_p(L), _p(R), W, H, W, D, r, _p(disp), _p(s32), _p(s64))
+    return disp, s32, s64
+
+
+GUIDE_BLOCK = 16   # pixels per side of a guide group
+GUIDE_MARGIN = 4   # disparities searched below / above the group's coarse range
+
+
+def guide_ranges(coarse, W, H):
+    """Search ranges of the guided mode (MatcherUseDisparity,
+    BlockMatcherNCC.cu:980-1168), per pixel: coarse is an int16 disparity map
+    (-1 = no disparity) with W / coarse.shape[1] = s an integer. Pixel (x, y)
+    reads the coarse disparity at (x // s, y // s), scaled by s; the pixels of
+    each 16 x 16 block (blocks aligned to multiples of 16) share the range
+    [max(0, min - 4), max + 4] of their block's scaled coarse disparities, or
+    no range (lo > hi) when the block has none. -> (lo, hi) int32 (H, W)."""
+    coarse = np.asarray(coarse, np.int16)
+    Hc, Wc = coarse.shape
+    s = W // Wc
+    assert s * Wc == W and -(-H // s) <= Hc
+    ys, xs = np.arange(H) // s, np.arange(W) // s
+    up = coarse[ys][:, xs].astype(np.int64)
+    up = np.where(up >= 0, up * s, -1)
+    B = GUIDE_BLOCK
+    gh, gw = -(-H // B), -(-W // B)
+    lo = np.full((gh, gw), 1 << 20, np.int64)
+    hi = np.full((gh, gw), -1, np.int64)
+    for gy in range(gh):
+        for gx in range(gw):
+            blk = up[gy * B:(gy + 1) * B, gx * B:(gx + 1) * B]
+            v = blk[blk >= 0]
+            if v.size:
+                lo[gy, gx] = max(0, int(v.min()) - GUIDE_MARGIN)
+                hi[gy, gx] = int(v.max()) + GUIDE_MARGIN
+    return (np.ascontiguousarray(np.repeat(np.repeat(lo, B, 0), B, 1)[:H, :W], np.int32),
+            np.ascontiguousarray(np.repeat(np.repeat(hi, B, 0), B, 1)[:H, :W], np.int32))
+
+
+def match_ncc_guided(L, R, D, coarse, r=5):
+    """Guided NCC (see guide_ranges) -> (disp int16, score32, score64)."""
+    L, R = _u8(L), _u8(R)
+    H, W = L.shape
+    lo, hi = guide_ranges(coarse, W, H)
+    disp = np.empty((H, W), np.int16)
+    s32 = np.empty((H, W), np.float32)
+    s64 = np.empty((H, W), np.float64)
+    lib().or_match_ncc_guided(_p(L), _p(R), W, H, W, D, r, _p(lo), _p(hi), _p(disp), _p(s32), _p(s64))
     return disp, s32, s64
 
 

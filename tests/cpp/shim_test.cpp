@@ -75,7 +75,6 @@ static int RunCpu() {
         BlockMatcherNCC::SParameter p;
         p.Set(dc, 0, 0.f, 0.f, 1, true, BlockMatcherNCC::EConfig::Patch_11x11);
         BlockMatcherNCC::CDriver d;
-        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "NCC guided mode must be rejected");
         p.iUseDispInput = 0;
         p.xDispConfig.Set(5, 128);
         CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "NCC iMin != 0 must be rejected");
@@ -206,6 +205,23 @@ static int RunGpu(const char* weights) {
                     low += s[size_t(y) * W + x] < 0.9999f;
                 }
         CHECK(bad == 0 && low == 0, "NCC: %d interior pixels off, %d scores below 1", bad, low);
+
+        // guided: a coarse map at half resolution holding K / 2 everywhere
+        // (scaled 2 * (K / 2) = K - 1; the block ranges contain K)
+        std::vector<uint8_t> coarse(size_t(W / 2) * ((H + 1) / 2), uint8_t(K / 2));
+        CDeviceSurface init(SImageFormat(W / 2, (H + 1) / 2));
+        init.CopyFrom(coarse.data());
+        p.iUseDispInput = 1;
+        BlockMatcherNCC::CDriver g;
+        g.Configure(dev, fin, p);
+        CHECK(ThrownCode([&] { g.Process(disp, surfL, surfR, _CDeviceSurface(), score); }) == CT_EINVAL,
+              "guided NCC without a coarse map");
+        ProcessKernel(g, disp, surfL, surfR, init, score);
+        auto gv = disp.CopyInto<uint16_t>();
+        int gbad = 0;
+        for (int y = 0; y < H; ++y)
+            for (int x = 0; x < W; ++x) gbad += interior(x, y, 5) && gv[size_t(y) * W + x] != v[size_t(y) * W + x];
+        CHECK(gbad == 0, "guided NCC: %d interior pixels differ from the full search", gbad);
     }
     {  // AW1 shifted windows, sub-pixel
         _SDisparityConfig dc;

@@ -130,10 +130,58 @@ def test_ncc_config2_full_size(ct, oracle, cuda):
     assert err <= TOL
 
 
-def test_ncc_rejects_guided_mode(ct, cuda):
+def _coarse_map(ct, oracle, L, R, D, s, holes, seed):
+    """Coarse disparities at 1/s: NCC (oracle) on s x s box-averaged images,
+    with a fraction `holes` of them removed (-1)."""
+    H, W = L.shape
+    Hc, Wc = -(-H // s), W // s
+
+    def down(img):
+        pad = np.zeros((Hc * s, Wc * s), np.float64)
+        pad[:H] = img[:, :Wc * s]
+        pad[H:] = img[-1, :Wc * s]
+        return np.round(pad.reshape(Hc, s, Wc, s).mean(axis=(1, 3))).astype(np.uint8)
+
+    c, _, _ = oracle.match_ncc(down(L), down(R), max(2, D // s), 2)
+    rng = np.random.default_rng(seed)
+    c = np.where(rng.random(c.shape) < holes, -1, c).astype(np.int16)
+    return c
+
+
+@pytest.mark.parametrize("W,H,D,r,s,holes,ctype", [
+    (200, 90, 64, 5, 2, 0.0, torch.uint8),
+    (332, 111, 128, 5, 4, 0.3, torch.int16),    # two disparity blocks per tile
+    (160, 64, 48, 2, 8, 0.5, torch.uint8),      # empty guide blocks
+    (128, 48, 64, 4, 1, 0.8, torch.int16),      # scale 1: per-pixel coarse hints
+])
+def test_ncc_guided_matches_oracle(ct, oracle, cuda, W, H, D, r, s, holes, ctype):
+    L, R, _, _ = ct.synth_pair(2, 40 + W + s, W, H, D - 1)
+    coarse = _coarse_map(ct, oracle, L, R, D, s, holes, seed=W)
+    d, s32, _ = oracle.match_ncc_guided(L, R, D, coarse, r)
+    enc = oracle.to_u8(coarse) if ctype == torch.uint8 else oracle.to_u16(coarse)
+    init = to_dev(np.ascontiguousarray(enc), cuda)
+    m = ct.BlockMatcherNCC()
+    m.configure(0, W, H, D, radius=r)
+    out = ct.alloc_image(H, W, torch.uint8, cuda)
+    score = ct.alloc_image(H, W, torch.float32, cuda)
+    m.process(out, to_dev(L, cuda), to_dev(R, cuda), score=score, disp_init=init)
+    torch.cuda.synchronize()
+    assert m.device_status() == 0
+    np.testing.assert_array_equal(out.cpu().numpy(), oracle.to_u8(d))
+    v = d >= 0
+    np.testing.assert_array_equal(score.cpu().numpy()[v], s32[v])
+    # the guide restricts the search: most pixels keep the unguided answer
+    du, _, _ = oracle.match_ncc(L, R, D, r)
+    if holes == 0.0:
+        assert (d == du).mean() > 0.8
+
+
+def test_ncc_guided_rejects_a_scale_that_does_not_divide(ct, cuda):
     m = ct.BlockMatcherNCC()
     m.configure(0, 64, 32, 16)
     a = ct.alloc_image(32, 64, torch.uint8, cuda)
-    with pytest.raises(ct.CtError) as e:
-        m.process(a, a, a, disp_init=a)
-    assert e.value.code == ct.CT_EINVAL
+    for w, h in ((48, 32), (32, 15)):
+        init = ct.alloc_image(h, w, torch.uint8, cuda)
+        with pytest.raises(ct.CtError) as e:
+            m.process(a, a, a, disp_init=init)
+        assert e.value.code == ct.CT_EFORMAT

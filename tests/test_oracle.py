@@ -133,3 +133,51 @@ def test_validity_rules(oracle):
     d, _ = oracle.match_census(L, R, 16, left_to_right=False)
     v = d >= 0
     assert (d[v] <= (W - 1 - 2) - xs[v]).all()
+
+
+def test_guide_ranges_known_answer(oracle):
+    """Scale 2, two coarse hints: block (0, 0) covers coarse columns 0..7,
+    block (0, 1) columns 8..15; the second block row has no hint."""
+    coarse = np.full((16, 16), -1, np.int16)
+    coarse[0, 0] = 3    # -> 6 at full resolution
+    coarse[2, 5] = 1    # -> 2, same block: range [max(0, 2 - 4), 6 + 4]
+    coarse[7, 9] = 10   # -> 20: range [16, 24]
+    lo, hi = oracle.guide_ranges(coarse, 32, 32)
+    assert (lo[:16, :16] == 0).all() and (hi[:16, :16] == 10).all()
+    assert (lo[:16, 16:] == 16).all() and (hi[:16, 16:] == 24).all()
+    assert (lo[16:] > hi[16:]).all()
+
+
+def test_guided_ncc_is_the_argmax_over_the_guide_range(oracle):
+    """The guided oracle against a direct restatement: per pixel, FP32 NCC
+    from direct window sums for each d in its range, strict '>' argmax."""
+    H, W, D, r = 24, 40, 12, 2
+    rng = np.random.default_rng(3)
+    L = rng.integers(0, 256, (H, W), dtype=np.uint8)
+    R = np.roll(L, -4, axis=1)
+    R[:, -4:] = rng.integers(0, 256, (H, 4), dtype=np.uint8)
+    R = np.clip(R.astype(np.int32) + rng.integers(-6, 7, (H, W)), 0, 255).astype(np.uint8)
+    coarse = np.where(rng.random((H // 2, W // 2)) < 0.3, -1, rng.integers(0, 6, (H // 2, W // 2))).astype(np.int16)
+    coarse[6:, 10:] = -1  # a block without hints
+    lo, hi = oracle.guide_ranges(coarse, W, H)
+    got, s32, _ = oracle.match_ncc_guided(L, R, D, coarse, r)
+    n = (2 * r + 1) ** 2
+    want = np.full((H, W), -1, np.int16)
+    for y in range(r, H - r):
+        for x in range(r, W - r):
+            a = L[y - r:y + r + 1, x - r:x + r + 1].astype(np.int64)
+            best, bd = np.float32(-2), -1
+            for d in range(D):
+                if x - d - r < 0 or d < lo[y, x] or d > hi[y, x]:
+                    continue
+                b = R[y - r:y + r + 1, x - d - r:x - d + r + 1].astype(np.int64)
+                sx, sy = a.sum(), b.sum()
+                vx, vy = n * (a * a).sum() - sx * sx, n * (b * b).sum() - sy * sy
+                num = n * (a * b).sum() - sx * sy
+                sc = np.float32(0) if vx * vy < n ** 4 else \
+                    np.float32(num) / np.sqrt(np.float32(vx) * np.float32(vy))
+                if sc > best:
+                    best, bd = sc, d
+            want[y, x] = bd
+    np.testing.assert_array_equal(got, want)
+    assert (lo[16:, 32:] > hi[16:, 32:]).all() and (got[16:, 32:] == -1).all()  # the block without hints
