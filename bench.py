@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="census1080",
-                    choices=["census1080", "sad640", "ncc1080", "aw1440", "batch64", "confnet1080"],
+                    choices=["census1080", "sad640", "ncc1080", "ncc1080g", "aw1440", "batch64", "confnet1080"],
                     help="census1080 (default, the headline) or another configuration, one JSON line each")
     ap.add_argument("--eval-pairs", type=int, default=None,
                     help="held-out 1080p pairs for the confidence-net AUC (default 4 in the census line, 24 in confnet1080)")
@@ -567,6 +567,7 @@ def run_workload(args):
     stream = torch.cuda.current_stream(dev)
     flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     wl = args.workload
+    unit = UNIT
 
     def up(a):
         t = ct.alloc_image(a.shape[0], a.shape[1], torch.from_numpy(a).dtype, dev)
@@ -605,7 +606,7 @@ def run_workload(args):
         launches = 2
     else:
         W, H, D, kind = {"sad640": (640, 480, 64, 1), "ncc1080": (1920, 1080, 128, 2),
-                         "aw1440": (2560, 1440, 256, 3)}[wl]
+                         "ncc1080g": (1920, 1080, 128, 2), "aw1440": (2560, 1440, 256, 3)}[wl]
         L, R, G, O = ct.synth_pair(kind, SEED + rank, W, H, D - 1)
         dL, dR = up(L), up(R)
         if wl == "sad640":
@@ -625,6 +626,42 @@ def run_workload(args):
             check_fn = lambda: np.array_equal(out.cpu().numpy(), oracle.to_u8(oracle.match_ncc(L, R, D, 5)[0]))
             cpu_fn = lambda: oracle.match_ncc(L, R, D, 5)
             metric, launches = "Mpix*disp/s NCC 11x11 FP32, 1920x1080 D=128", 4
+        elif wl == "ncc1080g":
+            # coarse-to-fine: census + L-R check on the 4x box-averaged pair
+            # (480x270, D=32; the pyramid level is prepared on the host, as a
+            # camera pipeline would deliver it), then the guided 11x11 NCC at
+            # full resolution searching [min - 4, max + 4] of the scaled
+            # coarse disparities per 16x16 block
+            def down4(img):
+                return np.round(img.reshape(H // 4, 4, W // 4, 4).mean(axis=(1, 3))).astype(np.uint8)
+            Lc, Rc = down4(L), down4(R)
+            dLc, dRc = up(Lc), up(Rc)
+            mc = ct.BlockMatcherCensus()
+            mc.configure(local, W // 4, H // 4, D // 4)
+            coarse = ct.alloc_image(H // 4, W // 4, torch.uint8, dev)
+            m = ct.BlockMatcherNCC()
+            m.configure(local, W, H, D, radius=5)
+            out = ct.alloc_image(H, W, torch.uint8, dev)
+            score = ct.alloc_image(H, W, torch.float32, dev)
+
+            def step():
+                mc.process_lr(dLc, dRc, disp_checked=coarse, tol=1, stream=stream)
+                m.process(out, dL, dR, score=score, disp_init=coarse, stream=stream)
+
+            def coarse_cpu():
+                c, _ = oracle.crosscheck(oracle.match_census(Lc, Rc, D // 4, 2, True)[0],
+                                         oracle.match_census(Lc, Rc, D // 4, 2, False)[0], 1, True)
+                return np.where(c >= 0, c, -1).astype(np.int16)
+
+            def check_fn():
+                c = coarse_cpu()
+                if not np.array_equal(coarse.cpu().numpy(), oracle.to_u8(c)):
+                    return False
+                return np.array_equal(out.cpu().numpy(), oracle.to_u8(oracle.match_ncc_guided(L, R, D, c, 5)[0]))
+
+            def cpu_fn():
+                oracle.match_ncc_guided(L, R, D, coarse_cpu(), 5)
+            metric, launches = "frames/s coarse-to-fine NCC (census L-R at 1/4, guided 11x11), 1920x1080 D=128", 10
         else:
             m = ct.BlockMatcherAW()
             m.configure(local, W, H, D)
@@ -635,6 +672,10 @@ def run_workload(args):
             metric, launches = "Mpix*disp/s adaptive window (5 x 7x7) + sub-pixel, 2560x1440 D=256", 2
         units = W * H * D
         cfg = {"workload": f"{wl}", "width": W, "height": H, "D": D}
+        if wl == "ncc1080g":
+            units, unit = 1e6, "frames/s"  # value = frames per second
+            cfg.update(coarse="480x270 D=32 census 9x7 + 5x5 + L-R check (tol 1) of the 4x box-averaged pair",
+                       guide_block=16, guide_margin=4)
 
         def cpu_sample():
             t0 = time.perf_counter()
@@ -657,16 +698,16 @@ def run_workload(args):
     ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev) / args.steps, world, dev)
     value = world * units / (ms * 1e-3) / 1e6
     out_line = {
-        "metric": metric, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": metric, "value": round(value, 1), "unit": unit, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u8 pixels / integer costs" + (" / fp32 score" if wl == "ncc1080" else ""),
+        "vs_baseline": None, "dtype": "u8 pixels / integer costs" + (" / fp32 score" if wl in ("ncc1080", "ncc1080g") else ""),
         "data": "synthetic (seeded generator)", "config": dict(cfg, l2="flushed before every timed step"),
         "gpu_launches": launches * args.steps, "clocks": clocks,
     }
     if rank == 0:
         out_line["parity_rank0"] = bool(check_fn())
         v, sample = cpu_sample()
-        out_line["cpu_baseline"] = {"value": round(v, 1), "unit": UNIT, "cores": oracle.num_threads(),
+        out_line["cpu_baseline"] = {"value": round(v, 1), "unit": unit, "cores": oracle.num_threads(),
                                     "kind": "port", "sample": sample}
         print(json.dumps(out_line), flush=True)
     close_ranks(world)

@@ -141,11 +141,6 @@ __global__ void __launch_bounds__(kNT, 1)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int xs = blockIdx.x * TWO - R;
     const int y0 = blockIdx.y * a.th;
-    const int dz0 = blockIdx.z * kDPC;
-    const int dw = dz0 + warp * kDPW;
-    const bool warp_active = dw < a.D;
-    const int ab = xs & ~15;
-    const int am = (xs - dz0 - (kDPC - 1)) & ~15;
 
     if (tid == 0) {
         dev::prefetch_tmap(&tmB);
@@ -154,15 +149,13 @@ __global__ void __launch_bounds__(kNT, 1)
         dev::fence_barrier_init();
     }
     for (int i = tid; i < a.th * TWO; i += kNT) sKey[i] = 0ull;
-    __syncthreads();
-    if (tid == 0) {
-        dev::mbar_arrive_expect_tx(bar, uint32_t(kBW * NR + kMWs * NR));
-        dev::tma_load_2d(sB, &tmB, ab, y0 - R, bar);
-        dev::tma_load_2d(sM, &tmM, am, y0 - R, bar);
-    }
-    // guided: skip the matching when no block of this tile searches this
-    // CTA's disparities (the outputs are still written below)
-    bool searches = true;
+    // Disparity block z covers dz0 = base + z kDPC .. + kDPC - 1. Unguided,
+    // base = 0. Guided, base starts at the low end (rounded down to kDPW) of
+    // the union of the search ranges of the 16 x 16 blocks this tile's
+    // outputs fall in, so a tile whose union is narrow needs one block; the
+    // others, and the warps of a block above the union, do no matching (the
+    // outputs are still written below).
+    int base = 0, ulo = 0, uhi = a.D - 1;
     if (a.guide) {
         int* uni = reinterpret_cast<int*>(bar + 1);  // 8 spare bytes after the mbarrier
         if (tid == 0) { uni[0] = 1 << 20; uni[1] = -1; }
@@ -178,7 +171,21 @@ __global__ void __launch_bounds__(kNT, 1)
             }
         }
         __syncthreads();
-        searches = uni[0] <= uni[1] && uni[1] >= dz0 && uni[0] < dz0 + kDPC;
+        ulo = uni[0];
+        uhi = min(uni[1], a.D - 1);
+        if (ulo <= uhi) base = ulo & ~(kDPW - 1);
+    }
+    const int dz0 = base + int(blockIdx.z) * kDPC;
+    const int dw = dz0 + warp * kDPW;
+    const bool warp_active = dw < a.D;
+    const bool searches = ulo <= uhi && dw <= uhi && dw + kDPW - 1 >= ulo;
+    const int ab = xs & ~15;
+    const int am = (xs - dz0 - (kDPC - 1)) & ~15;
+    __syncthreads();
+    if (tid == 0) {
+        dev::mbar_arrive_expect_tx(bar, uint32_t(kBW * NR + kMWs * NR));
+        dev::tma_load_2d(sB, &tmB, ab, y0 - R, bar);
+        dev::tma_load_2d(sM, &tmM, am, y0 - R, bar);
     }
     const bool got = dev::mbar_wait_bounded(bar, 0);
     if (__syncthreads_or(!got)) {
