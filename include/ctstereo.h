@@ -295,6 +295,13 @@ int ct_bm_aw_configure(ct_handle* h, int32_t device, const ct_format* fmt, const
 /* disp: F32 (sub-pixel, -1 invalid) or U8/U16 (integer WTA). */
 int ct_bm_aw_process(ct_handle* h, const ct_image* disp, const ct_image* left,
                      const ct_image* right, ct_stream stream);
+/* Guided mode: CDriver::Process with xImageDispInit and iUseDispInput
+ * (MatcherUseDisparity, BlockMatcherAW1.cu:996-1180). disp_init is a coarse
+ * disparity map as for ct_bm_ncc_process; each 16 x 16 block takes its winner
+ * over [max(0, min - 4), max + 4] of its scaled coarse disparities only (no
+ * disparity when it has none); the sub-pixel step is unchanged. */
+int ct_bm_aw_process_guided(ct_handle* h, const ct_image* disp, const ct_image* left,
+                            const ct_image* right, const ct_image* disp_init, ct_stream stream);
 
 /* ---- cross-check: CrossCheckDisparityMaps::CDriver ------------------------
  * Replaces CrossCheckDisparityMaps.h:38-117 / .cu:63-190. For each pixel of

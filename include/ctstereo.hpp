@@ -41,9 +41,8 @@
  *     CError(CT_EINVAL) when a gate that would change the winner is switched
  *     on (fGradThresh > 0); thresholds that only label the unbuilt cost
  *     channels are accepted and ignored.
- *   - Guided matching (iUseDispInput + xImageDispInit) is built for
- *     BlockMatcherNCC (search ranges per 16 x 16 block, see
- *     ct_bm_ncc_process); BlockMatcherAW1 rejects it.
+ *   - Guided matching (iUseDispInput + xImageDispInit) searches per 16 x 16
+ *     block (see ct_bm_ncc_process / ct_bm_aw_process_guided).
  *   - BlockMatcherAW1 computes the "best of 5 shifted 7x7 windows" cost with
  *     sub-pixel refinement (EConfig::Shifted5_7x7); the reference's 2-of-4
  *     sub-window configurations throw.
@@ -311,9 +310,6 @@ inline void RequireInputFormat(const SImageFormat& f, const char* who) {
 inline void RequireDispConfig(const _SDisparityConfig& c, const char* who) {
     if (c.iMin != 0) throw CError(CT_EINVAL, std::string(who) + ": disparities start at 0 (iMin must be 0)");
 }
-inline void RequireNoGuide(const _CDeviceSurface& init, const char* who) {
-    if (init.IsValid()) throw CError(CT_EINVAL, std::string(who) + ": guided matching (xImageDispInit) is not built");
-}
 }  // namespace detail
 
 /* ---- CensusTransform (CensusTransform.h:44-70) ----------------------------- */
@@ -504,7 +500,7 @@ public:
         if (xPars.eSimType != ESimType::AbsoluteDifference)
             throw CError(CT_EINVAL, "BlockMatcherAW1: only ESimType::AbsoluteDifference is built");
         if (xPars.fGradThresh > 0.f) throw CError(CT_EINVAL, "BlockMatcherAW1: the gradient gate is not built");
-        if (xPars.iUseDispInput) throw CError(CT_EINVAL, "BlockMatcherAW1: guided matching is not built");
+        m_bUseDispInput = xPars.iUseDispInput != 0;
         EnsureHandle(ct_bm_aw_create);
         const ct_format f = xFormat.ToC();
         const ct_aw_params p{xPars.xDispConfig.iRange, xPars.bLeftToRight ? 1 : 0, 0, 0};
@@ -512,16 +508,26 @@ public:
     }
 
     /* xImageDisp: Single (sub-pixel, -1 invalid) or UInt8 / UInt16 (integer
-     * winner-take-all). xImageDispInit must be empty; xImageDebug is unused. */
+     * winner-take-all). With iUseDispInput set, xImageDispInit is the coarse
+     * map of the guided mode (ct_bm_aw_process_guided); without it, it is
+     * ignored. xImageDebug is unused. */
     void Process(_CDeviceSurface& xImageDisp, const _CDeviceSurface& xImageL, const _CDeviceSurface& xImageR,
                  const _CDeviceSurface& xImageDispInit, const _CDeviceSurface& /*xImageDebug*/) {
-        detail::RequireNoGuide(xImageDispInit, "BlockMatcherAW1");
-        Ensure(ct_bm_aw_process(m_pHandle, xImageDisp.C(), xImageL.C(), xImageR.C(), S()),
+        if (!m_bUseDispInput) {
+            Ensure(ct_bm_aw_process(m_pHandle, xImageDisp.C(), xImageL.C(), xImageR.C(), S()),
+                   "BlockMatcherAW1::Process");
+            return;
+        }
+        if (!xImageDispInit.IsValid()) throw CError(CT_EINVAL, "BlockMatcherAW1: iUseDispInput needs xImageDispInit");
+        Ensure(ct_bm_aw_process_guided(m_pHandle, xImageDisp.C(), xImageL.C(), xImageR.C(), xImageDispInit.C(), S()),
                "BlockMatcherAW1::Process");
     }
     void Process(_CDeviceSurface& xImageDisp, const _CDeviceSurface& xImageL, const _CDeviceSurface& xImageR) {
         Process(xImageDisp, xImageL, xImageR, _CDeviceSurface(), _CDeviceSurface());
     }
+
+private:
+    bool m_bUseDispInput = false;
 };
 
 }  // namespace BlockMatcherAW1

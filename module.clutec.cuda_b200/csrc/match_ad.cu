@@ -23,6 +23,7 @@
 // through a global key buffer.
 #include "ct_internal.h"
 #include "ct_device.cuh"
+#include "guide.cuh"
 
 namespace ct {
 namespace ad {
@@ -38,6 +39,8 @@ __host__ __device__ constexpr int two_of(int R, bool aw) { return kTWV - 2 * ext
 
 struct Args {
     int W, H, D, th;
+    const uint32_t* guide;  // AW guided mode: search range per 16 x 16 block (guide.cuh), or null
+    int guide_gw;
     uint32_t* keys;      // global keys when gridDim.z > 1 (or always for AW)
     void* out;
     size_t out_pitch;
@@ -109,9 +112,23 @@ __global__ void __launch_bounds__(kNT, 1)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int xs = blockIdx.x * TWO - EXT;
     const int y0 = blockIdx.y * a.th;
-    const int dz0 = blockIdx.z * kDPC;
+    for (int i = tid; i < a.th * TWO; i += kNT) sKey[i] = 0xFFFFFFFFu;
+    // Guided (AW, left-to-right): disparity block z covers base + z kDPC ..,
+    // base at the low end (rounded down to kDPW) of the union of the search
+    // ranges of the 16 x 16 blocks this tile's outputs fall in; warps outside
+    // the union skip the matching. Unguided, base = 0 and every warp below D
+    // matches.
+    int base = 0, ulo = 0, uhi = a.D - 1;
+    if (a.guide) {
+        const int2 u = guide::tile_union(a.guide, a.guide_gw, xs + EXT, min(xs + EXT + TWO, a.W) - 1, y0,
+                                         min(y0 + a.th, a.H) - 1, reinterpret_cast<int*>(bar + 1));
+        ulo = u.x;
+        uhi = min(u.y, a.D - 1);
+        if (ulo <= uhi) base = ulo & ~(kDPW - 1);
+    }
+    const int dz0 = base + int(blockIdx.z) * kDPC;
     const int dw = dz0 + warp * kDPW;
-    const bool warp_active = dw < a.D;
+    const bool warp_active = dw < a.D && ulo <= uhi && dw <= uhi && dw + kDPW - 1 >= ulo;
     const int ab = floor16(xs);
     const int am = DIR == 0 ? floor16(xs - dz0 - (kDPC - 1)) : floor16(xs + dz0);
     // AW windows reach EXT = 6 columns; SAD ones r columns.
@@ -125,7 +142,6 @@ __global__ void __launch_bounds__(kNT, 1)
         dev::mbar_init(bar, 1);
         dev::fence_barrier_init();
     }
-    for (int i = tid; i < a.th * TWO; i += kNT) sKey[i] = 0xFFFFFFFFu;
     __syncthreads();
     if (tid == 0) {
         dev::mbar_arrive_expect_tx(bar, uint32_t(kBW * NR + kMWs * NR));
@@ -241,13 +257,22 @@ __global__ void __launch_bounds__(kNT, 1)
                 const int x = xs + v;
                 int lim = DIR == 0 ? x - EXT : a.W - 1 - EXT - x;
                 lim = min(lim, a.D - 1);
+                int glo = 0;
+                if (a.guide) {  // this pixel's block range (pixels outside the image search nothing)
+                    const int y = y0 + oy;
+                    const uint32_t g = (y < a.H && x < a.W)
+                                           ? __ldg(&a.guide[(size_t)(y / guide::kBlock) * a.guide_gw + x / guide::kBlock])
+                                           : 0x0000FFFFu;
+                    glo = int(g & 0xFFFFu);
+                    lim = min(lim, int(g >> 16));
+                }
 #pragma unroll
                 for (int p = 0; p < 4; ++p) {
                     uint32_t klo = __byte_perm(A[p][c], dlo[p], 0x1054);        // cost_lo << 16 | d
                     uint32_t khi = (A[p][c] & 0xFFFF0000u) | (dlo[p] + 1);       // cost_hi << 16 | d+1
-                    if (!interior) {
-                        if (int(dlo[p]) > lim) klo |= 0xFFFF0000u;
-                        if (int(dlo[p]) + 1 > lim) khi |= 0xFFFF0000u;
+                    if (!interior || a.guide) {
+                        if (int(dlo[p]) > lim || int(dlo[p]) < glo) klo |= 0xFFFF0000u;
+                        if (int(dlo[p]) + 1 > lim || int(dlo[p]) + 1 < glo) khi |= 0xFFFF0000u;
                     }
                     best = min(best, min(klo, khi));
                 }
@@ -351,10 +376,12 @@ struct AdHandle : ct_handle {
     ~AdHandle() override {
         if (device >= 0) cudaSetDevice(device);
         cudaFree(keys);
+        cudaFree(guide);
     }
     ct_format fmt{};
     int D = 0, R = 4, dir = 0;
     uint32_t* keys = nullptr;
+    uint32_t* guide = nullptr;  // AW guided mode: one search range per 16 x 16 block
     int th = 32;
 };
 
@@ -370,7 +397,8 @@ int set_attr() {
 }
 
 template <int R, bool AW, int DIR>
-int launch_ad(AdHandle* h, const ct_image* disp, const ct_image* L, const ct_image* Rimg, cudaStream_t s) {
+int launch_ad(AdHandle* h, const ct_image* disp, const ct_image* L, const ct_image* Rimg, cudaStream_t s,
+              const ct_image* init = nullptr) {
     using namespace ad;
     if (int rc = set_attr<R, AW, DIR>()) return rc;
     const int W = h->fmt.width, H = h->fmt.height;
@@ -380,6 +408,14 @@ int launch_ad(AdHandle* h, const ct_image* disp, const ct_image* L, const ct_ima
     a.keys = h->keys;
     a.out = disp->ptr; a.out_pitch = disp->pitch_bytes; a.out_type = disp->type;
     a.status = h->d_status;
+    if (init) {
+        const int gw = (W + guide::kBlock - 1) / guide::kBlock, gh = (H + guide::kBlock - 1) / guide::kBlock;
+        guide::range_kernel<<<dim3((gw + 127) / 128, gh), 128, 0, s>>>(init->ptr, init->pitch_bytes, init->type,
+                                                                       W / init->width, W, H, h->guide, gw, gh);
+        CT_LAUNCH_CHECK();
+        a.guide = h->guide;
+        a.guide_gw = gw;
+    }
     const int NR = a.th + 2 * EXT;
     const ct_image* B = DIR == 0 ? L : Rimg;
     const ct_image* M = DIR == 0 ? Rimg : L;
@@ -409,12 +445,17 @@ int configure_ad(AdHandle* h, int32_t device, const ct_format* fmt, int D, int R
     if (D < 1 || D > 256) return fail(CT_EINVAL, "disp_count must be 1..256");
     if (int rc = use_device(device)) return rc;
     cudaFree(h->keys);
+    cudaFree(h->guide);
     h->keys = nullptr;
+    h->guide = nullptr;
     h->device = device;
     if (int rc = h->init_status()) return rc;
     if (cudaMalloc(&h->keys, (size_t)fmt->width * fmt->height * 4) != cudaSuccess)
         return fail(CT_ENOMEM, "key scratch");
     CT_CUDA_TRY(cudaMemset(h->keys, 0xFF, (size_t)fmt->width * fmt->height * 4));
+    const size_t G = size_t((fmt->width + guide::kBlock - 1) / guide::kBlock) *
+                     ((fmt->height + guide::kBlock - 1) / guide::kBlock);
+    if (cudaMalloc(&h->guide, G * 4) != cudaSuccess) return fail(CT_ENOMEM, "guide ranges");
     h->fmt = *fmt;
     h->D = D;
     h->R = R;
@@ -511,6 +552,27 @@ int ct_bm_aw_process(ct_handle* hh, const ct_image* disp, const ct_image* left, 
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     h->last_stream = s;
     return launch_ad<3, true, 0>(h, disp, left, right, s);
+}
+
+int ct_bm_aw_process_guided(ct_handle* hh, const ct_image* disp, const ct_image* left, const ct_image* right,
+                            const ct_image* disp_init, ct_stream stream) {
+    clear_error();
+    auto* h = (hh && hh->kind == Kind::BmAw) ? static_cast<AdHandle*>(hh) : nullptr;
+    if (!h) return fail(CT_ESTATE, "not an AW matcher handle");
+    if (int rc = check_io(h, disp, left, right, (1u << CT_PIX_U8) | (1u << CT_PIX_U16) | (1u << CT_PIX_F32)))
+        return rc;
+    if (int rc = check_image(disp_init, "disp_init", (1u << CT_PIX_U8) | (1u << CT_PIX_U16))) return rc;
+    const int sc = left->width / disp_init->width;
+    if (sc < 1 || sc * disp_init->width != left->width)
+        return fail(CT_EFORMAT, "disp_init width must divide the image width (%d / %d)", left->width,
+                    disp_init->width);
+    if (disp_init->height < (left->height + sc - 1) / sc)
+        return fail(CT_EFORMAT, "disp_init needs at least ceil(height / %d) = %d rows", sc,
+                    (left->height + sc - 1) / sc);
+    if (int rc = use_device(h->device)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    h->last_stream = s;
+    return launch_ad<3, true, 0>(h, disp, left, right, s, disp_init);
 }
 
 }  // extern "C"

@@ -14,6 +14,7 @@
 // highest score wins, then the lowest d.
 #include "ct_internal.h"
 #include "ct_device.cuh"
+#include "guide.cuh"
 
 namespace ct {
 namespace ncc {
@@ -64,41 +65,7 @@ __device__ __forceinline__ float unordered(uint32_t o) {
     return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
 }
 
-// Guided mode (MatcherUseDisparity, BlockMatcherNCC.cu:980-1168): pixels
-// are grouped in 16 x 16 blocks; a block searches only
-// [max(0, min - 4), max + 4] of its pixels' coarse disparities scaled by s
-// (pixel (x, y) reads the coarse map at (x / s, y / s)), and nothing when
-// none of them has a coarse disparity. One thread per block; the range is
-// packed lo | hi << 16 (lo > hi: no search).
-constexpr int kGuideBlock = 16, kGuideMargin = 4;
-
-__global__ void guide_range_kernel(const void* coarse, size_t pitch, int type, int s, int W, int H, uint32_t* ranges,
-                                   int gw, int gh) {
-    const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y;
-    if (gx >= gw || gy >= gh) return;
-    const int x0 = gx * kGuideBlock, x1 = min(x0 + kGuideBlock, W) - 1;
-    const int y0 = gy * kGuideBlock, y1 = min(y0 + kGuideBlock, H) - 1;
-    int lo = 1 << 20, hi = -1;
-    for (int cy = y0 / s; cy <= y1 / s; ++cy) {
-        const char* row = static_cast<const char*>(coarse) + (size_t)cy * pitch;
-        for (int cx = x0 / s; cx <= x1 / s; ++cx) {
-            int d;
-            if (type == CT_PIX_U8) {
-                const int v = reinterpret_cast<const uint8_t*>(row)[cx];
-                d = v == 0xFF ? -1 : v;
-            } else {
-                const int v = reinterpret_cast<const uint16_t*>(row)[cx];
-                d = (v >= CT_DISP_FIRST && v <= CT_DISP_LAST) ? v - 1 : -1;
-            }
-            if (d >= 0) {
-                lo = min(lo, d * s);
-                hi = max(hi, d * s);
-            }
-        }
-    }
-    ranges[(size_t)gy * gw + gx] =
-        hi < 0 ? 0x0000FFFFu : (uint32_t(max(0, lo - kGuideMargin)) | (uint32_t(min(hi + kGuideMargin, 0xFFFF)) << 16));
-}
+constexpr int kGuideBlock = guide::kBlock;
 
 struct Args {
     int W, H, D, th;
@@ -157,22 +124,10 @@ __global__ void __launch_bounds__(kNT, 1)
     // outputs are still written below).
     int base = 0, ulo = 0, uhi = a.D - 1;
     if (a.guide) {
-        int* uni = reinterpret_cast<int*>(bar + 1);  // 8 spare bytes after the mbarrier
-        if (tid == 0) { uni[0] = 1 << 20; uni[1] = -1; }
-        __syncthreads();
-        const int gx0 = max(xs + R, 0) / kGuideBlock, gx1 = (min(xs + R + TWO, a.W) - 1) / kGuideBlock;
-        const int gy0 = y0 / kGuideBlock, gy1 = (min(y0 + a.th, a.H) - 1) / kGuideBlock;
-        const int ngx = gx1 - gx0 + 1;
-        for (int i = tid; i < ngx * (gy1 - gy0 + 1); i += kNT) {
-            const uint32_t g = a.guide[(size_t)(gy0 + i / ngx) * a.guide_gw + gx0 + i % ngx];
-            if ((g & 0xFFFFu) <= (g >> 16)) {
-                atomicMin(&uni[0], int(g & 0xFFFFu));
-                atomicMax(&uni[1], int(g >> 16));
-            }
-        }
-        __syncthreads();
-        ulo = uni[0];
-        uhi = min(uni[1], a.D - 1);
+        const int2 u = guide::tile_union(a.guide, a.guide_gw, xs + R, min(xs + R + TWO, a.W) - 1, y0,
+                                         min(y0 + a.th, a.H) - 1, reinterpret_cast<int*>(bar + 1));
+        ulo = u.x;
+        uhi = min(u.y, a.D - 1);
         if (ulo <= uhi) base = ulo & ~(kDPW - 1);
     }
     const int dz0 = base + int(blockIdx.z) * kDPC;
@@ -356,8 +311,8 @@ int launch_ncc(NccHandle* h, const ct_image* disp, const ct_image* score, const 
     a.status = h->d_status;
     if (init) {
         const int gw = (W + kGuideBlock - 1) / kGuideBlock, gh = (H + kGuideBlock - 1) / kGuideBlock;
-        guide_range_kernel<<<dim3((gw + 127) / 128, gh), 128, 0, s>>>(init->ptr, init->pitch_bytes, init->type,
-                                                                      W / init->width, W, H, h->guide, gw, gh);
+        guide::range_kernel<<<dim3((gw + 127) / 128, gh), 128, 0, s>>>(init->ptr, init->pitch_bytes, init->type,
+                                                                       W / init->width, W, H, h->guide, gw, gh);
         CT_LAUNCH_CHECK();
         a.guide = h->guide;
         a.guide_gw = gw;

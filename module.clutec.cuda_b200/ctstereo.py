@@ -160,6 +160,7 @@ def _declare(L: C.CDLL) -> None:
         "ct_bm_aw_create": [P(H)],
         "ct_bm_aw_configure": [H, C.c_int32, fmt, P(ct_aw_params)],
         "ct_bm_aw_process": [H, img, img, img, C.c_void_p],
+        "ct_bm_aw_process_guided": [H, img, img, img, img, C.c_void_p],
         "ct_crosscheck_create": [P(H)],
         "ct_crosscheck_configure": [H, C.c_int32, fmt, P(ct_crosscheck_params)],
         "ct_crosscheck_process": [H, img, img, img, C.c_void_p],
@@ -387,9 +388,14 @@ class BlockMatcherAW(_Driver):
         check(lib().ct_bm_aw_configure(self._h, device, C.byref(_fmt(width, height)),
                                        C.byref(ct_aw_params(disp_count, 1, 0, 0))))
 
-    def process(self, disp, left, right, stream=None):
-        check(lib().ct_bm_aw_process(self._h, _img_ref(disp), _img_ref(left), _img_ref(right),
-                                     _stream(stream)))
+    def process(self, disp, left, right, disp_init=None, stream=None):
+        """disp_init: coarse disparity map of the guided mode (or None)."""
+        if disp_init is None:
+            check(lib().ct_bm_aw_process(self._h, _img_ref(disp), _img_ref(left), _img_ref(right),
+                                         _stream(stream)))
+        else:
+            check(lib().ct_bm_aw_process_guided(self._h, _img_ref(disp), _img_ref(left), _img_ref(right),
+                                                _img_ref(disp_init), _stream(stream)))
 
 
 class CrossCheckDisparityMaps(_Driver):

@@ -220,8 +220,20 @@ void or_match_sad(const uint8_t* L, const uint8_t* R, int W, int H, int pitch,
 // float(d) + that), sub64 in FP64. Skipped (sub = d) when d = 0, d = D-1, d+1
 // is invalid or den <= 0. Invalid pixels: disp -1, sub -1.
 // ---------------------------------------------------------------------------
+// Guided variant (MatcherUseDisparity, BlockMatcherAW1.cu:996-1180): the
+// winner of pixel (x, y) is taken over d in [lo[y W + x], hi[y W + x]] only
+// (lo > hi: no disparity); the sub-pixel neighbours c-, c+ are the costs at
+// d - 1 and d + 1 whether or not they lie in the range.
+void or_match_aw_guided(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, int D, const int32_t* lo,
+                        const int32_t* hi, int16_t* disp, int32_t* best_cost, float* sub32, double* sub64);
+
 void or_match_aw(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, int D,
                  int16_t* disp, int32_t* best_cost, float* sub32, double* sub64) {
+    or_match_aw_guided(L, R, W, H, pitch, D, nullptr, nullptr, disp, best_cost, sub32, sub64);
+}
+
+void or_match_aw_guided(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, int D, const int32_t* lo,
+                        const int32_t* hi, int16_t* disp, int32_t* best_cost, float* sub32, double* sub64) {
     const int r = 3, sh = 3, ext = r + sh, K = 2 * r + 1;
     const int nb = (H + kBand - 1) / kBand;
 #pragma omp parallel
@@ -289,7 +301,9 @@ void or_match_aw(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, in
                             }
                             const size_t o = ro + x;
                             if (need[o]) { cp1[o] = a; need[o] = 0; }
-                            if (dv && a < best[o]) {
+                            const bool in_range =
+                                !lo || (d >= lo[(size_t)y * W + x] && d <= hi[(size_t)y * W + x]);
+                            if (dv && in_range && a < best[o]) {
                                 best[o] = a; bd[o] = int16_t(d);
                                 cm1[o] = prevA[o];
                                 need[o] = 1; cp1[o] = -1;

@@ -41,6 +41,7 @@ def lib() -> C.CDLL:
         _lib.or_match_census.argtypes = [vp, vp, i, i, i, i, i, i, vp, vp, vp, i]
         _lib.or_match_sad.argtypes = [vp, vp, i, i, i, i, i, i, vp, vp]
         _lib.or_match_aw.argtypes = [vp, vp, i, i, i, i, vp, vp, vp, vp]
+        _lib.or_match_aw_guided.argtypes = [vp, vp, i, i, i, i, vp, vp, vp, vp, vp, vp]
         _lib.or_match_ncc.argtypes = [vp, vp, i, i, i, i, i, vp, vp, vp]
         _lib.or_match_ncc_guided.argtypes = [vp, vp, i, i, i, i, i, vp, vp, vp, vp, vp]
         _lib.or_crosscheck.argtypes = [vp, vp, i, i, i, i, vp, vp]
@@ -124,6 +125,19 @@ def match_aw(L, R, D):
     s32 = np.empty((H, W), np.float32)
     s64 = np.empty((H, W), np.float64)
     lib().or_match_aw(_p(L), _p(R), W, H, W, D, _p(disp), _p(cost), _p(s32), _p(s64))
+    return disp, cost, s32, s64
+
+
+def match_aw_guided(L, R, D, coarse):
+    """Guided adaptive-window matcher (see guide_ranges) -> as match_aw."""
+    L, R = _u8(L), _u8(R)
+    H, W = L.shape
+    lo, hi = guide_ranges(coarse, W, H)
+    disp = np.empty((H, W), np.int16)
+    cost = np.empty((H, W), np.int32)
+    s32 = np.empty((H, W), np.float32)
+    s64 = np.empty((H, W), np.float64)
+    lib().or_match_aw_guided(_p(L), _p(R), W, H, W, D, _p(lo), _p(hi), _p(disp), _p(cost), _p(s32), _p(s64))
     return disp, cost, s32, s64
 
 

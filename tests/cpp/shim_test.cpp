@@ -238,6 +238,21 @@ static int RunGpu(const char* weights) {
         for (int y = 0; y < H; ++y)
             for (int x = 0; x < W; ++x) bad += interior(x, y, 6) && !(std::fabs(v[size_t(y) * W + x] - K) < 0.5f);
         CHECK(bad == 0, "AW1: %d interior pixels not within 0.5 of %d", bad, K);
+
+        // guided, with a coarse map at quarter resolution holding K / 4
+        // (scaled 4 * (K / 4) = 4; the block ranges [0, 8] contain K)
+        std::vector<uint8_t> coarse(size_t(W / 4) * (H / 4), uint8_t(K / 4));
+        CDeviceSurface init(SImageFormat(W / 4, H / 4));
+        init.CopyFrom(coarse.data());
+        p.iUseDispInput = 1;
+        BlockMatcherAW1::CDriver g;
+        g.Configure(dev, fin, p);
+        ProcessKernel(g, disp, surfL, surfR, init, _CDeviceSurface());
+        auto gv = disp.CopyInto<float>();
+        int gbad = 0;
+        for (int y = 0; y < H; ++y)
+            for (int x = 0; x < W; ++x) gbad += interior(x, y, 6) && gv[size_t(y) * W + x] != v[size_t(y) * W + x];
+        CHECK(gbad == 0, "guided AW1: %d interior pixels differ from the full search", gbad);
     }
     {  // census both ways + cross-check driver on the two maps
         _SDisparityConfig dc;

@@ -185,3 +185,27 @@ def test_ncc_guided_rejects_a_scale_that_does_not_divide(ct, cuda):
         with pytest.raises(ct.CtError) as e:
             m.process(a, a, a, disp_init=init)
         assert e.value.code == ct.CT_EFORMAT
+
+
+@pytest.mark.parametrize("W,H,D,s,holes,ctype", [
+    (200, 90, 64, 2, 0.0, torch.uint8),
+    (332, 111, 128, 4, 0.3, torch.int16),     # two disparity blocks per tile
+    (160, 64, 48, 8, 0.5, torch.uint8),       # empty guide blocks
+])
+def test_aw_guided_matches_oracle(ct, oracle, cuda, W, H, D, s, holes, ctype):
+    L, R, _, _ = ct.synth_pair(3, 70 + W + s, W, H, D - 1)
+    coarse = _coarse_map(ct, oracle, L, R, D, s, holes, seed=W + 1)
+    d, _, s32, _ = oracle.match_aw_guided(L, R, D, coarse)
+    enc = oracle.to_u8(coarse) if ctype == torch.uint8 else oracle.to_u16(coarse)
+    init = to_dev(np.ascontiguousarray(enc), cuda)
+    m = ct.BlockMatcherAW()
+    m.configure(0, W, H, D)
+    dL, dR = to_dev(L, cuda), to_dev(R, cuda)
+    out = ct.alloc_image(H, W, torch.uint8, cuda)
+    sub = ct.alloc_image(H, W, torch.float32, cuda)
+    m.process(out, dL, dR, disp_init=init)
+    m.process(sub, dL, dR, disp_init=init)
+    torch.cuda.synchronize()
+    assert m.device_status() == 0
+    np.testing.assert_array_equal(out.cpu().numpy(), oracle.to_u8(d))
+    np.testing.assert_array_equal(sub.cpu().numpy(), s32)
