@@ -60,6 +60,7 @@ typedef struct CUstream_st* ct_stream;
 #define CT_PIX_U16 2
 #define CT_PIX_U64 3
 #define CT_PIX_F32 4
+#define CT_PIX_RGBA8 5  /* 4 bytes per pixel: r, g, b, a (visualisation output) */
 
 /* EDisparityId codes used in CT_PIX_U16 maps (DisparityId.h:35-47). */
 #define CT_DISP_FIRST 0x0001
@@ -397,6 +398,41 @@ int ct_census_stream_wait(ct_handle* h, int64_t frame);
  * milliseconds from the mark to the end of the last download. */
 int ct_census_stream_timer_start(ct_handle* h);
 int ct_census_stream_timer_stop(ct_handle* h, float* ms);
+
+/* ---- disparity visualisation: ColorDisparityImage::CDriver -----------------
+ * Replaces ColorDisparityImage.h:37-120 / ColorDisparityImage.cu:45-300,
+ * writing a headless device image instead of a GL surface. disp: U16
+ * (EDisparityId codes) or U8 (d, read as code d + 1; 255 as CannotEvaluate).
+ * t = (code - disp_min) / (disp_max - disp_min) in FP32, q(t, M) =
+ * rint(clamp(t, 0, 1) * M). Styles (EStyle):
+ *   CT_COLOR_ANALYSIS  out RGBA8: disparities gray q(t, 255); each other code
+ *                      its colour from `colors` (unknown codes: red)
+ *   CT_COLOR_GRAY      out U16: disparities q(t, 65535), others 0
+ *   CT_COLOR_COLOR     out RGBA8: the blue-green-red ramp of NormFloatToColor
+ *                      (Conversion.h:56-74), others black
+ *   CT_COLOR_DISP_ABS  out U16: disparities their code, others 0
+ *   CT_COLOR_DISP_REL  out U16: (0x7FFF + inf_offset) - (code - 1), others 0
+ * Colours are RGBA8 words with r in the low byte, in the order unknown,
+ * cannot evaluate, saturated, not specific, not found, not unique,
+ * inconsistent. disp_min / disp_max are codes (d + 1). */
+#define CT_COLOR_ANALYSIS 0
+#define CT_COLOR_GRAY 1
+#define CT_COLOR_COLOR 2
+#define CT_COLOR_DISP_ABS 3
+#define CT_COLOR_DISP_REL 4
+typedef struct ct_color_params {
+    int32_t style;        /* CT_COLOR_* */
+    int32_t disp_min;     /* uDispMin (code) */
+    int32_t disp_max;     /* uDispMax (code) */
+    int32_t inf_offset;   /* uDispInfOffset (DISP_REL) */
+    uint32_t colors[7];   /* pixUnknown .. pixInconsistent */
+} ct_color_params;
+
+/* SParameter's defaults (ColorDisparityImage.h:76-84): range First .. Last,
+ * the reference's ID colours. */
+int ct_color_params_default(int32_t style, ct_color_params* p);
+/* CDriver::Process(color image, disparity image, style); asynchronous. */
+int ct_color_disparity(const ct_image* out, const ct_image* disp, const ct_color_params* p, ct_stream stream);
 
 /* ---- synthetic stereo pairs -----------------------------------------------
  * Seeded generator of rectified stereo pairs with ground truth (host memory).

@@ -17,6 +17,8 @@
  *   Clu::Cuda::CKernelDriverBase (KernelDriverBase.h:46-177), ProcessKernel
  *     (KernelDriverBase.h:180-199)              -> CKernelDriverBase, ProcessKernel
  *   Clu::Cuda::EDisparityId (DisparityId.h:35-47) -> EDisparityId
+ *   ColorDisparityImage::{EStyle, SParameter, CDriver} (ColorDisparityImage.h:37-120),
+ *     into a headless RGBA8 / U16 device image
  *   CensusTransform::CDriver (CensusTransform.h:44-70)
  *   BlockMatcherSAD1::{EConfig, SParameter, CDriver} (BlockMatcherSAD1.h:42-127)
  *   BlockMatcherNCC::{EConfig, SParameter, CDriver} (BlockMatcherNCC.h:41-144)
@@ -100,6 +102,7 @@ enum class EDataType : int32_t {
     UInt16 = CT_PIX_U16,
     UInt64 = CT_PIX_U64,
     Single = CT_PIX_F32,
+    RGBA8 = CT_PIX_RGBA8,  // 4 bytes: r, g, b, a
 };
 
 inline size_t BytesPerPixel(EDataType t) {
@@ -108,6 +111,7 @@ inline size_t BytesPerPixel(EDataType t) {
         case EDataType::UInt16: return 2;
         case EDataType::UInt64: return 8;
         case EDataType::Single: return 4;
+        case EDataType::RGBA8: return 4;
     }
     return 0;
 }
@@ -586,6 +590,75 @@ private:
 };
 
 }  // namespace CrossCheckDisparityMaps
+
+/* ---- ColorDisparityImage (ColorDisparityImage.h:37-120) -------------------- */
+namespace ColorDisparityImage {
+
+enum class EStyle : int32_t {
+    Analysis = CT_COLOR_ANALYSIS,
+    Gray = CT_COLOR_GRAY,
+    Color = CT_COLOR_COLOR,
+    DispAbs = CT_COLOR_DISP_ABS,
+    DispRel = CT_COLOR_DISP_REL,
+};
+
+/* Colours are RGBA8 words, r in the low byte (pixUnknown ..
+ * pixInconsistent); the defaults are the reference's. */
+struct SParameter {
+    uint16_t uDispMin = CT_DISP_FIRST, uDispMax = CT_DISP_LAST, uDispInfOffset = 0;
+    uint32_t pixUnknown, pixCannotEvaluate, pixSaturated, pixNotSpecific, pixNotFound, pixNotUnique, pixInconsistent;
+
+    SParameter() {
+        ct_color_params d;
+        Ensure(ct_color_params_default(CT_COLOR_ANALYSIS, &d), "ColorDisparityImage::SParameter");
+        pixUnknown = d.colors[0];
+        pixCannotEvaluate = d.colors[1];
+        pixSaturated = d.colors[2];
+        pixNotSpecific = d.colors[3];
+        pixNotFound = d.colors[4];
+        pixNotUnique = d.colors[5];
+        pixInconsistent = d.colors[6];
+    }
+    void Set(uint16_t _uDispMin, uint16_t _uDispMax, uint16_t _uDispInfOffset) {
+        uDispMin = _uDispMin;
+        uDispMax = _uDispMax;
+        uDispInfOffset = _uDispInfOffset;
+    }
+};
+
+class CDriver : public CKernelDriverBase {
+public:
+    CDriver() : CKernelDriverBase("Color Disparity Image") {}
+
+    void Configure(const CDevice& xDevice, const SImageFormat& /*xFormat*/, const SParameter& xPars) {
+        m_xPars = xPars;
+        EnsureCuda(cudaSetDevice(xDevice.iDevice), "ColorDisparityImage::Configure");
+    }
+
+    /* xColorImage: EDataType::RGBA8 for Analysis / Color, UInt16 for the
+     * other styles; xDisparityImage: UInt16 codes or UInt8 disparities. */
+    void Process(_CDeviceSurface& xColorImage, const _CDeviceSurface& xDisparityImage, EStyle eStyle) {
+        ct_color_params p{};
+        p.style = static_cast<int32_t>(eStyle);
+        p.disp_min = m_xPars.uDispMin;
+        p.disp_max = m_xPars.uDispMax;
+        p.inf_offset = m_xPars.uDispInfOffset;
+        const uint32_t c[7] = {m_xPars.pixUnknown, m_xPars.pixCannotEvaluate, m_xPars.pixSaturated,
+                               m_xPars.pixNotSpecific, m_xPars.pixNotFound, m_xPars.pixNotUnique,
+                               m_xPars.pixInconsistent};
+        for (int i = 0; i < 7; ++i) p.colors[i] = c[i];
+        ct_image out = *xColorImage.C();
+        if (eStyle == EStyle::Analysis || eStyle == EStyle::Color) out.type = CT_PIX_RGBA8;
+        Ensure(ct_color_disparity(&out, xDisparityImage.C(), &p, S()), "ColorDisparityImage::Process");
+    }
+
+    void EnsureDeviceStatus() {}  // no device-side waits
+
+private:
+    SParameter m_xPars;
+};
+
+}  // namespace ColorDisparityImage
 
 /* ---- no reference counterpart ----------------------------------------------- */
 

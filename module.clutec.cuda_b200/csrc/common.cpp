@@ -46,6 +46,7 @@ size_t pix_size(int32_t type) {
         case CT_PIX_U16: return 2;
         case CT_PIX_U64: return 8;
         case CT_PIX_F32: return 4;
+        case CT_PIX_RGBA8: return 4;
         default: return 0;
     }
 }

@@ -24,7 +24,8 @@ LIB_PATH = _PKG / "libctstereo.so"
 # status codes (ctstereo.h)
 CT_OK, CT_EINVAL, CT_ETYPE, CT_EFORMAT, CT_ECUDA, CT_ETIMEOUT, CT_ESTATE, CT_ENOMEM, CT_EINTERNAL = range(9)
 # pixel types
-CT_PIX_U8, CT_PIX_U16, CT_PIX_U64, CT_PIX_F32 = 1, 2, 3, 4
+CT_PIX_U8, CT_PIX_U16, CT_PIX_U64, CT_PIX_F32, CT_PIX_RGBA8 = 1, 2, 3, 4, 5
+CT_COLOR_ANALYSIS, CT_COLOR_GRAY, CT_COLOR_COLOR, CT_COLOR_DISP_ABS, CT_COLOR_DISP_REL = range(5)
 # EDisparityId codes
 DISP_FIRST, DISP_LAST = 0x0001, 0xFFEF
 DISP_CANNOT_EVALUATE, DISP_INCONSISTENT, DISP_U8_INVALID = 0xFFFF, 0xFFFA, 0xFF
@@ -91,6 +92,11 @@ class ct_batch_item(C.Structure):
 class ct_curves(C.Structure):
     _fields_ = [("ptr", C.c_void_p), ("pitch_bytes", C.c_size_t), ("width", C.c_int32), ("height", C.c_int32),
                 ("disp_count", C.c_int32), ("reserved", C.c_int32)]
+
+
+class ct_color_params(C.Structure):
+    _fields_ = [("style", C.c_int32), ("disp_min", C.c_int32), ("disp_max", C.c_int32), ("inf_offset", C.c_int32),
+                ("colors", C.c_uint32 * 7)]
 
 
 CT_CONFNET_PARAMS = 12673
@@ -172,6 +178,8 @@ def _declare(L: C.CDLL) -> None:
         "ct_batch_strip_height": [H, C.c_int32, P(C.c_int32)],
         "ct_batch_graph_create": [H, P(ct_batch_item), C.c_int32],
         "ct_batch_graph_launch": [H, C.c_void_p],
+        "ct_color_params_default": [C.c_int32, P(ct_color_params)],
+        "ct_color_disparity": [img, img, P(ct_color_params), C.c_void_p],
         "ct_census_stream_create": [P(H)],
         "ct_census_stream_configure": [H, C.c_int32, fmt, P(ct_census_match_params), C.c_int32, C.c_int32],
         "ct_census_stream_submit": [H, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
@@ -219,11 +227,14 @@ def _pix_type(t) -> int:
     return m[t.dtype]
 
 
-def image(t) -> ct_image:
-    """Describes a 2-D CUDA tensor (row stride may exceed the width) as a ct_image."""
+def image(t, type_=None) -> ct_image:
+    """Describes a 2-D CUDA tensor (row stride may exceed the width) as a
+    ct_image; type_ overrides the pixel type (CT_PIX_RGBA8 for an int32 or
+    uint32 tensor of packed r, g, b, a bytes)."""
     if t.dim() != 2 or t.stride(1) != 1:
         raise CtError(CT_EINVAL, "images must be 2-D tensors with unit column stride")
-    return ct_image(t.data_ptr(), t.stride(0) * t.element_size(), t.shape[1], t.shape[0], _pix_type(t), 0)
+    return ct_image(t.data_ptr(), t.stride(0) * t.element_size(), t.shape[1], t.shape[0],
+                    _pix_type(t) if type_ is None else type_, 0)
 
 
 def _img_ref(t):
@@ -457,6 +468,21 @@ class BatchStereo(_Driver):
 
     def graph_launch(self, stream=None):
         check(lib().ct_batch_graph_launch(self._h, _stream(stream)))
+
+
+def color_params(style: int) -> ct_color_params:
+    """ColorDisparityImage::SParameter defaults for a style."""
+    p = ct_color_params()
+    check(lib().ct_color_params_default(style, C.byref(p)))
+    return p
+
+
+def color_disparity(out, disp, params: ct_color_params, stream=None):
+    """ColorDisparityImage::CDriver::Process: out is an int32 tensor (RGBA8
+    styles, bytes r, g, b, a) or uint16/int16 (the U16 styles)."""
+    rgba = params.style in (CT_COLOR_ANALYSIS, CT_COLOR_COLOR)
+    o = image(out, CT_PIX_RGBA8 if rgba else None)
+    check(lib().ct_color_disparity(C.byref(o), _img_ref(disp), C.byref(params), _stream(stream)))
 
 
 class CensusStream(_Driver):

@@ -198,6 +198,45 @@ def match_ncc_guided(L, R, D, coarse, r=5):
     return disp, s32, s64
 
 
+def color_disparity(codes, style, disp_min=1, disp_max=0xFFEF, inf_offset=0, colors=None):
+    """Disparity visualisation (ColorDisparityImage.cu:45-300; the ramp of
+    NormFloatToColor, Conversion.h:56-74) on a U16 EDisparityId code map.
+    RGBA8 styles return uint32 words (r in the low byte), the others uint16.
+    NormFloatTo (CluTec.Core, not in the reference tree) is restated as
+    rint(clamp(t, 0, 1) * max)."""
+    f32 = np.float32
+    c = np.asarray(codes).astype(np.int64)
+    disp = (c >= 1) & (c <= 0xFFEF)
+    t = (c - disp_min).astype(f32) / f32(disp_max - disp_min)
+
+    def q(v, M):
+        return np.rint(np.fmin(np.fmax(v, f32(0)), f32(1)) * f32(M)).astype(np.uint32)
+
+    def rgba(r, g, b):
+        return (r | (g << 8) | (b << 16) | np.uint32(0xFF000000)).astype(np.uint32)
+
+    if style == 0:
+        g = q(t, 255)
+        out = np.full(c.shape, 0xFF0000FF, np.uint32)  # unknown codes red
+        ids = [0, 0xFFFF, 0xFFFE, 0xFFFC, 0xFFFD, 0xFFFB, 0xFFFA]
+        for k, code in enumerate(ids):
+            out[c == code] = colors[k]
+        return np.where(disp, rgba(g, g, g), out).astype(np.uint32)
+    if style == 2:
+        with np.errstate(divide="ignore", invalid="ignore"):
+            fb = f32(1) - np.fmin(t / f32(0.7), f32(1))
+            fg = f32(1) - np.fmin(np.abs(t - f32(0.5)) / f32(0.59), f32(1))
+            fr = f32(1) - np.fmin(np.abs(t - f32(0.8)) / f32(0.7), f32(1))
+            fm = np.fmax(np.fmax(fr, fg), fb)
+            col = rgba(q(fr / fm, 255), q(fg / fm, 255), q(fb / fm, 255))
+        return np.where(disp, col, np.uint32(0xFF000000)).astype(np.uint32)
+    if style == 1:
+        return np.where(disp, q(t, 65535), 0).astype(np.uint16)
+    if style == 3:
+        return np.where(disp, c, 0).astype(np.uint16)
+    return np.where(disp, (0x7FFF + inf_offset) - (c - 1), 0).astype(np.uint16)
+
+
 def crosscheck(base, other, tol=1, left_to_right=True):
     """-> (out int16 with -2 = inconsistent, (min, max))"""
     base = np.ascontiguousarray(base, np.int16)

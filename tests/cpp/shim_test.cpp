@@ -206,6 +206,21 @@ static int RunGpu(const char* weights) {
                 }
         CHECK(bad == 0 && low == 0, "NCC: %d interior pixels off, %d scores below 1", bad, low);
 
+        // visualisation of the map: interior pixels gray at t = K / 128,
+        // border pixels (CannotEvaluate) in the default colour
+        ColorDisparityImage::SParameter cp;
+        cp.Set(1, 129, 0);
+        ColorDisparityImage::CDriver col;
+        col.Configure(dev, f16, cp);
+        CDeviceSurface rgba(SImageFormat(W, H, EDataType::RGBA8));
+        ProcessKernel(col, rgba, disp, ColorDisparityImage::EStyle::Analysis);
+        auto cv = rgba.CopyInto<uint32_t>();
+        const uint32_t gray = uint32_t(std::lrint(float(K) / 128.f * 255.f));
+        const uint32_t want_gray = gray | (gray << 8) | (gray << 16) | 0xFF000000u;
+        CHECK(cv[size_t(60) * W + 100] == want_gray, "colour: interior %08x, want %08x", cv[size_t(60) * W + 100],
+              want_gray);
+        CHECK(cv[0] == cp.pixCannotEvaluate, "colour: border %08x, want %08x", cv[0], cp.pixCannotEvaluate);
+
         // guided: a coarse map at half resolution holding K / 2 everywhere
         // (scaled 2 * (K / 2) = K - 1; the block ranges contain K)
         std::vector<uint8_t> coarse(size_t(W / 2) * ((H + 1) / 2), uint8_t(K / 2));
