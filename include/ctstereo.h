@@ -428,7 +428,7 @@ typedef struct ct_color_params {
     uint32_t colors[7];   /* pixUnknown .. pixInconsistent */
 } ct_color_params;
 
-/* SParameter's defaults (ColorDisparityImage.h:76-84): range First .. Last,
+/* SParameter's defaults (ColorDisparityImage.h:75-87): range First .. Last,
  * the reference's ID colours. */
 int ct_color_params_default(int32_t style, ct_color_params* p);
 /* CDriver::Process(color image, disparity image, style); asynchronous. */

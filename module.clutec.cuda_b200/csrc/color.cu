@@ -127,7 +127,7 @@ int ct_color_params_default(int32_t style, ct_color_params* p) {
     p->disp_min = CT_DISP_FIRST;
     p->disp_max = CT_DISP_LAST;
     p->inf_offset = 0;
-    // SParameter's defaults (ColorDisparityImage.h:76-84), RGBA8 with r in the low byte
+    // SParameter's defaults (ColorDisparityImage.h:75-87), RGBA8 with r in the low byte
     const uint8_t c[7][3] = {{10, 100, 180}, {0, 150, 50}, {0, 200, 200}, {200, 0, 200},
                              {200, 50, 50}, {240, 50, 150}, {100, 10, 10}};
     for (int i = 0; i < 7; ++i) p->colors[i] = uint32_t(c[i][0]) | (uint32_t(c[i][1]) << 8) | (uint32_t(c[i][2]) << 16) | 0xFF000000u;
