@@ -95,7 +95,7 @@ __device__ __forceinline__ void hsum(const uint32_t (&V)[kCPT], uint32_t (&C)[kC
     }
 }
 
-template <int R, bool AW, int DIR>
+template <int R, bool AW, int DIR, bool G>  // G: guided (AW only)
 __global__ void __launch_bounds__(kNT, 1)
     ad_match_kernel(const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmM, Args a) {
     constexpr int EXT = ext_of(R, AW);
@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(kNT, 1)
     // the union skip the matching. Unguided, base = 0 and every warp below D
     // matches.
     int base = 0, ulo = 0, uhi = a.D - 1;
-    if (a.guide) {
+    if constexpr (G) {
         const int2 u = guide::tile_union(a.guide, a.guide_gw, xs + EXT, min(xs + EXT + TWO, a.W) - 1, y0,
                                          min(y0 + a.th, a.H) - 1, reinterpret_cast<int*>(bar + 1));
         ulo = u.x;
@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(kNT, 1)
                 int lim = DIR == 0 ? x - EXT : a.W - 1 - EXT - x;
                 lim = min(lim, a.D - 1);
                 int glo = 0;
-                if (a.guide) {  // this pixel's block range (pixels outside the image search nothing)
+                if constexpr (G) {  // this pixel's block range (pixels outside the image search nothing)
                     const int y = y0 + oy;
                     const uint32_t g = (y < a.H && x < a.W)
                                            ? __ldg(&a.guide[(size_t)(y / guide::kBlock) * a.guide_gw + x / guide::kBlock])
@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(kNT, 1)
                 for (int p = 0; p < 4; ++p) {
                     uint32_t klo = __byte_perm(A[p][c], dlo[p], 0x1054);        // cost_lo << 16 | d
                     uint32_t khi = (A[p][c] & 0xFFFF0000u) | (dlo[p] + 1);       // cost_hi << 16 | d+1
-                    if (!interior || a.guide) {
+                    if (!interior || G) {
                         if (int(dlo[p]) > lim || int(dlo[p]) < glo) klo |= 0xFFFF0000u;
                         if (int(dlo[p]) + 1 > lim || int(dlo[p]) + 1 < glo) khi |= 0xFFFF0000u;
                     }
@@ -385,11 +385,11 @@ struct AdHandle : ct_handle {
     int th = 32;
 };
 
-template <int R, bool AW, int DIR>
+template <int R, bool AW, int DIR, bool G>
 int set_attr() {
     static bool done = false;
     if (!done) {
-        CT_CUDA_TRY(cudaFuncSetAttribute(ad::ad_match_kernel<R, AW, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CT_CUDA_TRY(cudaFuncSetAttribute(ad::ad_match_kernel<R, AW, DIR, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)ad::smem_bytes(64, R, AW)));
         done = true;
     }
@@ -400,7 +400,12 @@ template <int R, bool AW, int DIR>
 int launch_ad(AdHandle* h, const ct_image* disp, const ct_image* L, const ct_image* Rimg, cudaStream_t s,
               const ct_image* init = nullptr) {
     using namespace ad;
-    if (int rc = set_attr<R, AW, DIR>()) return rc;
+    const bool guided = AW && init;  // the guided variant exists for the AW matcher only
+    if constexpr (AW) {
+        if (int rc = guided ? set_attr<R, AW, DIR, true>() : set_attr<R, AW, DIR, false>()) return rc;
+    } else {
+        if (int rc = set_attr<R, AW, DIR, false>()) return rc;
+    }
     const int W = h->fmt.width, H = h->fmt.height;
     constexpr int EXT = ext_of(R, AW), TWO = two_of(R, AW);
     Args a{};
@@ -408,7 +413,7 @@ int launch_ad(AdHandle* h, const ct_image* disp, const ct_image* L, const ct_ima
     a.keys = h->keys;
     a.out = disp->ptr; a.out_pitch = disp->pitch_bytes; a.out_type = disp->type;
     a.status = h->d_status;
-    if (init) {
+    if (guided) {
         const int gw = (W + guide::kBlock - 1) / guide::kBlock, gh = (H + guide::kBlock - 1) / guide::kBlock;
         guide::range_kernel<<<dim3((gw + 127) / 128, gh), 128, 0, s>>>(init->ptr, init->pitch_bytes, init->type,
                                                                        W / init->width, W, H, h->guide, gw, gh);
@@ -423,7 +428,14 @@ int launch_ad(AdHandle* h, const ct_image* disp, const ct_image* L, const ct_ima
     if (int rc = make_tmap_2d(&tb, B->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, W, H, B->pitch_bytes, kBW, NR)) return rc;
     if (int rc = make_tmap_2d(&tm, M->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, W, H, M->pitch_bytes, kMWs, NR)) return rc;
     dim3 grid((W + TWO - 1) / TWO, (H + a.th - 1) / a.th, (h->D + kDPC - 1) / kDPC);
-    ad_match_kernel<R, AW, DIR><<<grid, kNT, smem_bytes(a.th, R, AW), s>>>(tb, tm, a);
+    if constexpr (AW) {
+        if (guided)
+            ad_match_kernel<R, AW, DIR, true><<<grid, kNT, smem_bytes(a.th, R, AW), s>>>(tb, tm, a);
+        else
+            ad_match_kernel<R, AW, DIR, false><<<grid, kNT, smem_bytes(a.th, R, AW), s>>>(tb, tm, a);
+    } else {
+        ad_match_kernel<R, AW, DIR, false><<<grid, kNT, smem_bytes(a.th, R, AW), s>>>(tb, tm, a);
+    }
     CT_LAUNCH_CHECK();
     if (AW) {
         aw_subpixel_kernel<<<dim3((W + 127) / 128, H), 128, 0, s>>>(
