@@ -32,6 +32,9 @@
 // into the fp32 accumulator columns with tcgen05.st before each layer; the
 // epilogues read them with tcgen05.ld, apply ReLU, round to bf16 and store
 // the next layer's A operand back into the tensor memory they have consumed.
+// Each tile's block of curve words (all disparity groups of its 128 columns)
+// arrives by one TMA load issued a tile ahead; the disparity entries are read
+// two tiles ahead, so no thread waits on a global load inside the loop.
 #include "ct_internal.h"
 #include "ct_device.cuh"
 #include "census_match.cuh"
