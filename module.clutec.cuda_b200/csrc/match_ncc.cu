@@ -209,13 +209,26 @@ __global__ void __launch_bounds__(kNT, 1)
 #pragma unroll
                 for (int c = 1; c < kCPT; ++c) { s = s + win[c + 2 * R] - win[c - 1]; C[j][c] = s; }
             }
-            if (y >= a.H) continue;
+            if (y < R || y >= a.H - R) continue;
+            // right-view statistics of the 11 match columns this thread's 4
+            // columns x 8 disparities read: column xs + 4 lane - dw - 7 + k
+            int syk[kCPT + kDPW - 1], vyk[kCPT + kDPW - 1];
+            {
+                const int cb = xs + 4 * lane - dw - (kDPW - 1);
+                const size_t ob = (size_t)y * a.W;
+#pragma unroll
+                for (int k = 0; k < kCPT + kDPW - 1; ++k) {
+                    const bool in = cb + k >= 0 && cb + k < a.W;
+                    syk[k] = in ? __ldg(&a.Sy[ob + cb + k]) : 0;
+                    vyk[k] = in ? __ldg(&a.Vy[ob + cb + k]) : 0;
+                }
+            }
 #pragma unroll
             for (int c = 0; c < kCPT; ++c) {
                 const int v = 4 * lane + c;
                 if (v < R || v >= kTWV - R) continue;
                 const int x = xs + v;
-                if (x < R || x >= a.W - R || y < R || y >= a.H - R) continue;
+                if (x < R || x >= a.W - R) continue;
                 const size_t o = (size_t)y * a.W + x;
                 const int sx = a.Sx[o], vx = a.Vx[o];
                 const float fvx = __int2float_rn(vx);
@@ -230,7 +243,7 @@ __global__ void __launch_bounds__(kNT, 1)
                 for (int j = 0; j < kDPW; ++j) {
                     const int d = dw + j;
                     if (d > ghi || d < glo || x - d - R < 0) continue;
-                    const int sy = a.Sy[o - d], vy = a.Vy[o - d];
+                    const int sy = syk[c - j + kDPW - 1], vy = vyk[c - j + kDPW - 1];  // column x - d
                     const int num = n * C[j][c] - sx * sy;
                     float sc = 0.0f;
                     if ((long long)vx * (long long)vy >= n4)
