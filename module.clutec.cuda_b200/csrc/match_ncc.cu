@@ -93,7 +93,7 @@ __device__ __forceinline__ void store_ncc(const Args& a, int x, int y, bool vali
 }
 
 template <int R>
-__global__ void __launch_bounds__(kNT, 1)
+__global__ void __launch_bounds__(kNT, 2)
     ncc_match_kernel(const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmM, Args a) {
     constexpr int TWO = two_of(R);
     constexpr int n = (2 * R + 1) * (2 * R + 1);
