@@ -128,6 +128,10 @@ int ct_census_configure(ct_handle* h, int32_t device, const ct_format* fmt, cons
 /* CDriver::Process(trg, src) (CensusTransform.cu:138-157): src U8, dst U64
  * (9x7) or U8 (3x3), same width/height as configured. */
 int ct_census_process(ct_handle* h, const ct_image* dst, const ct_image* src, ct_stream stream);
+/* Both views of a stereo pair in one launch (CT_CENSUS_9X7 only): the same
+ * result as two ct_census_process calls; the two outputs share one pitch. */
+int ct_census_process_pair(ct_handle* h, const ct_image* dst_left, const ct_image* dst_right,
+                           const ct_image* src_left, const ct_image* src_right, ct_stream stream);
 
 /* ---- census block matcher -----------------------------------------------
  * 9x7 census of both images + Hamming cost (CensusDifference,

@@ -22,6 +22,18 @@ __global__ void __launch_bounds__(kNT) census9x7_kernel(const __grid_constant__ 
     census_tile(&tm_img, W, H, blockIdx.x * kTX, blockIdx.y * kTY, out, out_pitch_elems, planar, status, sm);
 }
 
+// Both views of a pair in one launch (blockIdx.z = view), so the tail wave
+// of one view overlaps the other's tiles.
+__global__ void __launch_bounds__(kNT) census9x7_pair_kernel(const __grid_constant__ CUtensorMap tm0,
+                                                              const __grid_constant__ CUtensorMap tm1, int W, int H,
+                                                              uint64_t* out0, uint64_t* out1, size_t out_pitch_elems,
+                                                              int32_t* status, int planar) {
+    __shared__ __align__(128) TileSmem sm;
+    const bool second = blockIdx.z == 1;
+    census_tile(second ? &tm1 : &tm0, W, H, blockIdx.x * kTX, blockIdx.y * kTY, second ? out1 : out0,
+                out_pitch_elems, planar, status, sm);
+}
+
 // 3x3 / 8-bit reference transform (CensusTransform.cu:60-120): bits 7..0 =
 // (-1,-1),(0,-1),(+1,-1),(-1,0),(+1,0),(-1,+1),(0,+1),(+1,+1), strict '>',
 // 1-px border not written.
@@ -54,6 +66,22 @@ int launch9x7(const ct_image* src, uint64_t* dst, size_t dst_pitch_elems, int32_
         return rc;
     dim3 grid((src->width + kTX - 1) / kTX, (src->height + kTY - 1) / kTY);
     census9x7_kernel<<<grid, kNT, 0, s>>>(tm, src->width, src->height, dst, dst_pitch_elems, status, planar);
+    CT_LAUNCH_CHECK();
+    return CT_OK;
+}
+
+// Both views (same size) in one launch.
+int launch9x7_pair(const ct_image* a, const ct_image* b, uint64_t* da, uint64_t* db, size_t dst_pitch_elems,
+                   int32_t* status, cudaStream_t s, int planar) {
+    CUtensorMap ta, tb;
+    if (int rc = make_tmap_2d(&ta, a->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, a->width, a->height, a->pitch_bytes,
+                              kBoxW, kBoxH))
+        return rc;
+    if (int rc = make_tmap_2d(&tb, b->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, b->width, b->height, b->pitch_bytes,
+                              kBoxW, kBoxH))
+        return rc;
+    dim3 grid((a->width + kTX - 1) / kTX, (a->height + kTY - 1) / kTY, 2);
+    census9x7_pair_kernel<<<grid, kNT, 0, s>>>(ta, tb, a->width, a->height, da, db, dst_pitch_elems, status, planar);
     CT_LAUNCH_CHECK();
     return CT_OK;
 }
@@ -143,9 +171,7 @@ int census_match_pass(BmCensusHandle* h, int dir, const ct_image* disp, cudaStre
 }
 
 int census_both(BmCensusHandle* h, const ct_image* left, const ct_image* right, cudaStream_t s) {
-    if (int rc = census::launch9x7(left, h->left_desc(), h->desc_pitch, h->d_status, s, 1)) return rc;
-    if (int rc = census::launch9x7(right, h->right_desc(), h->desc_pitch, h->d_status, s, 1)) return rc;
-    return CT_OK;
+    return census::launch9x7_pair(left, right, h->left_desc(), h->right_desc(), h->desc_pitch, h->d_status, s, 1);
 }
 
 }  // namespace
@@ -178,6 +204,29 @@ int ct_census_configure(ct_handle* hh, int32_t device, const ct_format* fmt, con
     h->par = *p;
     h->configured = true;
     return CT_OK;
+}
+
+int ct_census_process_pair(ct_handle* hh, const ct_image* dst_left, const ct_image* dst_right,
+                           const ct_image* src_left, const ct_image* src_right, ct_stream stream) {
+    clear_error();
+    auto* h = as<CensusHandle>(hh, Kind::Census);
+    if (!h) return fail(CT_ESTATE, "not a census handle");
+    if (!h->configured) return fail(CT_ESTATE, "process before configure");
+    if (h->par.window != CT_CENSUS_9X7) return fail(CT_EINVAL, "the pair launch is built for the 9x7 transform");
+    for (const ct_image* im : {src_left, src_right})
+        if (int rc = check_image(im, "src", 1u << CT_PIX_U8)) return rc;
+    for (const ct_image* im : {dst_left, dst_right})
+        if (int rc = check_image(im, "dst", 1u << CT_PIX_U64)) return rc;
+    for (const ct_image* im : {dst_left, dst_right, src_right})
+        if (int rc = check_same_size(im, src_left, "image", "src_left")) return rc;
+    if (src_left->width != h->fmt.width || src_left->height != h->fmt.height)
+        return fail(CT_EFORMAT, "image size differs from the configured format");
+    if (dst_left->pitch_bytes != dst_right->pitch_bytes) return fail(CT_EFORMAT, "the two outputs need one pitch");
+    if (int rc = use_device(h->device)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    h->last_stream = s;
+    return census::launch9x7_pair(src_left, src_right, static_cast<uint64_t*>(dst_left->ptr),
+                                  static_cast<uint64_t*>(dst_right->ptr), dst_left->pitch_bytes / 8, h->d_status, s, 0);
 }
 
 int ct_census_process(ct_handle* hh, const ct_image* dst, const ct_image* src, ct_stream stream) {

@@ -136,6 +136,7 @@ def _declare(L: C.CDLL) -> None:
         "ct_census_create": [P(H)],
         "ct_census_configure": [H, C.c_int32, fmt, P(ct_census_params)],
         "ct_census_process": [H, img, img, C.c_void_p],
+        "ct_census_process_pair": [H, img, img, img, img, C.c_void_p],
         "ct_bm_census_create": [P(H)],
         "ct_bm_census_configure": [H, C.c_int32, fmt, P(ct_census_match_params)],
         "ct_bm_census_process": [H, img, img, img, C.c_void_p],
@@ -295,6 +296,11 @@ class CensusTransform(_Driver):
 
     def process(self, dst, src, stream=None):
         check(lib().ct_census_process(self._h, _img_ref(dst), _img_ref(src), _stream(stream)))
+
+    def process_pair(self, dst_left, dst_right, src_left, src_right, stream=None):
+        """Both views in one launch (9x7 only)."""
+        check(lib().ct_census_process_pair(self._h, _img_ref(dst_left), _img_ref(dst_right), _img_ref(src_left),
+                                           _img_ref(src_right), _stream(stream)))
 
 
 class BlockMatcherCensus(_Driver):

@@ -28,6 +28,19 @@ def test_census9x7_bit_exact(ct, oracle, cuda, W, H):
     assert ctr.device_status() == 0
 
 
+@pytest.mark.parametrize("W,H", [(131, 45), (640, 480)])
+def test_census9x7_pair_launch_equals_two_calls(ct, oracle, cuda, W, H):
+    L, R = pair(ct, 1, 9, W, H, 64)
+    ctr = ct.CensusTransform()
+    ctr.configure(0, W, H, ct.CENSUS_9X7)
+    dl, dr = ct.alloc_image(H, W, torch.int64, cuda), ct.alloc_image(H, W, torch.int64, cuda)
+    ctr.process_pair(dl, dr, to_dev(L, cuda), to_dev(R, cuda))
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(dl.cpu().numpy().view(np.uint64), oracle.census9x7(L))
+    np.testing.assert_array_equal(dr.cpu().numpy().view(np.uint64), oracle.census9x7(R))
+    assert ctr.device_status() == 0
+
+
 def test_census3x3_reference_semantics(ct, oracle, cuda):
     W, H = 95, 61
     L, _ = pair(ct, 1, 4, W, H, 30)
