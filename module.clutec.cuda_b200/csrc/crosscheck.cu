@@ -6,6 +6,8 @@
 // codes are copied through. The kept range is reduced on the device with one
 // warp reduction and one atomic per warp, into a word pair that a memset
 // clears (min is stored as INT_MAX - d so that both halves reduce with max).
+// Rows are 16-byte aligned (checked at the C ABI), so each thread moves 16
+// bytes of the base and result rows with one load and one store.
 #include "ct_internal.h"
 #include "ct_device.cuh"
 
@@ -34,33 +36,57 @@ __device__ __forceinline__ uint8_t inconsistent<uint8_t>() { return 0xFF; }
 template <>
 __device__ __forceinline__ uint16_t inconsistent<uint16_t>() { return CT_DISP_INCONSISTENT; }
 
+// One thread per 16 bytes of a row (16 U8 or 8 U16 pixels): one 16-byte
+// load of the base row and one 16-byte store, the other map read where each
+// disparity points (L1-cached).
 template <typename T>
 __global__ void crosscheck_kernel(T* out, size_t po, const T* base, size_t pb, const T* other, size_t pt, int W,
                                   int H, int tol, int lr, int32_t* range) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    constexpr int PX = 16 / sizeof(T);
+    const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * PX;
     const int y = blockIdx.y;
-    int kept = -1;
-    if (x < W) {
-        const T v = reinterpret_cast<const T*>(reinterpret_cast<const char*>(base) + (size_t)y * pb)[x];
-        T r = v;
-        int d;
-        if (decode<T>(v, d)) {
-            const int xo = lr ? x - d : x + d;
-            r = inconsistent<T>();
-            if (xo >= 0 && xo < W) {
-                const T vo = reinterpret_cast<const T*>(reinterpret_cast<const char*>(other) + (size_t)y * pt)[xo];
-                int dd;
-                if (decode<T>(vo, dd) && abs(dd - d) <= tol) {
-                    r = v;
-                    kept = d;
+    int kmin = 0x7FFFFFFF, kmax = -1;
+    if (x0 < W) {
+        const T* brow = reinterpret_cast<const T*>(reinterpret_cast<const char*>(base) + (size_t)y * pb);
+        const T* orow = reinterpret_cast<const T*>(reinterpret_cast<const char*>(other) + (size_t)y * pt);
+        T* rrow = reinterpret_cast<T*>(reinterpret_cast<char*>(out) + (size_t)y * po);
+        const bool full = x0 + PX <= W;  // rows are 16-byte aligned, x0 a multiple of PX
+        union {
+            uint4 q;
+            T v[PX];
+        } in, res;
+        if (full) in.q = *reinterpret_cast<const uint4*>(brow + x0);
+        else
+            for (int i = 0; i < PX; ++i) in.v[i] = x0 + i < W ? brow[x0 + i] : T(0);
+#pragma unroll
+        for (int i = 0; i < PX; ++i) {
+            const int x = x0 + i;
+            const T v = in.v[i];
+            T r = v;
+            int d;
+            if (decode<T>(v, d)) {
+                const int xo = lr ? x - d : x + d;
+                r = inconsistent<T>();
+                if (xo >= 0 && xo < W) {
+                    const T vo = __ldg(orow + xo);
+                    int dd;
+                    if (decode<T>(vo, dd) && abs(dd - d) <= tol) {
+                        r = v;
+                        kmin = min(kmin, d);
+                        kmax = max(kmax, d);
+                    }
                 }
             }
+            res.v[i] = r;
         }
-        reinterpret_cast<T*>(reinterpret_cast<char*>(out) + (size_t)y * po)[x] = r;
+        if (full) *reinterpret_cast<uint4*>(rrow + x0) = res.q;
+        else
+            for (int i = 0; i < PX; ++i)
+                if (x0 + i < W) rrow[x0 + i] = res.v[i];
     }
     if (range) {
-        const unsigned mn = __reduce_max_sync(0xffffffffu, kept >= 0 ? unsigned(0x7FFFFFFF - kept) : 0u);
-        const unsigned mx = __reduce_max_sync(0xffffffffu, unsigned(kept + 1));
+        const unsigned mn = __reduce_max_sync(0xffffffffu, kmax >= 0 ? unsigned(0x7FFFFFFF - kmin) : 0u);
+        const unsigned mx = __reduce_max_sync(0xffffffffu, unsigned(kmax + 1));
         if ((threadIdx.x & 31) == 0) {
             if (mn) atomicMax(reinterpret_cast<unsigned*>(&range[0]), mn);
             if (mx) atomicMax(reinterpret_cast<unsigned*>(&range[1]), mx);
@@ -84,7 +110,8 @@ struct CrossCheckHandle : ct_handle {
 int crosscheck_launch(const ct_image* result, const ct_image* base, const ct_image* other, int tol, int lr,
                       int32_t* range, cudaStream_t s) {
     const int W = base->width, H = base->height;
-    dim3 grid((W + 127) / 128, H);
+    const int px = 16 / int(pix_size(base->type));  // pixels per thread
+    dim3 grid((W + 128 * px - 1) / (128 * px), H);
     if (range) CT_CUDA_TRY(cudaMemsetAsync(range, 0, 2 * sizeof(int32_t), s));
     if (base->type == CT_PIX_U8) {
         crosscheck_kernel<uint8_t><<<grid, 128, 0, s>>>(
