@@ -284,7 +284,7 @@ def confnet_compare(ct, dev, stream, m, dL, dR, hL, hR, flush, steps, eval_pairs
                 "invalid_fraction": round(auc["invalid_fraction"], 4), "eval_pairs": auc["pairs"],
                 "eval_pixels": auc["pixels"], "threshold": 0.5,
                 "weights": "module.clutec.cuda_b200/confnet_census128.f32 (2000 seeded training pairs)",
-                "launches_learned": 4, "launches_plain": 5})
+                "launches_learned": 3, "launches_plain": 4})
     return res
 
 
@@ -434,7 +434,7 @@ def run_ours(args):
     units_launch = W_ * H_ * D_
     achieved_popc = 2.0 * units_launch / (match_ms * 1e-3)          # 2 POPC per unit
     int_peak = rates["iadd3_per_clk_sm"] * sms * clock_hz
-    launches = 5  # census x2, census_match_kernel x2 (D halves merged in-kernel), cross-check
+    launches = 4  # census of both views, census_match_kernel x2 (D halves merged in-kernel), cross-check
 
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
