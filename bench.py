@@ -661,7 +661,7 @@ def run_workload(args):
 
             def cpu_fn():
                 oracle.match_ncc_guided(L, R, D, coarse_cpu(), 5)
-            metric, launches = "frames/s coarse-to-fine NCC (census L-R at 1/4, guided 11x11), 1920x1080 D=128", 10
+            metric, launches = "frames/s coarse-to-fine NCC (census L-R at 1/4, guided 11x11), 1920x1080 D=128", 9
         else:
             m = ct.BlockMatcherAW()
             m.configure(local, W, H, D)
