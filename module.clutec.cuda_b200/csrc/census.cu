@@ -19,6 +19,9 @@ __global__ void __launch_bounds__(kNT) census9x7_kernel(const __grid_constant__ 
                                                          uint64_t* out, size_t out_pitch_elems,
                                                          int32_t* status, int planar) {
     __shared__ __align__(128) TileSmem sm;
+    // a matcher launched next with programmatic stream serialisation may
+    // start its prologue now; it waits for these descriptors itself
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     census_tile(&tm_img, W, H, blockIdx.x * kTX, blockIdx.y * kTY, out, out_pitch_elems, planar, status, sm);
 }
 
@@ -29,6 +32,7 @@ __global__ void __launch_bounds__(kNT) census9x7_pair_kernel(const __grid_consta
                                                               uint64_t* out0, uint64_t* out1, size_t out_pitch_elems,
                                                               int32_t* status, int planar) {
     __shared__ __align__(128) TileSmem sm;
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");  // as census9x7_kernel
     const bool second = blockIdx.z == 1;
     census_tile(second ? &tm1 : &tm0, W, H, blockIdx.x * kTX, blockIdx.y * kTY, second ? out1 : out0,
                 out_pitch_elems, planar, status, sm);

@@ -505,7 +505,16 @@ __global__ void __launch_bounds__(Var<DPW>::kNT, 1)
                         MatchArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const Smem sm(smem_raw);
+    // A kernel launched after this one with programmatic stream
+    // serialisation (the other direction, the cross-check, the
+    // confidence-net inference) may be scheduled once every CTA of this grid
+    // has started; it waits for this grid's results itself
+    // (griddepcontrol.wait). Without such a launch this is a no-op.
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     init_barriers(sm);
+    // This launch is itself programmatic: the previous kernel (census or the
+    // other direction) must be complete before any global read or write.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     uint32_t par[2] = {0, 0};
     const Tile t{int(blockIdx.x), int(blockIdx.y), int(blockIdx.z), int(gridDim.x), int(gridDim.z)};
     run_tile<DIR, DPW, CURVE>(&tmB, &tmM, a, t, sm, par);
@@ -583,14 +592,27 @@ template <int DIR>
 inline cudaError_t launch_census_match(const CUtensorMap& tb, const CUtensorMap& tm, const MatchArgs& a,
                                        cudaStream_t s, int dpw = 4) {
     dim3 grid((a.W + kTWO - 1) / kTWO, (a.H + a.th - 1) / a.th, (a.D + kDPC - 1) / kDPC);
-    if (a.curve) {
-        if (dpw == 8) census_match_kernel<DIR, 8, true><<<grid, Var<8>::kNT, smem_bytes(), s>>>(tb, tm, a);
-        else census_match_kernel<DIR, 4, true><<<grid, Var<4>::kNT, smem_bytes(), s>>>(tb, tm, a);
-    } else {
-        if (dpw == 8) census_match_kernel<DIR, 8><<<grid, Var<8>::kNT, smem_bytes(), s>>>(tb, tm, a);
-        else census_match_kernel<DIR, 4><<<grid, Var<4>::kNT, smem_bytes(), s>>>(tb, tm, a);
-    }
-    cudaError_t e = cudaGetLastError();
+    // programmatic stream serialisation: the launch overlaps the previous
+    // kernel's tail; the kernel waits (griddepcontrol.wait) before reading
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(dpw == 8 ? Var<8>::kNT : Var<4>::kNT);
+    cfg.dynamicSmemBytes = smem_bytes();
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e;
+    if (a.curve)
+        e = dpw == 8 ? cudaLaunchKernelEx(&cfg, census_match_kernel<DIR, 8, true>, tb, tm, a)
+                     : cudaLaunchKernelEx(&cfg, census_match_kernel<DIR, 4, true>, tb, tm, a);
+    else
+        e = dpw == 8 ? cudaLaunchKernelEx(&cfg, census_match_kernel<DIR, 8, false>, tb, tm, a)
+                     : cudaLaunchKernelEx(&cfg, census_match_kernel<DIR, 4, false>, tb, tm, a);
+    if (e != cudaSuccess) return e;
+    e = cudaGetLastError();
     if (e != cudaSuccess || grid.z == 1 || a.merge_last) return e;
     keys_finalize_kernel<<<dim3((a.W + 255) / 256, a.H), 256, 0, s>>>(a.keys, a.W, a.H, kAR, a.out, a.out_pitch,
                                                                       a.out_type);

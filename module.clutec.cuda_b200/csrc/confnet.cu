@@ -688,6 +688,11 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(const __grid_constant__ C
     fence_after();
     const uint32_t tm = *tslot;
     const uint32_t tl = tm + (uint32_t(warp * 32) << 16);  // this warp's lane quarter
+    // Launched with programmatic stream serialisation, this kernel may start
+    // while the matcher that writes the curves and winners is still running:
+    // everything above reads only the weight image; wait here for the
+    // previous grid's results before the first curve or disparity read.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 
     const float* bias = reinterpret_cast<const float*>(smem + kWImg + kBias);
     const float* w5 = bias + 160;
@@ -1351,7 +1356,20 @@ int ct_confnet_infer(ct_handle* hh, const ct_image* score, const ct_curves* curv
     const uint32_t box[3] = {uint32_t(inf::kBoxWords), uint32_t(inf::kGroups), 1};
     if (int rc = make_tmap_nd(&tm_curve, curves->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, 3, dims, strides, box))
         return rc;
-    inf::infer_kernel<<<grid, inf::kNT, inf::kSmem, s>>>(tm_curve, a);
+    // programmatic stream serialisation: the kernel's prologue (weight
+    // image, barriers, TMEM) overlaps the tail of the previous kernel on the
+    // stream; griddepcontrol.wait in the kernel orders the data
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(inf::kNT);
+    cfg.dynamicSmemBytes = inf::kSmem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CT_CUDA_TRY(cudaLaunchKernelEx(&cfg, inf::infer_kernel, tm_curve, a));
     CT_LAUNCH_CHECK();
     return CT_OK;
 }

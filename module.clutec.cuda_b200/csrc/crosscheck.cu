@@ -43,6 +43,8 @@ template <typename T>
 __global__ void crosscheck_kernel(T* out, size_t po, const T* base, size_t pb, const T* other, size_t pt, int W,
                                   int H, int tol, int lr, int32_t* range) {
     constexpr int PX = 16 / sizeof(T);
+    // launched with programmatic stream serialisation after the matcher
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * PX;
     const int y = blockIdx.y;
     int kmin = 0x7FFFFFFF, kmax = -1;
@@ -113,14 +115,25 @@ int crosscheck_launch(const ct_image* result, const ct_image* base, const ct_ima
     const int px = 16 / int(pix_size(base->type));  // pixels per thread
     dim3 grid((W + 128 * px - 1) / (128 * px), H);
     if (range) CT_CUDA_TRY(cudaMemsetAsync(range, 0, 2 * sizeof(int32_t), s));
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(128);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
     if (base->type == CT_PIX_U8) {
-        crosscheck_kernel<uint8_t><<<grid, 128, 0, s>>>(
-            static_cast<uint8_t*>(result->ptr), result->pitch_bytes, static_cast<const uint8_t*>(base->ptr),
-            base->pitch_bytes, static_cast<const uint8_t*>(other->ptr), other->pitch_bytes, W, H, tol, lr, range);
+        CT_CUDA_TRY(cudaLaunchKernelEx(&cfg, crosscheck_kernel<uint8_t>, static_cast<uint8_t*>(result->ptr),
+                                       result->pitch_bytes, static_cast<const uint8_t*>(base->ptr), base->pitch_bytes,
+                                       static_cast<const uint8_t*>(other->ptr), other->pitch_bytes, W, H, tol, lr,
+                                       range));
     } else {
-        crosscheck_kernel<uint16_t><<<grid, 128, 0, s>>>(
-            static_cast<uint16_t*>(result->ptr), result->pitch_bytes, static_cast<const uint16_t*>(base->ptr),
-            base->pitch_bytes, static_cast<const uint16_t*>(other->ptr), other->pitch_bytes, W, H, tol, lr, range);
+        CT_CUDA_TRY(cudaLaunchKernelEx(&cfg, crosscheck_kernel<uint16_t>, static_cast<uint16_t*>(result->ptr),
+                                       result->pitch_bytes, static_cast<const uint16_t*>(base->ptr), base->pitch_bytes,
+                                       static_cast<const uint16_t*>(other->ptr), other->pitch_bytes, W, H, tol, lr,
+                                       range));
     }
     CT_LAUNCH_CHECK();
     return CT_OK;
