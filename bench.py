@@ -56,7 +56,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="census1080",
-                    choices=["census1080", "sad640", "ncc1080", "ncc1080g", "aw1440", "batch64", "confnet1080"],
+                    choices=["census1080", "sad640", "ncc1080", "ncc1080g", "aw1440", "batch64", "confnet1080",
+                             "mip1080"],
                     help="census1080 (default, the headline) or another configuration, one JSON line each")
     ap.add_argument("--eval-pairs", type=int, default=None,
                     help="held-out 1080p pairs for the confidence-net AUC (default 4 in the census line, 24 in confnet1080)")
@@ -604,6 +605,38 @@ def run_workload(args):
             oracle.crosscheck(dl, dr, 1, True)
             return 2 * L.shape[0] * L.shape[1] * D / (time.perf_counter() - t0) / 1e6, f"pair 0 alone ({L.shape[1]}x{L.shape[0]}, D={D})"
         launches = 2
+    elif wl == "mip1080":
+        # disparity mip-maps of a 1920x1080 U16 code map: the ground truth of
+        # the seeded census pair (codes d + 1, occluded pixels CannotEvaluate),
+        # every level the reference writes by default (levels 0 .. max - 1)
+        W, H, D = 1920, 1080, 128
+        _, _, G, O = ct.synth_pair(2, SEED + rank, W, H, D - 1)
+        codes = np.where(np.asarray(O) != 0, 0xFFFF, np.asarray(G).astype(np.int64) + 1).astype(np.uint16)
+        disp = up(codes.view(np.int16))
+        pw, nmax = ct.disp_mipmap_format(W, H)
+        mipmap = ct.alloc_image(H, pw, torch.float32, dev)
+        step = lambda: ct.disp_mipmaps(mipmap, disp, 0, stream=stream)
+        _, rects = oracle.mipmap_layout(W, H)
+        written = sum(w * h for (_, _, w, h) in rects[:nmax])
+        alg_bytes = 2 * W * H + 4 * written
+
+        def check_fn():
+            want, _ = oracle.disp_mipmaps(codes, 0, np.zeros((H, pw), np.float32))
+            got = mipmap.cpu().numpy()
+            return all(np.array_equal(got[y:y + h, x:x + w].view(np.uint32), want[y:y + h, x:x + w].view(np.uint32))
+                       for (x, y, w, h) in rects[:nmax])
+
+        def cpu_sample():
+            t0 = time.perf_counter()
+            for _ in range(5):
+                oracle.disp_mipmaps(codes, 0)
+            return 5 * W * H / (time.perf_counter() - t0) / 1e6, "5 full pyramids (numpy restatement, 1 thread)"
+        units, unit = W * H, "Mpix/s"
+        metric = "Mpix/s disparity mip-maps (CreateDispMipMaps, all default levels), 1920x1080 U16"
+        big = sum(1 for (_, _, w, h) in rects[2:nmax] if w * h > 16384)
+        launches = 1 + big + (1 if nmax - 1 > 1 + big else 0)
+        cfg = {"workload": "mip1080_disp_mipmaps", "width": W, "height": H, "levels_written": nmax,
+               "packed_width": pw}
     else:
         W, H, D, kind = {"sad640": (640, 480, 64, 1), "ncc1080": (1920, 1080, 128, 2),
                          "ncc1080g": (1920, 1080, 128, 2), "aw1440": (2560, 1440, 256, 3)}[wl]
@@ -704,6 +737,17 @@ def run_workload(args):
         "data": "synthetic (seeded generator)", "config": dict(cfg, l2="flushed before every timed step"),
         "gpu_launches": launches * args.steps, "clocks": clocks,
     }
+    if wl == "mip1080":
+        out_line["dtype"] = "u16 codes / fp32 levels"
+        try:
+            peak, src = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"], "of measured"
+        except (OSError, KeyError, ValueError):
+            peak, src = 6650.0, "of fallback"
+        ach = alg_bytes / (ms * 1e-3) / 1e9
+        out_line["roofline"] = {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                                "frac": round(ach / peak, 4), "traffic": None, "peak_source": src,
+                                "algorithmic_bytes": alg_bytes,
+                                "note": "whole call (all launches) timed; 2 B read + 4 B per written level pixel"}
     if rank == 0:
         out_line["parity_rank0"] = bool(check_fn())
         v, sample = cpu_sample()

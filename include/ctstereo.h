@@ -438,6 +438,36 @@ int ct_color_params_default(int32_t style, ct_color_params* p);
 /* CDriver::Process(color image, disparity image, style); asynchronous. */
 int ct_color_disparity(const ct_image* out, const ct_image* disp, const ct_color_params* p, ct_stream stream);
 
+/* ---- disparity mip-maps: CreateDispMipMaps::CDriver ------------------------
+ * Replaces CreateDispMipMaps.h:44-80 / CreateDispMipMaps.cu:66-330 and the
+ * packed mip-map surface _CDeviceSurfMipMap / CDeviceSurfMipMap
+ * (DeviceSurfMipMap.h:40-150, DeviceSurfMipMap.cpp:68-146). One F32 image
+ * holds every level: level 0 (W x H) at (0, 0), level k >= 1 at
+ * (X1, H_1 + ... + H_{k-1}) with X1 = W rounded up to a multiple of 4,
+ * W_{k+1} = (W_k - 1) / 2 and H_{k+1} = (H_k - 1) / 2; the image is
+ * (X1 + (W - 1) / 2) x H. Level 0 = the codes as floats (First .. Last ->
+ * the code, other IDs -> 0 = Unknown; U8 maps are read as code d + 1, 255 as
+ * CannotEvaluate); level k + 1 = the 1-2-1 weighted mean of the non-zero
+ * entries of level k horizontally at x = 2i .. 2i + 2, then vertically at
+ * y = 2j .. 2j + 2, times 0.5 (SmoothHorizontalLum / SmoothVerticalLum,
+ * bit-identical, IEEE division). */
+
+/* Packed image width for a width x height disparity map (its height is
+ * height) and the maximal level count (CDeviceSurfMipMap::Create and
+ * MaxMipMapLevelCount; the number of levels k >= 1 that are not empty). */
+int ct_disp_mipmap_format(int32_t width, int32_t height, int32_t* packed_width, int32_t* max_levels);
+/* Origin and size of level 0 .. max_levels in the packed image
+ * (_CDeviceSurfMipMap::GetOrigin / Format). Every origin is 16-byte aligned
+ * in a 16-byte aligned image, so a level can be passed on as a ct_image. */
+int ct_disp_mipmap_level(int32_t width, int32_t height, int32_t level, int32_t* x, int32_t* y, int32_t* w,
+                         int32_t* h);
+/* CDriver::Run(mip-map, temp, disparity, level_count): writes levels
+ * 0 .. level_count - 1 of `mipmap` (F32, the packed size) from disp (U16 or
+ * U8). As in the reference, level_count > max_levels is CT_EINVAL,
+ * level_count <= 0 means max_levels, and level_count == 1 writes nothing.
+ * Asynchronous; no scratch memory. */
+int ct_disp_mipmaps(const ct_image* mipmap, const ct_image* disp, int32_t level_count, ct_stream stream);
+
 /* ---- synthetic stereo pairs -----------------------------------------------
  * Seeded generator of rectified stereo pairs with ground truth (host memory).
  *   kind 1: fractal value noise (4 octaves) left image; disparity = 4

@@ -660,6 +660,93 @@ private:
 
 }  // namespace ColorDisparityImage
 
+/* ---- CDeviceSurfMipMap (DeviceSurfMipMap.h:40-150) ------------------------- */
+
+/* The packed disparity mip-map: one F32 image holding every level (layout:
+ * ct_disp_mipmap_format / ct_disp_mipmap_level). GetMipMap returns a view of
+ * one level that any driver taking an F32 image accepts. */
+class CDeviceSurfMipMap {
+public:
+    CDeviceSurfMipMap() = default;
+    explicit CDeviceSurfMipMap(const SImageFormat& xFormat) { Create(xFormat); }
+
+    /* xFormat: the format of level 0 (the disparity map's size). */
+    void Create(const SImageFormat& xFormat) {
+        int32_t pw = 0, n = 0;
+        Ensure(ct_disp_mipmap_format(xFormat.iWidth, xFormat.iHeight, &pw, &n), "CDeviceSurfMipMap::Create");
+        m_xImage.Create(SImageFormat(pw, xFormat.iHeight, EDataType::Single));
+        m_xFormat = SImageFormat(xFormat.iWidth, xFormat.iHeight, EDataType::Single);
+        m_iMax = n;
+        m_iActive = 0;
+    }
+
+    int MaxMipMapLevelCount() const { return m_iMax; }
+    int GetActiveMipMapLevelCount() const { return m_iActive; }
+    void SetActiveMipMapLevelCount(int iCount) {
+        if (iCount < 0 || iCount > m_iMax) throw CError(CT_EINVAL, "Given mip-map level count out of range");
+        m_iActive = iCount;
+    }
+
+    void GetOrigin(int& iX, int& iY, int iLevel) const {
+        int32_t x, y, w, h;
+        Ensure(ct_disp_mipmap_level(m_xFormat.iWidth, m_xFormat.iHeight, iLevel, &x, &y, &w, &h), "GetOrigin");
+        iX = x;
+        iY = y;
+    }
+    SImageFormat Format(int iLevel) const {
+        int32_t x, y, w, h;
+        Ensure(ct_disp_mipmap_level(m_xFormat.iWidth, m_xFormat.iHeight, iLevel, &x, &y, &w, &h), "Format");
+        return SImageFormat(w, h, EDataType::Single);
+    }
+    _CDeviceSurface GetMipMap(int iLevel) const {
+        int iX = 0, iY = 0;
+        GetOrigin(iX, iY, iLevel);
+        char* p = static_cast<char*>(m_xImage.DataPointer()) + size_t(iY) * m_xImage.Pitch() + size_t(iX) * 4;
+        return _CDeviceSurface(p, m_xImage.Pitch(), Format(iLevel));
+    }
+    /* The whole packed image. */
+    const CDeviceSurface& Surface() const { return m_xImage; }
+
+private:
+    CDeviceSurface m_xImage;
+    SImageFormat m_xFormat;
+    int m_iMax = 0, m_iActive = 0;
+};
+
+/* ---- CreateDispMipMaps (CreateDispMipMaps.h:44-80) ------------------------- */
+namespace CreateDispMipMaps {
+
+class CDriver : public CKernelDriverBase {
+public:
+    CDriver() : CKernelDriverBase("Create Disparity Mip Maps") {}
+
+    void Configure(const CDevice& xDevice, const SImageFormat& xFormat) {
+        EnsureCuda(cudaSetDevice(xDevice.iDevice), "CreateDispMipMaps::Configure");
+        m_xFormat = xFormat;
+    }
+
+    /* CDriver::Run (CreateDispMipMaps.cu:246-330): levels 0 .. iLevelCount - 1
+     * of xMipMap from surfDisp (UInt16 codes or UInt8 disparities); <= 0 =
+     * all, 1 = nothing, more than MaxMipMapLevelCount() throws. xTemp is
+     * not used (the horizontal and vertical passes are one kernel). Timed
+     * like the reference's Run (LastProcessTime). */
+    void Run(CDeviceSurfMipMap& xMipMap, CDeviceSurface& /*xTemp*/, const _CDeviceSurface& surfDisp,
+             int iLevelCount = 0) {
+        Begin();
+        Ensure(ct_disp_mipmaps(xMipMap.Surface().C(), surfDisp.C(), iLevelCount, S()), "CreateDispMipMaps::Run");
+        End();
+        if (iLevelCount != 1) xMipMap.SetActiveMipMapLevelCount(iLevelCount <= 0 ? xMipMap.MaxMipMapLevelCount()
+                                                                                 : iLevelCount);
+    }
+
+    void EnsureDeviceStatus() {}  // no device-side waits
+
+private:
+    SImageFormat m_xFormat;
+};
+
+}  // namespace CreateDispMipMaps
+
 /* ---- no reference counterpart ----------------------------------------------- */
 
 /* Device cost-curve volume for BlockMatcherCensus::ProcessCurves and

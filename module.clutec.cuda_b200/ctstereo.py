@@ -181,6 +181,10 @@ def _declare(L: C.CDLL) -> None:
         "ct_batch_graph_launch": [H, C.c_void_p],
         "ct_color_params_default": [C.c_int32, P(ct_color_params)],
         "ct_color_disparity": [img, img, P(ct_color_params), C.c_void_p],
+        "ct_disp_mipmap_format": [C.c_int32, C.c_int32, P(C.c_int32), P(C.c_int32)],
+        "ct_disp_mipmap_level": [C.c_int32, C.c_int32, C.c_int32, P(C.c_int32), P(C.c_int32), P(C.c_int32),
+                                 P(C.c_int32)],
+        "ct_disp_mipmaps": [img, img, C.c_int32, C.c_void_p],
         "ct_census_stream_create": [P(H)],
         "ct_census_stream_configure": [H, C.c_int32, fmt, P(ct_census_match_params), C.c_int32, C.c_int32],
         "ct_census_stream_submit": [H, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
@@ -489,6 +493,29 @@ def color_disparity(out, disp, params: ct_color_params, stream=None):
     rgba = params.style in (CT_COLOR_ANALYSIS, CT_COLOR_COLOR)
     o = image(out, CT_PIX_RGBA8 if rgba else None)
     check(lib().ct_color_disparity(C.byref(o), _img_ref(disp), C.byref(params), _stream(stream)))
+
+
+def disp_mipmap_format(width: int, height: int):
+    """-> (packed image width, maximal level count) of the packed mip-map of a
+    width x height disparity map (CDeviceSurfMipMap::Create,
+    DeviceSurfMipMap.cpp:68-146); the packed image is `height` rows high."""
+    pw, n = C.c_int32(), C.c_int32()
+    check(lib().ct_disp_mipmap_format(width, height, C.byref(pw), C.byref(n)))
+    return pw.value, n.value
+
+
+def disp_mipmap_level(width: int, height: int, level: int):
+    """-> (x, y, w, h) of a level in the packed mip-map
+    (_CDeviceSurfMipMap::GetOrigin / Format)."""
+    v = [C.c_int32() for _ in range(4)]
+    check(lib().ct_disp_mipmap_level(width, height, level, *[C.byref(x) for x in v]))
+    return tuple(x.value for x in v)
+
+
+def disp_mipmaps(mipmap, disp, level_count: int = 0, stream=None):
+    """CreateDispMipMaps::CDriver::Run: mipmap is a float32 CUDA tensor of the
+    packed size, disp a uint8 or int16/uint16 disparity map."""
+    check(lib().ct_disp_mipmaps(C.byref(image(mipmap)), _img_ref(disp), level_count, _stream(stream)))
 
 
 class CensusStream(_Driver):

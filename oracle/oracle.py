@@ -237,6 +237,71 @@ def color_disparity(codes, style, disp_min=1, disp_max=0xFFEF, inf_offset=0, col
     return np.where(disp, (0x7FFF + inf_offset) - (c - 1), 0).astype(np.uint16)
 
 
+def mipmap_layout(W, H):
+    """Packed mip-map layout of a W x H map (DeviceSurfMipMap.h:78-120,
+    DeviceSurfMipMap.cpp:68-146): -> (packed width, [(x, y, w, h) of level
+    0 .. max]); the packed image is H rows high and max = len(rects) - 1."""
+    nxt = lambda n: (n - 1) // 2 if n >= 1 else 0  # noqa: E731  C's (n - 1) / 2 for n >= 1
+    x1 = (W // 4 + (1 if W % 4 else 0)) * 4
+    rects, yy = [(0, 0, W, H)], 0
+    w, h = W, H
+    while nxt(w) > 0 and nxt(h) > 0:
+        w, h = nxt(w), nxt(h)
+        rects.append((x1, yy, w, h))
+        yy += h
+    return x1 + nxt(W), rects
+
+
+def disp_mipmaps(codes, level_count=0, init=None):
+    """Packed disparity mip-map (CreateDispMipMaps.cu:66-330 on the surface
+    layout of DeviceSurfMipMap.h:78-120 / DeviceSurfMipMap.cpp:68-146) of a
+    U16 EDisparityId code map, in float32 with the reference's operation
+    order: CopyDispChannel (:90-114), then per level SmoothHorizontalLum
+    (:117-176) into a temporary of width (W - 1) / 2 and SmoothVerticalLum
+    (:179-238) with the 0.5 factor. `init` is the packed image before the
+    call (pixels not written keep it; zeros if None). Returns (packed image,
+    [(x, y, w, h) per level 0 .. max])."""
+    f32 = np.float32
+    c = np.asarray(codes).astype(np.int64)
+    H, W = c.shape
+    pw, rects = mipmap_layout(W, H)
+    dims = [(w, h) for (_, _, w, h) in rects]
+    max_levels = len(rects) - 1
+    out = np.zeros((H, pw), f32) if init is None else np.array(init, f32, copy=True)
+    if level_count > max_levels:
+        raise ValueError("level count larger than the maximal possible level")
+    if level_count <= 0:
+        level_count = max_levels
+    elif level_count == 1:
+        return out, rects
+
+    def mean121(a, b, cc):
+        cnt = np.zeros(a.shape, f32)
+        s = np.zeros(a.shape, f32)
+        m = a != 0
+        cnt = np.where(m, cnt + f32(1), cnt)
+        s = np.where(m, s + a, s)
+        m = b != 0
+        cnt = np.where(m, cnt + f32(2), cnt)
+        s = np.where(m, s + b * f32(2), s)
+        m = cc != 0
+        cnt = np.where(m, cnt + f32(1), cnt)
+        s = np.where(m, s + cc, s)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            return np.where(cnt > 0, s / cnt, f32(0)).astype(f32)
+
+    lvl = np.where((c >= 1) & (c <= 0xFFEF), c, 0).astype(f32)
+    out[:H, :W] = lvl
+    for k in range(level_count - 1):
+        w1, h1 = dims[k + 1]
+        h0 = lvl.shape[0]
+        tmp = mean121(lvl[:h0, 0:2 * w1:2], lvl[:h0, 1:2 * w1 + 1:2], lvl[:h0, 2:2 * w1 + 2:2])
+        lvl = (f32(0.5) * mean121(tmp[0:2 * h1:2], tmp[1:2 * h1 + 1:2], tmp[2:2 * h1 + 2:2])).astype(f32)
+        x, y, _, _ = rects[k + 1]
+        out[y:y + h1, x:x + w1] = lvl
+    return out, rects
+
+
 def crosscheck(base, other, tol=1, left_to_right=True):
     """-> (out int16 with -2 = inconsistent, (min, max))"""
     base = np.ascontiguousarray(base, np.int16)

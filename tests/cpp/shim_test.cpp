@@ -221,6 +221,24 @@ static int RunGpu(const char* weights) {
               want_gray);
         CHECK(cv[0] == cp.pixCannotEvaluate, "colour: border %08x, want %08x", cv[0], cp.pixCannotEvaluate);
 
+        // mip-maps of the map: level 1 interior = 0.5 * code (K + 1), level 0
+        // border (CannotEvaluate) = 0
+        CDeviceSurfMipMap mip(f16);
+        CreateDispMipMaps::CDriver mm;
+        mm.Configure(dev, f16);
+        CDeviceSurface tmp;
+        CHECK(ThrownCode([&] { mm.Run(mip, tmp, disp, mip.MaxMipMapLevelCount() + 1); }) == CT_EINVAL,
+              "mip-map level count above the maximum");
+        mm.Run(mip, tmp, disp, 0);
+        CHECK(mip.GetActiveMipMapLevelCount() == mip.MaxMipMapLevelCount(), "mip-map active level count");
+        auto mv = mip.Surface().CopyInto<float>();
+        const int mpw = mip.Surface().Format().iWidth;
+        int mx = 0, my = 0;
+        mip.GetOrigin(mx, my, 1);
+        const float l1 = mv[size_t(my + 30) * mpw + mx + 50];
+        CHECK(l1 == 0.5f * float(K + 1) && mv[0] == 0.f, "mip-map: level 1 %g, want %g; level 0 border %g", l1,
+              0.5f * float(K + 1), mv[0]);
+
         // guided: a coarse map at half resolution holding K / 2 everywhere
         // (scaled 2 * (K / 2) = K - 1; the block ranges contain K)
         std::vector<uint8_t> coarse(size_t(W / 2) * ((H + 1) / 2), uint8_t(K / 2));
