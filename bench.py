@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="census1080",
                     choices=["census1080", "sad640", "ncc1080", "ncc1080g", "aw1440", "batch64", "confnet1080",
-                             "mip1080"],
+                             "mip1080", "map3d1080"],
                     help="census1080 (default, the headline) or another configuration, one JSON line each")
     ap.add_argument("--eval-pairs", type=int, default=None,
                     help="held-out 1080p pairs for the confidence-net AUC (default 4 in the census line, 24 in confnet1080)")
@@ -637,6 +637,37 @@ def run_workload(args):
         launches = 1 + big + (1 if nmax - 1 > 1 + big else 0)
         cfg = {"workload": "mip1080_disp_mipmaps", "width": W, "height": H, "levels_written": nmax,
                "packed_width": pw}
+    elif wl == "map3d1080":
+        # 3D points of a 1920x1080 U16 code map (the seeded pair's ground
+        # truth, occluded pixels CannotEvaluate) for a rectified pinhole pair
+        # (f = 1400 px, baseline 0.12)
+        W, H, D = 1920, 1080, 128
+        _, _, G, O = ct.synth_pair(2, SEED + rank, W, H, D - 1)
+        codes = np.where(np.asarray(O) != 0, 0xFFFF, np.asarray(G).astype(np.int64) + 1).astype(np.uint16)
+        disp = up(codes.view(np.int16))
+        cams = [(1400.0, 1400.0, W / 2, H / 2, np.eye(3), (0.0, 0.0, 0.0)),
+                (1400.0, 1400.0, W / 2, H / 2, np.eye(3), (0.12, 0.0, 0.0))]
+        m3 = ct.MapDisparityTo3D()
+        m3.configure(local, W, H, *[ct.pinhole(fx, fy, cx, cy, R, c) for (fx, fy, cx, cy, R, c) in cams])
+        pts = ct.alloc_map3d(H, W, dev)
+        step = lambda: m3.process(pts, disp, stream=stream)
+        alg_bytes = 2 * W * H + 16 * W * H
+
+        def check_fn():
+            want, _, hit = oracle.map3d(codes, cams)
+            got = pts.cpu().numpy().astype(np.float64)
+            dist = np.linalg.norm(want[..., :3], axis=-1, keepdims=True)
+            return bool((np.abs(got[..., :3] - want[..., :3]) <= 2e-4 * dist + 1e-6).all()
+                        and np.array_equal(got[..., 3], want[..., 3]))
+
+        def cpu_sample():
+            t0 = time.perf_counter()
+            oracle.map3d(codes, cams)
+            return W * H / (time.perf_counter() - t0) / 1e6, "one 1920x1080 map (numpy FP64 restatement, 1 thread)"
+        units, unit = W * H, "Mpix/s"
+        metric = "Mpix/s disparity to 3D points (MapDisparityTo3D, pinhole pair), 1920x1080 U16"
+        launches = 1
+        cfg = {"workload": "map3d1080_disparity_to_3d", "width": W, "height": H, "focal_px": 1400.0, "baseline": 0.12}
     else:
         W, H, D, kind = {"sad640": (640, 480, 64, 1), "ncc1080": (1920, 1080, 128, 2),
                          "ncc1080g": (1920, 1080, 128, 2), "aw1440": (2560, 1440, 256, 3)}[wl]
@@ -737,8 +768,8 @@ def run_workload(args):
         "data": "synthetic (seeded generator)", "config": dict(cfg, l2="flushed before every timed step"),
         "gpu_launches": launches * args.steps, "clocks": clocks,
     }
-    if wl == "mip1080":
-        out_line["dtype"] = "u16 codes / fp32 levels"
+    if wl in ("mip1080", "map3d1080"):
+        out_line["dtype"] = "u16 codes / fp32 levels" if wl == "mip1080" else "u16 codes / fp32 points"
         try:
             peak, src = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"], "of measured"
         except (OSError, KeyError, ValueError):
@@ -747,7 +778,8 @@ def run_workload(args):
         out_line["roofline"] = {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                                 "frac": round(ach / peak, 4), "traffic": None, "peak_source": src,
                                 "algorithmic_bytes": alg_bytes,
-                                "note": "whole call (all launches) timed; 2 B read + 4 B per written level pixel"}
+                                "note": ("whole call (all launches) timed; 2 B read + 4 B per written level pixel"
+                                         if wl == "mip1080" else "2 B read + 16 B written per pixel")}
     if rank == 0:
         out_line["parity_rank0"] = bool(check_fn())
         v, sample = cpu_sample()

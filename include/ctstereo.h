@@ -61,6 +61,7 @@ typedef struct CUstream_st* ct_stream;
 #define CT_PIX_U64 3
 #define CT_PIX_F32 4
 #define CT_PIX_RGBA8 5  /* 4 bytes per pixel: r, g, b, a (visualisation output) */
+#define CT_PIX_F32X4 6  /* 16 bytes per pixel: 4 floats (3D map: x, y, z, valid) */
 
 /* EDisparityId codes used in CT_PIX_U16 maps (DisparityId.h:35-47). */
 #define CT_DISP_FIRST 0x0001
@@ -541,6 +542,46 @@ int ct_confnet_scores(ct_handle* h, float* scores, const uint8_t* samples, int32
  * (synchronises the previous stream). */
 int ct_confnet_infer(ct_handle* h, const ct_image* score, const ct_curves* curves, const ct_image* disp,
                      const ct_image* checked, float threshold, ct_stream stream);
+
+/* ---- disparity to 3D: MapDisparityTo3D::CDriver ---------------------------
+ * Replaces MapDisparityTo3D.h:41-150 / MapDisparityTo3D.cu:75-330. The
+ * reference's stereo camera (Clu::Camera::_CStereoPinhole, CluTec.Core, not in
+ * the reference tree) is replaced by two explicit pinhole cameras: pixel
+ * (x, y) of a camera looks along R ((x - cx) / fx, (y - cy) / fy, 1) from its
+ * centre (camera axes x right, y down, z forward; R = camera-to-world
+ * rotation, row-major). For each pixel of the left disparity map: code c
+ * (U16 as stored; U8 d read as d + 1, 255 as CannotEvaluate; F32 sub-pixel
+ * d >= 0 read as d + 1, negative as CannotEvaluate) is valid if disp_min <=
+ * c <= disp_max; the disparity is c - 1 if valid, else disp_min (as the
+ * reference, MapDisparityTo3D.cu:111-121); the left ray through (x, y) and
+ * the right ray through (x - d, y) are intersected at the midpoint of their
+ * closest points. Output (F32X4): (X, Y, Z, valid) in world coordinates, with
+ * Y and Z negated when cs_rut = 1 (x right, y up, z towards, the reference's
+ * bIsCsRUT); (0, 0, 0, 0) where the rays are parallel. The range of the
+ * valid intersected points is reduced on the device (ct_map3d_range). */
+typedef struct ct_pinhole {
+    float fx, fy;       /* focal lengths in pixels */
+    float cx, cy;       /* principal point in pixels */
+    float rot[9];       /* camera-to-world rotation, row-major */
+    float center[3];    /* projection centre in world coordinates */
+} ct_pinhole;
+
+typedef struct ct_map3d_params {
+    int32_t disp_min, disp_max;  /* valid codes (uDispMin, uDispMax) */
+    int32_t cs_rut;              /* bIsCsRUT */
+    int32_t reserved;            /* 0 */
+    ct_pinhole cam[2];           /* left, right (camStereoPinhole) */
+} ct_map3d_params;
+
+int ct_map3d_create(ct_handle** out);
+/* CDriver::Configure(device, format, parameters); format = the disparity
+ * map's size and type (U8, U16 or F32). */
+int ct_map3d_configure(ct_handle* h, int32_t device, const ct_format* fmt, const ct_map3d_params* p);
+/* CDriver::Process(3D map, disparity map): map3d F32X4, same size. */
+int ct_map3d_process(ct_handle* h, const ct_image* map3d, const ct_image* disp, ct_stream stream);
+/* pixMin / pixMax of the last process call (x, y, z of the valid intersected
+ * points; FLT_MAX / -FLT_MAX when there were none). Synchronises. */
+int ct_map3d_range(ct_handle* h, float* min_xyz, float* max_xyz);
 
 /* ---- pipe-rate probe ---------------------------------------------------------
  * Measures the issue rate of the integer operations the matchers are built

@@ -103,6 +103,7 @@ enum class EDataType : int32_t {
     UInt64 = CT_PIX_U64,
     Single = CT_PIX_F32,
     RGBA8 = CT_PIX_RGBA8,  // 4 bytes: r, g, b, a
+    RGBA_Single = CT_PIX_F32X4,  // 4 floats (3D map)
 };
 
 inline size_t BytesPerPixel(EDataType t) {
@@ -112,6 +113,7 @@ inline size_t BytesPerPixel(EDataType t) {
         case EDataType::UInt64: return 8;
         case EDataType::Single: return 4;
         case EDataType::RGBA8: return 4;
+        case EDataType::RGBA_Single: return 16;
     }
     return 0;
 }
@@ -659,6 +661,57 @@ private:
 };
 
 }  // namespace ColorDisparityImage
+
+/* ---- MapDisparityTo3D (MapDisparityTo3D.h:41-150) ------------------------- */
+namespace MapDisparityTo3D {
+
+/* Replaces Clu::Camera::_CStereoPinhole (CluTec.Core, not in the reference
+ * tree): the left and right pinhole cameras (ct_pinhole). */
+struct CStereoPinhole {
+    ct_pinhole cam[2];
+};
+
+struct SParameter {
+    uint16_t uDispMin = CT_DISP_FIRST, uDispMax = CT_DISP_LAST;
+    bool bIsCsRUT = false;  // x right, y up, z towards (else y down, z away)
+    CStereoPinhole camStereoPinhole{};
+    void Set(uint16_t _uDispMin, uint16_t _uDispMax, bool _bIsCsRUT, const CStereoPinhole& _cam) {
+        uDispMin = _uDispMin;
+        uDispMax = _uDispMax;
+        bIsCsRUT = _bIsCsRUT;
+        camStereoPinhole = _cam;
+    }
+};
+
+class CDriver : public CKernelDriverBase {
+public:
+    CDriver() : CKernelDriverBase("Map Disparity To 3D") {}
+
+    /* xFormat: the disparity map (UInt16 codes, UInt8 or Single sub-pixel). */
+    void Configure(const CDevice& xDevice, const SImageFormat& xFormat, const SParameter& xPars) {
+        ct_map3d_params p{};
+        p.disp_min = xPars.uDispMin;
+        p.disp_max = xPars.uDispMax;
+        p.cs_rut = xPars.bIsCsRUT ? 1 : 0;
+        p.cam[0] = xPars.camStereoPinhole.cam[0];
+        p.cam[1] = xPars.camStereoPinhole.cam[1];
+        const ct_format f = xFormat.ToC();
+        Ensure(ct_map3d_configure(EnsureHandle(ct_map3d_create), xDevice.iDevice, &f, &p),
+               "MapDisparityTo3D::Configure");
+    }
+
+    /* surfMap3D: EDataType::RGBA_Single (x, y, z, valid). */
+    void Process(_CDeviceSurface& surfMap3D, const _CDeviceSurface& surfDisparity) {
+        Ensure(ct_map3d_process(m_pHandle, surfMap3D.C(), surfDisparity.C(), S()), "MapDisparityTo3D::Process");
+    }
+
+    /* pixMin / pixMax of the last Process (synchronises). */
+    void GetRange(float (&afMin)[3], float (&afMax)[3]) {
+        Ensure(ct_map3d_range(m_pHandle, afMin, afMax), "MapDisparityTo3D::GetRange");
+    }
+};
+
+}  // namespace MapDisparityTo3D
 
 /* ---- CDeviceSurfMipMap (DeviceSurfMipMap.h:40-150) ------------------------- */
 

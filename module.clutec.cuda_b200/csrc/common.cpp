@@ -47,6 +47,7 @@ size_t pix_size(int32_t type) {
         case CT_PIX_U64: return 8;
         case CT_PIX_F32: return 4;
         case CT_PIX_RGBA8: return 4;
+        case CT_PIX_F32X4: return 16;
         default: return 0;
     }
 }

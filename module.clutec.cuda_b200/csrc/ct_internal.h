@@ -27,6 +27,7 @@ enum class Kind : int32_t {
     Batch = 7,
     ConfNet = 8,
     Stream = 9,
+    Map3D = 10,
 };
 
 // Sets the thread-local message returned by ct_last_error_string and returns

@@ -24,7 +24,7 @@ LIB_PATH = _PKG / "libctstereo.so"
 # status codes (ctstereo.h)
 CT_OK, CT_EINVAL, CT_ETYPE, CT_EFORMAT, CT_ECUDA, CT_ETIMEOUT, CT_ESTATE, CT_ENOMEM, CT_EINTERNAL = range(9)
 # pixel types
-CT_PIX_U8, CT_PIX_U16, CT_PIX_U64, CT_PIX_F32, CT_PIX_RGBA8 = 1, 2, 3, 4, 5
+CT_PIX_U8, CT_PIX_U16, CT_PIX_U64, CT_PIX_F32, CT_PIX_RGBA8, CT_PIX_F32X4 = 1, 2, 3, 4, 5, 6
 CT_COLOR_ANALYSIS, CT_COLOR_GRAY, CT_COLOR_COLOR, CT_COLOR_DISP_ABS, CT_COLOR_DISP_REL = range(5)
 # EDisparityId codes
 DISP_FIRST, DISP_LAST = 0x0001, 0xFFEF
@@ -74,6 +74,16 @@ class ct_ncc_params(C.Structure):
 class ct_aw_params(C.Structure):
     _fields_ = [("disp_count", C.c_int32), ("left_to_right", C.c_int32), ("reserved0", C.c_int32),
                 ("reserved1", C.c_int32)]
+
+
+class ct_pinhole(C.Structure):
+    _fields_ = [("fx", C.c_float), ("fy", C.c_float), ("cx", C.c_float), ("cy", C.c_float),
+                ("rot", C.c_float * 9), ("center", C.c_float * 3)]
+
+
+class ct_map3d_params(C.Structure):
+    _fields_ = [("disp_min", C.c_int32), ("disp_max", C.c_int32), ("cs_rut", C.c_int32), ("reserved", C.c_int32),
+                ("cam", ct_pinhole * 2)]
 
 
 class ct_crosscheck_params(C.Structure):
@@ -172,6 +182,10 @@ def _declare(L: C.CDLL) -> None:
         "ct_crosscheck_configure": [H, C.c_int32, fmt, P(ct_crosscheck_params)],
         "ct_crosscheck_process": [H, img, img, img, C.c_void_p],
         "ct_crosscheck_range": [H, P(C.c_int32), P(C.c_int32)],
+        "ct_map3d_create": [P(H)],
+        "ct_map3d_configure": [H, C.c_int32, fmt, P(ct_map3d_params)],
+        "ct_map3d_process": [H, img, img, C.c_void_p],
+        "ct_map3d_range": [H, P(C.c_float), P(C.c_float)],
         "ct_batch_create": [P(H)],
         "ct_batch_configure": [H, C.c_int32, P(ct_batch_shape), C.c_int32, C.c_int32],
         "ct_batch_process": [H, P(ct_batch_item), C.c_int32, C.c_void_p],
@@ -437,6 +451,44 @@ class CrossCheckDisparityMaps(_Driver):
         lo, hi = C.c_int32(), C.c_int32()
         check(lib().ct_crosscheck_range(self._h, C.byref(lo), C.byref(hi)))
         return lo.value, hi.value
+
+
+def pinhole(fx, fy, cx, cy, rot=None, center=(0.0, 0.0, 0.0)) -> ct_pinhole:
+    """A pinhole camera: focal lengths and principal point in pixels,
+    camera-to-world rotation (3x3, row-major; identity if None) and the
+    projection centre in world coordinates."""
+    r = [1, 0, 0, 0, 1, 0, 0, 0, 1] if rot is None else [float(v) for row in rot for v in row]
+    return ct_pinhole(fx, fy, cx, cy, (C.c_float * 9)(*r), (C.c_float * 3)(*center))
+
+
+def alloc_map3d(height: int, width: int, device="cuda"):
+    """A (height, width, 4) float32 tensor with a 256-byte aligned row pitch
+    (x, y, z, valid per pixel)."""
+    import torch
+    return alloc_image(height, 4 * width, torch.float32, device).unflatten(1, (width, 4))
+
+
+class MapDisparityTo3D(_Driver):
+    """MapDisparityTo3D::CDriver with explicit pinhole cameras (ct_map3d_*)."""
+    _create = "ct_map3d_create"
+
+    def configure(self, device: int, width: int, height: int, cam_left: ct_pinhole, cam_right: ct_pinhole,
+                  disp_min: int = 1, disp_max: int = 0xFFEF, cs_rut: bool = False, type_: int = CT_PIX_U16):
+        p = ct_map3d_params(disp_min, disp_max, int(cs_rut), 0, (ct_pinhole * 2)(cam_left, cam_right))
+        check(lib().ct_map3d_configure(self._h, device, C.byref(_fmt(width, height, type_)), C.byref(p)))
+
+    def process(self, map3d, disp, stream=None):
+        """map3d: a (H, W, 4) float32 CUDA tensor (alloc_map3d)."""
+        if map3d.dim() != 3 or map3d.shape[2] != 4 or map3d.stride(2) != 1 or map3d.stride(1) != 4:
+            raise CtError(CT_EINVAL, "map3d must be (H, W, 4) float32 with packed pixels")
+        m = ct_image(map3d.data_ptr(), map3d.stride(0) * 4, map3d.shape[1], map3d.shape[0], CT_PIX_F32X4, 0)
+        check(lib().ct_map3d_process(self._h, C.byref(m), _img_ref(disp), _stream(stream)))
+
+    def range(self):
+        """(min xyz, max xyz) of the valid points of the last call (synchronises)."""
+        lo, hi = (C.c_float * 3)(), (C.c_float * 3)()
+        check(lib().ct_map3d_range(self._h, lo, hi))
+        return tuple(lo), tuple(hi)
 
 
 class BatchStereo(_Driver):

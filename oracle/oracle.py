@@ -302,6 +302,47 @@ def disp_mipmaps(codes, level_count=0, init=None):
     return out, rects
 
 
+def map3d(codes, cams, disp_min=1, disp_max=0xFFEF, cs_rut=False):
+    """Disparity map -> 3D points (MapDisparityTo3D.cu:75-240) in float64 with
+    explicit pinhole cameras, the library's replacement for the reference's
+    _CStereoPinhole (not in the reference tree: parity of the camera model is
+    unpinned). cams = [(fx, fy, cx, cy, R 3x3, centre 3)] * 2; codes are U16
+    EDisparityId codes (float codes allowed for sub-pixel maps). Invalid codes
+    use disparity disp_min, as the reference (:111-121). The rays through
+    (x, y) and (x - d, y) meet at the midpoint of their closest points.
+    Returns (H x W x 4 array (x, y, z, valid), (min xyz, max xyz) over the
+    valid intersected points or None, mask of the pixels whose rays meet)."""
+    c = np.asarray(codes, np.float64)
+    H, W = c.shape
+    valid = (c >= disp_min) & (c <= disp_max)
+    d = np.where(valid, c - 1, float(disp_min))
+    yy, xx = np.mgrid[0:H, 0:W].astype(np.float64)
+
+    def ray(cam, x, y):
+        fx, fy, cx, cy, R, _ = cam
+        v = np.stack([(x - cx) / fx, (y - cy) / fy, np.ones_like(x)], -1)
+        return v @ np.asarray(R, np.float64).T
+
+    dl, dr = ray(cams[0], xx, yy), ray(cams[1], xx - d, yy)
+    oL, oR = np.asarray(cams[0][5], np.float64), np.asarray(cams[1][5], np.float64)
+    n = np.cross(dl, dr)
+    nn = (n * n).sum(-1)
+    hit = nn > 1e-14 * (dl * dl).sum(-1) * (dr * dr).sum(-1)
+    b = oR - oL
+    with np.errstate(divide="ignore", invalid="ignore"):
+        s = (np.cross(b, dr) * n).sum(-1) / nn
+        t = (np.cross(b, dl) * n).sum(-1) / nn
+    P = 0.5 * ((oL + s[..., None] * dl) + (oR + t[..., None] * dr))
+    if cs_rut:
+        P = P * np.array([1.0, -1.0, -1.0])
+    out = np.zeros((H, W, 4))
+    out[..., :3] = np.where(hit[..., None], P, 0.0)
+    out[..., 3] = np.where(hit & valid, 1.0, 0.0)
+    good = hit & valid
+    rng = (P[good].min(0), P[good].max(0)) if good.any() else None
+    return out, rng, hit
+
+
 def crosscheck(base, other, tol=1, left_to_right=True):
     """-> (out int16 with -2 = inconsistent, (min, max))"""
     base = np.ascontiguousarray(base, np.int16)

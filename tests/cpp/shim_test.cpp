@@ -221,6 +221,26 @@ static int RunGpu(const char* weights) {
               want_gray);
         CHECK(cv[0] == cp.pixCannotEvaluate, "colour: border %08x, want %08x", cv[0], cp.pixCannotEvaluate);
 
+        // 3D points of the map with a rectified pair (f = 500 px, baseline 0.2):
+        // interior depth f B / K
+        MapDisparityTo3D::CStereoPinhole cams{};
+        for (int c = 0; c < 2; ++c) {
+            cams.cam[c] = ct_pinhole{500.f, 500.f, W / 2.f, H / 2.f, {1, 0, 0, 0, 1, 0, 0, 0, 1}, {0.2f * c, 0, 0}};
+        }
+        MapDisparityTo3D::SParameter mp;
+        mp.Set(uint16_t(EDisparityId::First), uint16_t(EDisparityId::Last), false, cams);
+        MapDisparityTo3D::CDriver m3;
+        m3.Configure(dev, f16, mp);
+        CDeviceSurface pts(SImageFormat(W, H, EDataType::RGBA_Single));
+        ProcessKernel(m3, pts, disp);
+        auto pv = pts.CopyInto<float4>();
+        const float4 pc = pv[size_t(60) * W + 100];
+        float lo[3], hi[3];
+        m3.GetRange(lo, hi);
+        const float zw = 500.f * 0.2f / float(K);
+        CHECK(std::fabs(pc.z - zw) < 1e-4f * zw && pc.w == 1.f && lo[2] <= pc.z && hi[2] >= pc.z,
+              "3D: z %g (want %g), valid %g, z range %g .. %g", pc.z, zw, pc.w, lo[2], hi[2]);
+
         // mip-maps of the map: level 1 interior = 0.5 * code (K + 1), level 0
         // border (CannotEvaluate) = 0
         CDeviceSurfMipMap mip(f16);
