@@ -9,9 +9,10 @@
 // s = ((oR - oL) x dR) . n / |n|^2, t = ((oR - oL) x dL) . n / |n|^2 (no
 // 1 - cos^2 cancellation for the nearly parallel rays of small
 // disparities); rays with |n|^2 <= 1e-14 |dL|^2 |dR|^2 count as parallel.
-// The range of the valid points is reduced per warp (__reduce_min_sync on
-// order-preserving integer keys) with one atomic per warp and component,
-// instead of the reference's lock-guarded per-thread table
+// The range of the valid points is reduced per block (__reduce_min_sync on
+// order-preserving integer keys, then shared memory) with at most one
+// atomic per block and component, issued only when it can lower the stored
+// key, instead of the reference's lock-guarded per-thread table
 // (MapDisparityTo3D.cu:200-236).
 #include "ct_internal.h"
 
@@ -105,11 +106,22 @@ __global__ void __launch_bounds__(256) map3d_kernel(float4* out, size_t opitch, 
     const uint32_t k[6] = {good ? fkey(P.x) : 0xFFFFFFFFu,  good ? fkey(P.y) : 0xFFFFFFFFu,
                            good ? fkey(P.z) : 0xFFFFFFFFu,  good ? fkey(-P.x) : 0xFFFFFFFFu,
                            good ? fkey(-P.y) : 0xFFFFFFFFu, good ? fkey(-P.z) : 0xFFFFFFFFu};
-    const unsigned any = __ballot_sync(0xffffffffu, good);
+    // warp minima -> block minima -> one atomic per component, and only when
+    // the stored key is larger (it only decreases, so a stale read can only
+    // cause an unneeded atomic, never a missed one)
+    __shared__ uint32_t red[256 / 32][6];
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
         const uint32_t m = __reduce_min_sync(0xffffffffu, k[i]);
-        if (any && (threadIdx.x & 31) == 0) atomicMin(&range[i], m);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][i] = m;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        uint32_t m = red[0][threadIdx.x];
+#pragma unroll
+        for (int w = 1; w < 256 / 32; ++w) m = min(m, red[w][threadIdx.x]);
+        if (m != 0xFFFFFFFFu && m < *reinterpret_cast<volatile uint32_t*>(&range[threadIdx.x]))
+            atomicMin(&range[threadIdx.x], m);
     }
 }
 
