@@ -16,6 +16,7 @@
 // (MapDisparityTo3D.cu:200-236).
 #include "ct_internal.h"
 
+#include <algorithm>
 #include <cfloat>
 
 namespace ct {
@@ -72,11 +73,11 @@ __device__ __forceinline__ float code_of(const T* row, int x) {
 template <typename T>
 __global__ void __launch_bounds__(256) map3d_kernel(float4* out, size_t opitch, const T* disp, size_t dpitch, int W,
                                                      int H, Params p, uint32_t* range) {
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    bool good = false;
-    float3 P = make_float3(0.f, 0.f, 0.f);
-    if (x < W) {
+    // blocks stride over the rows (grid y is a few blocks per SM), so the
+    // range is reduced once per block
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t k[6] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu};
+    for (int y = blockIdx.y; y < H && x < W; y += gridDim.y) {
         const T* drow = reinterpret_cast<const T*>(reinterpret_cast<const char*>(disp) + (size_t)y * dpitch);
         const float code = code_of(drow, x);
         const bool valid = code >= float(p.disp_min) && code <= float(p.disp_max);
@@ -93,19 +94,23 @@ __global__ void __launch_bounds__(256) map3d_kernel(float4* out, size_t opitch, 
                                          p.cam[1].c[2] - p.cam[0].c[2]);
             const float s = __fdiv_rn(dot(cross(b, dr), n), nn);
             const float t = __fdiv_rn(dot(cross(b, dl), n), nn);
-            P = make_float3(0.5f * ((p.cam[0].c[0] + s * dl.x) + (p.cam[1].c[0] + t * dr.x)),
-                            0.5f * ((p.cam[0].c[1] + s * dl.y) + (p.cam[1].c[1] + t * dr.y)),
-                            0.5f * ((p.cam[0].c[2] + s * dl.z) + (p.cam[1].c[2] + t * dr.z)));
+            float3 P = make_float3(0.5f * ((p.cam[0].c[0] + s * dl.x) + (p.cam[1].c[0] + t * dr.x)),
+                                   0.5f * ((p.cam[0].c[1] + s * dl.y) + (p.cam[1].c[1] + t * dr.y)),
+                                   0.5f * ((p.cam[0].c[2] + s * dl.z) + (p.cam[1].c[2] + t * dr.z)));
             P.y *= p.sy;
             P.z *= p.sz;
             o = make_float4(P.x, P.y, P.z, valid ? 1.f : 0.f);
+            if (valid) {
+                k[0] = min(k[0], fkey(P.x));
+                k[1] = min(k[1], fkey(P.y));
+                k[2] = min(k[2], fkey(P.z));
+                k[3] = min(k[3], fkey(-P.x));
+                k[4] = min(k[4], fkey(-P.y));
+                k[5] = min(k[5], fkey(-P.z));
+            }
         }
         reinterpret_cast<float4*>(reinterpret_cast<char*>(out) + (size_t)y * opitch)[x] = o;
-        good = valid && hit;
     }
-    const uint32_t k[6] = {good ? fkey(P.x) : 0xFFFFFFFFu,  good ? fkey(P.y) : 0xFFFFFFFFu,
-                           good ? fkey(P.z) : 0xFFFFFFFFu,  good ? fkey(-P.x) : 0xFFFFFFFFu,
-                           good ? fkey(-P.y) : 0xFFFFFFFFu, good ? fkey(-P.z) : 0xFFFFFFFFu};
     // warp minima -> block minima -> one atomic per component, and only when
     // the stored key is larger (it only decreases, so a stale read can only
     // cause an unneeded atomic, never a missed one)
@@ -207,7 +212,9 @@ int ct_map3d_process(ct_handle* hh, const ct_image* map3d, const ct_image* disp,
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     h->last_stream = s;
     CT_CUDA_TRY(cudaMemsetAsync(h->range, 0xFF, 8 * sizeof(uint32_t), s));
-    const dim3 grid((disp->width + 255) / 256, disp->height);
+    const int gx = (disp->width + 255) / 256;
+    const int gy = std::max(1, std::min(disp->height, 8 * sm_count(h->device) / gx));
+    const dim3 grid(gx, gy);
     float4* out = static_cast<float4*>(map3d->ptr);
     if (disp->type == CT_PIX_U8)
         m3d::map3d_kernel<uint8_t><<<grid, 256, 0, s>>>(out, map3d->pitch_bytes, static_cast<const uint8_t*>(disp->ptr),
