@@ -91,6 +91,20 @@ def test_capi_layout_queries(ct, oracle):
             ct.disp_mipmap_level(W, H, n + 1)
 
 
+def test_capi_layout_sweep(ct, oracle):
+    # the library's packed layout equals the reference's formulas for random sizes
+    r = np.random.default_rng(12)
+    for W, H in zip(r.integers(1, 9000, 300), r.integers(1, 9000, 300)):
+        W, H = int(W), int(H)
+        opw, rects = oracle.mipmap_layout(W, H)
+        pw, n = ct.disp_mipmap_format(W, H)
+        assert (pw, n) == (opw, len(rects) - 1)
+        for k in (0, n // 2, n):
+            x, y, w, h = ct.disp_mipmap_level(W, H, k)
+            assert (x, y, w, h) == rects[k]
+            assert x % 4 == 0 and y + h <= H and x + w <= pw  # 16-byte aligned, inside the image
+
+
 def test_capi_argument_checks(ct):
     L = ct.lib()
     fake = 1 << 20  # never dereferenced: every check fails before a device call
