@@ -124,6 +124,26 @@ static int RunCpu() {
         CHECK(ThrownCode([&] { d.Configure(dev, f, p, 1, EDataType::Single); }) == CT_ETYPE, "F32 stream maps");
         CHECK(ThrownCode([&] { d.Submit(nullptr, 0, nullptr, 0, nullptr, 0); }) == CT_ESTATE, "unconfigured stream");
     }
+    {
+        // disparity to 3D: parameter checks before any device call
+        MapDisparityTo3D::CStereoPinhole cams{};
+        for (int c = 0; c < 2; ++c) cams.cam[c] = ct_pinhole{500.f, 500.f, 160.f, 60.f, {1, 0, 0, 0, 1, 0, 0, 0, 1}, {0.1f * c, 0, 0}};
+        MapDisparityTo3D::SParameter mp;
+        mp.Set(uint16_t(EDisparityId::First), uint16_t(EDisparityId::Last), true, cams);
+        MapDisparityTo3D::CDriver m3;
+        CHECK(ThrownCode([&] { m3.Configure(dev, SImageFormat(320, 120, EDataType::RGBA8), mp); }) == CT_ETYPE,
+              "3D: RGBA8 disparity maps must be rejected");
+        mp.camStereoPinhole.cam[1].fx = 0.f;
+        CHECK(ThrownCode([&] { m3.Configure(dev, SImageFormat(320, 120, EDataType::UInt16), mp); }) == CT_EINVAL,
+              "3D: a zero focal length must be rejected");
+        mp.Set(90, 20, true, cams);
+        CHECK(ThrownCode([&] { m3.Configure(dev, SImageFormat(320, 120, EDataType::UInt16), mp); }) == CT_EINVAL,
+              "3D: disp_min above disp_max must be rejected");
+        // mip-maps: the packed layout needs no device
+        int32_t pw = 0, levels = 0;
+        Ensure(ct_disp_mipmap_format(320, 120, &pw, &levels), "format");
+        CHECK(pw == 320 + 159 && levels == 5, "mip-map format %d / %d", pw, levels);
+    }
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
     if (n == 0) {
