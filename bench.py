@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--profile", default=None, choices=["census_match", "confnet_infer", "pipelines"],
                     help="for ncu captures on the 1080p D=128 pair, then exit: census_match or confnet_infer = that "
                          "kernel twice; pipelines = the plain L-R pipeline 3x, then the learned one 3x")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="default run: measure the headline only, without the other configurations")
     return ap.parse_args()
 
 
@@ -119,14 +121,35 @@ def units_per_step():
     return 2 * W_ * H_ * D_
 
 
+def census_config():
+    """The headline workload, identical in both arms."""
+    return {"workload": "census9x7_5x5_lrcheck_1920x1080_d128", "width": W_, "height": H_, "D": D_,
+            "census": "9x7", "agg": "5x5", "crosscheck_tol": 1, "seed": SEED, "generator": "kind 2 (slanted planes)",
+            "l2": "GPU L2 flushed before every timed step (256 MiB memset); the CPU arm has no GPU L2"}
+
+
+_ORACLE = None
+
+
+def cpu_oracle():
+    """The CPU restatement (oracle/), built on this host with -march=native
+    for the timed CPU legs; -> (module, march actually used)."""
+    global _ORACLE
+    if _ORACLE is None:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle  # the CPU restatement: CPU baseline, reference arm and parity checks only
+        march = oracle.use_native()
+        oracle.lib()
+        _ORACLE = (oracle, march)
+    return _ORACLE
+
+
 # ---------------------------------------------------------------------------
 # CPU implementation (oracle port) — the cpu_baseline leg and --impl reference
 # ---------------------------------------------------------------------------
 
 def cpu_pipeline_time(L, R, reps: int) -> tuple[float, int]:
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle  # the CPU restatement; timed here as the baseline only
-    oracle.lib()
+    oracle, _ = cpu_oracle()
     t0 = time.perf_counter()
     for _ in range(reps):
         dl, _ = oracle.match_census(L, R, D_, 2, True)
@@ -152,11 +175,11 @@ def run_reference(args):
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u8/u64 integer", "data": "synthetic (seeded generator)",
-        "config": {"workload": "census9x7_5x5_lrcheck_1920x1080_d128", "width": W_, "height": H_, "D": D_,
-                   "seed": SEED, "l2": "n/a (CPU)"},
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8 pixels / u64 census / int costs",
+        "data": "synthetic (seeded generator)", "config": census_config(),
         "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": "one full 1920x1080 D=128 pipeline per step (LR + RL + check)"},
+                         "sample": "one full 1920x1080 D=128 pipeline per step (LR + RL + check)",
+                         "build": f"-O3 -march={cpu_oracle()[1]} -fopenmp"},
         "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -273,20 +296,56 @@ def confnet_compare(ct, dev, stream, m, dL, dR, hL, hR, flush, steps, eval_pairs
         return sum(a.elapsed_time(b) for a, b in ev) / steps
 
     res = {"plain_ms": timed(plain), "learned_ms": timed(learned),
-           "plain_e2e_ms": timed(plain, ck_plain), "learned_e2e_ms": timed(learned, ck_learned)}
+           "plain_e2e_ms": timed(plain, ck_plain), "learned_e2e_ms": timed(learned, ck_learned),
+           "infer_ms": timed(lambda: net.infer(None, cv, disp, checked=ck_learned, threshold=0.5, stream=stream))}
     if m.device_status() != 0 or net.device_status() != 0:
         raise RuntimeError("device status set in the confidence-net comparison")
-    auc = T.evaluate({"net": net}, device_index, eval_pairs, W_, H_)
     res = {k: round(v, 4) for k, v in res.items()}
+    # quality on held-out pairs of the training generator (kind 1) and of the
+    # headline's slanted-plane generator (kind 2)
+    evals = {}
+    for kind in (1, 2):
+        a = T.evaluate({"net": net}, device_index, eval_pairs, W_, H_, kind=kind)
+        evals[f"kind{kind}"] = {
+            "auc_net": round(a["net"], 4), "auc_lr_check": round(a["lr_check"], 4),
+            "lr_check_tpr": round(a["lr_check_tpr"], 4), "lr_check_fpr": round(a["lr_check_fpr"], 5),
+            "net_tpr_at_0.5": round(a["net_tpr"], 4), "net_fpr_at_0.5": round(a["net_fpr"], 5),
+            "net_tpr_at_lr_fpr": round(a["net_tpr_at_lr_fpr"], 4),
+            "net_fpr_at_lr_fpr": round(a["net_fpr_at_lr_fpr"], 5),
+            "net_threshold_at_lr_fpr": round(a["net_threshold_at_lr_fpr"], 4),
+            "invalid_fraction": round(a["invalid_fraction"], 4), "eval_pairs": a["pairs"],
+            "eval_pixels": a["pixels"]}
+    auc = evals["kind1"]
+    macs = 1120 + 9216 + 2048 + 2048 + 64  # per pixel: conv1, conv2, conv3, fc1, fc2
+    flops = 2.0 * macs * W_ * H_
+    try:
+        peak, src = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["bf16_tflops"], "of measured (burst)"
+    except (OSError, KeyError, ValueError):
+        peak, src = 1590.0, "of fallback"
+    ach = flops / (res["infer_ms"] * 1e-3) / 1e12
     res.update({"speedup": round(res["plain_ms"] / res["learned_ms"], 3),
                 "speedup_e2e": round(res["plain_e2e_ms"] / res["learned_e2e_ms"], 3),
-                "auc_net": round(auc["net"], 4), "auc_lr_check": round(auc["lr_check"], 4),
-                "lr_check_tpr": round(auc["lr_check_tpr"], 4), "lr_check_fpr": round(auc["lr_check_fpr"], 5),
-                "invalid_fraction": round(auc["invalid_fraction"], 4), "eval_pairs": auc["pairs"],
-                "eval_pixels": auc["pixels"], "threshold": 0.5,
+                "auc_net": auc["auc_net"], "auc_lr_check": auc["auc_lr_check"],
+                "lr_check_tpr": auc["lr_check_tpr"], "lr_check_fpr": auc["lr_check_fpr"],
+                "invalid_fraction": auc["invalid_fraction"], "eval_pairs": auc["eval_pairs"],
+                "eval_pixels": auc["eval_pixels"], "threshold": 0.5, "eval": evals,
+                "eval_200_pairs": "module.clutec.cuda_b200/confnet_census128.json (200 held-out kind-1 pairs)",
+                "infer_roofline": {"bound": "tensor", "achieved": round(ach, 2), "peak": peak, "unit": "TFLOP/s",
+                                   "frac": round(ach / peak, 4), "traffic": None, "peak_source": src,
+                                   "algorithmic_per_unit": f"{macs} MAC per pixel (bf16 x bf16, fp32 accumulate)"},
                 "weights": "module.clutec.cuda_b200/confnet_census128.f32 (2000 seeded training pairs)",
                 "launches_learned": 3, "launches_plain": 4})
     return res
+
+
+def confnet_entry(c):
+    """The learned-confidence pipeline as an entry of the default run's configs."""
+    return {"metric": "frames/s census 1080p D=128 + learned confidence (replaces the R->L pass and the L-R check)",
+            "value": round(1e3 / c["learned_ms"], 1), "unit": "frames/s", "ms_per_step": c["learned_ms"],
+            "plain_lr_pipeline_ms": c["plain_ms"], "speedup": c["speedup"], "speedup_e2e": c["speedup_e2e"],
+            "roofline": c["infer_roofline"], "eval": c["eval"],
+            "config": {"workload": "confnet_1920x1080_d128", "width": W_, "height": H_, "D": D_},
+            "gpu_launches": None}
 
 
 def run_ours(args):
@@ -408,21 +467,24 @@ def run_ours(args):
             raise RuntimeError("device status set in the streamed run")
         stream_ok = bool(torch.equal(souts[(args.steps - 1) % 3], hOut))
         conf = confnet_compare(ct, dev, stream, m, dL, dR, hL, hR, flush, args.steps,
-                               args.eval_pairs or 4, local) if rank == 0 else None
+                               args.eval_pairs or 12, local) if rank == 0 else None
     clocks = clk.summary()
 
     status = m.device_status()
     if status != 0:
         raise RuntimeError(f"device status {status} after the timed runs")
 
-    # correctness spot check of the last output against the oracle (rank 0)
+    # correctness of the timed step's three maps against the oracle (rank 0)
     parity = None
     if rank == 0:
         import numpy as np
-        sys.path.insert(0, str(ROOT / "oracle"))
-        import oracle
+        oracle, _ = cpu_oracle()
         want_l, _ = oracle.match_census(L, R, D_, 2, True)
-        parity = bool(np.array_equal(lr.cpu().numpy(), oracle.to_u8(want_l)))
+        want_r, _ = oracle.match_census(L, R, D_, 2, False)
+        want_c, _ = oracle.crosscheck(want_l, want_r, 1, True)
+        parity = {name: bool(np.array_equal(got.cpu().numpy(), oracle.to_u8(np.where(want == -2, -1, want))))
+                  for name, got, want in (("lr", lr, want_l), ("rl", rl, want_r), ("checked", ck, want_c))}
+        parity["all"] = all(parity.values())
 
     ms = total_ms / args.steps
     value = world * units_per_step() / (ms * 1e-3) / 1e6
@@ -441,10 +503,7 @@ def run_ours(args):
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8 pixels / u64 census / int costs", "data": "synthetic (seeded generator)",
-        "config": {"workload": "census9x7_5x5_lrcheck_1920x1080_d128", "width": W_, "height": H_, "D": D_,
-                   "agg": "5x5", "census": "9x7", "crosscheck_tol": 1, "seed": SEED,
-                   "l2": "flushed before every timed step (256 MiB memset)", "parallelism": f"replicas x{world}",
-                   "launch_shape": tuning},
+        "config": census_config(), "parallelism": f"replicas x{world}", "launch_shape": tuning,
         "e2e": {"value": round(e2e_stream, 1), "unit": UNIT, "ms_per_step": round(stream_ms, 4),
                 "h2d_bytes_per_step": 2 * W_ * H_, "d2h_bytes_per_step": W_ * H_,
                 "api": "ct_census_stream_submit per frame (pinned host images in, checked map out), "
@@ -473,7 +532,21 @@ def run_ours(args):
     if rank == 0:
         cpu_ms, cores = cpu_pipeline_time(L, R, 3)
         out["cpu_baseline"] = {"value": round(units_per_step() / cpu_ms / 1e6, 1), "unit": UNIT, "cores": cores,
-                               "kind": "port", "sample": "3 full pipelines (1920x1080, D=128, LR+RL+check)"}
+                               "kind": "port", "sample": "3 full pipelines (1920x1080, D=128, LR+RL+check)",
+                               "build": f"-O3 -march={cpu_oracle()[1]} -fopenmp"}
+    if world == 1 and not args.no_configs:
+        # the other configurations, one entry each (1 GPU only: at N > 1 the
+        # headline alone is measured)
+        out["configs"] = {}
+        for wl in CONFIG_WORKLOADS:
+            line = workload_line(wl, args, ct, dev, stream, flush_buf, world, rank, local, rates)
+            out["configs"][wl] = {k: line.get(k) for k in ("metric", "value", "unit", "ms_per_step", "config",
+                                                           "roofline", "cpu_baseline", "parity_rank0", "clocks",
+                                                           "gpu_launches")}
+        if conf is not None:
+            out["configs"]["confnet1080"] = confnet_entry(conf)
+        out["gpu_launches_configs"] = sum(v.get("gpu_launches") or 0 for v in out["configs"].values())
+    if rank == 0:
         print(json.dumps(out), flush=True)
     close_ranks(world)
     return 0
@@ -543,6 +616,8 @@ def run_profile(args):
 # Other configurations (--workload): one JSON line each, same timing rules
 # ---------------------------------------------------------------------------
 
+# the other configurations measured by the default run (configs entry of its line)
+CONFIG_WORKLOADS = ["sad640", "ncc1080", "aw1440", "batch64"]
 BATCH_SIZES = [(320, 240), (640, 480), (1280, 720), (1920, 1080)]
 BATCH_DISPS = [32, 64, 128, 256]
 
@@ -554,20 +629,41 @@ def batch_shapes(n=64, seed=4):
     return [(*BATCH_SIZES[int(r.integers(4))], BATCH_DISPS[int(r.integers(4))]) for _ in range(n)]
 
 
-def run_workload(args):
+# Algorithmic cost per pixel x disparity of each matcher (the roofline's
+# numerator) and the pipe that bounds it.
+#   sad640 : |a - b| (2 INT) + 4 box add/sub + compare/select (2) = 8 INT
+#   aw1440 : |a - b| (2) + 7x7 running box (4) + 5-window min and add (5)
+#            + compare/select (2) = 13 INT
+#   ncc1080: product + 4 box add/sub (5 INT) + normalisation and argmax
+#            (~10 FP32/INT) = 15 lane operations at the issue rate
+#            (128 per SM per clock: 4 schedulers x 32 lanes)
+#   batch64: as the census headline, 2 POPC (64-bit Hamming)
+ROOF = {"sad640": ("int", 8, "iadd3_per_clk_sm"), "aw1440": ("int", 13, "iadd3_per_clk_sm"),
+        "ncc1080": ("issue", 15, None), "batch64": ("popc", 2, "popc_per_clk_sm")}
+
+
+def pipe_roofline(kind, ops_per_unit, rate_key, units_per_s, rates, sm_mhz):
+    """Integer / issue roofline of a matcher: achieved operations per second
+    (units/s x algorithmic ops per unit) against the pipe peak measured on
+    this GPU by ct_probe_pipe_rates (per SM per clock x SMs x SM clock)."""
+    clock_hz = (sm_mhz or rates["sm_clock_mhz"]) * 1e6
+    per_clk = 128.0 if rate_key is None else rates[rate_key]
+    peak = per_clk * rates["sm_count"] * clock_hz
+    ach = units_per_s * ops_per_unit
+    return {"bound": kind, "achieved": round(ach / 1e12, 4), "peak": round(peak / 1e12, 4),
+            "unit": {"int": "Tintop/s", "popc": "Tpopc/s", "issue": "Tlaneop/s"}[kind],
+            "frac": round(ach / peak, 4), "traffic": None, "algorithmic_per_unit": f"{ops_per_unit} {kind} ops",
+            "peak_source": ("ct_probe_pipe_rates measured in this run" if rate_key else
+                            "issue limit 128 lane-ops/clk/SM") + " x SMs x median SM clock"}
+
+
+def workload_line(wl, args, ct, dev, stream, flush_buf, world, rank, local, rates=None):
+    """Measures one configuration (--workload, or an entry of the default
+    run's `configs`) with the bench's timing rules; returns the JSON line on
+    rank 0 (None elsewhere)."""
     import numpy as np
     import torch
-    import ctstereo as ct
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle  # CPU baseline leg only
-
-    rank, world, local = dist_info()
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    init_ranks(world, dev)
-    stream = torch.cuda.current_stream(dev)
-    flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    wl = args.workload
+    oracle, march = cpu_oracle()  # CPU baseline leg and post-timing parity check only
     unit = UNIT
 
     def up(a):
@@ -591,11 +687,11 @@ def run_workload(args):
         metric = "Mpix*disp/s batched census + L-R check, 64 mixed pairs, one graph"
         cfg = {"workload": "batch64_census_lrcheck_mixed", "pairs": 64, "sizes": BATCH_SIZES, "disps": BATCH_DISPS,
                "strip_heights": sorted(set(ths))}
-        check_fn = lambda: all(np.array_equal(  # each pair vs the oracle, first 4 pairs
+        check_fn = lambda: all(np.array_equal(  # every pair vs the oracle
             pairs[i][2].cpu().numpy().view(np.uint16),
             oracle.to_u16(oracle.crosscheck(oracle.match_census(host[i][0], host[i][1], host[i][2])[0],
                                             oracle.match_census(host[i][0], host[i][1], host[i][2], 2, False)[0],
-                                            1, True)[0])) for i in range(4))
+                                            1, True)[0])) for i in range(len(host)))
 
         def cpu_sample():
             L, R, D = host[0]
@@ -780,12 +876,33 @@ def run_workload(args):
                                 "algorithmic_bytes": alg_bytes,
                                 "note": ("whole call (all launches) timed; 2 B read + 4 B per written level pixel"
                                          if wl == "mip1080" else "2 B read + 16 B written per pixel")}
-    if rank == 0:
-        out_line["parity_rank0"] = bool(check_fn())
-        v, sample = cpu_sample()
-        out_line["cpu_baseline"] = {"value": round(v, 1), "unit": unit, "cores": oracle.num_threads(),
-                                    "kind": "port", "sample": sample}
-        print(json.dumps(out_line), flush=True)
+    elif wl in ROOF:
+        if rates is None:
+            rates = ct.probe_pipe_rates(local)
+        kind, ops, key = ROOF[wl]
+        out_line["roofline"] = pipe_roofline(kind, ops, key, units / (ms * 1e-3), rates, clocks.get("sm_mhz"))
+        out_line["roofline"]["note"] = "whole call timed (all its launches)"
+    if rank != 0:
+        return None
+    out_line["parity_rank0"] = bool(check_fn())
+    v, sample = cpu_sample()
+    out_line["cpu_baseline"] = {"value": round(v, 1), "unit": unit, "cores": oracle.num_threads(),
+                                "kind": "port", "sample": sample, "build": f"-O3 -march={march} -fopenmp"}
+    return out_line
+
+
+def run_workload(args):
+    import torch
+    import ctstereo as ct
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    init_ranks(world, dev)
+    stream = torch.cuda.current_stream(dev)
+    flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    line = workload_line(args.workload, args, ct, dev, stream, flush_buf, world, rank, local)
+    if line is not None:
+        print(json.dumps(line), flush=True)
     close_ranks(world)
     return 0
 

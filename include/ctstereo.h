@@ -223,13 +223,19 @@ int ct_bm_census_set_tuning(ct_handle* h, int32_t strip_height, int32_t disp_per
  * pixels with rows rounded up to a multiple of 4 (1920 x 1080 fits; larger
  * -> CT_EINVAL).
  * Runs on the current device. Its first call on a device looks up the array
- * addresses: make it before any stream capture. Calls share the array, so
- * calls that overlap on the GPU race; serialise them. device_status
- * (nullable, caller-owned device int32) receives CT_ETIMEOUT if a bounded
- * wait gives up. */
+ * addresses: make it before any stream capture (the lookup is repeated when
+ * the device's current context handle changes, e.g. after cudaDeviceReset).
+ * Calls share the array, so calls that overlap on the GPU race; serialise
+ * them. device_status (nullable, caller-owned device int32) receives
+ * CT_ETIMEOUT if a bounded wait gives up; with NULL the code goes to a static
+ * word that ct_bm_census_static_status reads. */
 int ct_bm_census_process_static(const ct_image* disp, const ct_image* left, const ct_image* right,
                                 int32_t disp_count, int32_t left_to_right, int32_t* device_status,
                                 ct_stream stream);
+/* Status word of the ct_bm_census_process_static calls on the current device
+ * that passed no device_status: 0 = fine, else a CT_E* code. Synchronises the
+ * device, then clears the word. Allocates nothing. */
+int ct_bm_census_static_status(int32_t* status);
 
 /* ---- SAD block matcher: BlockMatcherSAD1::CDriver ------------------------
  * Replaces BlockMatcherSAD1.h:42-127 / BlockMatcherSAD1.cu:493-596 for the
@@ -469,21 +475,6 @@ int ct_disp_mipmap_level(int32_t width, int32_t height, int32_t level, int32_t* 
  * Asynchronous; no scratch memory. */
 int ct_disp_mipmaps(const ct_image* mipmap, const ct_image* disp, int32_t level_count, ct_stream stream);
 
-/* ---- synthetic stereo pairs -----------------------------------------------
- * Seeded generator of rectified stereo pairs with ground truth (host memory).
- *   kind 1: fractal value noise (4 octaves) left image; disparity = 4
- *           background + 8 fronto-parallel rectangles in [0, dmax]; right =
- *           forward warp with occlusion handling + N(0, 2^2); disoccluded
- *           right pixels get fresh noise.
- *   kind 2: 24 slanted planes (|grad d| <= 0.1 px/px, rounded), noise 3.
- *   kind 3: 6 smooth Gaussians scaled to [0, dmax] + 12 sharp rectangles,
- *           right-image gain in [0.9, 1.1], noise 2.
- * gt: int16 left-view ground truth disparity; occ: 1 where the left pixel is
- * occluded in the right view (or maps outside it). Any output may be NULL.
- */
-int ct_synth_pair(int32_t kind, uint64_t seed, int32_t width, int32_t height, int32_t dmax,
-                  uint8_t* left, uint8_t* right, int16_t* gt, uint8_t* occ);
-
 /* ---- learned confidence ------------------------------------------------------
  * A small network that scores, per pixel, how likely the census matcher's
  * winner-take-all disparity is correct, from the pixel's cost curve
@@ -598,6 +589,16 @@ typedef struct ct_pipe_rates {
     int32_t reserved;
 } ct_pipe_rates;
 int ct_probe_pipe_rates(int32_t device, ct_pipe_rates* out);
+
+/* Self-test of the failure reporting of bounded device waits (the reference
+ * has none: its kernels do not wait on each other). Launches one CTA on the
+ * handle's device that waits on an mbarrier nothing ever arrives at, with a
+ * limit of poll_limit polls (1 .. 1048576), through the same bounded wait the
+ * TMA consumers use. The wait gives up and writes CT_ETIMEOUT into the
+ * handle's device status word, which ct_handle_device_status then returns,
+ * as it would for a tile that never arrived; the kernel returns normally and
+ * the context stays usable. The handle must be configured. */
+int ct_handle_test_wait_timeout(ct_handle* h, uint32_t poll_limit, ct_stream stream);
 
 #ifdef __cplusplus
 }

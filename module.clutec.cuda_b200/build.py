@@ -2,7 +2,9 @@
 
 Every .cu / .cpp file under csrc/ is compiled to an object file in
 _build/ (in parallel) and linked into module.clutec.cuda_b200/libctstereo.so,
-which is what ctstereo.py loads. Run: python module.clutec.cuda_b200/build.py
+which is what ctstereo.py loads. The seeded stereo-pair generator (gen/) is a
+separate host-only library, libctsynth.so, built with g++.
+Run: python module.clutec.cuda_b200/build.py
 """
 from __future__ import annotations
 
@@ -17,6 +19,8 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libctstereo.so"
+SYNTH_SRC = PKG / "gen" / "synth.cpp"
+SYNTH_LIB = PKG / "libctsynth.so"
 INCLUDE = PKG.parent / "include"
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -56,7 +60,24 @@ def _compile(src: Path, verbose_ptxas: bool) -> Path:
     return obj
 
 
+def build_synth() -> Path:
+    """libctsynth.so (the generator) from gen/synth.cpp, rebuilt when older
+    than its sources."""
+    deps = [SYNTH_SRC, INCLUDE / "ctsynth.h", INCLUDE / "ctstereo.h"]
+    if SYNTH_LIB.exists() and SYNTH_LIB.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
+        return SYNTH_LIB
+    cxx = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
+    tmp = SYNTH_LIB.with_suffix(".so.tmp")
+    r = subprocess.run([cxx, "-O3", "-std=c++17", "-fPIC", "-fopenmp", "-shared", "-I", str(INCLUDE),
+                        str(SYNTH_SRC), "-o", str(tmp)], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"g++ failed for {SYNTH_SRC.name}:\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, SYNTH_LIB)
+    return SYNTH_LIB
+
+
 def build(verbose_ptxas: bool = False) -> Path:
+    build_synth()
     BUILD.mkdir(exist_ok=True)
     srcs = _sources()
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:

@@ -58,14 +58,14 @@ def save_weights(params: np.ndarray, path=WEIGHTS) -> None:
     np.asarray(params, dtype="<f4").tofile(path)
 
 
-def _pairs(seeds, W, H):
+def _pairs(seeds, W, H, kind=KIND):
     """Seeded pairs, generated one ahead on a worker thread."""
     with ThreadPoolExecutor(1) as ex:
-        fut = ex.submit(ct.synth_pair, KIND, int(seeds[0]), W, H, D - 1)
+        fut = ex.submit(ct.synth_pair, kind, int(seeds[0]), W, H, D - 1)
         for k in range(len(seeds)):
             cur = fut.result()
             if k + 1 < len(seeds):
-                fut = ex.submit(ct.synth_pair, KIND, int(seeds[k + 1]), W, H, D - 1)
+                fut = ex.submit(ct.synth_pair, kind, int(seeds[k + 1]), W, H, D - 1)
             yield cur
 
 
@@ -153,15 +153,33 @@ def _auc_from_hist(h_inv, h_val):
     return float((h_inv * (below + 0.5 * h_val)).sum() / (float(n_inv) * float(n_val)))
 
 
-def evaluate(nets, device=0, n_pairs=200, W=1920, H=1080, log=None):
-    """AUCs over held-out pairs: {name: auc} for each net in `nets` (a dict
-    name -> ConfNet) plus 'lr_check', and the invalid-pixel statistics."""
+def _matched_operating_point(h_inv, h_val, fpr_target):
+    """Flagging the pixels whose invalidity bin is >= k: the smallest k whose
+    false-positive rate (valid pixels flagged) is <= fpr_target; returns
+    (tpr, fpr, score threshold 1 - k / N_BINS)."""
+    val_tail = np.cumsum(h_val[::-1])[::-1] / max(1, h_val.sum())   # FPR when flagging bins >= k
+    inv_tail = np.cumsum(h_inv[::-1])[::-1] / max(1, h_inv.sum())
+    ok = np.flatnonzero(val_tail <= fpr_target)
+    k = int(ok[0]) if ok.size else N_BINS
+    if k >= N_BINS:
+        return 0.0, 0.0, 0.0
+    return float(inv_tail[k]), float(val_tail[k]), 1.0 - k / N_BINS
+
+
+def evaluate(nets, device=0, n_pairs=200, W=1920, H=1080, log=None, kind=KIND, threshold=0.5):
+    """AUCs over held-out pairs of generator `kind`: {name: auc} for each net
+    in `nets` (a dict name -> ConfNet) plus 'lr_check', the invalid-pixel
+    statistics, and each net's operating points: its true/false-positive
+    rates for flagging invalid pixels at score < threshold (the threshold the
+    checked map uses) and at the score threshold whose false-positive rate
+    matches the left-right check's."""
     g = _Device(device, W, H)
     hists = {k: (np.zeros(N_BINS, np.int64), np.zeros(N_BINS, np.int64)) for k in nets}
+    at_thr = {k: np.zeros((2, 2), np.int64) for k in nets}  # [invalid?][score < threshold?]
     lr_counts = np.zeros((2, 2), np.int64)  # [invalid?][flagged?]
-    seeds = EVAL_SEED0 + np.arange(n_pairs)
+    seeds = EVAL_SEED0 + (0 if kind == KIND else 100_000 * kind) + np.arange(n_pairs)
     t0 = time.perf_counter()
-    for i, (L, R, G, O) in enumerate(_pairs(seeds, W, H)):
+    for i, (L, R, G, O) in enumerate(_pairs(seeds, W, H, kind)):
         g.upload(L, R)
         g.m.process_lr(g.L, g.R, disp_checked=g.chk, tol=1)
         has, correct = _labels(g.curves(), G, O)
@@ -178,6 +196,9 @@ def evaluate(nets, device=0, n_pairs=200, W=1920, H=1080, log=None):
             b = np.minimum((((1.0 - s) * N_BINS)).astype(np.int64), N_BINS - 1)  # invalidity bin
             hists[name][0][:] += np.bincount(b[inv], minlength=N_BINS)
             hists[name][1][:] += np.bincount(b[val], minlength=N_BINS)
+            low = s < threshold
+            at_thr[name] += np.array([[int((val & ~low).sum()), int((val & low).sum())],
+                                      [int((inv & ~low).sum()), int((inv & low).sum())]], np.int64)
         if log and (i + 1) % 25 == 0:
             log(f"  eval pairs {i + 1}/{n_pairs} ({time.perf_counter() - t0:.1f} s)")
     out = {name: _auc_from_hist(*hists[name]) for name in nets}
@@ -189,6 +210,15 @@ def evaluate(nets, device=0, n_pairs=200, W=1920, H=1080, log=None):
     out["invalid_fraction"] = float(lr_counts[1].sum() / max(1, lr_counts.sum()))
     out["pixels"] = int(lr_counts.sum())
     out["pairs"] = int(n_pairs)
+    out["kind"] = int(kind)
+    for name in nets:
+        c = at_thr[name]
+        out[f"{name}_tpr"] = float(c[1, 1] / max(1, c[1].sum()))
+        out[f"{name}_fpr"] = float(c[0, 1] / max(1, c[0].sum()))
+        out[f"{name}_threshold"] = float(threshold)
+        m_tpr, m_fpr, m_thr = _matched_operating_point(*hists[name], out["lr_check_fpr"])
+        out[f"{name}_tpr_at_lr_fpr"], out[f"{name}_fpr_at_lr_fpr"] = m_tpr, m_fpr
+        out[f"{name}_threshold_at_lr_fpr"] = m_thr
     return out
 
 

@@ -21,8 +21,16 @@
 //    streams, other host threads) race and corrupt each other's results.
 //    Serialise them, e.g. on one stream.
 //  * The arrays keep the previous call's contents; the merge keys must start
-//    at 0xFFFFFFFF, so every call clears them first (cudaMemsetAsync, which
-//    allocates nothing).
+//    at 0xFFFFFFFF, so every call whose disparities span more than one CTA
+//    clears them first (cudaMemsetAsync, which allocates nothing; the
+//    finalize kernel also resets every key it reads, the clear guards against
+//    a call that was cut short).
+//  * Bounded device waits that give up write CT_ETIMEOUT into the caller's
+//    status word, or, when the caller passes none, into a static word that
+//    ct_bm_census_static_status reads and clears.
+//  * The looked-up addresses belong to the device's current CUDA context; if
+//    that context changes (cudaDeviceReset, a new primary context), the next
+//    call looks them up again.
 #include "ct_internal.h"
 #include "ct_device.cuh"
 #include "census_match.cuh"
@@ -45,6 +53,7 @@ static __device__ __align__(256) uint32_t g_static_keys[kStaticMaxPixels];
 static __device__ __align__(256) int32_t g_static_status[64];
 
 struct StaticScratch {
+    CUcontext ctx = nullptr;  // context the addresses were looked up in
     uint64_t* desc = nullptr;
     uint32_t* keys = nullptr;
     int32_t* status = nullptr;
@@ -53,6 +62,22 @@ struct StaticScratch {
 std::mutex g_mu;
 std::vector<StaticScratch> g_scratch;  // by device ordinal
 
+// The current context of this thread through the driver's entry point (the
+// library does not link libcuda directly); NULL if none is bound yet.
+CUcontext current_context() {
+    static PFN_cuCtxGetCurrent_v4000 get = nullptr;
+    if (!get) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        get = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(fn);
+    }
+    CUcontext ctx = nullptr;
+    return get(&ctx) == CUDA_SUCCESS ? ctx : nullptr;
+}
+
 // Device addresses of the arrays on `device` (which is current). Host code
 // must not pass the symbols themselves to a kernel: on the host they name a
 // host-side shadow, not device memory.
@@ -60,12 +85,16 @@ int static_scratch(int device, StaticScratch* out) {
     std::lock_guard<std::mutex> lk(g_mu);
     if ((int)g_scratch.size() <= device) g_scratch.resize(device + 1);
     StaticScratch& s = g_scratch[device];
-    if (!s.desc) {
+    // NULL before the runtime has bound a context to this thread; the lookup
+    // below binds the device's primary context.
+    CUcontext ctx = current_context();
+    if (!s.desc || !ctx || s.ctx != ctx) {
         StaticScratch t;
         CT_CUDA_TRY(cudaGetSymbolAddress(reinterpret_cast<void**>(&t.desc), g_static_desc));
         CT_CUDA_TRY(cudaGetSymbolAddress(reinterpret_cast<void**>(&t.keys), g_static_keys));
         CT_CUDA_TRY(cudaGetSymbolAddress(reinterpret_cast<void**>(&t.status), g_static_status));
         CT_CUDA_TRY(cm::prepare_census_match());  // function attributes only
+        t.ctx = current_context();
         s = t;
     }
     *out = s;
@@ -106,7 +135,8 @@ extern "C" int ct_bm_census_process_static(const ct_image* disp, const ct_image*
     using namespace cm;
     uint64_t* dl = sc.desc;
     uint64_t* dr = sc.desc + pitch * H;
-    CT_CUDA_TRY(cudaMemsetAsync(sc.keys, 0xFF, (size_t)W * H * sizeof(uint32_t), s));
+    if (disp_count > kDPC)  // the keys merge several disparity CTAs
+        CT_CUDA_TRY(cudaMemsetAsync(sc.keys, 0xFF, (size_t)W * H * sizeof(uint32_t), s));
     if (int rc = census::launch9x7(left, dl, pitch, status, s, 1)) return rc;
     if (int rc = census::launch9x7(right, dr, pitch, status, s, 1)) return rc;
     const int dir = left_to_right ? 0 : 1;
@@ -121,5 +151,21 @@ extern "C" int ct_bm_census_process_static(const ct_image* disp, const ct_image*
     a.status = status;
     const cudaError_t e = dir == 0 ? launch_census_match<0>(tb, tm, a, s) : launch_census_match<1>(tb, tm, a, s);
     if (e != cudaSuccess) return fail(CT_ECUDA, "census match launch failed: %s", cudaGetErrorString(e));
+    return CT_OK;
+}
+
+extern "C" int ct_bm_census_static_status(int32_t* status) {
+    clear_error();
+    if (!status) return fail(CT_EINVAL, "null argument");
+    *status = 0;
+    int device = 0;
+    CT_CUDA_TRY(cudaGetDevice(&device));
+    StaticScratch sc;
+    if (int rc = static_scratch(device, &sc)) return rc;
+    CT_CUDA_TRY(cudaDeviceSynchronize());
+    int32_t v = 0;
+    CT_CUDA_TRY(cudaMemcpy(&v, sc.status, sizeof v, cudaMemcpyDeviceToHost));
+    CT_CUDA_TRY(cudaMemset(sc.status, 0, sizeof v));
+    *status = v;
     return CT_OK;
 }

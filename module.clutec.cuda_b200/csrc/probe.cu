@@ -6,9 +6,26 @@
 // or coupled so the compiler cannot fold iterations. The SM clock is taken
 // from clock64() against %globaltimer on one thread of the same launch.
 #include "ct_internal.h"
+#include "ct_device.cuh"
 
 namespace ct {
 namespace {
+
+// One CTA waits on an mbarrier that nothing arrives at (no TMA is issued, no
+// thread arrives), through the same bounded wait every TMA consumer uses, with
+// `polls` as its limit. The wait gives up, and the kernel records CT_ETIMEOUT
+// in the status word exactly as a kernel whose tile never arrived would, then
+// returns normally: nothing is in flight, so the context stays usable.
+__global__ void __launch_bounds__(32) wait_timeout_kernel(uint32_t polls, int32_t* status) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        dev::mbar_init(&bar, 1);
+        dev::fence_barrier_init();
+    }
+    __syncwarp();
+    const bool ok = dev::mbar_wait_bounded(&bar, 0, polls);
+    if (!ok && threadIdx.x == 0) dev::report(status, CT_ETIMEOUT);
+}
 
 enum Op { kPopc = 0, kIadd3 = 1, kLop3 = 2, kVimnmx3 = 3, kImad = 4 };
 
@@ -110,5 +127,20 @@ extern "C" int ct_probe_pipe_rates(int32_t device, ct_pipe_rates* out) {
     if (int rc = run_probe<kVimnmx3>(sms, &out->vimnmx_per_clk_sm, &m)) return rc;
     if (int rc = run_probe<kImad>(sms, &out->imad_per_clk_sm, &m)) return rc;
     out->sm_clock_mhz = mhz;
+    return CT_OK;
+}
+
+extern "C" int ct_handle_test_wait_timeout(ct_handle* h, uint32_t poll_limit, ct_stream stream) {
+    using namespace ct;
+    clear_error();
+    if (!h) return fail(CT_EINVAL, "null handle");
+    if (!h->configured || !h->d_status) return fail(CT_ESTATE, "handle not configured");
+    if (poll_limit < 1 || poll_limit > dev::kWaitLimit)
+        return fail(CT_EINVAL, "poll_limit must be 1..%u", dev::kWaitLimit);
+    if (int rc = use_device(h->device)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    wait_timeout_kernel<<<1, 32, 0, s>>>(poll_limit, h->d_status);
+    CT_LAUNCH_CHECK();
+    h->last_stream = s;
     return CT_OK;
 }

@@ -20,6 +20,7 @@ from pathlib import Path
 
 _PKG = Path(__file__).resolve().parent
 LIB_PATH = _PKG / "libctstereo.so"
+SYNTH_PATH = _PKG / "libctsynth.so"
 
 # status codes (ctstereo.h)
 CT_OK, CT_EINVAL, CT_ETYPE, CT_EFORMAT, CT_ECUDA, CT_ETIMEOUT, CT_ESTATE, CT_ENOMEM, CT_EINTERNAL = range(9)
@@ -156,6 +157,8 @@ def _declare(L: C.CDLL) -> None:
         "ct_bm_census_tuning": [H, P(C.c_int32), P(C.c_int32)],
         "ct_bm_census_set_tuning": [H, C.c_int32, C.c_int32],
         "ct_bm_census_process_static": [img, img, img, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p],
+        "ct_bm_census_static_status": [P(C.c_int32)],
+        "ct_handle_test_wait_timeout": [H, C.c_uint32, C.c_void_p],
         "ct_curves_pitch": [C.c_int32, P(C.c_size_t)],
         "ct_bm_census_process_curves": [H, img, P(ct_curves), img, img, C.c_void_p],
         "ct_confnet_create": [P(H)],
@@ -206,8 +209,6 @@ def _declare(L: C.CDLL) -> None:
         "ct_census_stream_wait": [H, C.c_int64],
         "ct_census_stream_timer_start": [H],
         "ct_census_stream_timer_stop": [H, P(C.c_float)],
-        "ct_synth_pair": [C.c_int32, C.c_uint64, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
-                          C.c_void_p, C.c_void_p],
         "ct_probe_pipe_rates": [C.c_int32, P(ct_pipe_rates)],
     }
     for name, args in sigs.items():
@@ -218,9 +219,9 @@ def _declare(L: C.CDLL) -> None:
         f.restype = C.c_int
 
 
-def exported_symbols():
-    """Names of the ct_* entry points declared in include/ctstereo.h."""
-    hdr = (_PKG.parent / "include" / "ctstereo.h").read_text()
+def exported_symbols(header: str = "ctstereo.h"):
+    """Names of the ct_* entry points declared in include/<header>."""
+    hdr = (_PKG.parent / "include" / header).read_text()
     return sorted(set(re.findall(r"^(?:int|const char\s*\*)\s+(ct_[a-z0-9_]+)\s*\(", hdr, re.M)))
 
 
@@ -298,6 +299,11 @@ class _Driver:
         v = C.c_int32()
         check(lib().ct_handle_device_status(self._h, C.byref(v)))
         return v.value
+
+    def test_wait_timeout(self, poll_limit: int = 1024, stream=None):
+        """ct_handle_test_wait_timeout: a bounded device wait that nothing
+        completes gives up and sets this handle's status to CT_ETIMEOUT."""
+        check(lib().ct_handle_test_wait_timeout(self._h, poll_limit, _stream(stream)))
 
 
 def _fmt(width, height, type_=CT_PIX_U8):
@@ -664,21 +670,50 @@ class ConfNet(_Driver):
 def census_match_static(disp, left, right, disp_count: int, left_to_right: bool = True, device_status=None,
                         stream=None):
     """ct_bm_census_process_static: census matching with no device allocation
-    (static scratch; images up to 2,097,152 pixels with rows rounded to 32)."""
+    (static scratch; images up to 2,097,152 pixels with rows rounded up to a
+    multiple of 4). Without device_status, timeouts go to the static word
+    that census_static_status() reads."""
     st = None if device_status is None else C.c_void_p(device_status.data_ptr())
     check(lib().ct_bm_census_process_static(_img_ref(disp), _img_ref(left), _img_ref(right), disp_count,
                                             int(left_to_right), st, _stream(stream)))
 
 
+def census_static_status() -> int:
+    """ct_bm_census_static_status: reads and clears the static status word of
+    census_match_static calls made without a device_status (synchronises)."""
+    v = C.c_int32()
+    check(lib().ct_bm_census_static_status(C.byref(v)))
+    return v.value
+
+
+_synth = None
+
+
+def synth_lib() -> C.CDLL:
+    """Loads libctsynth.so, the host-only generator library (not the matcher)."""
+    global _synth
+    if _synth is None:
+        if not SYNTH_PATH.exists():
+            raise ImportError(f"{SYNTH_PATH} not built: run python module.clutec.cuda_b200/build.py")
+        _synth = C.CDLL(str(SYNTH_PATH))
+        _synth.ct_synth_pair.argtypes = [C.c_int32, C.c_uint64, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+                                         C.c_void_p, C.c_void_p, C.c_void_p]
+        _synth.ct_synth_pair.restype = C.c_int
+    return _synth
+
+
 def synth_pair(kind: int, seed: int, width: int, height: int, dmax: int):
-    """Seeded synthetic pair -> (left u8, right u8, gt int16, occ u8) numpy arrays."""
+    """Seeded synthetic pair -> (left u8, right u8, gt int16, occ u8) numpy
+    arrays, from libctsynth.so (ct_synth_pair, include/ctsynth.h)."""
     import numpy as np
     L = np.empty((height, width), np.uint8)
     R = np.empty((height, width), np.uint8)
     G = np.empty((height, width), np.int16)
     O = np.empty((height, width), np.uint8)
-    check(lib().ct_synth_pair(kind, seed, width, height, dmax, L.ctypes.data, R.ctypes.data, G.ctypes.data,
-                              O.ctypes.data))
+    rc = synth_lib().ct_synth_pair(kind, seed, width, height, dmax, L.ctypes.data, R.ctypes.data,
+                                   G.ctypes.data, O.ctypes.data)
+    if rc != CT_OK:
+        raise CtError(rc, f"ct_synth_pair: bad arguments (kind {kind}, {width}x{height}, dmax {dmax})")
     return L, R, G, O
 
 

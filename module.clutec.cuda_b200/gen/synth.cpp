@@ -14,7 +14,8 @@
 #include <algorithm>
 #include <omp.h>
 
-#include "../../include/ctstereo.h"
+#include "../../include/ctstereo.h"  // status codes
+#include "../../include/ctsynth.h"
 
 namespace {
 

@@ -26,6 +26,22 @@ def build() -> Path:
     return LIB_PATH
 
 
+def use_native() -> str:
+    """Switches this process to liboracle_native.so, compiled here with
+    -march=native for the host's own cores (the CPU-baseline timing). Must run
+    before the first lib() call; falls back to the portable x86-64-v3 build if
+    the compiler fails. Returns the -march used."""
+    global LIB_PATH
+    if _lib is not None:
+        return "native" if LIB_PATH.name == "liboracle_native.so" else "x86-64-v3"
+    # always rebuilt (-B): a copy built on another host may use instructions this one lacks
+    r = subprocess.run(["make", "-B", "-s", "-C", str(_DIR), "native"], capture_output=True, text=True)
+    if r.returncode == 0 and (_DIR / "liboracle_native.so").exists():
+        LIB_PATH = _DIR / "liboracle_native.so"
+        return "native"
+    return "x86-64-v3"
+
+
 def lib() -> C.CDLL:
     global _lib
     if _lib is None:

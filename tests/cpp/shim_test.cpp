@@ -423,6 +423,23 @@ static int RunGpu(const char* weights) {
             for (int x = K + 6; x < W2 - 6 - K; ++x) bad += v2[size_t(y) * W2 + x] != K + 1;
         CHECK(bad == 0, "batch: %d interior pixels not kept at d = %d", bad, K);
     }
+    {  // a bounded device wait that runs out becomes CError(CT_ETIMEOUT), and
+       // the driver keeps working afterwards
+        BlockMatcherCensus::SParameter p;
+        p.xDispConfig.Set(0, 64);
+        BlockMatcherCensus::CDriver d;
+        d.Configure(dev, fin, p);
+        Ensure(ct_handle_test_wait_timeout(d.Handle(), 1024, nullptr), "test wait");
+        CHECK(ThrownCode([&] { d.EnsureDeviceStatus(); }) == CT_ETIMEOUT, "timeout must surface as CT_ETIMEOUT");
+        CHECK(ThrownCode([&] { d.EnsureDeviceStatus(); }) == 0, "status must be cleared after it was read");
+        CDeviceSurface out(f8);
+        ProcessKernel(d, out, surfL, surfR);
+        auto v = out.CopyInto<uint8_t>();
+        int bad = 0;
+        for (int y = 5; y < H - 5; ++y)
+            for (int x = K + 6; x < W - 6 - K; ++x) bad += v[size_t(y) * W + x] != K;
+        CHECK(bad == 0, "census after a timeout: %d interior pixels not at d = %d", bad, K);
+    }
     return g_failures;
 }
 

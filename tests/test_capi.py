@@ -17,6 +17,15 @@ def test_every_declared_symbol_is_exported(ct):
     assert not missing, missing
 
 
+def test_generator_is_its_own_library(ct):
+    """ct_synth_pair lives in libctsynth.so (include/ctsynth.h), not in the
+    matcher library."""
+    names = ct.exported_symbols("ctsynth.h")
+    assert names == ["ct_synth_pair"]
+    assert all(hasattr(ct.synth_lib(), n) for n in names)
+    assert not hasattr(ct.lib(), "ct_synth_pair")
+
+
 def test_create_destroy_each_kind(ct):
     for cls in (ct.CensusTransform, ct.BlockMatcherCensus, ct.BlockMatcherSAD1, ct.BlockMatcherNCC,
                 ct.BlockMatcherAW, ct.CrossCheckDisparityMaps):
@@ -57,7 +66,7 @@ def test_parameter_validation_before_any_device_call(ct):
 
 
 def test_synth_rejects_bad_kind(ct):
-    assert ct.lib().ct_synth_pair(9, 1, 16, 16, 8, None, None, None, None) == ct.CT_EINVAL
+    assert ct.synth_lib().ct_synth_pair(9, 1, 16, 16, 8, None, None, None, None) == ct.CT_EINVAL
 
 
 def test_stream_argument_checks(ct):
