@@ -18,10 +18,12 @@
  *  - A handle may own device scratch (allocated in configure, freed by
  *    ct_destroy). It is not thread-safe: use one handle per host thread or
  *    lock externally; calls on one handle must not overlap on the GPU.
- *  - Disparity d in [0, D) maps a base pixel x to x - d in the other view for
- *    left-to-right matching and to x + d for right-to-left (the reference
- *    hides this in _SDisparityConfig::MapPixelPos, whose arithmetic is not
- *    available; this mapping is the library's definition).
+ *  - Disparity d in [disp_min, disp_min + D) maps a base pixel x to x - d in
+ *    the other view for left-to-right matching and to x + d for right-to-left
+ *    (the reference hides this in _SDisparityConfig::MapPixelPos, whose
+ *    arithmetic is not available; this mapping is the library's definition).
+ *    disp_min (the reference's xDispConfig.Min() / SAD1 iOffset) is 0 unless
+ *    a matcher's parameters set it; maps hold the absolute disparity d.
  *  - Disparity map encodings:
  *      CT_PIX_U8 : d itself, 255 = not a disparity (invalid/inconsistent);
  *                  requires D <= 255.
@@ -146,7 +148,9 @@ typedef struct ct_census_match_params {
     int32_t disp_count;     /* D, 1..256 */
     int32_t agg_radius;     /* r: 2 gives the 5x5 box (only 2 is built) */
     int32_t left_to_right;  /* 1: base = left image; 0: base = right image */
-    int32_t reserved;       /* must be 0 */
+    int32_t disp_min;       /* xDispConfig.Min(): disparities disp_min .. disp_min + D - 1
+                               (BlockMatcherNCC.cu:789-795); U8 maps need disp_min + D <= 255;
+                               cost curves need 0 */
 } ct_census_match_params;
 
 int ct_bm_census_create(ct_handle** out);
@@ -248,7 +252,7 @@ typedef struct ct_sad_params {
     int32_t disp_count;     /* iDispRange: D, 1..256 */
     int32_t radius;         /* EConfig patch: r = 4 gives 9x9; 1..4 */
     int32_t left_to_right;  /* 1: base = left image */
-    int32_t reserved;
+    int32_t disp_min;       /* iOffset: disparities disp_min .. disp_min + D - 1 */
 } ct_sad_params;
 
 int ct_bm_sad_create(ct_handle** out);
@@ -268,7 +272,7 @@ typedef struct ct_ncc_params {
     int32_t disp_count;     /* D, 1..256 */
     int32_t radius;         /* EConfig: 5 = Patch_11x11, 4 = Patch_9x9, 2 = Patch_5x5 */
     int32_t left_to_right;  /* must be 1 */
-    int32_t reserved;
+    int32_t disp_min;       /* xDispConfig.Min(): disparities disp_min .. disp_min + D - 1 */
 } ct_ncc_params;
 
 int ct_bm_ncc_create(ct_handle** out);
@@ -298,7 +302,7 @@ int ct_bm_ncc_process(ct_handle* h, const ct_image* disp, const ct_image* score,
 typedef struct ct_aw_params {
     int32_t disp_count;     /* D, 1..256 */
     int32_t left_to_right;  /* must be 1 */
-    int32_t reserved0;
+    int32_t disp_min;       /* xDispConfig.Min(): disparities disp_min .. disp_min + D - 1 */
     int32_t reserved1;
 } ct_aw_params;
 

@@ -34,15 +34,13 @@
  * reference. The C ABI itself never throws.
  *
  * Differences a caller sees (the build's semantics, not the reference's):
- *   - Disparities start at 0 (_SDisparityConfig::iMin must be 0) and U16
- *     disparity maps hold d + EDisparityId::First or an ID, U8 maps hold d or
- *     255; the 4 x uint16 TPixelEx output (cost and specificity channels) is
- *     not produced.
- *   - The reference's rejection gates (gradient threshold, SAD / NCC
- *     thresholds, minimum-delta specificity) are not built. Configure throws
- *     CError(CT_EINVAL) when a gate that would change the winner is switched
- *     on (fGradThresh > 0); thresholds that only label the unbuilt cost
- *     channels are accepted and ignored.
+ *   - Disparities run from _SDisparityConfig::iMin (SAD1: iOffset) over
+ *     iRange values; U16 disparity maps hold d + EDisparityId::First or an
+ *     ID, U8 maps hold d or 255 (iMin + iRange <= 255).
+ *   - The reference's ID thresholds (fSadThresh, fNccThresh, fSimThresh,
+ *     iMinDeltaThresh, fMinDeltaThresh) label pixels in its 4 x uint16
+ *     TPixelEx output, which the plain winner-take-all maps do not carry:
+ *     Configure throws CError(CT_EINVAL) when one of them is set.
  *   - Guided matching (iUseDispInput + xImageDispInit) searches per 16 x 16
  *     block (see ct_bm_ncc_process / ct_bm_aw_process_guided).
  *   - BlockMatcherAW1 computes the "best of 5 shifted 7x7 windows" cost with
@@ -314,7 +312,13 @@ inline void RequireInputFormat(const SImageFormat& f, const char* who) {
         throw CError(CT_ETYPE, std::string(who) + ": input images must be UInt8 luminance");
 }
 inline void RequireDispConfig(const _SDisparityConfig& c, const char* who) {
-    if (c.iMin != 0) throw CError(CT_EINVAL, std::string(who) + ": disparities start at 0 (iMin must be 0)");
+    if (c.iMin < 0) throw CError(CT_EINVAL, std::string(who) + ": iMin must be >= 0");
+}
+/* The ID thresholds act on the reference's 4 x uint16 output only. */
+inline void RejectIdThresholds(bool bAnySet, const char* who) {
+    if (bAnySet)
+        throw CError(CT_EINVAL, std::string(who) +
+                                    ": the ID thresholds label the 4 x uint16 output, not the plain disparity map");
 }
 }  // namespace detail
 
@@ -377,13 +381,15 @@ public:
 
     void Configure(const CDevice& xDevice, const SImageFormat& xFormat, const SParameter& xPars) {
         detail::RequireInputFormat(xFormat, "BlockMatcherSAD1");
-        if (xPars.iOffset != 0) throw CError(CT_EINVAL, "BlockMatcherSAD1: iOffset must be 0");
+        if (xPars.iOffset < 0) throw CError(CT_EINVAL, "BlockMatcherSAD1: iOffset must be >= 0");
         if (xPars.fGradThresh > 0.f) throw CError(CT_EINVAL, "BlockMatcherSAD1: the gradient gate is not built");
+        detail::RejectIdThresholds(xPars.fSadThresh != 0.f || xPars.iMinDeltaThresh != 0, "BlockMatcherSAD1");
         if (xPars.eConfig == EConfig::Patch_16x16)
             throw CError(CT_EINVAL, "BlockMatcherSAD1: Patch_16x16 is not built (odd windows 3x3 .. 9x9)");
         EnsureHandle(ct_bm_sad_create);
         const ct_format f = xFormat.ToC();
-        const ct_sad_params p{xPars.iDispRange, static_cast<int32_t>(xPars.eConfig), xPars.bLeftToRight ? 1 : 0, 0};
+        const ct_sad_params p{xPars.iDispRange, static_cast<int32_t>(xPars.eConfig), xPars.bLeftToRight ? 1 : 0,
+                              xPars.iOffset};
         Ensure(ct_bm_sad_configure(m_pHandle, xDevice.iDevice, &f, &p), "BlockMatcherSAD1::Configure");
     }
 
@@ -430,12 +436,13 @@ public:
         detail::RequireInputFormat(xFormat, "BlockMatcherNCC");
         detail::RequireDispConfig(xPars.xDispConfig, "BlockMatcherNCC");
         if (xPars.fGradThresh > 0.f) throw CError(CT_EINVAL, "BlockMatcherNCC: the gradient gate is not built");
+        detail::RejectIdThresholds(xPars.fNccThresh != 0.f || xPars.iMinDeltaThresh != 0, "BlockMatcherNCC");
         m_bUseDispInput = xPars.iUseDispInput != 0;
         static const int32_t radius[] = {5, 4, 2};
         EnsureHandle(ct_bm_ncc_create);
         const ct_format f = xFormat.ToC();
         const ct_ncc_params p{xPars.xDispConfig.iRange, radius[static_cast<int>(xPars.eConfig)],
-                              xPars.bLeftToRight ? 1 : 0, 0};
+                              xPars.bLeftToRight ? 1 : 0, xPars.xDispConfig.iMin};
         Ensure(ct_bm_ncc_configure(m_pHandle, xDevice.iDevice, &f, &p), "BlockMatcherNCC::Configure");
     }
 
@@ -506,10 +513,11 @@ public:
         if (xPars.eSimType != ESimType::AbsoluteDifference)
             throw CError(CT_EINVAL, "BlockMatcherAW1: only ESimType::AbsoluteDifference is built");
         if (xPars.fGradThresh > 0.f) throw CError(CT_EINVAL, "BlockMatcherAW1: the gradient gate is not built");
+        detail::RejectIdThresholds(xPars.fSimThresh != 0.f || xPars.fMinDeltaThresh != 0.f, "BlockMatcherAW1");
         m_bUseDispInput = xPars.iUseDispInput != 0;
         EnsureHandle(ct_bm_aw_create);
         const ct_format f = xFormat.ToC();
-        const ct_aw_params p{xPars.xDispConfig.iRange, xPars.bLeftToRight ? 1 : 0, 0, 0};
+        const ct_aw_params p{xPars.xDispConfig.iRange, xPars.bLeftToRight ? 1 : 0, xPars.xDispConfig.iMin, 0};
         Ensure(ct_bm_aw_configure(m_pHandle, xDevice.iDevice, &f, &p), "BlockMatcherAW1::Configure");
     }
 
@@ -850,7 +858,8 @@ public:
         detail::RequireDispConfig(xPars.xDispConfig, "BlockMatcherCensus");
         EnsureHandle(ct_bm_census_create);
         const ct_format f = xFormat.ToC();
-        const ct_census_match_params p{xPars.xDispConfig.iRange, xPars.iAggRadius, xPars.bLeftToRight ? 1 : 0, 0};
+        const ct_census_match_params p{xPars.xDispConfig.iRange, xPars.iAggRadius, xPars.bLeftToRight ? 1 : 0,
+                                       xPars.xDispConfig.iMin};
         Ensure(ct_bm_census_configure(m_pHandle, xDevice.iDevice, &f, &p), "BlockMatcherCensus::Configure");
     }
 
@@ -893,7 +902,7 @@ public:
         if (!xPars.bLeftToRight) throw CError(CT_EINVAL, "CensusStream: the checked map is the left view's");
         EnsureHandle(ct_census_stream_create);
         const ct_format f = xFormat.ToC();
-        const ct_census_match_params p{xPars.xDispConfig.iRange, xPars.iAggRadius, 1, 0};
+        const ct_census_match_params p{xPars.xDispConfig.iRange, xPars.iAggRadius, 1, xPars.xDispConfig.iMin};
         Ensure(ct_census_stream_configure(m_pHandle, xDevice.iDevice, &f, &p, iDispDeltaThresh,
                                           static_cast<int32_t>(eDispType)),
                "CensusStream::Configure");

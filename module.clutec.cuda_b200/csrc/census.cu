@@ -150,7 +150,12 @@ int census_match_pass_maps(BmCensusHandle* h, int dir, const ct_image* disp, con
                            const CUtensorMap& tm, cudaStream_t s, const ct_curves* curves = nullptr) {
     using namespace cm;
     MatchArgs a{};
-    a.W = h->fmt.width; a.H = h->fmt.height; a.D = h->par.disp_count;
+    a.W = h->fmt.width; a.H = h->fmt.height;
+    // an odd minimum disparity runs as the even one below it with relative
+    // d = 0 excluded (see MatchArgs)
+    a.dmin = h->par.disp_min & ~1;
+    a.dfirst = h->par.disp_min & 1;
+    a.D = h->par.disp_count + a.dfirst;
     a.th = h->th;
     a.keys = h->keys;
     a.counters = h->counters;
@@ -275,7 +280,8 @@ int ct_bm_census_configure(ct_handle* hh, int32_t device, const ct_format* fmt, 
         return fail(CT_EINVAL, "image size %dx%d out of range (8..32768)", fmt->width, fmt->height);
     if (p->disp_count < 1 || p->disp_count > 256) return fail(CT_EINVAL, "disp_count must be 1..256");
     if (p->agg_radius != cm::kAR) return fail(CT_EINVAL, "only agg_radius 2 (5x5) is built");
-    if (p->reserved != 0) return fail(CT_EINVAL, "reserved must be 0");
+    if (p->disp_min < 0 || p->disp_min + p->disp_count > 0xFFEF)
+        return fail(CT_EINVAL, "disp_min must be >= 0 with disp_min + disp_count <= 65519");
     if (int rc = use_device(device)) return rc;
     // release a previous configuration
     cudaFree(h->desc); cudaFree(h->keys); cudaFree(h->counters); cudaFree(h->tmp_lr); cudaFree(h->tmp_rl);
@@ -285,7 +291,7 @@ int ct_bm_census_configure(ct_handle* hh, int32_t device, const ct_format* fmt, 
     const int W = fmt->width, H = fmt->height;
     h->desc_pitch = cm::planar_pitch(W);  // pair-planar layout
     if (cudaMalloc(&h->desc, 2 * h->desc_pitch * H * 8) != cudaSuccess) return fail(CT_ENOMEM, "descriptor scratch");
-    const size_t zplanes = (p->disp_count + cm::kDPC - 1) / cm::kDPC;
+    const size_t zplanes = (p->disp_count + (p->disp_min & 1) + cm::kDPC - 1) / cm::kDPC;
     if (cudaMalloc(&h->keys, zplanes * W * H * 4) != cudaSuccess) return fail(CT_ENOMEM, "key scratch");
     // counters for the shortest strips any launch shape uses (11 rows)
     const size_t ngroups = size_t((H + 10) / 11) * ((W + cm::kTWO - 1) / cm::kTWO);
@@ -319,7 +325,8 @@ static int check_disp_out(BmCensusHandle* h, const ct_image* d, const char* name
     if (int rc = check_image(d, name, (1u << CT_PIX_U8) | (1u << CT_PIX_U16))) return rc;
     if (d->width != h->fmt.width || d->height != h->fmt.height)
         return fail(CT_EFORMAT, "%s size differs from the configured format", name);
-    if (d->type == CT_PIX_U8 && h->par.disp_count > 255) return fail(CT_ETYPE, "U8 maps need disp_count <= 255");
+    if (d->type == CT_PIX_U8 && h->par.disp_min + h->par.disp_count > 255)
+        return fail(CT_ETYPE, "U8 maps need disp_min + disp_count <= 255");
     return CT_OK;
 }
 
@@ -352,6 +359,7 @@ int ct_bm_census_process_curves(ct_handle* hh, const ct_image* disp, const ct_cu
     if (int rc = check_match_io(h, left, right)) return rc;
     if (int rc = check_disp_out(h, disp, "disp")) return rc;
     if (!curves || !curves->ptr) return fail(CT_EINVAL, "null curve volume");
+    if (h->par.disp_min != 0) return fail(CT_EINVAL, "cost curves are built for disp_min 0");
     if (curves->width != h->fmt.width || curves->height != h->fmt.height ||
         curves->disp_count != h->par.disp_count)
         return fail(CT_EFORMAT, "curve volume size differs from the configured format");

@@ -93,6 +93,11 @@ struct Var {
 // by atomicMin into one key plane that keys_finalize_kernel converts.
 struct MatchArgs {
     int W, H, D;
+    // Minimum disparity: relative disparity d is matched against column
+    // x -/+ (dmin + d) and stored as dmin + d. dmin is even (the match rows
+    // are read as column pairs); an odd minimum m runs as dmin = m - 1 with
+    // dfirst = 1, which excludes relative d = 0, and D one larger.
+    int dmin, dfirst;
     int th;             // output rows per CTA (strip height)
     uint32_t* keys;     // key plane(s), see above
     uint32_t* counters; // merge_last: one counter per (strip, column tile), 0 between calls
@@ -124,10 +129,11 @@ __host__ __device__ constexpr size_t smem_bytes() {
     return size_t(2) * (kStageB + kStageM) + size_t(2) * kGroups * kBR * kTWV * 4 + 2 * 8 + 16;
 }
 
-// Disparity code for an output pixel from its merged key (C << 16 | d).
+// Disparity code for an output pixel from its merged key (C << 16 | d), d
+// relative to dmin.
 __device__ __forceinline__ void store_disp(void* out, size_t pitch, int type, int x, int y, bool valid,
-                                           uint32_t key) {
-    const uint32_t d = key & 0xFFFFu;
+                                           uint32_t key, int dmin = 0) {
+    const uint32_t d = (key & 0xFFFFu) + uint32_t(dmin);
     const bool ok = valid && (key >> 16) < 2047u;
     if (type == 1) {  // CT_PIX_U8
         reinterpret_cast<uint8_t*>(static_cast<char*>(out) + (size_t)y * pitch)[x] = ok ? uint8_t(d) : uint8_t(0xFF);
@@ -185,7 +191,7 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
 #pragma unroll
     for (int c = 0; c < kCPT; ++c) {
         const int x = xs + 4 * lane + c;
-        lim[c] = min(DIR == 0 ? x - kAR : a.W - 1 - kAR - x, a.D - 1);
+        lim[c] = min(DIR == 0 ? x - kAR - a.dmin : a.W - 1 - kAR - x - a.dmin, a.D - 1);
     }
     // First match column this thread reads per row, as an (even) offset from
     // ms: its words are the pairs (ms + mstart) / 2 + u, u < NWD / 2.
@@ -312,7 +318,8 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
                 k[p] = (C[c][p] << 5) + dconst[p];
                 if (EDGE) {
                     const int dlo = dw + 2 * p;
-                    k[p] |= (dlo > lim[c] ? 0x0000FFFFu : 0u) | (dlo + 1 > lim[c] ? 0xFFFF0000u : 0u);
+                    k[p] |= (dlo > lim[c] || dlo < a.dfirst ? 0x0000FFFFu : 0u) |
+                            (dlo + 1 > lim[c] ? 0xFFFF0000u : 0u);
                 }
             }
             uint32_t m;
@@ -347,7 +354,7 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
             if (oy >= 0 && oy < rows_here && x < a.W) {
                 if (t.nbz == 1) {
                     const bool valid = x >= kAR && x < a.W - kAR && y >= kAR && y < a.H - kAR;
-                    store_disp(a.out, a.out_pitch, a.out_type, x, y, valid, best);
+                    store_disp(a.out, a.out_pitch, a.out_type, x, y, valid, best, a.dmin);
                 } else if (a.merge_last) {
                     a.keys[(size_t)t.bz * a.W * a.H + (size_t)y * a.W + x] = best;
                 } else {
@@ -427,7 +434,7 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
             uint32_t best = 0xFFFFFFFFu;
             for (int z = 0; z < t.nbz; ++z) best = min(best, __ldcg(kp + z * plane));
             const bool valid = x >= kAR && x < a.W - kAR && y >= kAR && y < a.H - kAR;
-            store_disp(a.out, a.out_pitch, a.out_type, x, y, valid, best);
+            store_disp(a.out, a.out_pitch, a.out_type, x, y, valid, best, a.dmin);
         }
     }
     return TileResult{last, false};
@@ -458,11 +465,13 @@ __device__ TileResult run_tile(const CUtensorMap* tmB, const CUtensorMap* tmM, c
     const int y0 = t.by * a.th;                   // first output row
     const int ye0 = y0 - kAR;                     // first cost row
     const int dz0 = t.bz * kDPC;
-    const int ms = DIR == 0 ? xs - dz0 - kDPC : xs + dz0;  // first staged match column
+    // first staged match column (even: xs, dz0, kDPC and dmin are)
+    const int ms = DIR == 0 ? xs - a.dmin - dz0 - kDPC : xs + a.dmin + dz0;
     const int rows_here = min(a.th, a.H - y0);
     const int nb = (rows_here + 2 * kAR + kBR - 1) / kBR;   // batches of 10 cost rows
-    const bool interior = (dz0 + kDPC <= a.D) &&
-                          (DIR == 0 ? (xs >= dz0 + kDPC - 1) : (xs + dz0 + kDPC - 1 + kTWV <= a.W));
+    const bool interior = (dz0 + kDPC <= a.D) && !(a.dfirst > 0 && dz0 == 0) &&
+                          (DIR == 0 ? (xs - a.dmin >= dz0 + kDPC - 1)
+                                    : (xs + a.dmin + dz0 + kDPC - 1 + kTWV <= a.W));
 
     if (tid == 0) {
         dev::prefetch_tmap(tmB);
@@ -523,7 +532,7 @@ __global__ void __launch_bounds__(Var<DPW>::kNT, 1)
 // Converts merged keys to disparities and resets the keys for the next call.
 // (static: each translation unit that launches it has its own copy.)
 static __global__ void keys_finalize_kernel(uint32_t* keys, int W, int H, int r, void* out, size_t out_pitch,
-                                            int out_type) {
+                                            int out_type, int dmin) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (x >= W) return;
@@ -531,7 +540,7 @@ static __global__ void keys_finalize_kernel(uint32_t* keys, int W, int H, int r,
     const uint32_t key = *kp;
     *kp = 0xFFFFFFFFu;
     const bool valid = x >= r && x < W - r && y >= r && y < H - r;
-    store_disp(out, out_pitch, out_type, x, y, valid, key);
+    store_disp(out, out_pitch, out_type, x, y, valid, key, dmin);
 }
 
 // Strip height: picks the height that minimises (waves of CTAs over the SMs)
@@ -615,7 +624,7 @@ inline cudaError_t launch_census_match(const CUtensorMap& tb, const CUtensorMap&
     e = cudaGetLastError();
     if (e != cudaSuccess || grid.z == 1 || a.merge_last) return e;
     keys_finalize_kernel<<<dim3((a.W + 255) / 256, a.H), 256, 0, s>>>(a.keys, a.W, a.H, kAR, a.out, a.out_pitch,
-                                                                      a.out_type);
+                                                                      a.out_type, a.dmin);
     return cudaGetLastError();
 }
 

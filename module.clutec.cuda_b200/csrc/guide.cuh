@@ -5,7 +5,8 @@
 // (x, y) takes the coarse disparity at (x / s, y / s) scaled by s, and a block
 // searches only [max(0, min - 4), max + 4] of its pixels' scaled coarse
 // disparities, nothing when none of them has one. One thread per block; the
-// range is packed lo | hi << 16 (lo > hi: no search).
+// range is packed lo | hi << 16 (lo > hi: no search), relative to the
+// matcher's minimum disparity dmin (clipped at 0).
 #pragma once
 
 #include <cstdint>
@@ -19,7 +20,7 @@ constexpr int kBlock = 16, kMargin = 4;
 
 template <int kUnused = 0>
 __global__ void range_kernel(const void* coarse, size_t pitch, int type, int s, int W, int H, uint32_t* ranges, int gw,
-                             int gh) {
+                             int gh, int dmin) {
     const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y;
     if (gx >= gw || gy >= gh) return;
     const int x0 = gx * kBlock, x1 = min(x0 + kBlock, W) - 1;
@@ -42,8 +43,9 @@ __global__ void range_kernel(const void* coarse, size_t pitch, int type, int s, 
             }
         }
     }
+    const int rlo = max(0, max(0, lo - kMargin) - dmin), rhi = hi + kMargin - dmin;
     ranges[(size_t)gy * gw + gx] =
-        hi < 0 ? 0x0000FFFFu : (uint32_t(max(0, lo - kMargin)) | (uint32_t(min(hi + kMargin, 0xFFFF)) << 16));
+        (hi < 0 || rhi < rlo) ? 0x0000FFFFu : (uint32_t(rlo) | (uint32_t(min(rhi, 0xFFFF)) << 16));
 }
 
 // Union of the ranges of the blocks that output columns [c0, c1] and rows

@@ -39,6 +39,7 @@ __host__ __device__ constexpr int two_of(int R, bool aw) { return kTWV - 2 * ext
 
 struct Args {
     int W, H, D, th;
+    int dmin;               // relative d matches column x -/+ (dmin + d); maps store dmin + d
     const uint32_t* guide;  // AW guided mode: search range per 16 x 16 block (guide.cuh), or null
     int guide_gw;
     uint32_t* keys;      // global keys when gridDim.z > 1 (or always for AW)
@@ -59,11 +60,12 @@ __host__ __device__ constexpr size_t smem_bytes(int th, int R, bool aw) {
 
 __device__ __forceinline__ int floor16(int v) { return v & ~15; }
 
-// U8 / U16 disparity store from a (cost << 16 | d) key; 0xFFFF cost = none.
+// U8 / U16 / F32 disparity store from a (cost << 16 | d) key, d relative to
+// dmin; 0xFFFF cost = none.
 __device__ __forceinline__ void store_key(void* out, size_t pitch, int type, int x, int y, bool valid,
-                                          uint32_t key) {
+                                          uint32_t key, int dmin) {
     const bool ok = valid && (key >> 16) != 0xFFFFu;
-    const uint32_t d = key & 0xFFFFu;
+    const uint32_t d = (key & 0xFFFFu) + uint32_t(dmin);
     char* row = static_cast<char*>(out) + (size_t)y * pitch;
     if (type == CT_PIX_U8) reinterpret_cast<uint8_t*>(row)[x] = ok ? uint8_t(d) : uint8_t(0xFF);
     else if (type == CT_PIX_U16) reinterpret_cast<uint16_t*>(row)[x] = ok ? uint16_t(d + 1) : uint16_t(0xFFFF);
@@ -130,11 +132,11 @@ __global__ void __launch_bounds__(kNT, 1)
     const int dw = dz0 + warp * kDPW;
     const bool warp_active = dw < a.D && ulo <= uhi && dw <= uhi && dw + kDPW - 1 >= ulo;
     const int ab = floor16(xs);
-    const int am = DIR == 0 ? floor16(xs - dz0 - (kDPC - 1)) : floor16(xs + dz0);
+    const int am = DIR == 0 ? floor16(xs - a.dmin - dz0 - (kDPC - 1)) : floor16(xs + a.dmin + dz0);
     // AW windows reach EXT = 6 columns; SAD ones r columns.
     const bool interior = (dz0 + kDPC <= a.D) &&
-                          (DIR == 0 ? (xs + EXT - EXT >= dz0 + kDPC - 1)
-                                    : (xs + kTWV - 1 - EXT + dz0 + kDPC - 1 + EXT <= a.W - 1));
+                          (DIR == 0 ? (xs + EXT - EXT - a.dmin >= dz0 + kDPC - 1)
+                                    : (xs + kTWV - 1 - EXT + a.dmin + dz0 + kDPC - 1 + EXT <= a.W - 1));
 
     if (tid == 0) {
         dev::prefetch_tmap(&tmB);
@@ -155,8 +157,8 @@ __global__ void __launch_bounds__(kNT, 1)
     }
 
     const int bo = xs - ab + 4 * lane;                                        // base column 0 in strip
-    const int mo = DIR == 0 ? (xs - dz0 - am) + 4 * lane - kDPW * warp - 7   // match column for (c=0, j=7)
-                            : (xs + dz0 - am) + 4 * lane + kDPW * warp;      // match column for (c=0, j=0)
+    const int mo = DIR == 0 ? (xs - a.dmin - dz0 - am) + 4 * lane - kDPW * warp - 7   // match column (c=0, j=7)
+                            : (xs + a.dmin + dz0 - am) + 4 * lane + kDPW * warp;      // match column (c=0, j=0)
     uint32_t dlo[4];
 #pragma unroll
     for (int p = 0; p < 4; ++p) dlo[p] = uint32_t(dw + 2 * p);
@@ -255,7 +257,7 @@ __global__ void __launch_bounds__(kNT, 1)
                 if (v < EXT || v >= kTWV - EXT) continue;
                 uint32_t best = 0xFFFFFFFFu;
                 const int x = xs + v;
-                int lim = DIR == 0 ? x - EXT : a.W - 1 - EXT - x;
+                int lim = DIR == 0 ? x - EXT - a.dmin : a.W - 1 - EXT - x - a.dmin;
                 lim = min(lim, a.D - 1);
                 int glo = 0;
                 if constexpr (G) {  // this pixel's block range (pixels outside the image search nothing)
@@ -291,21 +293,22 @@ __global__ void __launch_bounds__(kNT, 1)
         const uint32_t key = sKey[idx];
         if (direct) {
             const bool valid = x >= EXT && x < a.W - EXT && y >= EXT && y < a.H - EXT;
-            store_key(a.out, a.out_pitch, a.out_type, x, y, valid, key);
+            store_key(a.out, a.out_pitch, a.out_type, x, y, valid, key, a.dmin);
         } else {
             atomicMin(&a.keys[(size_t)y * a.W + x], key);
         }
     }
 }
 
-__global__ void ad_finalize_kernel(uint32_t* keys, int W, int H, int ext, void* out, size_t pitch, int type) {
+__global__ void ad_finalize_kernel(uint32_t* keys, int W, int H, int ext, void* out, size_t pitch, int type,
+                                   int dmin) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= W) return;
     uint32_t* kp = &keys[(size_t)y * W + x];
     const uint32_t key = *kp;
     *kp = 0xFFFFFFFFu;
     const bool valid = x >= ext && x < W - ext && y >= ext && y < H - ext;
-    store_key(out, pitch, type, x, y, valid, key);
+    store_key(out, pitch, type, x, y, valid, key, dmin);
 }
 
 // AW cost A(x, y, d) directly from the images (7x7 windows, shifts of 3).
@@ -337,10 +340,11 @@ __device__ int aw_cost_at(const uint8_t* L, size_t pl, const uint8_t* Rm, size_t
     return min(min(min(sc, sl), min(sr, su)), sd);
 }
 
-// Sub-pixel refinement from the merged AW keys: d* = d + (c- - c+) /
-// (2 (c- - 2 c0 + c+)) in IEEE FP32, skipped at d = 0, d = D-1 or when d+1 is
-// not searchable (x - (d+1) - 6 < 0). Resets the keys.
-__global__ void aw_subpixel_kernel(uint32_t* keys, int W, int H, int D, const uint8_t* L, size_t pl,
+// Sub-pixel refinement from the merged AW keys: with d the winner relative to
+// dmin and e = dmin + d its disparity, e* = e + (c- - c+) / (2 (c- - 2 c0 + c+))
+// in IEEE FP32, skipped at d = 0, d = D-1 or when e + 1 is not searchable
+// (x - (e+1) - 6 < 0). Resets the keys.
+__global__ void aw_subpixel_kernel(uint32_t* keys, int W, int H, int D, int dmin, const uint8_t* L, size_t pl,
                                    const uint8_t* Rm, size_t pr, void* out, size_t pitch, int type) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= W) return;
@@ -349,17 +353,18 @@ __global__ void aw_subpixel_kernel(uint32_t* keys, int W, int H, int D, const ui
     *kp = 0xFFFFFFFFu;
     const bool valid = x >= 6 && x < W - 6 && y >= 6 && y < H - 6 && (key >> 16) != 0xFFFFu;
     if (type != CT_PIX_F32 || !valid) {
-        store_key(out, pitch, type, x, y, valid, key);
+        store_key(out, pitch, type, x, y, valid, key, dmin);
         return;
     }
     const int d = int(key & 0xFFFFu);
+    const int e = dmin + d;
     const int c0 = int(key >> 16);
-    float s = float(d);
-    if (d > 0 && d < D - 1 && x - (d + 1) - 6 >= 0) {
-        const int cm = aw_cost_at(L, pl, Rm, pr, x, y, d - 1);
-        const int cp = aw_cost_at(L, pl, Rm, pr, x, y, d + 1);
+    float s = float(e);
+    if (d > 0 && d < D - 1 && x - (e + 1) - 6 >= 0) {
+        const int cm = aw_cost_at(L, pl, Rm, pr, x, y, e - 1);
+        const int cp = aw_cost_at(L, pl, Rm, pr, x, y, e + 1);
         const int den = cm - 2 * c0 + cp;
-        if (den > 0) s = __fadd_rn(float(d), __fdiv_rn(float(cm - cp), float(2 * den)));
+        if (den > 0) s = __fadd_rn(float(e), __fdiv_rn(float(cm - cp), float(2 * den)));
     }
     reinterpret_cast<float*>(static_cast<char*>(out) + (size_t)y * pitch)[x] = s;
 }
@@ -379,7 +384,7 @@ struct AdHandle : ct_handle {
         cudaFree(guide);
     }
     ct_format fmt{};
-    int D = 0, R = 4, dir = 0;
+    int D = 0, R = 4, dir = 0, dmin = 0;
     uint32_t* keys = nullptr;
     uint32_t* guide = nullptr;  // AW guided mode: one search range per 16 x 16 block
     int th = 32;
@@ -410,13 +415,15 @@ int launch_ad(AdHandle* h, const ct_image* disp, const ct_image* L, const ct_ima
     constexpr int EXT = ext_of(R, AW), TWO = two_of(R, AW);
     Args a{};
     a.W = W; a.H = H; a.D = h->D; a.th = h->th;
+    a.dmin = h->dmin;
     a.keys = h->keys;
     a.out = disp->ptr; a.out_pitch = disp->pitch_bytes; a.out_type = disp->type;
     a.status = h->d_status;
     if (guided) {
         const int gw = (W + guide::kBlock - 1) / guide::kBlock, gh = (H + guide::kBlock - 1) / guide::kBlock;
         guide::range_kernel<<<dim3((gw + 127) / 128, gh), 128, 0, s>>>(init->ptr, init->pitch_bytes, init->type,
-                                                                       W / init->width, W, H, h->guide, gw, gh);
+                                                                       W / init->width, W, H, h->guide, gw, gh,
+                                                                       h->dmin);
         CT_LAUNCH_CHECK();
         a.guide = h->guide;
         a.guide_gw = gw;
@@ -439,22 +446,23 @@ int launch_ad(AdHandle* h, const ct_image* disp, const ct_image* L, const ct_ima
     CT_LAUNCH_CHECK();
     if (AW) {
         aw_subpixel_kernel<<<dim3((W + 127) / 128, H), 128, 0, s>>>(
-            h->keys, W, H, h->D, static_cast<const uint8_t*>(L->ptr), L->pitch_bytes,
+            h->keys, W, H, h->D, h->dmin, static_cast<const uint8_t*>(L->ptr), L->pitch_bytes,
             static_cast<const uint8_t*>(Rimg->ptr), Rimg->pitch_bytes, disp->ptr, disp->pitch_bytes, disp->type);
         CT_LAUNCH_CHECK();
     } else if (grid.z > 1) {
         ad_finalize_kernel<<<dim3((W + 255) / 256, H), 256, 0, s>>>(h->keys, W, H, EXT, disp->ptr,
-                                                                    disp->pitch_bytes, disp->type);
+                                                                    disp->pitch_bytes, disp->type, h->dmin);
         CT_LAUNCH_CHECK();
     }
     return CT_OK;
 }
 
-int configure_ad(AdHandle* h, int32_t device, const ct_format* fmt, int D, int R, int dir) {
+int configure_ad(AdHandle* h, int32_t device, const ct_format* fmt, int D, int R, int dir, int dmin) {
     if (fmt->type != CT_PIX_U8) return fail(CT_ETYPE, "matcher input must be U8 (TPixel_Lum_UInt8)");
     if (fmt->width < 16 || fmt->height < 16 || fmt->width > 32768 || fmt->height > 32768)
         return fail(CT_EINVAL, "image size %dx%d out of range (16..32768)", fmt->width, fmt->height);
     if (D < 1 || D > 256) return fail(CT_EINVAL, "disp_count must be 1..256");
+    if (dmin < 0 || dmin + D > 0xFFEF) return fail(CT_EINVAL, "disp_min must be >= 0 with disp_min + disp_count <= 65519");
     if (int rc = use_device(device)) return rc;
     cudaFree(h->keys);
     cudaFree(h->guide);
@@ -472,6 +480,7 @@ int configure_ad(AdHandle* h, int32_t device, const ct_format* fmt, int D, int R
     h->D = D;
     h->R = R;
     h->dir = dir;
+    h->dmin = dmin;
     h->configured = true;
     return CT_OK;
 }
@@ -485,7 +494,8 @@ int check_io(AdHandle* h, const ct_image* disp, const ct_image* L, const ct_imag
         return fail(CT_EFORMAT, "image size differs from the configured format");
     if (int rc = check_image(disp, "disp", disp_types)) return rc;
     if (int rc = check_same_size(disp, L, "disp", "left")) return rc;
-    if (disp->type == CT_PIX_U8 && h->D > 255) return fail(CT_ETYPE, "U8 maps need disp_count <= 255");
+    if (disp->type == CT_PIX_U8 && h->dmin + h->D > 255)
+        return fail(CT_ETYPE, "U8 maps need disp_min + disp_count <= 255");
     return CT_OK;
 }
 
@@ -509,8 +519,7 @@ int ct_bm_sad_configure(ct_handle* hh, int32_t device, const ct_format* fmt, con
     if (!h) return fail(CT_ESTATE, "not a SAD matcher handle");
     if (!fmt || !p) return fail(CT_EINVAL, "null format or parameters");
     if (p->radius < 1 || p->radius > 4) return fail(CT_EINVAL, "radius must be 1..4 (3x3 .. 9x9)");
-    if (p->reserved != 0) return fail(CT_EINVAL, "reserved must be 0");
-    return configure_ad(h, device, fmt, p->disp_count, p->radius, p->left_to_right ? 0 : 1);
+    return configure_ad(h, device, fmt, p->disp_count, p->radius, p->left_to_right ? 0 : 1, p->disp_min);
 }
 
 int ct_bm_sad_process(ct_handle* hh, const ct_image* disp, const ct_image* left, const ct_image* right,
@@ -549,8 +558,8 @@ int ct_bm_aw_configure(ct_handle* hh, int32_t device, const ct_format* fmt, cons
     if (!h) return fail(CT_ESTATE, "not an AW matcher handle");
     if (!fmt || !p) return fail(CT_EINVAL, "null format or parameters");
     if (p->left_to_right != 1) return fail(CT_EINVAL, "the AW matcher is left-to-right only");
-    if (p->reserved0 || p->reserved1) return fail(CT_EINVAL, "reserved fields must be 0");
-    return configure_ad(h, device, fmt, p->disp_count, 3, 0);
+    if (p->reserved1) return fail(CT_EINVAL, "reserved field must be 0");
+    return configure_ad(h, device, fmt, p->disp_count, 3, 0, p->disp_min);
 }
 
 int ct_bm_aw_process(ct_handle* hh, const ct_image* disp, const ct_image* left, const ct_image* right,

@@ -69,6 +69,7 @@ constexpr int kGuideBlock = guide::kBlock;
 
 struct Args {
     int W, H, D, th;
+    int dmin;                // relative d matches column x - (dmin + d); maps store dmin + d
     const uint32_t* guide;   // per 16 x 16 block search range, or null (search all D)
     int guide_gw;
     const int32_t *Sx, *Vx, *Sy, *Vy;   // stats of the left / right image (W*H)
@@ -83,7 +84,7 @@ struct Args {
 
 __device__ __forceinline__ void store_ncc(const Args& a, int x, int y, bool valid, unsigned long long key) {
     const bool ok = valid && key != 0ull;
-    const uint32_t d = ok ? 0xFFFFFFFFu - uint32_t(key & 0xFFFFFFFFull) : 0u;
+    const uint32_t d = ok ? 0xFFFFFFFFu - uint32_t(key & 0xFFFFFFFFull) + uint32_t(a.dmin) : 0u;
     char* row = static_cast<char*>(a.out) + (size_t)y * a.out_pitch;
     if (a.out_type == CT_PIX_U8) reinterpret_cast<uint8_t*>(row)[x] = ok ? uint8_t(d) : uint8_t(0xFF);
     else reinterpret_cast<uint16_t*>(row)[x] = ok ? uint16_t(d + 1) : uint16_t(0xFFFF);
@@ -135,7 +136,7 @@ __global__ void __launch_bounds__(kNT, 2)
     const bool warp_active = dw < a.D;
     const bool searches = ulo <= uhi && dw <= uhi && dw + kDPW - 1 >= ulo;
     const int ab = xs & ~15;
-    const int am = (xs - dz0 - (kDPC - 1)) & ~15;
+    const int am = (xs - a.dmin - dz0 - (kDPC - 1)) & ~15;
     __syncthreads();
     if (tid == 0) {
         dev::mbar_arrive_expect_tx(bar, uint32_t(kBW * NR + kMWs * NR));
@@ -148,7 +149,7 @@ __global__ void __launch_bounds__(kNT, 2)
         return;
     }
     const int bo = xs - ab + 4 * lane;
-    const int mo = (xs - dz0 - am) + 4 * lane - kDPW * warp - 7;
+    const int mo = (xs - a.dmin - dz0 - am) + 4 * lane - kDPW * warp - 7;
 
     int V[kDPW][kCPT];
 #pragma unroll
@@ -211,10 +212,10 @@ __global__ void __launch_bounds__(kNT, 2)
             }
             if (y < R || y >= a.H - R) continue;
             // right-view statistics of the 11 match columns this thread's 4
-            // columns x 8 disparities read: column xs + 4 lane - dw - 7 + k
+            // columns x 8 disparities read: column xs + 4 lane - dmin - dw - 7 + k
             int syk[kCPT + kDPW - 1], vyk[kCPT + kDPW - 1];
             {
-                const int cb = xs + 4 * lane - dw - (kDPW - 1);
+                const int cb = xs + 4 * lane - a.dmin - dw - (kDPW - 1);
                 const size_t ob = (size_t)y * a.W;
 #pragma unroll
                 for (int k = 0; k < kCPT + kDPW - 1; ++k) {
@@ -242,8 +243,8 @@ __global__ void __launch_bounds__(kNT, 2)
 #pragma unroll
                 for (int j = 0; j < kDPW; ++j) {
                     const int d = dw + j;
-                    if (d > ghi || d < glo || x - d - R < 0) continue;
-                    const int sy = syk[c - j + kDPW - 1], vy = vyk[c - j + kDPW - 1];  // column x - d
+                    if (d > ghi || d < glo || x - a.dmin - d - R < 0) continue;
+                    const int sy = syk[c - j + kDPW - 1], vy = vyk[c - j + kDPW - 1];  // column x - dmin - d
                     const int num = n * C[j][c] - sx * sy;
                     float sc = 0.0f;
                     if ((long long)vx * (long long)vy >= n4)
@@ -316,6 +317,7 @@ int launch_ncc(NccHandle* h, const ct_image* disp, const ct_image* score, const 
     const size_t N = (size_t)W * H;
     Args a{};
     a.W = W; a.H = H; a.D = h->par.disp_count; a.th = h->th;
+    a.dmin = h->par.disp_min;
     a.Sx = h->stats; a.Vx = h->stats + N; a.Sy = h->stats + 2 * N; a.Vy = h->stats + 3 * N;
     a.keys = h->keys;
     a.out = disp->ptr; a.out_pitch = disp->pitch_bytes; a.out_type = disp->type;
@@ -325,7 +327,8 @@ int launch_ncc(NccHandle* h, const ct_image* disp, const ct_image* score, const 
     if (init) {
         const int gw = (W + kGuideBlock - 1) / kGuideBlock, gh = (H + kGuideBlock - 1) / kGuideBlock;
         guide::range_kernel<<<dim3((gw + 127) / 128, gh), 128, 0, s>>>(init->ptr, init->pitch_bytes, init->type,
-                                                                       W / init->width, W, H, h->guide, gw, gh);
+                                                                       W / init->width, W, H, h->guide, gw, gh,
+                                                                       a.dmin);
         CT_LAUNCH_CHECK();
         a.guide = h->guide;
         a.guide_gw = gw;
@@ -377,7 +380,8 @@ int ct_bm_ncc_configure(ct_handle* hh, int32_t device, const ct_format* fmt, con
     if (p->radius != 2 && p->radius != 4 && p->radius != 5)
         return fail(CT_EINVAL, "radius must be 5 (Patch_11x11), 4 (Patch_9x9) or 2 (Patch_5x5)");
     if (p->left_to_right != 1) return fail(CT_EINVAL, "the NCC matcher is left-to-right only");
-    if (p->reserved != 0) return fail(CT_EINVAL, "reserved must be 0");
+    if (p->disp_min < 0 || p->disp_min + p->disp_count > 0xFFEF)
+        return fail(CT_EINVAL, "disp_min must be >= 0 with disp_min + disp_count <= 65519");
     if (int rc = use_device(device)) return rc;
     cudaFree(h->stats); cudaFree(h->keys); cudaFree(h->guide);
     h->stats = nullptr; h->keys = nullptr; h->guide = nullptr;
@@ -409,7 +413,8 @@ int ct_bm_ncc_process(ct_handle* hh, const ct_image* disp, const ct_image* score
         return fail(CT_EFORMAT, "image size differs from the configured format");
     if (int rc = check_image(disp, "disp", (1u << CT_PIX_U8) | (1u << CT_PIX_U16))) return rc;
     if (int rc = check_same_size(disp, left, "disp", "left")) return rc;
-    if (disp->type == CT_PIX_U8 && h->par.disp_count > 255) return fail(CT_ETYPE, "U8 maps need disp_count <= 255");
+    if (disp->type == CT_PIX_U8 && h->par.disp_min + h->par.disp_count > 255)
+        return fail(CT_ETYPE, "U8 maps need disp_min + disp_count <= 255");
     if (score) {
         if (int rc = check_image(score, "score", 1u << CT_PIX_F32)) return rc;
         if (int rc = check_same_size(score, left, "score", "left")) return rc;

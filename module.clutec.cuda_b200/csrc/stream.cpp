@@ -93,7 +93,8 @@ int ct_census_stream_configure(ct_handle* hh, int32_t device, const ct_format* f
     if (!fmt || !p) return fail(CT_EINVAL, "null format or parameters");
     if (tol < 0) return fail(CT_EINVAL, "tol must be >= 0");
     if (out_type != CT_PIX_U8 && out_type != CT_PIX_U16) return fail(CT_ETYPE, "maps must be U8 or U16");
-    if (out_type == CT_PIX_U8 && p->disp_count > 255) return fail(CT_ETYPE, "U8 maps hold at most 255 disparities");
+    if (out_type == CT_PIX_U8 && p->disp_min + p->disp_count > 255)
+        return fail(CT_ETYPE, "U8 maps hold disparities below 255 (disp_min + disp_count <= 255)");
     h->release();
     if (int rc = ct_bm_census_create(&h->matcher)) return rc;
     if (int rc = ct_bm_census_configure(h->matcher, device, fmt, p)) return rc;

@@ -59,21 +59,21 @@ class ct_census_params(C.Structure):
 
 class ct_census_match_params(C.Structure):
     _fields_ = [("disp_count", C.c_int32), ("agg_radius", C.c_int32), ("left_to_right", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("disp_min", C.c_int32)]
 
 
 class ct_sad_params(C.Structure):
     _fields_ = [("disp_count", C.c_int32), ("radius", C.c_int32), ("left_to_right", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("disp_min", C.c_int32)]
 
 
 class ct_ncc_params(C.Structure):
     _fields_ = [("disp_count", C.c_int32), ("radius", C.c_int32), ("left_to_right", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("disp_min", C.c_int32)]
 
 
 class ct_aw_params(C.Structure):
-    _fields_ = [("disp_count", C.c_int32), ("left_to_right", C.c_int32), ("reserved0", C.c_int32),
+    _fields_ = [("disp_count", C.c_int32), ("left_to_right", C.c_int32), ("disp_min", C.c_int32),
                 ("reserved1", C.c_int32)]
 
 
@@ -332,9 +332,10 @@ class BlockMatcherCensus(_Driver):
     _create = "ct_bm_census_create"
 
     def configure(self, device: int, width: int, height: int, disp_count: int, left_to_right: bool = True,
-                  agg_radius: int = 2):
+                  agg_radius: int = 2, disp_min: int = 0):
+        """Disparities disp_min .. disp_min + disp_count - 1."""
         check(lib().ct_bm_census_configure(self._h, device, C.byref(_fmt(width, height)), C.byref(
-            ct_census_match_params(disp_count, agg_radius, int(left_to_right), 0))))
+            ct_census_match_params(disp_count, agg_radius, int(left_to_right), disp_min))))
 
     def process(self, disp, left, right, stream=None):
         check(lib().ct_bm_census_process(self._h, _img_ref(disp), _img_ref(left), _img_ref(right),
@@ -399,9 +400,9 @@ class BlockMatcherSAD1(_Driver):
     _create = "ct_bm_sad_create"
 
     def configure(self, device: int, width: int, height: int, disp_count: int, radius: int = 4,
-                  left_to_right: bool = True):
+                  left_to_right: bool = True, disp_min: int = 0):
         check(lib().ct_bm_sad_configure(self._h, device, C.byref(_fmt(width, height)),
-                                        C.byref(ct_sad_params(disp_count, radius, int(left_to_right), 0))))
+                                        C.byref(ct_sad_params(disp_count, radius, int(left_to_right), disp_min))))
 
     def process(self, disp, left, right, stream=None):
         check(lib().ct_bm_sad_process(self._h, _img_ref(disp), _img_ref(left), _img_ref(right),
@@ -412,9 +413,10 @@ class BlockMatcherNCC(_Driver):
     """BlockMatcherNCC::CDriver with an FP32 (unquantised) score."""
     _create = "ct_bm_ncc_create"
 
-    def configure(self, device: int, width: int, height: int, disp_count: int, radius: int = 5):
+    def configure(self, device: int, width: int, height: int, disp_count: int, radius: int = 5,
+                  disp_min: int = 0):
         check(lib().ct_bm_ncc_configure(self._h, device, C.byref(_fmt(width, height)),
-                                        C.byref(ct_ncc_params(disp_count, radius, 1, 0))))
+                                        C.byref(ct_ncc_params(disp_count, radius, 1, disp_min))))
 
     def process(self, disp, left, right, score=None, disp_init=None, stream=None):
         check(lib().ct_bm_ncc_process(self._h, _img_ref(disp), _img_ref(score), _img_ref(left),
@@ -425,9 +427,9 @@ class BlockMatcherAW(_Driver):
     """BlockMatcherAW1/AW2: best of 5 shifted 7x7 SAD windows + sub-pixel."""
     _create = "ct_bm_aw_create"
 
-    def configure(self, device: int, width: int, height: int, disp_count: int):
+    def configure(self, device: int, width: int, height: int, disp_count: int, disp_min: int = 0):
         check(lib().ct_bm_aw_configure(self._h, device, C.byref(_fmt(width, height)),
-                                       C.byref(ct_aw_params(disp_count, 1, 0, 0))))
+                                       C.byref(ct_aw_params(disp_count, 1, disp_min, 0))))
 
     def process(self, disp, left, right, disp_init=None, stream=None):
         """disp_init: coarse disparity map of the guided mode (or None)."""

@@ -38,8 +38,10 @@ constexpr int kBand = 16;  // output rows per OpenMP work item
 
 // Exhaustive WTA over a (2r+1)^2 box-aggregated per-pixel cost.
 //
-// dir = 0: left-to-right; base = left, match column xm = x - d.
-// dir = 1: right-to-left; base = right, match column xm = x + d.
+// dir = 0: left-to-right; base = left, match column xm = x - (dmin + d).
+// dir = 1: right-to-left; base = right, match column xm = x + (dmin + d).
+// d runs over [0, D); the disparity stored is dmin + d (the reference's
+// search from xDispConfig.Min(), BlockMatcherNCC.cu:789-795).
 // A pixel is valid iff its window lies inside the image (r <= x < W-r and
 // r <= y < H-r); disparity d is valid for it iff the matched window lies
 // inside too (xm - r >= 0 and xm + r < W). WTA scans d ascending and keeps the
@@ -47,9 +49,9 @@ constexpr int kBand = 16;  // output rows per OpenMP work item
 // compares: BlockMatcherSAD1.cu:176, BlockMatcherNCC.cu:300).
 // cost(x, y, xm) is the per-pixel cost of base (x, y) against match (xm, y).
 // curve (optional): W*H*D bytes, aggregated cost >> curve_shift saturated at
-// 255, 255 for invalid d; only written for valid pixels.
+// 255, 255 for invalid d; only written for valid pixels; index d - dmin.
 template <typename CostFn>
-void wta_box(int W, int H, int D, int r, int dir, CostFn cost,
+void wta_box(int W, int H, int D, int dmin, int r, int dir, CostFn cost,
              int16_t* disp, int32_t* best_cost, uint8_t* curve, int curve_shift) {
     const int s = dir == 0 ? -1 : 1;
     const int K = 2 * r + 1;
@@ -67,7 +69,7 @@ void wta_box(int W, int H, int D, int r, int dir, CostFn cost,
             auto erow = [&](int yy, int d) {
                 int32_t* e = &ering[(size_t)(yy % K) * W];
                 for (int x = 0; x < W; ++x) {
-                    const int xm = x + s * d;
+                    const int xm = x + s * (dmin + d);
                     e[x] = (xm >= 0 && xm < W) ? cost(x, yy, xm) : 0;
                 }
                 return e;
@@ -88,9 +90,9 @@ void wta_box(int W, int H, int D, int r, int dir, CostFn cost,
                         int16_t* bdd = &bd[(size_t)(y - y0) * W];
                         for (int x = r; x < W - r; ++x) {
                             acc += colsum[x + r];
-                            const int xm = x + s * d;
+                            const int xm = x + s * (dmin + d);
                             const bool dv = (xm - r >= 0) && (xm + r < W);
-                            if (dv && acc < bst[x]) { bst[x] = acc; bdd[x] = int16_t(d); }
+                            if (dv && acc < bst[x]) { bst[x] = acc; bdd[x] = int16_t(dmin + d); }
                             if (curve)
                                 curve[((size_t)y * W + x) * D + d] =
                                     dv ? uint8_t(std::min(255, acc >> curve_shift)) : uint8_t(255);
@@ -176,9 +178,9 @@ void or_census9x7(const uint8_t* img, int W, int H, int pitch, uint64_t* out, in
 // Census matcher on precomputed descriptors (W*H uint64, pitch W): cost =
 // popcount(cB ^ cM) (CensusDifference, BlockMatcherNCC.cu:153-158, widened to
 // 64 bits), (2r+1)^2 box, WTA.
-void or_match_census_desc(const uint64_t* cb, const uint64_t* cm, int W, int H, int D, int r, int dir,
+void or_match_census_desc(const uint64_t* cb, const uint64_t* cm, int W, int H, int D, int dmin, int r, int dir,
                           int16_t* disp, int32_t* best_cost, uint8_t* curve, int curve_shift) {
-    wta_box(W, H, D, r, dir,
+    wta_box(W, H, D, dmin, r, dir,
             [&](int x, int y, int xm) { return popc64(cb[(size_t)y * W + x] ^ cm[(size_t)y * W + xm]); },
             disp, best_cost, curve, curve_shift);
 }
@@ -186,23 +188,23 @@ void or_match_census_desc(const uint64_t* cb, const uint64_t* cm, int W, int H, 
 // Census matcher from images: 9x7 census of both, then or_match_census_desc.
 // dir 0 uses (base, match) = (L, R); dir 1 uses (R, L).
 void or_match_census(const uint8_t* L, const uint8_t* R, int W, int H, int pitch,
-                     int D, int r, int dir, int16_t* disp, int32_t* best_cost,
+                     int D, int dmin, int r, int dir, int16_t* disp, int32_t* best_cost,
                      uint8_t* curve, int curve_shift) {
     std::vector<uint64_t> cl((size_t)W * H), cr((size_t)W * H);
     or_census9x7(L, W, H, pitch, cl.data(), W);
     or_census9x7(R, W, H, pitch, cr.data(), W);
     const uint64_t* cb = dir == 0 ? cl.data() : cr.data();
     const uint64_t* cm = dir == 0 ? cr.data() : cl.data();
-    or_match_census_desc(cb, cm, W, H, D, r, dir, disp, best_cost, curve, curve_shift);
+    or_match_census_desc(cb, cm, W, H, D, dmin, r, dir, disp, best_cost, curve, curve_shift);
 }
 
 // SAD matcher: (2r+1)^2 box of |B - M| (EvalSAD, BlockMatcherSAD1.cu:151-153),
 // exhaustive WTA (the reference's coarse/fine search is a separate mode).
 void or_match_sad(const uint8_t* L, const uint8_t* R, int W, int H, int pitch,
-                  int D, int r, int dir, int16_t* disp, int32_t* best_cost) {
+                  int D, int dmin, int r, int dir, int16_t* disp, int32_t* best_cost) {
     const uint8_t* b = dir == 0 ? L : R;
     const uint8_t* m = dir == 0 ? R : L;
-    wta_box(W, H, D, r, dir,
+    wta_box(W, H, D, dmin, r, dir,
             [&](int x, int y, int xm) { return std::abs(int(b[y * pitch + x]) - int(m[y * pitch + xm])); },
             disp, best_cost, nullptr, 0);
 }
@@ -213,27 +215,30 @@ void or_match_sad(const uint8_t* L, const uint8_t* R, int W, int H, int pitch,
 // SAD at disparity d. (The reference AW1 scores centre + best 2 of 4
 // sub-windows, Kernel.Algo.AdaptWnd_W32H16.h:240-285, and AW2 its SAD
 // min-variant, Kernel.Algo.AdaptWnd3D.h:244-300; the 5-window min is this
-// build's configuration.) Left-to-right. Pixel valid iff 6 <= x < W-6 and
-// 6 <= y < H-6; d valid iff x - d - 6 >= 0.
+// build's configuration.) Left-to-right, match column x - (dmin + d) for
+// d in [0, D), disparity dmin + d. Pixel valid iff 6 <= x < W-6 and
+// 6 <= y < H-6; d valid iff x - dmin - d - 6 >= 0.
 // Sub-pixel: d* = d + (c- - c+) / (2 (c- - 2 c0 + c+)) with c-, c0, c+ the
 // AW costs at d-1, d, d+1: sub32 in FP32 (float(c- - c+) / float(2 den), then
-// float(d) + that), sub64 in FP64. Skipped (sub = d) when d = 0, d = D-1, d+1
-// is invalid or den <= 0. Invalid pixels: disp -1, sub -1.
+// float(dmin + d) + that), sub64 in FP64. Skipped (sub = dmin + d) when
+// d = 0, d = D-1, d+1 is invalid or den <= 0. Invalid pixels: disp -1, sub -1.
 // ---------------------------------------------------------------------------
 // Guided variant (MatcherUseDisparity, BlockMatcherAW1.cu:996-1180): the
-// winner of pixel (x, y) is taken over d in [lo[y W + x], hi[y W + x]] only
-// (lo > hi: no disparity); the sub-pixel neighbours c-, c+ are the costs at
-// d - 1 and d + 1 whether or not they lie in the range.
-void or_match_aw_guided(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, int D, const int32_t* lo,
-                        const int32_t* hi, int16_t* disp, int32_t* best_cost, float* sub32, double* sub64);
+// winner of pixel (x, y) is taken over disparities in [lo[y W + x], hi[y W + x]]
+// only (lo > hi: no disparity); the sub-pixel neighbours c-, c+ are the costs
+// at the winner - 1 and + 1 whether or not they lie in the range.
+void or_match_aw_guided(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, int D, int dmin,
+                        const int32_t* lo, const int32_t* hi, int16_t* disp, int32_t* best_cost, float* sub32,
+                        double* sub64);
 
-void or_match_aw(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, int D,
+void or_match_aw(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, int D, int dmin,
                  int16_t* disp, int32_t* best_cost, float* sub32, double* sub64) {
-    or_match_aw_guided(L, R, W, H, pitch, D, nullptr, nullptr, disp, best_cost, sub32, sub64);
+    or_match_aw_guided(L, R, W, H, pitch, D, dmin, nullptr, nullptr, disp, best_cost, sub32, sub64);
 }
 
-void or_match_aw_guided(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, int D, const int32_t* lo,
-                        const int32_t* hi, int16_t* disp, int32_t* best_cost, float* sub32, double* sub64) {
+void or_match_aw_guided(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, int D, int dmin,
+                        const int32_t* lo, const int32_t* hi, int16_t* disp, int32_t* best_cost, float* sub32,
+                        double* sub64) {
     const int r = 3, sh = 3, ext = r + sh, K = 2 * r + 1;
     const int nb = (H + kBand - 1) / kBand;
 #pragma omp parallel
@@ -260,8 +265,9 @@ void or_match_aw_guided(const uint8_t* L, const uint8_t* R, int W, int H, int pi
                     auto erow = [&](int yy) {
                         int32_t* e = &ering[(size_t)(yy % K) * W];
                         for (int x = 0; x < W; ++x) {
-                            const int xm = x - d;
-                            e[x] = xm >= 0 ? std::abs(int(L[yy * pitch + x]) - int(R[yy * pitch + xm])) : 0;
+                            const int xm = x - dmin - d;
+                            e[x] = (xm >= 0 && xm < W) ? std::abs(int(L[yy * pitch + x]) - int(R[yy * pitch + xm]))
+                                                       : 0;
                         }
                         return e;
                     };
@@ -290,7 +296,7 @@ void or_match_aw_guided(const uint8_t* L, const uint8_t* R, int W, int H, int pi
                         const int32_t* sd = &S[(size_t)(y + sh - sa) * W];
                         const size_t ro = (size_t)(y - y0) * W;
                         for (int x = ext; x < W - ext; ++x) {
-                            const bool dv = (x - d - ext >= 0);
+                            const bool dv = (x - dmin - d - ext >= 0);
                             int32_t a = -1;
                             if (dv) {
                                 a = sc[x];
@@ -301,8 +307,8 @@ void or_match_aw_guided(const uint8_t* L, const uint8_t* R, int W, int H, int pi
                             }
                             const size_t o = ro + x;
                             if (need[o]) { cp1[o] = a; need[o] = 0; }
-                            const bool in_range =
-                                !lo || (d >= lo[(size_t)y * W + x] && d <= hi[(size_t)y * W + x]);
+                            const bool in_range = !lo || (dmin + d >= lo[(size_t)y * W + x] &&
+                                                          dmin + d <= hi[(size_t)y * W + x]);
                             if (dv && in_range && a < best[o]) {
                                 best[o] = a; bd[o] = int16_t(d);
                                 cm1[o] = prevA[o];
@@ -323,18 +329,18 @@ void or_match_aw_guided(const uint8_t* L, const uint8_t* R, int W, int H, int pi
                         sub32[o] = -1.0f; sub64[o] = -1.0;
                         continue;
                     }
-                    const int d = bd[q];
-                    disp[o] = int16_t(d);
+                    const int d = bd[q];  // relative; -1 if none
+                    disp[o] = int16_t(d < 0 ? -1 : dmin + d);
                     if (best_cost) best_cost[o] = best[q];
-                    float s32 = float(d);
-                    double s64 = double(d);
+                    float s32 = d < 0 ? -1.0f : float(dmin + d);
+                    double s64 = d < 0 ? -1.0 : double(dmin + d);
                     if (d > 0 && d < D - 1 && cp1[q] >= 0 && cm1[q] >= 0) {
                         const int32_t cm = cm1[q], c0 = best[q], cp = cp1[q];
                         const int32_t den = cm - 2 * c0 + cp;
                         if (den > 0) {
                             const float off = float(cm - cp) / float(2 * den);
-                            s32 = float(d) + off;
-                            s64 = double(d) + double(cm - cp) / (2.0 * double(den));
+                            s32 = float(dmin + d) + off;
+                            s64 = double(dmin + d) + double(cm - cp) / (2.0 * double(den));
                         }
                     }
                     sub32[o] = s32; sub64[o] = s64;
@@ -351,23 +357,25 @@ void or_match_aw_guided(const uint8_t* L, const uint8_t* R, int W, int H, int pi
 // when sigma_x sigma_y < 1 (:255-262), i.e. when vx vy < n^4. Otherwise
 // score32 = float(num) / sqrtf(float(vx) * float(vy)) with IEEE-rounded ops,
 // score64 = num / sqrt(vx vy) in double. Argmax over valid d with a strict
-// '>' scanning d ascending (lowest d on ties). Left-to-right; pixel valid iff
-// its window is inside; d valid iff x - d - r >= 0.
+// '>' scanning d ascending (lowest d on ties). Left-to-right, right column
+// x - (dmin + d), disparity dmin + d; pixel valid iff its window is inside;
+// d valid iff x - dmin - d - r >= 0.
 // Outputs: disp (int16, -1 invalid), best32 (FP32 score at the argmax),
 // best64 (FP64 score at that same d).
 // ---------------------------------------------------------------------------
 // Guided variant (MatcherUseDisparity, BlockMatcherNCC.cu:980-1168): pixel
-// (x, y) searches only d in [lo[y W + x], hi[y W + x]]; lo > hi means no
-// search (the pixel gets no disparity). or_match_ncc is the unguided case.
-void or_match_ncc_guided(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, int D, int r,
+// (x, y) searches only disparities in [lo[y W + x], hi[y W + x]]; lo > hi
+// means no search (the pixel gets no disparity). or_match_ncc is the
+// unguided case.
+void or_match_ncc_guided(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, int D, int dmin, int r,
                          const int32_t* lo, const int32_t* hi, int16_t* disp, float* best32, double* best64);
 
-void or_match_ncc(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, int D, int r,
+void or_match_ncc(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, int D, int dmin, int r,
                   int16_t* disp, float* best32, double* best64) {
-    or_match_ncc_guided(L, R, W, H, pitch, D, r, nullptr, nullptr, disp, best32, best64);
+    or_match_ncc_guided(L, R, W, H, pitch, D, dmin, r, nullptr, nullptr, disp, best32, best64);
 }
 
-void or_match_ncc_guided(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, int D, int r,
+void or_match_ncc_guided(const uint8_t* L, const uint8_t* R, int W, int H, int pitch, int D, int dmin, int r,
                          const int32_t* lo, const int32_t* hi, int16_t* disp, float* best32, double* best64) {
     const int n = (2 * r + 1) * (2 * r + 1), K = 2 * r + 1;
     const int64_t n4 = (int64_t)n * n * n * n;
@@ -404,8 +412,8 @@ void or_match_ncc_guided(const uint8_t* L, const uint8_t* R, int W, int H, int p
                     auto erow = [&](int yy) {
                         int32_t* e = &ering[(size_t)(yy % K) * W];
                         for (int x = 0; x < W; ++x) {
-                            const int xm = x - d;
-                            e[x] = xm >= 0 ? int(L[yy * pitch + x]) * int(R[yy * pitch + xm]) : 0;
+                            const int xm = x - dmin - d;
+                            e[x] = (xm >= 0 && xm < W) ? int(L[yy * pitch + x]) * int(R[yy * pitch + xm]) : 0;
                         }
                         return e;
                     };
@@ -422,9 +430,9 @@ void or_match_ncc_guided(const uint8_t* L, const uint8_t* R, int W, int H, int p
                         const size_t ro = (size_t)(y - y0) * W;
                         for (int x = r; x < W - r; ++x) {
                             acc += colsum[x + r];
-                            if (x - d - r >= 0 &&
-                                (!lo || (d >= lo[(size_t)y * W + x] && d <= hi[(size_t)y * W + x]))) {
-                                const size_t o = (size_t)y * W + x, om = o - d;
+                            if (x - dmin - d - r >= 0 &&
+                                (!lo || (dmin + d >= lo[(size_t)y * W + x] && dmin + d <= hi[(size_t)y * W + x]))) {
+                                const size_t o = (size_t)y * W + x, om = o - dmin - d;
                                 const int64_t sx = bl[o], sxx = bll[o], sy = br[om], syy = brr[om];
                                 const int64_t vx = n * sxx - sx * sx, vy = n * syy - sy * sy;
                                 const int64_t num = (int64_t)n * acc - sx * sy;
@@ -432,7 +440,7 @@ void or_match_ncc_guided(const uint8_t* L, const uint8_t* R, int W, int H, int p
                                 if (vx * vy < n4) s32 = 0.f;
                                 else s32 = float(num) / sqrtf(float(vx) * float(vy));
                                 if (s32 > b32[ro + x]) {
-                                    b32[ro + x] = s32; bd[ro + x] = int16_t(d);
+                                    b32[ro + x] = s32; bd[ro + x] = int16_t(dmin + d);
                                     b64[ro + x] = (vx * vy < n4) ? 0.0
                                                   : double(num) / std::sqrt(double(vx) * double(vy));
                                 }

@@ -53,13 +53,13 @@ def lib() -> C.CDLL:
         _lib.or_set_threads.argtypes = [i]
         _lib.or_census3x3.argtypes = [vp, i, i, i, vp, i]
         _lib.or_census9x7.argtypes = [vp, i, i, i, vp, i]
-        _lib.or_match_census_desc.argtypes = [vp, vp, i, i, i, i, i, vp, vp, vp, i]
-        _lib.or_match_census.argtypes = [vp, vp, i, i, i, i, i, i, vp, vp, vp, i]
-        _lib.or_match_sad.argtypes = [vp, vp, i, i, i, i, i, i, vp, vp]
-        _lib.or_match_aw.argtypes = [vp, vp, i, i, i, i, vp, vp, vp, vp]
-        _lib.or_match_aw_guided.argtypes = [vp, vp, i, i, i, i, vp, vp, vp, vp, vp, vp]
-        _lib.or_match_ncc.argtypes = [vp, vp, i, i, i, i, i, vp, vp, vp]
-        _lib.or_match_ncc_guided.argtypes = [vp, vp, i, i, i, i, i, vp, vp, vp, vp, vp]
+        _lib.or_match_census_desc.argtypes = [vp, vp, i, i, i, i, i, i, vp, vp, vp, i]
+        _lib.or_match_census.argtypes = [vp, vp, i, i, i, i, i, i, i, vp, vp, vp, i]
+        _lib.or_match_sad.argtypes = [vp, vp, i, i, i, i, i, i, i, vp, vp]
+        _lib.or_match_aw.argtypes = [vp, vp, i, i, i, i, i, vp, vp, vp, vp]
+        _lib.or_match_aw_guided.argtypes = [vp, vp, i, i, i, i, i, vp, vp, vp, vp, vp, vp]
+        _lib.or_match_ncc.argtypes = [vp, vp, i, i, i, i, i, i, vp, vp, vp]
+        _lib.or_match_ncc_guided.argtypes = [vp, vp, i, i, i, i, i, i, vp, vp, vp, vp, vp]
         _lib.or_crosscheck.argtypes = [vp, vp, i, i, i, i, vp, vp]
     return _lib
 
@@ -98,8 +98,9 @@ def census3x3(img, fill=0):
     return out
 
 
-def match_census(L, R, D, r=2, left_to_right=True, curve_shift=None):
-    """-> (disp int16, best cost int32[, curve uint8 HxWxD])"""
+def match_census(L, R, D, r=2, left_to_right=True, curve_shift=None, dmin=0):
+    """Disparities dmin .. dmin + D - 1 -> (disp int16, best cost int32[,
+    curve uint8 HxWxD indexed by disparity - dmin])"""
     L, R = _u8(L), _u8(R)
     H, W = L.shape
     disp = np.empty((H, W), np.int16)
@@ -107,32 +108,32 @@ def match_census(L, R, D, r=2, left_to_right=True, curve_shift=None):
     curve = None
     if curve_shift is not None:
         curve = np.full((H, W, D), 255, np.uint8)
-    lib().or_match_census(_p(L), _p(R), W, H, W, D, r, 0 if left_to_right else 1, _p(disp), _p(cost),
+    lib().or_match_census(_p(L), _p(R), W, H, W, D, dmin, r, 0 if left_to_right else 1, _p(disp), _p(cost),
                           _p(curve) if curve is not None else None, curve_shift or 0)
     return (disp, cost) if curve is None else (disp, cost, curve)
 
 
-def match_census_desc(cb, cm, D, r=2, left_to_right=True):
+def match_census_desc(cb, cm, D, r=2, left_to_right=True, dmin=0):
     cb = np.ascontiguousarray(cb, np.uint64)
     cm = np.ascontiguousarray(cm, np.uint64)
     H, W = cb.shape
     disp = np.empty((H, W), np.int16)
     cost = np.empty((H, W), np.int32)
-    lib().or_match_census_desc(_p(cb), _p(cm), W, H, D, r, 0 if left_to_right else 1, _p(disp), _p(cost),
+    lib().or_match_census_desc(_p(cb), _p(cm), W, H, D, dmin, r, 0 if left_to_right else 1, _p(disp), _p(cost),
                                None, 0)
     return disp, cost
 
 
-def match_sad(L, R, D, r=4, left_to_right=True):
+def match_sad(L, R, D, r=4, left_to_right=True, dmin=0):
     L, R = _u8(L), _u8(R)
     H, W = L.shape
     disp = np.empty((H, W), np.int16)
     cost = np.empty((H, W), np.int32)
-    lib().or_match_sad(_p(L), _p(R), W, H, W, D, r, 0 if left_to_right else 1, _p(disp), _p(cost))
+    lib().or_match_sad(_p(L), _p(R), W, H, W, D, dmin, r, 0 if left_to_right else 1, _p(disp), _p(cost))
     return disp, cost
 
 
-def match_aw(L, R, D):
+def match_aw(L, R, D, dmin=0):
     """-> (disp int16, cost int32, sub32 float32, sub64 float64)"""
     L, R = _u8(L), _u8(R)
     H, W = L.shape
@@ -140,11 +141,11 @@ def match_aw(L, R, D):
     cost = np.empty((H, W), np.int32)
     s32 = np.empty((H, W), np.float32)
     s64 = np.empty((H, W), np.float64)
-    lib().or_match_aw(_p(L), _p(R), W, H, W, D, _p(disp), _p(cost), _p(s32), _p(s64))
+    lib().or_match_aw(_p(L), _p(R), W, H, W, D, dmin, _p(disp), _p(cost), _p(s32), _p(s64))
     return disp, cost, s32, s64
 
 
-def match_aw_guided(L, R, D, coarse):
+def match_aw_guided(L, R, D, coarse, dmin=0):
     """Guided adaptive-window matcher (see guide_ranges) -> as match_aw."""
     L, R = _u8(L), _u8(R)
     H, W = L.shape
@@ -153,18 +154,19 @@ def match_aw_guided(L, R, D, coarse):
     cost = np.empty((H, W), np.int32)
     s32 = np.empty((H, W), np.float32)
     s64 = np.empty((H, W), np.float64)
-    lib().or_match_aw_guided(_p(L), _p(R), W, H, W, D, _p(lo), _p(hi), _p(disp), _p(cost), _p(s32), _p(s64))
+    lib().or_match_aw_guided(_p(L), _p(R), W, H, W, D, dmin, _p(lo), _p(hi), _p(disp), _p(cost), _p(s32),
+                             _p(s64))
     return disp, cost, s32, s64
 
 
-def match_ncc(L, R, D, r=5):
+def match_ncc(L, R, D, r=5, dmin=0):
     """-> (disp int16, score32 float32, score64 float64)"""
     L, R = _u8(L), _u8(R)
     H, W = L.shape
     disp = np.empty((H, W), np.int16)
     s32 = np.empty((H, W), np.float32)
     s64 = np.empty((H, W), np.float64)
-    lib().or_match_ncc(_p(L), _p(R), W, H, W, D, r, _p(disp), _p(s32), _p(s64))
+    lib().or_match_ncc(_p(L), _p(R), W, H, W, D, dmin, r, _p(disp), _p(s32), _p(s64))
     return disp, s32, s64
 
 
@@ -202,7 +204,7 @@ def guide_ranges(coarse, W, H):
             np.ascontiguousarray(np.repeat(np.repeat(hi, B, 0), B, 1)[:H, :W], np.int32))
 
 
-def match_ncc_guided(L, R, D, coarse, r=5):
+def match_ncc_guided(L, R, D, coarse, r=5, dmin=0):
     """Guided NCC (see guide_ranges) -> (disp int16, score32, score64)."""
     L, R = _u8(L), _u8(R)
     H, W = L.shape
@@ -210,7 +212,7 @@ def match_ncc_guided(L, R, D, coarse, r=5):
     disp = np.empty((H, W), np.int16)
     s32 = np.empty((H, W), np.float32)
     s64 = np.empty((H, W), np.float64)
-    lib().or_match_ncc_guided(_p(L), _p(R), W, H, W, D, r, _p(lo), _p(hi), _p(disp), _p(s32), _p(s64))
+    lib().or_match_ncc_guided(_p(L), _p(R), W, H, W, D, dmin, r, _p(lo), _p(hi), _p(disp), _p(s32), _p(s64))
     return disp, s32, s64
 
 

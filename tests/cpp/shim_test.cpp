@@ -61,8 +61,14 @@ static int RunCpu() {
         p.fGradThresh = 2.f;
         CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "SAD gradient gate must be rejected");
         p = sad;
-        p.iOffset = 3;
-        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "SAD offset must be rejected");
+        p.iOffset = -1;
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "SAD negative offset must be rejected");
+        p = sad;
+        p.fSadThresh = 30.f;
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "SAD fSadThresh must be rejected");
+        p = sad;
+        p.iMinDeltaThresh = 2;
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "SAD iMinDeltaThresh must be rejected");
         CHECK(ThrownCode([&] { d.Configure(dev, SImageFormat(320, 120, EDataType::UInt16), sad); }) == CT_ETYPE,
               "SAD UInt16 input must be rejected");
         p = sad;
@@ -76,9 +82,12 @@ static int RunCpu() {
         p.Set(dc, 0, 0.f, 0.f, 1, true, BlockMatcherNCC::EConfig::Patch_11x11);
         BlockMatcherNCC::CDriver d;
         p.iUseDispInput = 0;
-        p.xDispConfig.Set(5, 128);
-        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "NCC iMin != 0 must be rejected");
+        p.xDispConfig.Set(-1, 128);
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "NCC iMin < 0 must be rejected");
         p.xDispConfig.Set(0, 128);
+        p.fNccThresh = 0.5f;
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "NCC fNccThresh must be rejected");
+        p.fNccThresh = 0.f;
         p.bLeftToRight = false;
         CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "NCC right-to-left must be rejected");
     }

@@ -181,3 +181,48 @@ def test_guided_ncc_is_the_argmax_over_the_guide_range(oracle):
             want[y, x] = bd
     np.testing.assert_array_equal(got, want)
     assert (lo[16:, 32:] > hi[16:, 32:]).all() and (got[16:, 32:] == -1).all()  # the block without hints
+
+
+def _brute_wta(cost, D, dmin, r, lr, valid_match):
+    """Brute-force box-aggregated WTA over disparities dmin .. dmin + D - 1:
+    cost(y, x, xm) per pixel, windows and searchability as the oracle
+    defines them (ties to the lowest disparity)."""
+    H, W = cost.shape[:2]
+    out = np.full((H, W), -1, np.int16)
+    for y in range(r, H - r):
+        for x in range(r, W - r):
+            best = None
+            for d in range(dmin, dmin + D):
+                xm = x - d if lr else x + d
+                if not valid_match(xm):
+                    continue
+                c = sum(int(cost[y + dy, x + dx, d]) for dy in range(-r, r + 1) for dx in range(-r, r + 1))
+                if best is None or c < best:
+                    best, out[y, x] = c, d
+    return out
+
+
+@pytest.mark.parametrize("lr", [True, False])
+@pytest.mark.parametrize("dmin", [0, 3, 7])
+def test_min_disparity_sad_and_census_against_brute_force(oracle, lr, dmin):
+    """A minimum disparity shifts the search to x -/+ (dmin + d) and the
+    stored disparity to dmin + d (BlockMatcherNCC.cu:789-795)."""
+    rng = np.random.default_rng(dmin * 2 + lr)
+    W, H, D, r = 29, 13, 6, 1
+    L = rng.integers(0, 256, (H, W), dtype=np.uint8)
+    R = rng.integers(0, 256, (H, W), dtype=np.uint8)
+    b, m = (L, R) if lr else (R, L)
+    Dt = dmin + D
+    sad = np.zeros((H, W, Dt), np.int64)
+    cb, cm = oracle.census9x7(b), oracle.census9x7(m)
+    ham = np.zeros((H, W, Dt), np.int64)
+    for d in range(Dt):
+        for x in range(W):
+            xm = x - d if lr else x + d
+            if 0 <= xm < W:
+                sad[:, x, d] = np.abs(b[:, x].astype(int) - m[:, xm].astype(int))
+                ham[:, x, d] = [bin(int(u) ^ int(v)).count("1") for u, v in zip(cb[:, x], cm[:, xm])]
+    ok = lambda xm: xm - r >= 0 and xm + r < W  # noqa: E731
+    np.testing.assert_array_equal(oracle.match_sad(L, R, D, r, lr, dmin=dmin)[0], _brute_wta(sad, D, dmin, r, lr, ok))
+    got = oracle.match_census(L, R, D, r, lr, dmin=dmin)[0]
+    np.testing.assert_array_equal(got, _brute_wta(ham, D, dmin, r, lr, ok))
