@@ -64,6 +64,7 @@ typedef struct CUstream_st* ct_stream;
 #define CT_PIX_F32 4
 #define CT_PIX_RGBA8 5  /* 4 bytes per pixel: r, g, b, a (visualisation output) */
 #define CT_PIX_F32X4 6  /* 16 bytes per pixel: 4 floats (3D map: x, y, z, valid) */
+#define CT_PIX_U16X4 7  /* 8 bytes per pixel: 4 x uint16 (the reference matchers' TPixelEx output) */
 
 /* EDisparityId codes used in CT_PIX_U16 maps (DisparityId.h:35-47). */
 #define CT_DISP_FIRST 0x0001
@@ -318,6 +319,89 @@ int ct_bm_aw_process(ct_handle* h, const ct_image* disp, const ct_image* left,
  * disparity when it has none); the sub-pixel step is unchanged. */
 int ct_bm_aw_process_guided(ct_handle* h, const ct_image* disp, const ct_image* left,
                             const ct_image* right, const ct_image* disp_init, ct_stream stream);
+
+/* ---- gradient gate of the plain matchers -----------------------------------
+ * EvalGrad of the reference drivers (BlockMatcherSAD1.cu:226-249,
+ * BlockMatcherNCC.cu:388-413, BlockMatcherAW1.cu:331-417): a pixel whose
+ * patch has too little texture gets no disparity (U8 255, U16
+ * CannotEvaluate, F32 -1; NCC score 0). SAD and NCC handles test the mean
+ * |I(x) - I(x+1)| over the matching window (I = 0 beyond the right edge);
+ * the AW handle tests the standard deviation over the 13 x 13 extent of its
+ * five windows, truncated to an integer, in percent of 255. The base image
+ * is the left one (the right one for right-to-left SAD). Applies to later
+ * process calls; 0 (the default) switches it off. */
+int ct_bm_set_gradient_gate(ct_handle* h, float grad_thresh);
+
+/* ---- reference-compat output: the matchers' 4 x uint16 pixel ---------------
+ * The reference matchers write TPixelEx = 4 x uint16 per pixel:
+ *   x: disparity + EDisparityId::First, or Saturated (winner within the
+ *      saturation band at the ends of the range), NotFound (score beyond the
+ *      score threshold), NotSpecific (the scores next to the winner are within
+ *      the minimum delta), CannotEvaluate (gradient gate, or the patch leaves
+ *      the image), Unknown (no candidate);
+ *   y: the winning score: SAD / N (SAD1, AW2), the NCC quantised to 0..255
+ *      (NCC), or the similarity as a 16-bit percentage (AW1, BlockMatcher1);
+ *   z, w: the specificity deltas before / after the winner, as the
+ *      reference's sequential scan over the disparities records them.
+ * Methods (each restates its driver, scan order and ID rules):
+ *   CT_COMPAT_SAD1: BlockMatcherSAD1 (BlockMatcherSAD1.cu:279-488): P x P SAD
+ *     (P = 3..16, Patch_16x16 centred at +8), scan from the largest disparity
+ *     in steps of 4, then every disparity within 4 of the pixel's winner; a
+ *     new minimum needs SAD / (P*P) < fSadThresh; z / w against the SAD before
+ *     / after; Saturated for the 3 largest disparities; NotSpecific unless
+ *     both deltas > iMinDeltaThresh. x holds the disparity + First (the
+ *     reference's x holds the scan index + First).
+ *   CT_COMPAT_NCC: BlockMatcherNCC (BlockMatcherNCC.cu:180-592): FP32 NCC
+ *     from means and standard deviations, 0 when sigma_x sigma_y < 1,
+ *     clamped at 0 and quantised to uint8; argmax ascending with the SSimStore
+ *     bookkeeping; NotFound when max / 255 < fNccThresh; Saturated for the
+ *     first 2 and the last disparity; NotSpecific unless both deltas >=
+ *     iMinDeltaThresh. P = 5, 9, 11.
+ *   CT_COMPAT_AW1: BlockMatcherAW1 (BlockMatcherAW1.cu:246-635): centre + best
+ *     2 of 4 neighbouring s x s sub-windows (s = 3: Patch_9x9, 5:
+ *     Patch_15x15, AdaptWnd_W32H16.h:240-285) of 255 - |a - b| (sim_type 0)
+ *     or the signed product (1); thresholds fSimThresh and fMinDeltaThresh in
+ *     percent.
+ *   CT_COMPAT_AW2: BlockMatcherAW2 (BlockMatcherAW2.cu:143-382): centre + 2
+ *     lowest of 4 sub-window SADs (AdaptWnd3D.h:244-300), scanned from the
+ *     largest disparity; Saturated within 5 of the largest / 4 of the
+ *     smallest scan index, as the reference compares them.
+ *   CT_COMPAT_BM1: BlockMatcher1 (BlockMatcher1.cu:190-565): plain P x P
+ *     window of (255 - |a - b|) >> 1 or the signed product x 127 (P = 5, 9,
+ *     11, 15), thresholds as AW1.
+ * Gates (grad_thresh > 0): mean |I(x) - I(x+1)| over the patch (SAD1, NCC),
+ * the patch's standard deviation in percent (AW1 after truncation to an
+ * integer, BM1), the AW2 neighbourhood over gradient sub-sums (AW2).
+ * Divergences from the reference (its results there depend on its thread
+ * tiling): a pixel is evaluated iff its patch is inside the image (else
+ * (CannotEvaluate, 0, 0, 0)); a disparity is searched iff the matched patch
+ * is inside; SAD1's fine pass is decided per pixel, not per thread block.
+ */
+#define CT_COMPAT_SAD1 0
+#define CT_COMPAT_NCC 1
+#define CT_COMPAT_AW1 2
+#define CT_COMPAT_AW2 3
+#define CT_COMPAT_BM1 4
+typedef struct ct_compat_params {
+    int32_t method;          /* CT_COMPAT_* */
+    int32_t disp_count;      /* iDispRange / xDispConfig range: 1..256 */
+    int32_t disp_min;        /* iOffset / xDispConfig.Min() */
+    int32_t patch;           /* window side (SAD1, NCC, BM1) or sub-window side (AW1, AW2) */
+    int32_t sim_type;        /* AW1, BM1: 0 absolute difference, 1 signed product */
+    int32_t left_to_right;   /* 1: base = left, match x - d; 0: base = right, x + d */
+    float grad_thresh;       /* fGradThresh (0: no gate) */
+    float score_thresh;      /* fSadThresh / fNccThresh / fSimThresh */
+    float min_delta_thresh;  /* iMinDeltaThresh (integer part; SAD1, NCC, AW2) / fMinDeltaThresh (AW1, BM1) */
+    int32_t reserved[3];     /* 0 */
+} ct_compat_params;
+
+int ct_bm_compat_create(ct_handle** out);
+/* CDriver::Configure of the chosen reference driver. */
+int ct_bm_compat_configure(ct_handle* h, int32_t device, const ct_format* fmt, const ct_compat_params* p);
+/* CDriver::Process(disp, left, right): disp CT_PIX_U16X4 (all four channels)
+ * or CT_PIX_U16 (the x channel only); left / right U8. */
+int ct_bm_compat_process(ct_handle* h, const ct_image* disp, const ct_image* left, const ct_image* right,
+                         ct_stream stream);
 
 /* ---- cross-check: CrossCheckDisparityMaps::CDriver ------------------------
  * Replaces CrossCheckDisparityMaps.h:38-117 / .cu:63-190. For each pixel of

@@ -37,10 +37,15 @@
  *   - Disparities run from _SDisparityConfig::iMin (SAD1: iOffset) over
  *     iRange values; U16 disparity maps hold d + EDisparityId::First or an
  *     ID, U8 maps hold d or 255 (iMin + iRange <= 255).
- *   - The reference's ID thresholds (fSadThresh, fNccThresh, fSimThresh,
- *     iMinDeltaThresh, fMinDeltaThresh) label pixels in its 4 x uint16
- *     TPixelEx output, which the plain winner-take-all maps do not carry:
- *     Configure throws CError(CT_EINVAL) when one of them is set.
+ *   - The output surface's type picks the semantics. EDataType::UInt16x4
+ *     gets the reference's own TPixelEx output (ct_bm_compat_*: its score
+ *     quantisation, scan order, gates, ID thresholds and specificity
+ *     channels; BlockMatcher1, BlockMatcherAW2 and the AW1 2-of-4 patches
+ *     write only that, or its x channel into UInt16). UInt8 / UInt16 / Single
+ *     get the plain winner-take-all maps (exhaustive search, lowest
+ *     disparity on ties, unquantised NCC, gradient gate); the ID thresholds
+ *     (fSadThresh, fNccThresh, fSimThresh, iMinDeltaThresh, fMinDeltaThresh)
+ *     label the TPixelEx output only and must be 0 on that path.
  *   - Guided matching (iUseDispInput + xImageDispInit) searches per 16 x 16
  *     block (see ct_bm_ncc_process / ct_bm_aw_process_guided).
  *   - BlockMatcherAW1 computes the "best of 5 shifted 7x7 windows" cost with
@@ -102,6 +107,7 @@ enum class EDataType : int32_t {
     Single = CT_PIX_F32,
     RGBA8 = CT_PIX_RGBA8,  // 4 bytes: r, g, b, a
     RGBA_Single = CT_PIX_F32X4,  // 4 floats (3D map)
+    UInt16x4 = CT_PIX_U16X4,     // 4 x uint16: the reference matchers' TPixelEx output
 };
 
 inline size_t BytesPerPixel(EDataType t) {
@@ -112,6 +118,7 @@ inline size_t BytesPerPixel(EDataType t) {
         case EDataType::Single: return 4;
         case EDataType::RGBA8: return 4;
         case EDataType::RGBA_Single: return 16;
+        case EDataType::UInt16x4: return 8;
     }
     return 0;
 }
@@ -275,6 +282,7 @@ public:
     /* Reads (and clears) the device status word of the handle's launches; a
      * bounded device-side wait that gave up becomes CError(CT_ETIMEOUT). */
     void EnsureDeviceStatus() {
+        if (!m_pHandle) return;  // drivers whose only path has no device-side waits
         int32_t st = 0;
         Ensure(ct_handle_device_status(m_pHandle, &st), m_sKernelName.c_str());
         if (st != 0) throw CError(st, m_sKernelName + ": device status " + std::to_string(st));
@@ -320,6 +328,48 @@ inline void RejectIdThresholds(bool bAnySet, const char* who) {
         throw CError(CT_EINVAL, std::string(who) +
                                     ": the ID thresholds label the 4 x uint16 output, not the plain disparity map");
 }
+
+/* A reference-compat matcher handle (ct_bm_compat_*) owned by a driver:
+ * the path that writes the reference's 4 x uint16 TPixelEx output. */
+class CCompat {
+public:
+    CCompat() = default;
+    ~CCompat() { ct_destroy(m_pHandle); }
+    CCompat(const CCompat&) = delete;
+    CCompat& operator=(const CCompat&) = delete;
+    void Configure(int iDevice, const ct_format& f, const ct_compat_params& p, const char* who) {
+        if (!m_pHandle) Ensure(ct_bm_compat_create(&m_pHandle), who);
+        Ensure(ct_bm_compat_configure(m_pHandle, iDevice, &f, &p), who);
+        m_bConfigured = true;
+    }
+    bool IsConfigured() const { return m_bConfigured; }
+    void Process(const ct_image* disp, const ct_image* l, const ct_image* r, ct_stream s, const char* who) {
+        if (!m_bConfigured) throw CError(CT_ESTATE, std::string(who) + ": this configuration has no 4 x uint16 output");
+        Ensure(ct_bm_compat_process(m_pHandle, disp, l, r, s), who);
+    }
+    ct_handle* Handle() const { return m_pHandle; }
+
+private:
+    ct_handle* m_pHandle = nullptr;
+    bool m_bConfigured = false;
+};
+
+inline ct_compat_params CompatParams(int32_t method, int32_t range, int32_t dmin, int32_t patch, int32_t sim,
+                                     bool bLeftToRight, float fGrad, float fScore, float fDelta) {
+    ct_compat_params p{};
+    p.method = method;
+    p.disp_count = range;
+    p.disp_min = dmin;
+    p.patch = patch;
+    p.sim_type = sim;
+    p.left_to_right = bLeftToRight ? 1 : 0;
+    p.grad_thresh = fGrad;
+    p.score_thresh = fScore;
+    p.min_delta_thresh = fDelta;
+    return p;
+}
+
+inline bool IsU16x4(const _CDeviceSurface& x) { return x.Format().eDataType == EDataType::UInt16x4; }
 }  // namespace detail
 
 /* ---- CensusTransform (CensusTransform.h:44-70) ----------------------------- */
@@ -351,8 +401,8 @@ public:
 /* ---- BlockMatcherSAD1 (BlockMatcherSAD1.h:42-127) -------------------------- */
 namespace BlockMatcherSAD1 {
 
-/* The reference's only configuration is Patch_16x16, an even window this
- * build does not centre; the odd windows up to 9x9 are built. */
+/* Patch_16x16 (the reference's configuration) feeds the 4 x uint16 output;
+ * the plain exhaustive matcher takes the odd windows 3x3 .. 9x9. */
 enum class EConfig { Patch_16x16 = 0, Patch_3x3, Patch_5x5, Patch_7x7, Patch_9x9 };
 
 struct SParameter {
@@ -375,6 +425,10 @@ struct SParameter {
     }
 };
 
+/* Process into a UInt16x4 surface: the reference's coarse / fine search with
+ * its gates and IDs (ct_bm_compat_*, CT_COMPAT_SAD1). Into UInt8 / UInt16:
+ * the exhaustive winner-take-all over all disparities with the gradient gate;
+ * the ID thresholds (fSadThresh, iMinDeltaThresh) must then be 0. */
 class CDriver : public CKernelDriverBase {
 public:
     CDriver() : CKernelDriverBase("Block Matcher SAD 1") {}
@@ -382,22 +436,39 @@ public:
     void Configure(const CDevice& xDevice, const SImageFormat& xFormat, const SParameter& xPars) {
         detail::RequireInputFormat(xFormat, "BlockMatcherSAD1");
         if (xPars.iOffset < 0) throw CError(CT_EINVAL, "BlockMatcherSAD1: iOffset must be >= 0");
-        if (xPars.fGradThresh > 0.f) throw CError(CT_EINVAL, "BlockMatcherSAD1: the gradient gate is not built");
-        detail::RejectIdThresholds(xPars.fSadThresh != 0.f || xPars.iMinDeltaThresh != 0, "BlockMatcherSAD1");
-        if (xPars.eConfig == EConfig::Patch_16x16)
-            throw CError(CT_EINVAL, "BlockMatcherSAD1: Patch_16x16 is not built (odd windows 3x3 .. 9x9)");
-        EnsureHandle(ct_bm_sad_create);
+        m_xPars = xPars;
         const ct_format f = xFormat.ToC();
-        const ct_sad_params p{xPars.iDispRange, static_cast<int32_t>(xPars.eConfig), xPars.bLeftToRight ? 1 : 0,
-                              xPars.iOffset};
-        Ensure(ct_bm_sad_configure(m_pHandle, xDevice.iDevice, &f, &p), "BlockMatcherSAD1::Configure");
+        const int patch = xPars.eConfig == EConfig::Patch_16x16 ? 16 : 2 * static_cast<int>(xPars.eConfig) + 1;
+        m_xCompat.Configure(xDevice.iDevice, f,
+                            detail::CompatParams(CT_COMPAT_SAD1, xPars.iDispRange, xPars.iOffset, patch, 0,
+                                                 xPars.bLeftToRight, xPars.fGradThresh, xPars.fSadThresh,
+                                                 float(xPars.iMinDeltaThresh)),
+                            "BlockMatcherSAD1::Configure");
+        if (xPars.eConfig != EConfig::Patch_16x16) {
+            EnsureHandle(ct_bm_sad_create);
+            const ct_sad_params p{xPars.iDispRange, static_cast<int32_t>(xPars.eConfig), xPars.bLeftToRight ? 1 : 0,
+                                  xPars.iOffset};
+            Ensure(ct_bm_sad_configure(m_pHandle, xDevice.iDevice, &f, &p), "BlockMatcherSAD1::Configure");
+            Ensure(ct_bm_set_gradient_gate(m_pHandle, xPars.fGradThresh), "BlockMatcherSAD1::Configure");
+        }
     }
 
-    /* xImageDisp: UInt8 or UInt16. */
+    /* xImageDisp: UInt16x4 (reference output) or UInt8 / UInt16 (plain map). */
     void Process(_CDeviceSurface& xImageDisp, const _CDeviceSurface& xImageL, const _CDeviceSurface& xImageR) {
+        if (detail::IsU16x4(xImageDisp)) {
+            m_xCompat.Process(xImageDisp.C(), xImageL.C(), xImageR.C(), S(), "BlockMatcherSAD1::Process");
+            return;
+        }
+        if (m_xPars.eConfig == EConfig::Patch_16x16)
+            throw CError(CT_EINVAL, "BlockMatcherSAD1: Patch_16x16 writes the UInt16x4 output only");
+        detail::RejectIdThresholds(m_xPars.fSadThresh != 0.f || m_xPars.iMinDeltaThresh != 0, "BlockMatcherSAD1");
         Ensure(ct_bm_sad_process(m_pHandle, xImageDisp.C(), xImageL.C(), xImageR.C(), S()),
                "BlockMatcherSAD1::Process");
     }
+
+private:
+    SParameter m_xPars;
+    detail::CCompat m_xCompat;
 };
 
 }  // namespace BlockMatcherSAD1
@@ -428,6 +499,11 @@ struct SParameter {
     }
 };
 
+/* Process into UInt16x4: the reference's uint8-quantised NCC with its
+ * gates, IDs and specificity channels (CT_COMPAT_NCC, either direction).
+ * Into UInt8 / UInt16 (+ Single score in xImageDebug): the FP32 NCC
+ * winner-take-all (left-to-right), optionally guided, with the gradient gate;
+ * fNccThresh and iMinDeltaThresh must then be 0. */
 class CDriver : public CKernelDriverBase {
 public:
     CDriver() : CKernelDriverBase("Block Matcher NCC") {}
@@ -435,24 +511,39 @@ public:
     void Configure(const CDevice& xDevice, const SImageFormat& xFormat, const SParameter& xPars) {
         detail::RequireInputFormat(xFormat, "BlockMatcherNCC");
         detail::RequireDispConfig(xPars.xDispConfig, "BlockMatcherNCC");
-        if (xPars.fGradThresh > 0.f) throw CError(CT_EINVAL, "BlockMatcherNCC: the gradient gate is not built");
-        detail::RejectIdThresholds(xPars.fNccThresh != 0.f || xPars.iMinDeltaThresh != 0, "BlockMatcherNCC");
+        m_xPars = xPars;
         m_bUseDispInput = xPars.iUseDispInput != 0;
         static const int32_t radius[] = {5, 4, 2};
-        EnsureHandle(ct_bm_ncc_create);
+        const int r = radius[static_cast<int>(xPars.eConfig)];
         const ct_format f = xFormat.ToC();
-        const ct_ncc_params p{xPars.xDispConfig.iRange, radius[static_cast<int>(xPars.eConfig)],
-                              xPars.bLeftToRight ? 1 : 0, xPars.xDispConfig.iMin};
-        Ensure(ct_bm_ncc_configure(m_pHandle, xDevice.iDevice, &f, &p), "BlockMatcherNCC::Configure");
+        m_xCompat.Configure(xDevice.iDevice, f,
+                            detail::CompatParams(CT_COMPAT_NCC, xPars.xDispConfig.iRange, xPars.xDispConfig.iMin,
+                                                 2 * r + 1, 0, xPars.bLeftToRight, xPars.fGradThresh,
+                                                 xPars.fNccThresh, float(xPars.iMinDeltaThresh)),
+                            "BlockMatcherNCC::Configure");
+        if (xPars.bLeftToRight) {  // the plain FP32 matcher is left-to-right
+            EnsureHandle(ct_bm_ncc_create);
+            const ct_ncc_params p{xPars.xDispConfig.iRange, r, 1, xPars.xDispConfig.iMin};
+            Ensure(ct_bm_ncc_configure(m_pHandle, xDevice.iDevice, &f, &p), "BlockMatcherNCC::Configure");
+            Ensure(ct_bm_set_gradient_gate(m_pHandle, xPars.fGradThresh), "BlockMatcherNCC::Configure");
+        }
     }
 
-    /* xImageDisp: UInt8 or UInt16; xImageDebug, when valid, receives the
-     * Single NCC score at the chosen disparity (the build's score output).
-     * With iUseDispInput set, xImageDispInit is the coarse disparity map of
-     * the guided mode (MatcherUseDisparity; see ct_bm_ncc_process); without
-     * it, xImageDispInit is ignored. */
+    /* xImageDisp: UInt16x4 (reference output) or UInt8 / UInt16; xImageDebug,
+     * when valid, receives the Single NCC score of the plain matcher. With
+     * iUseDispInput set, xImageDispInit is the coarse disparity map of the
+     * guided mode (MatcherUseDisparity; see ct_bm_ncc_process); without it,
+     * xImageDispInit is ignored. */
     void Process(_CDeviceSurface& xImageDisp, const _CDeviceSurface& xImageL, const _CDeviceSurface& xImageR,
                  const _CDeviceSurface& xImageDispInit, const _CDeviceSurface& xImageDebug) {
+        if (detail::IsU16x4(xImageDisp)) {
+            if (m_bUseDispInput)
+                throw CError(CT_EINVAL, "BlockMatcherNCC: the guided mode writes the plain maps only");
+            m_xCompat.Process(xImageDisp.C(), xImageL.C(), xImageR.C(), S(), "BlockMatcherNCC::Process");
+            return;
+        }
+        if (!m_pHandle) throw CError(CT_EINVAL, "BlockMatcherNCC: right-to-left writes the UInt16x4 output only");
+        detail::RejectIdThresholds(m_xPars.fNccThresh != 0.f || m_xPars.iMinDeltaThresh != 0, "BlockMatcherNCC");
         if (m_bUseDispInput && !xImageDispInit.IsValid())
             throw CError(CT_EINVAL, "BlockMatcherNCC: iUseDispInput needs xImageDispInit");
         Ensure(ct_bm_ncc_process(m_pHandle, xImageDisp.C(), xImageDebug.C(), xImageL.C(), xImageR.C(),
@@ -464,7 +555,9 @@ public:
     }
 
 private:
+    SParameter m_xPars;
     bool m_bUseDispInput = false;
+    detail::CCompat m_xCompat;
 };
 
 }  // namespace BlockMatcherNCC
@@ -472,9 +565,11 @@ private:
 /* ---- BlockMatcherAW1 (BlockMatcherAW1.h:41-157) ---------------------------- */
 namespace BlockMatcherAW1 {
 
-/* Patch_15x15 / Patch_9x9: the reference's 2-of-4 sub-window scores (not
- * built). Shifted5_7x7: minimum of the 7x7 SAD over the centred window and
- * the windows shifted by +-3 px in x and y, with FP32 sub-pixel refinement. */
+/* Patch_15x15 / Patch_9x9: the reference's centre + best 2 of 4 sub-window
+ * score (5 x 5 / 3 x 3 sub-windows) with its gates and IDs, written as the
+ * UInt16x4 output or its x channel into UInt16 (CT_COMPAT_AW1).
+ * Shifted5_7x7: minimum of the 7x7 SAD over the centred window and the
+ * windows shifted by +-3 px in x and y, with FP32 sub-pixel refinement. */
 enum class EConfig { Patch_15x15 = 0, Patch_9x9, Shifted5_7x7 };
 enum class ESimType { AbsoluteDifference = 0, SignedProduct };
 
@@ -508,25 +603,40 @@ public:
     void Configure(const CDevice& xDevice, const SImageFormat& xFormat, const SParameter& xPars) {
         detail::RequireInputFormat(xFormat, "BlockMatcherAW1");
         detail::RequireDispConfig(xPars.xDispConfig, "BlockMatcherAW1");
-        if (xPars.eConfig != EConfig::Shifted5_7x7)
-            throw CError(CT_EINVAL, "BlockMatcherAW1: only EConfig::Shifted5_7x7 is built");
-        if (xPars.eSimType != ESimType::AbsoluteDifference)
-            throw CError(CT_EINVAL, "BlockMatcherAW1: only ESimType::AbsoluteDifference is built");
-        if (xPars.fGradThresh > 0.f) throw CError(CT_EINVAL, "BlockMatcherAW1: the gradient gate is not built");
-        detail::RejectIdThresholds(xPars.fSimThresh != 0.f || xPars.fMinDeltaThresh != 0.f, "BlockMatcherAW1");
+        m_xPars = xPars;
         m_bUseDispInput = xPars.iUseDispInput != 0;
-        EnsureHandle(ct_bm_aw_create);
         const ct_format f = xFormat.ToC();
+        if (xPars.eConfig != EConfig::Shifted5_7x7) {
+            if (m_bUseDispInput) throw CError(CT_EINVAL, "BlockMatcherAW1: the guided mode is built for Shifted5_7x7");
+            m_xCompat.Configure(
+                xDevice.iDevice, f,
+                detail::CompatParams(CT_COMPAT_AW1, xPars.xDispConfig.iRange, xPars.xDispConfig.iMin,
+                                     xPars.eConfig == EConfig::Patch_15x15 ? 5 : 3,
+                                     xPars.eSimType == ESimType::SignedProduct ? 1 : 0, xPars.bLeftToRight,
+                                     xPars.fGradThresh, xPars.fSimThresh, xPars.fMinDeltaThresh),
+                "BlockMatcherAW1::Configure");
+            return;
+        }
+        if (xPars.eSimType != ESimType::AbsoluteDifference)
+            throw CError(CT_EINVAL, "BlockMatcherAW1: Shifted5_7x7 is an absolute-difference cost");
+        detail::RejectIdThresholds(xPars.fSimThresh != 0.f || xPars.fMinDeltaThresh != 0.f, "BlockMatcherAW1");
+        EnsureHandle(ct_bm_aw_create);
         const ct_aw_params p{xPars.xDispConfig.iRange, xPars.bLeftToRight ? 1 : 0, xPars.xDispConfig.iMin, 0};
         Ensure(ct_bm_aw_configure(m_pHandle, xDevice.iDevice, &f, &p), "BlockMatcherAW1::Configure");
+        Ensure(ct_bm_set_gradient_gate(m_pHandle, xPars.fGradThresh), "BlockMatcherAW1::Configure");
     }
 
-    /* xImageDisp: Single (sub-pixel, -1 invalid) or UInt8 / UInt16 (integer
-     * winner-take-all). With iUseDispInput set, xImageDispInit is the coarse
-     * map of the guided mode (ct_bm_aw_process_guided); without it, it is
-     * ignored. xImageDebug is unused. */
+    /* Patch_15x15 / Patch_9x9: xImageDisp UInt16x4 (reference output) or
+     * UInt16 (its x channel). Shifted5_7x7: Single (sub-pixel, -1 invalid) or
+     * UInt8 / UInt16 (integer winner-take-all); with iUseDispInput set,
+     * xImageDispInit is the coarse map of the guided mode
+     * (ct_bm_aw_process_guided). xImageDebug is unused. */
     void Process(_CDeviceSurface& xImageDisp, const _CDeviceSurface& xImageL, const _CDeviceSurface& xImageR,
                  const _CDeviceSurface& xImageDispInit, const _CDeviceSurface& /*xImageDebug*/) {
+        if (m_xPars.eConfig != EConfig::Shifted5_7x7) {
+            m_xCompat.Process(xImageDisp.C(), xImageL.C(), xImageR.C(), S(), "BlockMatcherAW1::Process");
+            return;
+        }
         if (!m_bUseDispInput) {
             Ensure(ct_bm_aw_process(m_pHandle, xImageDisp.C(), xImageL.C(), xImageR.C(), S()),
                    "BlockMatcherAW1::Process");
@@ -541,10 +651,132 @@ public:
     }
 
 private:
+    SParameter m_xPars;
     bool m_bUseDispInput = false;
+    detail::CCompat m_xCompat;
 };
 
 }  // namespace BlockMatcherAW1
+
+/* ---- BlockMatcherAW2 (BlockMatcherAW2.h:41-135) ---------------------------- */
+namespace BlockMatcherAW2 {
+
+/* Centre + 2 lowest of 4 sub-window SADs (5 x 5 / 3 x 3 sub-windows),
+ * scanned from the largest disparity (CT_COMPAT_AW2). The reference centres
+ * its range on iOffset (x_R = x - iOffset - iDispRange / 2 + idx,
+ * BlockMatcherAW2.cu:539); here iOffset is the smallest disparity and the
+ * range never goes below 0. */
+enum class EConfig { Patch_15x15 = 0, Patch_9x9 };
+
+struct SParameter {
+    int iOffset = 0;
+    int iDispRange = 0;
+    int iMinDeltaThresh = 0;
+    float fSadThresh = 0.f;
+    float fGradThresh = 0.f;
+    int iUseDispInput = 0;
+    EConfig eConfig = EConfig::Patch_9x9;
+
+    void Set(int _iOffset, int _iDispRange, int _iMinDeltaThresh, float _fSadThresh, float _fGradThresh,
+             int _iUseDispInput, EConfig _eConfig) {
+        iOffset = _iOffset;
+        iDispRange = _iDispRange;
+        iMinDeltaThresh = _iMinDeltaThresh;
+        fSadThresh = _fSadThresh;
+        fGradThresh = _fGradThresh;
+        iUseDispInput = _iUseDispInput;
+        eConfig = _eConfig;
+    }
+};
+
+class CDriver : public CKernelDriverBase {
+public:
+    CDriver() : CKernelDriverBase("Block Matcher Adaptive Window 2") {}
+
+    void Configure(const CDevice& xDevice, const SImageFormat& xFormat, const SParameter& xPars) {
+        detail::RequireInputFormat(xFormat, "BlockMatcherAW2");
+        if (xPars.iOffset < 0) throw CError(CT_EINVAL, "BlockMatcherAW2: iOffset must be >= 0");
+        if (xPars.iUseDispInput) throw CError(CT_EINVAL, "BlockMatcherAW2: the guided mode is not built");
+        m_xCompat.Configure(xDevice.iDevice, xFormat.ToC(),
+                            detail::CompatParams(CT_COMPAT_AW2, xPars.iDispRange, xPars.iOffset,
+                                                 xPars.eConfig == EConfig::Patch_15x15 ? 5 : 3, 0, true,
+                                                 xPars.fGradThresh, xPars.fSadThresh, float(xPars.iMinDeltaThresh)),
+                            "BlockMatcherAW2::Configure");
+    }
+
+    /* xImageDisp: UInt16x4 (reference output) or UInt16 (its x channel). */
+    void Process(_CDeviceSurface& xImageDisp, const _CDeviceSurface& xImageL, const _CDeviceSurface& xImageR,
+                 const _CDeviceSurface& /*xImageDispInit*/ = _CDeviceSurface()) {
+        m_xCompat.Process(xImageDisp.C(), xImageL.C(), xImageR.C(), S(), "BlockMatcherAW2::Process");
+    }
+
+private:
+    detail::CCompat m_xCompat;
+};
+
+}  // namespace BlockMatcherAW2
+
+/* ---- BlockMatcher1 (BlockMatcher1.h:41-190) -------------------------------- */
+namespace BlockMatcher1 {
+
+/* Plain P x P window of (255 - |a - b|) >> 1 (AbsoluteDifference) or the
+ * signed product x 127 (SignedProduct), argmax with the reference's scan
+ * bookkeeping, gates and IDs (CT_COMPAT_BM1). */
+enum class EConfig { Patch_5x5 = 0, Patch_9x9, Patch_11x11, Patch_15x15 };
+enum class ESimType { AbsoluteDifference = 0, SignedProduct };
+
+struct SParameter {
+    _SDisparityConfig xDispConfig;
+    float fMinDeltaThresh = 0.f;
+    float fSimThresh = 0.f;
+    float fGradThresh = 0.f;
+    int iUseDispInput = 0;
+    EConfig eConfig = EConfig::Patch_9x9;
+    ESimType eSimType = ESimType::AbsoluteDifference;
+    bool bLeftToRight = true;
+
+    void Set(const _SDisparityConfig& _xDispConfig, float _fMinDeltaThresh, float _fSimThresh, float _fGradThresh,
+             int _iUseDispInput, bool _bLeftToRight, EConfig _eConfig, ESimType _eSimType) {
+        xDispConfig = _xDispConfig;
+        fMinDeltaThresh = _fMinDeltaThresh;
+        fSimThresh = _fSimThresh;
+        fGradThresh = _fGradThresh;
+        iUseDispInput = _iUseDispInput;
+        bLeftToRight = _bLeftToRight;
+        eConfig = _eConfig;
+        eSimType = _eSimType;
+    }
+};
+
+class CDriver : public CKernelDriverBase {
+public:
+    CDriver() : CKernelDriverBase("Block Matcher 1") {}
+
+    void Configure(const CDevice& xDevice, const SImageFormat& xFormat, const SParameter& xPars) {
+        detail::RequireInputFormat(xFormat, "BlockMatcher1");
+        detail::RequireDispConfig(xPars.xDispConfig, "BlockMatcher1");
+        if (xPars.iUseDispInput) throw CError(CT_EINVAL, "BlockMatcher1: the guided mode is not built");
+        static const int32_t patch[] = {5, 9, 11, 15};
+        m_xCompat.Configure(xDevice.iDevice, xFormat.ToC(),
+                            detail::CompatParams(CT_COMPAT_BM1, xPars.xDispConfig.iRange, xPars.xDispConfig.iMin,
+                                                 patch[static_cast<int>(xPars.eConfig)],
+                                                 xPars.eSimType == ESimType::SignedProduct ? 1 : 0, xPars.bLeftToRight,
+                                                 xPars.fGradThresh, xPars.fSimThresh, xPars.fMinDeltaThresh),
+                            "BlockMatcher1::Configure");
+    }
+
+    /* xImageDisp: UInt16x4 (reference output) or UInt16 (its x channel). */
+    void Process(_CDeviceSurface& xImageDisp, const _CDeviceSurface& xImageL, const _CDeviceSurface& xImageR,
+                 const _CDeviceSurface& /*xImageDispInit*/ = _CDeviceSurface(),
+                 const _CDeviceSurface& /*xImageDebug*/ = _CDeviceSurface()) {
+        m_xCompat.Process(xImageDisp.C(), xImageL.C(), xImageR.C(), S(), "BlockMatcher1::Process");
+    }
+
+private:
+    detail::CCompat m_xCompat;
+};
+
+}  // namespace BlockMatcher1
 
 /* ---- CrossCheckDisparityMaps (CrossCheckDisparityMaps.h:38-117) ------------- */
 namespace CrossCheckDisparityMaps {

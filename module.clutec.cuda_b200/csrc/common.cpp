@@ -48,6 +48,7 @@ size_t pix_size(int32_t type) {
         case CT_PIX_F32: return 4;
         case CT_PIX_RGBA8: return 4;
         case CT_PIX_F32X4: return 16;
+        case CT_PIX_U16X4: return 8;
         default: return 0;
     }
 }
@@ -165,6 +166,16 @@ const char* ct_version(void) { return "ctstereo 0.1.0 sm_100a"; }
 int ct_destroy(ct_handle* h) {
     ct::clear_error();
     delete h;
+    return CT_OK;
+}
+
+int ct_bm_set_gradient_gate(ct_handle* h, float grad_thresh) {
+    ct::clear_error();
+    if (!h) return ct::fail(CT_EINVAL, "null handle");
+    if (h->kind != ct::Kind::BmSad && h->kind != ct::Kind::BmNcc && h->kind != ct::Kind::BmAw)
+        return ct::fail(CT_ESTATE, "the gradient gate belongs to the SAD, NCC and AW matchers");
+    if (!(grad_thresh >= 0.0f)) return ct::fail(CT_EINVAL, "grad_thresh must be >= 0");
+    h->grad_thresh = grad_thresh;
     return CT_OK;
 }
 

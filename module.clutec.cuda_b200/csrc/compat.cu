@@ -1,0 +1,520 @@
+// compat.cu — the reference matchers' own output: BlockMatcherSAD1, NCC, AW1,
+// AW2 and BlockMatcher1 with their 4 x uint16 TPixelEx pixel
+//   x = disparity + EDisparityId::First, or Saturated / NotFound /
+//       NotSpecific / CannotEvaluate / Unknown,
+//   y = the winning score (SAD / N, uint8-quantised NCC, or the AW / BM
+//       similarity as a 16-bit percentage),
+//   z, w = the specificity channels: how far the scores next to the winner
+//       fall from it, as the reference's sequential scan records them,
+// the gradient gates (fGradThresh -> CannotEvaluate), the score thresholds
+// (fSadThresh / fNccThresh / fSimThresh -> NotFound) and the minimum-delta
+// thresholds (-> NotSpecific).
+//
+// Those channels come from a scan over the disparities in the reference's
+// order (NCC, AW1, BM1: ascending from xDispConfig.Min(); SAD1, AW2: from the
+// largest disparity down, SAD1 first in steps of 4 and then finely around
+// its winner), so here one thread owns one pixel and walks the disparities
+// in that order, keeping the reference's scan state in registers
+// (SSimStore, BlockMatcherNCC.cu:115-131; SAD1's ushort4 min range,
+// BlockMatcherSAD1.cu:158-190). A CTA owns a 32 x 8 pixel tile: its base
+// region and the match strip every disparity of the scan reads are staged in
+// shared memory once; per disparity the CTA writes the per-pixel similarity
+// of the region into shared memory and forms the window sums in two
+// separable passes (vertical, then horizontal; for the adaptive windows
+// first the sub-window sums, then the centre + best / lowest 2 of 4
+// neighbourhood of Kernel.Algo.AdaptWnd_W32H16.h:240-285 and
+// Kernel.Algo.AdaptWnd3D.h:244-300).
+//
+// Pixels whose patch leaves the image get (CannotEvaluate, 0, 0, 0) (the
+// reference leaves them unwritten); a disparity is searched iff the matched
+// patch is inside the image. Float steps use IEEE-rounded intrinsics in the
+// reference's operation order, without contraction, so results are
+// bit-exact against the CPU restatement.
+#include "ct_internal.h"
+#include "ct_device.cuh"
+
+namespace ct {
+namespace compat {
+
+constexpr int kTX = 32, kTY = 8, kNT = kTX * kTY;
+constexpr int kPMax = 16;                  // largest patch side (SAD1 Patch_16x16)
+constexpr int kRW = kTX + kPMax;           // staged base columns (one extra for the gradient)
+constexpr int kRH = kTY + kPMax - 1;       // staged rows
+constexpr int kMW = kTX + kPMax - 1 + 255; // staged match columns (region + D - 1)
+constexpr int kSubMax = 5;                 // AW sub-window side (Patch_15x15)
+
+enum Method { kSad1 = CT_COMPAT_SAD1, kNcc = CT_COMPAT_NCC, kAw1 = CT_COMPAT_AW1, kAw2 = CT_COMPAT_AW2,
+              kBm1 = CT_COMPAT_BM1 };
+
+struct Args {
+    int W, H, D, dmin, P, s, sim_type, dir;
+    float grad_t, score_t, delta_t;
+    const uint8_t* B;  // base image
+    const uint8_t* M;  // match image
+    size_t pb, pm;
+    const int32_t* mS;   // NCC: box sums of the match image (W * H), and of its squares
+    const int32_t* mQ;
+    void* out;
+    size_t out_pitch;
+    int out_type;
+};
+
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float i2f(int v) { return __int2float_rn(v); }
+
+// EvalSim SSimType_SignedProduct (BlockMatcherAW1.cu:209-218 scale 255,
+// BlockMatcher1.cu:201-210 scale 127), truncated.
+__device__ __forceinline__ int signed_product(int p, int q, float scale) {
+    float f1 = fmul(2.0f, fsub(fdiv(i2f(p), 255.0f), 0.5f));
+    const float f2 = fmul(2.0f, fsub(fdiv(i2f(q), 255.0f), 0.5f));
+    f1 = fmul(f1, f2);
+    f1 = fmul(f1, scale);
+    return __float2int_rz(f1);
+}
+
+// SimValueToFloat / SimFloatToInteger (BlockMatcherAW1.cu:155-176).
+__device__ __forceinline__ float sim_to_float(int v, int n) {
+    return fmul(fdiv(i2f(v), i2f(n)), fdiv(100.0f, 255.0f));
+}
+__device__ __forceinline__ uint16_t sim_to_u16(float f) {
+    float t = fdiv(fadd(fdiv(f, 100.0f), 1.0f), 2.0f);
+    t = fminf(fmaxf(t, 0.0f), 1.0f);
+    return uint16_t(__float2uint_rz(fmul(t, 65535.0f)));
+}
+
+__device__ __forceinline__ void store4(const Args& a, int x, int y, uint16_t c0, uint16_t c1, uint16_t c2,
+                                       uint16_t c3) {
+    char* row = static_cast<char*>(a.out) + (size_t)y * a.out_pitch;
+    if (a.out_type == CT_PIX_U16X4)
+        reinterpret_cast<ushort4*>(row)[x] = make_ushort4(c0, c1, c2, c3);
+    else
+        reinterpret_cast<uint16_t*>(row)[x] = c0;
+}
+
+template <int METHOD>
+__global__ void __launch_bounds__(kNT) compat_kernel(Args a) {
+    constexpr bool AW = METHOD == kAw1 || METHOD == kAw2;
+    constexpr bool SIM = METHOD == kNcc || METHOD == kAw1 || METHOD == kBm1;  // argmax scan
+    __shared__ uint8_t sB[kRH][kRW + 4];
+    __shared__ uint8_t sM[kRH][kMW + 1];
+    __shared__ int32_t sE[kRH][kRW];
+    __shared__ int32_t sV[kTY + 2 * kSubMax][kRW];
+    __shared__ int32_t sS[AW ? kTY + 2 * kSubMax : 1][AW ? kTX + 2 * kSubMax : 1];
+
+    const int tid = threadIdx.x, tx = tid % kTX, ty = tid / kTX;
+    const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
+    const int x = x0 + tx, y = y0 + ty;
+    const int P = a.P, s = a.s, pa = P / 2, pb = P - 1 - pa;
+    const int RWc = kTX + P - 1, RHc = kTY + P - 1;
+    const int rx0 = x0 - pa, ry0 = y0 - pa;
+    const int dmax = a.dmin + a.D - 1;
+    const int mx0 = a.dir ? rx0 - dmax : rx0 + a.dmin;  // first staged match column
+    const int MWc = RWc + a.D - 1;
+
+    // stage the base region (one extra column for the gradient) and the match strip
+    for (int i = tid; i < RHc * (RWc + 1); i += kNT) {
+        const int r = i / (RWc + 1), c = i % (RWc + 1);
+        const int xx = rx0 + c, yy = ry0 + r;
+        sB[r][c] = (xx >= 0 && xx < a.W && yy >= 0 && yy < a.H) ? a.B[(size_t)yy * a.pb + xx] : 0;
+    }
+    for (int i = tid; i < RHc * MWc; i += kNT) {
+        const int r = i / MWc, c = i % MWc;
+        const int xx = mx0 + c, yy = ry0 + r;
+        sM[r][c] = (xx >= 0 && xx < a.W && yy >= 0 && yy < a.H) ? a.M[(size_t)yy * a.pm + xx] : 0;
+    }
+    __syncthreads();
+
+    const bool valid = x - pa >= 0 && x + pb < a.W && y - pa >= 0 && y + pb < a.H;
+    const int n_eff = AW ? 3 * s * s : P * P;  // BasePatchElementCount
+
+    // ---- gradient gate (once per pixel, directly from the staged base) ----
+    bool gated = false;
+    if (valid && a.grad_t > 0.0f) {
+        if (METHOD == kSad1 || METHOD == kNcc) {  // mean |I(x) - I(x+1)| (SAD1.cu:226-249, NCC.cu:388-413)
+            int g = 0;
+            for (int r = 0; r < P; ++r)
+                for (int c = 0; c < P; ++c) g += abs(int(sB[ty + r][tx + c]) - int(sB[ty + r][tx + c + 1]));
+            gated = fdiv(i2f(g), i2f(P * P)) < a.grad_t;
+        } else if (METHOD == kBm1 || METHOD == kAw1) {  // std. dev. in % (BM1.cu:327-364, AW1.cu:331-417)
+            int sm = 0, sq = 0;
+            for (int r = 0; r < P; ++r)
+                for (int c = 0; c < P; ++c) {
+                    const int v = sB[ty + r][tx + c];
+                    sm += v;
+                    sq += v * v;
+                }
+            const float fm = fdiv(i2f(sm), i2f(P * P)), fm2 = fdiv(i2f(sq), i2f(P * P));
+            float sd = __fsqrt_rn(fabsf(fsub(fm2, fmul(fm, fm))));
+            if (METHOD == kAw1) sd = fmul(fdiv(i2f(__float2int_rz(sd)), 255.0f), 100.0f);  // stored as int first
+            else sd = fmul(fdiv(sd, 255.0f), 100.0f);
+            gated = sd < a.grad_t;
+        } else {  // AW2: centre + 2 lowest of 4 gradient sub-sums (AW2.cu:216-247)
+            auto sub = [&](int cx, int cy) {  // sub-window centred at region (cx, cy)
+                int g = 0;
+                for (int r = -s / 2; r <= s / 2; ++r)
+                    for (int c = -s / 2; c <= s / 2; ++c)
+                        g += abs(int(sB[cy + r][cx + c]) - int(sB[cy + r][cx + c + 1]));
+                return g;
+            };
+            const int cx = tx + pa, cy = ty + pa;
+            const int e1 = sub(cx - s, cy), e2 = sub(cx, cy + s), e3 = sub(cx + s, cy);
+            int m1 = sub(cx, cy - s), m2 = 0x7FFFFFFF;  // OrderedInsert (min): the two smallest
+            m2 = min(m2, max(m1, e1)); m1 = min(m1, e1);
+            m2 = min(m2, max(m1, e2)); m1 = min(m1, e2);
+            m2 = min(m2, max(m1, e3)); m1 = min(m1, e3);
+            gated = fdiv(i2f(sub(cx, cy) + m1 + m2), i2f(n_eff)) < a.grad_t;
+        }
+    }
+
+    // ---- NCC base statistics (EvalMsd, NCC.cu:339-373) ----
+    float bMean = 0.f, bStd = 0.f;
+    if (METHOD == kNcc && valid) {
+        int sm = 0, sq = 0;
+        for (int r = 0; r < P; ++r)
+            for (int c = 0; c < P; ++c) {
+                const int v = sB[ty + r][tx + c];
+                sm += v;
+                sq += v * v;
+            }
+        bMean = fdiv(i2f(sm), i2f(P * P));
+        bStd = __fsqrt_rn(fsub(fdiv(i2f(sq), i2f(P * P)), fmul(bMean, bMean)));
+    }
+
+    // ---- scan state ----
+    uint16_t disp = gated ? uint16_t(CT_DISP_CANNOT_EVALUATE) : uint16_t(CT_DISP_UNKNOWN);
+    int sPrev2 = 0, sPrev = 0, sMax = METHOD == kNcc ? 0 : -32767, sNext = 0, sNext2 = 0, sLast = 0;  // SIM
+    int mX = 0xFFFF, mY = 0, mZ = 0, mW = 0;                                                        // min range
+    // largest searchable disparity for this pixel
+    const int dlim = a.dir ? x - pa : a.W - 1 - pb - x;
+
+    const int nsteps = METHOD == kSad1 ? (a.D + 3) / 4 + a.D : a.D;
+    for (int k = 0; k < nsteps; ++k) {
+        int idx, inc = 1;
+        bool fine = false;
+        if (METHOD == kSad1) {
+            const int nc = (a.D + 3) / 4;
+            if (k < nc) { idx = 4 * k; inc = 4; }
+            else { idx = k - nc; fine = true; }
+        } else {
+            idx = k;
+        }
+        const int d = SIM ? a.dmin + idx : dmax - idx;
+        const int moff = a.dir ? dmax - d : d - a.dmin;  // strip column of region column 0
+
+        // per-pixel similarity of the region at disparity d
+        for (int i = tid; i < RHc * RWc; i += kNT) {
+            const int r = i / RWc, c = i % RWc;
+            const int p = sB[r][c], q = sM[r][c + moff];
+            int v;
+            if (METHOD == kSad1 || METHOD == kAw2) v = abs(p - q);
+            else if (METHOD == kNcc) v = p * q;
+            else if (METHOD == kAw1) v = a.sim_type ? signed_product(p, q, 255.0f) : 255 - abs(p - q);
+            else v = a.sim_type ? signed_product(p, q, 127.0f) : (255 - abs(p - q)) >> 1;
+            sE[r][c] = v;
+        }
+        __syncthreads();
+        int S;
+        if (!AW) {
+            for (int i = tid; i < kTY * RWc; i += kNT) {
+                const int r = i / RWc, c = i % RWc;
+                int t = 0;
+                for (int q = 0; q < P; ++q) t += sE[r + q][c];
+                sV[r][c] = t;
+            }
+            __syncthreads();
+            S = 0;
+            for (int q = 0; q < P; ++q) S += sV[ty][tx + q];
+        } else {
+            const int SR = kTY + 2 * s, SC = kTX + 2 * s;
+            for (int i = tid; i < SR * RWc; i += kNT) {
+                const int r = i / RWc, c = i % RWc;
+                int t = 0;
+                for (int q = 0; q < s; ++q) t += sE[r + q][c];
+                sV[r][c] = t;
+            }
+            __syncthreads();
+            for (int i = tid; i < SR * SC; i += kNT) {
+                const int r = i / SC, c = i % SC;
+                int t = 0;
+                for (int q = 0; q < s; ++q) t += sV[r][c + q];
+                sS[r][c] = t;
+            }
+            __syncthreads();
+            const int C = sS[ty + s][tx + s];
+            const int e0 = sS[ty][tx + s], e1 = sS[ty + s][tx], e2 = sS[ty + 2 * s][tx + s], e3 = sS[ty + s][tx + 2 * s];
+            if (METHOD == kAw1) {  // OrderedInsertMax: the two largest
+                int m1 = e0, m2 = -32767;
+                m2 = max(m2, min(m1, e1)); m1 = max(m1, e1);
+                m2 = max(m2, min(m1, e2)); m1 = max(m1, e2);
+                m2 = max(m2, min(m1, e3)); m1 = max(m1, e3);
+                S = C + m1 + m2;
+            } else {  // OrderedInsert (min): the two smallest
+                int m1 = e0, m2 = 0x7FFFFFFF;
+                m2 = min(m2, max(m1, e1)); m1 = min(m1, e1);
+                m2 = min(m2, max(m1, e2)); m1 = min(m1, e2);
+                m2 = min(m2, max(m1, e3)); m1 = min(m1, e3);
+                S = C + m1 + m2;
+            }
+        }
+
+        if (valid && d <= dlim) {
+            if (SIM) {
+                int v;
+                if (METHOD == kNcc) {  // uint8-quantised NCC (NCC.cu:218-271)
+                    const int xm = a.dir ? x - d : x + d;
+                    const size_t om = (size_t)y * a.W + xm;
+                    const float fCross = fdiv(i2f(S), i2f(P * P));
+                    const float fTm = fdiv(i2f(__ldg(&a.mS[om])), i2f(P * P));
+                    const float fTm2 = fdiv(i2f(__ldg(&a.mQ[om])), i2f(P * P));
+                    const float fTstd = __fsqrt_rn(fsub(fTm2, fmul(fTm, fTm)));
+                    const float fNorm = fmul(bStd, fTstd);
+                    float fNcc = fNorm < 1.0f ? 0.0f : fdiv(fsub(fCross, fmul(bMean, fTm)), fNorm);
+                    fNcc = fNcc > 0.0f ? fNcc : 0.0f;
+                    v = int(__float2uint_rz(fminf(255.0f, fmul(fNcc, 255.0f))) & 0xFFu);
+                } else {
+                    v = int(int16_t(S));
+                }
+                // EvalSim's bookkeeping (NCC.cu:296-329, AW1.cu:272-307, BM1.cu:262-300)
+                if (disp <= CT_DISP_LAST) {
+                    const int code = d + CT_DISP_FIRST;
+                    const bool above = v > sMax;
+                    const bool jb = !above && int(disp) + 1 == code;
+                    const bool j2b = !above && int(disp) + 2 == code;
+                    if (above) {
+                        sPrev2 = sPrev; sPrev = sLast; sMax = v; sNext = v; sNext2 = v;
+                        disp = uint16_t(code);
+                    }
+                    if (jb) sNext = v;
+                    if (j2b) sNext2 = v;
+                    sLast = v;
+                }
+            } else {
+                // SAD1 EvalSAD (SAD1.cu:158-190), AW2 UpdateDisp (AW2.cu:143-200)
+                const bool eval = !fine || (idx + 4 >= int(disp) && idx <= int(disp) + 4);
+                const bool skip = METHOD == kAw2 ? disp > CT_DISP_LAST : disp == CT_DISP_CANNOT_EVALUATE;
+                if (eval && !skip) {
+                    const int v = S;
+                    const float fmin = fdiv(i2f(v), i2f(n_eff));
+                    if (idx == 0) {
+                        mW = v; mY = v;
+                        if (METHOD == kAw2) mZ = v;
+                    }
+                    const bool below = v < mX && fmin < a.score_t;
+                    if (below) {
+                        mY = mW; mX = v; mZ = v;
+                        disp = uint16_t(idx);
+                    } else if (int(disp) + inc == idx) {
+                        mZ = v;
+                    }
+                    mW = v;
+                }
+            }
+        }
+        __syncthreads();  // the next disparity overwrites sE / sV / sS
+    }
+
+    if (x >= a.W || y >= a.H) return;
+    if (!valid) {
+        store4(a, x, y, CT_DISP_CANNOT_EVALUATE, 0, 0, 0);
+        return;
+    }
+    if (SIM) {
+        if (disp > CT_DISP_LAST || disp == CT_DISP_UNKNOWN) {
+            store4(a, x, y, disp, 0, 0, 0);
+            return;
+        }
+        const int dw = int(disp) - CT_DISP_FIRST;
+        const bool sat = dw <= a.dmin + 1 || dw >= a.dmin + a.D - 1;
+        if (METHOD == kNcc) {  // WriteDisparity (NCC.cu:520-575)
+            const float fNccMax = fdiv(i2f(sMax), 255.0f);
+            const int d1 = max(abs(sPrev - sMax), abs(sPrev2 - sMax));
+            const int d2 = max(abs(sNext - sMax), abs(sNext2 - sMax));
+            const int thr = int(a.delta_t);
+            uint16_t id;
+            if (fNccMax >= a.score_t) id = sat ? CT_DISP_SATURATED : (d1 >= thr && d2 >= thr ? disp : CT_DISP_NOT_SPECIFIC);
+            else id = CT_DISP_NOT_FOUND;
+            store4(a, x, y, id, uint16_t(sMax), uint16_t(d1), uint16_t(d2));
+        } else {  // WriteDisparity (AW1.cu:533-635, BM1.cu:466-565)
+            const float fMax = sim_to_float(sMax, n_eff);
+            const float fp2 = sim_to_float(sPrev2, n_eff), fp = sim_to_float(sPrev, n_eff);
+            const float fn = sim_to_float(sNext, n_eff), fn2 = sim_to_float(sNext2, n_eff);
+            const float fdp = fmaxf(fabsf(fsub(fp, fMax)), fabsf(fsub(fp2, fMax)));
+            const float fdn = fmaxf(fabsf(fsub(fn, fMax)), fabsf(fsub(fn2, fMax)));
+            const bool specific = fdp >= a.delta_t && fdn >= a.delta_t;
+            uint16_t id;
+            if (fMax >= a.score_t) id = sat ? CT_DISP_SATURATED : (specific ? disp : CT_DISP_NOT_SPECIFIC);
+            else id = CT_DISP_NOT_FOUND;
+            store4(a, x, y, id, sim_to_u16(fMax), sim_to_u16(fdp), sim_to_u16(fdn));
+        }
+        return;
+    }
+    if (disp > CT_DISP_LAST) {
+        store4(a, x, y, disp, 0, 0, 0);
+        return;
+    }
+    // SAD1 / AW2 output (SAD1.cu:438-486, AW2.cu:330-370): disp holds the scan
+    // index, compared against First-based bounds as the reference does
+    const float fmin = fdiv(i2f(mX), i2f(n_eff));
+    const int d1 = abs(mY - mX), d2 = abs(mZ - mX);
+    const int c = disp;
+    const bool sat = METHOD == kAw2 ? (c <= CT_DISP_FIRST + 4 || c >= CT_DISP_FIRST + a.D - 4)
+                                    : (c <= CT_DISP_FIRST + 1 || c >= CT_DISP_FIRST + a.D - 1);
+    const int thr = int(a.delta_t);
+    const bool spec = METHOD == kAw2 ? (d1 >= thr && d2 >= thr) : (d1 > thr && d2 > thr);
+    uint16_t id;
+    if (fmin < a.score_t) id = (spec && !sat) ? uint16_t(CT_DISP_FIRST + dmax - c) : (sat ? CT_DISP_SATURATED : CT_DISP_NOT_SPECIFIC);
+    else id = CT_DISP_NOT_FOUND;
+    store4(a, x, y, id, uint16_t(mX / n_eff), uint16_t(d1), uint16_t(d2));
+}
+
+// Box sums S (values) and Q (squares) of every pixel's P x P patch
+// [x - P/2, x - P/2 + P - 1] (0 where the patch leaves the image).
+__global__ void box_sq_kernel(const uint8_t* img, size_t pitch, int W, int H, int P, int32_t* S, int32_t* Q) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W) return;
+    const int pa = P / 2, pb = P - 1 - pa;
+    int s = 0, q = 0;
+    if (x - pa >= 0 && x + pb < W && y - pa >= 0 && y + pb < H) {
+        for (int r = -pa; r <= pb; ++r)
+            for (int c = -pa; c <= pb; ++c) {
+                const int v = img[(size_t)(y + r) * pitch + x + c];
+                s += v;
+                q += v * v;
+            }
+    }
+    S[(size_t)y * W + x] = s;
+    Q[(size_t)y * W + x] = q;
+}
+
+}  // namespace compat
+
+namespace {
+
+struct CompatHandle : ct_handle {
+    CompatHandle() : ct_handle(Kind::Compat) {}
+    ~CompatHandle() override {
+        if (device >= 0) cudaSetDevice(device);
+        cudaFree(stats);
+    }
+    ct_format fmt{};
+    ct_compat_params par{};
+    int32_t* stats = nullptr;  // NCC: S and Q planes of the match image
+};
+
+}  // namespace
+}  // namespace ct
+
+using namespace ct;
+
+extern "C" {
+
+int ct_bm_compat_create(ct_handle** out) {
+    clear_error();
+    if (!out) return fail(CT_EINVAL, "null output handle pointer");
+    *out = new CompatHandle();
+    return CT_OK;
+}
+
+int ct_bm_compat_configure(ct_handle* hh, int32_t device, const ct_format* fmt, const ct_compat_params* p) {
+    clear_error();
+    auto* h = (hh && hh->kind == Kind::Compat) ? static_cast<CompatHandle*>(hh) : nullptr;
+    if (!h) return fail(CT_ESTATE, "not a reference-compat matcher handle");
+    if (!fmt || !p) return fail(CT_EINVAL, "null format or parameters");
+    if (fmt->type != CT_PIX_U8) return fail(CT_ETYPE, "matcher input must be U8 (TPixel_Lum_UInt8)");
+    if (fmt->width < 16 || fmt->height < 16 || fmt->width > 32768 || fmt->height > 32768)
+        return fail(CT_EINVAL, "image size %dx%d out of range (16..32768)", fmt->width, fmt->height);
+    if (p->disp_count < 1 || p->disp_count > 256) return fail(CT_EINVAL, "disp_count must be 1..256");
+    if (p->disp_min < 0 || p->disp_min + p->disp_count > 0xFFEF)
+        return fail(CT_EINVAL, "disp_min must be >= 0 with disp_min + disp_count <= 65519");
+    if (p->sim_type != 0 && p->sim_type != 1) return fail(CT_EINVAL, "sim_type must be 0 or 1");
+    if (p->sim_type && p->method != CT_COMPAT_AW1 && p->method != CT_COMPAT_BM1)
+        return fail(CT_EINVAL, "the signed product is an AW1 / BlockMatcher1 similarity");
+    if (p->reserved[0] || p->reserved[1] || p->reserved[2]) return fail(CT_EINVAL, "reserved fields must be 0");
+    switch (p->method) {
+        case CT_COMPAT_SAD1:
+            if (p->patch < 3 || p->patch > 16) return fail(CT_EINVAL, "SAD1 patch must be 3..16");
+            break;
+        case CT_COMPAT_NCC:
+            if (p->patch != 5 && p->patch != 9 && p->patch != 11)
+                return fail(CT_EINVAL, "NCC patch must be 11 (Patch_11x11), 9 or 5");
+            break;
+        case CT_COMPAT_BM1:
+            if (p->patch != 5 && p->patch != 9 && p->patch != 11 && p->patch != 15)
+                return fail(CT_EINVAL, "BlockMatcher1 patch must be 5, 9, 11 or 15");
+            break;
+        case CT_COMPAT_AW1:
+        case CT_COMPAT_AW2:
+            if (p->patch != 3 && p->patch != 5)
+                return fail(CT_EINVAL, "AW sub-window must be 3 (Patch_9x9) or 5 (Patch_15x15)");
+            break;
+        default:
+            return fail(CT_EINVAL, "unknown method %d", p->method);
+    }
+    if (int rc = use_device(device)) return rc;
+    cudaFree(h->stats);
+    h->stats = nullptr;
+    h->device = device;
+    if (int rc = h->init_status()) return rc;
+    if (p->method == CT_COMPAT_NCC &&
+        cudaMalloc(&h->stats, 2 * (size_t)fmt->width * fmt->height * sizeof(int32_t)) != cudaSuccess)
+        return fail(CT_ENOMEM, "statistics scratch");
+    h->fmt = *fmt;
+    h->par = *p;
+    h->configured = true;
+    return CT_OK;
+}
+
+int ct_bm_compat_process(ct_handle* hh, const ct_image* disp, const ct_image* left, const ct_image* right,
+                         ct_stream stream) {
+    clear_error();
+    auto* h = (hh && hh->kind == Kind::Compat) ? static_cast<CompatHandle*>(hh) : nullptr;
+    if (!h) return fail(CT_ESTATE, "not a reference-compat matcher handle");
+    if (!h->configured) return fail(CT_ESTATE, "process before configure");
+    if (int rc = check_image(left, "left", 1u << CT_PIX_U8)) return rc;
+    if (int rc = check_image(right, "right", 1u << CT_PIX_U8)) return rc;
+    if (int rc = check_same_size(left, right, "left", "right")) return rc;
+    if (left->width != h->fmt.width || left->height != h->fmt.height)
+        return fail(CT_EFORMAT, "image size differs from the configured format");
+    if (int rc = check_image(disp, "disp", (1u << CT_PIX_U16X4) | (1u << CT_PIX_U16))) return rc;
+    if (int rc = check_same_size(disp, left, "disp", "left")) return rc;
+    if (int rc = use_device(h->device)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    h->last_stream = s;
+    const ct_compat_params& p = h->par;
+    const bool aw = p.method == CT_COMPAT_AW1 || p.method == CT_COMPAT_AW2;
+    const ct_image* B = p.left_to_right ? left : right;
+    const ct_image* M = p.left_to_right ? right : left;
+    compat::Args a{};
+    a.W = h->fmt.width; a.H = h->fmt.height; a.D = p.disp_count; a.dmin = p.disp_min;
+    a.s = aw ? p.patch : 0;
+    a.P = aw ? 3 * p.patch : p.patch;
+    a.sim_type = p.sim_type;
+    a.dir = p.left_to_right ? 1 : 0;
+    a.grad_t = p.grad_thresh; a.score_t = p.score_thresh; a.delta_t = p.min_delta_thresh;
+    a.B = static_cast<const uint8_t*>(B->ptr); a.pb = B->pitch_bytes;
+    a.M = static_cast<const uint8_t*>(M->ptr); a.pm = M->pitch_bytes;
+    a.out = disp->ptr; a.out_pitch = disp->pitch_bytes; a.out_type = disp->type;
+    if (p.method == CT_COMPAT_NCC) {
+        const size_t N = (size_t)a.W * a.H;
+        a.mS = h->stats;
+        a.mQ = h->stats + N;
+        compat::box_sq_kernel<<<dim3((a.W + 127) / 128, a.H), 128, 0, s>>>(a.M, a.pm, a.W, a.H, a.P, h->stats,
+                                                                          h->stats + N);
+        CT_LAUNCH_CHECK();
+    }
+    const dim3 grid((a.W + compat::kTX - 1) / compat::kTX, (a.H + compat::kTY - 1) / compat::kTY);
+    switch (p.method) {
+        case CT_COMPAT_SAD1: compat::compat_kernel<CT_COMPAT_SAD1><<<grid, compat::kNT, 0, s>>>(a); break;
+        case CT_COMPAT_NCC: compat::compat_kernel<CT_COMPAT_NCC><<<grid, compat::kNT, 0, s>>>(a); break;
+        case CT_COMPAT_AW1: compat::compat_kernel<CT_COMPAT_AW1><<<grid, compat::kNT, 0, s>>>(a); break;
+        case CT_COMPAT_AW2: compat::compat_kernel<CT_COMPAT_AW2><<<grid, compat::kNT, 0, s>>>(a); break;
+        default: compat::compat_kernel<CT_COMPAT_BM1><<<grid, compat::kNT, 0, s>>>(a); break;
+    }
+    CT_LAUNCH_CHECK();
+    return CT_OK;
+}
+
+}  // extern "C"

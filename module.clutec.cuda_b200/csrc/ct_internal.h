@@ -28,6 +28,7 @@ enum class Kind : int32_t {
     ConfNet = 8,
     Stream = 9,
     Map3D = 10,
+    Compat = 11,
 };
 
 // Sets the thread-local message returned by ct_last_error_string and returns
@@ -61,6 +62,7 @@ struct Handle {
     bool configured = false;
     int32_t* d_status = nullptr;   // one int32 in device memory
     cudaStream_t last_stream = nullptr;
+    float grad_thresh = 0.0f;      // gradient gate of the SAD / NCC / AW matchers (0: off)
     explicit Handle(Kind k) : kind(k) {}
     virtual ~Handle();
     int init_status();             // allocates d_status on the current device
@@ -92,6 +94,12 @@ int make_tmap_nd(CUtensorMap* map, const void* base, CUtensorMapDataType dtype, 
 
 // Device properties cached per device.
 int sm_count(int device);
+
+// Gradient gate on a finished disparity map (gate.cu): kind 0 = mean
+// |I(x) - I(x+1)| over the P x P patch, 1 = standard deviation in percent;
+// gated pixels become "no disparity" (and score 0). thresh <= 0: no-op.
+int gate_launch(const ct_image* disp, const ct_image* score, const ct_image* base, int kind, int P, float thresh,
+                cudaStream_t s);
 
 }  // namespace ct
 

@@ -444,6 +444,7 @@ int launch_ad(AdHandle* h, const ct_image* disp, const ct_image* L, const ct_ima
         ad_match_kernel<R, AW, DIR, false><<<grid, kNT, smem_bytes(a.th, R, AW), s>>>(tb, tm, a);
     }
     CT_LAUNCH_CHECK();
+    const ct_image* base = DIR == 0 ? L : Rimg;
     if (AW) {
         aw_subpixel_kernel<<<dim3((W + 127) / 128, H), 128, 0, s>>>(
             h->keys, W, H, h->D, h->dmin, static_cast<const uint8_t*>(L->ptr), L->pitch_bytes,
@@ -454,7 +455,9 @@ int launch_ad(AdHandle* h, const ct_image* disp, const ct_image* L, const ct_ima
                                                                     disp->pitch_bytes, disp->type, h->dmin);
         CT_LAUNCH_CHECK();
     }
-    return CT_OK;
+    // EvalGrad: SAD1's mean gradient over its window, AW1's standard
+    // deviation over the whole 13 x 13 extent of the five windows
+    return gate_launch(disp, nullptr, base, AW ? 1 : 0, AW ? 2 * EXT + 1 : 2 * R + 1, h->grad_thresh, s);
 }
 
 int configure_ad(AdHandle* h, int32_t device, const ct_format* fmt, int D, int R, int dir, int dmin) {

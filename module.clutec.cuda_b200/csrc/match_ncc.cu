@@ -351,7 +351,7 @@ int launch_ncc(NccHandle* h, const ct_image* disp, const ct_image* score, const 
         ncc_finalize_kernel<<<dim3((W + 255) / 256, H), 256, 0, s>>>(a, R);
         CT_LAUNCH_CHECK();
     }
-    return CT_OK;
+    return gate_launch(disp, score, L, 0, 2 * R + 1, h->grad_thresh, s);  // EvalGrad (NCC.cu:388-413)
 }
 
 }  // namespace

@@ -25,7 +25,8 @@ SYNTH_PATH = _PKG / "libctsynth.so"
 # status codes (ctstereo.h)
 CT_OK, CT_EINVAL, CT_ETYPE, CT_EFORMAT, CT_ECUDA, CT_ETIMEOUT, CT_ESTATE, CT_ENOMEM, CT_EINTERNAL = range(9)
 # pixel types
-CT_PIX_U8, CT_PIX_U16, CT_PIX_U64, CT_PIX_F32, CT_PIX_RGBA8, CT_PIX_F32X4 = 1, 2, 3, 4, 5, 6
+CT_PIX_U8, CT_PIX_U16, CT_PIX_U64, CT_PIX_F32, CT_PIX_RGBA8, CT_PIX_F32X4, CT_PIX_U16X4 = 1, 2, 3, 4, 5, 6, 7
+CT_COMPAT_SAD1, CT_COMPAT_NCC, CT_COMPAT_AW1, CT_COMPAT_AW2, CT_COMPAT_BM1 = 0, 1, 2, 3, 4
 CT_COLOR_ANALYSIS, CT_COLOR_GRAY, CT_COLOR_COLOR, CT_COLOR_DISP_ABS, CT_COLOR_DISP_REL = range(5)
 # EDisparityId codes
 DISP_FIRST, DISP_LAST = 0x0001, 0xFFEF
@@ -75,6 +76,12 @@ class ct_ncc_params(C.Structure):
 class ct_aw_params(C.Structure):
     _fields_ = [("disp_count", C.c_int32), ("left_to_right", C.c_int32), ("disp_min", C.c_int32),
                 ("reserved1", C.c_int32)]
+
+
+class ct_compat_params(C.Structure):
+    _fields_ = [("method", C.c_int32), ("disp_count", C.c_int32), ("disp_min", C.c_int32), ("patch", C.c_int32),
+                ("sim_type", C.c_int32), ("left_to_right", C.c_int32), ("grad_thresh", C.c_float),
+                ("score_thresh", C.c_float), ("min_delta_thresh", C.c_float), ("reserved", C.c_int32 * 3)]
 
 
 class ct_pinhole(C.Structure):
@@ -158,6 +165,10 @@ def _declare(L: C.CDLL) -> None:
         "ct_bm_census_set_tuning": [H, C.c_int32, C.c_int32],
         "ct_bm_census_process_static": [img, img, img, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p],
         "ct_bm_census_static_status": [P(C.c_int32)],
+        "ct_bm_set_gradient_gate": [H, C.c_float],
+        "ct_bm_compat_create": [P(H)],
+        "ct_bm_compat_configure": [H, C.c_int32, fmt, P(ct_compat_params)],
+        "ct_bm_compat_process": [H, img, img, img, C.c_void_p],
         "ct_handle_test_wait_timeout": [H, C.c_uint32, C.c_void_p],
         "ct_curves_pitch": [C.c_int32, P(C.c_size_t)],
         "ct_bm_census_process_curves": [H, img, P(ct_curves), img, img, C.c_void_p],
@@ -299,6 +310,11 @@ class _Driver:
         v = C.c_int32()
         check(lib().ct_handle_device_status(self._h, C.byref(v)))
         return v.value
+
+    def set_gradient_gate(self, grad_thresh: float):
+        """ct_bm_set_gradient_gate (SAD, NCC and AW matchers): pixels whose
+        patch has too little texture get no disparity."""
+        check(lib().ct_bm_set_gradient_gate(self._h, grad_thresh))
 
     def test_wait_timeout(self, poll_limit: int = 1024, stream=None):
         """ct_handle_test_wait_timeout: a bounded device wait that nothing
@@ -467,6 +483,42 @@ def pinhole(fx, fy, cx, cy, rot=None, center=(0.0, 0.0, 0.0)) -> ct_pinhole:
     projection centre in world coordinates."""
     r = [1, 0, 0, 0, 1, 0, 0, 0, 1] if rot is None else [float(v) for row in rot for v in row]
     return ct_pinhole(fx, fy, cx, cy, (C.c_float * 9)(*r), (C.c_float * 3)(*center))
+
+
+def alloc_u16x4(height: int, width: int, device="cuda"):
+    """A (height, width, 4) int16 tensor with a 256-byte aligned row pitch for
+    the reference matchers' 4 x uint16 pixels (BlockMatcherCompat)."""
+    import torch
+    return alloc_image(height, 4 * width, torch.int16, device).unflatten(1, (width, 4))
+
+
+def _u16x4_ref(t):
+    """ct_image of a (H, W, 4) int16 tensor (CT_PIX_U16X4), or of a 2-D U16 map."""
+    if t.dim() == 2:
+        return C.byref(image(t))
+    if t.dim() != 3 or t.shape[2] != 4 or t.stride(2) != 1 or t.stride(1) != 4 or t.element_size() != 2:
+        raise CtError(CT_EINVAL, "4 x uint16 images must be (H, W, 4) 16-bit tensors with packed pixels")
+    return C.byref(ct_image(t.data_ptr(), t.stride(0) * 2, t.shape[1], t.shape[0], CT_PIX_U16X4, 0))
+
+
+class BlockMatcherCompat(_Driver):
+    """The reference matchers' own 4 x uint16 output (ct_bm_compat_*):
+    method CT_COMPAT_SAD1 / NCC / AW1 / AW2 / BM1 with their gates, thresholds
+    and scan bookkeeping; patch = window side (SAD1, NCC, BM1) or sub-window
+    side (AW1, AW2)."""
+    _create = "ct_bm_compat_create"
+
+    def configure(self, device: int, width: int, height: int, method: int, disp_count: int, patch: int,
+                  disp_min: int = 0, sim_type: int = 0, left_to_right: bool = True, grad_thresh: float = 0.0,
+                  score_thresh: float = 0.0, min_delta_thresh: float = 0.0):
+        p = ct_compat_params(method, disp_count, disp_min, patch, sim_type, int(left_to_right), grad_thresh,
+                             score_thresh, min_delta_thresh)
+        check(lib().ct_bm_compat_configure(self._h, device, C.byref(_fmt(width, height)), C.byref(p)))
+
+    def process(self, disp, left, right, stream=None):
+        """disp: alloc_u16x4 tensor (all channels) or a 2-D int16 map (x only)."""
+        check(lib().ct_bm_compat_process(self._h, _u16x4_ref(disp), _img_ref(left), _img_ref(right),
+                                         _stream(stream)))
 
 
 def alloc_map3d(height: int, width: int, device="cuda"):

@@ -61,6 +61,9 @@ def lib() -> C.CDLL:
         _lib.or_match_ncc.argtypes = [vp, vp, i, i, i, i, i, i, vp, vp, vp]
         _lib.or_match_ncc_guided.argtypes = [vp, vp, i, i, i, i, i, i, vp, vp, vp, vp, vp]
         _lib.or_crosscheck.argtypes = [vp, vp, i, i, i, i, vp, vp]
+        f = C.c_float
+        _lib.or_compat_match.argtypes = [vp, vp, i, i, i, i, i, i, i, i, i, f, f, f, vp]
+        _lib.or_gate_mask.argtypes = [vp, i, i, i, i, i, f, vp]
     return _lib
 
 
@@ -387,3 +390,31 @@ def to_u16(disp):
     out = np.where(d >= 0, d + 1, 0xFFFF)
     out = np.where(d == -2, 0xFFFA, out)
     return out.astype(np.uint16)
+
+
+COMPAT_METHODS = {"sad1": 0, "ncc": 1, "aw1": 2, "aw2": 3, "bm1": 4}
+
+
+def compat_match(L, R, method, D, patch, dmin=0, sim_type=0, left_to_right=True, grad_thresh=0.0,
+                 score_thresh=0.0, min_delta_thresh=0.0):
+    """The reference matchers' 4 x uint16 output (oracle/compat.cpp):
+    method in COMPAT_METHODS; patch = window side (SAD1, NCC, BM1) or
+    sub-window side (AW1, AW2). -> (H, W, 4) uint16: x = disparity + 1 or an
+    EDisparityId, y = score, z / w = specificity."""
+    L, R = _u8(L), _u8(R)
+    H, W = L.shape
+    out = np.empty((H, W, 4), np.uint16)
+    lib().or_compat_match(_p(L), _p(R), W, H, W, COMPAT_METHODS[method], D, dmin, patch, sim_type,
+                          1 if left_to_right else 0, grad_thresh, score_thresh, min_delta_thresh, _p(out))
+    return out
+
+
+def gate_mask(img, kind, P, thresh):
+    """Gradient gate of the plain matchers (oracle/compat.cpp or_gate_mask):
+    kind 0 mean |dI/dx| (SAD1, NCC), 1 standard deviation in % (AW1) over
+    the P x P patch -> bool (H, W), True where the pixel is gated."""
+    img = _u8(img)
+    H, W = img.shape
+    m = np.empty((H, W), np.uint8)
+    lib().or_gate_mask(_p(img), W, H, W, kind, P, thresh, _p(m))
+    return m.astype(bool)

@@ -54,21 +54,9 @@ static int RunCpu() {
     CHECK(sad.iDispRange == 64 && sad.eConfig == BlockMatcherSAD1::EConfig::Patch_9x9, "SAD Set");
     {
         BlockMatcherSAD1::SParameter p = sad;
-        p.eConfig = BlockMatcherSAD1::EConfig::Patch_16x16;
         BlockMatcherSAD1::CDriver d;
-        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "SAD Patch_16x16 must be rejected");
-        p = sad;
-        p.fGradThresh = 2.f;
-        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "SAD gradient gate must be rejected");
-        p = sad;
         p.iOffset = -1;
         CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "SAD negative offset must be rejected");
-        p = sad;
-        p.fSadThresh = 30.f;
-        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "SAD fSadThresh must be rejected");
-        p = sad;
-        p.iMinDeltaThresh = 2;
-        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "SAD iMinDeltaThresh must be rejected");
         CHECK(ThrownCode([&] { d.Configure(dev, SImageFormat(320, 120, EDataType::UInt16), sad); }) == CT_ETYPE,
               "SAD UInt16 input must be rejected");
         p = sad;
@@ -84,24 +72,43 @@ static int RunCpu() {
         p.iUseDispInput = 0;
         p.xDispConfig.Set(-1, 128);
         CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "NCC iMin < 0 must be rejected");
-        p.xDispConfig.Set(0, 128);
-        p.fNccThresh = 0.5f;
-        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "NCC fNccThresh must be rejected");
-        p.fNccThresh = 0.f;
-        p.bLeftToRight = false;
-        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "NCC right-to-left must be rejected");
+        p.xDispConfig.Set(0, 300);
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "NCC range 300 must be rejected");
     }
     {
         _SDisparityConfig dc;
         dc.Set(0, 256);
         BlockMatcherAW1::SParameter p;
-        p.Set(dc, 0.f, 0.f, 0.f, 0, true, BlockMatcherAW1::EConfig::Patch_15x15,
+        p.Set(dc, 0.f, 0.f, 0.f, 1, true, BlockMatcherAW1::EConfig::Patch_15x15,
               BlockMatcherAW1::ESimType::AbsoluteDifference);
         BlockMatcherAW1::CDriver d;
-        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "AW1 2-of-4 must be rejected");
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "AW1 2-of-4 guided must be rejected");
+        p.iUseDispInput = 0;
         p.eConfig = BlockMatcherAW1::EConfig::Shifted5_7x7;
         p.eSimType = BlockMatcherAW1::ESimType::SignedProduct;
-        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "AW1 signed product must be rejected");
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "Shifted5_7x7 signed product must be rejected");
+        p.eSimType = BlockMatcherAW1::ESimType::AbsoluteDifference;
+        p.fSimThresh = 50.f;
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "Shifted5_7x7 fSimThresh must be rejected");
+    }
+    {
+        BlockMatcherAW2::SParameter p;
+        p.Set(-2, 64, 0, 30.f, 0.f, 0, BlockMatcherAW2::EConfig::Patch_9x9);
+        BlockMatcherAW2::CDriver d;
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "AW2 negative offset must be rejected");
+        p.Set(0, 64, 0, 30.f, 0.f, 1, BlockMatcherAW2::EConfig::Patch_9x9);
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "AW2 guided mode must be rejected");
+    }
+    {
+        _SDisparityConfig dc;
+        dc.Set(0, 64);
+        BlockMatcher1::SParameter p;
+        p.Set(dc, 0.f, 40.f, 0.f, 1, true, BlockMatcher1::EConfig::Patch_9x9, BlockMatcher1::ESimType::SignedProduct);
+        BlockMatcher1::CDriver d;
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "BM1 guided mode must be rejected");
+        p.iUseDispInput = 0;
+        p.xDispConfig.Set(0, 0);
+        CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "BM1 range 0 must be rejected");
     }
     {
         CrossCheckDisparityMaps::SParameter p;
@@ -214,6 +221,54 @@ static int RunGpu(const char* weights) {
         for (int y = 0; y < H; ++y)
             for (int x = 0; x < W; ++x) bad += interior(x, y, 4) && v[size_t(y) * W + x] != K;
         CHECK(bad == 0, "SAD: %d interior pixels not at d = %d", bad, K);
+    }
+    {  // reference 4 x uint16 output of every driver on the shift: x = K + First
+        const SImageFormat f4(W, H, EDataType::UInt16x4);
+        auto check4 = [&](const char* who, CKernelDriverBase& drv, const std::function<void(CDeviceSurface&)>& run,
+                          int r) {
+            CDeviceSurface out(f4);
+            drv.Begin();
+            run(out);
+            drv.End();
+            auto v = out.CopyInto<uint64_t>();
+            int bad = 0;
+            for (int y = 0; y < H; ++y)
+                for (int x = 0; x < W; ++x)
+                    bad += interior(x, y, r + 1) && (v[size_t(y) * W + x] & 0xFFFF) != uint64_t(K + 1);
+            CHECK(bad == 0, "%s (UInt16x4): %d interior pixels not at d = %d", who, bad, K);
+        };
+        BlockMatcherSAD1::SParameter ps;
+        ps.Set(0, 32, 0, 1000.f, 0.f, BlockMatcherSAD1::EConfig::Patch_16x16);  // the reference's only patch
+        BlockMatcherSAD1::CDriver sad;
+        sad.Configure(dev, fin, ps);
+        check4("SAD1 16x16", sad, [&](CDeviceSurface& o) { sad.Process(o, surfL, surfR); }, 8);
+        CDeviceSurface plain(f16);  // Patch_16x16 has no plain map
+        CHECK(ThrownCode([&] { sad.Process(plain, surfL, surfR); }) == CT_EINVAL, "SAD1 16x16 into UInt16");
+        _SDisparityConfig dc;
+        dc.Set(0, 32);
+        BlockMatcherNCC::SParameter pn;
+        pn.Set(dc, 0, 0.5f, 0.f, 0, true, BlockMatcherNCC::EConfig::Patch_11x11);
+        BlockMatcherNCC::CDriver ncc;
+        ncc.Configure(dev, fin, pn);
+        check4("NCC", ncc, [&](CDeviceSurface& o) { ncc.Process(o, surfL, surfR); }, 5);
+        CHECK(ThrownCode([&] { ncc.Process(plain, surfL, surfR); }) == CT_EINVAL,
+              "fNccThresh on the plain map must be rejected");
+        BlockMatcherAW1::SParameter pa;
+        pa.Set(dc, 0.f, 50.f, 0.f, 0, true, BlockMatcherAW1::EConfig::Patch_15x15,
+               BlockMatcherAW1::ESimType::AbsoluteDifference);
+        BlockMatcherAW1::CDriver aw1;
+        aw1.Configure(dev, fin, pa);
+        check4("AW1 15x15", aw1, [&](CDeviceSurface& o) { aw1.Process(o, surfL, surfR); }, 7);
+        BlockMatcherAW2::SParameter p2;
+        p2.Set(0, 32, 0, 1000.f, 0.f, 0, BlockMatcherAW2::EConfig::Patch_9x9);
+        BlockMatcherAW2::CDriver aw2;
+        aw2.Configure(dev, fin, p2);
+        check4("AW2 9x9", aw2, [&](CDeviceSurface& o) { aw2.Process(o, surfL, surfR); }, 4);
+        BlockMatcher1::SParameter p1;
+        p1.Set(dc, 0.f, 10.f, 0.f, 0, true, BlockMatcher1::EConfig::Patch_9x9, BlockMatcher1::ESimType::SignedProduct);
+        BlockMatcher1::CDriver bm1;
+        bm1.Configure(dev, fin, p1);
+        check4("BM1 9x9", bm1, [&](CDeviceSurface& o) { bm1.Process(o, surfL, surfR); }, 4);
     }
     {  // NCC 11x11, UInt16 + score
         _SDisparityConfig dc;
