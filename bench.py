@@ -61,9 +61,12 @@ def parse():
                     help="census1080 (default, the headline) or another configuration, one JSON line each")
     ap.add_argument("--eval-pairs", type=int, default=None,
                     help="held-out 1080p pairs for the confidence-net AUC (default 4 in the census line, 24 in confnet1080)")
-    ap.add_argument("--profile", default=None, choices=["census_match", "confnet_infer", "pipelines"],
-                    help="for ncu captures on the 1080p D=128 pair, then exit: census_match or confnet_infer = that "
-                         "kernel twice; pipelines = the plain L-R pipeline 3x, then the learned one 3x")
+    ap.add_argument("--profile", default=None,
+                    choices=["census_match", "confnet_infer", "pipelines", "sad640", "ncc1080", "aw1440", "batch64",
+                             "compat_ncc1080"],
+                    help="for ncu captures, then exit: census_match or confnet_infer = that kernel twice on the "
+                         "1080p D=128 pair; pipelines = the plain L-R pipeline 3x, then the learned one 3x; a "
+                         "configuration name = its step twice (no autotuning, no CPU work)")
     ap.add_argument("--no-configs", action="store_true",
                     help="default run: measure the headline only, without the other configurations")
     return ap.parse_args()
@@ -552,11 +555,69 @@ def run_ours(args):
     return 0
 
 
-def run_profile(args):
-    """Two launches of one kernel on the default workload, nothing else (or
-    the two pipelines, three times each)."""
+def profile_config(args):
+    """--profile <configuration>: that configuration's step twice on its own
+    inputs (the sizes the bench measures), nothing else."""
     import torch
     import ctstereo as ct
+    dev = torch.device("cuda", 0)
+
+    def up(a):
+        t = ct.alloc_image(a.shape[0], a.shape[1], torch.from_numpy(a).dtype, dev)
+        t.copy_(torch.from_numpy(a))
+        return t
+
+    wl = args.profile
+    if wl == "batch64":
+        shapes = batch_shapes()
+        pairs = []
+        for i, (W, H, D) in enumerate(shapes):
+            L, R, _, _ = ct.synth_pair(1, 1000 + i, W, H, D - 1)
+            pairs.append((up(L), up(R), ct.alloc_image(H, W, torch.int16, dev)))
+        m = ct.BatchStereo()
+        m.configure(0, shapes, tol=1)
+        step = lambda: m.process(pairs)
+    else:
+        W, H, D, kind = {"sad640": (640, 480, 64, 1), "ncc1080": (1920, 1080, 128, 2), "aw1440": (2560, 1440, 256, 3),
+                         "compat_ncc1080": (1920, 1080, 128, 2)}[wl]
+        L, R, _, _ = ct.synth_pair(kind, SEED, W, H, D - 1)
+        dL, dR = up(L), up(R)
+        if wl == "sad640":
+            m = ct.BlockMatcherSAD1()
+            m.configure(0, W, H, D, radius=4)
+            out = ct.alloc_image(H, W, torch.uint8, dev)
+            step = lambda: m.process(out, dL, dR)
+        elif wl == "ncc1080":
+            m = ct.BlockMatcherNCC()
+            m.configure(0, W, H, D, radius=5)
+            out = ct.alloc_image(H, W, torch.uint8, dev)
+            score = ct.alloc_image(H, W, torch.float32, dev)
+            step = lambda: m.process(out, dL, dR, score=score)
+        elif wl == "aw1440":
+            m = ct.BlockMatcherAW()
+            m.configure(0, W, H, D)
+            out = ct.alloc_image(H, W, torch.float32, dev)
+            step = lambda: m.process(out, dL, dR)
+        else:
+            m = ct.BlockMatcherCompat()
+            m.configure(0, W, H, ct.CT_COMPAT_NCC, D, 11, score_thresh=0.5, min_delta_thresh=2)
+            out = ct.alloc_u16x4(H, W, dev)
+            step = lambda: m.process(out, dL, dR)
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    if m.device_status() != 0:
+        raise RuntimeError("device status set")
+    return 0
+
+
+def run_profile(args):
+    """Two launches of one kernel on the default workload, nothing else (or
+    the two pipelines, three times each, or a configuration's step twice)."""
+    import torch
+    import ctstereo as ct
+    if args.profile not in ("census_match", "confnet_infer", "pipelines"):
+        return profile_config(args)
     dev = torch.device("cuda", 0)
     if args.profile in ("confnet_infer", "pipelines"):
         import confnet_train as T
