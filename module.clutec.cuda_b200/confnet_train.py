@@ -6,8 +6,9 @@ on the pixel's winning disparity, and scores how likely that winner-take-all
 disparity is correct. Everything it
 learns from is produced by the library itself on seeded synthetic pairs:
 
-  * pairs: ct_synth_pair kind 1 (fractal-noise texture, 8 fronto-parallel
-    rectangles over a background, occlusions filled with fresh noise);
+  * pairs: ct_synth_pair kinds 1 and 2 alternating (fractal-noise texture;
+    kind 1: 8 fronto-parallel rectangles over a background, kind 2: 24
+    slanted planes; occlusions filled with fresh noise);
   * cost curves and winner-take-all disparities: ct_bm_census_process_curves;
   * labels: a pixel with a disparity is "correct" iff it is not occluded in
     the right view and |d_wta - d_gt| <= 1 (generator ground truth);
@@ -101,8 +102,21 @@ class _Device:
         return self.disp.cpu().numpy().view(np.uint16)
 
 
-def make_training_set(net, device=0, n_pairs=2000, W=640, H=480, per_pair=2048, seed=0, log=None):
-    """Samples (n, 128) uint8 and labels (n,) uint8 on the GPU."""
+def _mixed_pairs(seeds, W, H, kinds):
+    """Seeded pairs, pair i of generator kind kinds[i % len(kinds)]."""
+    with ThreadPoolExecutor(1) as ex:
+        nxt = lambda k: ex.submit(ct.synth_pair, kinds[k % len(kinds)], int(seeds[k]), W, H, D - 1)  # noqa: E731
+        fut = nxt(0)
+        for k in range(len(seeds)):
+            cur = fut.result()
+            if k + 1 < len(seeds):
+                fut = nxt(k + 1)
+            yield cur
+
+
+def make_training_set(net, device=0, n_pairs=2000, W=640, H=480, per_pair=2048, seed=0, log=None, kinds=(KIND,)):
+    """Samples (n, 128) uint8 and labels (n,) uint8 on the GPU; pair i comes
+    from generator kind kinds[i % len(kinds)]."""
     import torch
     g = _Device(device, W, H)
     rng = np.random.default_rng(seed)
@@ -111,7 +125,7 @@ def make_training_set(net, device=0, n_pairs=2000, W=640, H=480, per_pair=2048, 
     labels = np.empty(n, np.uint8)
     seeds = TRAIN_SEED0 + np.arange(n_pairs)
     t0 = time.perf_counter()
-    for i, (L, R, G, O) in enumerate(_pairs(seeds, W, H)):
+    for i, (L, R, G, O) in enumerate(_mixed_pairs(seeds, W, H, kinds)):
         g.upload(L, R)
         has, correct = _labels(g.curves(), G, O)
         idx = np.flatnonzero(has.ravel())
@@ -233,6 +247,9 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=3e-3)
     ap.add_argument("--eval-pairs", type=int, default=200)
     ap.add_argument("--eval-size", default="1920x1080")
+    ap.add_argument("--kinds", default="1,2",
+                    help="generator kinds of the training pairs, alternating (1: fronto-parallel rectangles, "
+                         "2: slanted planes)")
     ap.add_argument("--out", default=str(WEIGHTS))
     ap.add_argument("--report", default=None, help="write the JSON summary here too")
     a = ap.parse_args(argv)
@@ -243,7 +260,8 @@ def main(argv=None):
     net.configure(a.device, a.batch)
     net.init(1)
     t0 = time.perf_counter()
-    samples, labels = make_training_set(net, a.device, a.train_pairs, tw, th, a.per_pair, log=log)
+    kinds = tuple(int(k) for k in a.kinds.split(","))
+    samples, labels = make_training_set(net, a.device, a.train_pairs, tw, th, a.per_pair, log=log, kinds=kinds)
     t_data = time.perf_counter() - t0
     t0 = time.perf_counter()
     hist = train(net, samples, labels, a.steps, a.batch, a.lr, log=log)
@@ -253,8 +271,10 @@ def main(argv=None):
     untrained = ct.ConfNet()
     untrained.configure(a.device, 16)
     untrained.init(1)
-    res = evaluate({"net": net, "untrained": untrained}, a.device, a.eval_pairs, ew, eh, log=log)
-    summary = {"train_pairs": a.train_pairs, "train_size": a.train_size, "samples": int(samples.shape[0]),
+    res = {f"kind{k}": evaluate({"net": net, "untrained": untrained}, a.device, a.eval_pairs, ew, eh, log=log,
+                                 kind=k) for k in (1, 2)}
+    summary = {"train_pairs": a.train_pairs, "train_kinds": list(kinds), "train_size": a.train_size,
+               "samples": int(samples.shape[0]),
                "positive_fraction": float(labels.float().mean().item()), "steps": a.steps, "batch": a.batch,
                "lr": a.lr, "loss_history": hist, "data_s": round(t_data, 1), "train_s": round(t_train, 1),
                "eval_size": a.eval_size, "auc": res, "weights": str(a.out)}
