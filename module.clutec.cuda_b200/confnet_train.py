@@ -6,9 +6,9 @@ on the pixel's winning disparity, and scores how likely that winner-take-all
 disparity is correct. Everything it
 learns from is produced by the library itself on seeded synthetic pairs:
 
-  * pairs: ct_synth_pair kinds 1 and 2 alternating (fractal-noise texture;
-    kind 1: 8 fronto-parallel rectangles over a background, kind 2: 24
-    slanted planes; occlusions filled with fresh noise);
+  * pairs: ct_synth_pair kind 1 (fractal-noise texture, 8 fronto-parallel
+    rectangles over a background, occlusions filled with fresh noise);
+    --kinds 1,2 alternates it with kind 2 (24 slanted planes);
   * cost curves and winner-take-all disparities: ct_bm_census_process_curves;
   * labels: a pixel with a disparity is "correct" iff it is not occluded in
     the right view and |d_wta - d_gt| <= 1 (generator ground truth);
@@ -247,7 +247,7 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=3e-3)
     ap.add_argument("--eval-pairs", type=int, default=200)
     ap.add_argument("--eval-size", default="1920x1080")
-    ap.add_argument("--kinds", default="1,2",
+    ap.add_argument("--kinds", default="1",
                     help="generator kinds of the training pairs, alternating (1: fronto-parallel rectangles, "
                          "2: slanted planes)")
     ap.add_argument("--out", default=str(WEIGHTS))

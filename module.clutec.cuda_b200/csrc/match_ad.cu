@@ -460,6 +460,24 @@ int launch_ad(AdHandle* h, const ct_image* disp, const ct_image* L, const ct_ima
     return gate_launch(disp, nullptr, base, AW ? 1 : 0, AW ? 2 * EXT + 1 : 2 * R + 1, h->grad_thresh, s);
 }
 
+// Strip height: each SM works through ceil(CTAs / SMs) strips of th + 2 ext
+// staged rows; pick the th in 8 .. 64 that minimises that (small images get
+// enough strips to reach every SM, large ones fewer redundant halo rows).
+int pick_ad_strip_height(int W, int H, int D, int ext, int two, int sms) {
+    const long tiles = long((W + two - 1) / two) * ((D + ad::kDPC - 1) / ad::kDPC);
+    int best = 32;
+    long best_cost = -1;
+    for (int th = 8; th <= 64; th += 2) {
+        const long ctas = tiles * ((H + th - 1) / th);
+        const long cost = (ctas + sms - 1) / sms * long(min(th, H) + 2 * ext);
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = th;
+        }
+    }
+    return best;
+}
+
 int configure_ad(AdHandle* h, int32_t device, const ct_format* fmt, int D, int R, int dir, int dmin) {
     if (fmt->type != CT_PIX_U8) return fail(CT_ETYPE, "matcher input must be U8 (TPixel_Lum_UInt8)");
     if (fmt->width < 16 || fmt->height < 16 || fmt->width > 32768 || fmt->height > 32768)
@@ -484,6 +502,8 @@ int configure_ad(AdHandle* h, int32_t device, const ct_format* fmt, int D, int R
     h->R = R;
     h->dir = dir;
     h->dmin = dmin;
+    const bool aw = h->kind == Kind::BmAw;
+    h->th = pick_ad_strip_height(fmt->width, fmt->height, D, ad::ext_of(R, aw), ad::two_of(R, aw), sm_count(device));
     h->configured = true;
     return CT_OK;
 }

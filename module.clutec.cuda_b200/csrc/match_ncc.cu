@@ -214,6 +214,7 @@ __global__ void __launch_bounds__(kNT, 2)
             // right-view statistics of the 11 match columns this thread's 4
             // columns x 8 disparities read: column xs + 4 lane - dmin - dw - 7 + k
             int syk[kCPT + kDPW - 1], vyk[kCPT + kDPW - 1];
+            float ryk[kCPT + kDPW - 1];  // ~1 / sqrt(vy) of those columns (estimates only)
             {
                 const int cb = xs + 4 * lane - a.dmin - dw - (kDPW - 1);
                 const size_t ob = (size_t)y * a.W;
@@ -222,6 +223,7 @@ __global__ void __launch_bounds__(kNT, 2)
                     const bool in = cb + k >= 0 && cb + k < a.W;
                     syk[k] = in ? __ldg(&a.Sy[ob + cb + k]) : 0;
                     vyk[k] = in ? __ldg(&a.Vy[ob + cb + k]) : 0;
+                    ryk[k] = rsqrtf(__int2float_rn(vyk[k]));
                 }
             }
 #pragma unroll
@@ -240,18 +242,33 @@ __global__ void __launch_bounds__(kNT, 2)
                     ghi = min(int(g >> 16), a.D - 1);
                 }
                 unsigned long long best = 0ull;
+                // The IEEE score (a divide and a square root) is evaluated
+                // only for a disparity that may beat this thread's best so
+                // far: num * rsqrt(vx) * rsqrt(vy) estimates it within a few
+                // ulp (relative 1e-6), so a disparity whose estimate lies
+                // more than 1e-5 (relative) below the best cannot win or tie.
+                // The winner and its score are unchanged.
+                float bestf = -INFINITY;
+                const float rvx = rsqrtf(fvx);
 #pragma unroll
                 for (int j = 0; j < kDPW; ++j) {
                     const int d = dw + j;
                     if (d > ghi || d < glo || x - a.dmin - d - R < 0) continue;
-                    const int sy = syk[c - j + kDPW - 1], vy = vyk[c - j + kDPW - 1];  // column x - dmin - d
+                    const int kk = c - j + kDPW - 1;
+                    const int sy = syk[kk], vy = vyk[kk];  // column x - dmin - d
                     const int num = n * C[j][c] - sx * sy;
                     float sc = 0.0f;
-                    if ((long long)vx * (long long)vy >= n4)
+                    if ((long long)vx * (long long)vy >= n4) {
+                        const float est = __fmul_rn(__fmul_rn(__int2float_rn(num), rvx), ryk[kk]);
+                        if (est < bestf - fabsf(bestf) * 1e-5f) continue;
                         sc = __fdiv_rn(__int2float_rn(num), __fsqrt_rn(__fmul_rn(fvx, __int2float_rn(vy))));
+                    }
                     const unsigned long long key =
                         ((unsigned long long)ordered(sc) << 32) | (0xFFFFFFFFu - uint32_t(d));
-                    best = key > best ? key : best;
+                    if (key > best) {
+                        best = key;
+                        bestf = sc;
+                    }
                 }
                 if (best) atomicMax(&sKey[oy * TWO + v - R], best);
             }
@@ -396,6 +413,19 @@ int ct_bm_ncc_configure(ct_handle* hh, int32_t device, const ct_format* fmt, con
     if (cudaMalloc(&h->guide, G * sizeof(uint32_t)) != cudaSuccess) return fail(CT_ENOMEM, "guide ranges");
     h->fmt = *fmt;
     h->par = *p;
+    {  // strip height: fewest staged rows per SM over the waves (th 8 .. 64)
+        const int R = p->radius, two = ncc::two_of(R), sms = sm_count(device);
+        const long tiles = long((fmt->width + two - 1) / two) * ((p->disp_count + ncc::kDPC - 1) / ncc::kDPC);
+        long best_cost = -1;
+        for (int th = 8; th <= 64; th += 2) {
+            const long ctas = tiles * ((fmt->height + th - 1) / th);
+            const long cost = (ctas + 2 * sms - 1) / (2 * sms) * long(min(th, fmt->height) + 2 * R);  // 2 CTAs / SM
+            if (best_cost < 0 || cost < best_cost) {
+                best_cost = cost;
+                h->th = th;
+            }
+        }
+    }
     h->configured = true;
     return CT_OK;
 }
