@@ -464,12 +464,11 @@ constexpr int kM = 128;   // pixels per tile = MMA M
 constexpr int kChunkBytes = kM * 16;  // one K-chunk (8 elements) of the 128-row A1 operand
 
 // Shared memory:
-//   box    the tile's curve block: the disparity groups g_lo .. g_hi its
-//          pixels read (one TMA load of kLoadGroups groups, or two when the
-//          tile's winners spread wider), x kBoxWords words starting at word
-//          x0 (the tile's first column x0 is word x0 + 2), group g at
-//          (g - g_lo) * kBoxWords words; pixel m reads column m + 2 (lanes of
-//          a warp on distinct banks when they share the group)
+//   box    the tile's curve block, brought in by one TMA load: all 32
+//          disparity groups x kBoxWords words starting at word x0 (the tile's
+//          first column x0 is word x0 + 2), group g at g * kBoxWords words;
+//          pixel m reads column m + 2 (lanes of a warp on distinct banks
+//          when they share the group)
 //   A1     conv1 operand, f16, K-major without swizzle in K-chunk panels
 //          (element (pixel r, k) at (k / 8) * 2048 + r * 16 + (k % 8) * 2):
 //          window t = chunks 2t, 2t + 1 holds codes 15t .. 15t + 15 of the
@@ -479,8 +478,6 @@ constexpr int kChunkBytes = kM * 16;  // one K-chunk (8 elements) of the 128-row
 constexpr int kGroups = 32;       // 128 disparities / 4 per word
 constexpr int kBoxWords = kM + 4; // 2 halo words + 128 columns, rounded to 16 bytes
 constexpr int kBoxBytes = kGroups * kBoxWords * 4;
-constexpr int kLoadGroups = 16;   // groups per TMA load of the curve block
-constexpr int kLoadBytes = kLoadGroups * kBoxWords * 4;
 constexpr int kBox = 0;
 constexpr int kA1 = kBox + kBoxBytes;
 constexpr int kA1Chunks = 6;
@@ -494,8 +491,7 @@ constexpr int kBias = kB4 + 4 * 1024;   // fp32: b1[32] b2[32] b3[32] b4[64] w5[
 constexpr int kWBytes = kBias + (32 + 32 + 32 + 64 + 64 + 4) * 4;
 constexpr int kBar = kWImg + kWBytes;   // 3 mbarriers: MMA commits (2), curve block
 constexpr int kTmemSlot = kBar + 3 * 8;
-constexpr int kRange = kTmemSlot + 16;  // per warp: min / max winner of the next tile (2 x 4 ints)
-constexpr int kSmem = kRange + 32;
+constexpr int kSmem = kTmemSlot + 16;
 static_assert(kWBytes % 16 == 0, "weight image must be a whole number of 16-byte words");
 static_assert(kBoxWords * 4 % 16 == 0 && kA1 % 128 == 0, "TMA box rows and A1 panels 16-byte aligned");
 static_assert(2 * kSmem <= 228 * 1024, "two CTAs per SM");
@@ -669,7 +665,6 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(const __grid_constant__ C
     const int m = tid;  // pixel of the tile / TMEM lane
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kBar);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kTmemSlot);
-    int* rng = reinterpret_cast<int*>(smem + kRange);
     unsigned char* A1 = smem + kA1;
     const uint32_t* box = reinterpret_cast<const uint32_t*>(smem + kBox) + m + 2;  // this pixel's column
     const uint32_t sA1 = dev::smem_u32(A1), sW = dev::smem_u32(smem + kWImg);
@@ -772,33 +767,10 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(const __grid_constant__ C
         const int x = q.tx * kM + m;
         return x < a.W ? disp_entry(a.disp, a.disp_pitch, a.disp_type, x, q.y) : 0u;
     };
-    // First disparity group of the box of the tile whose winners were last
-    // reduced into rng (all threads keep it for build_a1).
-    int g_lo_cur = 0, g_lo_next = 0;
-    // Every thread: the tile's winner range, warp-reduced into rng (read after
-    // the next CTA barrier).
-    auto publish_range = [&](uint32_t e) {
-        const int w = entry_winner(e, a.disp_type);
-        const int lo = __reduce_min_sync(0xffffffffu, w), hi = __reduce_max_sync(0xffffffffu, w);
+    auto load_box = [&](TilePos q) {  // warp 1, all lanes (they count the loads)
         if ((tid & 31) == 0) {
-            rng[warp] = lo;
-            rng[4 + warp] = hi;
-        }
-    };
-    // The tile's groups: pixel d reads groups (d - 12) >> 2 .. that + 9.
-    auto box_groups = [&](int& g_lo, int& n_loads) {
-        const int lo = min(min(rng[0], rng[1]), min(rng[2], rng[3]));
-        const int hi = max(max(rng[4], rng[5]), max(rng[6], rng[7]));
-        g_lo = max(0, (lo - 12) >> 2);
-        const int g_hi = min(kGroups - 1, ((hi - 12) >> 2) + 9);
-        n_loads = g_hi - g_lo < kLoadGroups ? 1 : 2;
-    };
-    auto load_box = [&](TilePos q, int g_lo, int n_loads) {  // warp 1, all lanes (they count the loads)
-        if ((tid & 31) == 0) {
-            dev::mbar_arrive_expect_tx(&bars[2], uint32_t(n_loads * kLoadBytes));
-            for (int k = 0; k < n_loads; ++k)
-                dev::tma_load_3d(smem + kBox + k * kLoadBytes, &tm_curve, q.tx * kM, g_lo + k * kLoadGroups, q.y,
-                                 &bars[2]);
+            dev::mbar_arrive_expect_tx(&bars[2], kBoxBytes);
+            dev::tma_load_3d(smem + kBox, &tm_curve, q.tx * kM, 0, q.y, &bars[2]);
         }
         ++cm[2];
     };
@@ -806,7 +778,7 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(const __grid_constant__ C
     // A1 of the tile whose curve block is in the box: the 35 codes around
     // the winner d (curve bytes d - 12 .. d + 22; 255 outside the curve),
     // 15 per K=16 window
-    auto build_a1 = [&](int d, int g_lo) {
+    auto build_a1 = [&](int d) {
         const int g0 = (d - 12) >> 2;  // floor: word of the first code
         const int c0 = (d - 12) - 4 * g0;
         // words g0 .. g0 + 9 hold the 35 codes (bytes c0 .. c0 + 34); later
@@ -815,7 +787,7 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(const __grid_constant__ C
 #pragma unroll
         for (int k = 0; k < 10; ++k) {
             const int g = g0 + k;
-            w[k] = unsigned(g) < unsigned(kGroups) ? box[(g - g_lo) * kBoxWords] : 0xFFFFFFFFu;
+            w[k] = unsigned(g) < unsigned(kGroups) ? box[g * kBoxWords] : 0xFFFFFFFFu;
         }
         w[10] = w[11] = w[12] = 0xFFFFFFFFu;
 #pragma unroll
@@ -846,13 +818,9 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(const __grid_constant__ C
     uint32_t e_cur = 0, e_next = 0, e_next2 = 0;  // their disparity entries
     if (t < tiles) {
         e_cur = load_entry(p_cur);
-        publish_range(e_cur);
-        __syncthreads();
-        int n_loads;
-        box_groups(g_lo_cur, n_loads);
-        if (warp == 1) load_box(p_cur, g_lo_cur, n_loads);
+        if (warp == 1) load_box(p_cur);
         if (__syncthreads_or(!wait_bar(2))) failed = true;
-        else build_a1(entry_winner(e_cur, a.disp_type), g_lo_cur);
+        else build_a1(entry_winner(e_cur, a.disp_type));
     }
     if (t + (int)gridDim.x < tiles) e_next = load_entry(p_next);
     for (; t < tiles && !failed; t += gridDim.x) {
@@ -860,7 +828,6 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(const __grid_constant__ C
         // ---- conv1 biases into C1 (A1 was built while the previous tile's fc1 ran)
 #pragma unroll
         for (int q = 0; q < 7; ++q) st32(tl + 32 * q, bias1);
-        publish_range(e_next);  // the next tile's box groups, read after this barrier
         hand_to_issuer(true);
         // ---- conv1: window t = positions 3t .. 3t + 2 (N = 96; the last window N = 32)
         if (warp == 0) {  // MMA issue: whole warp, one elected lane
@@ -871,11 +838,7 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(const __grid_constant__ C
             commit_to(0);
         }
         // the next tile's curve block (the box was last read by this tile's A1 build)
-        {
-            int n_loads;
-            box_groups(g_lo_next, n_loads);
-            if (warp == 1 && t + (int)gridDim.x < tiles) load_box(p_next, g_lo_next, n_loads);
-        }
+        if (warp == 1 && t + (int)gridDim.x < tiles) load_box(p_next);
         if (t + 2 * (int)gridDim.x < tiles) e_next2 = load_entry(p_next2);
         if (__syncthreads_or(!wait_bar(0))) { failed = true; break; }
         fence_after();
@@ -952,7 +915,7 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(const __grid_constant__ C
         bool box_ok = true;
         if (t + (int)gridDim.x < tiles) {
             box_ok = wait_bar(2);
-            if (box_ok) build_a1(entry_winner(e_next, a.disp_type), g_lo_next);
+            if (box_ok) build_a1(entry_winner(e_next, a.disp_type));
         }
         if (__syncthreads_or(!box_ok || !wait_bar(1))) { failed = true; break; }
         fence_after();
@@ -1390,7 +1353,7 @@ int ct_confnet_infer(ct_handle* hh, const ct_image* score, const ct_curves* curv
     CUtensorMap tm_curve;
     const uint64_t dims[3] = {uint64_t(a.W) + 2, uint64_t(inf::kGroups), uint64_t(a.H)};
     const uint64_t strides[2] = {curves->pitch_bytes, curves->pitch_bytes * inf::kGroups};
-    const uint32_t box[3] = {uint32_t(inf::kBoxWords), uint32_t(inf::kLoadGroups), 1};
+    const uint32_t box[3] = {uint32_t(inf::kBoxWords), uint32_t(inf::kGroups), 1};
     if (int rc = make_tmap_nd(&tm_curve, curves->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, 3, dims, strides, box))
         return rc;
     // programmatic stream serialisation: the kernel's prologue (weight

@@ -228,46 +228,70 @@ __global__ void __launch_bounds__(kNT, 2)
             }
 #pragma unroll
             for (int c = 0; c < kCPT; ++c) {
+                // every lane stays in the loop (the candidate loop below is
+                // warp-synchronous); columns without an output search nothing
                 const int v = 4 * lane + c;
-                if (v < R || v >= kTWV - R) continue;
                 const int x = xs + v;
-                if (x < R || x >= a.W - R) continue;
-                const size_t o = (size_t)y * a.W + x;
+                const bool colok = v >= R && v < kTWV - R && x >= R && x < a.W - R;
+                const size_t o = (size_t)y * a.W + (colok ? x : R);
                 const int sx = a.Sx[o], vx = a.Vx[o];
                 const float fvx = __int2float_rn(vx);
-                int glo = 0, ghi = a.D - 1;
-                if (a.guide) {
+                int glo = 0, ghi = colok ? a.D - 1 : -1;
+                if (a.guide && colok) {
                     const uint32_t g = __ldg(&a.guide[(size_t)(y / kGuideBlock) * a.guide_gw + x / kGuideBlock]);
                     glo = int(g & 0xFFFFu);
                     ghi = min(int(g >> 16), a.D - 1);
                 }
-                unsigned long long best = 0ull;
-                // The IEEE score (a divide and a square root) is evaluated
-                // only for a disparity that may beat this thread's best so
-                // far: num * rsqrt(vx) * rsqrt(vy) estimates it within a few
-                // ulp (relative 1e-6), so a disparity whose estimate lies
-                // more than 1e-5 (relative) below the best cannot win or tie.
-                // The winner and its score are unchanged.
-                float bestf = -INFINITY;
+                // The IEEE score (a divide and a square root) decides the
+                // winner. It is evaluated for this column's best estimate
+                // num * rsqrt(vx) * rsqrt(vy) (within a few ulp, relative
+                // 1e-6, of the score) and then for any other disparity whose
+                // estimate lies within 2e-5 (relative) of that one: the others
+                // cannot win or tie. Every lane evaluates its own candidate in
+                // the same instruction stream, so the warp runs one IEEE
+                // score per column unless some lane has a near-tie.
                 const float rvx = rsqrtf(fvx);
+                float est[kDPW];
+                uint32_t cand = 0;  // bit j: disparity dw + j is searched
+                float emax = -INFINITY;
 #pragma unroll
                 for (int j = 0; j < kDPW; ++j) {
                     const int d = dw + j;
-                    if (d > ghi || d < glo || x - a.dmin - d - R < 0) continue;
                     const int kk = c - j + kDPW - 1;
-                    const int sy = syk[kk], vy = vyk[kk];  // column x - dmin - d
-                    const int num = n * C[j][c] - sx * sy;
-                    float sc = 0.0f;
-                    if ((long long)vx * (long long)vy >= n4) {
-                        const float est = __fmul_rn(__fmul_rn(__int2float_rn(num), rvx), ryk[kk]);
-                        if (est < bestf - fabsf(bestf) * 1e-5f) continue;
-                        sc = __fdiv_rn(__int2float_rn(num), __fsqrt_rn(__fmul_rn(fvx, __int2float_rn(vy))));
-                    }
-                    const unsigned long long key =
-                        ((unsigned long long)ordered(sc) << 32) | (0xFFFFFFFFu - uint32_t(d));
-                    if (key > best) {
-                        best = key;
-                        bestf = sc;
+                    est[j] = -INFINITY;
+                    if (d > ghi || d < glo || x - a.dmin - d - R < 0) continue;
+                    const int num = n * C[j][c] - sx * syk[kk];
+                    // 0 exactly when sigma_x sigma_y < 1 (vx vy < n^4)
+                    est[j] = (long long)vx * (long long)vyk[kk] >= n4
+                                 ? __fmul_rn(__fmul_rn(__int2float_rn(num), rvx), ryk[kk])
+                                 : 0.0f;
+                    cand |= 1u << j;
+                    emax = fmaxf(emax, est[j]);
+                }
+                const float thr = emax - fabsf(emax) * 2e-5f;
+#pragma unroll
+                for (int j = 0; j < kDPW; ++j)
+                    if (!(est[j] >= thr)) cand &= ~(1u << j);
+                unsigned long long best = 0ull;
+                while (__any_sync(0xffffffffu, cand != 0)) {
+                    if (cand) {
+                        const int j = __ffs(cand) - 1;
+                        cand &= cand - 1;
+                        // the candidate's inputs by selection (no indexed registers)
+                        int num = 0, vy = 0;
+#pragma unroll
+                        for (int q = 0; q < kDPW; ++q)
+                            if (q == j) {
+                                const int kk = c - q + kDPW - 1;
+                                num = n * C[q][c] - sx * syk[kk];
+                                vy = vyk[kk];
+                            }
+                        float sc = 0.0f;
+                        if ((long long)vx * (long long)vy >= n4)
+                            sc = __fdiv_rn(__int2float_rn(num), __fsqrt_rn(__fmul_rn(fvx, __int2float_rn(vy))));
+                        const unsigned long long key =
+                            ((unsigned long long)ordered(sc) << 32) | (0xFFFFFFFFu - uint32_t(dw + j));
+                        best = key > best ? key : best;
                     }
                 }
                 if (best) atomicMax(&sKey[oy * TWO + v - R], best);
