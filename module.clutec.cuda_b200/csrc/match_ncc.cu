@@ -226,76 +226,93 @@ __global__ void __launch_bounds__(kNT, 2)
                     ryk[k] = rsqrtf(__int2float_rn(vyk[k]));
                 }
             }
+            // The IEEE score (a divide and a square root) decides the winner.
+            // It is evaluated for each column's best estimate
+            // num * rsqrt(vx) * rsqrt(vy) (within a few ulp, relative 1e-6,
+            // of the score) and then for any other disparity whose estimate
+            // lies within 2e-5 (relative) of that one: the others cannot win
+            // or tie. The four columns' first candidates are evaluated
+            // together (independent chains), the rare near-ties after that in
+            // a warp-synchronous loop. Every lane runs every step (columns
+            // without an output have no candidates).
+            int sxc[kCPT], vxc[kCPT];
+            float fvxc[kCPT];
+            uint32_t cand[kCPT];  // per column: near-tie candidates left after the first
+            unsigned long long best[kCPT];
+            // exact score key of candidate j of column c (inputs by selection,
+            // no indexed registers)
+            auto exact_key = [&](int c, int j) {
+                int num = 0, vy = 0;
+#pragma unroll
+                for (int q = 0; q < kDPW; ++q)
+                    if (q == j) {
+                        const int kk = c - q + kDPW - 1;
+                        num = n * C[q][c] - sxc[c] * syk[kk];
+                        vy = vyk[kk];
+                    }
+                float sc = 0.0f;
+                if ((long long)vxc[c] * (long long)vy >= n4)
+                    sc = __fdiv_rn(__int2float_rn(num), __fsqrt_rn(__fmul_rn(fvxc[c], __int2float_rn(vy))));
+                return ((unsigned long long)ordered(sc) << 32) | (0xFFFFFFFFu - uint32_t(dw + j));
+            };
 #pragma unroll
             for (int c = 0; c < kCPT; ++c) {
-                // every lane stays in the loop (the candidate loop below is
-                // warp-synchronous); columns without an output search nothing
                 const int v = 4 * lane + c;
                 const int x = xs + v;
                 const bool colok = v >= R && v < kTWV - R && x >= R && x < a.W - R;
                 const size_t o = (size_t)y * a.W + (colok ? x : R);
-                const int sx = a.Sx[o], vx = a.Vx[o];
-                const float fvx = __int2float_rn(vx);
+                sxc[c] = a.Sx[o];
+                vxc[c] = a.Vx[o];
+                fvxc[c] = __int2float_rn(vxc[c]);
                 int glo = 0, ghi = colok ? a.D - 1 : -1;
                 if (a.guide && colok) {
                     const uint32_t g = __ldg(&a.guide[(size_t)(y / kGuideBlock) * a.guide_gw + x / kGuideBlock]);
                     glo = int(g & 0xFFFFu);
                     ghi = min(int(g >> 16), a.D - 1);
                 }
-                // The IEEE score (a divide and a square root) decides the
-                // winner. It is evaluated for this column's best estimate
-                // num * rsqrt(vx) * rsqrt(vy) (within a few ulp, relative
-                // 1e-6, of the score) and then for any other disparity whose
-                // estimate lies within 2e-5 (relative) of that one: the others
-                // cannot win or tie. Every lane evaluates its own candidate in
-                // the same instruction stream, so the warp runs one IEEE
-                // score per column unless some lane has a near-tie.
-                const float rvx = rsqrtf(fvx);
+                const float rvx = rsqrtf(fvxc[c]);
                 float est[kDPW];
-                uint32_t cand = 0;  // bit j: disparity dw + j is searched
                 float emax = -INFINITY;
+                int jmax = 0;
+                uint32_t searched = 0;
 #pragma unroll
                 for (int j = 0; j < kDPW; ++j) {
                     const int d = dw + j;
                     const int kk = c - j + kDPW - 1;
-                    est[j] = -INFINITY;
-                    if (d > ghi || d < glo || x - a.dmin - d - R < 0) continue;
-                    const int num = n * C[j][c] - sx * syk[kk];
+                    const int num = n * C[j][c] - sxc[c] * syk[kk];
                     // 0 exactly when sigma_x sigma_y < 1 (vx vy < n^4)
-                    est[j] = (long long)vx * (long long)vyk[kk] >= n4
+                    est[j] = (long long)vxc[c] * (long long)vyk[kk] >= n4
                                  ? __fmul_rn(__fmul_rn(__int2float_rn(num), rvx), ryk[kk])
                                  : 0.0f;
-                    cand |= 1u << j;
-                    emax = fmaxf(emax, est[j]);
-                }
-                const float thr = emax - fabsf(emax) * 2e-5f;
-#pragma unroll
-                for (int j = 0; j < kDPW; ++j)
-                    if (!(est[j] >= thr)) cand &= ~(1u << j);
-                unsigned long long best = 0ull;
-                while (__any_sync(0xffffffffu, cand != 0)) {
-                    if (cand) {
-                        const int j = __ffs(cand) - 1;
-                        cand &= cand - 1;
-                        // the candidate's inputs by selection (no indexed registers)
-                        int num = 0, vy = 0;
-#pragma unroll
-                        for (int q = 0; q < kDPW; ++q)
-                            if (q == j) {
-                                const int kk = c - q + kDPW - 1;
-                                num = n * C[q][c] - sx * syk[kk];
-                                vy = vyk[kk];
-                            }
-                        float sc = 0.0f;
-                        if ((long long)vx * (long long)vy >= n4)
-                            sc = __fdiv_rn(__int2float_rn(num), __fsqrt_rn(__fmul_rn(fvx, __int2float_rn(vy))));
-                        const unsigned long long key =
-                            ((unsigned long long)ordered(sc) << 32) | (0xFFFFFFFFu - uint32_t(dw + j));
-                        best = key > best ? key : best;
+                    const bool s_ = !(d > ghi || d < glo || x - a.dmin - d - R < 0);
+                    searched |= uint32_t(s_) << j;
+                    if (s_ && est[j] > emax) {
+                        emax = est[j];
+                        jmax = j;
                     }
                 }
-                if (best) atomicMax(&sKey[oy * TWO + v - R], best);
+                const float thr = emax - fabsf(emax) * 2e-5f;
+                cand[c] = 0;
+#pragma unroll
+                for (int j = 0; j < kDPW; ++j)
+                    if ((searched & (1u << j)) && j != jmax && est[j] >= thr) cand[c] |= 1u << j;
+                // the best estimate's exact score (no candidate: key 0)
+                best[c] = searched ? exact_key(c, jmax) : 0ull;
             }
+            // near-ties: every other disparity within the margin (rare)
+            while (__any_sync(0xffffffffu, (cand[0] | cand[1] | cand[2] | cand[3]) != 0)) {
+#pragma unroll
+                for (int c = 0; c < kCPT; ++c)
+                    if (cand[c]) {
+                        const int j = __ffs(cand[c]) - 1;
+                        cand[c] &= cand[c] - 1;
+                        const unsigned long long key = exact_key(c, j);
+                        best[c] = key > best[c] ? key : best[c];
+                    }
+            }
+#pragma unroll
+            for (int c = 0; c < kCPT; ++c)
+                if (best[c]) atomicMax(&sKey[oy * TWO + 4 * lane + c - R], best[c]);
         }
     }
     __syncthreads();
@@ -437,18 +454,13 @@ int ct_bm_ncc_configure(ct_handle* hh, int32_t device, const ct_format* fmt, con
     if (cudaMalloc(&h->guide, G * sizeof(uint32_t)) != cudaSuccess) return fail(CT_ENOMEM, "guide ranges");
     h->fmt = *fmt;
     h->par = *p;
-    {  // strip height: fewest staged rows per SM over the waves (th 8 .. 64)
-        const int R = p->radius, two = ncc::two_of(R), sms = sm_count(device);
+    {  // strip height: 32 rows (measured faster at 1080p than the taller strips
+       // of fewer waves); lower only while the grid would not fill one wave of
+       // 2 CTAs per SM
+        const int two = ncc::two_of(p->radius), sms = sm_count(device);
         const long tiles = long((fmt->width + two - 1) / two) * ((p->disp_count + ncc::kDPC - 1) / ncc::kDPC);
-        long best_cost = -1;
-        for (int th = 8; th <= 64; th += 2) {
-            const long ctas = tiles * ((fmt->height + th - 1) / th);
-            const long cost = (ctas + 2 * sms - 1) / (2 * sms) * long(min(th, fmt->height) + 2 * R);  // 2 CTAs / SM
-            if (best_cost < 0 || cost < best_cost) {
-                best_cost = cost;
-                h->th = th;
-            }
-        }
+        h->th = 32;
+        while (h->th > 8 && tiles * ((fmt->height + h->th - 1) / h->th) < 2L * sms) h->th -= 2;
     }
     h->configured = true;
     return CT_OK;
