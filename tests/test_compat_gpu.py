@@ -73,3 +73,17 @@ def test_compat_640x480(ct, oracle, cuda, method, patch, sim):
                                min_delta_thresh=thr[2])
     got = run_gpu(ct, cuda, L, R, method, patch, sim, True, 0, D, *thr)
     np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("method,patch,sim,thr", [("ncc", 11, 0, (2.0, 0.6, 3)), ("sad1", 9, 0, (3.0, 40.0, 60)),
+                                                  ("aw1", 5, 0, (5.0, 90.0, 0.3)), ("aw2", 3, 0, (3.0, 20.0, 30)),
+                                                  ("bm1", 9, 1, (8.0, 5.0, 0.5))])
+def test_compat_1080p_d128(ct, oracle, cuda, method, patch, sim, thr):
+    """The 1920x1080 D=128 slanted-plane pair (generator kind 2, seed 2024),
+    every channel bit-exact with the gates and ID thresholds active."""
+    W, H, D = 1920, 1080, 128
+    L, R, _, _ = ct.synth_pair(2, 2024, W, H, D - 1)
+    want = oracle.compat_match(L, R, method, D, patch, sim_type=sim, grad_thresh=thr[0], score_thresh=thr[1],
+                               min_delta_thresh=thr[2])
+    got = run_gpu(ct, cuda, L, R, method, patch, sim, True, 0, D, *thr)
+    np.testing.assert_array_equal(got, want)
