@@ -30,9 +30,13 @@ __host__ __device__ constexpr size_t smem_bytes(int th, int R) {
     return strip_bytes(th, R) + size_t(th) * two_of(R) * 8 + 16;
 }
 
-// Box sum S and n*Q - S^2 for every pixel whose window is inside the image.
+// Box sum S and n*Q - S^2 for every pixel whose window is inside the image,
+// and (T non-null) the zero-score threshold of the left view: the smallest vy
+// with V * vy >= n^4, i.e. ceil(n^4 / V) (INT_MAX when V = 0), so that the
+// matcher's test sigma_x sigma_y >= 1 is one 32-bit compare vy >= T.
 template <int R>
-__global__ void box_stats_kernel(const uint8_t* img, size_t pitch, int W, int H, int32_t* S, int32_t* V) {
+__global__ void box_stats_kernel(const uint8_t* img, size_t pitch, int W, int H, int32_t* S, int32_t* V,
+                                 int32_t* T) {
     constexpr int TX = 32, TY = 8, SW = TX + 2 * R, SH = TY + 2 * R;
     __shared__ uint8_t t[SH][SW];
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
@@ -53,8 +57,12 @@ __global__ void box_stats_kernel(const uint8_t* img, size_t pitch, int W, int H,
             q += v * v;
         }
     constexpr int n = (2 * R + 1) * (2 * R + 1);
+    constexpr long long n4 = (long long)n * n * n * n;
+    static_assert(n4 < 0x7FFFFFFFll, "the threshold fits in int32");
+    const int v = n * q - s * s;
     S[(size_t)y * W + x] = s;
-    V[(size_t)y * W + x] = n * q - s * s;
+    V[(size_t)y * W + x] = v;
+    if (T) T[(size_t)y * W + x] = v > 0 ? int32_t((n4 + v - 1) / v) : 0x7FFFFFFF;
 }
 
 __device__ __forceinline__ uint32_t ordered(float f) {
@@ -73,6 +81,7 @@ struct Args {
     const uint32_t* guide;   // per 16 x 16 block search range, or null (search all D)
     int guide_gw;
     const int32_t *Sx, *Vx, *Sy, *Vy;   // stats of the left / right image (W*H)
+    const int32_t* Tx;                  // zero-score threshold of the left image (box_stats_kernel)
     unsigned long long* keys;          // global keys when gridDim.z > 1
     void* out;
     size_t out_pitch;
@@ -98,7 +107,6 @@ __global__ void __launch_bounds__(kNT, 2)
     ncc_match_kernel(const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmM, Args a) {
     constexpr int TWO = two_of(R);
     constexpr int n = (2 * R + 1) * (2 * R + 1);
-    constexpr long long n4 = (long long)n * n * n * n;
     extern __shared__ __align__(128) unsigned char smem[];
     const int NR = a.th + 2 * R;
     uint8_t* sB = smem;
@@ -227,32 +235,45 @@ __global__ void __launch_bounds__(kNT, 2)
                 }
             }
             // The IEEE score (a divide and a square root) decides the winner.
-            // It is evaluated for each column's best estimate
-            // num * rsqrt(vx) * rsqrt(vy) (within a few ulp, relative 1e-6,
-            // of the score) and then for any other disparity whose estimate
-            // lies within 2e-5 (relative) of that one: the others cannot win
-            // or tie. The four columns' first candidates are evaluated
-            // together (independent chains), the rare near-ties after that in
-            // a warp-synchronous loop. Every lane runs every step (columns
-            // without an output have no candidates).
-            int sxc[kCPT], vxc[kCPT];
-            float fvxc[kCPT];
+            // Per column, disparities are ranked by the estimate
+            // num * rsqrt(vy), the score times sqrt(vx) (a positive factor
+            // common to the column) within a few ulp (relative 1e-6); the
+            // IEEE score is evaluated for the lowest disparity whose estimate
+            // lies within 2e-5 (relative) of the column's best, and then for
+            // the other such near-ties in a warp-synchronous loop (rare):
+            // the rest cannot win or tie. An estimate is exactly 0 if and only
+            // if the score is +0 (num = 0, or sigma_x sigma_y < 1, tested as
+            // vy >= Tx), so a column whose best estimate is 0 needs no IEEE
+            // work. Every lane runs every step (columns without an output
+            // have no candidates).
+            int sxc[kCPT] = {}, tc[kCPT] = {};
+            float fvxc[kCPT] = {};
             uint32_t cand[kCPT];  // per column: near-tie candidates left after the first
             unsigned long long best[kCPT];
-            // exact score key of candidate j of column c (inputs by selection,
-            // no indexed registers)
+            // v[j] of eight registers by a three-level select on the bits of j
+            auto sel8 = [](int v0, int v1, int v2, int v3, int v4, int v5, int v6, int v7, int j) {
+                const bool b0 = j & 1, b1 = j & 2, b2 = j & 4;
+                const int a0 = b0 ? v1 : v0, a1 = b0 ? v3 : v2, a2 = b0 ? v5 : v4, a3 = b0 ? v7 : v6;
+                const int c0 = b1 ? a1 : a0, c1 = b1 ? a3 : a2;
+                return b2 ? c1 : c0;
+            };
+            // key of disparity j of column c: IEEE score << 32 | ~d
             auto exact_key = [&](int c, int j) {
-                int num = 0, vy = 0;
-#pragma unroll
-                for (int q = 0; q < kDPW; ++q)
-                    if (q == j) {
-                        const int kk = c - q + kDPW - 1;
-                        num = n * C[q][c] - sxc[c] * syk[kk];
-                        vy = vyk[kk];
-                    }
-                float sc = 0.0f;
-                if ((long long)vxc[c] * (long long)vy >= n4)
-                    sc = __fdiv_rn(__int2float_rn(num), __fsqrt_rn(__fmul_rn(fvxc[c], __int2float_rn(vy))));
+#define CT_SEL_C(q) C[q][c]
+#define CT_SEL_K(arr, q) arr[c - (q) + kDPW - 1]
+                static_assert(kDPW == 8, "sel8 selects among 8 disparities");
+                const int cq = sel8(CT_SEL_C(0), CT_SEL_C(1), CT_SEL_C(2), CT_SEL_C(3), CT_SEL_C(4), CT_SEL_C(5),
+                                    CT_SEL_C(6), CT_SEL_C(7), j);
+                const int sy = sel8(CT_SEL_K(syk, 0), CT_SEL_K(syk, 1), CT_SEL_K(syk, 2), CT_SEL_K(syk, 3),
+                                    CT_SEL_K(syk, 4), CT_SEL_K(syk, 5), CT_SEL_K(syk, 6), CT_SEL_K(syk, 7), j);
+                const int vy = sel8(CT_SEL_K(vyk, 0), CT_SEL_K(vyk, 1), CT_SEL_K(vyk, 2), CT_SEL_K(vyk, 3),
+                                    CT_SEL_K(vyk, 4), CT_SEL_K(vyk, 5), CT_SEL_K(vyk, 6), CT_SEL_K(vyk, 7), j);
+#undef CT_SEL_C
+#undef CT_SEL_K
+                const int num = n * cq - sxc[c] * sy;
+                const float sc =
+                    vy >= tc[c] ? __fdiv_rn(__int2float_rn(num), __fsqrt_rn(__fmul_rn(fvxc[c], __int2float_rn(vy))))
+                                : 0.0f;
                 return ((unsigned long long)ordered(sc) << 32) | (0xFFFFFFFFu - uint32_t(dw + j));
             };
 #pragma unroll
@@ -262,42 +283,41 @@ __global__ void __launch_bounds__(kNT, 2)
                 const bool colok = v >= R && v < kTWV - R && x >= R && x < a.W - R;
                 const size_t o = (size_t)y * a.W + (colok ? x : R);
                 sxc[c] = a.Sx[o];
-                vxc[c] = a.Vx[o];
-                fvxc[c] = __int2float_rn(vxc[c]);
-                int glo = 0, ghi = colok ? a.D - 1 : -1;
+                fvxc[c] = __int2float_rn(a.Vx[o]);
+                tc[c] = a.Tx[o];
+                // searched disparities dw + j: j in [jlo, jhi] (guide range,
+                // match column x - dmin - d - R >= 0)
+                int glo = 0, ghi = a.D - 1;
                 if (a.guide && colok) {
                     const uint32_t g = __ldg(&a.guide[(size_t)(y / kGuideBlock) * a.guide_gw + x / kGuideBlock]);
                     glo = int(g & 0xFFFFu);
                     ghi = min(int(g >> 16), a.D - 1);
                 }
-                const float rvx = rsqrtf(fvxc[c]);
-                float est[kDPW];
+                const int jlo = max(glo - dw, 0), jhi = min(min(ghi, x - a.dmin - R) - dw, kDPW - 1);
+                const uint32_t smask = (colok && jlo <= jhi) ? ((2u << jhi) - (1u << jlo)) : 0u;
+                float val[kDPW];
                 float emax = -INFINITY;
-                int jmax = 0;
-                uint32_t searched = 0;
 #pragma unroll
                 for (int j = 0; j < kDPW; ++j) {
-                    const int d = dw + j;
                     const int kk = c - j + kDPW - 1;
                     const int num = n * C[j][c] - sxc[c] * syk[kk];
-                    // 0 exactly when sigma_x sigma_y < 1 (vx vy < n^4)
-                    est[j] = (long long)vxc[c] * (long long)vyk[kk] >= n4
-                                 ? __fmul_rn(__fmul_rn(__int2float_rn(num), rvx), ryk[kk])
-                                 : 0.0f;
-                    const bool s_ = !(d > ghi || d < glo || x - a.dmin - d - R < 0);
-                    searched |= uint32_t(s_) << j;
-                    if (s_ && est[j] > emax) {
-                        emax = est[j];
-                        jmax = j;
-                    }
+                    const float e = vyk[kk] >= tc[c] ? __fmul_rn(__int2float_rn(num), ryk[kk]) : 0.0f;
+                    val[j] = (smask >> j) & 1u ? e : -INFINITY;
+                    emax = fmaxf(emax, val[j]);
                 }
+                uint32_t cm = 0;
                 const float thr = emax - fabsf(emax) * 2e-5f;
-                cand[c] = 0;
 #pragma unroll
-                for (int j = 0; j < kDPW; ++j)
-                    if ((searched & (1u << j)) && j != jmax && est[j] >= thr) cand[c] |= 1u << j;
-                // the best estimate's exact score (no candidate: key 0)
-                best[c] = searched ? exact_key(c, jmax) : 0ull;
+                for (int j = 0; j < kDPW; ++j) cm |= uint32_t(val[j] >= thr) << j;
+                cm &= smask;
+                const int j1 = __ffs(cm) - 1;
+                if (emax == 0.0f) {  // every candidate scores +0: the lowest d wins
+                    best[c] = ((unsigned long long)ordered(0.0f) << 32) | (0xFFFFFFFFu - uint32_t(dw + j1));
+                    cand[c] = 0;
+                } else {
+                    best[c] = cm ? exact_key(c, j1) : 0ull;
+                    cand[c] = cm & (cm - 1);
+                }
             }
             // near-ties: every other disparity within the margin (rare)
             while (__any_sync(0xffffffffu, (cand[0] | cand[1] | cand[2] | cand[3]) != 0)) {
@@ -355,7 +375,7 @@ struct NccHandle : ct_handle {
     }
     ct_format fmt{};
     ct_ncc_params par{};
-    int32_t* stats = nullptr;  // Sx, Vx, Sy, Vy
+    int32_t* stats = nullptr;  // Sx, Vx, Sy, Vy, Tx
     unsigned long long* keys = nullptr;
     uint32_t* guide = nullptr;  // guided mode: one search range per 16 x 16 block
     int th = 32;
@@ -377,6 +397,7 @@ int launch_ncc(NccHandle* h, const ct_image* disp, const ct_image* score, const 
     a.W = W; a.H = H; a.D = h->par.disp_count; a.th = h->th;
     a.dmin = h->par.disp_min;
     a.Sx = h->stats; a.Vx = h->stats + N; a.Sy = h->stats + 2 * N; a.Vy = h->stats + 3 * N;
+    a.Tx = h->stats + 4 * N;
     a.keys = h->keys;
     a.out = disp->ptr; a.out_pitch = disp->pitch_bytes; a.out_type = disp->type;
     a.score = score ? static_cast<float*>(score->ptr) : nullptr;
@@ -393,9 +414,9 @@ int launch_ncc(NccHandle* h, const ct_image* disp, const ct_image* score, const 
     }
     dim3 sb(32, 8), sg((W + 31) / 32, (H + 7) / 8);
     box_stats_kernel<R><<<sg, sb, 0, s>>>(static_cast<const uint8_t*>(L->ptr), L->pitch_bytes, W, H, h->stats,
-                                          h->stats + N);
+                                          h->stats + N, h->stats + 4 * N);
     box_stats_kernel<R><<<sg, sb, 0, s>>>(static_cast<const uint8_t*>(Rr->ptr), Rr->pitch_bytes, W, H,
-                                          h->stats + 2 * N, h->stats + 3 * N);
+                                          h->stats + 2 * N, h->stats + 3 * N, nullptr);
     CT_LAUNCH_CHECK();
     const int NR = a.th + 2 * R;
     CUtensorMap tb, tm;
@@ -446,7 +467,7 @@ int ct_bm_ncc_configure(ct_handle* hh, int32_t device, const ct_format* fmt, con
     h->device = device;
     if (int rc = h->init_status()) return rc;
     const size_t N = (size_t)fmt->width * fmt->height;
-    if (cudaMalloc(&h->stats, 4 * N * sizeof(int32_t)) != cudaSuccess) return fail(CT_ENOMEM, "stats scratch");
+    if (cudaMalloc(&h->stats, 5 * N * sizeof(int32_t)) != cudaSuccess) return fail(CT_ENOMEM, "stats scratch");
     if (cudaMalloc(&h->keys, N * sizeof(unsigned long long)) != cudaSuccess) return fail(CT_ENOMEM, "key scratch");
     CT_CUDA_TRY(cudaMemset(h->keys, 0, N * sizeof(unsigned long long)));
     const size_t G = size_t((fmt->width + ncc::kGuideBlock - 1) / ncc::kGuideBlock) *
