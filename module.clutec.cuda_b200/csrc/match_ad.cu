@@ -34,6 +34,16 @@ constexpr int kMWs = kTWV + kDPC + 16; // staged match columns (208)
 constexpr int kRing = 7;              // AW: rows of S kept
 constexpr int kRingW = kTWV + 8;      // AW: padded ring row (4 words each side)
 
+// Per-pixel costs are formed two disparities at a time in the 16-bit halves
+// of a register as max(b + 256 - m, m + 256 - b) = |b - m| + 256 (no borrow
+// crosses the halves); the 256 cancels in the running sums' add/subtract
+// pairs, so every box sum carries (2r+1)^2 * 256 on top of the SAD (at most
+// 81 * 511 = 41391 for 9x9: the 16-bit cost field never reaches 0xFFFF, the
+// "no disparity" marker). The winner's cost in a key is biased by that much.
+constexpr uint32_t kAbsBias = 0x01000100u;
+__host__ __device__ constexpr int box_bias(int R) { return (2 * R + 1) * (2 * R + 1) * 256; }
+static_assert(81 * 511 < 0xFFFF, "biased 9x9 box sums fit the 16-bit cost field");
+
 __host__ __device__ constexpr int ext_of(int R, bool aw) { return aw ? 2 * R : R; }
 __host__ __device__ constexpr int two_of(int R, bool aw) { return kTWV - 2 * ext_of(R, aw); }
 
@@ -166,21 +176,25 @@ __global__ void __launch_bounds__(kNT, 1)
     auto row_pairs = [&](int i, uint32_t (&P)[kCPT][4]) {
         const uint8_t* rb = sB + i * kBW + bo;
         const uint8_t* rm = sM + i * kMWs + mo;
-        int b[kCPT], m[11];
+        uint32_t b2[kCPT], m2[10];
 #pragma unroll
-        for (int c = 0; c < kCPT; ++c) b[c] = rb[c];
+        for (int c = 0; c < kCPT; ++c) b2[c] = uint32_t(rb[c]) * 0x10001u;  // b in both halves
+        // match pixel pairs: the low half is disparity 2p of the pair, the
+        // high half 2p + 1 (left-to-right: columns k0, k0 - 1; right-to-left:
+        // k0, k0 + 1)
+        {
+            uint32_t m[11];
 #pragma unroll
-        for (int k = 0; k < 11; ++k) m[k] = rm[k];
+            for (int k = 0; k < 11; ++k) m[k] = rm[k];
+#pragma unroll
+            for (int k = 0; k < 10; ++k) m2[k] = DIR == 0 ? m[k + 1] + (m[k] << 16) : m[k] + (m[k + 1] << 16);
+        }
 #pragma unroll
         for (int c = 0; c < kCPT; ++c)
 #pragma unroll
             for (int p = 0; p < 4; ++p) {
-                const int j0 = 2 * p, j1 = 2 * p + 1;
-                const int k0 = DIR == 0 ? c - j0 + 7 : c + j0;
-                const int k1 = DIR == 0 ? c - j1 + 7 : c + j1;
-                const uint32_t e0 = uint32_t(abs(b[c] - m[k0]));
-                const uint32_t e1 = uint32_t(abs(b[c] - m[k1]));
-                P[c][p] = e0 | (e1 << 16);
+                const uint32_t mp = m2[DIR == 0 ? c - 2 * p + 6 : c + 2 * p];
+                P[c][p] = __vmaxu2(b2[c] + kAbsBias - mp, mp + kAbsBias - b2[c]);  // |b - m| + 256 per half
             }
     };
 
@@ -358,7 +372,7 @@ __global__ void aw_subpixel_kernel(uint32_t* keys, int W, int H, int D, int dmin
     }
     const int d = int(key & 0xFFFFu);
     const int e = dmin + d;
-    const int c0 = int(key >> 16);
+    const int c0 = int(key >> 16) - box_bias(3);  // the 7x7 SAD (keys carry the box bias)
     float s = float(e);
     if (d > 0 && d < D - 1 && x - (e + 1) - 6 >= 0) {
         const int cm = aw_cost_at(L, pl, Rm, pr, x, y, e - 1);
