@@ -325,61 +325,114 @@ __global__ void ad_finalize_kernel(uint32_t* keys, int W, int H, int ext, void* 
     store_key(out, pitch, type, x, y, valid, key, dmin);
 }
 
-// AW cost A(x, y, d) directly from the images (7x7 windows, shifts of 3).
-// Column sums of 7 rows around y over columns x-6..x+6 give the three
-// horizontally shifted windows; the two vertical shifts are summed directly.
-__device__ int aw_cost_at(const uint8_t* L, size_t pl, const uint8_t* Rm, size_t pr, int x, int y, int d) {
-    int col[13];
-#pragma unroll
-    for (int k = 0; k < 13; ++k) {
-        const int xx = x - 6 + k;
-        int s = 0;
-#pragma unroll
-        for (int dy = -3; dy <= 3; ++dy)
-            s += abs(int(L[(size_t)(y + dy) * pl + xx]) - int(Rm[(size_t)(y + dy) * pr + xx - d]));
-        col[k] = s;
-    }
-    int sc = 0, sl = 0, sr = 0;
-#pragma unroll
-    for (int k = 0; k < 7; ++k) { sl += col[k]; sc += col[k + 3]; sr += col[k + 6]; }
-    int su = 0, sd = 0;
-#pragma unroll
-    for (int dy = -3; dy <= 3; ++dy)
-#pragma unroll
-        for (int dx = -3; dx <= 3; ++dx) {
-            const int xx = x + dx;
-            su += abs(int(L[(size_t)(y - 3 + dy) * pl + xx]) - int(Rm[(size_t)(y - 3 + dy) * pr + xx - d]));
-            sd += abs(int(L[(size_t)(y + 3 + dy) * pl + xx]) - int(Rm[(size_t)(y + 3 + dy) * pr + xx - d]));
-        }
-    return min(min(min(sc, sl), min(sr, su)), sd);
-}
-
 // Sub-pixel refinement from the merged AW keys: with d the winner relative to
 // dmin and e = dmin + d its disparity, e* = e + (c- - c+) / (2 (c- - 2 c0 + c+))
 // in IEEE FP32, skipped at d = 0, d = D-1 or when e + 1 is not searchable
-// (x - (e+1) - 6 < 0). Resets the keys.
-__global__ void aw_subpixel_kernel(uint32_t* keys, int W, int H, int D, int dmin, const uint8_t* L, size_t pl,
-                                   const uint8_t* Rm, size_t pr, void* out, size_t pitch, int type) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= W) return;
-    uint32_t* kp = &keys[(size_t)y * W + x];
-    const uint32_t key = *kp;
-    *kp = 0xFFFFFFFFu;
-    const bool valid = x >= 6 && x < W - 6 && y >= 6 && y < H - 6 && (key >> 16) != 0xFFFFu;
-    if (type != CT_PIX_F32 || !valid) {
-        store_key(out, pitch, type, x, y, valid, key, dmin);
-        return;
+// (x - (e+1) - 6 < 0). c-, c+ are the AW costs at e - 1, e + 1: the minimum
+// of the five 7x7 SADs centred at (x, y), (x -/+ 3, y), (x, y -/+ 3). Resets
+// the keys.
+// A CTA refines a 32 x 8 pixel tile. It stages the base view's 20 x 44 pixels
+// around the tile and the match view's rows over the band of columns the
+// tile's winners reach (at most 32 + 255 + 14 columns for D <= 256), then
+// each thread forms the 133 cells of its plus-shaped 13 x 13 neighbourhood
+// with both disparities in the two 16-bit halves (|b - m| + 256, as in the
+// matcher) and sums the five windows from partial column sums.
+constexpr int kSpX = 32, kSpY = 8;                   // pixels per CTA
+constexpr int kSpRows = kSpY + 12, kSpLCols = kSpX + 12;
+constexpr int kSpRCols = kSpX + 255 + 14 + 3;        // match band (padded to 304)
+
+__global__ void __launch_bounds__(kSpX * kSpY) aw_subpixel_kernel(uint32_t* keys, int W, int H, int D, int dmin,
+                                                                const uint8_t* L, size_t pl, const uint8_t* Rm,
+                                                                size_t pr, void* out, size_t pitch, int type) {
+    __shared__ uint8_t sL[kSpRows][kSpLCols];
+    __shared__ uint8_t sR[kSpRows][kSpRCols];
+    __shared__ int sRange[2];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kSpX + tx;
+    const int x0 = blockIdx.x * kSpX, y0 = blockIdx.y * kSpY;
+    const int x = x0 + tx, y = y0 + ty;
+    if (tid == 0) {
+        sRange[0] = 0x7FFFFFFF;
+        sRange[1] = -0x7FFFFFFF;
     }
+    const bool inb = x < W && y < H;
+    uint32_t key = 0xFFFFFFFFu;
+    if (inb) {
+        uint32_t* kp = &keys[(size_t)y * W + x];
+        key = *kp;
+        *kp = 0xFFFFFFFFu;
+    }
+    const bool valid = inb && x >= 6 && x < W - 6 && y >= 6 && y < H - 6 && (key >> 16) != 0xFFFFu;
     const int d = int(key & 0xFFFFu);
     const int e = dmin + d;
-    const int c0 = int(key >> 16) - box_bias(3);  // the 7x7 SAD (keys carry the box bias)
-    float s = float(e);
-    if (d > 0 && d < D - 1 && x - (e + 1) - 6 >= 0) {
-        const int cm = aw_cost_at(L, pl, Rm, pr, x, y, e - 1);
-        const int cp = aw_cost_at(L, pl, Rm, pr, x, y, e + 1);
-        const int den = cm - 2 * c0 + cp;
-        if (den > 0) s = __fadd_rn(float(e), __fdiv_rn(float(cm - cp), float(2 * den)));
+    const bool need = type == CT_PIX_F32 && valid && d > 0 && d < D - 1 && x - (e + 1) - 6 >= 0;
+    if (inb && !need) {
+        if (type != CT_PIX_F32 || !valid) store_key(out, pitch, type, x, y, valid, key, dmin);
+        else reinterpret_cast<float*>(static_cast<char*>(out) + (size_t)y * pitch)[x] = float(e);
     }
+    __syncthreads();  // sRange initialised
+    const int lo = __reduce_min_sync(0xffffffffu, need ? e : 0x7FFFFFFF);
+    const int hi = __reduce_max_sync(0xffffffffu, need ? e : -0x7FFFFFFF);
+    if ((tid & 31) == 0) {
+        atomicMin(&sRange[0], lo);
+        atomicMax(&sRange[1], hi);
+    }
+    __syncthreads();
+    const int emin = sRange[0], emax = sRange[1];
+    if (emin > emax) return;  // no pixel of the tile is refined
+    // match band: column rx0 + c for c < bw (emax - emin <= D - 1 <= 255)
+    const int rx0 = x0 - emax - 7, bw = emax - emin + kSpX + 14;
+    for (int i = tid; i < kSpRows * kSpLCols; i += kSpX * kSpY) {
+        const int r = i / kSpLCols, c = i - r * kSpLCols;
+        const int gy = y0 - 6 + r, gx = x0 - 6 + c;
+        sL[r][c] = (gy >= 0 && gy < H && gx >= 0 && gx < W) ? L[(size_t)gy * pl + gx] : 0;
+    }
+    for (int i = tid; i < kSpRows * bw; i += kSpX * kSpY) {
+        const int r = i / bw, c = i - r * bw;
+        const int gy = y0 - 6 + r, gx = rx0 + c;
+        sR[r][c] = (gy >= 0 && gy < H && gx >= 0 && gx < W) ? Rm[(size_t)gy * pr + gx] : 0;
+    }
+    __syncthreads();
+    if (!need) return;
+    // cell (r, k): row y - 6 + r, column x - 6 + k; base pixel sL[ty + r][tx + k];
+    // match pixel of disparity e -/+ 1 at band column base + k + 2 / base + k
+    const int base = x - e - 7 - rx0;
+    auto cell = [&](int r, int k) {
+        const uint32_t b2 = uint32_t(sL[ty + r][tx + k]) * 0x10001u;
+        const uint32_t m2 = uint32_t(sR[ty + r][base + k + 2]) + (uint32_t(sR[ty + r][base + k]) << 16);
+        return __vmaxu2(b2 + kAbsBias - m2, m2 + kAbsBias - b2);  // (|b - m-| + 256) | (|b - m+| + 256) << 16
+    };
+    // partial column sums: top rows 0-2, middle 3-5, centre 6, lower 7-9, bottom 10-12
+    uint32_t mid[13], sl = 0, sc = 0, sr = 0, su = 0, sd = 0;
+#pragma unroll
+    for (int k = 0; k < 13; ++k) {
+        uint32_t a = 0, m = cell(6, k), c = 0;
+#pragma unroll
+        for (int r = 3; r < 6; ++r) a += cell(r, k);
+#pragma unroll
+        for (int r = 7; r < 10; ++r) c += cell(r, k);
+        mid[k] = a + m + c;
+        if (k >= 3 && k <= 9) {
+            uint32_t t = 0, b = 0;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) t += cell(r, k);
+#pragma unroll
+            for (int r = 10; r < 13; ++r) b += cell(r, k);
+            su += t + a + m;
+            sd += m + c + b;
+            sc += mid[k];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+        sl += mid[k];
+        sr += mid[k + 6];
+    }
+    const uint32_t mn = __vminu2(__vminu2(__vminu2(sc, sl), __vminu2(sr, su)), sd);
+    const int cm = int(mn & 0xFFFFu) - box_bias(3), cp = int(mn >> 16) - box_bias(3);
+    const int c0 = int(key >> 16) - box_bias(3);  // the winner's 7x7 AW cost (keys carry the box bias)
+    float s = float(e);
+    const int den = cm - 2 * c0 + cp;
+    if (den > 0) s = __fadd_rn(float(e), __fdiv_rn(float(cm - cp), float(2 * den)));
     reinterpret_cast<float*>(static_cast<char*>(out) + (size_t)y * pitch)[x] = s;
 }
 
@@ -460,7 +513,7 @@ int launch_ad(AdHandle* h, const ct_image* disp, const ct_image* L, const ct_ima
     CT_LAUNCH_CHECK();
     const ct_image* base = DIR == 0 ? L : Rimg;
     if (AW) {
-        aw_subpixel_kernel<<<dim3((W + 127) / 128, H), 128, 0, s>>>(
+        aw_subpixel_kernel<<<dim3((W + kSpX - 1) / kSpX, (H + kSpY - 1) / kSpY), dim3(kSpX, kSpY), 0, s>>>(
             h->keys, W, H, h->D, h->dmin, static_cast<const uint8_t*>(L->ptr), L->pitch_bytes,
             static_cast<const uint8_t*>(Rimg->ptr), Rimg->pitch_bytes, disp->ptr, disp->pitch_bytes, disp->type);
         CT_LAUNCH_CHECK();
