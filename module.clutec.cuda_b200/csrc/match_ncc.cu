@@ -34,35 +34,52 @@ __host__ __device__ constexpr size_t smem_bytes(int th, int R) {
 // and (T non-null) the zero-score threshold of the left view: the smallest vy
 // with V * vy >= n^4, i.e. ceil(n^4 / V) (INT_MAX when V = 0), so that the
 // matcher's test sigma_x sigma_y >= 1 is one 32-bit compare vy >= T.
+// Separable: a CTA stages a (32 + 2R) x (8 + 2R) tile, sums every staged row
+// horizontally (S and Q of 2R+1 pixels) into shared memory, then each thread
+// sums its column of 2R+1 row sums.
 template <int R>
-__global__ void box_stats_kernel(const uint8_t* img, size_t pitch, int W, int H, int32_t* S, int32_t* V,
-                                 int32_t* T) {
+__global__ void __launch_bounds__(256) box_stats_kernel(const uint8_t* img, size_t pitch, int W, int H, int32_t* S,
+                                                        int32_t* V, int32_t* T) {
     constexpr int TX = 32, TY = 8, SW = TX + 2 * R, SH = TY + 2 * R;
     __shared__ uint8_t t[SH][SW];
+    __shared__ int hs[SH][TX], hq[SH][TX];
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-    for (int i = threadIdx.y * TX + threadIdx.x; i < SW * SH; i += TX * TY) {
+    const int tid = threadIdx.y * TX + threadIdx.x;
+    for (int i = tid; i < SW * SH; i += TX * TY) {
         const int yy = y0 - R + i / SW, xx = x0 - R + i % SW;
         t[i / SW][i % SW] = (xx >= 0 && xx < W && yy >= 0 && yy < H) ? img[(size_t)yy * pitch + xx] : 0;
+    }
+    __syncthreads();
+    for (int i = tid; i < SH * TX; i += TX * TY) {
+        const int r = i / TX, c = i % TX;
+        int s = 0, q = 0;
+#pragma unroll
+        for (int dx = 0; dx <= 2 * R; ++dx) {
+            const int v = t[r][c + dx];
+            s += v;
+            q += v * v;
+        }
+        hs[r][c] = s;
+        hq[r][c] = q;
     }
     __syncthreads();
     const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
     if (x >= W || y >= H) return;
     int s = 0, q = 0;
 #pragma unroll
-    for (int dy = 0; dy <= 2 * R; ++dy)
-#pragma unroll
-        for (int dx = 0; dx <= 2 * R; ++dx) {
-            const int v = t[threadIdx.y + dy][threadIdx.x + dx];
-            s += v;
-            q += v * v;
-        }
+    for (int dy = 0; dy <= 2 * R; ++dy) {
+        s += hs[threadIdx.y + dy][threadIdx.x];
+        q += hq[threadIdx.y + dy][threadIdx.x];
+    }
     constexpr int n = (2 * R + 1) * (2 * R + 1);
     constexpr long long n4 = (long long)n * n * n * n;
     static_assert(n4 < 0x7FFFFFFFll, "the threshold fits in int32");
+    // n^4 + V - 1 < 2^32 (V <= n^2 255^2 / 4): one 32-bit division
+    static_assert(n4 + (long long)n * n * 255 * 255 / 4 < 0xFFFFFFFFll, "32-bit threshold division");
     const int v = n * q - s * s;
     S[(size_t)y * W + x] = s;
     V[(size_t)y * W + x] = v;
-    if (T) T[(size_t)y * W + x] = v > 0 ? int32_t((n4 + v - 1) / v) : 0x7FFFFFFF;
+    if (T) T[(size_t)y * W + x] = v > 0 ? int32_t((uint32_t(n4) + uint32_t(v) - 1u) / uint32_t(v)) : 0x7FFFFFFF;
 }
 
 __device__ __forceinline__ uint32_t ordered(float f) {
@@ -82,7 +99,8 @@ struct Args {
     int guide_gw;
     const int32_t *Sx, *Vx, *Sy, *Vy;   // stats of the left / right image (W*H)
     const int32_t* Tx;                  // zero-score threshold of the left image (box_stats_kernel)
-    unsigned long long* keys;          // global keys when gridDim.z > 1
+    unsigned long long* keys;          // global keys when gridDim.z > 1 (0 between calls)
+    uint32_t* counters;                // gridDim.z > 1: CTAs done per (strip, column tile), 0 between calls
     void* out;
     size_t out_pitch;
     int out_type;
@@ -152,10 +170,10 @@ __global__ void __launch_bounds__(kNT, 2)
         dev::tma_load_2d(sM, &tmM, am, y0 - R, bar);
     }
     const bool got = dev::mbar_wait_bounded(bar, 0);
-    if (__syncthreads_or(!got)) {
-        if (tid == 0) dev::report(a.status, CT_ETIMEOUT);
-        return;
-    }
+    // a strip that never arrived: report, match nothing, still take part in
+    // the merge below so that the group's counter and keys stay consistent
+    const bool aborted = __syncthreads_or(!got);
+    if (aborted && tid == 0) dev::report(a.status, CT_ETIMEOUT);
     const int bo = xs - ab + 4 * lane;
     const int mo = (xs - a.dmin - dz0 - am) + 4 * lane - kDPW * warp - 7;
 
@@ -165,7 +183,7 @@ __global__ void __launch_bounds__(kNT, 2)
 #pragma unroll
         for (int c = 0; c < kCPT; ++c) V[j][c] = 0;
 
-    if (warp_active && searches) {
+    if (warp_active && searches && !aborted) {
         for (int i = 0; i < NR; ++i) {
             {
                 const uint8_t* rb = sB + i * kBW + bo;
@@ -349,16 +367,32 @@ __global__ void __launch_bounds__(kNT, 2)
             atomicMax(&a.keys[(size_t)y * a.W + x], key);
         }
     }
-}
-
-__global__ void ncc_finalize_kernel(Args a, int R) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= a.W) return;
-    unsigned long long* kp = &a.keys[(size_t)y * a.W + x];
-    const unsigned long long key = *kp;
-    *kp = 0ull;
-    const bool valid = x >= R && x < a.W - R && y >= R && y < a.H - R;
-    store_ncc(a, x, y, valid, key);
+    if (direct) return;
+    // D split over gridDim.z CTAs: the last of the (strip, column tile) group
+    // to finish writes the merged keys as the outputs and resets keys and
+    // counter. Writers fence before counting; the merger fences after.
+    __threadfence();
+    __syncthreads();
+    int* last = reinterpret_cast<int*>(bar + 1);
+    if (tid == 0) {
+        uint32_t* ctr = &a.counters[blockIdx.y * gridDim.x + blockIdx.x];
+        const bool l = atomicAdd(ctr, 1u) == gridDim.z - 1;
+        if (l) *ctr = 0u;
+        *last = l;
+    }
+    __syncthreads();
+    if (!*last) return;
+    __threadfence();
+    for (int idx = tid; idx < a.th * TWO; idx += kNT) {
+        const int oy = idx / TWO, ox = idx - oy * TWO;
+        const int x = xs + R + ox, y = y0 + oy;
+        if (x >= a.W || y >= a.H) continue;
+        unsigned long long* kp = &a.keys[(size_t)y * a.W + x];
+        const unsigned long long key = __ldcg(kp);
+        *kp = 0ull;
+        const bool valid = x >= R && x < a.W - R && y >= R && y < a.H - R;
+        store_ncc(a, x, y, valid, key);
+    }
 }
 
 }  // namespace ncc
@@ -372,12 +406,14 @@ struct NccHandle : ct_handle {
         cudaFree(stats);
         cudaFree(keys);
         cudaFree(guide);
+        cudaFree(counters);
     }
     ct_format fmt{};
     ct_ncc_params par{};
     int32_t* stats = nullptr;  // Sx, Vx, Sy, Vy, Tx
     unsigned long long* keys = nullptr;
     uint32_t* guide = nullptr;  // guided mode: one search range per 16 x 16 block
+    uint32_t* counters = nullptr;  // one per (strip, column tile) at the smallest strip height
     int th = 32;
 };
 
@@ -399,6 +435,7 @@ int launch_ncc(NccHandle* h, const ct_image* disp, const ct_image* score, const 
     a.Sx = h->stats; a.Vx = h->stats + N; a.Sy = h->stats + 2 * N; a.Vy = h->stats + 3 * N;
     a.Tx = h->stats + 4 * N;
     a.keys = h->keys;
+    a.counters = h->counters;
     a.out = disp->ptr; a.out_pitch = disp->pitch_bytes; a.out_type = disp->type;
     a.score = score ? static_cast<float*>(score->ptr) : nullptr;
     a.score_pitch = score ? score->pitch_bytes : 0;
@@ -426,10 +463,6 @@ int launch_ncc(NccHandle* h, const ct_image* disp, const ct_image* score, const 
     dim3 grid((W + two_of(R) - 1) / two_of(R), (H + a.th - 1) / a.th, (a.D + kDPC - 1) / kDPC);
     ncc_match_kernel<R><<<grid, kNT, smem_bytes(a.th, R), s>>>(tb, tm, a);
     CT_LAUNCH_CHECK();
-    if (grid.z > 1) {
-        ncc_finalize_kernel<<<dim3((W + 255) / 256, H), 256, 0, s>>>(a, R);
-        CT_LAUNCH_CHECK();
-    }
     return gate_launch(disp, score, L, 0, 2 * R + 1, h->grad_thresh, s);  // EvalGrad (NCC.cu:388-413)
 }
 
@@ -462,8 +495,8 @@ int ct_bm_ncc_configure(ct_handle* hh, int32_t device, const ct_format* fmt, con
     if (p->disp_min < 0 || p->disp_min + p->disp_count > 0xFFEF)
         return fail(CT_EINVAL, "disp_min must be >= 0 with disp_min + disp_count <= 65519");
     if (int rc = use_device(device)) return rc;
-    cudaFree(h->stats); cudaFree(h->keys); cudaFree(h->guide);
-    h->stats = nullptr; h->keys = nullptr; h->guide = nullptr;
+    cudaFree(h->stats); cudaFree(h->keys); cudaFree(h->guide); cudaFree(h->counters);
+    h->stats = nullptr; h->keys = nullptr; h->guide = nullptr; h->counters = nullptr;
     h->device = device;
     if (int rc = h->init_status()) return rc;
     const size_t N = (size_t)fmt->width * fmt->height;
@@ -473,6 +506,12 @@ int ct_bm_ncc_configure(ct_handle* hh, int32_t device, const ct_format* fmt, con
     const size_t G = size_t((fmt->width + ncc::kGuideBlock - 1) / ncc::kGuideBlock) *
                      ((fmt->height + ncc::kGuideBlock - 1) / ncc::kGuideBlock);
     if (cudaMalloc(&h->guide, G * sizeof(uint32_t)) != cudaSuccess) return fail(CT_ENOMEM, "guide ranges");
+    {  // merge counters for every strip height the configuration below may pick (>= 8 rows)
+        const size_t C = size_t((fmt->width + ncc::two_of(p->radius) - 1) / ncc::two_of(p->radius)) *
+                         ((fmt->height + 7) / 8);
+        if (cudaMalloc(&h->counters, C * sizeof(uint32_t)) != cudaSuccess) return fail(CT_ENOMEM, "merge counters");
+        CT_CUDA_TRY(cudaMemset(h->counters, 0, C * sizeof(uint32_t)));
+    }
     h->fmt = *fmt;
     h->par = *p;
     {  // strip height: 32 rows (measured faster at 1080p than the taller strips
