@@ -331,21 +331,22 @@ __global__ void ad_finalize_kernel(uint32_t* keys, int W, int H, int ext, void* 
 // (x - (e+1) - 6 < 0). c-, c+ are the AW costs at e - 1, e + 1: the minimum
 // of the five 7x7 SADs centred at (x, y), (x -/+ 3, y), (x, y -/+ 3). Resets
 // the keys.
-// A CTA refines a 32 x 8 pixel tile. It stages the base view's 20 x 44 pixels
-// around the tile and the match view's rows over the band of columns the
-// tile's winners reach (at most 32 + 255 + 14 columns for D <= 256), then
+// A CTA refines a 32 x 8 pixel tile. It stages the base view's 20 rows x 64
+// columns around the tile and the match view's rows over the band of columns
+// the tile's winners reach (at most 21 16-byte chunks for D <= 256), then
 // each thread forms the 133 cells of its plus-shaped 13 x 13 neighbourhood
 // with both disparities in the two 16-bit halves (|b - m| + 256, as in the
 // matcher) and sums the five windows from partial column sums.
 constexpr int kSpX = 32, kSpY = 8;                   // pixels per CTA
-constexpr int kSpRows = kSpY + 12, kSpLCols = kSpX + 12;
-constexpr int kSpRCols = kSpX + 255 + 14 + 3;        // match band (padded to 304)
+constexpr int kSpRows = kSpY + 12;
+constexpr int kSpLCols = 64;                         // base columns x0 - 16 .. x0 + 47 (16-byte chunks)
+constexpr int kSpRCols = 21 * 16;                    // match band rounded out to 16-byte chunks
 
 __global__ void __launch_bounds__(kSpX * kSpY) aw_subpixel_kernel(uint32_t* keys, int W, int H, int D, int dmin,
                                                                 const uint8_t* L, size_t pl, const uint8_t* Rm,
                                                                 size_t pr, void* out, size_t pitch, int type) {
-    __shared__ uint8_t sL[kSpRows][kSpLCols];
-    __shared__ uint8_t sR[kSpRows][kSpRCols];
+    __shared__ __align__(16) uint8_t sL[kSpRows][kSpLCols];
+    __shared__ __align__(16) uint8_t sR[kSpRows][kSpRCols];
     __shared__ int sRange[2];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kSpX + tx;
     const int x0 = blockIdx.x * kSpX, y0 = blockIdx.y * kSpY;
@@ -379,25 +380,44 @@ __global__ void __launch_bounds__(kSpX * kSpY) aw_subpixel_kernel(uint32_t* keys
     __syncthreads();
     const int emin = sRange[0], emax = sRange[1];
     if (emin > emax) return;  // no pixel of the tile is refined
-    // match band: column rx0 + c for c < bw (emax - emin <= D - 1 <= 255)
-    const int rx0 = x0 - emax - 7, bw = emax - emin + kSpX + 14;
-    for (int i = tid; i < kSpRows * kSpLCols; i += kSpX * kSpY) {
-        const int r = i / kSpLCols, c = i - r * kSpLCols;
-        const int gy = y0 - 6 + r, gx = x0 - 6 + c;
-        sL[r][c] = (gy >= 0 && gy < H && gx >= 0 && gx < W) ? L[(size_t)gy * pl + gx] : 0;
+    // Staged in 16-byte chunks (the images' rows start 16-byte aligned, as
+    // their TMA maps require); a chunk reaching past the width is read byte
+    // by byte, chunks outside the image read 0. Base: columns x0 - 16 + c;
+    // match band: columns rs + c covering x0 - emax - 7 .. x0 + 38 - emin
+    // (emax - emin <= D - 3 <= 253: at most 21 chunks).
+    const int rs = (x0 - emax - 7) & ~15;
+    const int nch = (x0 + 38 - emin - rs) / 16 + 1;
+    auto chunk = [&](const uint8_t* img, size_t pitch, int gy, int gx, uint8_t* dst) {
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (gy >= 0 && gy < H && gx >= 0 && gx < W) {
+            const uint8_t* src = img + (size_t)gy * pitch + gx;
+            if (gx + 16 <= W) {
+                v = *reinterpret_cast<const uint4*>(src);
+            } else {
+                uint32_t w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+                for (int k = 0; k < 16; ++k)
+                    if (gx + k < W) w[k >> 2] |= uint32_t(src[k]) << (8 * (k & 3));
+                v = make_uint4(w[0], w[1], w[2], w[3]);
+            }
+        }
+        *reinterpret_cast<uint4*>(dst) = v;
+    };
+    for (int i = tid; i < kSpRows * (kSpLCols / 16); i += kSpX * kSpY) {
+        const int r = i / (kSpLCols / 16), j = i - r * (kSpLCols / 16);
+        chunk(L, pl, y0 - 6 + r, x0 - 16 + 16 * j, &sL[r][16 * j]);
     }
-    for (int i = tid; i < kSpRows * bw; i += kSpX * kSpY) {
-        const int r = i / bw, c = i - r * bw;
-        const int gy = y0 - 6 + r, gx = rx0 + c;
-        sR[r][c] = (gy >= 0 && gy < H && gx >= 0 && gx < W) ? Rm[(size_t)gy * pr + gx] : 0;
+    for (int i = tid; i < kSpRows * nch; i += kSpX * kSpY) {
+        const int r = i / nch, j = i - r * nch;
+        chunk(Rm, pr, y0 - 6 + r, rs + 16 * j, &sR[r][16 * j]);
     }
     __syncthreads();
     if (!need) return;
-    // cell (r, k): row y - 6 + r, column x - 6 + k; base pixel sL[ty + r][tx + k];
+    // cell (r, k): row y - 6 + r, column x - 6 + k; base pixel sL[ty + r][tx + 10 + k];
     // match pixel of disparity e -/+ 1 at band column base + k + 2 / base + k
-    const int base = x - e - 7 - rx0;
+    const int base = x - e - 7 - rs;
     auto cell = [&](int r, int k) {
-        const uint32_t b2 = uint32_t(sL[ty + r][tx + k]) * 0x10001u;
+        const uint32_t b2 = uint32_t(sL[ty + r][tx + 10 + k]) * 0x10001u;
         const uint32_t m2 = uint32_t(sR[ty + r][base + k + 2]) + (uint32_t(sR[ty + r][base + k]) << 16);
         return __vmaxu2(b2 + kAbsBias - m2, m2 + kAbsBias - b2);  // (|b - m-| + 256) | (|b - m+| + 256) << 16
     };
