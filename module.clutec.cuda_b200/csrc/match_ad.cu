@@ -331,48 +331,61 @@ __global__ void ad_finalize_kernel(uint32_t* keys, int W, int H, int ext, void* 
 // (x - (e+1) - 6 < 0). c-, c+ are the AW costs at e - 1, e + 1: the minimum
 // of the five 7x7 SADs centred at (x, y), (x -/+ 3, y), (x, y -/+ 3). Resets
 // the keys.
-// A CTA refines a 32 x 8 pixel tile. It stages the base view's 20 rows x 64
-// columns around the tile and the match view's rows over the band of columns
-// the tile's winners reach (at most 21 16-byte chunks for D <= 256), then
+// A CTA refines a 32 x 16 pixel tile (two rows per thread). It stages the
+// base view's 28 rows x 64 columns around the tile and the match view's rows
+// over the band of columns the tile's winners reach (at most 21 16-byte
+// chunks for D <= 256), then
 // each thread forms the 133 cells of its plus-shaped 13 x 13 neighbourhood
 // with both disparities in the two 16-bit halves (|b - m| + 256, as in the
 // matcher) and sums the five windows from partial column sums.
-constexpr int kSpX = 32, kSpY = 8;                   // pixels per CTA
+constexpr int kSpX = 32, kSpTY = 8, kSpQ = 2, kSpY = kSpTY * kSpQ;  // 32 x 16 pixels, 2 rows per thread
 constexpr int kSpRows = kSpY + 12;
 constexpr int kSpLCols = 64;                         // base columns x0 - 16 .. x0 + 47 (16-byte chunks)
 constexpr int kSpRCols = 21 * 16;                    // match band rounded out to 16-byte chunks
 
-__global__ void __launch_bounds__(kSpX * kSpY) aw_subpixel_kernel(uint32_t* keys, int W, int H, int D, int dmin,
-                                                                const uint8_t* L, size_t pl, const uint8_t* Rm,
-                                                                size_t pr, void* out, size_t pitch, int type) {
+__global__ void __launch_bounds__(kSpX * kSpTY) aw_subpixel_kernel(uint32_t* keys, int W, int H, int D, int dmin,
+                                                                 const uint8_t* L, size_t pl, const uint8_t* Rm,
+                                                                 size_t pr, void* out, size_t pitch, int type) {
     __shared__ __align__(16) uint8_t sL[kSpRows][kSpLCols];
     __shared__ __align__(16) uint8_t sR[kSpRows][kSpRCols];
     __shared__ int sRange[2];
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kSpX + tx;
+    const int tx = threadIdx.x, tid = threadIdx.y * kSpX + tx;
     const int x0 = blockIdx.x * kSpX, y0 = blockIdx.y * kSpY;
-    const int x = x0 + tx, y = y0 + ty;
+    const int x = x0 + tx;
     if (tid == 0) {
         sRange[0] = 0x7FFFFFFF;
         sRange[1] = -0x7FFFFFFF;
     }
-    const bool inb = x < W && y < H;
-    uint32_t key = 0xFFFFFFFFu;
-    if (inb) {
-        uint32_t* kp = &keys[(size_t)y * W + x];
-        key = *kp;
-        *kp = 0xFFFFFFFFu;
-    }
-    const bool valid = inb && x >= 6 && x < W - 6 && y >= 6 && y < H - 6 && (key >> 16) != 0xFFFFu;
-    const int d = int(key & 0xFFFFu);
-    const int e = dmin + d;
-    const bool need = type == CT_PIX_F32 && valid && d > 0 && d < D - 1 && x - (e + 1) - 6 >= 0;
-    if (inb && !need) {
-        if (type != CT_PIX_F32 || !valid) store_key(out, pitch, type, x, y, valid, key, dmin);
-        else reinterpret_cast<float*>(static_cast<char*>(out) + (size_t)y * pitch)[x] = float(e);
+    // this thread's pixels: rows ty = threadIdx.y + 8 q of the tile
+    uint32_t key[kSpQ];
+    bool need[kSpQ];
+    int lo = 0x7FFFFFFF, hi = -0x7FFFFFFF;
+#pragma unroll
+    for (int q = 0; q < kSpQ; ++q) {
+        const int y = y0 + threadIdx.y + kSpTY * q;
+        const bool inb = x < W && y < H;
+        key[q] = 0xFFFFFFFFu;
+        if (inb) {
+            uint32_t* kp = &keys[(size_t)y * W + x];
+            key[q] = *kp;
+            *kp = 0xFFFFFFFFu;
+        }
+        const bool valid = inb && x >= 6 && x < W - 6 && y >= 6 && y < H - 6 && (key[q] >> 16) != 0xFFFFu;
+        const int d = int(key[q] & 0xFFFFu);
+        const int e = dmin + d;
+        need[q] = type == CT_PIX_F32 && valid && d > 0 && d < D - 1 && x - (e + 1) - 6 >= 0;
+        if (inb && !need[q]) {
+            if (type != CT_PIX_F32 || !valid) store_key(out, pitch, type, x, y, valid, key[q], dmin);
+            else reinterpret_cast<float*>(static_cast<char*>(out) + (size_t)y * pitch)[x] = float(e);
+        }
+        if (need[q]) {
+            lo = min(lo, e);
+            hi = max(hi, e);
+        }
     }
     __syncthreads();  // sRange initialised
-    const int lo = __reduce_min_sync(0xffffffffu, need ? e : 0x7FFFFFFF);
-    const int hi = __reduce_max_sync(0xffffffffu, need ? e : -0x7FFFFFFF);
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
     if ((tid & 31) == 0) {
         atomicMin(&sRange[0], lo);
         atomicMax(&sRange[1], hi);
@@ -387,10 +400,10 @@ __global__ void __launch_bounds__(kSpX * kSpY) aw_subpixel_kernel(uint32_t* keys
     // (emax - emin <= D - 3 <= 253: at most 21 chunks).
     const int rs = (x0 - emax - 7) & ~15;
     const int nch = (x0 + 38 - emin - rs) / 16 + 1;
-    auto chunk = [&](const uint8_t* img, size_t pitch, int gy, int gx, uint8_t* dst) {
+    auto chunk = [&](const uint8_t* img, size_t ip, int gy, int gx, uint8_t* dst) {
         uint4 v = make_uint4(0, 0, 0, 0);
         if (gy >= 0 && gy < H && gx >= 0 && gx < W) {
-            const uint8_t* src = img + (size_t)gy * pitch + gx;
+            const uint8_t* src = img + (size_t)gy * ip + gx;
             if (gx + 16 <= W) {
                 v = *reinterpret_cast<const uint4*>(src);
             } else {
@@ -403,57 +416,62 @@ __global__ void __launch_bounds__(kSpX * kSpY) aw_subpixel_kernel(uint32_t* keys
         }
         *reinterpret_cast<uint4*>(dst) = v;
     };
-    for (int i = tid; i < kSpRows * (kSpLCols / 16); i += kSpX * kSpY) {
+    for (int i = tid; i < kSpRows * (kSpLCols / 16); i += kSpX * kSpTY) {
         const int r = i / (kSpLCols / 16), j = i - r * (kSpLCols / 16);
         chunk(L, pl, y0 - 6 + r, x0 - 16 + 16 * j, &sL[r][16 * j]);
     }
-    for (int i = tid; i < kSpRows * nch; i += kSpX * kSpY) {
+    for (int i = tid; i < kSpRows * nch; i += kSpX * kSpTY) {
         const int r = i / nch, j = i - r * nch;
         chunk(Rm, pr, y0 - 6 + r, rs + 16 * j, &sR[r][16 * j]);
     }
     __syncthreads();
-    if (!need) return;
-    // cell (r, k): row y - 6 + r, column x - 6 + k; base pixel sL[ty + r][tx + 10 + k];
-    // match pixel of disparity e -/+ 1 at band column base + k + 2 / base + k
-    const int base = x - e - 7 - rs;
-    auto cell = [&](int r, int k) {
-        const uint32_t b2 = uint32_t(sL[ty + r][tx + 10 + k]) * 0x10001u;
-        const uint32_t m2 = uint32_t(sR[ty + r][base + k + 2]) + (uint32_t(sR[ty + r][base + k]) << 16);
-        return __vmaxu2(b2 + kAbsBias - m2, m2 + kAbsBias - b2);  // (|b - m-| + 256) | (|b - m+| + 256) << 16
-    };
-    // partial column sums: top rows 0-2, middle 3-5, centre 6, lower 7-9, bottom 10-12
-    uint32_t mid[13], sl = 0, sc = 0, sr = 0, su = 0, sd = 0;
 #pragma unroll
-    for (int k = 0; k < 13; ++k) {
-        uint32_t a = 0, m = cell(6, k), c = 0;
+    for (int q = 0; q < kSpQ; ++q) {
+        if (!need[q]) continue;
+        const int ty = threadIdx.y + kSpTY * q, y = y0 + ty;
+        const int e = dmin + int(key[q] & 0xFFFFu);
+        // cell (r, k): row y - 6 + r, column x - 6 + k; base pixel sL[ty + r][tx + 10 + k];
+        // match pixel of disparity e -/+ 1 at band column base + k + 2 / base + k
+        const int base = x - e - 7 - rs;
+        auto cell = [&](int r, int k) {
+            const uint32_t b2 = uint32_t(sL[ty + r][tx + 10 + k]) * 0x10001u;
+            const uint32_t m2 = uint32_t(sR[ty + r][base + k + 2]) + (uint32_t(sR[ty + r][base + k]) << 16);
+            return __vmaxu2(b2 + kAbsBias - m2, m2 + kAbsBias - b2);  // (|b - m-| + 256) | (|b - m+| + 256) << 16
+        };
+        // partial column sums: top rows 0-2, middle 3-5, centre 6, lower 7-9, bottom 10-12
+        uint32_t mid[13], sl = 0, sc = 0, sr = 0, su = 0, sd = 0;
 #pragma unroll
-        for (int r = 3; r < 6; ++r) a += cell(r, k);
+        for (int k = 0; k < 13; ++k) {
+            uint32_t a = 0, m = cell(6, k), c = 0;
 #pragma unroll
-        for (int r = 7; r < 10; ++r) c += cell(r, k);
-        mid[k] = a + m + c;
-        if (k >= 3 && k <= 9) {
-            uint32_t t = 0, b = 0;
+            for (int r = 3; r < 6; ++r) a += cell(r, k);
 #pragma unroll
-            for (int r = 0; r < 3; ++r) t += cell(r, k);
+            for (int r = 7; r < 10; ++r) c += cell(r, k);
+            mid[k] = a + m + c;
+            if (k >= 3 && k <= 9) {
+                uint32_t t = 0, b = 0;
 #pragma unroll
-            for (int r = 10; r < 13; ++r) b += cell(r, k);
-            su += t + a + m;
-            sd += m + c + b;
-            sc += mid[k];
+                for (int r = 0; r < 3; ++r) t += cell(r, k);
+#pragma unroll
+                for (int r = 10; r < 13; ++r) b += cell(r, k);
+                su += t + a + m;
+                sd += m + c + b;
+                sc += mid[k];
+            }
         }
-    }
 #pragma unroll
-    for (int k = 0; k < 7; ++k) {
-        sl += mid[k];
-        sr += mid[k + 6];
+        for (int k = 0; k < 7; ++k) {
+            sl += mid[k];
+            sr += mid[k + 6];
+        }
+        const uint32_t mn = __vminu2(__vminu2(__vminu2(sc, sl), __vminu2(sr, su)), sd);
+        const int cm = int(mn & 0xFFFFu) - box_bias(3), cp = int(mn >> 16) - box_bias(3);
+        const int c0 = int(key[q] >> 16) - box_bias(3);  // the winner's 7x7 AW cost (keys carry the box bias)
+        float sp = float(e);
+        const int den = cm - 2 * c0 + cp;
+        if (den > 0) sp = __fadd_rn(float(e), __fdiv_rn(float(cm - cp), float(2 * den)));
+        reinterpret_cast<float*>(static_cast<char*>(out) + (size_t)y * pitch)[x] = sp;
     }
-    const uint32_t mn = __vminu2(__vminu2(__vminu2(sc, sl), __vminu2(sr, su)), sd);
-    const int cm = int(mn & 0xFFFFu) - box_bias(3), cp = int(mn >> 16) - box_bias(3);
-    const int c0 = int(key >> 16) - box_bias(3);  // the winner's 7x7 AW cost (keys carry the box bias)
-    float s = float(e);
-    const int den = cm - 2 * c0 + cp;
-    if (den > 0) s = __fadd_rn(float(e), __fdiv_rn(float(cm - cp), float(2 * den)));
-    reinterpret_cast<float*>(static_cast<char*>(out) + (size_t)y * pitch)[x] = s;
 }
 
 }  // namespace ad
@@ -533,7 +551,7 @@ int launch_ad(AdHandle* h, const ct_image* disp, const ct_image* L, const ct_ima
     CT_LAUNCH_CHECK();
     const ct_image* base = DIR == 0 ? L : Rimg;
     if (AW) {
-        aw_subpixel_kernel<<<dim3((W + kSpX - 1) / kSpX, (H + kSpY - 1) / kSpY), dim3(kSpX, kSpY), 0, s>>>(
+        aw_subpixel_kernel<<<dim3((W + kSpX - 1) / kSpX, (H + kSpY - 1) / kSpY), dim3(kSpX, kSpTY), 0, s>>>(
             h->keys, W, H, h->D, h->dmin, static_cast<const uint8_t*>(L->ptr), L->pitch_bytes,
             static_cast<const uint8_t*>(Rimg->ptr), Rimg->pitch_bytes, disp->ptr, disp->pitch_bytes, disp->type);
         CT_LAUNCH_CHECK();
