@@ -65,6 +65,7 @@ __host__ __device__ inline bool is_weight(int p) {
 }
 
 __device__ __forceinline__ float bf16r(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
+__device__ __forceinline__ uint16_t bf16_bits(float v) { return __bfloat16_as_ushort(__float2bfloat16_rn(v)); }
 
 // ---------------------------------------------------------------------------
 // Gather: samples[n][128] from a curve volume at pixel list xy[n][2]
@@ -124,98 +125,89 @@ struct Act {  // per-sample activations and gradient signals, [n][...]
     float* dz3;     // [32]
     float* dz2;     // [2][32]
     float* dm1;     // [7][32]
+    // bf16 operands of the tensor-core GEMMs (tg::gemm_kernel): row-major
+    // [n][features] and transposed [features][ldt] (samples contiguous;
+    // columns n .. n rounded up to 8 hold 0)
+    uint16_t *a1p, *a1pt;  // [n][256]: slot 0 = 0, slots 1..7 = conv1 positions 0..6; [256][ldt]
+    uint16_t *a2b, *a2t, *a3b, *a3t;
+    uint16_t *dz4b, *dz4t, *dz3b, *dz3t, *dz2b, *dz2t;
+    float* d;              // GEMM output scratch [n][224]
+    int ldt;
 };
 constexpr int kQ = 7;   // pooled conv1 positions
 constexpr int kR = 2;   // conv2 positions
 
 constexpr int kSY = 16;  // samples per CTA
 
-// conv1 (k=5, stride 5) over the 35 central codes, ReLU, bf16
+// conv1 (k=5, stride 5) over the 35 central codes, ReLU, bf16; also the
+// bf16 operand copies of the conv2 GEMMs (forward and weight gradient)
 __global__ void __launch_bounds__(32 * kSY) fwd1_kernel(const uint8_t* x, const float* wq, Act A, int n) {
     __shared__ float xs[kSY][kLen];
     const int o = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * kSY + sl;
     for (int k = threadIdx.x; k < kLen; k += 32) xs[sl][k] = s < n ? float(x[(size_t)s * kLen + k]) : 0.f;
     __syncthreads();
-    if (s >= n) return;
+    if (s >= ((n + 7) & ~7)) return;
+    if (s >= n) {  // transposed columns past n read as 0
+#pragma unroll
+        for (int q = 0; q <= kQ; ++q) A.a1pt[(size_t)(q * 32 + o) * A.ldt + s] = 0;
+        return;
+    }
     float w[5];
 #pragma unroll
     for (int j = 0; j < 5; ++j) w[j] = wq[kOffW1 + o * 5 + j];
     const float b = wq[kOffB1 + o];
+    A.a1p[(size_t)s * 256 + o] = 0;
+    A.a1pt[(size_t)o * A.ldt + s] = 0;
 #pragma unroll
     for (int q = 0; q < kQ; ++q) {
         float z = b;
 #pragma unroll
         for (int j = 0; j < 5; ++j) z = fmaf(w[j], xs[sl][kCropLo + 5 * q + j], z);
-        A.a1[(size_t)s * 224 + q * 32 + o] = bf16r(fmaxf(z, 0.f));
+        const float v = bf16r(fmaxf(z, 0.f));
+        A.a1[(size_t)s * 224 + q * 32 + o] = v;
+        const uint16_t vb = bf16_bits(v);
+        A.a1p[(size_t)s * 256 + (q + 1) * 32 + o] = vb;
+        A.a1pt[(size_t)((q + 1) * 32 + o) * A.ldt + s] = vb;
     }
 }
 
-// conv2 (k=5, stride 3, pad 1): 2 positions
-__global__ void __launch_bounds__(32 * kSY) fwd2_kernel(const float* wq, Act A, int n) {
-    __shared__ float wt[32][5][32];  // [in][tap][out]
-    __shared__ float as[kSY][kQ][32];
-    const int o = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * kSY + sl;
-    const int tid = sl * 32 + o;
-    for (int k = tid; k < 5120; k += 32 * kSY) {
-        const int oo = k / 160, i = (k / 5) % 32, j = k % 5;
-        wt[i][j][oo] = wq[kOffW2 + k];
-    }
-    for (int k = o; k < 224; k += 32) as[sl][k / 32][k % 32] = s < n ? A.a1[(size_t)s * 224 + k] : 0.f;
-    __syncthreads();
-    if (s >= n) return;
-    float z[kR];
-#pragma unroll
-    for (int r = 0; r < kR; ++r) z[r] = wq[kOffB2 + o];
-    for (int i = 0; i < 32; ++i) {
-#pragma unroll
-        for (int j = 0; j < 5; ++j) {
-            const float w = wt[i][j][o];
-#pragma unroll
-            for (int r = 0; r < kR; ++r) {
-                const int q = 3 * r + j - 1;
-                if (q >= 0 && q < kQ) z[r] = fmaf(w, as[sl][q][i], z[r]);
-            }
+// Epilogue of a forward GEMM (block (32, 8), 8 samples): v = ReLU(d + bias)
+// (bias[col % bmod]; rounded to bf16 when rnd) into f [n][N] and the bf16
+// operand copies b [n][N] and t [N][ldt] when given.
+__global__ void ep_fwd_kernel(const float* d, int N, const float* bias, int bmod, int rnd, float* f, uint16_t* b,
+                              uint16_t* t, int ldt, int n) {
+    const int s = blockIdx.x * 8 + threadIdx.y;
+    if (s >= ((n + 7) & ~7)) return;
+    for (int c = threadIdx.x; c < N; c += 32) {
+        if (s >= n) {
+            if (t) t[(size_t)c * ldt + s] = 0;
+            continue;
         }
+        float v = fmaxf(d[(size_t)s * N + c] + bias[c % bmod], 0.f);
+        if (rnd) v = bf16r(v);
+        f[(size_t)s * N + c] = v;
+        if (b) b[(size_t)s * N + c] = bf16_bits(v);
+        if (t) t[(size_t)c * ldt + s] = bf16_bits(v);
     }
-#pragma unroll
-    for (int r = 0; r < kR; ++r) A.a2[(size_t)s * 64 + r * 32 + o] = bf16r(fmaxf(z[r], 0.f));
 }
 
-// conv3 (k=5, pad 2, one output): taps 2, 3 on positions 0, 1
-__global__ void __launch_bounds__(32 * kSY) fwd3_kernel(const float* wq, Act A, int n) {
-    __shared__ float wt[32][2][32];  // [in][tap - 2][out]
-    __shared__ float as[kSY][kR][32];
-    const int o = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * kSY + sl;
-    const int tid = sl * 32 + o;
-    for (int k = tid; k < 2048; k += 32 * kSY) {
-        const int oo = k / 64, i = (k / 2) % 32, j = k % 2;
-        wt[i][j][oo] = wq[kOffW3 + oo * 160 + i * 5 + 2 + j];
+// Epilogue of a data-gradient GEMM (block (32, 8)): g = act > 0 ? d : 0 into
+// f [n][N] and the bf16 copies b, t when given.
+__global__ void ep_bwd_kernel(const float* d, int N, const float* act, float* f, uint16_t* b, uint16_t* t, int ldt,
+                              int n) {
+    const int s = blockIdx.x * 8 + threadIdx.y;
+    if (s >= ((n + 7) & ~7)) return;
+    for (int c = threadIdx.x; c < N; c += 32) {
+        if (s >= n) {
+            if (t) t[(size_t)c * ldt + s] = 0;
+            continue;
+        }
+        const size_t k = (size_t)s * N + c;
+        const float g = act[k] > 0.f ? d[k] : 0.f;
+        f[k] = g;
+        if (b) b[k] = bf16_bits(g);
+        if (t) t[(size_t)c * ldt + s] = bf16_bits(g);
     }
-    for (int k = o; k < 64; k += 32) as[sl][k / 32][k % 32] = s < n ? A.a2[(size_t)s * 64 + k] : 0.f;
-    __syncthreads();
-    if (s >= n) return;
-    float z = wq[kOffB3 + o];
-    for (int i = 0; i < 32; ++i) {
-#pragma unroll
-        for (int j = 0; j < 2; ++j) z = fmaf(wt[i][j][o], as[sl][j][i], z);
-    }
-    A.a3[(size_t)s * 32 + o] = bf16r(fmaxf(z, 0.f));
-}
-
-// block (64, 8)
-__global__ void __launch_bounds__(512) fwd4_kernel(const float* wq, Act A, int n) {
-    __shared__ float wt[32][64];  // [in][hidden]
-    __shared__ float as[8][32];
-    const int h = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * 8 + sl;
-    const int tid = sl * 64 + h;
-    for (int k = tid; k < 2048; k += 512) wt[k % 32][k / 32] = wq[kOffW4 + k];
-    if (h < 32) as[sl][h] = s < n ? A.a3[(size_t)s * 32 + h] : 0.f;
-    __syncthreads();
-    if (s >= n) return;
-    float z = wq[kOffB4 + h];
-#pragma unroll 8
-    for (int i = 0; i < 32; ++i) z = fmaf(wt[i][h], as[sl][i], z);
-    A.a4[(size_t)s * 64 + h] = fmaxf(z, 0.f);
 }
 
 // one thread per sample: logit, loss, dloss/dlogit (labels may be null: scores only)
@@ -234,79 +226,25 @@ __global__ void head_kernel(const float* wq, Act A, const uint8_t* labels, float
     }
 }
 
-// block (64, 8): dz4 = dl * w5 * (a4 > 0)
+// block (64, 8): dz4 = dl * w5 * (a4 > 0), with its bf16 operand copies
 __global__ void bwd4_kernel(const float* wq, Act A, int n) {
     const int h = threadIdx.x, s = blockIdx.x * 8 + threadIdx.y;
-    if (s >= n) return;
+    if (s >= ((n + 7) & ~7)) return;
+    if (s >= n) {
+        A.dz4t[(size_t)h * A.ldt + s] = 0;
+        return;
+    }
     const float a = A.a4[(size_t)s * 64 + h];
-    A.dz4[(size_t)s * 64 + h] = a > 0.f ? A.dl[s] * wq[kOffW5 + h] : 0.f;
+    const float g = a > 0.f ? A.dl[s] * wq[kOffW5 + h] : 0.f;
+    A.dz4[(size_t)s * 64 + h] = g;
+    A.dz4b[(size_t)s * 64 + h] = bf16_bits(g);
+    A.dz4t[(size_t)h * A.ldt + s] = bf16_bits(g);
 }
 
-// block (32, 16): dz3 = (W4^T dz4) * (a3 > 0)
-__global__ void __launch_bounds__(32 * kSY) bwd3_kernel(const float* wq, Act A, int n) {
-    __shared__ float w4[64][33];
-    const int o = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * kSY + sl;
-    for (int k = sl * 32 + o; k < 2048; k += 32 * kSY) w4[k / 32][k % 32] = wq[kOffW4 + k];
-    __syncthreads();
-    if (s >= n) return;
-    float g = 0.f;
-    for (int h = 0; h < 64; ++h) g = fmaf(A.dz4[(size_t)s * 64 + h], w4[h][o], g);
-    A.dz3[(size_t)s * 32 + o] = A.a3[(size_t)s * 32 + o] > 0.f ? g : 0.f;
-}
-
-// block (32, 16), thread = input channel i: dz2[pos][i] = sum_o dz3[o] w3[o][i][pos+2], masked
-__global__ void __launch_bounds__(32 * kSY) bwd2_kernel(const float* wq, Act A, int n) {
-    __shared__ float w3[32][32][3];  // [out][in][tap - 2], padded
-    __shared__ float g3[kSY][32];
-    const int i = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * kSY + sl;
-    for (int k = sl * 32 + i; k < 2048; k += 32 * kSY) {
-        const int o = k / 64, ii = (k / 2) % 32, j = k % 2;
-        w3[o][ii][j] = wq[kOffW3 + o * 160 + ii * 5 + 2 + j];
-    }
-    g3[sl][i] = s < n ? A.dz3[(size_t)s * 32 + i] : 0.f;
-    __syncthreads();
-    if (s >= n) return;
-#pragma unroll
-    for (int pos = 0; pos < kR; ++pos) {
-        float g = 0.f;
-        for (int o = 0; o < 32; ++o) g = fmaf(g3[sl][o], w3[o][i][pos], g);
-        const size_t k = (size_t)s * 64 + pos * 32 + i;
-        A.dz2[k] = A.a2[k] > 0.f ? g : 0.f;
-    }
-}
-
-// block (32, 16), thread = input channel i: dm1[q][i] = sum_{r,j: 3r+j-1=q} sum_o dz2[r][o] w2[o][i][j], masked
-__global__ void __launch_bounds__(32 * kSY) bwd1_kernel(const float* wq, Act A, int n) {
-    __shared__ float w2[32][32][6];
-    __shared__ float g2[kSY][kR][32];
-    const int i = threadIdx.x, sl = threadIdx.y, s = blockIdx.x * kSY + sl;
-    for (int k = sl * 32 + i; k < 5120; k += 32 * kSY) w2[k / 160][(k / 5) % 32][k % 5] = wq[kOffW2 + k];
-    for (int k = i; k < 64; k += 32) g2[sl][k / 32][k % 32] = s < n ? A.dz2[(size_t)s * 64 + k] : 0.f;
-    __syncthreads();
-    if (s >= n) return;
-    float da[kQ];
-#pragma unroll
-    for (int q = 0; q < kQ; ++q) da[q] = 0.f;
-    for (int o = 0; o < 32; ++o) {
-#pragma unroll
-        for (int r = 0; r < kR; ++r) {
-            const float g = g2[sl][r][o];
-#pragma unroll
-            for (int j = 0; j < 5; ++j) {
-                const int q = 3 * r + j - 1;
-                if (q >= 0 && q < kQ) da[q] = fmaf(g, w2[o][i][j], da[q]);
-            }
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < kQ; ++q) {
-        const size_t k = (size_t)s * 224 + q * 32 + i;
-        A.dm1[k] = A.a1[k] > 0.f ? da[q] : 0.f;
-    }
-}
-
-// Weight gradients of one layer (blockIdx.y) over one chunk of samples
-// (blockIdx.x), written to part[chunk][param]. 256 threads.
+// Weight gradients of one chunk of samples (blockIdx.x) on the CUDA cores,
+// written to part[chunk][param]: conv1 (blockIdx.y 0), the biases of conv2,
+// conv3 and fc1 (1, 2, 3; their weights come from the tensor-core GEMMs)
+// and fc2 (4). 256 threads.
 constexpr int kChunk = 256;
 
 __global__ void __launch_bounds__(256) wgrad_kernel(const uint8_t* x, Act A, int n, float* part) {
@@ -330,80 +268,30 @@ __global__ void __launch_bounds__(256) wgrad_kernel(const uint8_t* x, Act A, int
             P[bias ? kOffB1 + o : kOffW1 + t] = acc;
             break;
         }
-        case 1: {  // w2: pairs (o, i) = t + 256 k, k < 4; b2 for t < 32
-            float acc[4][5] = {};
+        case 1: {  // b2 (w2 by the tensor-core GEMM, tg::kW2T)
+            if (t >= 32) return;
             float bacc = 0.f;
-            for (int s = s0; s < s1; ++s) {
-                const float* a1 = A.a1 + (size_t)s * 224;
-                const float* g2 = A.dz2 + (size_t)s * 64;
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int pi = t + 256 * k, o = pi / 32, i = pi % 32;
-                    float g[kR], av[kQ];
-#pragma unroll
-                    for (int r = 0; r < kR; ++r) g[r] = g2[r * 32 + o];
-#pragma unroll
-                    for (int q = 0; q < kQ; ++q) av[q] = a1[q * 32 + i];
-#pragma unroll
-                    for (int j = 0; j < 5; ++j)
-#pragma unroll
-                        for (int r = 0; r < kR; ++r) {
-                            const int q = 3 * r + j - 1;
-                            if (q >= 0 && q < kQ) acc[k][j] = fmaf(g[r], av[q], acc[k][j]);
-                        }
-                }
-                if (t < 32)
-                    for (int r = 0; r < kR; ++r) bacc += g2[r * 32 + t];
-            }
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int pi = t + 256 * k, o = pi / 32, i = pi % 32;
-#pragma unroll
-                for (int j = 0; j < 5; ++j) P[kOffW2 + o * 160 + i * 5 + j] = acc[k][j];
-            }
-            if (t < 32) P[kOffB2 + t] = bacc;
+            for (int s = s0; s < s1; ++s)
+                for (int r = 0; r < kR; ++r) bacc += A.dz2[(size_t)s * 64 + r * 32 + t];
+            P[kOffB2 + t] = bacc;
             break;
         }
-        case 2: {  // w3: pairs (o, i); only taps 2, 3 meet data; b3 for t < 32
-            float acc[4][2] = {};
+        case 2: {  // b3, and 0 for the taps of w3 that meet no data (taps 2, 3 by tg::kW3T)
+            for (int k = t; k < 32 * 32 * 3; k += 256) {
+                const int oi = k / 3, j = k % 3;
+                P[kOffW3 + oi * 5 + (j == 2 ? 4 : j)] = 0.f;
+            }
+            if (t >= 32) return;
             float bacc = 0.f;
-            for (int s = s0; s < s1; ++s) {
-                const float* a2 = A.a2 + (size_t)s * 64;
-                const float* g3 = A.dz3 + (size_t)s * 32;
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int pi = t + 256 * k, o = pi / 32, i = pi % 32;
-                    const float g = g3[o];
-#pragma unroll
-                    for (int j = 0; j < 2; ++j) acc[k][j] = fmaf(g, a2[j * 32 + i], acc[k][j]);
-                }
-                if (t < 32) bacc += g3[t];
-            }
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int pi = t + 256 * k, o = pi / 32, i = pi % 32;
-#pragma unroll
-                for (int j = 0; j < 5; ++j) P[kOffW3 + o * 160 + i * 5 + j] = (j == 2 || j == 3) ? acc[k][j - 2] : 0.f;
-            }
-            if (t < 32) P[kOffB3 + t] = bacc;
+            for (int s = s0; s < s1; ++s) bacc += A.dz3[(size_t)s * 32 + t];
+            P[kOffB3 + t] = bacc;
             break;
         }
-        case 3: {  // w4: pairs (h, i) = t + 256 k, k < 8; b4 for t < 64
-            float acc[8] = {};
+        case 3: {  // b4 (w4 by tg::kW4)
+            if (t >= 64) return;
             float bacc = 0.f;
-            for (int s = s0; s < s1; ++s) {
-                const float* a3 = A.a3 + (size_t)s * 32;
-                const float* g4 = A.dz4 + (size_t)s * 64;
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    const int pi = t + 256 * k;
-                    acc[k] = fmaf(g4[pi / 32], a3[pi % 32], acc[k]);
-                }
-                if (t < 64) bacc += g4[t];
-            }
-#pragma unroll
-            for (int k = 0; k < 8; ++k) P[kOffW4 + t + 256 * k] = acc[k];
-            if (t < 64) P[kOffB4 + t] = bacc;
+            for (int s = s0; s < s1; ++s) bacc += A.dz4[(size_t)s * 64 + t];
+            P[kOffB4 + t] = bacc;
             break;
         }
         default: {  // w5 for t < 64, b5 for t == 64
@@ -982,6 +870,241 @@ __global__ void __launch_bounds__(kNT, 2) infer_kernel(const __grid_constant__ C
 }  // namespace inf
 
 // ---------------------------------------------------------------------------
+// Training GEMMs on the tensor cores (tcgen05)
+// ---------------------------------------------------------------------------
+// The dense layers of training (conv2, conv3, fc1 forward; their data
+// gradients; the weight gradients of conv2, conv3 and fc1) are GEMMs
+//   D[M x N] (fp32, TMEM) = sum over passes of A_p[M x K] x B_p[N x K]^T
+// with bf16 operands stored row-major (K contiguous) in global memory. conv1
+// (one input channel, 1.1 K of the 14.5 K MAC per sample), the head and the
+// elementwise steps stay on the CUDA cores.
+namespace tg {
+
+constexpr int kTM = 128;   // rows per tile = MMA M
+constexpr int kKS = 64;    // K per pipeline stage: 8 panels of 8, 4 MMAs of K = 16
+constexpr int kNT = 128;   // one warpgroup; warp w drains TMEM lanes 32 w .. 32 w + 31
+constexpr int kMaxN = 256;
+
+__host__ __device__ constexpr int stage_bytes(int N) { return (kTM + N) * kKS * 2; }
+constexpr int kMaxSmem = 2 * stage_bytes(kMaxN) + 64;  // the largest launch (N = 256)
+
+// Where a D element goes. kPlain: out[y * out_chunk + m * out_ld + n]. The
+// weight-gradient layouts write into the parameter vector of chunk y
+// (out = part, out_chunk = kParams): kW2T m = tap * 32 + in, n = out;
+// kW3T m = (tap - 2) * 32 + in, n = out; kW4 m = hidden, n = in.
+enum OutMap { kPlain = 0, kW2T = 1, kW3T = 2, kW4 = 3 };
+
+struct GemmArgs {
+    int N;           // columns of D: a multiple of 32, at most 256
+    int npass;       // operand pairs accumulated into D (1 or 2)
+    int klen;        // K of each pass
+    int ksplit;      // K per blockIdx.y (a multiple of kKS)
+    int m_valid;     // rows of D that are stored
+    int map;         // OutMap
+    float* out;
+    size_t out_ld, out_chunk;
+    uint32_t tmem_cols;  // power of two >= max(N, 32)
+    int32_t* status;
+};
+
+// D (TMEM) = A x B (acc = 0) or D += A x B (acc = 1); whole warp, one elected lane issues
+__device__ __forceinline__ void mma_ss_acc(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
+    asm volatile(
+        "{\n.reg .pred p, e;\nsetp.ne.b32 p, %4, 0;\nelect.sync _|e, 0xffffffff;\n"
+        "@e tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(id), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ int out_index(int map, int m, int n) {
+    switch (map) {
+        case kW2T: return m < 160 ? kOffW2 + n * 160 + (m % 32) * 5 + m / 32 : -1;
+        case kW3T: return m < 64 ? kOffW3 + n * 160 + (m % 32) * 5 + 2 + m / 32 : -1;
+        case kW4: return m < 64 ? kOffW4 + m * 32 + n : -1;
+        default: return -1;
+    }
+}
+
+// Operands through 3-D tensor maps over the row-major bf16 matrices: dims
+// (8 elements, K / 8 panels, rows), one box per panel = 8 elements x rows, so
+// that shared memory holds each 8-wide K panel as rows x 16 bytes: the
+// canonical K-major layout without swizzle (core matrices of 8 rows x 16
+// bytes, 128 bytes apart along M/N, one panel apart along K). Rows and K
+// beyond the matrix read as 0.
+__global__ void __launch_bounds__(kNT, 1) gemm_kernel(const __grid_constant__ CUtensorMap a0,
+                                                     const __grid_constant__ CUtensorMap b0,
+                                                     const __grid_constant__ CUtensorMap a1,
+                                                     const __grid_constant__ CUtensorMap b1, GemmArgs g) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int SB = stage_bytes(g.N);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * SB);  // full[2], free[2], done
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 5);
+    const int m0 = blockIdx.x * kTM;
+    const int k0 = blockIdx.y * g.ksplit;
+    const int kend = min(k0 + g.ksplit, g.klen);
+    const int nk = kend > k0 ? (kend - k0 + kKS - 1) / kKS : 0;  // stages per pass
+    const int total = nk * g.npass;
+    if (tid == 0) {
+        for (int i = 0; i < 5; ++i) dev::mbar_init(&bars[i], 1);
+        dev::fence_barrier_init();
+        dev::prefetch_tmap(&a0);
+        dev::prefetch_tmap(&b0);
+        if (g.npass > 1) {
+            dev::prefetch_tmap(&a1);
+            dev::prefetch_tmap(&b1);
+        }
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dev::smem_u32(tslot)),
+                     "r"(g.tmem_cols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    inf::fence_before();
+    __syncthreads();
+    inf::fence_after();
+    const uint32_t tm = *tslot;
+    // instruction descriptor: bf16 x bf16 -> fp32, both K-major, M = 128
+    const uint32_t id = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(g.N >> 3) << 17) | (uint32_t(kTM >> 4) << 24);
+
+    // warp 0: lane 0 loads stages, the whole warp issues the MMAs
+    bool ok = true;
+    int loaded = 0, consumed = 0;  // stages loaded / consumed (warp 0)
+    if (warp == 0) {
+        auto load = [&](int it) {
+            if (lane == 0) {
+                const int s = it & 1, pass = it / nk, kk = k0 + (it % nk) * kKS;
+                const CUtensorMap* ma = pass ? &a1 : &a0;
+                const CUtensorMap* mb = pass ? &b1 : &b0;
+                unsigned char* sa = smem + s * SB;
+                unsigned char* sb = sa + kTM * kKS * 2;
+                dev::mbar_arrive_expect_tx(&bars[s], uint32_t(SB));
+#pragma unroll
+                for (int c = 0; c < kKS / 8; ++c) {
+                    dev::tma_load_3d(sa + c * kTM * 16, ma, 0, kk / 8 + c, m0, &bars[s]);
+                    dev::tma_load_3d(sb + c * g.N * 16, mb, 0, kk / 8 + c, 0, &bars[s]);
+                }
+            }
+            __syncwarp();
+        };
+        uint32_t ph_full = 0u, ph_free = 0u;  // phase bit s of stage s's barriers
+        for (; loaded < total && loaded < 2; ++loaded) load(loaded);
+        for (int it = 0; it < total && ok; ++it) {
+            const int s = it & 1;
+            ok = __all_sync(0xffffffffu, dev::mbar_wait_bounded(&bars[s], (ph_full >> s) & 1u));
+            if (!ok) break;
+            ph_full ^= 1u << s;
+            ++consumed;
+            inf::fence_after();
+            const uint32_t sa = dev::smem_u32(smem + s * SB), sb = sa + kTM * kKS * 2;
+#pragma unroll
+            for (int q = 0; q < kKS / 16; ++q)
+                mma_ss_acc(tm, inf::sdesc(sa + q * 2 * kTM * 16, kTM * 16), inf::sdesc(sb + q * 2 * g.N * 16, g.N * 16),
+                           id, (it > 0 || q > 0) ? 1u : 0u);
+            inf::commit(&bars[2 + s]);  // stage s is free once these MMAs complete
+            if (it + 2 < total) {
+                ok = __all_sync(0xffffffffu, dev::mbar_wait_bounded(&bars[2 + s], (ph_free >> s) & 1u));
+                if (!ok) break;
+                ph_free ^= 1u << s;
+                load(it + 2);
+                ++loaded;
+            }
+        }
+        inf::commit(&bars[4]);  // every MMA issued so far
+    }
+    // all threads: the accumulator is complete (or the loop gave up)
+    const bool done = dev::mbar_wait_bounded(&bars[4], 0);
+    const bool fail = __syncthreads_or(!ok || !done);
+    inf::fence_after();
+    if (fail) {
+        if (tid == 0) dev::report(g.status, CT_ETIMEOUT);
+        // wait (bounded) for the stage loads still in flight before leaving
+        if (warp == 0 && lane == 0)
+            for (int it = consumed; it < loaded; ++it) dev::mbar_wait_bounded(&bars[it & 1], ((it >> 1) & 1));
+    } else if (total > 0) {
+        const int row = m0 + tid;
+        const uint32_t tl = tm + (uint32_t(warp * 32) << 16);
+        float* outc = g.out + (size_t)blockIdx.y * g.out_chunk;
+        for (int c0 = 0; c0 < g.N; c0 += 32) {
+            float v[32];
+            inf::ld32(tl + c0, v);
+            if (row < g.m_valid) {
+                if (g.map == kPlain) {
+                    float* o = outc + (size_t)row * g.out_ld + c0;
+#pragma unroll
+                    for (int j = 0; j < 32; j += 4) *reinterpret_cast<float4*>(o + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int p = out_index(g.map, row, c0 + j);
+                        if (p >= 0) outc[p] = v[j];
+                    }
+                }
+            }
+        }
+    }
+    inf::fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm), "r"(g.tmem_cols) : "memory");
+}
+
+// The bf16 B operands of the training GEMMs from the working weights wq:
+//   w2f [32 out][160 = tap * 32 + in]      conv2 forward
+//   w3f [32 out][64 = (tap - 2) * 32 + in]  conv3 forward (taps 2, 3)
+//   w4f [64 hidden][32 in]                  fc1 forward
+//   w4t [32 in][64 hidden]                  fc1 data gradient
+//   w3t [64 = (tap - 2) * 32 + in][32 out]  conv3 data gradient
+//   w2t [224 = q * 32 + in][64 = r * 32 + out] conv2 data gradient: W2[out][in][q - 3 r + 1] (0 outside the taps)
+struct TrainW {
+    uint16_t *w2f, *w3f, *w4f, *w4t, *w3t, *w2t;
+};
+constexpr int kTrainWElems = 32 * 160 + 32 * 64 + 64 * 32 + 32 * 64 + 64 * 32 + 224 * 64;
+
+__global__ void pack_train_weights_kernel(const float* wq, TrainW w) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < kTrainWElems; k += gridDim.x * blockDim.x) {
+        int e = k;
+        if (e < 32 * 160) {
+            const int o = e / 160, t = (e % 160) / 32, i = e % 32;
+            w.w2f[e] = bf16_bits(wq[kOffW2 + o * 160 + i * 5 + t]);
+            continue;
+        }
+        e -= 32 * 160;
+        if (e < 32 * 64) {
+            const int o = e / 64, t = (e % 64) / 32, i = e % 32;
+            w.w3f[e] = bf16_bits(wq[kOffW3 + o * 160 + i * 5 + 2 + t]);
+            continue;
+        }
+        e -= 32 * 64;
+        if (e < 64 * 32) {
+            w.w4f[e] = bf16_bits(wq[kOffW4 + e]);
+            continue;
+        }
+        e -= 64 * 32;
+        if (e < 32 * 64) {
+            const int i = e / 64, hh = e % 64;
+            w.w4t[e] = bf16_bits(wq[kOffW4 + hh * 32 + i]);
+            continue;
+        }
+        e -= 32 * 64;
+        if (e < 64 * 32) {
+            const int t = e / (32 * 32), i = (e / 32) % 32, o = e % 32;
+            w.w3t[e] = bf16_bits(wq[kOffW3 + o * 160 + i * 5 + 2 + t]);
+            continue;
+        }
+        e -= 64 * 32;
+        {
+            const int q = e / (32 * 64), i = (e / 64) % 32, r = (e % 64) / 32, o = e % 32;
+            const int j = q - 3 * r + 1;
+            w.w2t[e] = (j >= 0 && j < 5) ? bf16_bits(wq[kOffW2 + o * 160 + i * 5 + j]) : uint16_t(0);
+        }
+    }
+}
+
+}  // namespace tg
+
+// ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
 uint16_t f32_to_bf16_bits(float f) {
@@ -1016,6 +1139,7 @@ struct ConfNetHandle : ct_handle {
     float *master = nullptr, *m = nullptr, *v = nullptr, *wq = nullptr, *grad = nullptr, *part = nullptr;
     float* loss_out = nullptr;
     unsigned char* wimg = nullptr;  // packed inference weights
+    tg::TrainW tw{};                // bf16 B operands of the training GEMMs
     Act act{};
     int steps = 0;
     bool wimg_dirty = true;
@@ -1028,23 +1152,103 @@ ConfNetHandle* as_net(ct_handle* h) {
 
 int chunks_for(int n) { return (n + kChunk - 1) / kChunk; }
 
-// forward (+ backward when labels are given) of n samples on stream s
+// A row-major bf16 matrix [rows][K] (pitch in elements) as a GEMM operand
+// map: dims (8, K / 8, rows), one 8-wide panel x box_rows rows per box.
+int operand_map(CUtensorMap* m, const uint16_t* base, int rows, int K, size_t pitch, int box_rows) {
+    const uint64_t dims[3] = {8, uint64_t((K + 7) / 8), uint64_t(rows)};
+    const uint64_t strides[2] = {16, pitch * 2};
+    const uint32_t box[3] = {8, 1, uint32_t(box_rows)};
+    return make_tmap_nd(m, base, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, 3, dims, strides, box);
+}
+
+// D = sum over passes of A_p x B_p^T on the tensor cores (tg::gemm_kernel):
+// M rows of A, N rows of B (a multiple of 32), K = klen split into ksplit
+// per blockIdx.y.
+int tc_gemm(ConfNetHandle* h, const CUtensorMap& a0, const CUtensorMap& b0, const CUtensorMap* a1,
+            const CUtensorMap* b1, int M, int N, int klen, int ksplit, int map, float* out, size_t out_ld,
+            size_t out_chunk, cudaStream_t s) {
+    tg::GemmArgs g{};
+    g.N = N;
+    g.npass = a1 ? 2 : 1;
+    g.klen = klen;
+    g.ksplit = ksplit;
+    g.m_valid = M;
+    g.map = map;
+    g.out = out;
+    g.out_ld = out_ld;
+    g.out_chunk = out_chunk;
+    g.tmem_cols = N <= 32 ? 32u : N <= 64 ? 64u : N <= 128 ? 128u : 256u;
+    g.status = h->d_status;
+    const dim3 grid((M + tg::kTM - 1) / tg::kTM, (klen + ksplit - 1) / ksplit);
+    tg::gemm_kernel<<<grid, tg::kNT, 2 * tg::stage_bytes(N) + 64, s>>>(a0, b0, a1 ? *a1 : a0, b1 ? *b1 : b0, g);
+    CT_LAUNCH_CHECK();
+    return CT_OK;
+}
+
+// forward (+ backward when labels are given) of n samples on stream s:
+// conv1, the head and the elementwise steps on the CUDA cores, the dense
+// layers (conv2, conv3, fc1), their data gradients and their weight
+// gradients as bf16 GEMMs with fp32 accumulation on the tensor cores
 int run_train_graph(ConfNetHandle* h, const uint8_t* x, const uint8_t* labels, int n, float* scores,
                     cudaStream_t s) {
     const Act& A = h->act;
-    const dim3 b32(32, kSY), b64(64, 8);
-    const int g32 = (n + kSY - 1) / kSY, g64 = (n + 7) / 8;
+    const dim3 b32(32, kSY), b64(64, 8), be(32, 8);
+    const int g32 = (n + kSY - 1) / kSY, g64 = (n + 7) / 8, ge = (n + 7) / 8;
+    const int n8 = (n + 7) & ~7;
+    const size_t lt = size_t(A.ldt);
+    tg::pack_train_weights_kernel<<<(tg::kTrainWElems + 255) / 256, 256, 0, s>>>(h->wq, h->tw);
     fwd1_kernel<<<g32, b32, 0, s>>>(x, h->wq, A, n);
-    fwd2_kernel<<<g32, b32, 0, s>>>(h->wq, A, n);
-    fwd3_kernel<<<g32, b32, 0, s>>>(h->wq, A, n);
-    fwd4_kernel<<<g64, b64, 0, s>>>(h->wq, A, n);
+    CT_LAUNCH_CHECK();
+    const int kS = tg::kKS;
+    auto ks = [&](int k) { return (k + kS - 1) / kS * kS; };  // whole K in one CTA
+    CUtensorMap ma, mb, ma2, mb2;
+    // conv2: position r reads slots 3 r .. 3 r + 4 of a1p (160 contiguous values)
+    if (int rc = operand_map(&mb, h->tw.w2f, 32, 160, 160, 32)) return rc;
+    for (int r = 0; r < kR; ++r) {
+        if (int rc = operand_map(&ma, A.a1p + 96 * r, n, 160, 256, tg::kTM)) return rc;
+        if (int rc = tc_gemm(h, ma, mb, nullptr, nullptr, n, 32, 160, ks(160), tg::kPlain, A.d + 32 * r, 64, 0, s))
+            return rc;
+    }
+    ep_fwd_kernel<<<ge, be, 0, s>>>(A.d, 64, h->wq + kOffB2, 32, 1, A.a2, A.a2b, A.a2t, A.ldt, n);
+    // conv3 (taps 2, 3 over both positions) and fc1
+    if (int rc = operand_map(&ma, A.a2b, n, 64, 64, tg::kTM)) return rc;
+    if (int rc = operand_map(&mb, h->tw.w3f, 32, 64, 64, 32)) return rc;
+    if (int rc = tc_gemm(h, ma, mb, nullptr, nullptr, n, 32, 64, ks(64), tg::kPlain, A.d, 32, 0, s)) return rc;
+    ep_fwd_kernel<<<ge, be, 0, s>>>(A.d, 32, h->wq + kOffB3, 32, 1, A.a3, A.a3b, A.a3t, A.ldt, n);
+    if (int rc = operand_map(&ma, A.a3b, n, 32, 32, tg::kTM)) return rc;
+    if (int rc = operand_map(&mb, h->tw.w4f, 64, 32, 32, 64)) return rc;
+    if (int rc = tc_gemm(h, ma, mb, nullptr, nullptr, n, 64, 32, ks(32), tg::kPlain, A.d, 64, 0, s)) return rc;
+    ep_fwd_kernel<<<ge, be, 0, s>>>(A.d, 64, h->wq + kOffB4, 64, 0, A.a4, nullptr, nullptr, A.ldt, n);
     head_kernel<<<(n + 255) / 256, 256, 0, s>>>(h->wq, A, labels, 1.f / float(n), scores, n);
     CT_LAUNCH_CHECK();
     if (!labels) return CT_OK;
+    // data gradients
     bwd4_kernel<<<g64, b64, 0, s>>>(h->wq, A, n);
-    bwd3_kernel<<<g32, b32, 0, s>>>(h->wq, A, n);
-    bwd2_kernel<<<g32, b32, 0, s>>>(h->wq, A, n);
-    bwd1_kernel<<<g32, b32, 0, s>>>(h->wq, A, n);
+    if (int rc = operand_map(&ma, A.dz4b, n, 64, 64, tg::kTM)) return rc;
+    if (int rc = operand_map(&mb, h->tw.w4t, 32, 64, 64, 32)) return rc;
+    if (int rc = tc_gemm(h, ma, mb, nullptr, nullptr, n, 32, 64, ks(64), tg::kPlain, A.d, 32, 0, s)) return rc;
+    ep_bwd_kernel<<<ge, be, 0, s>>>(A.d, 32, A.a3, A.dz3, A.dz3b, A.dz3t, A.ldt, n);
+    if (int rc = operand_map(&ma, A.dz3b, n, 32, 32, tg::kTM)) return rc;
+    if (int rc = operand_map(&mb, h->tw.w3t, 64, 32, 32, 64)) return rc;
+    if (int rc = tc_gemm(h, ma, mb, nullptr, nullptr, n, 64, 32, ks(32), tg::kPlain, A.d, 64, 0, s)) return rc;
+    ep_bwd_kernel<<<ge, be, 0, s>>>(A.d, 64, A.a2, A.dz2, A.dz2b, A.dz2t, A.ldt, n);
+    if (int rc = operand_map(&ma, A.dz2b, n, 64, 64, tg::kTM)) return rc;
+    if (int rc = operand_map(&mb, h->tw.w2t, 224, 64, 64, 224)) return rc;
+    if (int rc = tc_gemm(h, ma, mb, nullptr, nullptr, n, 224, 64, ks(64), tg::kPlain, A.d, 224, 0, s)) return rc;
+    ep_bwd_kernel<<<ge, be, 0, s>>>(A.d, 224, A.a1, A.dm1, nullptr, nullptr, A.ldt, n);
+    // weight gradients per chunk of kChunk samples into part[chunk][param]
+    // conv2: sum over positions r of a1p slots 3 r .. 3 r + 4 (rows) x dz2 position r
+    if (int rc = operand_map(&ma, A.a1pt, 160, n8, lt, tg::kTM)) return rc;
+    if (int rc = operand_map(&mb, A.dz2t, 32, n8, lt, 32)) return rc;
+    if (int rc = operand_map(&ma2, A.a1pt + 96 * lt, 160, n8, lt, tg::kTM)) return rc;
+    if (int rc = operand_map(&mb2, A.dz2t + 32 * lt, 32, n8, lt, 32)) return rc;
+    if (int rc = tc_gemm(h, ma, mb, &ma2, &mb2, 160, 32, n8, kChunk, tg::kW2T, h->part, 0, kParams, s)) return rc;
+    if (int rc = operand_map(&ma, A.a2t, 64, n8, lt, tg::kTM)) return rc;
+    if (int rc = operand_map(&mb, A.dz3t, 32, n8, lt, 32)) return rc;
+    if (int rc = tc_gemm(h, ma, mb, nullptr, nullptr, 64, 32, n8, kChunk, tg::kW3T, h->part, 0, kParams, s)) return rc;
+    if (int rc = operand_map(&ma, A.dz4t, 64, n8, lt, tg::kTM)) return rc;
+    if (int rc = operand_map(&mb, A.a3t, 32, n8, lt, 32)) return rc;
+    if (int rc = tc_gemm(h, ma, mb, nullptr, nullptr, 64, 32, n8, kChunk, tg::kW4, h->part, 0, kParams, s)) return rc;
     wgrad_kernel<<<dim3(chunks_for(n), 5), 256, 0, s>>>(x, A, n, h->part);
     CT_LAUNCH_CHECK();
     return CT_OK;
@@ -1135,6 +1339,7 @@ int ct_confnet_configure(ct_handle* hh, int32_t device, int32_t max_batch) {
     h->device = device;
     if (int rc = h->init_status()) return rc;
     CT_CUDA_TRY(cudaFuncSetAttribute(inf::infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, inf::kSmem));
+    CT_CUDA_TRY(cudaFuncSetAttribute(tg::gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tg::kMaxSmem));
     h->sms = sm_count(device);
     const size_t n = size_t(max_batch);
     size_t bytes = 0;
@@ -1146,6 +1351,12 @@ int ct_confnet_configure(ct_handle* hh, int32_t device, int32_t max_batch) {
                  o_a3 = take(4 * 32 * n), o_a4 = take(4 * 64 * n), o_logit = take(4 * n), o_dl = take(4 * n),
                  o_ls = take(4 * n), o_dz4 = take(4 * 64 * n), o_dz3 = take(4 * 32 * n), o_dz2 = take(4 * 64 * n),
                  o_dm1 = take(4 * 224 * n);
+    const size_t ldt = (n + 7) / 8 * 8;  // transposed operands: samples per row, a multiple of 8
+    const size_t o_a1p = take(2 * 256 * n), o_a1pt = take(2 * 256 * ldt), o_a2b = take(2 * 64 * n),
+                 o_a2t = take(2 * 64 * ldt), o_a3b = take(2 * 32 * n), o_a3t = take(2 * 32 * ldt),
+                 o_dz4b = take(2 * 64 * n), o_dz4t = take(2 * 64 * ldt), o_dz3b = take(2 * 32 * n),
+                 o_dz3t = take(2 * 32 * ldt), o_dz2b = take(2 * 64 * n), o_dz2t = take(2 * 64 * ldt),
+                 o_d = take(4 * 224 * n), o_tw = take(2 * tg::kTrainWElems);
     cudaFree(h->arena);
     h->arena = nullptr;
     if (cudaMalloc(&h->arena, bytes) != cudaSuccess) return fail(CT_ENOMEM, "confidence-net scratch (%zu bytes)", bytes);
@@ -1170,6 +1381,28 @@ int ct_confnet_configure(ct_handle* hh, int32_t device, int32_t max_batch) {
     h->act.dz3 = reinterpret_cast<float*>(A + o_dz3);
     h->act.dz2 = reinterpret_cast<float*>(A + o_dz2);
     h->act.dm1 = reinterpret_cast<float*>(A + o_dm1);
+    auto u16 = [&](size_t o) { return reinterpret_cast<uint16_t*>(A + o); };
+    h->act.a1p = u16(o_a1p);
+    h->act.a1pt = u16(o_a1pt);
+    h->act.a2b = u16(o_a2b);
+    h->act.a2t = u16(o_a2t);
+    h->act.a3b = u16(o_a3b);
+    h->act.a3t = u16(o_a3t);
+    h->act.dz4b = u16(o_dz4b);
+    h->act.dz4t = u16(o_dz4t);
+    h->act.dz3b = u16(o_dz3b);
+    h->act.dz3t = u16(o_dz3t);
+    h->act.dz2b = u16(o_dz2b);
+    h->act.dz2t = u16(o_dz2t);
+    h->act.d = reinterpret_cast<float*>(A + o_d);
+    h->act.ldt = int(ldt);
+    uint16_t* tw = u16(o_tw);
+    h->tw.w2f = tw;
+    h->tw.w3f = h->tw.w2f + 32 * 160;
+    h->tw.w4f = h->tw.w3f + 32 * 64;
+    h->tw.w4t = h->tw.w4f + 64 * 32;
+    h->tw.w3t = h->tw.w4t + 32 * 64;
+    h->tw.w2t = h->tw.w3t + 64 * 32;
     h->max_batch = max_batch;
     h->configured = true;
     return ct_confnet_init(hh, 1);
