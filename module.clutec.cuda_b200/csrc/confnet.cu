@@ -17,11 +17,14 @@
 // Flat parameter order: w1[32][5], b1[32], w2[32][32][5] ([out][in][tap]),
 // b2[32], w3[32][32][5], b3[32], w4[64][32], b4[64], w5[64], b5[1].
 //
-// Training (CUDA cores): layer kernels with one thread per (sample, channel)
-// keep the activations each backward step needs; weight gradients are
-// reduced per chunk of samples into partial sums that the Adam kernel adds
-// in a fixed order (deterministic). Adam keeps fp32 master weights and
-// writes their bf16 roundings for the next forward.
+// Training: the dense layers (conv2, conv3, fc1: forward, data gradients
+// and weight gradients) are bf16 GEMMs with fp32 accumulation on the tensor
+// cores (tg::gemm_kernel); conv1, the head and the elementwise steps (bias,
+// ReLU, bf16 rounding, masks) run on the CUDA cores with one thread per
+// (sample, channel). Weight gradients are reduced per chunk of samples into
+// partial sums that the Adam kernel adds in a fixed order (deterministic).
+// Adam keeps fp32 master weights and writes their bf16 roundings for the
+// next forward.
 //
 // Inference (tensor cores, tcgen05): a persistent kernel of one warpgroup per
 // CTA, two CTAs per SM, 128 pixels (a row segment) per tile = the M of every
