@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="census1080",
                     choices=["census1080", "sad640", "ncc1080", "ncc1080g", "aw1440", "batch64", "confnet1080",
-                             "mip1080", "map3d1080"],
+                             "compat1080", "mip1080", "map3d1080"],
                     help="census1080 (default, the headline) or another configuration, one JSON line each")
     ap.add_argument("--eval-pairs", type=int, default=None,
                     help="held-out 1080p pairs for the confidence-net AUC (default 4 in the census line, 24 in confnet1080)")
@@ -541,14 +541,24 @@ def run_ours(args):
         # the other configurations, one entry each (1 GPU only: at N > 1 the
         # headline alone is measured)
         out["configs"] = {}
+        keys = ("metric", "value", "unit", "ms_per_step", "config", "roofline", "cpu_baseline", "parity_rank0",
+                "clocks", "gpu_launches")
         for wl in CONFIG_WORKLOADS:
             line = workload_line(wl, args, ct, dev, stream, flush_buf, world, rank, local, rates)
-            out["configs"][wl] = {k: line.get(k) for k in ("metric", "value", "unit", "ms_per_step", "config",
-                                                           "roofline", "cpu_baseline", "parity_rank0", "clocks",
-                                                           "gpu_launches")}
+            out["configs"][wl] = {k: line.get(k) for k in keys}
         if conf is not None:
             out["configs"]["confnet1080"] = confnet_entry(conf)
-        out["gpu_launches_configs"] = sum(v.get("gpu_launches") or 0 for v in out["configs"].values())
+        # the other rows of the path, beyond the five configurations: one
+        # entry each; a failure is reported in its entry, not raised
+        out["extras"] = {}
+        for wl in EXTRA_WORKLOADS:
+            try:
+                line = workload_line(wl, args, ct, dev, stream, flush_buf, world, rank, local, rates)
+                out["extras"][wl] = {k: line.get(k) for k in keys}
+            except Exception as e:  # noqa: BLE001 - reported in the line
+                out["extras"][wl] = {"error": f"{type(e).__name__}: {e}"}
+        out["gpu_launches_configs"] = sum(v.get("gpu_launches") or 0 for d in (out["configs"], out["extras"])
+                                          for v in d.values())
     if rank == 0:
         print(json.dumps(out), flush=True)
     close_ranks(world)
@@ -679,6 +689,7 @@ def run_profile(args):
 
 # the other configurations measured by the default run (configs entry of its line)
 CONFIG_WORKLOADS = ["sad640", "ncc1080", "aw1440", "batch64"]
+EXTRA_WORKLOADS = ["ncc1080g", "compat1080", "mip1080", "map3d1080"]
 BATCH_SIZES = [(320, 240), (640, 480), (1280, 720), (1920, 1080)]
 BATCH_DISPS = [32, 64, 128, 256]
 
@@ -699,8 +710,14 @@ def batch_shapes(n=64, seed=4):
 #            (~10 FP32/INT) = 15 lane operations at the issue rate
 #            (128 per SM per clock: 4 schedulers x 32 lanes)
 #   batch64: as the census headline, 2 POPC (64-bit Hamming)
+#   compat1080: the reference's per-disparity NCC (BlockMatcherNCC.cu:218-271:
+#            the cross mean, the test mean and mean square, the test
+#            standard deviation, the normalised and quantised score: 3
+#            divisions, a square root and ~10 other FP32 operations) + the
+#            window sum (5) + the scan update (~8) = 30 lane operations
 ROOF = {"sad640": ("int", 8, "iadd3_per_clk_sm"), "aw1440": ("int", 13, "iadd3_per_clk_sm"),
-        "ncc1080": ("issue", 15, None), "batch64": ("popc", 2, "popc_per_clk_sm")}
+        "ncc1080": ("issue", 15, None), "batch64": ("popc", 2, "popc_per_clk_sm"),
+        "compat1080": ("issue", 30, None)}
 
 
 def pipe_roofline(kind, ops_per_unit, rate_key, units_per_s, rates, sm_mhz):
@@ -825,6 +842,30 @@ def workload_line(wl, args, ct, dev, stream, flush_buf, world, rank, local, rate
         metric = "Mpix/s disparity to 3D points (MapDisparityTo3D, pinhole pair), 1920x1080 U16"
         launches = 1
         cfg = {"workload": "map3d1080_disparity_to_3d", "width": W, "height": H, "focal_px": 1400.0, "baseline": 0.12}
+    elif wl == "compat1080":
+        # the reference-compat output of the NCC 11x11 driver (the 4 x uint16
+        # TPixelEx pixel: disparity or EDisparityId, uint8-quantised score,
+        # specificity channels) with its gradient gate and thresholds active
+        W, H, D = 1920, 1080, 128
+        L, R, _, _ = ct.synth_pair(2, SEED + rank, W, H, D - 1)
+        dL, dR = up(L), up(R)
+        thr = dict(grad_thresh=2.0, score_thresh=0.6, min_delta_thresh=3)
+        m = ct.BlockMatcherCompat()
+        m.configure(local, W, H, ct.CT_COMPAT_NCC, D, 11, **thr)
+        out = ct.alloc_u16x4(H, W, dev)
+        step = lambda: m.process(out, dL, dR, stream=stream)
+        check_fn = lambda: np.array_equal(out.cpu().numpy().view(np.uint16),
+                                          oracle.compat_match(L, R, "ncc", D, 11, **thr))
+
+        def cpu_sample():
+            t0 = time.perf_counter()
+            oracle.compat_match(L, R, "ncc", D, 11, **thr)
+            return W * H * D / (time.perf_counter() - t0) / 1e6, f"one full frame {W}x{H} D={D}"
+        units = W * H * D
+        metric = ("Mpix*disp/s NCC 11x11 reference-compat output (4 x u16: ID, quantised score, specificity), "
+                  "1920x1080 D=128")
+        launches = 2
+        cfg = {"workload": "compat1080_ncc11_u16x4", "width": W, "height": H, "D": D, **thr}
     else:
         W, H, D, kind = {"sad640": (640, 480, 64, 1), "ncc1080": (1920, 1080, 128, 2),
                          "ncc1080g": (1920, 1080, 128, 2), "aw1440": (2560, 1440, 256, 3)}[wl]
@@ -921,7 +962,8 @@ def workload_line(wl, args, ct, dev, stream, flush_buf, world, rank, local, rate
     out_line = {
         "metric": metric, "value": round(value, 1), "unit": unit, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u8 pixels / integer costs" + (" / fp32 score" if wl in ("ncc1080", "ncc1080g") else ""),
+        "vs_baseline": None,
+        "dtype": "u8 pixels / integer costs" + (" / fp32 score" if wl in ("ncc1080", "ncc1080g", "compat1080") else ""),
         "data": "synthetic (seeded generator)", "config": dict(cfg, l2="flushed before every timed step"),
         "gpu_launches": launches * args.steps, "clocks": clocks,
     }

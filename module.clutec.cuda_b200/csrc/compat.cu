@@ -42,6 +42,7 @@ constexpr int kRW = kTX + kPMax;           // staged base columns (one extra for
 constexpr int kRH = kTY + kPMax - 1;       // staged rows
 constexpr int kMW = kTX + kPMax - 1 + 255; // staged match columns (region + D - 1)
 constexpr int kSubMax = 5;                 // AW sub-window side (Patch_15x15)
+constexpr int kU = 2;                      // scan steps whose window sums share one round of CTA barriers
 
 enum Method { kSad1 = CT_COMPAT_SAD1, kNcc = CT_COMPAT_NCC, kAw1 = CT_COMPAT_AW1, kAw2 = CT_COMPAT_AW2,
               kBm1 = CT_COMPAT_BM1 };
@@ -52,8 +53,8 @@ struct Args {
     const uint8_t* B;  // base image
     const uint8_t* M;  // match image
     size_t pb, pm;
-    const int32_t* mS;   // NCC: box sums of the match image (W * H), and of its squares
-    const int32_t* mQ;
+    const float* mMean;  // NCC: the match image's patch mean and standard deviation (W * H,
+    const float* mStd;   // EvalMsd's FP32 steps, BlockMatcherNCC.cu:222-230)
     void* out;
     size_t out_pitch;
     int out_type;
@@ -94,20 +95,23 @@ __device__ __forceinline__ void store4(const Args& a, int x, int y, uint16_t c0,
         reinterpret_cast<uint16_t*>(row)[x] = c0;
 }
 
-template <int METHOD>
+// PC: the patch side (sub-window side for AW1 / AW2) as a compile-time
+// constant, so that the window loops unroll; 0 = taken from the arguments.
+template <int METHOD, int PC>
 __global__ void __launch_bounds__(kNT) compat_kernel(Args a) {
     constexpr bool AW = METHOD == kAw1 || METHOD == kAw2;
     constexpr bool SIM = METHOD == kNcc || METHOD == kAw1 || METHOD == kBm1;  // argmax scan
     __shared__ uint8_t sB[kRH][kRW + 4];
     __shared__ uint8_t sM[kRH][kMW + 1];
-    __shared__ int32_t sE[kRH][kRW];
-    __shared__ int32_t sV[kTY + 2 * kSubMax][kRW];
-    __shared__ int32_t sS[AW ? kTY + 2 * kSubMax : 1][AW ? kTX + 2 * kSubMax : 1];
+    __shared__ int32_t sE[kU][kRH][kRW];
+    __shared__ int32_t sV[kU][kTY + 2 * kSubMax][kRW];
+    __shared__ int32_t sS[kU][AW ? kTY + 2 * kSubMax : 1][AW ? kTX + 2 * kSubMax : 1];
 
     const int tid = threadIdx.x, tx = tid % kTX, ty = tid / kTX;
     const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
     const int x = x0 + tx, y = y0 + ty;
-    const int P = a.P, s = a.s, pa = P / 2, pb = P - 1 - pa;
+    constexpr bool AWm = METHOD == kAw1 || METHOD == kAw2;
+    const int P = PC ? (AWm ? 3 * PC : PC) : a.P, s = PC ? (AWm ? PC : 0) : a.s, pa = P / 2, pb = P - 1 - pa;
     const int RWc = kTX + P - 1, RHc = kTY + P - 1;
     const int rx0 = x0 - pa, ry0 = y0 - pa;
     const int dmax = a.dmin + a.D - 1;
@@ -191,129 +195,164 @@ __global__ void __launch_bounds__(kNT) compat_kernel(Args a) {
     const int dlim = a.dir ? x - pa : a.W - 1 - pb - x;
 
     const int nsteps = METHOD == kSad1 ? (a.D + 3) / 4 + a.D : a.D;
-    for (int k = 0; k < nsteps; ++k) {
-        int idx, inc = 1;
-        bool fine = false;
+    // scan step k: index idx (disparity d), its increment and whether it is
+    // SAD1's fine pass; the staged match column of region column 0
+    struct Step {
+        int idx, inc, d, moff;
+        bool fine;
+    };
+    auto step_of = [&](int k) {
+        Step st;
+        st.inc = 1;
+        st.fine = false;
         if (METHOD == kSad1) {
             const int nc = (a.D + 3) / 4;
-            if (k < nc) { idx = 4 * k; inc = 4; }
-            else { idx = k - nc; fine = true; }
+            if (k < nc) { st.idx = 4 * k; st.inc = 4; }
+            else { st.idx = k - nc; st.fine = true; }
         } else {
-            idx = k;
+            st.idx = k;
         }
-        const int d = SIM ? a.dmin + idx : dmax - idx;
-        const int moff = a.dir ? dmax - d : d - a.dmin;  // strip column of region column 0
-
-        // per-pixel similarity of the region at disparity d
-        for (int i = tid; i < RHc * RWc; i += kNT) {
-            const int r = i / RWc, c = i % RWc;
-            const int p = sB[r][c], q = sM[r][c + moff];
-            int v;
-            if (METHOD == kSad1 || METHOD == kAw2) v = abs(p - q);
-            else if (METHOD == kNcc) v = p * q;
-            else if (METHOD == kAw1) v = a.sim_type ? signed_product(p, q, 255.0f) : 255 - abs(p - q);
-            else v = a.sim_type ? signed_product(p, q, 127.0f) : (255 - abs(p - q)) >> 1;
-            sE[r][c] = v;
+        st.d = SIM ? a.dmin + st.idx : dmax - st.idx;
+        st.moff = a.dir ? dmax - st.d : st.d - a.dmin;
+        return st;
+    };
+    for (int k0 = 0; k0 < nsteps; k0 += kU) {
+        const int nu = min(kU, nsteps - k0);
+        // per-pixel similarity of the region at the round's disparities
+        for (int u = 0; u < nu; ++u) {
+            const int moff = step_of(k0 + u).moff;
+            for (int r = ty; r < RHc; r += kTY)
+            for (int c = tx; c < RWc; c += kTX) {
+                const int p = sB[r][c], q = sM[r][c + moff];
+                int v;
+                if (METHOD == kSad1 || METHOD == kAw2) v = abs(p - q);
+                else if (METHOD == kNcc) v = p * q;
+                else if (METHOD == kAw1) v = a.sim_type ? signed_product(p, q, 255.0f) : 255 - abs(p - q);
+                else v = a.sim_type ? signed_product(p, q, 127.0f) : (255 - abs(p - q)) >> 1;
+                sE[u][r][c] = v;
+            }
         }
         __syncthreads();
-        int S;
+        int Su[kU];
         if (!AW) {
-            for (int i = tid; i < kTY * RWc; i += kNT) {
-                const int r = i / RWc, c = i % RWc;
-                int t = 0;
-                for (int q = 0; q < P; ++q) t += sE[r + q][c];
-                sV[r][c] = t;
-            }
+            for (int u = 0; u < nu; ++u)
+                for (int c = tx; c < RWc; c += kTX) {
+                    int t = 0;
+                    for (int q = 0; q < P; ++q) t += sE[u][ty + q][c];
+                    sV[u][ty][c] = t;
+                }
             __syncthreads();
-            S = 0;
-            for (int q = 0; q < P; ++q) S += sV[ty][tx + q];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                int S = 0;
+                if (u < nu)
+                    for (int q = 0; q < P; ++q) S += sV[u][ty][tx + q];
+                Su[u] = S;
+            }
         } else {
             const int SR = kTY + 2 * s, SC = kTX + 2 * s;
-            for (int i = tid; i < SR * RWc; i += kNT) {
-                const int r = i / RWc, c = i % RWc;
-                int t = 0;
-                for (int q = 0; q < s; ++q) t += sE[r + q][c];
-                sV[r][c] = t;
-            }
+            for (int u = 0; u < nu; ++u)
+                for (int r = ty; r < SR; r += kTY)
+                for (int c = tx; c < RWc; c += kTX) {
+                    int t = 0;
+                    for (int q = 0; q < s; ++q) t += sE[u][r + q][c];
+                    sV[u][r][c] = t;
+                }
             __syncthreads();
-            for (int i = tid; i < SR * SC; i += kNT) {
-                const int r = i / SC, c = i % SC;
-                int t = 0;
-                for (int q = 0; q < s; ++q) t += sV[r][c + q];
-                sS[r][c] = t;
-            }
+            for (int u = 0; u < nu; ++u)
+                for (int r = ty; r < SR; r += kTY)
+                for (int c = tx; c < SC; c += kTX) {
+                    int t = 0;
+                    for (int q = 0; q < s; ++q) t += sV[u][r][c + q];
+                    sS[u][r][c] = t;
+                }
             __syncthreads();
-            const int C = sS[ty + s][tx + s];
-            const int e0 = sS[ty][tx + s], e1 = sS[ty + s][tx], e2 = sS[ty + 2 * s][tx + s], e3 = sS[ty + s][tx + 2 * s];
-            if (METHOD == kAw1) {  // OrderedInsertMax: the two largest
-                int m1 = e0, m2 = -32767;
-                m2 = max(m2, min(m1, e1)); m1 = max(m1, e1);
-                m2 = max(m2, min(m1, e2)); m1 = max(m1, e2);
-                m2 = max(m2, min(m1, e3)); m1 = max(m1, e3);
-                S = C + m1 + m2;
-            } else {  // OrderedInsert (min): the two smallest
-                int m1 = e0, m2 = 0x7FFFFFFF;
-                m2 = min(m2, max(m1, e1)); m1 = min(m1, e1);
-                m2 = min(m2, max(m1, e2)); m1 = min(m1, e2);
-                m2 = min(m2, max(m1, e3)); m1 = min(m1, e3);
-                S = C + m1 + m2;
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                if (u >= nu) {
+                    Su[u] = 0;
+                    continue;
+                }
+                const int C = sS[u][ty + s][tx + s];
+                const int e0 = sS[u][ty][tx + s], e1 = sS[u][ty + s][tx], e2 = sS[u][ty + 2 * s][tx + s],
+                          e3 = sS[u][ty + s][tx + 2 * s];
+                if (METHOD == kAw1) {  // OrderedInsertMax: the two largest
+                    int m1 = e0, m2 = -32767;
+                    m2 = max(m2, min(m1, e1)); m1 = max(m1, e1);
+                    m2 = max(m2, min(m1, e2)); m1 = max(m1, e2);
+                    m2 = max(m2, min(m1, e3)); m1 = max(m1, e3);
+                    Su[u] = C + m1 + m2;
+                } else {  // OrderedInsert (min): the two smallest
+                    int m1 = e0, m2 = 0x7FFFFFFF;
+                    m2 = min(m2, max(m1, e1)); m1 = min(m1, e1);
+                    m2 = min(m2, max(m1, e2)); m1 = min(m1, e2);
+                    m2 = min(m2, max(m1, e3)); m1 = min(m1, e3);
+                    Su[u] = C + m1 + m2;
+                }
             }
         }
-
-        if (valid && d <= dlim) {
-            if (SIM) {
-                int v;
-                if (METHOD == kNcc) {  // uint8-quantised NCC (NCC.cu:218-271)
-                    const int xm = a.dir ? x - d : x + d;
-                    const size_t om = (size_t)y * a.W + xm;
-                    const float fCross = fdiv(i2f(S), i2f(P * P));
-                    const float fTm = fdiv(i2f(__ldg(&a.mS[om])), i2f(P * P));
-                    const float fTm2 = fdiv(i2f(__ldg(&a.mQ[om])), i2f(P * P));
-                    const float fTstd = __fsqrt_rn(fsub(fTm2, fmul(fTm, fTm)));
-                    const float fNorm = fmul(bStd, fTstd);
-                    float fNcc = fNorm < 1.0f ? 0.0f : fdiv(fsub(fCross, fmul(bMean, fTm)), fNorm);
-                    fNcc = fNcc > 0.0f ? fNcc : 0.0f;
-                    v = int(__float2uint_rz(fminf(255.0f, fmul(fNcc, 255.0f))) & 0xFFu);
+        // the scan updates of the round's steps, in scan order
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            if (u >= nu) break;
+            const Step st = step_of(k0 + u);
+            const int idx = st.idx, inc = st.inc, d = st.d;
+            const bool fine = st.fine;
+            const int S = Su[u];
+            if (valid && d <= dlim) {
+                if (SIM) {
+                    int v;
+                    if (METHOD == kNcc) {  // uint8-quantised NCC (NCC.cu:218-271)
+                        const int xm = a.dir ? x - d : x + d;
+                        const size_t om = (size_t)y * a.W + xm;
+                        const float fCross = fdiv(i2f(S), i2f(P * P));
+                        const float fTm = __ldg(&a.mMean[om]);
+                        const float fTstd = __ldg(&a.mStd[om]);
+                        const float fNorm = fmul(bStd, fTstd);
+                        float fNcc = fNorm < 1.0f ? 0.0f : fdiv(fsub(fCross, fmul(bMean, fTm)), fNorm);
+                        fNcc = fNcc > 0.0f ? fNcc : 0.0f;
+                        v = int(__float2uint_rz(fminf(255.0f, fmul(fNcc, 255.0f))) & 0xFFu);
+                    } else {
+                        v = int(int16_t(S));
+                    }
+                    // EvalSim's bookkeeping (NCC.cu:296-329, AW1.cu:272-307, BM1.cu:262-300)
+                    if (disp <= CT_DISP_LAST) {
+                        const int code = d + CT_DISP_FIRST;
+                        const bool above = v > sMax;
+                        const bool jb = !above && int(disp) + 1 == code;
+                        const bool j2b = !above && int(disp) + 2 == code;
+                        if (above) {
+                            sPrev2 = sPrev; sPrev = sLast; sMax = v; sNext = v; sNext2 = v;
+                            disp = uint16_t(code);
+                        }
+                        if (jb) sNext = v;
+                        if (j2b) sNext2 = v;
+                        sLast = v;
+                    }
                 } else {
-                    v = int(int16_t(S));
-                }
-                // EvalSim's bookkeeping (NCC.cu:296-329, AW1.cu:272-307, BM1.cu:262-300)
-                if (disp <= CT_DISP_LAST) {
-                    const int code = d + CT_DISP_FIRST;
-                    const bool above = v > sMax;
-                    const bool jb = !above && int(disp) + 1 == code;
-                    const bool j2b = !above && int(disp) + 2 == code;
-                    if (above) {
-                        sPrev2 = sPrev; sPrev = sLast; sMax = v; sNext = v; sNext2 = v;
-                        disp = uint16_t(code);
+                    // SAD1 EvalSAD (SAD1.cu:158-190), AW2 UpdateDisp (AW2.cu:143-200)
+                    const bool eval = !fine || (idx + 4 >= int(disp) && idx <= int(disp) + 4);
+                    const bool skip = METHOD == kAw2 ? disp > CT_DISP_LAST : disp == CT_DISP_CANNOT_EVALUATE;
+                    if (eval && !skip) {
+                        const int v = S;
+                        const float fmin = fdiv(i2f(v), i2f(n_eff));
+                        if (idx == 0) {
+                            mW = v; mY = v;
+                            if (METHOD == kAw2) mZ = v;
+                        }
+                        const bool below = v < mX && fmin < a.score_t;
+                        if (below) {
+                            mY = mW; mX = v; mZ = v;
+                            disp = uint16_t(idx);
+                        } else if (int(disp) + inc == idx) {
+                            mZ = v;
+                        }
+                        mW = v;
                     }
-                    if (jb) sNext = v;
-                    if (j2b) sNext2 = v;
-                    sLast = v;
-                }
-            } else {
-                // SAD1 EvalSAD (SAD1.cu:158-190), AW2 UpdateDisp (AW2.cu:143-200)
-                const bool eval = !fine || (idx + 4 >= int(disp) && idx <= int(disp) + 4);
-                const bool skip = METHOD == kAw2 ? disp > CT_DISP_LAST : disp == CT_DISP_CANNOT_EVALUATE;
-                if (eval && !skip) {
-                    const int v = S;
-                    const float fmin = fdiv(i2f(v), i2f(n_eff));
-                    if (idx == 0) {
-                        mW = v; mY = v;
-                        if (METHOD == kAw2) mZ = v;
-                    }
-                    const bool below = v < mX && fmin < a.score_t;
-                    if (below) {
-                        mY = mW; mX = v; mZ = v;
-                        disp = uint16_t(idx);
-                    } else if (int(disp) + inc == idx) {
-                        mZ = v;
-                    }
-                    mW = v;
                 }
             }
         }
-        __syncthreads();  // the next disparity overwrites sE / sV / sS
+        __syncthreads();  // the next round overwrites sE / sV / sS
     }
 
     if (x >= a.W || y >= a.H) return;
@@ -370,9 +409,11 @@ __global__ void __launch_bounds__(kNT) compat_kernel(Args a) {
     store4(a, x, y, id, uint16_t(mX / n_eff), uint16_t(d1), uint16_t(d2));
 }
 
-// Box sums S (values) and Q (squares) of every pixel's P x P patch
-// [x - P/2, x - P/2 + P - 1] (0 where the patch leaves the image).
-__global__ void box_sq_kernel(const uint8_t* img, size_t pitch, int W, int H, int P, int32_t* S, int32_t* Q) {
+// Mean and standard deviation of every pixel's P x P patch [x - P/2,
+// x - P/2 + P - 1] of the match image, in the reference's FP32 steps
+// (fTestMean = S / P^2, fTestMean2 = Q / P^2, sqrt(fTestMean2 - fTestMean^2));
+// 0 where the patch leaves the image (never read there).
+__global__ void box_sq_kernel(const uint8_t* img, size_t pitch, int W, int H, int P, float* mean, float* sd) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= W) return;
     const int pa = P / 2, pb = P - 1 - pa;
@@ -385,8 +426,10 @@ __global__ void box_sq_kernel(const uint8_t* img, size_t pitch, int W, int H, in
                 q += v * v;
             }
     }
-    S[(size_t)y * W + x] = s;
-    Q[(size_t)y * W + x] = q;
+    const float fTm = fdiv(i2f(s), i2f(P * P));
+    const float fTm2 = fdiv(i2f(q), i2f(P * P));
+    mean[(size_t)y * W + x] = fTm;
+    sd[(size_t)y * W + x] = __fsqrt_rn(fsub(fTm2, fmul(fTm, fTm)));
 }
 
 }  // namespace compat
@@ -401,7 +444,7 @@ struct CompatHandle : ct_handle {
     }
     ct_format fmt{};
     ct_compat_params par{};
-    int32_t* stats = nullptr;  // NCC: S and Q planes of the match image
+    float* stats = nullptr;  // NCC: patch mean and standard deviation planes of the match image
 };
 
 }  // namespace
@@ -459,7 +502,7 @@ int ct_bm_compat_configure(ct_handle* hh, int32_t device, const ct_format* fmt, 
     h->device = device;
     if (int rc = h->init_status()) return rc;
     if (p->method == CT_COMPAT_NCC &&
-        cudaMalloc(&h->stats, 2 * (size_t)fmt->width * fmt->height * sizeof(int32_t)) != cudaSuccess)
+        cudaMalloc(&h->stats, 2 * (size_t)fmt->width * fmt->height * sizeof(float)) != cudaSuccess)
         return fail(CT_ENOMEM, "statistics scratch");
     h->fmt = *fmt;
     h->par = *p;
@@ -499,20 +542,41 @@ int ct_bm_compat_process(ct_handle* hh, const ct_image* disp, const ct_image* le
     a.out = disp->ptr; a.out_pitch = disp->pitch_bytes; a.out_type = disp->type;
     if (p.method == CT_COMPAT_NCC) {
         const size_t N = (size_t)a.W * a.H;
-        a.mS = h->stats;
-        a.mQ = h->stats + N;
+        a.mMean = h->stats;
+        a.mStd = h->stats + N;
         compat::box_sq_kernel<<<dim3((a.W + 127) / 128, a.H), 128, 0, s>>>(a.M, a.pm, a.W, a.H, a.P, h->stats,
                                                                           h->stats + N);
         CT_LAUNCH_CHECK();
     }
     const dim3 grid((a.W + compat::kTX - 1) / compat::kTX, (a.H + compat::kTY - 1) / compat::kTY);
+#define CT_COMPAT_LAUNCH(M, PC) compat::compat_kernel<M, PC><<<grid, compat::kNT, 0, s>>>(a)
+    const int pc = p.patch;
     switch (p.method) {
-        case CT_COMPAT_SAD1: compat::compat_kernel<CT_COMPAT_SAD1><<<grid, compat::kNT, 0, s>>>(a); break;
-        case CT_COMPAT_NCC: compat::compat_kernel<CT_COMPAT_NCC><<<grid, compat::kNT, 0, s>>>(a); break;
-        case CT_COMPAT_AW1: compat::compat_kernel<CT_COMPAT_AW1><<<grid, compat::kNT, 0, s>>>(a); break;
-        case CT_COMPAT_AW2: compat::compat_kernel<CT_COMPAT_AW2><<<grid, compat::kNT, 0, s>>>(a); break;
-        default: compat::compat_kernel<CT_COMPAT_BM1><<<grid, compat::kNT, 0, s>>>(a); break;
+        case CT_COMPAT_SAD1:
+            if (pc == 16) CT_COMPAT_LAUNCH(CT_COMPAT_SAD1, 16);
+            else CT_COMPAT_LAUNCH(CT_COMPAT_SAD1, 0);
+            break;
+        case CT_COMPAT_NCC:
+            if (pc == 11) CT_COMPAT_LAUNCH(CT_COMPAT_NCC, 11);
+            else if (pc == 9) CT_COMPAT_LAUNCH(CT_COMPAT_NCC, 9);
+            else CT_COMPAT_LAUNCH(CT_COMPAT_NCC, 5);
+            break;
+        case CT_COMPAT_AW1:
+            if (pc == 3) CT_COMPAT_LAUNCH(CT_COMPAT_AW1, 3);
+            else CT_COMPAT_LAUNCH(CT_COMPAT_AW1, 5);
+            break;
+        case CT_COMPAT_AW2:
+            if (pc == 3) CT_COMPAT_LAUNCH(CT_COMPAT_AW2, 3);
+            else CT_COMPAT_LAUNCH(CT_COMPAT_AW2, 5);
+            break;
+        default:
+            if (pc == 5) CT_COMPAT_LAUNCH(CT_COMPAT_BM1, 5);
+            else if (pc == 9) CT_COMPAT_LAUNCH(CT_COMPAT_BM1, 9);
+            else if (pc == 11) CT_COMPAT_LAUNCH(CT_COMPAT_BM1, 11);
+            else CT_COMPAT_LAUNCH(CT_COMPAT_BM1, 15);
+            break;
     }
+#undef CT_COMPAT_LAUNCH
     CT_LAUNCH_CHECK();
     return CT_OK;
 }
