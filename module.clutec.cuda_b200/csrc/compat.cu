@@ -103,8 +103,10 @@ __global__ void __launch_bounds__(kNT) compat_kernel(Args a) {
     constexpr bool SIM = METHOD == kNcc || METHOD == kAw1 || METHOD == kBm1;  // argmax scan
     __shared__ uint8_t sB[kRH][kRW + 4];
     __shared__ uint8_t sM[kRH][kMW + 1];
-    __shared__ int32_t sE[kU][kRH][kRW];
+    constexpr bool kFillE = AW || METHOD == kBm1;  // similarity staged once per step (AW; BM1's signed product)
+    __shared__ int32_t sE[kFillE ? kU : 1][kFillE ? kRH : 1][kFillE ? kRW : 1];
     __shared__ int32_t sV[kU][kTY + 2 * kSubMax][kRW];
+    __shared__ int32_t sH[AW ? 1 : kU][AW ? 1 : kTY][AW ? 1 : kTX];
     __shared__ int32_t sS[kU][AW ? kTY + 2 * kSubMax : 1][AW ? kTX + 2 * kSubMax : 1];
 
     const int tid = threadIdx.x, tx = tid % kTX, ty = tid / kTX;
@@ -218,38 +220,69 @@ __global__ void __launch_bounds__(kNT) compat_kernel(Args a) {
     };
     for (int k0 = 0; k0 < nsteps; k0 += kU) {
         const int nu = min(kU, nsteps - k0);
-        // per-pixel similarity of the region at the round's disparities
-        for (int u = 0; u < nu; ++u) {
-            const int moff = step_of(k0 + u).moff;
-            for (int r = ty; r < RHc; r += kTY)
-            for (int c = tx; c < RWc; c += kTX) {
-                const int p = sB[r][c], q = sM[r][c + moff];
-                int v;
-                if (METHOD == kSad1 || METHOD == kAw2) v = abs(p - q);
-                else if (METHOD == kNcc) v = p * q;
-                else if (METHOD == kAw1) v = a.sim_type ? signed_product(p, q, 255.0f) : 255 - abs(p - q);
-                else v = a.sim_type ? signed_product(p, q, 127.0f) : (255 - abs(p - q)) >> 1;
-                sE[u][r][c] = v;
-            }
-        }
-        __syncthreads();
+        // per-pixel similarity at a round step's disparity (staged region row r, column c)
+        auto sim = [&](int r, int c, int moff) {
+            const int p = sB[r][c], q = sM[r][c + moff];
+            if (METHOD == kSad1 || METHOD == kAw2) return abs(p - q);
+            if (METHOD == kNcc) return p * q;
+            if (METHOD == kAw1) return a.sim_type ? signed_product(p, q, 255.0f) : 255 - abs(p - q);
+            return a.sim_type ? signed_product(p, q, 127.0f) : (255 - abs(p - q)) >> 1;
+        };
         int Su[kU];
         if (!AW) {
-            for (int u = 0; u < nu; ++u)
-                for (int c = tx; c < RWc; c += kTX) {
-                    int t = 0;
-                    for (int q = 0; q < P; ++q) t += sE[u][ty + q][c];
-                    sV[u][ty][c] = t;
+            // Plain windows. Vertical P-row sums by running sums down each
+            // staged column (one thread per step and column), the similarity
+            // computed on the fly (SAD1, NCC, BM1's absolute difference) or
+            // staged once (BM1's signed product, several FP32 steps); then
+            // horizontal P-wide sums, 4 outputs per thread by running sums
+            // along each row; then each pixel reads its own.
+            const bool staged = kFillE && a.sim_type;
+            if (staged) {
+                for (int u = 0; u < nu; ++u) {
+                    const int moff = step_of(k0 + u).moff;
+                    for (int r = ty; r < RHc; r += kTY)
+                    for (int c = tx; c < RWc; c += kTX) sE[u][r][c] = sim(r, c, moff);
                 }
+                __syncthreads();
+            }
+            for (int i = tid; i < nu * RWc; i += kNT) {
+                const int u = i / RWc, c = i - u * RWc;
+                const int moff = step_of(k0 + u).moff;
+                auto e = [&](int r) {  // (sE has one element unless kFillE)
+                    return staged ? sE[kFillE ? u : 0][kFillE ? r : 0][kFillE ? c : 0] : sim(r, c, moff);
+                };
+                int v = 0;
+                for (int r = 0; r < P; ++r) v += e(r);
+                sV[u][0][c] = v;
+#pragma unroll
+                for (int r = 1; r < kTY; ++r) {
+                    v += e(r + P - 1) - e(r - 1);
+                    sV[u][r][c] = v;
+                }
+            }
+            __syncthreads();
+            for (int i = tid; i < nu * kTY * (kTX / 4); i += kNT) {
+                const int u = i / (kTY * (kTX / 4)), j = i - u * (kTY * (kTX / 4));
+                const int r = j / (kTX / 4), c0 = 4 * (j % (kTX / 4));
+                int v = 0;
+                for (int q = 0; q < P; ++q) v += sV[u][r][c0 + q];
+                sH[u][r][c0] = v;
+#pragma unroll
+                for (int k = 1; k < 4; ++k) {
+                    v += sV[u][r][c0 + k + P - 1] - sV[u][r][c0 + k - 1];
+                    sH[u][r][c0 + k] = v;
+                }
+            }
             __syncthreads();
 #pragma unroll
-            for (int u = 0; u < kU; ++u) {
-                int S = 0;
-                if (u < nu)
-                    for (int q = 0; q < P; ++q) S += sV[u][ty][tx + q];
-                Su[u] = S;
-            }
+            for (int u = 0; u < kU; ++u) Su[u] = u < nu ? sH[u][ty][tx] : 0;
         } else {
+            for (int u = 0; u < nu; ++u) {
+                const int moff = step_of(k0 + u).moff;
+                for (int r = ty; r < RHc; r += kTY)
+                for (int c = tx; c < RWc; c += kTX) sE[u][r][c] = sim(r, c, moff);
+            }
+            __syncthreads();
             const int SR = kTY + 2 * s, SC = kTX + 2 * s;
             for (int u = 0; u < nu; ++u)
                 for (int r = ty; r < SR; r += kTY)
