@@ -42,7 +42,9 @@ constexpr int kRW = kTX + kPMax;           // staged base columns (one extra for
 constexpr int kRH = kTY + kPMax - 1;       // staged rows
 constexpr int kMW = kTX + kPMax - 1 + 255; // staged match columns (region + D - 1)
 constexpr int kSubMax = 5;                 // AW sub-window side (Patch_15x15)
-constexpr int kU = 2;                      // scan steps whose window sums share one round of CTA barriers
+// scan steps whose window sums share one round of CTA barriers (AW, with
+// its sub-window planes, 2; the plain windows 4)
+__host__ __device__ constexpr int steps_per_round(bool aw) { return aw ? 2 : 4; }
 
 enum Method { kSad1 = CT_COMPAT_SAD1, kNcc = CT_COMPAT_NCC, kAw1 = CT_COMPAT_AW1, kAw2 = CT_COMPAT_AW2,
               kBm1 = CT_COMPAT_BM1 };
@@ -104,10 +106,11 @@ __global__ void __launch_bounds__(kNT) compat_kernel(Args a) {
     __shared__ uint8_t sB[kRH][kRW + 4];
     __shared__ uint8_t sM[kRH][kMW + 1];
     constexpr bool kFillE = AW || METHOD == kBm1;  // similarity staged once per step (AW; BM1's signed product)
+    constexpr int kU = steps_per_round(AW);
     __shared__ int32_t sE[kFillE ? kU : 1][kFillE ? kRH : 1][kFillE ? kRW : 1];
-    __shared__ int32_t sV[kU][kTY + 2 * kSubMax][kRW];
+    __shared__ int32_t sV[kU][AW ? kTY + 2 * kSubMax : kTY][kRW];
     __shared__ int32_t sH[AW ? 1 : kU][AW ? 1 : kTY][AW ? 1 : kTX];
-    __shared__ int32_t sS[kU][AW ? kTY + 2 * kSubMax : 1][AW ? kTX + 2 * kSubMax : 1];
+    __shared__ int32_t sS[AW ? kU : 1][AW ? kTY + 2 * kSubMax : 1][AW ? kTX + 2 * kSubMax : 1];
 
     const int tid = threadIdx.x, tx = tid % kTX, ty = tid / kTX;
     const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
@@ -446,21 +449,43 @@ __global__ void __launch_bounds__(kNT) compat_kernel(Args a) {
 // x - P/2 + P - 1] of the match image, in the reference's FP32 steps
 // (fTestMean = S / P^2, fTestMean2 = Q / P^2, sqrt(fTestMean2 - fTestMean^2));
 // 0 where the patch leaves the image (never read there).
-__global__ void box_sq_kernel(const uint8_t* img, size_t pitch, int W, int H, int P, float* mean, float* sd) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= W) return;
-    const int pa = P / 2, pb = P - 1 - pa;
-    int s = 0, q = 0;
-    if (x - pa >= 0 && x + pb < W && y - pa >= 0 && y + pb < H) {
-        for (int r = -pa; r <= pb; ++r)
-            for (int c = -pa; c <= pb; ++c) {
-                const int v = img[(size_t)(y + r) * pitch + x + c];
-                s += v;
-                q += v * v;
-            }
+__global__ void __launch_bounds__(kNT) box_sq_kernel(const uint8_t* img, size_t pitch, int W, int H, int P,
+                                                     float* mean, float* sd) {
+    // separable: the (32 + P - 1) x (8 + P - 1) region of a 32 x 8 tile,
+    // row sums of P pixels (values and squares), then column sums of P rows
+    __shared__ uint8_t t[kTY + kPMax - 1][kTX + kPMax];
+    __shared__ int hs[kTY + kPMax - 1][kTX], hq[kTY + kPMax - 1][kTX];
+    const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+    const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY, pa = P / 2;
+    const int RW = kTX + P - 1, RH = kTY + P - 1;
+    for (int r = ty; r < RH; r += kTY)
+        for (int c = tx; c < RW; c += kTX) {
+            const int yy = y0 - pa + r, xx = x0 - pa + c;
+            t[r][c] = (xx >= 0 && xx < W && yy >= 0 && yy < H) ? img[(size_t)yy * pitch + xx] : 0;
+        }
+    __syncthreads();
+    for (int r = ty; r < RH; r += kTY) {
+        int sv = 0, sq = 0;
+        for (int c = 0; c < P; ++c) {
+            const int v = t[r][tx + c];
+            sv += v;
+            sq += v * v;
+        }
+        hs[r][tx] = sv;
+        hq[r][tx] = sq;
     }
-    const float fTm = fdiv(i2f(s), i2f(P * P));
-    const float fTm2 = fdiv(i2f(q), i2f(P * P));
+    __syncthreads();
+    const int x = x0 + tx, y = y0 + ty;
+    if (x >= W || y >= H) return;
+    const int pb = P - 1 - pa;
+    int sv = 0, sq = 0;
+    if (x - pa >= 0 && x + pb < W && y - pa >= 0 && y + pb < H)
+        for (int r = 0; r < P; ++r) {
+            sv += hs[ty + r][tx];
+            sq += hq[ty + r][tx];
+        }
+    const float fTm = fdiv(i2f(sv), i2f(P * P));
+    const float fTm2 = fdiv(i2f(sq), i2f(P * P));
     mean[(size_t)y * W + x] = fTm;
     sd[(size_t)y * W + x] = __fsqrt_rn(fsub(fTm2, fmul(fTm, fTm)));
 }
@@ -577,8 +602,8 @@ int ct_bm_compat_process(ct_handle* hh, const ct_image* disp, const ct_image* le
         const size_t N = (size_t)a.W * a.H;
         a.mMean = h->stats;
         a.mStd = h->stats + N;
-        compat::box_sq_kernel<<<dim3((a.W + 127) / 128, a.H), 128, 0, s>>>(a.M, a.pm, a.W, a.H, a.P, h->stats,
-                                                                          h->stats + N);
+        compat::box_sq_kernel<<<dim3((a.W + compat::kTX - 1) / compat::kTX, (a.H + compat::kTY - 1) / compat::kTY),
+                                compat::kNT, 0, s>>>(a.M, a.pm, a.W, a.H, a.P, h->stats, h->stats + N);
         CT_LAUNCH_CHECK();
     }
     const dim3 grid((a.W + compat::kTX - 1) / compat::kTX, (a.H + compat::kTY - 1) / compat::kTY);
