@@ -86,8 +86,12 @@ def _params(seed):
     return p.astype(np.float32)
 
 
-def test_training_forward_and_gradient_vs_oracle(ct, oracle, cuda):
-    n = 600
+@pytest.mark.parametrize("n", [600, 37, 1023])
+def test_training_forward_and_gradient_vs_oracle(ct, oracle, cuda, n):
+    """Scores, loss and gradient of a batch against the FP64 oracle. The
+    batch sizes cover partial 128-row GEMM tiles, a batch below one tile and
+    batches that are not a multiple of 8 (the zero-padded sample columns of
+    the weight-gradient GEMMs) and of the 256-sample chunks."""
     x = _real_samples(ct, oracle, n, 7)
     y = (np.random.default_rng(2).random(n) < 0.7).astype(np.uint8)
     p = _params(3)
