@@ -4,8 +4,8 @@
 //   parabolic sub-pixel refinement).
 //
 // Layout (same decomposition as the census matcher): a CTA owns 128 "V
-// columns" x th output rows x 64 disparities; warp w owns 8 disparities and
-// lane L the 4 adjacent columns 4L..4L+3. The uint8 image strips the CTA needs
+// columns" x th output rows x 64 disparities; warp w owns DPW = 4 or 8
+// disparities (16 or 8 warps) and lane L the 4 adjacent columns 4L..4L+3. The uint8 image strips the CTA needs
 // (th + 2*ext rows of the base view, 128 + 16 columns; of the match view,
 // 192 + 16 columns) are staged in shared memory by two 2D TMA loads. Each
 // thread walks the strip downwards keeping vertical running sums of |B - M|
@@ -28,7 +28,12 @@
 namespace ct {
 namespace ad {
 
-constexpr int kCPT = 4, kTWV = 128, kDPW = 8, kNW = 8, kNT = kNW * 32, kDPC = kDPW * kNW;
+constexpr int kCPT = 4, kTWV = 128, kDPC = 64;
+constexpr int kPairs = kDPC / 2;         // disparity pairs per CTA (two disparities per 32-bit register)
+// Disparities per warp DPW (4: 16 warps, 8: 8 warps per CTA; the kernel is
+// instantiated for both): warps, threads, pairs per thread, match columns a
+// thread reads per row.
+__host__ __device__ constexpr int nt_of(int dpw) { return kDPC / dpw * 32; }
 constexpr int kBW = kTWV + 16;        // staged base columns
 constexpr int kMWs = kTWV + kDPC + 16; // staged match columns (208)
 constexpr int kRing = 7;              // AW: rows of S kept
@@ -64,7 +69,7 @@ __host__ __device__ constexpr size_t strip_bytes(int th, int R, bool aw) {
            (size_t(kMWs) * (th + 2 * ext_of(R, aw)) + 127) / 128 * 128;
 }
 __host__ __device__ constexpr size_t smem_bytes(int th, int R, bool aw) {
-    return strip_bytes(th, R, aw) + (aw ? size_t(kRing) * kNW * 4 * kRingW * 4 : 0) +
+    return strip_bytes(th, R, aw) + (aw ? size_t(kRing) * kPairs * kRingW * 4 : 0) +
            size_t(th) * two_of(R, aw) * 4 + 16;
 }
 
@@ -107,9 +112,11 @@ __device__ __forceinline__ void hsum(const uint32_t (&V)[kCPT], uint32_t (&C)[kC
     }
 }
 
-template <int R, bool AW, int DIR, bool G>  // G: guided (AW only)
-__global__ void __launch_bounds__(kNT, 1)
+template <int R, bool AW, int DIR, bool G, int DPW>  // G: guided (AW only)
+__global__ void __launch_bounds__(nt_of(DPW), 1)
     ad_match_kernel(const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmM, Args a) {
+    constexpr int kDPW = DPW, kNW = kDPC / DPW, kNT = nt_of(DPW), kNP = DPW / 2, kMC = kCPT + DPW - 1;
+    static_assert(kNW * kNP == kPairs, "pairs per CTA");
     constexpr int EXT = ext_of(R, AW);
     constexpr int TWO = two_of(R, AW);
     extern __shared__ __align__(128) unsigned char smem[];
@@ -118,7 +125,7 @@ __global__ void __launch_bounds__(kNT, 1)
     uint8_t* sM = smem + (size_t(kBW) * NR + 127) / 128 * 128;
     unsigned char* after = smem + strip_bytes(a.th, R, AW);
     uint32_t* ring = reinterpret_cast<uint32_t*>(after);  // AW only
-    uint32_t* sKey = reinterpret_cast<uint32_t*>(after + (AW ? size_t(kRing) * kNW * 4 * kRingW * 4 : 0));
+    uint32_t* sKey = reinterpret_cast<uint32_t*>(after + (AW ? size_t(kRing) * kNW * kNP * kRingW * 4 : 0));
     uint64_t* bar = reinterpret_cast<uint64_t*>(sKey + a.th * TWO);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -167,95 +174,95 @@ __global__ void __launch_bounds__(kNT, 1)
     }
 
     const int bo = xs - ab + 4 * lane;                                        // base column 0 in strip
-    const int mo = DIR == 0 ? (xs - a.dmin - dz0 - am) + 4 * lane - kDPW * warp - 7   // match column (c=0, j=7)
-                            : (xs + a.dmin + dz0 - am) + 4 * lane + kDPW * warp;      // match column (c=0, j=0)
-    uint32_t dlo[4];
+    const int mo = DIR == 0 ? (xs - a.dmin - dz0 - am) + 4 * lane - kDPW * warp - (kDPW - 1)  // (c=0, j=kDPW-1)
+                            : (xs + a.dmin + dz0 - am) + 4 * lane + kDPW * warp;                // (c=0, j=0)
+    uint32_t dlo[kNP];
 #pragma unroll
-    for (int p = 0; p < 4; ++p) dlo[p] = uint32_t(dw + 2 * p);
+    for (int p = 0; p < kNP; ++p) dlo[p] = uint32_t(dw + 2 * p);
 
-    auto row_pairs = [&](int i, uint32_t (&P)[kCPT][4]) {
+    auto row_pairs = [&](int i, uint32_t (&P)[kCPT][kNP]) {
         const uint8_t* rb = sB + i * kBW + bo;
         const uint8_t* rm = sM + i * kMWs + mo;
-        uint32_t b2[kCPT], m2[10];
+        uint32_t b2[kCPT], m2[kMC - 1];
 #pragma unroll
         for (int c = 0; c < kCPT; ++c) b2[c] = uint32_t(rb[c]) * 0x10001u;  // b in both halves
         // match pixel pairs: the low half is disparity 2p of the pair, the
         // high half 2p + 1 (left-to-right: columns k0, k0 - 1; right-to-left:
         // k0, k0 + 1)
         {
-            uint32_t m[11];
+            uint32_t m[kMC];
 #pragma unroll
-            for (int k = 0; k < 11; ++k) m[k] = rm[k];
+            for (int k = 0; k < kMC; ++k) m[k] = rm[k];
 #pragma unroll
-            for (int k = 0; k < 10; ++k) m2[k] = DIR == 0 ? m[k + 1] + (m[k] << 16) : m[k] + (m[k + 1] << 16);
+            for (int k = 0; k < kMC - 1; ++k) m2[k] = DIR == 0 ? m[k + 1] + (m[k] << 16) : m[k] + (m[k + 1] << 16);
         }
 #pragma unroll
         for (int c = 0; c < kCPT; ++c)
 #pragma unroll
-            for (int p = 0; p < 4; ++p) {
-                const uint32_t mp = m2[DIR == 0 ? c - 2 * p + 6 : c + 2 * p];
+            for (int p = 0; p < kNP; ++p) {
+                const uint32_t mp = m2[DIR == 0 ? c - 2 * p + kDPW - 2 : c + 2 * p];
                 P[c][p] = __vmaxu2(b2[c] + kAbsBias - mp, mp + kAbsBias - b2[c]);  // |b - m| + 256 per half
             }
     };
 
-    uint32_t V[4][kCPT];  // [pair][column]
+    uint32_t V[kNP][kCPT];  // [pair][column]
 #pragma unroll
-    for (int p = 0; p < 4; ++p)
+    for (int p = 0; p < kNP; ++p)
 #pragma unroll
         for (int c = 0; c < kCPT; ++c) V[p][c] = 0;
 
     if (warp_active) {
         for (int i = 0; i < NR; ++i) {
-            uint32_t Pn[kCPT][4];
+            uint32_t Pn[kCPT][kNP];
             row_pairs(i, Pn);
             if (i >= 2 * R + 1) {
-                uint32_t Po[kCPT][4];
+                uint32_t Po[kCPT][kNP];
                 row_pairs(i - 2 * R - 1, Po);
 #pragma unroll
                 for (int c = 0; c < kCPT; ++c)
 #pragma unroll
-                    for (int p = 0; p < 4; ++p) V[p][c] = V[p][c] + Pn[c][p] - Po[c][p];
+                    for (int p = 0; p < kNP; ++p) V[p][c] = V[p][c] + Pn[c][p] - Po[c][p];
             } else {
 #pragma unroll
                 for (int c = 0; c < kCPT; ++c)
 #pragma unroll
-                    for (int p = 0; p < 4; ++p) V[p][c] += Pn[c][p];
+                    for (int p = 0; p < kNP; ++p) V[p][c] += Pn[c][p];
             }
             if (i < 2 * R) continue;
             // S (box sums) of strip row i - R, all 4 pairs
-            uint32_t S[4][kCPT];
+            uint32_t S[kNP][kCPT];
 #pragma unroll
-            for (int p = 0; p < 4; ++p) hsum<R>(V[p], S[p]);
+            for (int p = 0; p < kNP; ++p) hsum<R>(V[p], S[p]);
             int oy;
-            uint32_t A[4][kCPT];
+            uint32_t A[kNP][kCPT];
             if (!AW) {
                 oy = i - 2 * R;
 #pragma unroll
-                for (int p = 0; p < 4; ++p)
+                for (int p = 0; p < kNP; ++p)
 #pragma unroll
                     for (int c = 0; c < kCPT; ++c) A[p][c] = S[p][c];
             } else {
                 // S row index since the first S row: s = i - 2R; ring slot s % 7
                 const int s = i - 2 * R;
-                uint32_t* slot = ring + size_t(s % kRing) * kNW * 4 * kRingW;
+                uint32_t* slot = ring + size_t(s % kRing) * kNW * kNP * kRingW;
 #pragma unroll
-                for (int p = 0; p < 4; ++p)
-                    *reinterpret_cast<uint4*>(slot + (warp * 4 + p) * kRingW + 4 + 4 * lane) =
+                for (int p = 0; p < kNP; ++p)
+                    *reinterpret_cast<uint4*>(slot + (warp * kNP + p) * kRingW + 4 + 4 * lane) =
                         make_uint4(S[p][0], S[p][1], S[p][2], S[p][3]);
                 __syncwarp();
                 if (s < 2 * R) continue;  // need S rows s - 3 and s - 6
                 oy = s - 2 * R;
-                const uint32_t* mid = ring + size_t((s - R) % kRing) * kNW * 4 * kRingW;
-                const uint32_t* top = ring + size_t((s - 2 * R) % kRing) * kNW * 4 * kRingW;
+                const uint32_t* mid = ring + size_t((s - R) % kRing) * kNW * kNP * kRingW;
+                const uint32_t* top = ring + size_t((s - 2 * R) % kRing) * kNW * kNP * kRingW;
 #pragma unroll
-                for (int p = 0; p < 4; ++p) {
-                    const uint32_t* rm = mid + (warp * 4 + p) * kRingW + 4 * lane;  // padded index of col 4L-4
+                for (int p = 0; p < kNP; ++p) {
+                    const uint32_t* rm = mid + (warp * kNP + p) * kRingW + 4 * lane;  // padded index of col 4L-4
                     const uint4 q0 = *reinterpret_cast<const uint4*>(rm);
                     const uint4 q1 = *reinterpret_cast<const uint4*>(rm + 4);
                     const uint4 q2 = *reinterpret_cast<const uint4*>(rm + 8);
                     const uint32_t w12[12] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w,
                                               q2.x, q2.y, q2.z, q2.w};  // cols 4L-4 .. 4L+7
-                    const uint4 t = *reinterpret_cast<const uint4*>(top + (warp * 4 + p) * kRingW + 4 + 4 * lane);
+                    const uint4 t = *reinterpret_cast<const uint4*>(top + (warp * kNP + p) * kRingW + 4 + 4 * lane);
                     const uint32_t tw[4] = {t.x, t.y, t.z, t.w};
 #pragma unroll
                     for (int c = 0; c < kCPT; ++c) {
@@ -283,7 +290,7 @@ __global__ void __launch_bounds__(kNT, 1)
                     lim = min(lim, int(g >> 16));
                 }
 #pragma unroll
-                for (int p = 0; p < 4; ++p) {
+                for (int p = 0; p < kNP; ++p) {
                     uint32_t klo = __byte_perm(A[p][c], dlo[p], 0x1054);        // cost_lo << 16 | d
                     uint32_t khi = (A[p][c] & 0xFFFF0000u) | (dlo[p] + 1);       // cost_hi << 16 | d+1
                     if (!interior || G) {
@@ -495,26 +502,37 @@ struct AdHandle : ct_handle {
     int th = 32;
 };
 
-template <int R, bool AW, int DIR, bool G>
+template <int R, bool AW, int DIR, bool G, int DPW>
 int set_attr() {
     static bool done = false;
     if (!done) {
-        CT_CUDA_TRY(cudaFuncSetAttribute(ad::ad_match_kernel<R, AW, DIR, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CT_CUDA_TRY(cudaFuncSetAttribute(ad::ad_match_kernel<R, AW, DIR, G, DPW>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)ad::smem_bytes(64, R, AW)));
         done = true;
     }
     return CT_OK;
 }
 
+// Disparities per warp: 4 (16 warps per CTA) for the adaptive windows and
+// the SAD windows from 7x7 up, which are bound by instruction latency at one
+// CTA per SM; 8 for the smaller SAD windows, where loading each base pixel
+// for 8 disparities saves more than the extra warps hide (measured: AW
+// 2560x1440 1.162 -> 1.025 ms and SAD 9x9 640x480 0.0266 -> 0.0245 ms with 4;
+// SAD 5x5 1920x1080 0.1833 ms with 8 against 0.1933 with 4).
+template <int R, bool AW>
+constexpr int dpw_for() { return (AW || R >= 3) ? 4 : 8; }
+
 template <int R, bool AW, int DIR>
 int launch_ad(AdHandle* h, const ct_image* disp, const ct_image* L, const ct_image* Rimg, cudaStream_t s,
               const ct_image* init = nullptr) {
     using namespace ad;
     const bool guided = AW && init;  // the guided variant exists for the AW matcher only
+    constexpr int DPW = dpw_for<R, AW>();
     if constexpr (AW) {
-        if (int rc = guided ? set_attr<R, AW, DIR, true>() : set_attr<R, AW, DIR, false>()) return rc;
+        if (int rc = guided ? set_attr<R, AW, DIR, true, DPW>() : set_attr<R, AW, DIR, false, DPW>()) return rc;
     } else {
-        if (int rc = set_attr<R, AW, DIR, false>()) return rc;
+        if (int rc = set_attr<R, AW, DIR, false, DPW>()) return rc;
     }
     const int W = h->fmt.width, H = h->fmt.height;
     constexpr int EXT = ext_of(R, AW), TWO = two_of(R, AW);
@@ -540,13 +558,14 @@ int launch_ad(AdHandle* h, const ct_image* disp, const ct_image* L, const ct_ima
     if (int rc = make_tmap_2d(&tb, B->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, W, H, B->pitch_bytes, kBW, NR)) return rc;
     if (int rc = make_tmap_2d(&tm, M->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, W, H, M->pitch_bytes, kMWs, NR)) return rc;
     dim3 grid((W + TWO - 1) / TWO, (H + a.th - 1) / a.th, (h->D + kDPC - 1) / kDPC);
+    constexpr int NT = nt_of(DPW);
     if constexpr (AW) {
         if (guided)
-            ad_match_kernel<R, AW, DIR, true><<<grid, kNT, smem_bytes(a.th, R, AW), s>>>(tb, tm, a);
+            ad_match_kernel<R, AW, DIR, true, DPW><<<grid, NT, smem_bytes(a.th, R, AW), s>>>(tb, tm, a);
         else
-            ad_match_kernel<R, AW, DIR, false><<<grid, kNT, smem_bytes(a.th, R, AW), s>>>(tb, tm, a);
+            ad_match_kernel<R, AW, DIR, false, DPW><<<grid, NT, smem_bytes(a.th, R, AW), s>>>(tb, tm, a);
     } else {
-        ad_match_kernel<R, AW, DIR, false><<<grid, kNT, smem_bytes(a.th, R, AW), s>>>(tb, tm, a);
+        ad_match_kernel<R, AW, DIR, false, DPW><<<grid, NT, smem_bytes(a.th, R, AW), s>>>(tb, tm, a);
     }
     CT_LAUNCH_CHECK();
     const ct_image* base = DIR == 0 ? L : Rimg;
