@@ -390,23 +390,11 @@ __global__ void __launch_bounds__(kSpX * kSpTY) aw_subpixel_kernel(uint32_t* key
             hi = max(hi, e);
         }
     }
-    __syncthreads();  // sRange initialised
-    lo = __reduce_min_sync(0xffffffffu, lo);
-    hi = __reduce_max_sync(0xffffffffu, hi);
-    if ((tid & 31) == 0) {
-        atomicMin(&sRange[0], lo);
-        atomicMax(&sRange[1], hi);
-    }
-    __syncthreads();
-    const int emin = sRange[0], emax = sRange[1];
-    if (emin > emax) return;  // no pixel of the tile is refined
-    // Staged in 16-byte chunks (the images' rows start 16-byte aligned, as
+    // Staging in 16-byte chunks (the images' rows start 16-byte aligned, as
     // their TMA maps require); a chunk reaching past the width is read byte
-    // by byte, chunks outside the image read 0. Base: columns x0 - 16 + c;
-    // match band: columns rs + c covering x0 - emax - 7 .. x0 + 38 - emin
-    // (emax - emin <= D - 3 <= 253: at most 21 chunks).
-    const int rs = (x0 - emax - 7) & ~15;
-    const int nch = (x0 + 38 - emin - rs) / 16 + 1;
+    // by byte, chunks outside the image read 0. The base tile (columns
+    // x0 - 16 + c) does not depend on the winners: its loads go out with the
+    // key loads, before the range reduction.
     auto chunk = [&](const uint8_t* img, size_t ip, int gy, int gx, uint8_t* dst) {
         uint4 v = make_uint4(0, 0, 0, 0);
         if (gy >= 0 && gy < H && gx >= 0 && gx < W) {
@@ -427,6 +415,20 @@ __global__ void __launch_bounds__(kSpX * kSpTY) aw_subpixel_kernel(uint32_t* key
         const int r = i / (kSpLCols / 16), j = i - r * (kSpLCols / 16);
         chunk(L, pl, y0 - 6 + r, x0 - 16 + 16 * j, &sL[r][16 * j]);
     }
+    __syncthreads();  // sRange initialised
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    if ((tid & 31) == 0) {
+        atomicMin(&sRange[0], lo);
+        atomicMax(&sRange[1], hi);
+    }
+    __syncthreads();
+    const int emin = sRange[0], emax = sRange[1];
+    if (emin > emax) return;  // no pixel of the tile is refined
+    // match band: columns rs + c covering x0 - emax - 7 .. x0 + 38 - emin
+    // (emax - emin <= D - 3 <= 253: at most 21 chunks)
+    const int rs = (x0 - emax - 7) & ~15;
+    const int nch = (x0 + 38 - emin - rs) / 16 + 1;
     for (int i = tid; i < kSpRows * nch; i += kSpX * kSpTY) {
         const int r = i / nch, j = i - r * nch;
         chunk(Rm, pr, y0 - 6 + r, rs + 16 * j, &sR[r][16 * j]);
