@@ -119,6 +119,7 @@ struct BmCensusHandle : ct_handle {
         cudaFree(counters);
         cudaFree(tmp_lr);
         cudaFree(tmp_rl);
+        cudaFree(rl_keys);
     }
     ct_format fmt{};
     ct_census_match_params par{};
@@ -126,6 +127,8 @@ struct BmCensusHandle : ct_handle {
     size_t desc_pitch = 0;         // elements
     uint32_t* keys = nullptr;      // ceil(D/64) planes of W*H merge keys
     uint32_t* counters = nullptr;  // one per (strip, column tile); 0 between calls
+    uint32_t* rl_keys = nullptr;   // W*H right-view keys of the fused pass; 0xFFFFFFFF between calls
+    int fuse_rl = 1;               // process_lr: right-to-left winners from the left-to-right pass
     uint16_t* tmp_lr = nullptr;    // U16 maps for process_lr when the caller wants only one
     uint16_t* tmp_rl = nullptr;
     size_t tmp_pitch = 0;
@@ -147,7 +150,8 @@ H* as(ct_handle* h, Kind k) {
 }
 
 int census_match_pass_maps(BmCensusHandle* h, int dir, const ct_image* disp, const CUtensorMap& tb,
-                           const CUtensorMap& tm, cudaStream_t s, const ct_curves* curves = nullptr) {
+                           const CUtensorMap& tm, cudaStream_t s, const ct_curves* curves = nullptr,
+                           const ct_image* disp_rl = nullptr) {
     using namespace cm;
     MatchArgs a{};
     a.W = h->fmt.width; a.H = h->fmt.height;
@@ -167,9 +171,15 @@ int census_match_pass_maps(BmCensusHandle* h, int dir, const ct_image* disp, con
         a.curve_pitch = curves->pitch_bytes / 4;
         a.curve_groups = (a.D + 3) / 4;
     }
+    if (disp_rl) a.rl_keys = h->rl_keys;  // left-to-right pass bidding for the right view too
     const cudaError_t e = dir == 0 ? launch_census_match<0>(tb, tm, a, s, h->dpw)
                                    : launch_census_match<1>(tb, tm, a, s, h->dpw);
     if (e != cudaSuccess) return fail(CT_ECUDA, "census match launch failed: %s", cudaGetErrorString(e));
+    if (disp_rl) {
+        rl_finalize_kernel<<<dim3((a.W + 255) / 256, a.H), 256, 0, s>>>(h->rl_keys, a.W, a.H, kAR, disp_rl->ptr,
+                                                                        disp_rl->pitch_bytes, disp_rl->type);
+        CT_LAUNCH_CHECK();
+    }
     return CT_OK;
 }
 
@@ -285,7 +295,9 @@ int ct_bm_census_configure(ct_handle* hh, int32_t device, const ct_format* fmt, 
     if (int rc = use_device(device)) return rc;
     // release a previous configuration
     cudaFree(h->desc); cudaFree(h->keys); cudaFree(h->counters); cudaFree(h->tmp_lr); cudaFree(h->tmp_rl);
+    cudaFree(h->rl_keys);
     h->desc = nullptr; h->keys = nullptr; h->counters = nullptr; h->tmp_lr = nullptr; h->tmp_rl = nullptr;
+    h->rl_keys = nullptr;
     h->device = device;
     if (int rc = h->init_status()) return rc;
     const int W = fmt->width, H = fmt->height;
@@ -300,6 +312,8 @@ int ct_bm_census_configure(ct_handle* hh, int32_t device, const ct_format* fmt, 
     h->tmp_pitch = ((size_t)W * 2 + 255) / 256 * 256;
     if (cudaMalloc(&h->tmp_lr, h->tmp_pitch * H) != cudaSuccess) return fail(CT_ENOMEM, "map scratch");
     if (cudaMalloc(&h->tmp_rl, h->tmp_pitch * H) != cudaSuccess) return fail(CT_ENOMEM, "map scratch");
+    if (cudaMalloc(&h->rl_keys, W * H * 4) != cudaSuccess) return fail(CT_ENOMEM, "right-view key scratch");
+    CT_CUDA_TRY(cudaMemset(h->rl_keys, 0xFF, W * H * 4));
     h->fmt = *fmt;  // left_desc() / right_desc() below depend on the height
     h->th = cm::pick_strip_height(W, H, p->disp_count, sm_count(device));
     CT_CUDA_TRY(cm::prepare_census_match());
@@ -400,10 +414,16 @@ int ct_bm_census_process_lr(ct_handle* hh, const ct_image* disp_lr, const ct_ima
     const ct_image* lr = disp_lr ? disp_lr : &tlr;
     const ct_image* rl = disp_rl ? disp_rl : &trl;
     const bool need_lr = disp_lr || disp_checked, need_rl = disp_rl || disp_checked;
-    if (need_lr)
-        if (int rc = census_match_pass(h, 0, lr, s)) return rc;
-    if (need_rl)
-        if (int rc = census_match_pass(h, 1, rl, s)) return rc;
+    if (need_lr && need_rl && h->fuse_rl) {
+        // one pass: the left-to-right costs also decide the right-to-left
+        // winners (the same windows; same maps as two passes)
+        if (int rc = census_match_pass_maps(h, 0, lr, h->tm_lb, h->tm_rm, s, nullptr, rl)) return rc;
+    } else {
+        if (need_lr)
+            if (int rc = census_match_pass(h, 0, lr, s)) return rc;
+        if (need_rl)
+            if (int rc = census_match_pass(h, 1, rl, s)) return rc;
+    }
     if (disp_checked) return crosscheck_launch(disp_checked, lr, rl, tol, 1, nullptr, s);
     return CT_OK;
 }

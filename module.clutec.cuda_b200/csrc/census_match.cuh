@@ -116,6 +116,13 @@ struct MatchArgs {
     uint32_t* curve;
     size_t curve_pitch;  // 32-bit words per row, a multiple of 4
     int curve_groups;    // ceil(D / 4)
+    // Fused right-to-left winner (left-to-right kernels instantiated with
+    // RL = true): one key per right-view pixel, W * H, 0xFFFFFFFF between
+    // calls (rl_finalize_kernel resets it). The 5x5 Hamming cost of right
+    // pixel x_R at disparity e equals the left-to-right cost of left pixel
+    // x_R + e at e (the same two windows), so every cost this pass computes
+    // also bids for the right view: key (C << 16) | e, e = dmin + d absolute.
+    uint32_t* rl_keys;
 };
 
 // Curve word pitch for width W: words 0 .. W + 1 used, rounded up to 64
@@ -128,6 +135,11 @@ __host__ __device__ constexpr size_t curve_pitch_words(int W) { return (size_t(W
 __host__ __device__ constexpr size_t smem_bytes() {
     return size_t(2) * (kStageB + kStageM) + size_t(2) * kGroups * kBR * kTWV * 4 + 2 * 8 + 16;
 }
+// The fused right-to-left keys: 2 buffers x kBR rows x kRLW right-view
+// columns (V columns minus the 64 disparities of the CTA), after the rest.
+constexpr int kRLW = kTWV + kDPC;  // 192 (191 used)
+__host__ __device__ constexpr size_t rl_offset() { return (smem_bytes() + 127) / 128 * 128; }
+__host__ __device__ constexpr size_t smem_bytes_rl() { return rl_offset() + size_t(2) * kBR * kRLW * 4; }
 
 // Disparity code for an output pixel from its merged key (C << 16 | d), d
 // relative to dmin.
@@ -158,11 +170,13 @@ struct TileResult {
     bool aborted;
 };
 
-template <int DIR, bool EDGE, int DPW, bool CURVE>
+template <int DIR, bool EDGE, int DPW, bool CURVE, bool RL = false>
 __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const CUtensorMap* tmM,
                                                  const MatchArgs& a, const Tile& t, uint64_t* sB, uint64_t* sM,
                                                  uint32_t* sKey, uint64_t* bars, int* sflag, const uint32_t* par,
-                                                 int nb, int rows_here, int xs, int y0, int ye0, int dz0, int ms) {
+                                                 int nb, int rows_here, int xs, int y0, int ye0, int dz0, int ms,
+                                                 uint32_t* sKeyRL = nullptr) {
+    static_assert(!RL || (DIR == 0 && !CURVE), "the fused right-to-left keys ride on the plain left-to-right pass");
     using VT = Var<DPW>;
     constexpr int NP = VT::kNP, NT = VT::kNT, NWD = VT::kWords;
     constexpr uint32_t kBytes = kTxB + kTxM;
@@ -193,6 +207,18 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
         const int x = xs + 4 * lane + c;
         lim[c] = min(DIR == 0 ? x - kAR - a.dmin : a.W - 1 - kAR - x - a.dmin, a.D - 1);
     }
+    // fused right-to-left: columns whose costs may not bid (the halo columns,
+    // and columns whose window leaves the image on the right: right pixel
+    // x - e must keep x - e + e + 2 <= W - 1) get cost 0xFFFF in both halves
+    uint32_t rlbad[kCPT];
+    uint32_t rld[DPW];  // absolute disparity of relative d = dw + j
+#pragma unroll
+    for (int c = 0; c < kCPT; ++c) {
+        const int v = 4 * lane + c, x = xs + v;
+        rlbad[c] = (v < kAR || v >= kAR + kTWO || x > a.W - 1 - kAR) ? 0xFFFFFFFFu : 0u;
+    }
+#pragma unroll
+    for (int j = 0; j < DPW; ++j) rld[j] = uint32_t(a.dmin + dw + j);
     // First match column this thread reads per row, as an (even) offset from
     // ms: its words are the pairs (ms + mstart) / 2 + u, u < NWD / 2.
     const int mstart = DIR == 0 ? 4 * lane + kDPC - DPW - DPW * warp : 4 * lane + DPW * warp;
@@ -336,6 +362,37 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
             m = dev::min_u16x2(m, __byte_perm(m, 0u, 0x1032));  // both halves = the minimum
             atomicMin(&krow[c * 32], m);
         }
+        if constexpr (RL) {
+            // cost of (column c, relative disparity dw + j) bids for right
+            // pixel index c - j + base: min along each anti-diagonal
+            // a = c - j, one shared atomic each
+            uint32_t Cm[kCPT][NP];
+#pragma unroll
+            for (int c = 0; c < kCPT; ++c)
+#pragma unroll
+                for (int p = 0; p < NP; ++p) {
+                    Cm[c][p] = C[c][p] | rlbad[c];
+                    if (EDGE) {
+                        const int dlo = dw + 2 * p;
+                        Cm[c][p] |= (dlo > lim[c] || dlo < a.dfirst ? 0x0000FFFFu : 0u) |
+                                    (dlo + 1 > lim[c] ? 0xFFFF0000u : 0u);
+                    }
+                }
+            auto key = [&](int c, int j) {
+                return (j & 1) ? ((Cm[c][j >> 1] & 0xFFFF0000u) | rld[j]) : ((Cm[c][j >> 1] << 16) | rld[j]);
+            };
+            uint32_t* rrow = sKeyRL + (buf * kBR + r) * kRLW + (4 * lane - (dw - dz0) + (kDPC - 1));
+#pragma unroll
+            for (int ad = -(DPW - 1); ad <= kCPT - 1; ++ad) {
+                uint32_t m = 0xFFFFFFFFu;
+#pragma unroll
+                for (int c = 0; c < kCPT; ++c) {
+                    const int j = c - ad;
+                    if (j >= 0 && j < DPW) m = min(m, key(c, j));
+                }
+                atomicMin(&rrow[ad], m);
+            }
+        }
     };
 
     // Merges the groups of key buffer `buf`, slots r0 .. r1-1 (output row
@@ -364,6 +421,22 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
                 } else {
                     atomicMin(&a.keys[(size_t)y * a.W + x], best);
                 }
+            }
+        }
+    };
+    // The fused right-to-left keys of buffer `buf`, slots r0 .. r1-1: bids
+    // into the global plane, slots reset.
+    auto flush_rl = [&](int buf, int oy0, int r0, int r1) {
+        if constexpr (RL) {
+            const int xr0 = xs - a.dmin - dz0 - (kDPC - 1);  // right-view column of index 0
+            for (int idx = tid; idx < (r1 - r0) * kRLW; idx += NT) {
+                const int r = r0 + idx / kRLW, i = idx % kRLW;
+                uint32_t* kp = sKeyRL + (buf * kBR + r) * kRLW + i;
+                const uint32_t key = *kp;
+                *kp = 0xFFFFFFFFu;
+                const int oy = oy0 + r, x = xr0 + i, y = y0 + oy;
+                if (key != 0xFFFFFFFFu && oy >= 0 && oy < rows_here && x >= 0 && x < a.W)
+                    atomicMin(&a.rl_keys[(size_t)y * a.W + x], key);
             }
         }
     };
@@ -409,11 +482,13 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
             dev::tma_load_4d(sM + s * (kStageM / 8), tmM, 0, j0, 0, ye0 + (b + 2) * kBR, &bars[s]);
         }
         flush(b & 1, kBR * b - kRB, b == 0 ? kRB : 0, kBR);
+        flush_rl(b & 1, kBR * b - kRB, b == 0 ? kRB : 0, kBR);
     }
     // the window ending at the last staged row: output kBR * nb - 5, buffer nb & 1, slot 0
     if (warp_active) emit(nb & 1, 0, kBR * nb - kRB);
     __syncthreads();
     flush(nb & 1, kBR * nb - kRB, 0, 1);
+    flush_rl(nb & 1, kBR * nb - kRB, 0, 1);
 
     if (t.nbz == 1) return TileResult{true, false};
     if (!a.merge_last) return TileResult{false, false};
@@ -451,17 +526,19 @@ struct Smem {
     uint32_t* sKey;   // [2][kGroups][kBR][kTWV]
     uint64_t* bars;   // [2]
     int* sflag;       // [4]
+    uint32_t* sKeyRL; // [2][kBR][kRLW] (kernels with the fused right-to-left keys only)
     __device__ explicit Smem(unsigned char* raw)
         : sB(reinterpret_cast<uint64_t*>(raw)),
           sM(reinterpret_cast<uint64_t*>(raw + 2 * kStageB)),
           sKey(reinterpret_cast<uint32_t*>(raw + 2 * (kStageB + kStageM))),
           bars(reinterpret_cast<uint64_t*>(raw + 2 * (kStageB + kStageM) + size_t(2) * kGroups * kBR * kTWV * 4)),
-          sflag(reinterpret_cast<int*>(bars + 2)) {}
+          sflag(reinterpret_cast<int*>(bars + 2)),
+          sKeyRL(reinterpret_cast<uint32_t*>(raw + rl_offset())) {}
 };
 
 // Runs one tile. The mbarriers must be initialised; par[s] counts the phases
 // stage s has completed so far in this CTA and is advanced here.
-template <int DIR, int DPW, bool CURVE = false>
+template <int DIR, int DPW, bool CURVE = false, bool RL = false>
 __device__ TileResult run_tile(const CUtensorMap* tmB, const CUtensorMap* tmM, const MatchArgs& a, const Tile& t,
                                const Smem& sm, uint32_t* par) {
     const int tid = threadIdx.x;
@@ -483,6 +560,8 @@ __device__ TileResult run_tile(const CUtensorMap* tmB, const CUtensorMap* tmM, c
         sm.sflag[0] = 0;
     }
     for (int i = tid; i < 2 * kGroups * kBR * kTWV; i += Var<DPW>::kNT) sm.sKey[i] = 0xFFFFFFFFu;
+    if constexpr (RL)
+        for (int i = tid; i < 2 * kBR * kRLW; i += Var<DPW>::kNT) sm.sKeyRL[i] = 0xFFFFFFFFu;
     __syncthreads();
     if (tid == 0) {
         for (int b = 0; b < 2 && b < nb; ++b) {
@@ -493,10 +572,10 @@ __device__ TileResult run_tile(const CUtensorMap* tmB, const CUtensorMap* tmM, c
         }
     }
     const TileResult res =
-        interior ? match_body<DIR, false, DPW, CURVE>(tmB, tmM, a, t, sm.sB, sm.sM, sm.sKey, sm.bars, sm.sflag, par,
-                                                      nb, rows_here, xs, y0, ye0, dz0, ms)
-                 : match_body<DIR, true, DPW, CURVE>(tmB, tmM, a, t, sm.sB, sm.sM, sm.sKey, sm.bars, sm.sflag, par,
-                                                     nb, rows_here, xs, y0, ye0, dz0, ms);
+        interior ? match_body<DIR, false, DPW, CURVE, RL>(tmB, tmM, a, t, sm.sB, sm.sM, sm.sKey, sm.bars, sm.sflag,
+                                                          par, nb, rows_here, xs, y0, ye0, dz0, ms, sm.sKeyRL)
+                 : match_body<DIR, true, DPW, CURVE, RL>(tmB, tmM, a, t, sm.sB, sm.sM, sm.sKey, sm.bars, sm.sflag,
+                                                         par, nb, rows_here, xs, y0, ye0, dz0, ms, sm.sKeyRL);
     par[0] += (nb + 1) / 2;
     par[1] += nb / 2;
     __syncthreads();  // the next tile reuses the shared memory
@@ -512,7 +591,7 @@ __device__ __forceinline__ void init_barriers(const Smem& sm) {
     __syncthreads();
 }
 
-template <int DIR, int DPW, bool CURVE = false>
+template <int DIR, int DPW, bool CURVE = false, bool RL = false>
 __global__ void __launch_bounds__(Var<DPW>::kNT, 1)
     census_match_kernel(const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmM,
                         MatchArgs a) {
@@ -530,7 +609,21 @@ __global__ void __launch_bounds__(Var<DPW>::kNT, 1)
     asm volatile("griddepcontrol.wait;" ::: "memory");
     uint32_t par[2] = {0, 0};
     const Tile t{int(blockIdx.x), int(blockIdx.y), int(blockIdx.z), int(gridDim.x), int(gridDim.z)};
-    run_tile<DIR, DPW, CURVE>(&tmB, &tmM, a, t, sm, par);
+    run_tile<DIR, DPW, CURVE, RL>(&tmB, &tmM, a, t, sm, par);
+}
+
+// Turns the fused right-to-left keys into the right-view map and resets
+// them (the disparity in a key is absolute).
+static __global__ void rl_finalize_kernel(uint32_t* keys, int W, int H, int r, void* out, size_t out_pitch,
+                                          int out_type) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= W) return;
+    uint32_t* kp = &keys[(size_t)y * W + x];
+    const uint32_t key = *kp;
+    *kp = 0xFFFFFFFFu;
+    const bool valid = x >= r && x < W - r && y >= r && y < H - r;
+    store_disp(out, out_pitch, out_type, x, y, valid, key, 0);
 }
 
 // Converts merged keys to disparities and resets the keys for the next call.
@@ -597,6 +690,13 @@ inline cudaError_t prepare_census_match() {
         const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
     }
+    const void* fused[] = {reinterpret_cast<const void*>(census_match_kernel<0, 4, false, true>),
+                           reinterpret_cast<const void*>(census_match_kernel<0, 8, false, true>)};
+    for (const void* k : fused) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_bytes_rl()));
+        if (e != cudaSuccess) return e;
+    }
     return cudaSuccess;
 }
 
@@ -618,7 +718,11 @@ inline cudaError_t launch_census_match(const CUtensorMap& tb, const CUtensorMap&
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     cudaError_t e;
-    if (a.curve)
+    if (DIR == 0 && a.rl_keys) {
+        cfg.dynamicSmemBytes = smem_bytes_rl();
+        e = dpw == 8 ? cudaLaunchKernelEx(&cfg, census_match_kernel<0, 8, false, true>, tb, tm, a)
+                     : cudaLaunchKernelEx(&cfg, census_match_kernel<0, 4, false, true>, tb, tm, a);
+    } else if (a.curve)
         e = dpw == 8 ? cudaLaunchKernelEx(&cfg, census_match_kernel<DIR, 8, true>, tb, tm, a)
                      : cudaLaunchKernelEx(&cfg, census_match_kernel<DIR, 4, true>, tb, tm, a);
     else
