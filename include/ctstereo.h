@@ -217,6 +217,13 @@ int ct_bm_census_tuning(ct_handle* h, int32_t* strip_height, int32_t* disp_per_w
  * strip_height + 4 a multiple of 5 (11..511), disp_per_warp 4 or 8. Results do
  * not depend on it. */
 int ct_bm_census_set_tuning(ct_handle* h, int32_t strip_height, int32_t disp_per_warp);
+/* ct_bm_census_process_lr computes both directions in one matching pass by
+ * default: the 5x5 Hamming cost of right pixel x_R at disparity e is the
+ * left-to-right cost of left pixel x_R + e at e (the same two windows), so
+ * the left-to-right pass also decides the right-to-left winners. enable = 0
+ * selects two passes (one per direction, as the reference runs them); the
+ * maps are identical either way. */
+int ct_bm_census_set_fused_lr(ct_handle* h, int32_t enable);
 
 /* Census matching that allocates nothing. No counterpart in the reference:
  * it exists for callers that cannot call cudaMalloc (a stream being captured

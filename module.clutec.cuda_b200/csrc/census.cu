@@ -488,6 +488,15 @@ int ct_bm_census_tuning(ct_handle* hh, int32_t* strip_height, int32_t* disp_per_
     return CT_OK;
 }
 
+int ct_bm_census_set_fused_lr(ct_handle* hh, int32_t enable) {
+    clear_error();
+    auto* h = as<BmCensusHandle>(hh, Kind::BmCensus);
+    if (!h) return fail(CT_ESTATE, "not a census matcher handle");
+    if (enable != 0 && enable != 1) return fail(CT_EINVAL, "enable must be 0 or 1");
+    h->fuse_rl = enable;
+    return CT_OK;
+}
+
 int ct_bm_census_set_tuning(ct_handle* hh, int32_t strip_height, int32_t disp_per_warp) {
     clear_error();
     auto* h = as<BmCensusHandle>(hh, Kind::BmCensus);

@@ -163,6 +163,7 @@ def _declare(L: C.CDLL) -> None:
         "ct_bm_census_autotune": [H, img, img, C.c_void_p],
         "ct_bm_census_tuning": [H, P(C.c_int32), P(C.c_int32)],
         "ct_bm_census_set_tuning": [H, C.c_int32, C.c_int32],
+        "ct_bm_census_set_fused_lr": [H, C.c_int32],
         "ct_bm_census_process_static": [img, img, img, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p],
         "ct_bm_census_static_status": [P(C.c_int32)],
         "ct_bm_set_gradient_gate": [H, C.c_float],
@@ -364,6 +365,10 @@ class BlockMatcherCensus(_Driver):
 
     def set_tuning(self, strip_height: int, disp_per_warp: int):
         check(lib().ct_bm_census_set_tuning(self._h, strip_height, disp_per_warp))
+
+    def set_fused_lr(self, enable: bool):
+        """process_lr in one matching pass (default) or two (one per direction); same maps."""
+        check(lib().ct_bm_census_set_fused_lr(self._h, 1 if enable else 0))
 
     def tuning(self):
         th, dpw = C.c_int32(), C.c_int32()

@@ -195,3 +195,41 @@ def test_autotune_keeps_results(ct, oracle, cuda):
     np.testing.assert_array_equal(out.cpu().numpy(), oracle.to_u8(want))
     with pytest.raises(ct.CtError):
         m.set_tuning(12, 4)
+
+
+@pytest.mark.parametrize("W,H,D,dmin,kind,dtype", [
+    (67, 43, 40, 0, 1, torch.int16),     # one column tile, D below one disparity block
+    (400, 150, 96, 0, 2, torch.int16),   # D split over two blocks (last-arriver merge)
+    (333, 111, 128, 5, 1, torch.int16),  # odd minimum disparity (relative d = 0 excluded)
+    (515, 97, 200, 2, 2, torch.uint8),   # ragged D and width, U8 maps
+    (1280, 720, 256, 0, 2, torch.int16),
+])
+def test_process_lr_fused_equals_two_passes(ct, oracle, cuda, W, H, D, dmin, kind, dtype):
+    """ct_bm_census_process_lr decides both directions in one pass (the right
+    view's winners from the left-to-right costs); its three maps equal the
+    two-pass result and, where the oracle is quick, the oracle's."""
+    L, R = pair(ct, kind, 1000 + W, W, H, dmin + D - 1)
+    m = ct.BlockMatcherCensus()
+    m.configure(0, W, H, D, disp_min=dmin)
+    dl, dr = to_dev(L, cuda), to_dev(R, cuda)
+    maps = {}
+    for fused in (True, False):
+        m.set_fused_lr(fused)
+        out = [ct.alloc_image(H, W, dtype, cuda) for _ in range(3)]
+        for o in out:
+            o.fill_(0x5A5A if dtype == torch.int16 else 0x5A)
+        m.process_lr(dl, dr, disp_lr=out[0], disp_rl=out[1], disp_checked=out[2], tol=1)
+        torch.cuda.synchronize()
+        assert m.device_status() == 0
+        maps[fused] = [o.cpu().numpy() for o in out]
+    for a, b, name in zip(maps[True], maps[False], ("lr", "rl", "checked")):
+        np.testing.assert_array_equal(a, b, err_msg=name)
+    if W * H * D <= 400 * 150 * 128:
+        wl, _ = oracle.match_census(L, R, D, 2, True, dmin=dmin)
+        wr, _ = oracle.match_census(L, R, D, 2, False, dmin=dmin)
+        wc, _ = oracle.crosscheck(wl, wr, 1, True)
+        enc = (lambda v: oracle.to_u16(v)) if dtype == torch.int16 else (
+            lambda v: oracle.to_u8(np.where(v == -2, -1, v)))
+        for got, want, name in zip(maps[True], (wl, wr, wc), ("lr", "rl", "checked")):
+            view = got.view(np.uint16) if dtype == torch.int16 else got
+            np.testing.assert_array_equal(view, enc(want), err_msg=name)
