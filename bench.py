@@ -63,7 +63,8 @@ def parse():
     ap.add_argument("--eval-pairs", type=int, default=None,
                     help="held-out 1080p pairs for the confidence-net AUC (default 4 in the census line, 24 in confnet1080)")
     ap.add_argument("--profile", default=None,
-                    choices=["census_match", "confnet_infer", "pipelines", "sad640", "ncc1080", "aw1440", "batch64",
+                    choices=["census_match", "census_fused", "confnet_infer", "pipelines", "sad640", "ncc1080",
+                             "aw1440", "batch64",
                              "compat_ncc1080"],
                     help="for ncu captures, then exit: census_match or confnet_infer = that kernel twice on the "
                          "1080p D=128 pair; pipelines = the plain L-R pipeline 3x, then the learned one 3x; a "
@@ -666,7 +667,7 @@ def run_profile(args):
     the two pipelines, three times each, or a configuration's step twice)."""
     import torch
     import ctstereo as ct
-    if args.profile not in ("census_match", "confnet_infer", "pipelines"):
+    if args.profile not in ("census_match", "census_fused", "confnet_infer", "pipelines"):
         return profile_config(args)
     dev = torch.device("cuda", 0)
     if args.profile in ("confnet_infer", "pipelines"):
@@ -715,8 +716,13 @@ def run_profile(args):
     m = ct.BlockMatcherCensus()
     m.configure(0, W_, H_, D_)
     out = ct.alloc_image(H_, W_, torch.uint8, dev)
-    for _ in range(2):
-        m.match_desc(out, desc_l, desc_r, True)
+    if args.profile == "census_fused":  # process_lr with both maps: census x2, the fused pass, finalize
+        rl = ct.alloc_image(H_, W_, torch.uint8, dev)
+        for _ in range(2):
+            m.process_lr(dL, dR, disp_lr=out, disp_rl=rl)
+    else:
+        for _ in range(2):
+            m.match_desc(out, desc_l, desc_r, True)
     torch.cuda.synchronize()
     if m.device_status() != 0:
         raise RuntimeError("device status set")
