@@ -127,7 +127,8 @@ struct BmCensusHandle : ct_handle {
     size_t desc_pitch = 0;         // elements
     uint32_t* keys = nullptr;      // ceil(D/64) planes of W*H merge keys
     uint32_t* counters = nullptr;  // one per (strip, column tile); 0 between calls
-    uint32_t* rl_keys = nullptr;   // W*H right-view keys of the fused pass; 0xFFFFFFFF between calls
+    uint32_t* rl_keys = nullptr;   // right-view keys of the fused pass, rows of cm::rl_pitch_words(W)
+    int rl_next_tag = cm::kRLTags - 1;  // tag of the next fused pass; < 0: reset the plane first
     int fuse_rl = 1;               // process_lr: right-to-left winners from the left-to-right pass
     uint16_t* tmp_lr = nullptr;    // U16 maps for process_lr when the caller wants only one
     uint16_t* tmp_rl = nullptr;
@@ -149,9 +150,11 @@ H* as(ct_handle* h, Kind k) {
     return (h && h->kind == k) ? static_cast<H*>(h) : nullptr;
 }
 
+// rl_tag >= 0: the left-to-right pass also bids for the right view into
+// h->rl_keys with that tag (the fused kernel).
 int census_match_pass_maps(BmCensusHandle* h, int dir, const ct_image* disp, const CUtensorMap& tb,
                            const CUtensorMap& tm, cudaStream_t s, const ct_curves* curves = nullptr,
-                           const ct_image* disp_rl = nullptr) {
+                           int rl_tag = -1) {
     using namespace cm;
     MatchArgs a{};
     a.W = h->fmt.width; a.H = h->fmt.height;
@@ -171,15 +174,57 @@ int census_match_pass_maps(BmCensusHandle* h, int dir, const ct_image* disp, con
         a.curve_pitch = curves->pitch_bytes / 4;
         a.curve_groups = (a.D + 3) / 4;
     }
-    if (disp_rl) a.rl_keys = h->rl_keys;  // left-to-right pass bidding for the right view too
+    if (rl_tag >= 0) {  // left-to-right pass bidding for the right view too
+        a.rl_keys = h->rl_keys;
+        a.rl_pitch = rl_pitch_words(a.W);
+        a.rl_tag = uint32_t(rl_tag) << kRLTagShift;
+    }
     const cudaError_t e = dir == 0 ? launch_census_match<0>(tb, tm, a, s, h->dpw)
                                    : launch_census_match<1>(tb, tm, a, s, h->dpw);
     if (e != cudaSuccess) return fail(CT_ECUDA, "census match launch failed: %s", cudaGetErrorString(e));
-    if (disp_rl) {
-        rl_finalize_kernel<<<dim3((a.W + 255) / 256, a.H), 256, 0, s>>>(h->rl_keys, a.W, a.H, kAR, disp_rl->ptr,
-                                                                        disp_rl->pitch_bytes, disp_rl->type);
-        CT_LAUNCH_CHECK();
+    return CT_OK;
+}
+
+// process_lr in one matching pass: the left-to-right kernel decides both
+// directions' winners (the left map into lr, the right view's as tagged keys),
+// then one kernel writes the right-view map (disp_rl, when asked for) and the
+// cross-check of lr against the keys (disp_checked, when asked for).
+int census_process_fused(BmCensusHandle* h, const ct_image* lr, const ct_image* disp_rl,
+                         const ct_image* disp_checked, int tol, cudaStream_t s) {
+    using namespace cm;
+    const int W = h->fmt.width, H = h->fmt.height;
+    const size_t kpitch = rl_pitch_words(W);
+    if (h->rl_next_tag < 0) {  // every tag used since the plane was last set: set it again
+        CT_CUDA_TRY(cudaMemsetAsync(h->rl_keys, 0xFF, kpitch * H * 4, s));
+        h->rl_next_tag = kRLTags - 1;
     }
+    const int tag_no = h->rl_next_tag--;
+    if (int rc = census_match_pass_maps(h, 0, lr, h->tm_lb, h->tm_rm, s, nullptr, tag_no)) return rc;
+    const uint32_t tag = uint32_t(tag_no) << kRLTagShift;
+    const int type = lr->type;
+    const int px = 16 / int(pix_size(type));
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((W + 128 * px - 1) / (128 * px), H);
+    cfg.blockDim = dim3(128);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    void* rl_ptr = disp_rl ? disp_rl->ptr : nullptr;
+    const size_t rl_pb = disp_rl ? disp_rl->pitch_bytes : 0;
+    void* ck_ptr = disp_checked ? disp_checked->ptr : nullptr;
+    const size_t ck_pb = disp_checked ? disp_checked->pitch_bytes : 0;
+    if (type == CT_PIX_U8)
+        CT_CUDA_TRY(cudaLaunchKernelEx(&cfg, rl_check_kernel<uint8_t>, h->rl_keys, kpitch, tag, W, H, int(kAR),
+                                       static_cast<uint8_t*>(rl_ptr), rl_pb, static_cast<const uint8_t*>(lr->ptr),
+                                       lr->pitch_bytes, static_cast<uint8_t*>(ck_ptr), ck_pb, tol));
+    else
+        CT_CUDA_TRY(cudaLaunchKernelEx(&cfg, rl_check_kernel<uint16_t>, h->rl_keys, kpitch, tag, W, H, int(kAR),
+                                       static_cast<uint16_t*>(rl_ptr), rl_pb, static_cast<const uint16_t*>(lr->ptr),
+                                       lr->pitch_bytes, static_cast<uint16_t*>(ck_ptr), ck_pb, tol));
+    CT_LAUNCH_CHECK();
     return CT_OK;
 }
 
@@ -312,8 +357,10 @@ int ct_bm_census_configure(ct_handle* hh, int32_t device, const ct_format* fmt, 
     h->tmp_pitch = ((size_t)W * 2 + 255) / 256 * 256;
     if (cudaMalloc(&h->tmp_lr, h->tmp_pitch * H) != cudaSuccess) return fail(CT_ENOMEM, "map scratch");
     if (cudaMalloc(&h->tmp_rl, h->tmp_pitch * H) != cudaSuccess) return fail(CT_ENOMEM, "map scratch");
-    if (cudaMalloc(&h->rl_keys, W * H * 4) != cudaSuccess) return fail(CT_ENOMEM, "right-view key scratch");
-    CT_CUDA_TRY(cudaMemset(h->rl_keys, 0xFF, W * H * 4));
+    const size_t rl_bytes = cm::rl_pitch_words(W) * H * 4;
+    if (cudaMalloc(&h->rl_keys, rl_bytes) != cudaSuccess) return fail(CT_ENOMEM, "right-view key scratch");
+    CT_CUDA_TRY(cudaMemset(h->rl_keys, 0xFF, rl_bytes));
+    h->rl_next_tag = cm::kRLTags - 1;
     h->fmt = *fmt;  // left_desc() / right_desc() below depend on the height
     h->th = cm::pick_strip_height(W, H, p->disp_count, sm_count(device));
     CT_CUDA_TRY(cm::prepare_census_match());
@@ -414,11 +461,9 @@ int ct_bm_census_process_lr(ct_handle* hh, const ct_image* disp_lr, const ct_ima
     const ct_image* lr = disp_lr ? disp_lr : &tlr;
     const ct_image* rl = disp_rl ? disp_rl : &trl;
     const bool need_lr = disp_lr || disp_checked, need_rl = disp_rl || disp_checked;
-    if (need_lr && need_rl && h->fuse_rl) {
-        // one pass: the left-to-right costs also decide the right-to-left
-        // winners (the same windows; same maps as two passes)
-        if (int rc = census_match_pass_maps(h, 0, lr, h->tm_lb, h->tm_rm, s, nullptr, rl)) return rc;
-    } else {
+    if (need_lr && need_rl && h->fuse_rl)  // the same maps as two passes
+        return census_process_fused(h, lr, disp_rl, disp_checked, tol, s);
+    {
         if (need_lr)
             if (int rc = census_match_pass(h, 0, lr, s)) return rc;
         if (need_rl)

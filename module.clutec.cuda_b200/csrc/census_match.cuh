@@ -117,13 +117,24 @@ struct MatchArgs {
     size_t curve_pitch;  // 32-bit words per row, a multiple of 4
     int curve_groups;    // ceil(D / 4)
     // Fused right-to-left winner (left-to-right kernels instantiated with
-    // RL = true): one key per right-view pixel, W * H, 0xFFFFFFFF between
-    // calls (rl_finalize_kernel resets it). The 5x5 Hamming cost of right
-    // pixel x_R at disparity e equals the left-to-right cost of left pixel
-    // x_R + e at e (the same two windows), so every cost this pass computes
-    // also bids for the right view: key (C << 16) | e, e = dmin + d absolute.
+    // RL = true): one key per right-view pixel, row y at rl_keys + y *
+    // rl_pitch. The 5x5 Hamming cost of right pixel x_R at disparity e equals
+    // the left-to-right cost of left pixel x_R + e at e (the same two
+    // windows), so every cost this pass computes also bids for the right
+    // view: key rl_tag | (C << 16) | e, e = dmin + d absolute, C < 2047.
+    // rl_tag (bits 27..31) is one less on every call, so this call's bids are
+    // below every key an earlier call left and the plane needs no reset pass
+    // (rl_check_kernel ignores keys of another tag; the plane is set to
+    // 0xFFFFFFFF again when the tag wraps).
     uint32_t* rl_keys;
+    size_t rl_pitch;     // words, a multiple of 4
+    uint32_t rl_tag;     // tag << 27
 };
+
+// Right-view key plane pitch for width W (words): rows 16-byte aligned.
+__host__ __device__ constexpr size_t rl_pitch_words(int W) { return (size_t(W) + 3) / 4 * 4; }
+constexpr int kRLTagShift = 27;
+constexpr int kRLTags = 32;  // tags 31 .. 0, then the plane is reset
 
 // Curve word pitch for width W: words 0 .. W + 1 used, rounded up to 64
 // words (256 bytes) so every row starts 16-byte aligned.
@@ -435,8 +446,8 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
                 const uint32_t key = *kp;
                 *kp = 0xFFFFFFFFu;
                 const int oy = oy0 + r, x = xr0 + i, y = y0 + oy;
-                if (key != 0xFFFFFFFFu && oy >= 0 && oy < rows_here && x >= 0 && x < a.W)
-                    atomicMin(&a.rl_keys[(size_t)y * a.W + x], key);
+                if ((key >> 16) < 2047u && oy >= 0 && oy < rows_here && x >= 0 && x < a.W)
+                    atomicMin(&a.rl_keys[(size_t)y * a.rl_pitch + x], key | a.rl_tag);
             }
         }
     };
@@ -612,18 +623,101 @@ __global__ void __launch_bounds__(Var<DPW>::kNT, 1)
     run_tile<DIR, DPW, CURVE, RL>(&tmB, &tmM, a, t, sm, par);
 }
 
-// Turns the fused right-to-left keys into the right-view map and resets
-// them (the disparity in a key is absolute).
-static __global__ void rl_finalize_kernel(uint32_t* keys, int W, int H, int r, void* out, size_t out_pitch,
-                                          int out_type) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+// Map code of a right-view key of the fused pass (what store_disp writes
+// for it): a disparity iff the key carries this call's tag, a cost below
+// 2047 and the pixel is inside the border.
+template <typename T>
+__device__ __forceinline__ T rl_code(uint32_t key, uint32_t tag, bool inside) {
+    const bool ok = inside && (key & (0x1Fu << kRLTagShift)) == tag && ((key >> 16) & 0x7FFu) < 2047u;
+    const uint32_t d = key & 0xFFFFu;
+    if constexpr (sizeof(T) == 1) return ok ? T(d) : T(0xFF);
+    else return ok ? T(d + 1) : T(0xFFFF);
+}
+// Disparity of a map code (the cross-check's reading: U8 0xFF and U16
+// codes outside CT_DISP_FIRST .. CT_DISP_LAST are not disparities).
+template <typename T>
+__device__ __forceinline__ bool map_disp(T v, int& d) {
+    if constexpr (sizeof(T) == 1) {
+        d = v;
+        return v != 0xFF;
+    } else {
+        d = int(v) - 1;
+        return v >= CT_DISP_FIRST && v <= CT_DISP_LAST;
+    }
+}
+
+// After the fused pass, one thread per 16 bytes of a map row (16 U8 or 8 U16
+// pixels): writes the right-view map from the keys of this call (rl_out, when
+// given) and the left-to-right cross-check of the left map lr (ck_out, when
+// given): a left disparity d at x is kept iff the right view's winner at
+// x - d is a disparity within tol of d (the reading of crosscheck_kernel on
+// the right-view map, from the keys directly). The keys stay in place.
+template <typename T>
+__global__ void __launch_bounds__(128) rl_check_kernel(const uint32_t* keys, size_t kpitch, uint32_t tag, int W,
+                                                       int H, int r, T* rl_out, size_t rl_pitch_b, const T* lr,
+                                                       size_t lr_pitch_b, T* ck_out, size_t ck_pitch_b, int tol) {
+    constexpr int PX = 16 / sizeof(T);
+    // launched with programmatic stream serialisation after the matcher
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * PX;
     const int y = blockIdx.y;
-    if (x >= W) return;
-    uint32_t* kp = &keys[(size_t)y * W + x];
-    const uint32_t key = *kp;
-    *kp = 0xFFFFFFFFu;
-    const bool valid = x >= r && x < W - r && y >= r && y < H - r;
-    store_disp(out, out_pitch, out_type, x, y, valid, key, 0);
+    if (x0 >= W) return;
+    const uint32_t* krow = keys + (size_t)y * kpitch;
+    const bool yin = y >= r && y < H - r;
+    const bool full = x0 + PX <= W;  // map rows are 16-byte aligned, x0 a multiple of PX
+    union Px {
+        uint4 q;
+        T v[PX];
+    };
+    if (rl_out) {
+        T* orow = reinterpret_cast<T*>(reinterpret_cast<char*>(rl_out) + (size_t)y * rl_pitch_b);
+        Px o;
+#pragma unroll
+        for (int q = 0; q < PX / 4; ++q) {
+            // key rows are 16-byte aligned with a multiple of 4 words
+            uint4 k4 = make_uint4(~0u, ~0u, ~0u, ~0u);
+            if (x0 + 4 * q < W) k4 = *reinterpret_cast<const uint4*>(krow + x0 + 4 * q);
+            const uint32_t kk[4] = {k4.x, k4.y, k4.z, k4.w};
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int x = x0 + 4 * q + i;
+                o.v[4 * q + i] = rl_code<T>(kk[i], tag, yin && x >= r && x < W - r);
+            }
+        }
+        if (full) *reinterpret_cast<uint4*>(orow + x0) = o.q;
+        else
+            for (int i = 0; i < PX; ++i)
+                if (x0 + i < W) orow[x0 + i] = o.v[i];
+    }
+    if (ck_out) {
+        const T* brow = reinterpret_cast<const T*>(reinterpret_cast<const char*>(lr) + (size_t)y * lr_pitch_b);
+        T* crow = reinterpret_cast<T*>(reinterpret_cast<char*>(ck_out) + (size_t)y * ck_pitch_b);
+        Px in, res;
+        if (full) in.q = *reinterpret_cast<const uint4*>(brow + x0);
+        else
+            for (int i = 0; i < PX; ++i) in.v[i] = x0 + i < W ? brow[x0 + i] : T(0);
+#pragma unroll
+        for (int i = 0; i < PX; ++i) {
+            const int x = x0 + i;
+            const T v = in.v[i];
+            T out = v;
+            int d;
+            if (map_disp<T>(v, d)) {
+                const int xo = x - d;
+                out = sizeof(T) == 1 ? T(0xFF) : T(CT_DISP_INCONSISTENT);
+                if (xo >= 0 && xo < W) {
+                    const T vo = rl_code<T>(__ldg(krow + xo), tag, yin && xo >= r && xo < W - r);
+                    int dd;
+                    if (map_disp<T>(vo, dd) && abs(dd - d) <= tol) out = v;
+                }
+            }
+            res.v[i] = out;
+        }
+        if (full) *reinterpret_cast<uint4*>(crow + x0) = res.q;
+        else
+            for (int i = 0; i < PX; ++i)
+                if (x0 + i < W) crow[x0 + i] = res.v[i];
+    }
 }
 
 // Converts merged keys to disparities and resets the keys for the next call.

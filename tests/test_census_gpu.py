@@ -233,3 +233,44 @@ def test_process_lr_fused_equals_two_passes(ct, oracle, cuda, W, H, D, dmin, kin
         for got, want, name in zip(maps[True], (wl, wr, wc), ("lr", "rl", "checked")):
             view = got.view(np.uint16) if dtype == torch.int16 else got
             np.testing.assert_array_equal(view, enc(want), err_msg=name)
+
+
+@pytest.mark.parametrize("dtype", [torch.uint8, torch.int16])
+def test_process_lr_fused_many_calls(ct, cuda, dtype):
+    """The fused pass keeps the right view's keys between calls and tells this
+    call's apart by a tag that wraps every 32 calls. Over 70 calls that
+    alternate two pairs (with different disparity ranges, so a stale key
+    would change a map) and the subsets of outputs, every map equals the
+    two-pass one."""
+    W, H, D = 300, 70, 64
+    pairs = [pair(ct, 1, 31, W, H, D - 1), pair(ct, 2, 32, W, H, 20)]
+    m = ct.BlockMatcherCensus()
+    m.configure(0, W, H, D)
+    dev = [(to_dev(L, cuda), to_dev(R, cuda)) for L, R in pairs]
+    want = []
+    m.set_fused_lr(False)
+    for dl, dr in dev:
+        out = [ct.alloc_image(H, W, dtype, cuda) for _ in range(3)]
+        m.process_lr(dl, dr, disp_lr=out[0], disp_rl=out[1], disp_checked=out[2], tol=1)
+        want.append([o.cpu().numpy() for o in out])
+    m.set_fused_lr(True)
+    out = [ct.alloc_image(H, W, dtype, cuda) for _ in range(3)]
+    for call in range(70):
+        k = call % 2
+        dl, dr = dev[k]
+        for o in out:
+            o.fill_(0x1234 if dtype == torch.int16 else 0x5A)
+        mode = (call // 2) % 3
+        if mode == 0:
+            m.process_lr(dl, dr, disp_lr=out[0], disp_rl=out[1], disp_checked=out[2], tol=1)
+            check = (0, 1, 2)
+        elif mode == 1:
+            m.process_lr(dl, dr, disp_rl=out[1], disp_checked=out[2], tol=1)
+            check = (1, 2)
+        else:
+            m.process_lr(dl, dr, disp_lr=out[0], disp_rl=out[1])
+            check = (0, 1)
+        torch.cuda.synchronize()
+        for i in check:
+            np.testing.assert_array_equal(out[i].cpu().numpy(), want[k][i], err_msg=f"call {call} map {i}")
+    assert m.device_status() == 0
