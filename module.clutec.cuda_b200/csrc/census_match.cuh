@@ -148,7 +148,14 @@ __host__ __device__ constexpr size_t smem_bytes() {
 }
 // The fused right-to-left keys: 2 buffers x kBR rows x kRLW right-view
 // columns (V columns minus the 64 disparities of the CTA), after the rest.
+// Right-view index i of a row lives at word (i & 3) * kRLQ + (i >> 2): a
+// thread's bids for one anti-diagonal are at i = 4 * lane + const, so the 32
+// lanes' shared atomics hit 32 consecutive words (with i itself as the word
+// index they would be 4-way bank conflicts).
 constexpr int kRLW = kTWV + kDPC;  // 192 (191 used)
+constexpr int kRLQ = kRLW / 4;
+static_assert(kRLW % 4 == 0 && (kDPC - 1) % 4 == 3, "right-view key interleave");
+__host__ __device__ constexpr int rl_word(int i) { return (i & 3) * kRLQ + (i >> 2); }
 __host__ __device__ constexpr size_t rl_offset() { return (smem_bytes() + 127) / 128 * 128; }
 __host__ __device__ constexpr size_t smem_bytes_rl() { return rl_offset() + size_t(2) * kBR * kRLW * 4; }
 
@@ -188,6 +195,7 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
                                                  int nb, int rows_here, int xs, int y0, int ye0, int dz0, int ms,
                                                  uint32_t* sKeyRL = nullptr) {
     static_assert(!RL || (DIR == 0 && !CURVE), "the fused right-to-left keys ride on the plain left-to-right pass");
+    static_assert(!RL || DPW % 4 == 0, "the right-view key interleave assumes warps of 4k disparities");
     using VT = Var<DPW>;
     constexpr int NP = VT::kNP, NT = VT::kNT, NWD = VT::kWords;
     constexpr uint32_t kBytes = kTxB + kTxM;
@@ -392,7 +400,10 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
             auto key = [&](int c, int j) {
                 return (j & 1) ? ((Cm[c][j >> 1] & 0xFFFF0000u) | rld[j]) : ((Cm[c][j >> 1] << 16) | rld[j]);
             };
-            uint32_t* rrow = sKeyRL + (buf * kBR + r) * kRLW + (4 * lane - (dw - dz0) + (kDPC - 1));
+            // right-view index i = 4 * lane + (kDPC - 1) - (dw - dz0) + ad;
+            // (kDPC - 1) - (dw - dz0) = 4 q + 3 (dw - dz0 a multiple of 4), so
+            // word(i) = ((3 + ad) & 3) * kRLQ + lane + q + ((3 + ad) >> 2)
+            uint32_t* rrow = sKeyRL + (buf * kBR + r) * kRLW + lane + ((kDPC - 1 - (dw - dz0)) >> 2);
 #pragma unroll
             for (int ad = -(DPW - 1); ad <= kCPT - 1; ++ad) {
                 uint32_t m = 0xFFFFFFFFu;
@@ -401,7 +412,7 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
                     const int j = c - ad;
                     if (j >= 0 && j < DPW) m = min(m, key(c, j));
                 }
-                atomicMin(&rrow[ad], m);
+                atomicMin(&rrow[((3 + ad) & 3) * kRLQ + ((3 + ad) >> 2)], m);
             }
         }
     };
@@ -442,7 +453,7 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
             const int xr0 = xs - a.dmin - dz0 - (kDPC - 1);  // right-view column of index 0
             for (int idx = tid; idx < (r1 - r0) * kRLW; idx += NT) {
                 const int r = r0 + idx / kRLW, i = idx % kRLW;
-                uint32_t* kp = sKeyRL + (buf * kBR + r) * kRLW + i;
+                uint32_t* kp = sKeyRL + (buf * kBR + r) * kRLW + rl_word(i);
                 const uint32_t key = *kp;
                 *kp = 0xFFFFFFFFu;
                 const int oy = oy0 + r, x = xr0 + i, y = y0 + oy;
