@@ -146,8 +146,10 @@ __host__ __device__ constexpr size_t curve_pitch_words(int W) { return (size_t(W
 __host__ __device__ constexpr size_t smem_bytes() {
     return size_t(2) * (kStageB + kStageM) + size_t(2) * kGroups * kBR * kTWV * 4 + 2 * 8 + 16;
 }
-// The fused right-to-left keys: 2 buffers x kBR rows x kRLW right-view
-// columns (V columns minus the 64 disparities of the CTA), after the rest.
+// The fused right-to-left keys: 2 buffers x kGroups x kBR rows x kRLW
+// right-view columns (V columns minus the 64 disparities of the CTA), after
+// the rest; one row set per group of 32 disparities, whose 16-bit keys carry
+// d & 31 (as the left-to-right key buffers).
 // Right-view index i of a row lives at word (i & 3) * kRLQ + (i >> 2): a
 // thread's bids for one anti-diagonal are at i = 4 * lane + const, so the 32
 // lanes' shared atomics hit 32 consecutive words (with i itself as the word
@@ -157,7 +159,7 @@ constexpr int kRLQ = kRLW / 4;
 static_assert(kRLW % 4 == 0 && (kDPC - 1) % 4 == 3, "right-view key interleave");
 __host__ __device__ constexpr int rl_word(int i) { return (i & 3) * kRLQ + (i >> 2); }
 __host__ __device__ constexpr size_t rl_offset() { return (smem_bytes() + 127) / 128 * 128; }
-__host__ __device__ constexpr size_t smem_bytes_rl() { return rl_offset() + size_t(2) * kBR * kRLW * 4; }
+__host__ __device__ constexpr size_t smem_bytes_rl() { return rl_offset() + size_t(2) * kGroups * kBR * kRLW * 4; }
 
 // Disparity code for an output pixel from its merged key (C << 16 | d), d
 // relative to dmin.
@@ -228,16 +230,13 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
     }
     // fused right-to-left: columns whose costs may not bid (the halo columns,
     // and columns whose window leaves the image on the right: right pixel
-    // x - e must keep x - e + e + 2 <= W - 1) get cost 0xFFFF in both halves
+    // x - e must keep x - e + e + 2 <= W - 1) get key 0xFFFF in both halves
     uint32_t rlbad[kCPT];
-    uint32_t rld[DPW];  // absolute disparity of relative d = dw + j
 #pragma unroll
     for (int c = 0; c < kCPT; ++c) {
         const int v = 4 * lane + c, x = xs + v;
         rlbad[c] = (v < kAR || v >= kAR + kTWO || x > a.W - 1 - kAR) ? 0xFFFFFFFFu : 0u;
     }
-#pragma unroll
-    for (int j = 0; j < DPW; ++j) rld[j] = uint32_t(a.dmin + dw + j);
     // First match column this thread reads per row, as an (even) offset from
     // ms: its words are the pairs (ms + mstart) / 2 + u, u < NWD / 2.
     const int mstart = DIR == 0 ? 4 * lane + kDPC - DPW - DPW * warp : 4 * lane + DPW * warp;
@@ -359,9 +358,12 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
             if (oy >= 0 && oy < rows_here) store_curve(C, oy);
         }
         uint32_t* krow = sKey + ((buf * kGroups + grp) * kBR + r) * kTWV + lane;
+        // 16-bit keys C << 5 | (d & 31) of (column c, relative disparities
+        // dw + 2p, dw + 2p + 1) in the halves of kk[c][p]
+        uint32_t kk[kCPT][NP];
 #pragma unroll
         for (int c = 0; c < kCPT; ++c) {
-            uint32_t k[NP];
+            uint32_t* k = kk[c];
 #pragma unroll
             for (int p = 0; p < NP; ++p) {
                 k[p] = (C[c][p] << 5) + dconst[p];
@@ -370,6 +372,9 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
                     k[p] |= (dlo > lim[c] || dlo < a.dfirst ? 0x0000FFFFu : 0u) |
                             (dlo + 1 > lim[c] ? 0xFFFF0000u : 0u);
                 }
+                // columns that may not bid for the right view (not outputs of
+                // this pass either, so their left-to-right keys do not matter)
+                if constexpr (RL) k[p] |= rlbad[c];
             }
             uint32_t m;
             if (NP == 4) {
@@ -382,37 +387,41 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
             atomicMin(&krow[c * 32], m);
         }
         if constexpr (RL) {
-            // cost of (column c, relative disparity dw + j) bids for right
+            // Cost of (column c, relative disparity dw + j) bids for right
             // pixel index c - j + base: min along each anti-diagonal
-            // a = c - j, one shared atomic each
-            uint32_t Cm[kCPT][NP];
+            // ad = c - j, one shared atomic each, on the same 16-bit keys.
+            // Word kk[c][p] holds diagonals c - 2p (low half) and c - 2p - 1
+            // (high half); M[a] = min over the words with c - 2p = a, so
+            // diagonal ad = min(low half of M[ad], high half of M[ad + 1]):
+            // one shift and one packed min put it in a high half.
+            constexpr int A0 = -(DPW - 2), A1 = kCPT - 1;
+            uint32_t M[A1 - A0 + 1];
 #pragma unroll
-            for (int c = 0; c < kCPT; ++c)
+            for (int q = 0; q <= A1 - A0; ++q) {
+                bool first = true;
 #pragma unroll
-                for (int p = 0; p < NP; ++p) {
-                    Cm[c][p] = C[c][p] | rlbad[c];
-                    if (EDGE) {
-                        const int dlo = dw + 2 * p;
-                        Cm[c][p] |= (dlo > lim[c] || dlo < a.dfirst ? 0x0000FFFFu : 0u) |
-                                    (dlo + 1 > lim[c] ? 0xFFFF0000u : 0u);
-                    }
-                }
-            auto key = [&](int c, int j) {
-                return (j & 1) ? ((Cm[c][j >> 1] & 0xFFFF0000u) | rld[j]) : ((Cm[c][j >> 1] << 16) | rld[j]);
-            };
+                for (int c = 0; c < kCPT; ++c)
+#pragma unroll
+                    for (int p = 0; p < NP; ++p)
+                        if (c - 2 * p == q + A0) {
+                            M[q] = first ? kk[c][p] : dev::min_u16x2(M[q], kk[c][p]);
+                            first = false;
+                        }
+            }
             // right-view index i = 4 * lane + (kDPC - 1) - (dw - dz0) + ad;
             // (kDPC - 1) - (dw - dz0) = 4 q + 3 (dw - dz0 a multiple of 4), so
-            // word(i) = ((3 + ad) & 3) * kRLQ + lane + q + ((3 + ad) >> 2)
-            uint32_t* rrow = sKeyRL + (buf * kBR + r) * kRLW + lane + ((kDPC - 1 - (dw - dz0)) >> 2);
+            // word(i) = ((3 + ad) & 3) * kRLQ + lane + q + ((3 + ad) >> 2).
+            // Slot values: the key in the high half (the low half only
+            // orders equal keys and is never read).
+            uint32_t* rrow =
+                sKeyRL + ((buf * kGroups + grp) * kBR + r) * kRLW + lane + ((kDPC - 1 - (dw - dz0)) >> 2);
 #pragma unroll
-            for (int ad = -(DPW - 1); ad <= kCPT - 1; ++ad) {
-                uint32_t m = 0xFFFFFFFFu;
-#pragma unroll
-                for (int c = 0; c < kCPT; ++c) {
-                    const int j = c - ad;
-                    if (j >= 0 && j < DPW) m = min(m, key(c, j));
-                }
-                atomicMin(&rrow[((3 + ad) & 3) * kRLQ + ((3 + ad) >> 2)], m);
+            for (int ad = A0 - 1; ad <= A1; ++ad) {
+                uint32_t z;
+                if (ad == A0 - 1) z = M[0];
+                else if (ad == A1) z = M[A1 - A0] << 16;
+                else z = dev::min_u16x2(M[ad - A0] << 16, M[ad + 1 - A0]);
+                atomicMin(&rrow[((3 + ad) & 3) * kRLQ + ((3 + ad) >> 2)], z);
             }
         }
     };
@@ -453,12 +462,18 @@ __device__ __forceinline__ TileResult match_body(const CUtensorMap* tmB, const C
             const int xr0 = xs - a.dmin - dz0 - (kDPC - 1);  // right-view column of index 0
             for (int idx = tid; idx < (r1 - r0) * kRLW; idx += NT) {
                 const int r = r0 + idx / kRLW, i = idx % kRLW;
-                uint32_t* kp = sKeyRL + (buf * kBR + r) * kRLW + rl_word(i);
-                const uint32_t key = *kp;
-                *kp = 0xFFFFFFFFu;
+                uint32_t best = 0xFFFFFFFFu;
+#pragma unroll
+                for (int g = 0; g < kGroups; ++g) {
+                    uint32_t* kp = sKeyRL + ((buf * kGroups + g) * kBR + r) * kRLW + rl_word(i);
+                    const uint32_t k16 = *kp >> 16;
+                    *kp = 0xFFFFFFFFu;
+                    if (k16 < (2047u << 5))  // a cost below 2047
+                        best = min(best, ((k16 >> 5) << 16) | (uint32_t(a.dmin + dz0 + 32 * g) + (k16 & 31u)));
+                }
                 const int oy = oy0 + r, x = xr0 + i, y = y0 + oy;
-                if ((key >> 16) < 2047u && oy >= 0 && oy < rows_here && x >= 0 && x < a.W)
-                    atomicMin(&a.rl_keys[(size_t)y * a.rl_pitch + x], key | a.rl_tag);
+                if (best != 0xFFFFFFFFu && oy >= 0 && oy < rows_here && x >= 0 && x < a.W)
+                    atomicMin(&a.rl_keys[(size_t)y * a.rl_pitch + x], best | a.rl_tag);
             }
         }
     };
@@ -548,7 +563,7 @@ struct Smem {
     uint32_t* sKey;   // [2][kGroups][kBR][kTWV]
     uint64_t* bars;   // [2]
     int* sflag;       // [4]
-    uint32_t* sKeyRL; // [2][kBR][kRLW] (kernels with the fused right-to-left keys only)
+    uint32_t* sKeyRL; // [2][kGroups][kBR][kRLW] (kernels with the fused right-to-left keys only)
     __device__ explicit Smem(unsigned char* raw)
         : sB(reinterpret_cast<uint64_t*>(raw)),
           sM(reinterpret_cast<uint64_t*>(raw + 2 * kStageB)),
@@ -583,7 +598,7 @@ __device__ TileResult run_tile(const CUtensorMap* tmB, const CUtensorMap* tmM, c
     }
     for (int i = tid; i < 2 * kGroups * kBR * kTWV; i += Var<DPW>::kNT) sm.sKey[i] = 0xFFFFFFFFu;
     if constexpr (RL)
-        for (int i = tid; i < 2 * kBR * kRLW; i += Var<DPW>::kNT) sm.sKeyRL[i] = 0xFFFFFFFFu;
+        for (int i = tid; i < 2 * kGroups * kBR * kRLW; i += Var<DPW>::kNT) sm.sKeyRL[i] = 0xFFFFFFFFu;
     __syncthreads();
     if (tid == 0) {
         for (int b = 0; b < 2 && b < nb; ++b) {
