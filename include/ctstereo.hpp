@@ -1113,6 +1113,12 @@ public:
         Ensure(ct_bm_census_process_curves(m_pHandle, xImageDisp.C(), xCurves.C(), xImageL.C(), xImageR.C(), S()),
                "BlockMatcherCensus::ProcessCurves");
     }
+
+    /* ProcessLR in one matching pass (default) or in two, one per direction;
+     * the maps are identical. */
+    void SetFusedLR(bool bEnable) {
+        Ensure(ct_bm_census_set_fused_lr(m_pHandle, bEnable ? 1 : 0), "BlockMatcherCensus::SetFusedLR");
+    }
 };
 
 }  // namespace BlockMatcherCensus

@@ -422,6 +422,18 @@ static int RunGpu(const char* weights) {
         CHECK(differ == 0, "ProcessLR and the cross-check driver disagree on %d pixels", differ);
         CHECK(cc.DispMin() <= K && cc.DispMax() >= K, "range %d..%d", cc.DispMin(), cc.DispMax());
         m.EnsureDeviceStatus();
+        {  // two matching passes give the same three maps as the fused one
+            CDeviceSurface lr2(f16), rl2(f16), chk2(f16);
+            m.SetFusedLR(false);
+            m.ProcessLR(lr2, rl2, chk2, 1, surfL, surfR);
+            m.SetFusedLR(true);
+            int d2 = 0;
+            const auto p1 = lr.CopyInto<uint16_t>(), p2 = lr2.CopyInto<uint16_t>();
+            const auto q1 = rl.CopyInto<uint16_t>(), q2 = rl2.CopyInto<uint16_t>();
+            const auto c2 = chk2.CopyInto<uint16_t>();
+            for (size_t i = 0; i < a.size(); ++i) d2 += (p1[i] != p2[i]) + (q1[i] != q2[i]) + (a[i] != c2[i]);
+            CHECK(d2 == 0, "SetFusedLR(false): %d map pixels differ from the fused pass", d2);
+        }
 
         // the same pair as a stream of frames from host memory
         CensusStream::CDriver st;
