@@ -411,13 +411,19 @@ int ct_bm_compat_process(ct_handle* h, const ct_image* disp, const ct_image* lef
                          ct_stream stream);
 
 /* ---- cross-check: CrossCheckDisparityMaps::CDriver ------------------------
- * Replaces CrossCheckDisparityMaps.h:38-117 / .cu:63-190. For each pixel of
- * disp_base holding a disparity d: x' = x - d (left_to_right = 1) or x + d;
- * if x' is outside the image, or disp_other(x') is not a disparity, or
- * |disp_other(x') - d| > disp_delta_thresh, the result is Inconsistent;
- * otherwise d is kept. Non-disparity inputs are copied through. The min / max
- * of the kept disparities is reduced on the device (the reference does a
- * per-thread atomic range plus two blocking copies and a host reduction).
+ * Replaces CrossCheckDisparityMaps.h:38-117 / .cu:63-190, with the
+ * reference kernel's rule exactly. For each pixel of disp_base inside the
+ * 1-pixel image frame holding a disparity code v = d + First: x' = x - d
+ * (left_to_right = 1) or x + d; if x' is outside the image, or
+ * |disp_other(x') - v| > disp_delta_thresh with disp_other's code compared
+ * raw (an ID or Unknown there is compared by its value, as the reference
+ * does), the result is Inconsistent; otherwise v is kept. Non-disparity
+ * inputs are copied through. The frame pixels of result are not written, as
+ * in the reference. U8 maps (255 = not a disparity; no reference
+ * counterpart) keep d only against a disparity within the tolerance. The
+ * min / max of the kept disparities is reduced on the device (the reference
+ * does a per-thread atomic range plus two blocking copies and a host
+ * reduction).
  */
 typedef struct ct_crosscheck_params {
     int32_t disp_delta_thresh;  /* iDispDeltaThresh */

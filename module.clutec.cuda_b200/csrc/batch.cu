@@ -107,7 +107,7 @@ __device__ void crosscheck_rows(const PairDev& P, int y0, int y1, int nt) {
             if (xo >= 0 && xo < W) {
                 const uint16_t vo = __ldcg(reinterpret_cast<const uint16_t*>(
                                                reinterpret_cast<const char*>(P.map[1]) + (size_t)y * P.map_pitch) + xo);
-                keep = vo >= CT_DISP_FIRST && vo <= CT_DISP_LAST && abs(int(vo) - 1 - d) <= P.tol;
+                keep = abs(int(vo) - int(v)) <= P.tol;  // raw codes, CrossCheckDisparityMaps.cu:94
             }
         }
         char* row = static_cast<char*>(P.out) + (size_t)y * P.out_pitch;

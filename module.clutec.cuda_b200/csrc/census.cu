@@ -141,7 +141,7 @@ struct BmCensusHandle : ct_handle {
 };
 
 int crosscheck_launch(const ct_image* result, const ct_image* base, const ct_image* other, int tol, int lr,
-                      int32_t* range, cudaStream_t s);  // crosscheck.cu
+                      int frame, int32_t* range, cudaStream_t s);  // crosscheck.cu
 
 namespace {
 
@@ -469,7 +469,7 @@ int ct_bm_census_process_lr(ct_handle* hh, const ct_image* disp_lr, const ct_ima
         if (need_rl)
             if (int rc = census_match_pass(h, 1, rl, s)) return rc;
     }
-    if (disp_checked) return crosscheck_launch(disp_checked, lr, rl, tol, 1, nullptr, s);
+    if (disp_checked) return crosscheck_launch(disp_checked, lr, rl, tol, 1, /*frame*/ 0, nullptr, s);
     return CT_OK;
 }
 

@@ -675,9 +675,10 @@ __device__ __forceinline__ bool map_disp(T v, int& d) {
 // After the fused pass, one thread per 16 bytes of a map row (16 U8 or 8 U16
 // pixels): writes the right-view map from the keys of this call (rl_out, when
 // given) and the left-to-right cross-check of the left map lr (ck_out, when
-// given): a left disparity d at x is kept iff the right view's winner at
-// x - d is a disparity within tol of d (the reading of crosscheck_kernel on
-// the right-view map, from the keys directly). The keys stay in place.
+// given): a left disparity d at x is kept iff the right view's code at x - d
+// confirms it as crosscheck_kernel reads the right-view map (U16: the codes
+// within tol; U8: a disparity within tol), from the keys directly. The keys
+// stay in place.
 template <typename T>
 __global__ void __launch_bounds__(128) rl_check_kernel(const uint32_t* keys, size_t kpitch, uint32_t tag, int W,
                                                        int H, int r, T* rl_out, size_t rl_pitch_b, const T* lr,
@@ -734,7 +735,11 @@ __global__ void __launch_bounds__(128) rl_check_kernel(const uint32_t* keys, siz
                 if (xo >= 0 && xo < W) {
                     const T vo = rl_code<T>(__ldg(krow + xo), tag, yin && xo >= r && xo < W - r);
                     int dd;
-                    if (map_disp<T>(vo, dd) && abs(dd - d) <= tol) out = v;
+                    // U16: raw codes compared (CrossCheckDisparityMaps.cu:94);
+                    // U8: only a disparity confirms
+                    const bool ok = sizeof(T) == 2 ? abs(int(vo) - int(v)) <= tol
+                                                   : map_disp<T>(vo, dd) && abs(dd - d) <= tol;
+                    if (ok) out = v;
                 }
             }
             res.v[i] = out;

@@ -496,4 +496,41 @@ void or_crosscheck(const int16_t* base, const int16_t* other, int W, int H, int 
     range[0] = mn; range[1] = mx;
 }
 
+// ---------------------------------------------------------------------------
+// Cross-check on EDisparityId codes, the reference rule exactly
+// (CrossCheckDisparityMaps.cu:63-110): for a base code v in [First, Last]
+// (disparity d = v - First) at an interior pixel, x' = x - d (lr = 1) or
+// x + d; x' outside the image -> Inconsistent; else kept iff
+// |other(x', y) - v| <= tol with other's code compared raw (an ID or Unknown
+// too), otherwise Inconsistent. Other base codes are copied through.
+// frame = 1: the 1-pixel image frame is not written (out keeps its values)
+// and not counted (the kernel's IsInside(x, y, 1, 1) early return, :71);
+// frame = 0: frame pixels are processed like the rest. range[0..1] = min /
+// max of the kept codes, (Last, First) when none is kept (ResetRange and the
+// host reduction, .cu:155-186).
+// ---------------------------------------------------------------------------
+void or_crosscheck_codes(const uint16_t* base, const uint16_t* other, int W, int H, int tol, int lr, int frame,
+                         uint16_t* out, int32_t* range) {
+    constexpr int kFirst = 1, kLast = 0xFFEF, kInconsistent = 0xFFFA;
+    int32_t mn = kLast, mx = kFirst;
+    const int f = frame ? 1 : 0;
+#pragma omp parallel for schedule(static) reduction(min : mn) reduction(max : mx)
+    for (int y = f; y < H - f; ++y) {
+        for (int x = f; x < W - f; ++x) {
+            const size_t o = (size_t)y * W + x;
+            const int v = base[o];
+            if (v < kFirst || v > kLast) { out[o] = uint16_t(v); continue; }
+            const int xo = lr ? x - (v - kFirst) : x + (v - kFirst);
+            if (xo < 0 || xo >= W) { out[o] = kInconsistent; continue; }
+            if (std::abs(int(other[(size_t)y * W + xo]) - v) <= tol) {
+                out[o] = uint16_t(v);
+                mn = std::min(mn, v); mx = std::max(mx, v);
+            } else {
+                out[o] = kInconsistent;
+            }
+        }
+    }
+    range[0] = mn; range[1] = mx;
+}
+
 }  // extern "C"

@@ -61,6 +61,7 @@ def lib() -> C.CDLL:
         _lib.or_match_ncc.argtypes = [vp, vp, i, i, i, i, i, i, vp, vp, vp]
         _lib.or_match_ncc_guided.argtypes = [vp, vp, i, i, i, i, i, i, vp, vp, vp, vp, vp]
         _lib.or_crosscheck.argtypes = [vp, vp, i, i, i, i, vp, vp]
+        _lib.or_crosscheck_codes.argtypes = [vp, vp, i, i, i, i, i, vp, vp]
         f = C.c_float
         _lib.or_compat_match.argtypes = [vp, vp, i, i, i, i, i, i, i, i, i, f, f, f, vp]
         _lib.or_gate_mask.argtypes = [vp, i, i, i, i, i, f, vp]
@@ -373,6 +374,20 @@ def crosscheck(base, other, tol=1, left_to_right=True):
     rng = np.zeros(2, np.int32)
     lib().or_crosscheck(_p(base), _p(other), W, H, tol, 1 if left_to_right else 0, _p(out), _p(rng))
     return out, (int(rng[0]), int(rng[1]))
+
+
+def crosscheck_codes(base, other, tol=1, left_to_right=True, frame=True, out=None):
+    """The reference's rule on uint16 EDisparityId codes (raw code compare).
+    frame=True leaves the 1-pixel frame of `out` as given (zeros if out is
+    None). -> (out uint16, (min code, max code)); (0xFFEF, 1) when none kept."""
+    base = np.ascontiguousarray(base, np.uint16)
+    other = np.ascontiguousarray(other, np.uint16)
+    H, W = base.shape
+    res = np.zeros((H, W), np.uint16) if out is None else np.array(out, np.uint16, copy=True)
+    rng = np.zeros(2, np.int32)
+    lib().or_crosscheck_codes(_p(base), _p(other), W, H, tol, 1 if left_to_right else 0, 1 if frame else 0,
+                              _p(res), _p(rng))
+    return res, (int(rng[0]), int(rng[1]))
 
 
 # ---- encodings of the library's output maps --------------------------------

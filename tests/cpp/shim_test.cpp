@@ -416,7 +416,8 @@ static int RunGpu(const char* weights) {
             for (int x = 0; x < W; ++x) {
                 const size_t i = size_t(y) * W + x;
                 bad += interior(x, y, 6) && a[i] != K + 1;
-                differ += a[i] != b[i];
+                // the driver leaves the 1-pixel frame unwritten (as the reference)
+                differ += x >= 1 && x < W - 1 && y >= 1 && y < H - 1 && a[i] != b[i];
             }
         CHECK(bad == 0, "census L-R: %d interior pixels not kept at d = %d", bad, K);
         CHECK(differ == 0, "ProcessLR and the cross-check driver disagree on %d pixels", differ);

@@ -135,15 +135,54 @@ def test_crosscheck_driver_and_range(ct, oracle, cuda, dtype):
     cc = ct.CrossCheckDisparityMaps()
     cc.configure(0, W, H, ct.CT_PIX_U8 if dtype == torch.uint8 else ct.CT_PIX_U16, disp_delta_thresh=1)
     res = ct.alloc_image(H, W, dtype, cuda)
+    res.fill_(0x5A)
     cc.process(res, base, other)
     lo, hi = cc.disp_range()
     want, (wlo, whi) = oracle.crosscheck(wl, wr, 1, True)
     got = res.cpu().numpy()
     if dtype == torch.int16:
-        np.testing.assert_array_equal(got.view(np.uint16), oracle.to_u16(want))
+        got, want = got.view(np.uint16), oracle.to_u16(want)
     else:
-        np.testing.assert_array_equal(got, oracle.to_u8(np.where(want == -2, -1, want)))
+        want = oracle.to_u8(np.where(want == -2, -1, want))
+    # the driver leaves the 1-pixel frame unwritten, as the reference kernel
+    np.testing.assert_array_equal(got[1:-1, 1:-1], want[1:-1, 1:-1])
+    frame = np.ones((H, W), bool)
+    frame[1:-1, 1:-1] = False
+    assert (got[frame] == 0x5A).all()
     assert (lo, hi) == (wlo, whi)
+
+
+@pytest.mark.parametrize("W,H,D,tol,lr", [(37, 23, 8, 1, True), (300, 77, 40, 0, False), (129, 64, 5, 12, True),
+                                          (1920, 1080, 128, 1, True)])
+def test_crosscheck_driver_reference_rule_on_codes(ct, oracle, cuda, W, H, D, tol, lr):
+    """U16 code maps with Unknown and IDs mixed in: the driver follows the
+    reference rule exactly (raw code compare, frame unwritten, range over the
+    kept codes), as the oracle that tests/test_ref_pin.py pins to the
+    reference's own kernel."""
+    rng = np.random.default_rng(W + H + D)
+
+    def codes():
+        c = rng.integers(1, D + 1, (H, W)).astype(np.uint16)
+        m = rng.random((H, W))
+        c[m < 0.05] = 0xFFFF
+        c[(m >= 0.05) & (m < 0.09)] = 0
+        c[(m >= 0.09) & (m < 0.11)] = 0xFFFA
+        c[(m >= 0.12) & (m < 0.13)] = 0xFFEF
+        return c
+
+    a, b = codes(), codes()
+    init = rng.integers(0, 65536, (H, W)).astype(np.uint16)
+    cc = ct.CrossCheckDisparityMaps()
+    cc.configure(0, W, H, ct.CT_PIX_U16, disp_delta_thresh=tol, left_to_right=lr)
+    res = to_dev(init.view(np.int16), cuda)
+    cc.process(res, to_dev(a.view(np.int16), cuda), to_dev(b.view(np.int16), cuda))
+    lo, hi = cc.disp_range()
+    want, (wlo, whi) = oracle.crosscheck_codes(a, b, tol, lr, frame=True, out=init)
+    np.testing.assert_array_equal(res.cpu().numpy().view(np.uint16), want)
+    if wlo <= whi:
+        assert (lo, hi) == (wlo - 1, whi - 1)
+    else:
+        assert lo > hi
 
 
 def test_format_mismatch_is_an_error(ct, cuda):
