@@ -497,6 +497,34 @@ void or_crosscheck(const int16_t* base, const int16_t* other, int W, int H, int 
 }
 
 // ---------------------------------------------------------------------------
+// Box sums of a KX x KY window anchored at its top-left pixel (x, y), for
+// x <= W - KX and y <= H - KY (out is (H - KY + 1) x (W - KX + 1)), by the
+// aggregation scheme of wta_box: running column sums over KY rows, then a
+// running horizontal sum over KX columns (wta_box centres the window: its sum
+// for centre (x, y) is this one at (x - r, y - r), KX = KY = 2r + 1). The
+// reference's AlgoArraySum_W32H16 (Kernel.Algo.ArraySum_W32H16.h:94-272)
+// computes the same sums per block tile in two passes of the same kind.
+// ---------------------------------------------------------------------------
+void or_box_sums(const int32_t* data, int W, int H, int KX, int KY, int32_t* out) {
+    const int OW = W - KX + 1, OH = H - KY + 1;
+    if (OW <= 0 || OH <= 0) return;
+    std::vector<int32_t> colsum(W, 0);
+    for (int yy = 0; yy < KY - 1; ++yy)
+        for (int x = 0; x < W; ++x) colsum[x] += data[(size_t)yy * W + x];
+    for (int y = 0; y < OH; ++y) {
+        for (int x = 0; x < W; ++x) colsum[x] += data[(size_t)(y + KY - 1) * W + x];
+        int32_t acc = 0;
+        for (int x = 0; x < KX - 1; ++x) acc += colsum[x];
+        for (int x = 0; x < OW; ++x) {
+            acc += colsum[x + KX - 1];
+            out[(size_t)y * OW + x] = acc;
+            acc -= colsum[x];
+        }
+        for (int x = 0; x < W; ++x) colsum[x] -= data[(size_t)y * W + x];
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Cross-check on EDisparityId codes, the reference rule exactly
 // (CrossCheckDisparityMaps.cu:63-110): for a base code v in [First, Last]
 // (disparity d = v - First) at an interior pixel, x' = x - d (lr = 1) or

@@ -62,6 +62,7 @@ def lib() -> C.CDLL:
         _lib.or_match_ncc_guided.argtypes = [vp, vp, i, i, i, i, i, i, vp, vp, vp, vp, vp]
         _lib.or_crosscheck.argtypes = [vp, vp, i, i, i, i, vp, vp]
         _lib.or_crosscheck_codes.argtypes = [vp, vp, i, i, i, i, i, vp, vp]
+        _lib.or_box_sums.argtypes = [vp, i, i, i, i, vp]
         f = C.c_float
         _lib.or_compat_match.argtypes = [vp, vp, i, i, i, i, i, i, i, i, i, f, f, f, vp]
         _lib.or_gate_mask.argtypes = [vp, i, i, i, i, i, f, vp]
@@ -374,6 +375,16 @@ def crosscheck(base, other, tol=1, left_to_right=True):
     rng = np.zeros(2, np.int32)
     lib().or_crosscheck(_p(base), _p(other), W, H, tol, 1 if left_to_right else 0, _p(out), _p(rng))
     return out, (int(rng[0]), int(rng[1]))
+
+
+def box_sums(data, kx, ky):
+    """int32 box sums of every kx x ky window inside `data`, anchored at the
+    window's top-left pixel (the matchers' aggregation): (H-ky+1, W-kx+1)."""
+    d = np.ascontiguousarray(data, np.int32)
+    H, W = d.shape
+    out = np.zeros((H - ky + 1, W - kx + 1), np.int32)
+    lib().or_box_sums(_p(d), W, H, kx, ky, _p(out))
+    return out
 
 
 def crosscheck_codes(base, other, tol=1, left_to_right=True, frame=True, out=None):

@@ -12,6 +12,7 @@ at build time:
                                                    minus class CDriver
   CluTec.Cuda.MultiView/CrossCheckDisparityMaps.cu namespace Kernel (Const, c_xPars, Transform)
   CluTec.Cuda.MultiView/DisparityId.h              included unchanged
+  CluTec.Cuda.ImgProc/Kernel.Algo.ArraySum_W32H16.h template struct AlgoArraySum_W32H16
 
 and compiles them, in one translation unit fed to g++ on standard input,
 against refshim.h (host stand-ins for the CUDA built-ins and the missing
@@ -86,6 +87,10 @@ def translation_unit(ref: Path) -> str:
     hdr = hdr[:cb] + hdr[ce:].lstrip().removeprefix(";")
     b, e = block(ccu, "namespace Kernel")
     cc_kernel = ccu[b:e]
+    asum = (ref / "CluTec.Cuda.ImgProc/Kernel.Algo.ArraySum_W32H16.h").read_text(errors="replace")
+    sb, se = block(asum, "struct AlgoArraySum_W32H16")
+    tb = asum.rfind("template", 0, sb)  # the struct's template head
+    array_sum = asum[tb:se] + ";"
     return "\n".join([
         '#include "refshim.h"',
         '#include "DisparityId.h"',
@@ -95,6 +100,9 @@ def translation_unit(ref: Path) -> str:
         "namespace Clu { namespace Cuda { namespace CrossCheckDisparityMaps {",
         hdr,
         cc_kernel,
+        "}}}",
+        "namespace Clu { namespace Cuda { namespace Kernel {",
+        array_sum,
         "}}}",
         '#include "harness.inc"',
         "",
@@ -106,7 +114,7 @@ def build(ref: Path = DEFAULT_REF) -> Path:
         raise FileNotFoundError(f"reference sources not found under {ref}")
     OUT_DIR.mkdir(exist_ok=True)
     cxx = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
-    cmd = [cxx, "-std=c++17", "-O1", "-fPIC", "-shared", "-w", "-x", "c++",
+    cmd = [cxx, "-std=c++20", "-pthread", "-O1", "-fPIC", "-shared", "-w", "-x", "c++",
            "-I", str(HERE), "-I", str(ref / "CluTec.Cuda.MultiView"), "-o", str(OUT), "-"]
     r = subprocess.run(cmd, input=translation_unit(ref), text=True, capture_output=True)
     if r.returncode != 0:

@@ -6,10 +6,12 @@
 //
 // What is stood in for, and what each stand-in assumes:
 //  * CUDA built-ins: __global__ / __device__ / __constant__ are plain host
-//    code; threadIdx / blockIdx are host variables set by run_grid(), which
-//    runs the threads of a grid one after another. Exact for kernels without
+//    code; threadIdx / blockIdx are host (thread-local) variables. run_grid()
+//    runs the threads of a grid one after another: exact for kernels without
 //    __syncthreads or warp intrinsics (the census transform and the
-//    cross-check); atomics are plain read-modify-write.
+//    cross-check); atomics are plain read-modify-write. run_block_threads()
+//    runs one block with one host thread per CUDA thread and __syncthreads()
+//    as a barrier over them (the block-level box sums).
 //  * Clu::Cuda::_CDeviceSurface (CluTec.Cuda.Base/DeviceSurface.h:139-197):
 //    Read2D / Write2D / ReadPixel2D / WritePixel2D at (x, y) of a pitched
 //    host buffer (surf2Dread / surf2Dwrite at byte column x * sizeof(element),
@@ -23,10 +25,13 @@
 //    left_to_right) = x - d or x + d (the library's own mapping; the
 //    reference's pixel mapping itself stays unpinned).
 #pragma once
+#include <barrier>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
+#include <vector>
 
 #define __global__
 #define __device__
@@ -41,7 +46,10 @@ struct dim3 {
     dim3() = default;
     dim3(unsigned a, unsigned b = 1, unsigned c = 1) : x(a), y(b), z(c) {}
 };
-inline dim3 threadIdx, blockIdx, blockDim, gridDim;
+inline thread_local dim3 threadIdx, blockIdx;
+inline dim3 blockDim, gridDim;
+inline std::barrier<>* g_block_barrier = nullptr;
+inline void __syncthreads() { g_block_barrier->arrive_and_wait(); }
 
 template <typename T>
 inline T atomicMin(T* p, T v) {
@@ -72,6 +80,26 @@ inline void run_grid(dim3 grid, dim3 block, F&& kernel) {
                             kernel();
                         }
             }
+}
+
+// Runs one block (blockIdx = b) with one host thread per CUDA thread, so
+// that __syncthreads() orders the block's shared data as on the device.
+template <typename F>
+inline void run_block_threads(dim3 block, dim3 b, F&& kernel) {
+    blockDim = block;
+    const unsigned n = block.x * block.y * block.z;
+    std::barrier<> bar(n);
+    g_block_barrier = &bar;
+    std::vector<std::thread> ts;
+    ts.reserve(n);
+    for (unsigned t = 0; t < n; ++t)
+        ts.emplace_back([&, t] {
+            blockIdx = b;
+            threadIdx = dim3(t % block.x, (t / block.x) % block.y, t / (block.x * block.y));
+            kernel();
+        });
+    for (auto& t : ts) t.join();
+    g_block_barrier = nullptr;
 }
 
 namespace Clu {

@@ -45,6 +45,8 @@ def lib() -> C.CDLL:
         vp, i = C.c_void_p, C.c_int
         _lib.ref_census3x3.argtypes = [vp, i, i, i, vp, i]
         _lib.ref_crosscheck.argtypes = [vp, vp, i, i, i, i, vp, vp]
+        _lib.ref_array_sum.argtypes = [i, i, i, vp, vp, vp]
+        _lib.ref_array_sum.restype = i
     return _lib
 
 
@@ -72,3 +74,29 @@ def crosscheck(lr_codes, rl_codes, tol, left_to_right, out_init):
     rng = np.zeros(2, np.int32)
     lib().ref_crosscheck(_p(a), _p(b), W, H, tol, 1 if left_to_right else 0, _p(out), _p(rng))
     return out, (int(rng[0]), int(rng[1]))
+
+
+ARRAY_SUM_PATCHES = [(3, 3), (5, 5), (7, 7), (9, 9), (11, 11), (16, 16), (9, 5)]
+
+
+def array_sum_dims(px, py):
+    """(DataArraySizeX, DataArraySizeY, PatchCountX, PatchCountY, ColGroupSizeX)
+    of AlgoArraySum_W32H16<128, px, py>."""
+    dims = np.zeros(5, np.int32)
+    if lib().ref_array_sum(px, py, 0, None, None, _p(dims)) != 0:
+        raise ValueError(f"patch {px}x{py} not instantiated")
+    return tuple(int(v) for v in dims)
+
+
+def array_sum(px, py, mode, tile):
+    """The reference's block box sums on one data tile (DataArraySizeY x
+    DataArraySizeX int32): mode 0 Sum, 1 SumCache, 2 SumCache3 (channels v,
+    v*v, 3v+1). -> (3, PatchCountY, DataArraySizeX) int32, -1 where no
+    result was delivered."""
+    sx, sy, _, ny, _ = array_sum_dims(px, py)
+    tile = np.ascontiguousarray(tile, np.int32)
+    assert tile.shape == (sy, sx)
+    out = np.zeros((3, ny, sx), np.int32)
+    dims = np.zeros(5, np.int32)
+    lib().ref_array_sum(px, py, mode, _p(tile), _p(out), _p(dims))
+    return out

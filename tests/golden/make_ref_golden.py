@@ -41,10 +41,39 @@ def code_map(rng, W, H, D):
     return c
 
 
+ARRAY_SUM_PATCHES = [(3, 3), (5, 5), (9, 9), (11, 11), (16, 16), (9, 5)]
+
+
+def array_sum_expected(oracle, px, py, dims, tile):
+    """What the reference's AlgoArraySum_W32H16<128, px, py> delivers for each
+    of Sum, SumCache, SumCache3, built from the oracle's box sums: (3 modes,
+    3 planes, PatchCountY, DataArraySizeX), -1 where nothing is delivered."""
+    sx, sy, pcx, pcy, _ = dims
+    t = tile.astype(np.int32)
+    out = np.full((3, 3, pcy, sx), -1, np.int32)
+    for mode in range(3):
+        chans = [t, t * t, 3 * t + 1] if mode == 2 else [t]
+        for c, ch in enumerate(chans):
+            out[mode, c, :, :pcx] = oracle.box_sums(ch, px, py)[:pcy, :pcx]
+    return out
+
+
+def digest(a) -> str:
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a, np.int32).tobytes()).hexdigest()
+
+
 def make(seed: int = 2024) -> dict:
     import ref_lib
     rng = np.random.default_rng(seed)
     out = {}
+    for k, (px, py) in enumerate(ARRAY_SUM_PATCHES):
+        dims = ref_lib.array_sum_dims(px, py)
+        tile = rng.integers(0, 256, (dims[1], dims[0])).astype(np.uint8)
+        res = np.stack([ref_lib.array_sum(px, py, mode, tile) for mode in range(3)])
+        out[f"asum{k}_tile"] = tile
+        out[f"asum{k}_par"] = np.array([px, py, *dims], np.int32)
+        out[f"asum{k}_sha256"] = np.array(digest(res))
     for k, (W, H) in enumerate(CENSUS_SIZES):
         img = census_input(rng, W, H)
         out[f"census{k}_in"] = img

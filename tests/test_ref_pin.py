@@ -2,8 +2,10 @@
 
 oracle/_ref/libctref.so is the reference's census-transform and cross-check
 kernels (CensusTransform.cu:60-120, CrossCheckDisparityMaps.cu:63-110, with
-the grid shapes of their drivers, KernelDriverBase.cpp:142-153) compiled for
-the host from the reference sources (oracle/ref/build_ref.py).
+the grid shapes of their drivers, KernelDriverBase.cpp:142-153) and its block
+box sums (AlgoArraySum_W32H16: Sum, SumCache, SumCache3,
+Kernel.Algo.ArraySum_W32H16.h:94-272, one host thread per CUDA thread)
+compiled for the host from the reference sources (oracle/ref/build_ref.py).
 tests/golden/ref_pin.npz holds its outputs on seeded inputs
 (tests/golden/make_ref_golden.py); the oracle must reproduce them. Where the
 reference sources are present the library is rebuilt and compared live, on
@@ -63,6 +65,21 @@ def test_crosscheck_codes_against_reference_fixture(oracle):
                          FIX[f"cc{k}_out"], FIX[f"cc{k}_range"])
 
 
+def test_box_sums_against_reference_fixture(oracle):
+    """The oracle's box sums (the matchers' aggregation) deliver exactly what
+    the reference's AlgoArraySum_W32H16 delivers, for every patch size the
+    reference matchers use and all three summation entry points."""
+    import sys
+    sys.path.insert(0, str(GOLDEN))
+    import make_ref_golden as g
+    n = len([k for k in FIX.files if k.startswith("asum") and k.endswith("_tile")])
+    assert n >= 6
+    for k in range(n):
+        px, py, *dims = (int(v) for v in FIX[f"asum{k}_par"])
+        want = g.array_sum_expected(oracle, px, py, dims, FIX[f"asum{k}_tile"])
+        assert g.digest(want) == str(FIX[f"asum{k}_sha256"]), (px, py)
+
+
 def test_crosscheck_codes_agrees_with_decoded_oracle_on_matcher_maps(oracle):
     """On maps a matcher produces (disparities and CannotEvaluate only) the
     raw-code rule and the decoded rule of oracle.crosscheck agree inside the
@@ -96,6 +113,18 @@ def test_fixture_regenerates_from_the_reference(ref_lib):
     assert sorted(fresh) == sorted(FIX.files)
     for k in FIX.files:
         np.testing.assert_array_equal(fresh[k], FIX[k], err_msg=k)
+
+
+def test_live_reference_box_sums_random(oracle, ref_lib):
+    import sys
+    sys.path.insert(0, str(GOLDEN))
+    import make_ref_golden as g
+    rng = np.random.default_rng(21)
+    for px, py in ref_lib.ARRAY_SUM_PATCHES:
+        dims = ref_lib.array_sum_dims(px, py)
+        tile = rng.integers(-300, 300, (dims[1], dims[0])).astype(np.int32)
+        got = np.stack([ref_lib.array_sum(px, py, mode, tile) for mode in range(3)])
+        np.testing.assert_array_equal(got, g.array_sum_expected(oracle, px, py, dims, tile), err_msg=f"{px}x{py}")
 
 
 @pytest.mark.parametrize("seed", [11, 12, 13])
