@@ -755,7 +755,10 @@ def batch_shapes(n=64, seed=4):
 #   ncc1080: product + 4 box add/sub (5 INT) + normalisation and argmax
 #            (~10 FP32/INT) = 15 lane operations at the issue rate
 #            (128 per SM per clock: 4 schedulers x 32 lanes)
-#   batch64: as the census headline, 2 POPC (64-bit Hamming)
+#   batch64: as the census headline, 2 POPC (64-bit Hamming) per direction
+#            unit; the fused pass evaluates each cost once for both
+#            directions, so frac counts direction units and frac_costs_once
+#            the costs it evaluates
 #   compat1080: the reference's per-disparity NCC (BlockMatcherNCC.cu:218-271:
 #            the cross mean, the test mean and mean square, the test
 #            standard deviation, the normalised and quantised score: 3
@@ -1031,6 +1034,11 @@ def workload_line(wl, args, ct, dev, stream, flush_buf, world, rank, local, rate
         kind, ops, key = ROOF[wl]
         out_line["roofline"] = pipe_roofline(kind, ops, key, units / (ms * 1e-3), rates, clocks.get("sm_mhz"))
         out_line["roofline"]["note"] = "whole call timed (all its launches)"
+        if wl == "batch64":  # one fused pass per pair decides both directions
+            rf = out_line["roofline"]
+            rf["frac_costs_once"] = round(rf["frac"] / 2, 4)
+            rf["note"] += ("; one fused matching pass per pair evaluates each cost once for both directions: "
+                           "frac counts the metric's direction units (2 per cost), frac_costs_once the costs")
     if rank != 0:
         return None
     out_line["parity_rank0"] = bool(check_fn())

@@ -8,12 +8,14 @@
 //   2. one census launch: every CTA is one 64 x 32 census tile of one image of
 //      one pair (census_tile.cuh), found by a scan of per-pair prefix counts;
 //   3. one persistent matching launch, one CTA per SM: each CTA takes work
-//      items (pair, direction, strip, column tile, disparity block) from a
-//      global atomic counter, largest pairs first, and runs the census match
-//      tile (census_match.cuh) on the pair's pair-planar descriptors. The
-//      last CTA of a (strip, column tile) group merges the disparity blocks;
-//      the last group of a strip (both directions, all column tiles) runs the
-//      cross-check of that strip into the caller's map. Counters reset
+//      items (pair, strip, column tile, disparity block) from a global atomic
+//      counter, largest pairs first, and runs the fused census match tile
+//      (census_match.cuh, left-to-right with the right view's winners bid
+//      into the pair's right-view key plane) on the pair's pair-planar
+//      descriptors. The last CTA of a (strip, column tile) group merges the
+//      disparity blocks; the last group of a strip (all column tiles) runs
+//      the cross-check of that strip into the caller's map from the left map
+//      and the right-view keys, then resets the strip's keys. Counters reset
 //      themselves, so nothing waits on anything.
 // Results are bit-identical to processing each pair alone: every tile's
 // arithmetic is the same and the winner-take-all keys are order-free.
@@ -39,11 +41,13 @@ struct PairDev {
     int census_tx, census_ty, census_item0;  // census tiles per image, prefix over census CTAs
     int match_item0, match_items;            // prefix over matching items
     uint64_t* desc[2];                       // pair-planar descriptors: left, right
-    uint32_t* keys[2];                       // per direction: zc key planes
-    uint32_t* counters[2];                   // per direction: strips x tiles_x group counters
+    uint32_t* keys;                          // zc left-to-right key planes
+    uint32_t* counters;                      // strips x tiles_x group counters
     uint32_t* strip_counter;                 // strips
-    uint16_t* map[2];                        // per direction: U16 disparity maps
+    uint16_t* map;                           // U16 left-to-right disparity map
     size_t map_pitch;                        // bytes
+    uint32_t* rl_keys;                       // right-view keys (tag 0), 0xFFFFFFFF between calls
+    size_t rl_pitch;                         // words
     // per call
     void* out;
     size_t out_pitch;
@@ -92,21 +96,23 @@ __global__ void __launch_bounds__(census::kNT) census_batch_kernel(const PairDev
                         P.desc[img], 0, 1, status, sm);
 }
 
-// Cross-check of rows [y0, y1) of a pair from its two U16 maps into the
-// caller's map (CrossCheckDisparityMaps.cu:63-110 rule, left-to-right).
+// Cross-check of rows [y0, y1) of a pair from its U16 left map and the
+// right-view keys into the caller's map (CrossCheckDisparityMaps.cu:63-110
+// rule, left-to-right: the right view's code at x - d, as its map would hold
+// it, within tol of the left code); then the rows' keys are reset.
 __device__ void crosscheck_rows(const PairDev& P, int y0, int y1, int nt) {
     const int W = P.W;
     for (int idx = threadIdx.x; idx < (y1 - y0) * W; idx += nt) {
         const int y = y0 + idx / W, x = idx % W;
         const uint16_t v = __ldcg(reinterpret_cast<const uint16_t*>(
-                                      reinterpret_cast<const char*>(P.map[0]) + (size_t)y * P.map_pitch) + x);
+                                      reinterpret_cast<const char*>(P.map) + (size_t)y * P.map_pitch) + x);
         const bool disp = v >= CT_DISP_FIRST && v <= CT_DISP_LAST;
         bool keep = false;
         if (disp) {
             const int d = int(v) - 1, xo = x - d;
             if (xo >= 0 && xo < W) {
-                const uint16_t vo = __ldcg(reinterpret_cast<const uint16_t*>(
-                                               reinterpret_cast<const char*>(P.map[1]) + (size_t)y * P.map_pitch) + xo);
+                const bool inside = y >= cm::kAR && y < P.H - cm::kAR && xo >= cm::kAR && xo < W - cm::kAR;
+                const uint16_t vo = cm::rl_code<uint16_t>(__ldcg(P.rl_keys + (size_t)y * P.rl_pitch + xo), 0u, inside);
                 keep = abs(int(vo) - int(v)) <= P.tol;  // raw codes, CrossCheckDisparityMaps.cu:94
             }
         }
@@ -117,6 +123,9 @@ __device__ void crosscheck_rows(const PairDev& P, int y0, int y1, int nt) {
             reinterpret_cast<uint16_t*>(row)[x] = keep ? v : (disp ? uint16_t(CT_DISP_INCONSISTENT) : v);
         }
     }
+    __syncthreads();  // every read of the rows' keys done
+    for (int idx = threadIdx.x; idx < (y1 - y0) * W; idx += nt)
+        P.rl_keys[(size_t)(y0 + idx / W) * P.rl_pitch + idx % W] = 0xFFFFFFFFu;
 }
 
 __global__ void __launch_bounds__(cm::Var<4>::kNT, 1)
@@ -139,38 +148,38 @@ __global__ void __launch_bounds__(cm::Var<4>::kNT, 1)
         const int p = find_pair(pairs, n, item, false);
         const PairDev& P = pairs[p];
         int local = item - P.match_item0;
-        const int per_dir = P.strips * P.tiles_x * P.zc;
-        if (local < 0 || local >= P.match_items || P.match_items != 2 * per_dir) {  // table inconsistent
-            if (tid == 0) dev::report(status, CT_EINTERNAL);
+        if (local < 0 || local >= P.match_items || P.match_items != P.strips * P.tiles_x * P.zc) {
+            if (tid == 0) dev::report(status, CT_EINTERNAL);  // table inconsistent
             break;
         }
-        const int dir = local / per_dir;
-        local %= per_dir;
         // disparity blocks of one group are consecutive items, so the group's
         // CTAs run close together and the merging one finds its inputs in L2
         const Tile t{(local / P.zc) % P.tiles_x, local / (P.zc * P.tiles_x), local % P.zc, P.tiles_x, P.zc};
         MatchArgs a{};
         a.W = P.W; a.H = P.H; a.D = P.D; a.th = P.th;
-        a.keys = P.keys[dir];
-        a.counters = P.counters[dir];
+        a.keys = P.keys;
+        a.counters = P.counters;
         a.merge_last = 1;
-        a.out = P.map[dir]; a.out_pitch = P.map_pitch; a.out_type = CT_PIX_U16;
+        a.out = P.map; a.out_pitch = P.map_pitch; a.out_type = CT_PIX_U16;
         a.status = status;
-        const CUtensorMap* tb = &match_maps[p * 4 + (dir == 0 ? 0 : 2)];
-        const CUtensorMap* tm = &match_maps[p * 4 + (dir == 0 ? 1 : 3)];
+        a.rl_keys = P.rl_keys;  // tag 0: the strip's cross-check resets the keys it read
+        a.rl_pitch = P.rl_pitch;
+        a.rl_tag = 0u;
+        const CUtensorMap* tb = &match_maps[p * 2 + 0];
+        const CUtensorMap* tm = &match_maps[p * 2 + 1];
         if (tid == 0) {  // maps written by a host copy: make them visible to the TMA unit
             tmap_acquire(tb);
             tmap_acquire(tm);
         }
-        const TileResult res = dir == 0 ? run_tile<0, 4>(tb, tm, a, t, sm, par) : run_tile<1, 4>(tb, tm, a, t, sm, par);
+        const TileResult res = run_tile<0, 4, false, true>(tb, tm, a, t, sm, par);
         if (res.aborted) break;  // status already set; the CTA stops taking work
         if (res.group_done) {
-            // one more finished (direction, column tile) group of this strip
+            // one more finished column tile group of this strip
             if (tid == 0) {
                 __threadfence();
                 unsigned* sc = reinterpret_cast<unsigned*>(&P.strip_counter[t.by]);
                 const unsigned prev = atomicAdd(sc, 1u);
-                s_last = prev == unsigned(2 * P.tiles_x) - 1;
+                s_last = prev == unsigned(P.tiles_x) - 1;
                 if (s_last) *sc = 0u;
             }
             __syncthreads();
@@ -296,7 +305,7 @@ int enqueue(BatchHandle* h, Staging& st, bool record, cudaStream_t s) {
     CT_CUDA_TRY(cudaMemsetAsync(h->d_queue, 0, sizeof(unsigned), s));
     census_batch_kernel<<<h->total_census, census::kNT, 0, s>>>(h->d_pairs, h->n, h->d_maps, h->d_status);
     CT_LAUNCH_CHECK();
-    match_batch_kernel<<<h->sms, cm::Var<4>::kNT, cm::smem_bytes(), s>>>(h->d_pairs, h->n, h->total_match,
+    match_batch_kernel<<<h->sms, cm::Var<4>::kNT, cm::smem_bytes_rl(), s>>>(h->d_pairs, h->n, h->total_match,
                                                                         h->d_match_maps, h->d_queue, h->d_status);
     CT_LAUNCH_CHECK();
     return CT_OK;
@@ -318,7 +327,7 @@ int layout(BatchHandle* h, const std::vector<int>& th) {
     // sizes
     size_t bytes = 0;
     auto take = [&](size_t b) { const size_t o = bytes; bytes += (b + 255) / 256 * 256; return o; };
-    struct Off { size_t desc[2], keys[2], cnt[2], strip, map[2]; };
+    struct Off { size_t desc[2], keys, cnt, strip, map, rl; };
     std::vector<Off> off(n);
     h->pairs.assign(n, PairDev{});
     int census0 = 0, match0 = 0;
@@ -336,20 +345,20 @@ int layout(BatchHandle* h, const std::vector<int>& th) {
         P.census_item0 = census0;
         census0 += 2 * P.census_tx * P.census_ty;
         P.match_item0 = match0;
-        P.match_items = 2 * P.strips * P.tiles_x * P.zc;
+        P.match_items = P.strips * P.tiles_x * P.zc;
         match0 += P.match_items;
         P.map_pitch = ((size_t)P.W * 2 + 255) / 256 * 256;
         Off& o = off[k];
         for (int v = 0; v < 2; ++v) o.desc[v] = take(cm::planar_pitch(P.W) * P.H * 8);
-        for (int d = 0; d < 2; ++d) {
-            o.keys[d] = take((size_t)P.zc * P.W * P.H * 4);
-            o.cnt[d] = take((size_t)P.strips * P.tiles_x * 4);
-            o.map[d] = take(P.map_pitch * P.H);
-        }
+        o.keys = take((size_t)P.zc * P.W * P.H * 4);
+        o.cnt = take((size_t)P.strips * P.tiles_x * 4);
+        o.map = take(P.map_pitch * P.H);
+        P.rl_pitch = cm::rl_pitch_words(P.W);
+        o.rl = take(P.rl_pitch * P.H * 4);
         o.strip = take((size_t)P.strips * 4);
     }
     const size_t o_pairs = take(sizeof(PairDev) * n), o_maps = take(sizeof(CallMaps) * n);
-    const size_t o_mmaps = take(sizeof(CUtensorMap) * 4 * n), o_queue = take(256);
+    const size_t o_mmaps = take(sizeof(CUtensorMap) * 2 * n), o_queue = take(256);
     cudaFree(h->arena);
     h->arena = nullptr;
     if (cudaMalloc(&h->arena, bytes) != cudaSuccess) return fail(CT_ENOMEM, "batch scratch (%zu bytes)", bytes);
@@ -358,11 +367,11 @@ int layout(BatchHandle* h, const std::vector<int>& th) {
     for (int k = 0; k < n; ++k) {
         PairDev& P = h->pairs[k];
         for (int v = 0; v < 2; ++v) P.desc[v] = reinterpret_cast<uint64_t*>(A + off[k].desc[v]);
-        for (int d = 0; d < 2; ++d) {
-            P.keys[d] = reinterpret_cast<uint32_t*>(A + off[k].keys[d]);
-            P.counters[d] = reinterpret_cast<uint32_t*>(A + off[k].cnt[d]);
-            P.map[d] = reinterpret_cast<uint16_t*>(A + off[k].map[d]);
-        }
+        P.keys = reinterpret_cast<uint32_t*>(A + off[k].keys);
+        P.counters = reinterpret_cast<uint32_t*>(A + off[k].cnt);
+        P.map = reinterpret_cast<uint16_t*>(A + off[k].map);
+        P.rl_keys = reinterpret_cast<uint32_t*>(A + off[k].rl);
+        CT_CUDA_TRY(cudaMemset(P.rl_keys, 0xFF, P.rl_pitch * P.H * 4));
         P.strip_counter = reinterpret_cast<uint32_t*>(A + off[k].strip);
     }
     h->d_pairs = reinterpret_cast<PairDev*>(A + o_pairs);
@@ -371,13 +380,12 @@ int layout(BatchHandle* h, const std::vector<int>& th) {
     h->d_queue = reinterpret_cast<unsigned*>(A + o_queue);
     h->total_census = census0;
     h->total_match = match0;
-    std::vector<CUtensorMap> mm(4 * n);
+    std::vector<CUtensorMap> mm(2 * n);  // left as base, right as match
     for (int k = 0; k < n; ++k) {
         const PairDev& P = h->pairs[k];
-        if (int rc = cm::make_planar_maps(&mm[4 * k + 0], &mm[4 * k + 1], P.desc[0], P.desc[1], P.W, P.H)) return rc;
-        if (int rc = cm::make_planar_maps(&mm[4 * k + 2], &mm[4 * k + 3], P.desc[1], P.desc[0], P.W, P.H)) return rc;
+        if (int rc = cm::make_planar_maps(&mm[2 * k + 0], &mm[2 * k + 1], P.desc[0], P.desc[1], P.W, P.H)) return rc;
     }
-    CT_CUDA_TRY(cudaMemcpy(h->d_match_maps, mm.data(), sizeof(CUtensorMap) * 4 * n, cudaMemcpyHostToDevice));
+    CT_CUDA_TRY(cudaMemcpy(h->d_match_maps, mm.data(), sizeof(CUtensorMap) * 2 * n, cudaMemcpyHostToDevice));
     if (h->graph_exec) {
         cudaGraphExecDestroy(h->graph_exec);
         h->graph_exec = nullptr;
@@ -419,7 +427,7 @@ int ct_batch_configure(ct_handle* hh, int32_t device, const ct_batch_shape* shap
     if (int rc = h->init_status()) return rc;
     CT_CUDA_TRY(cm::prepare_census_match());
     CT_CUDA_TRY(cudaFuncSetAttribute(match_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int(cm::smem_bytes())));
+                                     int(cm::smem_bytes_rl())));
     h->sms = sm_count(device);
     h->n = n;
     h->tol = tol;
