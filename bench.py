@@ -67,7 +67,8 @@ def parse():
                              "aw1440", "batch64",
                              "compat_ncc1080"],
                     help="for ncu captures, then exit: census_match or confnet_infer = that kernel twice on the "
-                         "1080p D=128 pair; pipelines = the plain L-R pipeline 3x, then the learned one 3x; a "
+                         "1080p D=128 pair; pipelines = the plain L-R pipeline 3x (one fused pass), 3x in two "
+                         "passes, then the learned one 3x; a "
                          "configuration name = its step twice (no autotuning, no CPU work)")
     ap.add_argument("--no-configs", action="store_true",
                     help="default run: measure the headline only, without the other configurations")
@@ -692,9 +693,12 @@ def run_profile(args):
         if args.profile == "confnet_infer":
             for _ in range(2):
                 net.infer(None, cv, disp, checked=ck)
-        else:
-            for _ in range(3):
-                m.process_lr(dL, dR, disp_checked=ck, tol=1)
+        else:  # plain (one fused pass), plain in two passes, learned: three times each
+            for fused in (True, False):
+                m.set_fused_lr(fused)
+                for _ in range(3):
+                    m.process_lr(dL, dR, disp_checked=ck, tol=1)
+            m.set_fused_lr(True)
             for _ in range(3):
                 m.process_curves(disp, cv, dL, dR)
                 net.infer(None, cv, disp, checked=ck)
