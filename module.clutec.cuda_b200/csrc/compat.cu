@@ -68,11 +68,26 @@ __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b)
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float i2f(int v) { return __int2float_rn(v); }
 
+// RN(x / d) for an integer-valued x (|x| <= 2^24) and a positive integer
+// divisor d, given zd = RN(1 / d): one multiply and the remainder correction
+// of P. Markstein (IA-64 and Elementary Functions, 2000): q = RN(x zd);
+// r = x - q d, exact through a fused multiply-add; q' = RN(q + r zd). Equal to
+// the IEEE quotient for every numerator in that range and every divisor the
+// kernels use (the patch element counts P^2, P = 1 .. 16, 3 s^2 for the
+// adaptive windows, and 255), checked exhaustively against IEEE division
+// (tests/test_compat_oracle.py). Three instructions instead of a division.
+__device__ __forceinline__ float div_int(float x, float d, float zd) {
+    const float q = __fmul_rn(x, zd);
+    const float r = __fmaf_rn(-q, d, x);
+    return __fmaf_rn(r, zd, q);
+}
+
 // EvalSim SSimType_SignedProduct (BlockMatcherAW1.cu:209-218 scale 255,
 // BlockMatcher1.cu:201-210 scale 127), truncated.
-__device__ __forceinline__ int signed_product(int p, int q, float scale) {
-    float f1 = fmul(2.0f, fsub(fdiv(i2f(p), 255.0f), 0.5f));
-    const float f2 = fmul(2.0f, fsub(fdiv(i2f(q), 255.0f), 0.5f));
+// z255 = RN(1 / 255).
+__device__ __forceinline__ int signed_product(int p, int q, float scale, float z255) {
+    float f1 = fmul(2.0f, fsub(div_int(i2f(p), 255.0f, z255), 0.5f));
+    const float f2 = fmul(2.0f, fsub(div_int(i2f(q), 255.0f, z255), 0.5f));
     f1 = fmul(f1, f2);
     f1 = fmul(f1, scale);
     return __float2int_rz(f1);
@@ -138,6 +153,9 @@ __global__ void __launch_bounds__(kNT) compat_kernel(Args a) {
 
     const bool valid = x - pa >= 0 && x + pb < a.W && y - pa >= 0 && y + pb < a.H;
     const int n_eff = AW ? 3 * s * s : P * P;  // BasePatchElementCount
+    const float f_eff = i2f(n_eff), z_eff = __frcp_rn(f_eff);
+    const float f_pp = i2f(P * P), z_pp = __frcp_rn(f_pp);
+    const float z255 = __frcp_rn(255.0f);
 
     // ---- gradient gate (once per pixel, directly from the staged base) ----
     bool gated = false;
@@ -228,8 +246,8 @@ __global__ void __launch_bounds__(kNT) compat_kernel(Args a) {
             const int p = sB[r][c], q = sM[r][c + moff];
             if (METHOD == kSad1 || METHOD == kAw2) return abs(p - q);
             if (METHOD == kNcc) return p * q;
-            if (METHOD == kAw1) return a.sim_type ? signed_product(p, q, 255.0f) : 255 - abs(p - q);
-            return a.sim_type ? signed_product(p, q, 127.0f) : (255 - abs(p - q)) >> 1;
+            if (METHOD == kAw1) return a.sim_type ? signed_product(p, q, 255.0f, z255) : 255 - abs(p - q);
+            return a.sim_type ? signed_product(p, q, 127.0f, z255) : (255 - abs(p - q)) >> 1;
         };
         int Su[kU];
         if (!AW) {
@@ -341,7 +359,7 @@ __global__ void __launch_bounds__(kNT) compat_kernel(Args a) {
                     if (METHOD == kNcc) {  // uint8-quantised NCC (NCC.cu:218-271)
                         const int xm = a.dir ? x - d : x + d;
                         const size_t om = (size_t)y * a.W + xm;
-                        const float fCross = fdiv(i2f(S), i2f(P * P));
+                        const float fCross = div_int(i2f(S), f_pp, z_pp);
                         const float fTm = __ldg(&a.mMean[om]);
                         const float fTstd = __ldg(&a.mStd[om]);
                         const float fNorm = fmul(bStd, fTstd);
@@ -371,7 +389,7 @@ __global__ void __launch_bounds__(kNT) compat_kernel(Args a) {
                     const bool skip = METHOD == kAw2 ? disp > CT_DISP_LAST : disp == CT_DISP_CANNOT_EVALUATE;
                     if (eval && !skip) {
                         const int v = S;
-                        const float fmin = fdiv(i2f(v), i2f(n_eff));
+                        const float fmin = div_int(i2f(v), f_eff, z_eff);
                         if (idx == 0) {
                             mW = v; mY = v;
                             if (METHOD == kAw2) mZ = v;

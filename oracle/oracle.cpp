@@ -497,6 +497,30 @@ void or_crosscheck(const int16_t* base, const int16_t* other, int W, int H, int 
 }
 
 // ---------------------------------------------------------------------------
+// Exhaustive check of the constant-divisor quotient the reference-compat
+// kernel uses instead of an IEEE division (Markstein's remainder correction:
+// q = RN(x z), r = RN(x - q d) by a fused multiply-add, q' = RN(q + r z),
+// z = RN(1 / d)): counts the integers x with |x| <= nmax where q' differs
+// from the IEEE quotient x / d in binary32.
+// ---------------------------------------------------------------------------
+long or_div_int_mismatches(int d, int nmax) {
+    const float df = float(d);
+    volatile float one = 1.0f;  // keeps the reciprocal a run-time IEEE division
+    const float z = one / df;
+    long bad = 0;
+#pragma omp parallel for schedule(static) reduction(+ : bad)
+    for (long n = -long(nmax); n <= long(nmax); ++n) {
+        const float x = float(n);
+        const float want = x / df;
+        const float q = x * z;
+        const float r = std::fma(-q, df, x);
+        const float q1 = std::fma(r, z, q);
+        bad += (q1 != want);
+    }
+    return bad;
+}
+
+// ---------------------------------------------------------------------------
 // Box sums of a KX x KY window anchored at its top-left pixel (x, y), for
 // x <= W - KX and y <= H - KY (out is (H - KY + 1) x (W - KX + 1)), by the
 // aggregation scheme of wta_box: running column sums over KY rows, then a

@@ -63,6 +63,8 @@ def lib() -> C.CDLL:
         _lib.or_crosscheck.argtypes = [vp, vp, i, i, i, i, vp, vp]
         _lib.or_crosscheck_codes.argtypes = [vp, vp, i, i, i, i, i, vp, vp]
         _lib.or_box_sums.argtypes = [vp, i, i, i, i, vp]
+        _lib.or_div_int_mismatches.argtypes = [i, i]
+        _lib.or_div_int_mismatches.restype = C.c_long
         f = C.c_float
         _lib.or_compat_match.argtypes = [vp, vp, i, i, i, i, i, i, i, i, i, f, f, f, vp]
         _lib.or_gate_mask.argtypes = [vp, i, i, i, i, i, f, vp]
@@ -375,6 +377,13 @@ def crosscheck(base, other, tol=1, left_to_right=True):
     rng = np.zeros(2, np.int32)
     lib().or_crosscheck(_p(base), _p(other), W, H, tol, 1 if left_to_right else 0, _p(out), _p(rng))
     return out, (int(rng[0]), int(rng[1]))
+
+
+def div_int_mismatches(d, nmax=1 << 24):
+    """Integers |x| <= nmax for which the reference-compat kernel's
+    constant-divisor quotient (multiply by RN(1/d), one remainder correction)
+    differs from the IEEE binary32 quotient x / d."""
+    return int(lib().or_div_int_mismatches(d, nmax))
 
 
 def box_sums(data, kx, ky):

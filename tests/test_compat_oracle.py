@@ -230,3 +230,14 @@ def test_second_restatement_agrees(ct, oracle, case):
     got = oracle.compat_match(L, R, method, D, patch, dmin=dmin, sim_type=sim, left_to_right=lr,
                               grad_thresh=grad, score_thresh=score, min_delta_thresh=delta)
     np.testing.assert_array_equal(got, want)
+
+
+def test_constant_divisor_quotient_is_ieee_exhaustive(oracle):
+    """The reference-compat kernel divides integer-valued sums by the patch
+    element count (and pixel values by 255) with a multiply by the rounded
+    reciprocal and one remainder correction instead of an IEEE division; for
+    every divisor it uses and every integer numerator up to 2^24 in magnitude
+    the quotient equals the IEEE binary32 quotient."""
+    divisors = sorted({p * p for p in range(1, 17)} | {3 * s * s for s in range(1, 6)} | {255})
+    bad = {d: oracle.div_int_mismatches(d) for d in divisors}
+    assert all(v == 0 for v in bad.values()), bad
