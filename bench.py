@@ -245,7 +245,8 @@ class ClockSampler:
 
 
 def traffic_from_profile():
-    """DRAM bytes per launch of census_match_kernel from the committed ncu summary."""
+    """DRAM bytes per launch of the fused census_match_kernel (the headline's
+    dominant kernel) from the committed ncu summary."""
     p = ROOT / "profiles" / "census_match_1080p_d128.json"
     if p.exists():
         try:
