@@ -274,6 +274,40 @@ def test_process_lr_fused_equals_two_passes(ct, oracle, cuda, W, H, D, dmin, kin
             np.testing.assert_array_equal(view, enc(want), err_msg=name)
 
 
+@pytest.mark.parametrize("W,H,D,dmin", [
+    (8, 8, 1, 0),        # smallest image, one disparity
+    (16, 9, 3, 1),       # odd minimum disparity, D tiny
+    (96, 64, 1, 0),      # D = 1
+    (130, 37, 64, 0),    # exactly one block of disparities, two column tiles
+    (124, 40, 65, 0),    # one column tile, D one past a block
+    (60, 30, 20, 50),    # minimum disparity close to the width: most pixels search nothing
+    (50, 20, 10, 60),    # minimum disparity beyond the width: no disparity anywhere
+])
+def test_process_lr_fused_edge_shapes(ct, oracle, cuda, W, H, D, dmin):
+    """The fused pass on degenerate shapes: all three maps equal the two-pass
+    result and the oracle's."""
+    L, R = pair(ct, 1, 500 + W + D, W, H, max(1, dmin + D - 1))
+    m = ct.BlockMatcherCensus()
+    m.configure(0, W, H, D, disp_min=dmin)
+    dl, dr = to_dev(L, cuda), to_dev(R, cuda)
+    maps = {}
+    for fused in (True, False):
+        m.set_fused_lr(fused)
+        out = [ct.alloc_image(H, W, torch.int16, cuda) for _ in range(3)]
+        for o in out:
+            o.fill_(0x2B2B)
+        m.process_lr(dl, dr, disp_lr=out[0], disp_rl=out[1], disp_checked=out[2], tol=1)
+        torch.cuda.synchronize()
+        assert m.device_status() == 0
+        maps[fused] = [o.cpu().numpy().view(np.uint16) for o in out]
+    wl, _ = oracle.match_census(L, R, D, 2, True, dmin=dmin)
+    wr, _ = oracle.match_census(L, R, D, 2, False, dmin=dmin)
+    wc, _ = oracle.crosscheck(wl, wr, 1, True)
+    for k, (want, name) in enumerate(zip((wl, wr, wc), ("lr", "rl", "checked"))):
+        np.testing.assert_array_equal(maps[True][k], maps[False][k], err_msg=name)
+        np.testing.assert_array_equal(maps[True][k], oracle.to_u16(want), err_msg=name)
+
+
 @pytest.mark.parametrize("dtype", [torch.uint8, torch.int16])
 def test_process_lr_fused_many_calls(ct, cuda, dtype):
     """The fused pass keeps the right view's keys between calls and tells this
