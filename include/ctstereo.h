@@ -444,13 +444,17 @@ int ct_crosscheck_range(ct_handle* h, int32_t* disp_min, int32_t* disp_max);
 
 /* ---- batched census stereo ------------------------------------------------
  * Many pairs of mixed size and disparity range per call: 9x7 census of both
- * images, census matching left-to-right and right-to-left, cross-check with
- * tolerance tol, for every pair. One batched census launch and one
- * persistent, work-queue-scheduled matching launch (one CTA per SM) whose
- * last CTAs per strip run the cross-check. Each pair's result equals
+ * images, census matching in both directions (one fused pass per pair that
+ * decides both directions' winners), cross-check with tolerance tol, for
+ * every pair. One batched census launch and one persistent,
+ * work-queue-scheduled matching launch (one CTA per SM) whose last CTAs per
+ * strip run the cross-check. Each pair's result equals
  * ct_bm_census_process_lr(disp_checked) run on that pair alone. No
  * counterpart in the reference (its drivers process one image per call).
- * The handle owns all scratch; pair shapes are fixed at configure. */
+ * The handle owns all scratch; pair shapes are fixed at configure. The
+ * scratch's counters and right-view keys return to their initial state at
+ * the end of every complete call; after a call whose status word reports
+ * CT_ETIMEOUT, configure the handle again before the next call. */
 typedef struct ct_batch_shape {
     int32_t width;
     int32_t height;
