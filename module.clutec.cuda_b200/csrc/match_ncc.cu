@@ -396,7 +396,11 @@ __global__ void __launch_bounds__(kNT, 2)
 }
 
 }  // namespace ncc
+}  // namespace ct
 
+#include "ncc_tc.cuh"
+
+namespace ct {
 namespace {
 
 struct NccHandle : ct_handle {
@@ -415,6 +419,8 @@ struct NccHandle : ct_handle {
     uint32_t* guide = nullptr;  // guided mode: one search range per 16 x 16 block
     uint32_t* counters = nullptr;  // one per (strip, column tile) at the smallest strip height
     int th = 32;
+    int tensor_cores = 0;  // unguided matching: window cross sums on the tensor cores (ncc_tc_kernel)
+    int th_tc = 64;        // its strip height
 };
 
 template <int R>
@@ -455,6 +461,20 @@ int launch_ncc(NccHandle* h, const ct_image* disp, const ct_image* score, const 
     box_stats_kernel<R><<<sg, sb, 0, s>>>(static_cast<const uint8_t*>(Rr->ptr), Rr->pitch_bytes, W, H,
                                           h->stats + 2 * N, h->stats + 3 * N, nullptr);
     CT_LAUNCH_CHECK();
+    if (!init && h->tensor_cores) {
+        static bool attr_tc = false;
+        if (!attr_tc) {
+            CT_CUDA_TRY(cudaFuncSetAttribute(ncc_tc_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             tc::kSmem));
+            attr_tc = true;
+        }
+        a.th = h->th_tc;
+        dim3 grid((W + tc::kM - 1) / tc::kM, (H + a.th - 1) / a.th, (a.D + tc::kDB - 1) / tc::kDB);
+        ncc_tc_kernel<R><<<grid, tc::kNT, tc::kSmem, s>>>(static_cast<const uint8_t*>(L->ptr), L->pitch_bytes,
+                                                         static_cast<const uint8_t*>(Rr->ptr), Rr->pitch_bytes, a);
+        CT_LAUNCH_CHECK();
+        return gate_launch(disp, score, L, 0, 2 * R + 1, h->grad_thresh, s);  // EvalGrad (NCC.cu:388-413)
+    }
     const int NR = a.th + 2 * R;
     CUtensorMap tb, tm;
     if (int rc = make_tmap_2d(&tb, L->ptr, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, W, H, L->pitch_bytes, kBW, NR)) return rc;
@@ -521,8 +541,27 @@ int ct_bm_ncc_configure(ct_handle* hh, int32_t device, const ct_format* fmt, con
         const long tiles = long((fmt->width + two - 1) / two) * ((p->disp_count + ncc::kDPC - 1) / ncc::kDPC);
         h->th = 32;
         while (h->th > 8 && tiles * ((fmt->height + h->th - 1) / h->th) < 2L * sms) h->th -= 2;
+        // tensor-core kernel (one CTA per SM): the strip height minimising
+        // waves x (rows + the strip's first window, worth ~6 rows)
+        const long tiles_tc = long((fmt->width + ncc::tc::kM - 1) / ncc::tc::kM) *
+                              ((p->disp_count + ncc::tc::kDB - 1) / ncc::tc::kDB);
+        long best = -1;
+        for (int th = 16; th <= 256; ++th) {
+            const long ctas = tiles_tc * ((fmt->height + th - 1) / th);
+            const long cost = ((ctas + sms - 1) / sms) * (th + 6);
+            if (best < 0 || cost < best) { best = cost; h->th_tc = th; }
+        }
     }
     h->configured = true;
+    return CT_OK;
+}
+
+int ct_bm_ncc_set_tensor_cores(ct_handle* hh, int32_t enable) {
+    clear_error();
+    auto* h = (hh && hh->kind == Kind::BmNcc) ? static_cast<NccHandle*>(hh) : nullptr;
+    if (!h) return fail(CT_ESTATE, "not an NCC matcher handle");
+    if (enable != 0 && enable != 1) return fail(CT_EINVAL, "enable must be 0 or 1");
+    h->tensor_cores = enable;
     return CT_OK;
 }
 

@@ -1,0 +1,493 @@
+// ncc_tc.cuh — the NCC matcher (match_ncc.cu) with its window cross sums on
+// the tensor cores. Included by match_ncc.cu after the CUDA-core kernel; the
+// scores, ranking and merge are the same, so are the maps.
+//
+// For output row y, pixel x and match column x' the window cross sum is
+//   C(x, x') = sum over rows r = y-R .. y+R of sum over i = -R .. R of
+//              L(x + i, r) R(x' + i, r),
+// i.e. for one image row r a product of two matrices: A_r (pixels x, one row
+// each holding the 2R+1 pixels of its window row) times B_r^T (match columns
+// x', the same). A CTA owns 128 output pixels x0 .. x0+127 of a strip of
+// rows and 128 disparities, i.e. match columns xb .. xb+255 (xb = x0 - dmin -
+// dz0 - 127): one tcgen05.mma of M = 128, N = 256, K = 16 (f16 operands,
+// exact for 8-bit pixels; fp32 accumulation, exact for the 11x11 sums of
+// products < 2^24) per image row. The accumulator in TMEM keeps the running
+// window sum down the strip: D(y+1) = D(y) + A_{y+R+1} B_{y+R+1}^T -
+// A_{y-R} B_{y-R}^T, the subtraction by the descriptor's negate-A bit, so a
+// row costs two MMAs. Operands are K-major, no swizzle: pixel row i of a
+// panel at i * 16 bytes, the second 8-element K chunk one panel column
+// (rows x 16 bytes) further. They are built in shared memory from two staged
+// image rows per step (bytes -> f16 through the exponent of 1024).
+//
+// Epilogue: TMEM lane m = pixel x0 + m holds C(x, x') for all 256 columns;
+// its disparities d = m + 127 - n (column n) form a 128-wide band. 16 warps:
+// lane quarter q = warp % 4 (the lanes a warp may read), column slice h =
+// warp / 4 of the quarter's band (40 columns each: 32 q + 40 h ..), read with
+// one 32-column and one 8-column tcgen05.ld per row. Ranking as the CUDA-core
+// kernel, by the estimate num * rsqrt(vy), num = n C - Sx Sy, here from the
+// fp32 sum: est = C (n r) - Sx (Sy r), whose error is at most 240 r plus a
+// relative 1e-6 (the products n C and Sx Sy are below 2^30); every disparity
+// whose estimate lies within that margin of the thread's best is scored
+// exactly (the IEEE score of the CUDA-core kernel, from the exact integer C),
+// so the exact argmax over the thread's disparities is always among them.
+// The 4 (column slices) x gridDim.z keys of a pixel merge by atomicMax, in
+// shared memory per row and, for D > 128, in global memory with the
+// last-arriver merge of the CUDA-core kernel.
+#pragma once
+
+namespace ct {
+namespace ncc {
+namespace tc {
+
+constexpr int kM = 128;    // output pixels per tile = MMA M = TMEM lanes
+constexpr int kN = 256;    // match columns per tile = MMA N = accumulator columns
+constexpr int kDB = 128;   // disparities per CTA
+constexpr int kNT = 512;   // 16 warps: 4 per TMEM lane quarter
+constexpr int kCols = 40;  // accumulator columns a thread ranks per row
+constexpr int kPA = kM * 16 * 2, kPB = kN * 16 * 2;  // panel bytes (K = 16 f16)
+constexpr int kSet = 2 * (kPA + kPB);                // entering + leaving row
+constexpr int kSL = kM + 16, kSR = kN + 16;          // staged bytes of one row (>= 128 + 2R, 256 + 2R)
+constexpr int kStage = 2 * (kSL + kSR);              // entering + leaving row
+// shared memory
+constexpr int kOffSet = 0;                        // 2 panel sets
+constexpr int kOffStage = 2 * kSet;               // 2 staging buffers
+constexpr int kOffCol = kOffStage + 2 * kStage;   // 2 rows x kN column records (int4)
+constexpr int kOffKey = kOffCol + 2 * kN * 16;    // 2 rows x kM merge keys
+constexpr int kOffBar = kOffKey + 2 * kM * 8;     // MMA completion
+constexpr int kOffSlot = kOffBar + 8;             // TMEM address, group-last flag
+constexpr int kSmem = kOffSlot + 16;
+static_assert(kOffStage % 1024 == 0 && kOffCol % 16 == 0 && kOffKey % 8 == 0 && kOffBar % 8 == 0, "alignment");
+constexpr uint32_t kTmemCols = 256;
+
+// Instruction descriptor, kind::f16: D fp32 (bit 4), A and B f16 (bits 7, 10
+// = 0), negate A (bit 13), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+constexpr uint32_t idesc(bool negate_a) {
+    return (1u << 4) | (uint32_t(negate_a) << 13) | (uint32_t(kN >> 3) << 17) | (uint32_t(kM >> 4) << 24);
+}
+// Shared-memory matrix descriptor: start, leading byte offset (the next K
+// chunk), stride byte offset 128 (the next 8 rows), version 1, no swizzle.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo) {
+    return uint64_t((saddr >> 4) & 0x3FFF) | (uint64_t((lbo >> 4) & 0x3FFF) << 16) | (uint64_t(128 >> 4) << 32) |
+           (uint64_t(1) << 46);
+}
+// D += A B^T (accumulate) or D = A B^T, issued by one elected lane of a
+// converged warp.
+__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t id, bool acc) {
+    asm volatile(
+        "{\n.reg .pred p, e;\nsetp.ne.b32 p, %4, 0;\nelect.sync _|e, 0xffffffff;\n"
+        "@e tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(id), "r"(uint32_t(acc))
+        : "memory");
+}
+__device__ __forceinline__ void commit(uint64_t* bar) {
+    asm volatile(
+        "{\n.reg .pred e;\nelect.sync _|e, 0xffffffff;\n"
+        "@e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n}\n" ::"r"(
+            dev::smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Columns taddr .. taddr + 39 of this thread's lane, waited for.
+__device__ __forceinline__ void ld40(uint32_t taddr, float (&v)[kCols]) {
+    uint32_t r[kCols];
+    asm volatile(
+        "{\n"
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,"
+        "%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%40];\n"
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%32,%33,%34,%35,%36,%37,%38,%39}, [%41];\n"
+        "tcgen05.wait::ld.sync.aligned;\n"
+        "}\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+          "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39])
+        : "r"(taddr), "r"(taddr + 32)
+        : "memory");
+#pragma unroll
+    for (int k = 0; k < kCols; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+// Two staged bytes -> an f16x2 of their values (exact: 1024 + b - 1024).
+__device__ __forceinline__ uint32_t bytes_f16x2(uint32_t lo, uint32_t hi) {
+    const uint32_t h = (lo | (hi << 16)) | 0x64006400u;
+    uint32_t d;
+    asm("sub.rn.f16x2 %0, %1, %2;" : "=r"(d) : "r"(h), "r"(0x64006400u));
+    return d;
+}
+
+// One pixel row of a panel: the 2R+1 staged bytes src[0 ..] as f16, then
+// zeros up to K = 16; chunk 0 at dst, chunk 1 at dst + lbo.
+template <int R>
+__device__ __forceinline__ void build_row(const uint8_t* src, unsigned char* dst, int lbo) {
+    constexpr int K = 2 * R + 1;
+    uint32_t w[8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const uint32_t lo = 2 * p < K ? src[2 * p] : 0u;
+        const uint32_t hi = 2 * p + 1 < K ? src[2 * p + 1] : 0u;
+        w[p] = 2 * p < K ? bytes_f16x2(lo, hi) : 0u;
+    }
+    *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
+    *reinterpret_cast<uint4*>(dst + lbo) = make_uint4(w[4], w[5], w[6], w[7]);
+}
+
+}  // namespace tc
+
+// One CTA: pixels x0 .. x0+127 (x0 = 128 blockIdx.x), output rows y0 ..
+// y0+th-1 (y0 = th blockIdx.y), relative disparities dz0 .. dz0+127 (dz0 =
+// 128 blockIdx.z). Same outputs as ncc_match_kernel<R> without a guide.
+template <int R>
+__global__ void __launch_bounds__(tc::kNT, 1)
+    ncc_tc_kernel(const uint8_t* __restrict__ Limg, size_t pl, const uint8_t* __restrict__ Rimg, size_t pr, Args a) {
+    using namespace tc;
+    constexpr int n = (2 * R + 1) * (2 * R + 1);
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kOffBar);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(smem + kOffSlot);
+    int4* colrec = reinterpret_cast<int4*>(smem + kOffCol);
+    unsigned long long* skey = reinterpret_cast<unsigned long long*>(smem + kOffKey);
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int q = warp & 3, h = warp >> 2;
+    const int m = 32 * q + lane;           // this thread's pixel = TMEM lane
+    const int c0 = 32 * q + kCols * h;     // first accumulator column it ranks
+    const int x0 = blockIdx.x * kM, x = x0 + m;
+    const int y0 = blockIdx.y * a.th;
+    const int rows = min(a.th, a.H - y0);
+    const int dz0 = blockIdx.z * kDB;
+    const int nd = min(kDB, a.D - dz0);
+    const int xb = x0 - a.dmin - dz0 - (kDB - 1);  // match column of accumulator column 0
+
+    if (tid == 0) {
+        dev::mbar_init(bar, 1);
+        dev::fence_barrier_init();
+    }
+    for (int i = tid; i < 2 * kM; i += tc::kNT) skey[i] = 0ull;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dev::smem_u32(slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = slot[0];
+    const uint32_t sbase = dev::smem_u32(smem);
+    uint32_t phase = 0;   // MMA commits waited for
+    uint32_t issued = 0;  // MMA commits issued (counted by every thread)
+    bool failed = false;
+
+    // stages image row r into staging buffer b, half s (0 entering, 1 leaving)
+    auto stage_row = [&](int b, int s, int r) {
+        uint8_t* dst = smem + kOffStage + b * kStage + s * (kSL + kSR);
+        const bool rin = r >= 0 && r < a.H;
+        for (int i = tid; i < kSL + kSR; i += tc::kNT) {
+            const bool left = i < kSL;
+            const int xx = left ? x0 - R + i : xb - R + (i - kSL);
+            const uint8_t* img = left ? Limg + (size_t)(rin ? r : 0) * pl : Rimg + (size_t)(rin ? r : 0) * pr;
+            dst[i] = (rin && xx >= 0 && xx < a.W) ? __ldg(img + xx) : uint8_t(0);
+        }
+    };
+    // the same staging split into the load (into a register, a step ahead)
+    // and the store: thread tid holds byte tid of half s of row r
+    auto fetch_byte = [&](int s, int r) -> uint32_t {
+        const int i = tid;
+        if (i >= kSL + kSR || r < 0 || r >= a.H) return 0u;
+        const bool left = i < kSL;
+        const int xx = left ? x0 - R + i : xb - R + (i - kSL);
+        if (xx < 0 || xx >= a.W) return 0u;
+        return left ? __ldg(Limg + (size_t)r * pl + xx) : __ldg(Rimg + (size_t)r * pr + xx);
+    };
+    auto store_byte = [&](int b, int s, uint32_t v) {
+        if (tid < kSL + kSR) smem[kOffStage + b * kStage + s * (kSL + kSR) + tid] = uint8_t(v);
+    };
+    // builds panels A, B of half s of panel set p from staging buffer b
+    auto build = [&](int p, int s, int b) {
+        const uint8_t* src = smem + kOffStage + b * kStage + s * (kSL + kSR);
+        unsigned char* set = smem + kOffSet + p * kSet;
+        for (int i = tid; i < kM + kN; i += tc::kNT) {
+            if (i < kM) tc::build_row<R>(src + i, set + s * kPA + i * 16, kM * 16);
+            else tc::build_row<R>(src + kSL + (i - kM), set + 2 * kPA + s * kPB + (i - kM) * 16, kN * 16);
+        }
+        dev::fence_proxy_async();  // generic-proxy writes -> the tensor core's reads
+    };
+    auto wait_mma = [&]() {
+        const bool ok = dev::mbar_wait_bounded(bar, phase & 1);
+        if (ok) ++phase;
+        return ok;
+    };
+    auto desc_a = [&](int p, int s) { return tc::sdesc(sbase + kOffSet + p * kSet + s * kPA, kM * 16); };
+    auto desc_b = [&](int p, int s) { return tc::sdesc(sbase + kOffSet + p * kSet + 2 * kPA + s * kPB, kN * 16); };
+    // column records of output row y into buffer b: {Sy, vy, n r, Sy r}
+    // (r ~ 1 / sqrt(vy)); columns whose window leaves the image are never
+    // read (outside every thread's column range below)
+    // column tid (tid < kN) of output row y: its Sy, vy (loaded a step
+    // before the record is stored)
+    auto fetch_col = [&](int y, int& sy, int& vy) {
+        const int xx = xb + tid;
+        sy = 0;
+        vy = -1;  // not a searchable column
+        if (tid < kN && xx >= R && xx < a.W - R && y >= 0 && y < a.H) {
+            const size_t o = (size_t)y * a.W + xx;
+            sy = a.Sy[o];
+            vy = a.Vy[o];
+        }
+    };
+    auto store_col = [&](int b, int sy, int vy) {
+        if (tid >= kN) return;
+        int4 rec = make_int4(0, 0, 0, 0);
+        if (vy >= 0) {
+            const float r = vy > 0 ? rsqrtf(__int2float_rn(vy)) : 0.0f;
+            rec = make_int4(sy, vy, __float_as_int(float(n) * r), __float_as_int(__int2float_rn(sy) * r));
+        }
+        colrec[b * kN + tid] = rec;
+    };
+    auto load_cols = [&](int b, int y) {
+        int sy, vy;
+        fetch_col(y, sy, vy);
+        store_col(b, sy, vy);
+    };
+
+    // ---- the strip's first window: rows y0 - R .. y0 + R -------------------
+    for (int k = 0; k <= 2 * R && !failed; ++k) {
+        stage_row(0, 0, y0 - R + k);
+        __syncthreads();
+        build(k & 1, 0, 0);
+        tc::fence_before();
+        __syncthreads();
+        if (warp == 0) {
+            tc::fence_after();
+            tc::mma(tmem, desc_a(k & 1, 0), desc_b(k & 1, 0), tc::idesc(false), k > 0);
+            tc::commit(bar);
+        }
+        ++issued;
+        if (__syncthreads_or(!wait_mma())) failed = true;
+    }
+    // the next step's rows (entering y0 + R + 1, leaving y0 - R) into buffer 1,
+    // their panels into set 1; the first row's column records into buffer 0
+    if (!failed) {
+        stage_row(1, 0, y0 + R + 1);
+        stage_row(1, 1, y0 - R);
+        load_cols(0, y0);
+        __syncthreads();
+        build(1, 0, 1);
+        build(1, 1, 1);
+        stage_row(0, 0, y0 + R + 2);
+        stage_row(0, 1, y0 - R + 1);
+    }
+    // loads in flight across a step: the staged bytes of the rows after next
+    // and the column inputs of the next row
+    uint32_t pf_in = fetch_byte(0, y0 + R + 3), pf_out = fetch_byte(1, y0 - R + 2);
+    int pf_sy, pf_vy;
+    fetch_col(y0 + 1, pf_sy, pf_vy);
+
+    // per pixel: Sx, float(vx), threshold; loaded a row ahead
+    auto pix = [&](int y, int& sx, float& fvx, int& tx, bool& ok) {
+        ok = x >= R && x < a.W - R && y >= R && y < a.H - R;
+        const size_t o = (size_t)(ok ? y : R) * a.W + (ok ? x : R);
+        sx = a.Sx[o];
+        fvx = __int2float_rn(a.Vx[o]);
+        tx = a.Tx[o];
+    };
+    int sx_n, tx_n;
+    float fvx_n;
+    bool ok_n;
+    pix(y0, sx_n, fvx_n, tx_n, ok_n);
+    // this thread's disparities: d = m + 127 - n for its columns n = c0 + j;
+    // searched iff jlo <= j <= jhi: d < nd, and the matched window inside the
+    // image (R <= xb + n < W - R)
+    const int jlo = max(m + kDB - nd - c0, R - xb - c0);
+    const int jhi = min(m + kDB - 1 - c0, a.W - R - 1 - xb - c0);
+
+    for (int oy = 0; oy < rows && !failed; ++oy) {
+        const int y = y0 + oy;
+        const int sx = sx_n, tx = tx_n;
+        const float fvx = fvx_n;
+        const bool pok = ok_n;
+        // ---- the window sums of row y: wait for them, read this thread's columns
+        if (phase < issued && __syncthreads_or(!wait_mma())) { failed = true; break; }
+        tc::fence_after();
+        float C[kCols];
+        tc::ld40(tmem + (uint32_t(32 * q) << 16) + uint32_t(c0), C);
+        tc::fence_before();
+        __syncthreads();  // the accumulator is read; panels and column records of the step are in place
+        // ---- next row: D(y + 1) = D(y) + entering row - leaving row
+        const int pb = (oy + 1) & 1;  // panel set of that update
+        if (oy + 1 < rows) {
+            if (warp == 0) {
+                tc::fence_after();
+                tc::mma(tmem, desc_a(pb, 0), desc_b(pb, 0), tc::idesc(false), true);
+                tc::mma(tmem, desc_a(pb, 1), desc_b(pb, 1), tc::idesc(true), true);
+                tc::commit(bar);
+            }
+            ++issued;
+        }
+        // ---- outputs of row y - 1 (its keys are complete)
+        if (oy > 0 && h == 0) {
+            const int yo = y - 1;
+            unsigned long long* kp = &skey[((oy - 1) & 1) * kM + m];
+            const unsigned long long key = *kp;
+            *kp = 0ull;
+            if (x < a.W) {
+                if (gridDim.z == 1) store_ncc(a, x, yo, x >= R && x < a.W - R && yo >= R && yo < a.H - R, key);
+                else if (key) atomicMax(&a.keys[(size_t)yo * a.W + x], key);
+            }
+        }
+        // ---- panels of the update after next (set oy & 1, free: D(y) is done),
+        // staging of the rows after that, column records of row y + 1
+        if (oy + 2 < rows) {
+            build(oy & 1, 0, oy & 1);
+            build(oy & 1, 1, oy & 1);
+        }
+        if (oy + 1 < rows) {
+            store_col((oy + 1) & 1, pf_sy, pf_vy);
+            fetch_col(y + 2, pf_sy, pf_vy);
+        }
+        if (oy + 3 < rows) {
+            // staging buffer (oy + 1) & 1 was read by the build of the previous step
+            store_byte((oy + 1) & 1, 0, pf_in);
+            store_byte((oy + 1) & 1, 1, pf_out);
+            pf_in = fetch_byte(0, y + R + 4);
+            pf_out = fetch_byte(1, y - R + 3);
+        }
+        if (oy + 1 < rows) pix(y + 1, sx_n, fvx_n, tx_n, ok_n);
+
+        // ---- rank this thread's disparities of row y
+        const int4* cr = colrec + (oy & 1) * kN + c0;
+        const float sxf = __int2float_rn(sx);
+        float best = -INFINITY, second = -INFINITY, mrmax = 0.0f;
+        float cbest = 0.0f;
+        int jbest = 0;
+        // the ranking estimate of column j (-inf outside the thread's range)
+        auto est_of = [&](int j, const int4& rec) {
+            const float e = rec.y >= tx ? fmaf(C[j], __int_as_float(rec.z), -sxf * __int_as_float(rec.w)) : 0.0f;
+            return (pok && j >= jlo && j <= jhi) ? e : -INFINITY;
+        };
+#pragma unroll
+        for (int j = 0; j < kCols; ++j) {
+            const int4 rec = cr[j];
+            const float v = est_of(j, rec);
+            const bool in = v > -INFINITY;
+            second = fmaxf(second, fminf(best, v));
+            const bool up = v >= best;  // ties: the lowest d (highest j)
+            best = up ? v : best;
+            cbest = up ? C[j] : cbest;
+            jbest = up ? j : jbest;
+            mrmax = in ? fmaxf(mrmax, __int_as_float(rec.z)) : mrmax;  // n r
+        }
+        // candidates: estimate >= best - 2 * 240 r_max - 4e-6 |best|
+        // (240 r = (240 / n) (n r))
+        // (no candidate at all when nothing was searched)
+        const float thr = best > -INFINITY ? best - (480.0f / float(n)) * mrmax - 4e-6f * fabsf(best) : INFINITY;
+        auto d_of = [&](int j) { return m + kDB - 1 - (c0 + j) + dz0; };  // relative to dmin
+        auto zero_key = [&](int j) {  // score +0 (sigma_x sigma_y < 1)
+            return ((unsigned long long)ordered(0.0f) << 32) | (0xFFFFFFFFu - uint32_t(d_of(j)));
+        };
+        // Candidates other than the best (rare): keys of the +0 scores at
+        // once, the others' integer sums kept for the IEEE scores below, so
+        // that no division runs while the 40 sums are live.
+        constexpr int kCand = 6;
+        int cj[kCand];
+        float cc[kCand];
+        int ncand = 0;
+        bool more = false;
+        unsigned long long key = 0ull;
+        if (__any_sync(0xffffffffu, best > -INFINITY && second >= thr)) {
+#pragma unroll
+            for (int j = 0; j < kCols; ++j) {
+                const int4 rec = cr[j];
+                if (j != jbest && est_of(j, rec) >= thr) {
+                    if (rec.y < tx) {
+                        const unsigned long long k2 = zero_key(j);
+                        key = k2 > key ? k2 : key;
+                    } else if (ncand < kCand) {
+#pragma unroll
+                        for (int t = 0; t < kCand; ++t)
+                            if (t == ncand) { cj[t] = j; cc[t] = C[j]; }
+                        ++ncand;
+                    } else {
+                        more = true;
+                    }
+                }
+            }
+        }
+        // IEEE score of column j with integer window sum c (exact in fp32)
+        auto exact_key = [&](float c, int j) {
+            const int4 rec = cr[j];
+            if (rec.y < tx) return zero_key(j);
+            const int num = n * __float2int_rn(c) - sx * rec.x;
+            const float sc = __fdiv_rn(__int2float_rn(num), __fsqrt_rn(__fmul_rn(fvx, __int2float_rn(rec.y))));
+            return ((unsigned long long)ordered(sc) << 32) | (0xFFFFFFFFu - uint32_t(d_of(j)));
+        };
+        if (more) {  // more near ties than kept (never seen): score all of them here
+#pragma unroll
+            for (int j = 0; j < kCols; ++j)
+                if (j != jbest && est_of(j, cr[j]) >= thr) {
+                    const unsigned long long k2 = exact_key(C[j], j);
+                    key = k2 > key ? k2 : key;
+                }
+        }
+        if (best > -INFINITY) {
+            const unsigned long long k1 = exact_key(cbest, jbest);
+            key = k1 > key ? k1 : key;
+        }
+#pragma unroll
+        for (int t = 0; t < kCand; ++t)
+            if (t < ncand) {
+                const unsigned long long k2 = exact_key(cc[t], cj[t]);
+                key = k2 > key ? k2 : key;
+            }
+        if (key) atomicMax(&skey[(oy & 1) * kM + m], key);
+    }
+    // ---- outputs of the last row
+    __syncthreads();
+    if (!failed && rows > 0 && h == 0) {
+        const int yo = y0 + rows - 1;
+        unsigned long long* kp = &skey[((rows - 1) & 1) * kM + m];
+        const unsigned long long key = *kp;
+        *kp = 0ull;
+        if (x < a.W) {
+            if (gridDim.z == 1) store_ncc(a, x, yo, x >= R && x < a.W - R && yo >= R && yo < a.H - R, key);
+            else if (key) atomicMax(&a.keys[(size_t)yo * a.W + x], key);
+        }
+    }
+    if (failed && tid == 0) dev::report(a.status, CT_ETIMEOUT);
+    // outstanding MMAs (a failed wait) complete before the TMEM is released
+    if (failed && warp == 0)
+        for (uint32_t k = phase; k < issued; ++k) dev::mbar_wait_bounded(bar, k & 1);
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    if (gridDim.z == 1) return;
+    // ---- D split over gridDim.z CTAs: the last of the (strip, column tile)
+    // group writes the merged keys as outputs and resets keys and counter
+    __threadfence();
+    __syncthreads();
+    int* last = reinterpret_cast<int*>(slot + 1);
+    if (tid == 0) {
+        uint32_t* ctr = &a.counters[blockIdx.y * gridDim.x + blockIdx.x];
+        const bool l = atomicAdd(ctr, 1u) == gridDim.z - 1;
+        if (l) *ctr = 0u;
+        *last = l;
+    }
+    __syncthreads();
+    if (!*last) return;
+    __threadfence();
+    for (int idx = tid; idx < rows * kM; idx += tc::kNT) {
+        const int oy = idx / kM, xx = x0 + idx % kM, yy = y0 + oy;
+        if (xx >= a.W) continue;
+        unsigned long long* kp = &a.keys[(size_t)yy * a.W + xx];
+        const unsigned long long key = __ldcg(kp);
+        *kp = 0ull;
+        store_ncc(a, xx, yy, xx >= R && xx < a.W - R && yy >= R && yy < a.H - R, key);
+    }
+}
+
+}  // namespace ncc
+}  // namespace ct

@@ -164,6 +164,7 @@ def _declare(L: C.CDLL) -> None:
         "ct_bm_census_tuning": [H, P(C.c_int32), P(C.c_int32)],
         "ct_bm_census_set_tuning": [H, C.c_int32, C.c_int32],
         "ct_bm_census_set_fused_lr": [H, C.c_int32],
+        "ct_bm_ncc_set_tensor_cores": [H, C.c_int32],
         "ct_bm_census_process_static": [img, img, img, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p],
         "ct_bm_census_static_status": [P(C.c_int32)],
         "ct_bm_set_gradient_gate": [H, C.c_float],
@@ -442,6 +443,10 @@ class BlockMatcherNCC(_Driver):
     def process(self, disp, left, right, score=None, disp_init=None, stream=None):
         check(lib().ct_bm_ncc_process(self._h, _img_ref(disp), _img_ref(score), _img_ref(left),
                                       _img_ref(right), _img_ref(disp_init), _stream(stream)))
+
+    def set_tensor_cores(self, enable: bool):
+        """Unguided matching on the tensor cores or on the CUDA cores (default); same maps."""
+        check(lib().ct_bm_ncc_set_tensor_cores(self._h, 1 if enable else 0))
 
 
 class BlockMatcherAW(_Driver):

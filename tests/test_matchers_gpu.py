@@ -209,3 +209,36 @@ def test_aw_guided_matches_oracle(ct, oracle, cuda, W, H, D, s, holes, ctype):
     assert m.device_status() == 0
     np.testing.assert_array_equal(out.cpu().numpy(), oracle.to_u8(d))
     np.testing.assert_array_equal(sub.cpu().numpy(), s32)
+
+
+@pytest.mark.parametrize("W,H,D,r,dmin", [
+    (67, 43, 13, 5, 0), (400, 150, 96, 5, 0), (150, 60, 40, 4, 0), (150, 60, 70, 2, 0),
+    (300, 100, 200, 5, 0),   # two blocks of 128 disparities, merged through global keys
+    (257, 90, 128, 5, 7),    # minimum disparity, ragged width
+    (129, 200, 128, 5, 0),   # one pixel past a 128-pixel tile, several strips
+])
+def test_ncc_tensor_cores_equal_cuda_cores(ct, oracle, cuda, W, H, D, r, dmin):
+    """Unguided NCC on the tensor cores gives the CUDA-core kernel's maps and
+    scores bit for bit (flat patches, noise-only rows and textured scenes)."""
+    L, R, _, _ = ct.synth_pair(2, 3 * W + D + dmin, W, H, dmin + D - 1)
+    L[5:25, 5:30] = 128                    # flat: the sigma < 1 rule
+    R[H // 2:H // 2 + 8] = np.random.default_rng(1).integers(0, 256, (8, W), dtype=np.uint8)  # no match
+    dl, dr = to_dev(L, cuda), to_dev(R, cuda)
+    res = {}
+    for tcores in (True, False):
+        m = ct.BlockMatcherNCC()
+        m.configure(0, W, H, D, radius=r, disp_min=dmin)
+        m.set_tensor_cores(tcores)
+        out = ct.alloc_image(H, W, torch.int16, cuda)
+        score = ct.alloc_image(H, W, torch.float32, cuda)
+        out.fill_(0x1111)
+        score.fill_(-7.0)
+        m.process(out, dl, dr, score=score)
+        torch.cuda.synchronize()
+        assert m.device_status() == 0
+        res[tcores] = (out.cpu().numpy().view(np.uint16), score.cpu().numpy())
+    np.testing.assert_array_equal(res[True][0], res[False][0])
+    np.testing.assert_array_equal(res[True][1].view(np.uint32), res[False][1].view(np.uint32))
+    if W * H * D <= 400 * 150 * 96:
+        d, s32, _ = oracle.match_ncc(L, R, D, r, dmin=dmin)
+        np.testing.assert_array_equal(res[True][0], oracle.to_u16(d))
