@@ -35,6 +35,8 @@
 // last-arriver merge of the CUDA-core kernel.
 #pragma once
 
+#include <type_traits>
+
 namespace ct {
 namespace ncc {
 namespace tc {
@@ -51,8 +53,9 @@ constexpr int kStage = 2 * (kSL + kSR);              // entering + leaving row
 // shared memory
 constexpr int kOffSet = 0;                        // 2 panel sets
 constexpr int kOffStage = 2 * kSet;               // 2 staging buffers
-constexpr int kOffCol = kOffStage + 2 * kStage;   // 2 rows x kN column records (int4)
-constexpr int kOffKey = kOffCol + 2 * kN * 16;    // 2 rows x kM merge keys
+constexpr int kOffCol = kOffStage + 2 * kStage;   // 3 rows x kN column records (int4)
+constexpr int kOffSy = kOffCol + 3 * kN * 16;     // 3 rows x kN column sums Sy
+constexpr int kOffKey = kOffSy + 3 * kN * 4;      // 2 rows x kM merge keys
 constexpr int kOffBar = kOffKey + 2 * kM * 8;     // MMA completion
 constexpr int kOffSlot = kOffBar + 8;             // TMEM address, group-last flag
 constexpr int kSmem = kOffSlot + 16;
@@ -110,6 +113,20 @@ __device__ __forceinline__ void ld40(uint32_t taddr, float (&v)[kCols]) {
     for (int k = 0; k < kCols; ++k) v[k] = __uint_as_float(r[k]);
 }
 
+// Column taddr of this thread's lane, waited for.
+__device__ __forceinline__ float ld1(uint32_t taddr) {
+    uint32_t r;
+    asm volatile(
+        "{\n"
+        "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n"
+        "tcgen05.wait::ld.sync.aligned;\n"
+        "}\n"
+        : "=r"(r)
+        : "r"(taddr)
+        : "memory");
+    return __uint_as_float(r);
+}
+
 // Two staged bytes -> an f16x2 of their values (exact: 1024 + b - 1024).
 __device__ __forceinline__ uint32_t bytes_f16x2(uint32_t lo, uint32_t hi) {
     const uint32_t h = (lo | (hi << 16)) | 0x64006400u;
@@ -148,6 +165,7 @@ __global__ void __launch_bounds__(tc::kNT, 1)
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kOffBar);
     uint32_t* slot = reinterpret_cast<uint32_t*>(smem + kOffSlot);
     int4* colrec = reinterpret_cast<int4*>(smem + kOffCol);
+    int* colsy = reinterpret_cast<int*>(smem + kOffSy);
     unsigned long long* skey = reinterpret_cast<unsigned long long*>(smem + kOffKey);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -237,14 +255,18 @@ __global__ void __launch_bounds__(tc::kNT, 1)
             vy = a.Vy[o];
         }
     };
+    // column record {vy, n r, Sy r, 240 r} (r ~ 1 / sqrt(vy); 240 r bounds
+    // the estimate's error) and Sy of column tid in buffer b
     auto store_col = [&](int b, int sy, int vy) {
         if (tid >= kN) return;
         int4 rec = make_int4(0, 0, 0, 0);
         if (vy >= 0) {
             const float r = vy > 0 ? rsqrtf(__int2float_rn(vy)) : 0.0f;
-            rec = make_int4(sy, vy, __float_as_int(float(n) * r), __float_as_int(__int2float_rn(sy) * r));
+            rec = make_int4(vy, __float_as_int(float(n) * r), __float_as_int(__int2float_rn(sy) * r),
+                            __float_as_int(240.0f * r));
         }
         colrec[b * kN + tid] = rec;
+        colsy[b * kN + tid] = sy;
     };
     auto load_cols = [&](int b, int y) {
         int sy, vy;
@@ -273,6 +295,7 @@ __global__ void __launch_bounds__(tc::kNT, 1)
         stage_row(1, 0, y0 + R + 1);
         stage_row(1, 1, y0 - R);
         load_cols(0, y0);
+        load_cols(1, y0 + 1);
         __syncthreads();
         build(1, 0, 1);
         build(1, 1, 1);
@@ -283,7 +306,7 @@ __global__ void __launch_bounds__(tc::kNT, 1)
     // and the column inputs of the next row
     uint32_t pf_in = fetch_byte(0, y0 + R + 3), pf_out = fetch_byte(1, y0 - R + 2);
     int pf_sy, pf_vy;
-    fetch_col(y0 + 1, pf_sy, pf_vy);
+    fetch_col(y0 + 2, pf_sy, pf_vy);
 
     // per pixel: Sx, float(vx), threshold; loaded a row ahead
     auto pix = [&](int y, int& sx, float& fvx, int& tx, bool& ok) {
@@ -303,19 +326,127 @@ __global__ void __launch_bounds__(tc::kNT, 1)
     const int jlo = max(m + kDB - nd - c0, R - xb - c0);
     const int jhi = min(m + kDB - 1 - c0, a.W - R - 1 - xb - c0);
 
+    // Step oy (output row y = y0 + oy): rank row y from D(y), then one
+    // barrier, then the update D(y) -> D(y + 1), the outputs of row y and the
+    // operands of the steps ahead. The slow path re-reads the accumulator,
+    // which stays D(y) until that barrier.
     for (int oy = 0; oy < rows && !failed; ++oy) {
         const int y = y0 + oy;
         const int sx = sx_n, tx = tx_n;
         const float fvx = fvx_n;
         const bool pok = ok_n;
-        // ---- the window sums of row y: wait for them, read this thread's columns
-        if (phase < issued && __syncthreads_or(!wait_mma())) { failed = true; break; }
+        const uint32_t tlane = tmem + (uint32_t(32 * q) << 16);
+        // ---- the window sums of row y
+        const bool ok = phase < issued ? wait_mma() : true;
         tc::fence_after();
-        float C[kCols];
-        tc::ld40(tmem + (uint32_t(32 * q) << 16) + uint32_t(c0), C);
+        const int4* cr = colrec + (oy % 3) * kN + c0;
+        const int* csy = colsy + (oy % 3) * kN + c0;
+        const float sxf = __int2float_rn(sx);
+        // Estimate of column j from its sum c (-inf outside the thread's range
+        // when MASK) and its error bound 240 r; exact (bound 0) when the score
+        // is +0 by sigma_x sigma_y < 1.
+        auto est_of = [&](float c, int j, const int4& rec, float& marg, bool mask) {
+            const bool zt = rec.x >= tx;
+            const float e = zt ? fmaf(c, __int_as_float(rec.y), -sxf * __int_as_float(rec.z)) : 0.0f;
+            marg = zt ? __int_as_float(rec.w) : 0.0f;
+            return (!mask || (pok && j >= jlo && j <= jhi)) ? e : -INFINITY;
+        };
+        // best estimate (ties: the lowest d, i.e. the highest j) and the two
+        // largest upper bounds estimate + bound, in 4 independent chains
+        float best, cbest, u1, u2;
+        int jbest;
+        {
+            float C[kCols];
+            tc::ld40(tlane + uint32_t(c0), C);  // garbage if the wait gave up (then unused)
+            float bv[4], bc[4], t1[4], t2[4];
+            int bj[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                bv[k] = t1[k] = t2[k] = -INFINITY;
+                bc[k] = 0.0f;
+                bj[k] = 0;
+            }
+            // every lane's columns all searched: no range test
+            const bool full = __all_sync(0xffffffffu, pok && jlo <= 0 && jhi >= kCols - 1);
+            auto pass = [&](auto masked) {
+#pragma unroll
+                for (int j = 0; j < kCols; ++j) {
+                    const int k = j & 3;
+                    const int4 rec = cr[j];
+                    float mg;
+                    const float v = est_of(C[j], j, rec, mg, decltype(masked)::value);
+                    const float u = v + mg;
+                    t2[k] = fmaxf(t2[k], fminf(t1[k], u));
+                    t1[k] = fmaxf(t1[k], u);
+                    const bool up = v >= bv[k];
+                    bv[k] = up ? v : bv[k];
+                    bc[k] = up ? C[j] : bc[k];
+                    bj[k] = up ? j : bj[k];
+                }
+            };
+            if (full) pass(std::integral_constant<bool, false>{});
+            else pass(std::integral_constant<bool, true>{});
+            best = bv[0];
+            cbest = bc[0];
+            jbest = bj[0];
+#pragma unroll
+            for (int k = 1; k < 4; ++k) {
+                const bool take = bv[k] > best || (bv[k] == best && bj[k] > jbest);
+                best = take ? bv[k] : best;
+                cbest = take ? bc[k] : cbest;
+                jbest = take ? bj[k] : jbest;
+            }
+            const float a0 = fmaxf(t1[0], t1[1]), b0 = fminf(t1[0], t1[1]);
+            const float a1 = fmaxf(t1[2], t1[3]), b1 = fminf(t1[2], t1[3]);
+            u1 = fmaxf(a0, a1);
+            u2 = fmaxf(fmaxf(fminf(a0, a1), fmaxf(b0, b1)), fmaxf(fmaxf(t2[0], t2[1]), fmaxf(t2[2], t2[3])));
+        }
+        float mbest;
+        {
+            const int4 rec = cr[jbest];
+            mbest = rec.x >= tx ? __int_as_float(rec.w) : 0.0f;
+        }
+        // Another column j can hold the exact maximum only if its upper bound
+        // u_j exceeds the best's lower bound (4e-6 |best| covers the relative
+        // error of r). The bounds are strict for inexact estimates, and equal
+        // exact estimates went to the lowest d above. Such a j exists iff the
+        // second largest upper bound exceeds the lower bound (jbest's own
+        // upper bound is at least as large as u_j, or u_j is the largest
+        // and then above jbest's) or the largest exceeds jbest's upper bound.
+        const float lower = best - mbest - 4e-6f * fabsf(best);
+        const bool searched = best > -INFINITY;
+        const bool others = u2 > lower || u1 > best + mbest;
+        auto d_of = [&](int j) { return m + kDB - 1 - (c0 + j) + dz0; };  // relative to dmin
+        // IEEE score of column j with window sum c (an exact integer in fp32)
+        auto exact_key = [&](float c, int j) {
+            const int4 rec = cr[j];
+            float sc = 0.0f;  // +0 when sigma_x sigma_y < 1
+            if (rec.x >= tx) {
+                const int num = n * __float2int_rn(c) - sx * csy[j];
+                sc = __fdiv_rn(__int2float_rn(num), __fsqrt_rn(__fmul_rn(fvx, __int2float_rn(rec.x))));
+            }
+            return ((unsigned long long)ordered(sc) << 32) | (0xFFFFFFFFu - uint32_t(d_of(j)));
+        };
+        unsigned long long key = searched ? exact_key(cbest, jbest) : 0ull;
+        // other candidates (rare): every lane of the warp re-reads each column
+        if (__any_sync(0xffffffffu, ok && searched && others)) {
+            for (int j = 0; j < kCols; ++j) {
+                const float c = tc::ld1(tlane + uint32_t(c0 + j));
+                const int4 rec = cr[j];
+                float mg;
+                const float v = est_of(c, j, rec, mg, true);
+                if (searched && j != jbest && v + mg > lower) {
+                    const unsigned long long k2 = exact_key(c, j);
+                    key = k2 > key ? k2 : key;
+                }
+            }
+        }
+        if (key) atomicMax(&skey[(oy & 1) * kM + m], key);
         tc::fence_before();
-        __syncthreads();  // the accumulator is read; panels and column records of the step are in place
-        // ---- next row: D(y + 1) = D(y) + entering row - leaving row
+        // the accumulator is read, the keys of row y are in, the operands of
+        // this step's update are in place
+        if (__syncthreads_or(!ok)) { failed = true; break; }
+        // ---- D(y + 1) = D(y) + entering row - leaving row
         const int pb = (oy + 1) & 1;  // panel set of that update
         if (oy + 1 < rows) {
             if (warp == 0) {
@@ -326,26 +457,26 @@ __global__ void __launch_bounds__(tc::kNT, 1)
             }
             ++issued;
         }
-        // ---- outputs of row y - 1 (its keys are complete)
-        if (oy > 0 && h == 0) {
-            const int yo = y - 1;
-            unsigned long long* kp = &skey[((oy - 1) & 1) * kM + m];
-            const unsigned long long key = *kp;
+        // ---- outputs of row y
+        if (h == 0) {
+            unsigned long long* kp = &skey[(oy & 1) * kM + m];
+            const unsigned long long kk = *kp;
             *kp = 0ull;
             if (x < a.W) {
-                if (gridDim.z == 1) store_ncc(a, x, yo, x >= R && x < a.W - R && yo >= R && yo < a.H - R, key);
-                else if (key) atomicMax(&a.keys[(size_t)yo * a.W + x], key);
+                if (gridDim.z == 1) store_ncc(a, x, y, x >= R && x < a.W - R && y >= R && y < a.H - R, kk);
+                else if (kk) atomicMax(&a.keys[(size_t)y * a.W + x], kk);
             }
         }
-        // ---- panels of the update after next (set oy & 1, free: D(y) is done),
-        // staging of the rows after that, column records of row y + 1
+        // ---- operands of the steps ahead: panels of the update after next
+        // (set oy & 1, free: D(y) is done), staged rows of the one after,
+        // column records of row y + 2 (read after the next barrier)
         if (oy + 2 < rows) {
             build(oy & 1, 0, oy & 1);
             build(oy & 1, 1, oy & 1);
         }
-        if (oy + 1 < rows) {
-            store_col((oy + 1) & 1, pf_sy, pf_vy);
-            fetch_col(y + 2, pf_sy, pf_vy);
+        if (oy + 2 < rows) {
+            store_col((oy + 2) % 3, pf_sy, pf_vy);
+            fetch_col(y + 3, pf_sy, pf_vy);
         }
         if (oy + 3 < rows) {
             // staging buffer (oy + 1) & 1 was read by the build of the previous step
@@ -355,105 +486,6 @@ __global__ void __launch_bounds__(tc::kNT, 1)
             pf_out = fetch_byte(1, y - R + 3);
         }
         if (oy + 1 < rows) pix(y + 1, sx_n, fvx_n, tx_n, ok_n);
-
-        // ---- rank this thread's disparities of row y
-        const int4* cr = colrec + (oy & 1) * kN + c0;
-        const float sxf = __int2float_rn(sx);
-        float best = -INFINITY, second = -INFINITY, mrmax = 0.0f;
-        float cbest = 0.0f;
-        int jbest = 0;
-        // the ranking estimate of column j (-inf outside the thread's range)
-        auto est_of = [&](int j, const int4& rec) {
-            const float e = rec.y >= tx ? fmaf(C[j], __int_as_float(rec.z), -sxf * __int_as_float(rec.w)) : 0.0f;
-            return (pok && j >= jlo && j <= jhi) ? e : -INFINITY;
-        };
-#pragma unroll
-        for (int j = 0; j < kCols; ++j) {
-            const int4 rec = cr[j];
-            const float v = est_of(j, rec);
-            const bool in = v > -INFINITY;
-            second = fmaxf(second, fminf(best, v));
-            const bool up = v >= best;  // ties: the lowest d (highest j)
-            best = up ? v : best;
-            cbest = up ? C[j] : cbest;
-            jbest = up ? j : jbest;
-            mrmax = in ? fmaxf(mrmax, __int_as_float(rec.z)) : mrmax;  // n r
-        }
-        // candidates: estimate >= best - 2 * 240 r_max - 4e-6 |best|
-        // (240 r = (240 / n) (n r))
-        // (no candidate at all when nothing was searched)
-        const float thr = best > -INFINITY ? best - (480.0f / float(n)) * mrmax - 4e-6f * fabsf(best) : INFINITY;
-        auto d_of = [&](int j) { return m + kDB - 1 - (c0 + j) + dz0; };  // relative to dmin
-        auto zero_key = [&](int j) {  // score +0 (sigma_x sigma_y < 1)
-            return ((unsigned long long)ordered(0.0f) << 32) | (0xFFFFFFFFu - uint32_t(d_of(j)));
-        };
-        // Candidates other than the best (rare): keys of the +0 scores at
-        // once, the others' integer sums kept for the IEEE scores below, so
-        // that no division runs while the 40 sums are live.
-        constexpr int kCand = 6;
-        int cj[kCand];
-        float cc[kCand];
-        int ncand = 0;
-        bool more = false;
-        unsigned long long key = 0ull;
-        if (__any_sync(0xffffffffu, best > -INFINITY && second >= thr)) {
-#pragma unroll
-            for (int j = 0; j < kCols; ++j) {
-                const int4 rec = cr[j];
-                if (j != jbest && est_of(j, rec) >= thr) {
-                    if (rec.y < tx) {
-                        const unsigned long long k2 = zero_key(j);
-                        key = k2 > key ? k2 : key;
-                    } else if (ncand < kCand) {
-#pragma unroll
-                        for (int t = 0; t < kCand; ++t)
-                            if (t == ncand) { cj[t] = j; cc[t] = C[j]; }
-                        ++ncand;
-                    } else {
-                        more = true;
-                    }
-                }
-            }
-        }
-        // IEEE score of column j with integer window sum c (exact in fp32)
-        auto exact_key = [&](float c, int j) {
-            const int4 rec = cr[j];
-            if (rec.y < tx) return zero_key(j);
-            const int num = n * __float2int_rn(c) - sx * rec.x;
-            const float sc = __fdiv_rn(__int2float_rn(num), __fsqrt_rn(__fmul_rn(fvx, __int2float_rn(rec.y))));
-            return ((unsigned long long)ordered(sc) << 32) | (0xFFFFFFFFu - uint32_t(d_of(j)));
-        };
-        if (more) {  // more near ties than kept (never seen): score all of them here
-#pragma unroll
-            for (int j = 0; j < kCols; ++j)
-                if (j != jbest && est_of(j, cr[j]) >= thr) {
-                    const unsigned long long k2 = exact_key(C[j], j);
-                    key = k2 > key ? k2 : key;
-                }
-        }
-        if (best > -INFINITY) {
-            const unsigned long long k1 = exact_key(cbest, jbest);
-            key = k1 > key ? k1 : key;
-        }
-#pragma unroll
-        for (int t = 0; t < kCand; ++t)
-            if (t < ncand) {
-                const unsigned long long k2 = exact_key(cc[t], cj[t]);
-                key = k2 > key ? k2 : key;
-            }
-        if (key) atomicMax(&skey[(oy & 1) * kM + m], key);
-    }
-    // ---- outputs of the last row
-    __syncthreads();
-    if (!failed && rows > 0 && h == 0) {
-        const int yo = y0 + rows - 1;
-        unsigned long long* kp = &skey[((rows - 1) & 1) * kM + m];
-        const unsigned long long key = *kp;
-        *kp = 0ull;
-        if (x < a.W) {
-            if (gridDim.z == 1) store_ncc(a, x, yo, x >= R && x < a.W - R && yo >= R && yo < a.H - R, key);
-            else if (key) atomicMax(&a.keys[(size_t)yo * a.W + x], key);
-        }
     }
     if (failed && tid == 0) dev::report(a.status, CT_ETIMEOUT);
     // outstanding MMAs (a failed wait) complete before the TMEM is released
