@@ -415,7 +415,19 @@ __global__ void __launch_bounds__(tc::kNT, 1)
         // and then above jbest's) or the largest exceeds jbest's upper bound.
         const float lower = best - mbest - 4e-6f * fabsf(best);
         const bool searched = best > -INFINITY;
-        const bool others = u2 > lower || u1 > best + mbest;
+        const bool others = ok && searched && (u2 > lower || u1 > best + mbest);
+        // those columns (rare), as a mask of j
+        uint32_t cm[2] = {0u, 0u};
+        if (__any_sync(0xffffffffu, others)) {
+            float C[kCols];
+            tc::ld40(tlane + uint32_t(c0), C);  // the same sums again
+#pragma unroll
+            for (int j = 0; j < kCols; ++j) {
+                float mg;
+                const float v = est_of(C[j], j, cr[j], mg, true);
+                cm[j >> 5] |= uint32_t(others && j != jbest && v + mg > lower) << (j & 31);
+            }
+        }
         auto d_of = [&](int j) { return m + kDB - 1 - (c0 + j) + dz0; };  // relative to dmin
         // IEEE score of column j with window sum c (an exact integer in fp32)
         auto exact_key = [&](float c, int j) {
@@ -428,14 +440,16 @@ __global__ void __launch_bounds__(tc::kNT, 1)
             return ((unsigned long long)ordered(sc) << 32) | (0xFFFFFFFFu - uint32_t(d_of(j)));
         };
         unsigned long long key = searched ? exact_key(cbest, jbest) : 0ull;
-        // other candidates (rare): every lane of the warp re-reads each column
-        if (__any_sync(0xffffffffu, ok && searched && others)) {
-            for (int j = 0; j < kCols; ++j) {
+        // the other candidates: the warp re-reads each column some lane needs
+        // (a warp-wide TMEM load) and scores it there
+        uint32_t wm[2] = {__reduce_or_sync(0xffffffffu, cm[0]), __reduce_or_sync(0xffffffffu, cm[1])};
+#pragma unroll
+        for (int w = 0; w < 2; ++w) {
+            while (wm[w]) {
+                const int j = 32 * w + __ffs(wm[w]) - 1;
+                wm[w] &= wm[w] - 1u;
                 const float c = tc::ld1(tlane + uint32_t(c0 + j));
-                const int4 rec = cr[j];
-                float mg;
-                const float v = est_of(c, j, rec, mg, true);
-                if (searched && j != jbest && v + mg > lower) {
+                if ((cm[w] >> (j & 31)) & 1u) {
                     const unsigned long long k2 = exact_key(c, j);
                     key = k2 > key ? k2 : key;
                 }
