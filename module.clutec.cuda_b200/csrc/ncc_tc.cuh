@@ -55,8 +55,8 @@ constexpr int kOffSet = 0;                        // 2 panel sets
 constexpr int kOffStage = 2 * kSet;               // 2 staging buffers
 constexpr int kOffCol = kOffStage + 2 * kStage;   // 3 rows x kN column records (int4)
 constexpr int kOffSy = kOffCol + 3 * kN * 16;     // 3 rows x kN column sums Sy
-constexpr int kOffKey = kOffSy + 3 * kN * 4;      // 2 rows x kM merge keys
-constexpr int kOffBar = kOffKey + 2 * kM * 8;     // MMA completion
+constexpr int kOffKey = kOffSy + 3 * kN * 4;      // 2 rows x 4 column slices x kM keys
+constexpr int kOffBar = kOffKey + 2 * 4 * kM * 8; // MMA completion
 constexpr int kOffSlot = kOffBar + 8;             // TMEM address, group-last flag
 constexpr int kSmem = kOffSlot + 16;
 static_assert(kOffStage % 1024 == 0 && kOffCol % 16 == 0 && kOffKey % 8 == 0 && kOffBar % 8 == 0, "alignment");
@@ -161,6 +161,7 @@ __global__ void __launch_bounds__(tc::kNT, 1)
     ncc_tc_kernel(const uint8_t* __restrict__ Limg, size_t pl, const uint8_t* __restrict__ Rimg, size_t pr, Args a) {
     using namespace tc;
     constexpr int n = (2 * R + 1) * (2 * R + 1);
+    constexpr int kSB = kSL + kSR;  // staged bytes of one image row
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kOffBar);
     uint32_t* slot = reinterpret_cast<uint32_t*>(smem + kOffSlot);
@@ -183,7 +184,6 @@ __global__ void __launch_bounds__(tc::kNT, 1)
         dev::mbar_init(bar, 1);
         dev::fence_barrier_init();
     }
-    for (int i = tid; i < 2 * kM; i += tc::kNT) skey[i] = 0ull;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dev::smem_u32(slot)),
                      "r"(kTmemCols)
@@ -199,38 +199,31 @@ __global__ void __launch_bounds__(tc::kNT, 1)
     uint32_t issued = 0;  // MMA commits issued (counted by every thread)
     bool failed = false;
 
-    // stages image row r into staging buffer b, half s (0 entering, 1 leaving)
-    auto stage_row = [&](int b, int s, int r) {
-        uint8_t* dst = smem + kOffStage + b * kStage + s * (kSL + kSR);
-        const bool rin = r >= 0 && r < a.H;
-        for (int i = tid; i < kSL + kSR; i += tc::kNT) {
-            const bool left = i < kSL;
-            const int xx = left ? x0 - R + i : xb - R + (i - kSL);
-            const uint8_t* img = left ? Limg + (size_t)(rin ? r : 0) * pl : Rimg + (size_t)(rin ? r : 0) * pr;
-            dst[i] = (rin && xx >= 0 && xx < a.W) ? __ldg(img + xx) : uint8_t(0);
-        }
-    };
-    // the same staging split into the load (into a register, a step ahead)
-    // and the store: thread tid holds byte tid of half s of row r
-    auto fetch_byte = [&](int s, int r) -> uint32_t {
-        const int i = tid;
-        if (i >= kSL + kSR || r < 0 || r >= a.H) return 0u;
+    // Byte b of a staging buffer: half s = b / kSB (0 the entering row, 1 the
+    // leaving row), index i = b % kSB: left view x0 - R + i (i < kSL), else
+    // right view xb - R + i - kSL; 0 outside the image.
+    auto fetch_byte = [&](int b, int r_in, int r_out) -> uint32_t {
+        const int s = b >= kSB, i = b - s * kSB, r = s ? r_out : r_in;
         const bool left = i < kSL;
         const int xx = left ? x0 - R + i : xb - R + (i - kSL);
-        if (xx < 0 || xx >= a.W) return 0u;
+        if (r < 0 || r >= a.H || xx < 0 || xx >= a.W) return 0u;
         return left ? __ldg(Limg + (size_t)r * pl + xx) : __ldg(Rimg + (size_t)r * pr + xx);
     };
-    auto store_byte = [&](int b, int s, uint32_t v) {
-        if (tid < kSL + kSR) smem[kOffStage + b * kStage + s * (kSL + kSR) + tid] = uint8_t(v);
+    // the whole staging buffer b (start of the strip)
+    auto stage_rows = [&](int b, int r_in, int r_out) {
+        for (int i = tid; i < 2 * kSB; i += tc::kNT) smem[kOffStage + b * kStage + i] = uint8_t(fetch_byte(i, r_in, r_out));
     };
-    // builds panels A, B of half s of panel set p from staging buffer b
-    auto build = [&](int p, int s, int b) {
-        const uint8_t* src = smem + kOffStage + b * kStage + s * (kSL + kSR);
+    // panel row k of panel set p (k < 2 (kM + kN): half k / (kM + kN), A rows
+    // first) from staging buffer b
+    auto build_item = [&](int p, int b, int k) {
+        const int s = k >= kM + kN, i = k - s * (kM + kN);
+        const uint8_t* src = smem + kOffStage + b * kStage + s * kSB;
         unsigned char* set = smem + kOffSet + p * kSet;
-        for (int i = tid; i < kM + kN; i += tc::kNT) {
-            if (i < kM) tc::build_row<R>(src + i, set + s * kPA + i * 16, kM * 16);
-            else tc::build_row<R>(src + kSL + (i - kM), set + 2 * kPA + s * kPB + (i - kM) * 16, kN * 16);
-        }
+        if (i < kM) tc::build_row<R>(src + i, set + s * kPA + i * 16, kM * 16);
+        else tc::build_row<R>(src + kSL + (i - kM), set + 2 * kPA + s * kPB + (i - kM) * 16, kN * 16);
+    };
+    auto build_all = [&](int p, int b) {
+        for (int k = tid; k < 2 * (kM + kN); k += tc::kNT) build_item(p, b, k);
         dev::fence_proxy_async();  // generic-proxy writes -> the tensor core's reads
     };
     auto wait_mma = [&]() {
@@ -240,45 +233,52 @@ __global__ void __launch_bounds__(tc::kNT, 1)
     };
     auto desc_a = [&](int p, int s) { return tc::sdesc(sbase + kOffSet + p * kSet + s * kPA, kM * 16); };
     auto desc_b = [&](int p, int s) { return tc::sdesc(sbase + kOffSet + p * kSet + 2 * kPA + s * kPB, kN * 16); };
-    // column records of output row y into buffer b: {Sy, vy, n r, Sy r}
-    // (r ~ 1 / sqrt(vy)); columns whose window leaves the image are never
-    // read (outside every thread's column range below)
-    // column tid (tid < kN) of output row y: its Sy, vy (loaded a step
-    // before the record is stored)
-    auto fetch_col = [&](int y, int& sy, int& vy) {
-        const int xx = xb + tid;
+    // column cx of output row y: its Sy, vy (loaded a step before the record
+    // is stored); columns whose window leaves the image are outside every
+    // thread's column range below (record 0)
+    auto fetch_col = [&](int cx, int y, int& sy, int& vy) {
+        const int xx = xb + cx;
         sy = 0;
         vy = -1;  // not a searchable column
-        if (tid < kN && xx >= R && xx < a.W - R && y >= 0 && y < a.H) {
+        if (xx >= R && xx < a.W - R && y >= 0 && y < a.H) {
             const size_t o = (size_t)y * a.W + xx;
             sy = a.Sy[o];
             vy = a.Vy[o];
         }
     };
-    // column record {vy, n r, Sy r, 240 r} (r ~ 1 / sqrt(vy); 240 r bounds
-    // the estimate's error) and Sy of column tid in buffer b
-    auto store_col = [&](int b, int sy, int vy) {
-        if (tid >= kN) return;
+    // column record {r, float(Sy), vy, 0} (r ~ 1 / sqrt(vy)) and Sy of
+    // column cx in buffer b
+    auto store_col = [&](int cx, int b, int sy, int vy) {
         int4 rec = make_int4(0, 0, 0, 0);
-        if (vy >= 0) {
-            const float r = vy > 0 ? rsqrtf(__int2float_rn(vy)) : 0.0f;
-            rec = make_int4(vy, __float_as_int(float(n) * r), __float_as_int(__int2float_rn(sy) * r),
-                            __float_as_int(240.0f * r));
-        }
-        colrec[b * kN + tid] = rec;
-        colsy[b * kN + tid] = sy;
+        if (vy >= 0)
+            rec = make_int4(__float_as_int(vy > 0 ? rsqrtf(__int2float_rn(vy)) : 0.0f),
+                            __float_as_int(__int2float_rn(sy)), vy, 0);
+        colrec[b * kN + cx] = rec;
+        colsy[b * kN + cx] = sy;
     };
-    auto load_cols = [&](int b, int y) {
-        int sy, vy;
-        fetch_col(y, sy, vy);
-        store_col(b, sy, vy);
+
+    // Duties after the barrier of a step, spread so that every warp's step
+    // takes about as long (the warps of column slices 0 and 3 rank with the
+    // range test): slices 1, 2 build the panels (3 panel rows a thread),
+    // slice 3 the column records (2 columns a thread), slice 0 the outputs,
+    // every thread one or two staged bytes.
+    const bool builder = h == 1 || h == 2;
+    const int bk0 = tid - kM;  // first panel row of a builder: bk0, bk0 + 256, bk0 + 512
+    const bool colder = h == 3;
+    const int cx0 = tid - 3 * kM;  // columns of slice 3's threads: cx0, cx0 + 128
+    auto build_mine = [&](int p, int b) {
+        if (!builder) return;
+#pragma unroll
+        for (int t = 0; t < 3; ++t) build_item(p, b, bk0 + 2 * kM * t);
+        dev::fence_proxy_async();
     };
 
     // ---- the strip's first window: rows y0 - R .. y0 + R -------------------
     for (int k = 0; k <= 2 * R && !failed; ++k) {
-        stage_row(0, 0, y0 - R + k);
+        stage_rows(0, y0 - R + k, y0 - R + k);
         __syncthreads();
-        build(k & 1, 0, 0);
+        for (int i = tid; i < kM + kN; i += tc::kNT) build_item(k & 1, 0, i);
+        dev::fence_proxy_async();
         tc::fence_before();
         __syncthreads();
         if (warp == 0) {
@@ -290,23 +290,30 @@ __global__ void __launch_bounds__(tc::kNT, 1)
         if (__syncthreads_or(!wait_mma())) failed = true;
     }
     // the next step's rows (entering y0 + R + 1, leaving y0 - R) into buffer 1,
-    // their panels into set 1; the first row's column records into buffer 0
+    // their panels into set 1; the first rows' column records into buffers
+    // 0, 1; buffer 0: the rows of the step after
     if (!failed) {
-        stage_row(1, 0, y0 + R + 1);
-        stage_row(1, 1, y0 - R);
-        load_cols(0, y0);
-        load_cols(1, y0 + 1);
+        stage_rows(1, y0 + R + 1, y0 - R);
+        for (int cx = tid; cx < kN; cx += tc::kNT) {
+            int sy, vy;
+            fetch_col(cx, y0, sy, vy);
+            store_col(cx, 0, sy, vy);
+            fetch_col(cx, y0 + 1, sy, vy);
+            store_col(cx, 1, sy, vy);
+        }
         __syncthreads();
-        build(1, 0, 1);
-        build(1, 1, 1);
-        stage_row(0, 0, y0 + R + 2);
-        stage_row(0, 1, y0 - R + 1);
+        build_all(1, 1);
+        stage_rows(0, y0 + R + 2, y0 - R + 1);
     }
     // loads in flight across a step: the staged bytes of the rows after next
-    // and the column inputs of the next row
-    uint32_t pf_in = fetch_byte(0, y0 + R + 3), pf_out = fetch_byte(1, y0 - R + 2);
-    int pf_sy, pf_vy;
-    fetch_col(y0 + 2, pf_sy, pf_vy);
+    // (bytes tid and tid + 512 of a buffer) and the column inputs of row y + 2
+    uint32_t pf0 = fetch_byte(tid, y0 + R + 3, y0 - R + 2);
+    uint32_t pf1 = tid + tc::kNT < 2 * kSB ? fetch_byte(tid + tc::kNT, y0 + R + 3, y0 - R + 2) : 0u;
+    int pf_sy0 = 0, pf_vy0 = -1, pf_sy1 = 0, pf_vy1 = -1;
+    if (colder) {
+        fetch_col(cx0, y0 + 2, pf_sy0, pf_vy0);
+        fetch_col(cx0 + kM, y0 + 2, pf_sy1, pf_vy1);
+    }
 
     // per pixel: Sx, float(vx), threshold; loaded a row ahead
     auto pix = [&](int y, int& sx, float& fvx, int& tx, bool& ok) {
@@ -328,8 +335,8 @@ __global__ void __launch_bounds__(tc::kNT, 1)
 
     // Step oy (output row y = y0 + oy): rank row y from D(y), then one
     // barrier, then the update D(y) -> D(y + 1), the outputs of row y and the
-    // operands of the steps ahead. The slow path re-reads the accumulator,
-    // which stays D(y) until that barrier.
+    // operands of the steps ahead. The rare near-tie path re-reads the
+    // accumulator, which stays D(y) until that barrier.
     for (int oy = 0; oy < rows && !failed; ++oy) {
         const int y = y0 + oy;
         const int sx = sx_n, tx = tx_n;
@@ -342,27 +349,32 @@ __global__ void __launch_bounds__(tc::kNT, 1)
         const int4* cr = colrec + (oy % 3) * kN + c0;
         const int* csy = colsy + (oy % 3) * kN + c0;
         const float sxf = __int2float_rn(sx);
-        // Estimate of column j from its sum c (-inf outside the thread's range
-        // when MASK) and its error bound 240 r; exact (bound 0) when the score
-        // is +0 by sigma_x sigma_y < 1.
-        auto est_of = [&](float c, int j, const int4& rec, float& marg, bool mask) {
-            const bool zt = rec.x >= tx;
-            const float e = zt ? fmaf(c, __int_as_float(rec.y), -sxf * __int_as_float(rec.z)) : 0.0f;
-            marg = zt ? __int_as_float(rec.w) : 0.0f;
+        // Estimate of column j from its sum c: num * r with num = n c - Sx Sy
+        // in fp32 with Sx Sy split exactly into a rounded product and its
+        // error (an fma), so that the estimate's error is relative only (at
+        // most 2^-23 of num, 2^-24 of the product and the error of r, ~1e-6
+        // in all); 0 when the score is +0 by sigma_x sigma_y < 1, -inf
+        // outside the thread's range (MASK).
+        auto est_of = [&](float c, int j, const int4& rec, bool mask) {
+            const float syf = __int_as_float(rec.y);
+            const float ph = __fmul_rn(sxf, syf);
+            const float plo = fmaf(sxf, syf, -ph);
+            const float num = __fsub_rn(fmaf(float(n), c, -ph), plo);
+            const float e = rec.z >= tx ? num * __int_as_float(rec.x) : 0.0f;
             return (!mask || (pok && j >= jlo && j <= jhi)) ? e : -INFINITY;
         };
-        // best estimate (ties: the lowest d, i.e. the highest j) and the two
-        // largest upper bounds estimate + bound, in 4 independent chains
-        float best, cbest, u1, u2;
+        // best estimate (ties: the lowest d, i.e. the highest j) and the
+        // second largest, in 4 independent chains
+        float best, cbest, v2;
         int jbest;
         {
             float C[kCols];
             tc::ld40(tlane + uint32_t(c0), C);  // garbage if the wait gave up (then unused)
-            float bv[4], bc[4], t1[4], t2[4];
+            float bv[4], bc[4], t2[4];
             int bj[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                bv[k] = t1[k] = t2[k] = -INFINITY;
+                bv[k] = t2[k] = -INFINITY;
                 bc[k] = 0.0f;
                 bj[k] = 0;
             }
@@ -372,12 +384,8 @@ __global__ void __launch_bounds__(tc::kNT, 1)
 #pragma unroll
                 for (int j = 0; j < kCols; ++j) {
                     const int k = j & 3;
-                    const int4 rec = cr[j];
-                    float mg;
-                    const float v = est_of(C[j], j, rec, mg, decltype(masked)::value);
-                    const float u = v + mg;
-                    t2[k] = fmaxf(t2[k], fminf(t1[k], u));
-                    t1[k] = fmaxf(t1[k], u);
+                    const float v = est_of(C[j], j, cr[j], decltype(masked)::value);
+                    t2[k] = fmaxf(t2[k], fminf(bv[k], v));
                     const bool up = v >= bv[k];
                     bv[k] = up ? v : bv[k];
                     bc[k] = up ? C[j] : bc[k];
@@ -396,46 +404,36 @@ __global__ void __launch_bounds__(tc::kNT, 1)
                 cbest = take ? bc[k] : cbest;
                 jbest = take ? bj[k] : jbest;
             }
-            const float a0 = fmaxf(t1[0], t1[1]), b0 = fminf(t1[0], t1[1]);
-            const float a1 = fmaxf(t1[2], t1[3]), b1 = fminf(t1[2], t1[3]);
-            u1 = fmaxf(a0, a1);
-            u2 = fmaxf(fmaxf(fminf(a0, a1), fmaxf(b0, b1)), fmaxf(fmaxf(t2[0], t2[1]), fmaxf(t2[2], t2[3])));
+            const float a0 = fmaxf(bv[0], bv[1]), b0 = fminf(bv[0], bv[1]);
+            const float a1 = fmaxf(bv[2], bv[3]), b1 = fminf(bv[2], bv[3]);
+            v2 = fmaxf(fmaxf(fminf(a0, a1), fmaxf(b0, b1)), fmaxf(fmaxf(t2[0], t2[1]), fmaxf(t2[2], t2[3])));
         }
-        float mbest;
-        {
-            const int4 rec = cr[jbest];
-            mbest = rec.x >= tx ? __int_as_float(rec.w) : 0.0f;
-        }
-        // Another column j can hold the exact maximum only if its upper bound
-        // u_j exceeds the best's lower bound (4e-6 |best| covers the relative
-        // error of r). The bounds are strict for inexact estimates, and equal
-        // exact estimates went to the lowest d above. Such a j exists iff the
-        // second largest upper bound exceeds the lower bound (jbest's own
-        // upper bound is at least as large as u_j, or u_j is the largest
-        // and then above jbest's) or the largest exceeds jbest's upper bound.
-        const float lower = best - mbest - 4e-6f * fabsf(best);
+        // Another column j can hold the exact maximum (the IEEE scores round
+        // the same quantity num / sqrt(vx vy), within a few 2^-24) only if
+        // its estimate is above best - 4e-6 |best|; exact estimates (0, the
+        // score +0) are equal only to each other, and those went to the
+        // lowest d above. Such a j exists iff the second largest estimate is
+        // above that bound.
+        const float lower = best - 4e-6f * fabsf(best);
         const bool searched = best > -INFINITY;
-        const bool others = ok && searched && (u2 > lower || u1 > best + mbest);
+        const bool others = ok && searched && v2 > lower;
         // those columns (rare), as a mask of j
         uint32_t cm[2] = {0u, 0u};
         if (__any_sync(0xffffffffu, others)) {
             float C[kCols];
             tc::ld40(tlane + uint32_t(c0), C);  // the same sums again
 #pragma unroll
-            for (int j = 0; j < kCols; ++j) {
-                float mg;
-                const float v = est_of(C[j], j, cr[j], mg, true);
-                cm[j >> 5] |= uint32_t(others && j != jbest && v + mg > lower) << (j & 31);
-            }
+            for (int j = 0; j < kCols; ++j)
+                cm[j >> 5] |= uint32_t(others && j != jbest && est_of(C[j], j, cr[j], true) > lower) << (j & 31);
         }
         auto d_of = [&](int j) { return m + kDB - 1 - (c0 + j) + dz0; };  // relative to dmin
         // IEEE score of column j with window sum c (an exact integer in fp32)
         auto exact_key = [&](float c, int j) {
-            const int4 rec = cr[j];
+            const int vy = cr[j].z;
             float sc = 0.0f;  // +0 when sigma_x sigma_y < 1
-            if (rec.x >= tx) {
+            if (vy >= tx) {
                 const int num = n * __float2int_rn(c) - sx * csy[j];
-                sc = __fdiv_rn(__int2float_rn(num), __fsqrt_rn(__fmul_rn(fvx, __int2float_rn(rec.x))));
+                sc = __fdiv_rn(__int2float_rn(num), __fsqrt_rn(__fmul_rn(fvx, __int2float_rn(vy))));
             }
             return ((unsigned long long)ordered(sc) << 32) | (0xFFFFFFFFu - uint32_t(d_of(j)));
         };
@@ -455,7 +453,7 @@ __global__ void __launch_bounds__(tc::kNT, 1)
                 }
             }
         }
-        if (key) atomicMax(&skey[(oy & 1) * kM + m], key);
+        skey[((oy & 1) * 4 + h) * kM + m] = key;  // this column slice's best for pixel m
         tc::fence_before();
         // the accumulator is read, the keys of row y are in, the operands of
         // this step's update are in place
@@ -471,33 +469,33 @@ __global__ void __launch_bounds__(tc::kNT, 1)
             }
             ++issued;
         }
-        // ---- outputs of row y
+        // ---- outputs of row y (slice 0: its own pixel)
         if (h == 0) {
-            unsigned long long* kp = &skey[(oy & 1) * kM + m];
-            const unsigned long long kk = *kp;
-            *kp = 0ull;
+            const unsigned long long* kp = &skey[(oy & 1) * 4 * kM + m];
+            const unsigned long long kk = max(max(kp[0], kp[kM]), max(kp[2 * kM], kp[3 * kM]));
             if (x < a.W) {
                 if (gridDim.z == 1) store_ncc(a, x, y, x >= R && x < a.W - R && y >= R && y < a.H - R, kk);
                 else if (kk) atomicMax(&a.keys[(size_t)y * a.W + x], kk);
             }
         }
         // ---- operands of the steps ahead: panels of the update after next
-        // (set oy & 1, free: D(y) is done), staged rows of the one after,
-        // column records of row y + 2 (read after the next barrier)
-        if (oy + 2 < rows) {
-            build(oy & 1, 0, oy & 1);
-            build(oy & 1, 1, oy & 1);
-        }
-        if (oy + 2 < rows) {
-            store_col((oy + 2) % 3, pf_sy, pf_vy);
-            fetch_col(y + 3, pf_sy, pf_vy);
+        // (set oy & 1, free: D(y) is done) from staging buffer oy & 1, column
+        // records of row y + 2 (read after the next barrier), staged rows of
+        // the update after that into staging buffer (oy + 1) & 1 (read by the
+        // previous step's build)
+        if (oy + 2 < rows) build_mine(oy & 1, oy & 1);
+        if (oy + 2 < rows && colder) {
+            store_col(cx0, (oy + 2) % 3, pf_sy0, pf_vy0);
+            store_col(cx0 + kM, (oy + 2) % 3, pf_sy1, pf_vy1);
+            fetch_col(cx0, y + 3, pf_sy0, pf_vy0);
+            fetch_col(cx0 + kM, y + 3, pf_sy1, pf_vy1);
         }
         if (oy + 3 < rows) {
-            // staging buffer (oy + 1) & 1 was read by the build of the previous step
-            store_byte((oy + 1) & 1, 0, pf_in);
-            store_byte((oy + 1) & 1, 1, pf_out);
-            pf_in = fetch_byte(0, y + R + 4);
-            pf_out = fetch_byte(1, y - R + 3);
+            unsigned char* st = smem + kOffStage + ((oy + 1) & 1) * kStage;
+            st[tid] = uint8_t(pf0);
+            if (tid + tc::kNT < 2 * kSB) st[tid + tc::kNT] = uint8_t(pf1);
+            pf0 = fetch_byte(tid, y + R + 4, y - R + 3);
+            pf1 = tid + tc::kNT < 2 * kSB ? fetch_byte(tid + tc::kNT, y + R + 4, y - R + 3) : 0u;
         }
         if (oy + 1 < rows) pix(y + 1, sx_n, fvx_n, tx_n, ok_n);
     }
