@@ -796,6 +796,7 @@ def workload_line(wl, args, ct, dev, stream, flush_buf, world, rank, local, rate
     import numpy as np
     import torch
     oracle, march = cpu_oracle()  # CPU baseline leg and post-timing parity check only
+    alt_kernel = None
     unit = UNIT
 
     def up(a):
@@ -941,7 +942,11 @@ def workload_line(wl, args, ct, dev, stream, flush_buf, world, rank, local, rate
             step = lambda: m.process(out, dL, dR, score=score, stream=stream)
             check_fn = lambda: np.array_equal(out.cpu().numpy(), oracle.to_u8(oracle.match_ncc(L, R, D, 5)[0]))
             cpu_fn = lambda: oracle.match_ncc(L, R, D, 5)
-            metric, launches = "Mpix*disp/s NCC 11x11 FP32, 1920x1080 D=128", 4
+            metric, launches = "Mpix*disp/s NCC 11x11 FP32, 1920x1080 D=128", 3  # statistics x 2, matcher
+            # the same step with the window sums on the CUDA cores, timed
+            # after the headline timing for comparison
+            alt_kernel = (m.set_tensor_cores,
+                          lambda: (out.cpu().numpy().copy(), score.cpu().numpy().view(np.uint32).copy()))
         elif wl == "ncc1080g":
             # coarse-to-fine: census + L-R check on the 4x box-averaged pair
             # (480x270, D=32; the pyramid level is prepared on the host, as a
@@ -988,6 +993,8 @@ def workload_line(wl, args, ct, dev, stream, flush_buf, world, rank, local, rate
             metric, launches = "Mpix*disp/s adaptive window (5 x 7x7) + sub-pixel, 2560x1440 D=256", 2
         units = W * H * D
         cfg = {"workload": f"{wl}", "width": W, "height": H, "D": D}
+        if wl == "ncc1080":
+            cfg.update(window_sums="tensor cores (ncc_tc_kernel: tcgen05 kind::f16 MMAs, fp32 sums in TMEM)")
         if wl == "ncc1080g":
             units, unit = 1e6, "frames/s"  # value = frames per second
             cfg.update(coarse="480x270 D=32 census 9x7 + 5x5 + L-R check (tol 1) of the 4x box-averaged pair",
@@ -1013,6 +1020,27 @@ def workload_line(wl, args, ct, dev, stream, flush_buf, world, rank, local, rate
     clocks = clk.summary()
     ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev) / args.steps, world, dev)
     value = world * units / (ms * 1e-3) / 1e6
+    alt_line = None
+    if alt_kernel is not None:  # the CUDA-core kernel on the same step, same timing rules
+        set_tc, snap = alt_kernel
+        maps_tc = snap()
+        set_tc(False)
+        for _ in range(max(3, args.warmup)):
+            flush_buf.zero_()
+            step()
+        ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush_buf.zero_()
+            ev2[k][0].record(stream)
+            step()
+            ev2[k][1].record(stream)
+        torch.cuda.synchronize(dev)
+        ms2 = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev2) / args.steps, world, dev)
+        maps_cc = snap()
+        set_tc(True)
+        alt_line = {"kernel": "ncc_match_kernel (window sums on the CUDA cores)", "ms_per_step": round(ms2, 4),
+                    "value": round(world * units / (ms2 * 1e-3) / 1e6, 1),
+                    "same_maps_and_scores": bool(all(np.array_equal(a, b) for a, b in zip(maps_tc, maps_cc)))}
     out_line = {
         "metric": metric, "value": round(value, 1), "unit": unit, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
@@ -1021,6 +1049,8 @@ def workload_line(wl, args, ct, dev, stream, flush_buf, world, rank, local, rate
         "data": "synthetic (seeded generator)", "config": dict(cfg, l2="flushed before every timed step"),
         "gpu_launches": launches * args.steps, "clocks": clocks,
     }
+    if alt_line is not None:
+        out_line["cuda_core_kernel"] = alt_line
     if wl in ("mip1080", "map3d1080"):
         out_line["dtype"] = "u16 codes / fp32 levels" if wl == "mip1080" else "u16 codes / fp32 points"
         try:

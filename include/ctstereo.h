@@ -297,9 +297,10 @@ int ct_bm_ncc_configure(ct_handle* h, int32_t device, const ct_format* fmt, cons
 int ct_bm_ncc_process(ct_handle* h, const ct_image* disp, const ct_image* score,
                       const ct_image* left, const ct_image* right, const ct_image* disp_init,
                       ct_stream stream);
-/* enable = 1: unguided matching computes the window cross sums on the tensor
- * cores (tcgen05 MMAs on f16 pixels, exact fp32 sums; same maps and scores
- * as the CUDA-core kernel, which guided matching always uses). Default 0. */
+/* enable = 1 (the default): unguided matching computes the window cross sums
+ * on the tensor cores (tcgen05 MMAs on f16 pixels, exact fp32 sums); 0: on
+ * the CUDA cores, as guided matching always does. Both give the same maps
+ * and scores. */
 int ct_bm_ncc_set_tensor_cores(ct_handle* h, int32_t enable);
 
 /* ---- adaptive-window block matcher: BlockMatcherAW1 / AW2 ----------------

@@ -419,7 +419,7 @@ struct NccHandle : ct_handle {
     uint32_t* guide = nullptr;  // guided mode: one search range per 16 x 16 block
     uint32_t* counters = nullptr;  // one per (strip, column tile) at the smallest strip height
     int th = 32;
-    int tensor_cores = 0;  // unguided matching: window cross sums on the tensor cores (ncc_tc_kernel)
+    int tensor_cores = 1;  // unguided matching: window cross sums on the tensor cores (ncc_tc_kernel)
     int th_tc = 64;        // its strip height
 };
 
@@ -465,12 +465,12 @@ int launch_ncc(NccHandle* h, const ct_image* disp, const ct_image* score, const 
         static bool attr_tc = false;
         if (!attr_tc) {
             CT_CUDA_TRY(cudaFuncSetAttribute(ncc_tc_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             tc::kSmem));
+                                             tc::smem_bytes<R>()));
             attr_tc = true;
         }
         a.th = h->th_tc;
         dim3 grid((W + tc::kM - 1) / tc::kM, (H + a.th - 1) / a.th, (a.D + tc::kDB - 1) / tc::kDB);
-        ncc_tc_kernel<R><<<grid, tc::kNT, tc::kSmem, s>>>(static_cast<const uint8_t*>(L->ptr), L->pitch_bytes,
+        ncc_tc_kernel<R><<<grid, tc::kNT, tc::smem_bytes<R>(), s>>>(static_cast<const uint8_t*>(L->ptr), L->pitch_bytes,
                                                          static_cast<const uint8_t*>(Rr->ptr), Rr->pitch_bytes, a);
         CT_LAUNCH_CHECK();
         return gate_launch(disp, score, L, 0, 2 * R + 1, h->grad_thresh, s);  // EvalGrad (NCC.cu:388-413)

@@ -47,7 +47,8 @@ constexpr int kDB = 128;   // disparities per CTA
 constexpr int kNT = 512;   // 16 warps: 4 per TMEM lane quarter
 constexpr int kCols = 40;  // accumulator columns a thread ranks per row
 constexpr int kPA = kM * 16 * 2, kPB = kN * 16 * 2;  // panel bytes (K = 16 f16)
-constexpr int kSet = 2 * (kPA + kPB);                // entering + leaving row
+constexpr int kPanel = kPA + kPB;                    // one image row's A and B panels
+constexpr int kSet = 2 * kPanel;                     // entering + leaving row
 constexpr int kSL = kM + 16, kSR = kN + 16;          // staged bytes of one row (>= 128 + 2R, 256 + 2R)
 constexpr int kStage = 2 * (kSL + kSR);              // entering + leaving row
 // shared memory
@@ -55,11 +56,16 @@ constexpr int kOffSet = 0;                        // 2 panel sets
 constexpr int kOffStage = 2 * kSet;               // 2 staging buffers
 constexpr int kOffCol = kOffStage + 2 * kStage;   // 3 rows x kN column records (int4)
 constexpr int kOffSy = kOffCol + 3 * kN * 16;     // 3 rows x kN column sums Sy
-constexpr int kOffKey = kOffSy + 3 * kN * 4;      // 2 rows x 4 column slices x kM keys
+constexpr int kOffPix = kOffSy + 3 * kN * 4;      // 3 rows x kM pixel records (int4)
+constexpr int kOffKey = kOffPix + 3 * kM * 16;    // 2 rows x 4 column slices x kM keys
 constexpr int kOffBar = kOffKey + 2 * 4 * kM * 8; // MMA completion
 constexpr int kOffSlot = kOffBar + 8;             // TMEM address, group-last flag
-constexpr int kSmem = kOffSlot + 16;
-static_assert(kOffStage % 1024 == 0 && kOffCol % 16 == 0 && kOffKey % 8 == 0 && kOffBar % 8 == 0, "alignment");
+// the strip's first window: its 2R+1 rows' panels and staged bytes
+constexpr int kOffInit = (kOffSlot + 16 + 1023) / 1024 * 1024;
+template <int R>
+constexpr int smem_bytes() { return kOffInit + (2 * R + 1) * (kPanel + kSL + kSR); }
+static_assert(kOffStage % 1024 == 0 && kOffCol % 16 == 0 && kOffPix % 16 == 0 && kOffKey % 8 == 0 &&
+                  kOffBar % 8 == 0, "alignment");
 constexpr uint32_t kTmemCols = 256;
 
 // Instruction descriptor, kind::f16: D fp32 (bit 4), A and B f16 (bits 7, 10
@@ -168,6 +174,7 @@ __global__ void __launch_bounds__(tc::kNT, 1)
     int4* colrec = reinterpret_cast<int4*>(smem + kOffCol);
     int* colsy = reinterpret_cast<int*>(smem + kOffSy);
     unsigned long long* skey = reinterpret_cast<unsigned long long*>(smem + kOffKey);
+    int4* pixrec = reinterpret_cast<int4*>(smem + kOffPix);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int q = warp & 3, h = warp >> 2;
@@ -273,26 +280,18 @@ __global__ void __launch_bounds__(tc::kNT, 1)
         dev::fence_proxy_async();
     };
 
-    // ---- the strip's first window: rows y0 - R .. y0 + R -------------------
-    for (int k = 0; k <= 2 * R && !failed; ++k) {
-        stage_rows(0, y0 - R + k, y0 - R + k);
-        __syncthreads();
-        for (int i = tid; i < kM + kN; i += tc::kNT) build_item(k & 1, 0, i);
-        dev::fence_proxy_async();
-        tc::fence_before();
-        __syncthreads();
-        if (warp == 0) {
-            tc::fence_after();
-            tc::mma(tmem, desc_a(k & 1, 0), desc_b(k & 1, 0), tc::idesc(false), k > 0);
-            tc::commit(bar);
+    // ---- the strip's first window D(y0), rows y0 - R .. y0 + R: all rows
+    // staged and built at once (panels of their own after the rest of the
+    // shared memory), one MMA each, one commit. With it: the rows of the
+    // first update (entering y0 + R + 1, leaving y0 - R) into staging buffer
+    // 1 and panel set 1, the first two rows' column records.
+    {
+        constexpr int NW = 2 * R + 1;
+        uint8_t* istage = smem + kOffInit + NW * kPanel;
+        for (int i = tid; i < NW * kSB; i += tc::kNT) {
+            const int k = i / kSB;
+            istage[i] = uint8_t(fetch_byte(i - k * kSB, y0 - R + k, 0));
         }
-        ++issued;
-        if (__syncthreads_or(!wait_mma())) failed = true;
-    }
-    // the next step's rows (entering y0 + R + 1, leaving y0 - R) into buffer 1,
-    // their panels into set 1; the first rows' column records into buffers
-    // 0, 1; buffer 0: the rows of the step after
-    if (!failed) {
         stage_rows(1, y0 + R + 1, y0 - R);
         for (int cx = tid; cx < kN; cx += tc::kNT) {
             int sy, vy;
@@ -302,7 +301,28 @@ __global__ void __launch_bounds__(tc::kNT, 1)
             store_col(cx, 1, sy, vy);
         }
         __syncthreads();
-        build_all(1, 1);
+        for (int i = tid; i < NW * (kM + kN); i += tc::kNT) {
+            const int k = i / (kM + kN), t = i - k * (kM + kN);
+            const uint8_t* src = istage + k * kSB;
+            unsigned char* pan = smem + kOffInit + k * kPanel;
+            if (t < kM) tc::build_row<R>(src + t, pan + t * 16, kM * 16);
+            else tc::build_row<R>(src + kSL + (t - kM), pan + kPA + (t - kM) * 16, kN * 16);
+        }
+        build_all(1, 1);  // ends with the proxy fence
+        tc::fence_before();
+        __syncthreads();
+        if (warp == 0) {
+            tc::fence_after();
+#pragma unroll
+            for (int k = 0; k < NW; ++k) {
+                const uint32_t pa = sbase + uint32_t(kOffInit + k * kPanel);
+                tc::mma(tmem, tc::sdesc(pa, kM * 16), tc::sdesc(pa + kPA, kN * 16), tc::idesc(false), k > 0);
+            }
+            tc::commit(bar);
+        }
+        ++issued;
+        // staging buffer 0: the rows of the update after (y0 + R + 2 in,
+        // y0 - R + 1 out)
         stage_rows(0, y0 + R + 2, y0 - R + 1);
     }
     // loads in flight across a step: the staged bytes of the rows after next
@@ -315,18 +335,24 @@ __global__ void __launch_bounds__(tc::kNT, 1)
         fetch_col(cx0 + kM, y0 + 2, pf_sy1, pf_vy1);
     }
 
-    // per pixel: Sx, float(vx), threshold; loaded a row ahead
-    auto pix = [&](int y, int& sx, float& fvx, int& tx, bool& ok) {
-        ok = x >= R && x < a.W - R && y >= R && y < a.H - R;
-        const size_t o = (size_t)(ok ? y : R) * a.W + (ok ? x : R);
-        sx = a.Sx[o];
-        fvx = __int2float_rn(a.Vx[o]);
-        tx = a.Tx[o];
+    // Pixel records {Sx, float(vx), threshold Tx, inside} of output row y:
+    // slice 0's thread of pixel m loads them a step before it stores them,
+    // two steps before they are read.
+    auto fetch_pix = [&](int y, int4& p) {
+        const bool in = x >= R && x < a.W - R && y >= R && y < a.H - R;
+        const size_t o = (size_t)(in ? y : R) * a.W + (in ? x : R);
+        p = make_int4(a.Sx[o], __float_as_int(__int2float_rn(a.Vx[o])), a.Tx[o], in);
     };
-    int sx_n, tx_n;
-    float fvx_n;
-    bool ok_n;
-    pix(y0, sx_n, fvx_n, tx_n, ok_n);
+    int4 pf_pix = make_int4(0, 0, 0, 0);
+    if (h == 0) {
+        int4 p;
+        fetch_pix(y0, p);
+        pixrec[m] = p;
+        fetch_pix(y0 + 1, p);
+        pixrec[kM + m] = p;
+        fetch_pix(y0 + 2, pf_pix);
+    }
+    __syncthreads();
     // this thread's disparities: d = m + 127 - n for its columns n = c0 + j;
     // searched iff jlo <= j <= jhi: d < nd, and the matched window inside the
     // image (R <= xb + n < W - R)
@@ -339,9 +365,10 @@ __global__ void __launch_bounds__(tc::kNT, 1)
     // accumulator, which stays D(y) until that barrier.
     for (int oy = 0; oy < rows && !failed; ++oy) {
         const int y = y0 + oy;
-        const int sx = sx_n, tx = tx_n;
-        const float fvx = fvx_n;
-        const bool pok = ok_n;
+        const int4 pr = pixrec[(oy % 3) * kM + m];
+        const int sx = pr.x, tx = pr.z;
+        const float fvx = __int_as_float(pr.y);
+        const bool pok = pr.w != 0;
         const uint32_t tlane = tmem + (uint32_t(32 * q) << 16);
         // ---- the window sums of row y
         const bool ok = phase < issued ? wait_mma() : true;
@@ -417,15 +444,6 @@ __global__ void __launch_bounds__(tc::kNT, 1)
         const float lower = best - 4e-6f * fabsf(best);
         const bool searched = best > -INFINITY;
         const bool others = ok && searched && v2 > lower;
-        // those columns (rare), as a mask of j
-        uint32_t cm[2] = {0u, 0u};
-        if (__any_sync(0xffffffffu, others)) {
-            float C[kCols];
-            tc::ld40(tlane + uint32_t(c0), C);  // the same sums again
-#pragma unroll
-            for (int j = 0; j < kCols; ++j)
-                cm[j >> 5] |= uint32_t(others && j != jbest && est_of(C[j], j, cr[j], true) > lower) << (j & 31);
-        }
         auto d_of = [&](int j) { return m + kDB - 1 - (c0 + j) + dz0; };  // relative to dmin
         // IEEE score of column j with window sum c (an exact integer in fp32)
         auto exact_key = [&](float c, int j) {
@@ -438,16 +456,13 @@ __global__ void __launch_bounds__(tc::kNT, 1)
             return ((unsigned long long)ordered(sc) << 32) | (0xFFFFFFFFu - uint32_t(d_of(j)));
         };
         unsigned long long key = searched ? exact_key(cbest, jbest) : 0ull;
-        // the other candidates: the warp re-reads each column some lane needs
-        // (a warp-wide TMEM load) and scores it there
-        uint32_t wm[2] = {__reduce_or_sync(0xffffffffu, cm[0]), __reduce_or_sync(0xffffffffu, cm[1])};
-#pragma unroll
-        for (int w = 0; w < 2; ++w) {
-            while (wm[w]) {
-                const int j = 32 * w + __ffs(wm[w]) - 1;
-                wm[w] &= wm[w] - 1u;
+        // those columns (rare: a few warps in a thousand): the warp re-reads
+        // every column (a warp-wide TMEM load) and scores the candidates
+        if (__any_sync(0xffffffffu, others)) {
+#pragma unroll 1
+            for (int j = 0; j < kCols; ++j) {
                 const float c = tc::ld1(tlane + uint32_t(c0 + j));
-                if ((cm[w] >> (j & 31)) & 1u) {
+                if (others && j != jbest && est_of(c, j, cr[j], true) > lower) {
                     const unsigned long long k2 = exact_key(c, j);
                     key = k2 > key ? k2 : key;
                 }
@@ -497,7 +512,10 @@ __global__ void __launch_bounds__(tc::kNT, 1)
             pf0 = fetch_byte(tid, y + R + 4, y - R + 3);
             pf1 = tid + tc::kNT < 2 * kSB ? fetch_byte(tid + tc::kNT, y + R + 4, y - R + 3) : 0u;
         }
-        if (oy + 1 < rows) pix(y + 1, sx_n, fvx_n, tx_n, ok_n);
+        if (oy + 2 < rows && h == 0) {
+            pixrec[((oy + 2) % 3) * kM + m] = pf_pix;
+            fetch_pix(y + 3, pf_pix);
+        }
     }
     if (failed && tid == 0) dev::report(a.status, CT_ETIMEOUT);
     // outstanding MMAs (a failed wait) complete before the TMEM is released

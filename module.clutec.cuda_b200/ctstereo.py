@@ -445,7 +445,7 @@ class BlockMatcherNCC(_Driver):
                                       _img_ref(right), _img_ref(disp_init), _stream(stream)))
 
     def set_tensor_cores(self, enable: bool):
-        """Unguided matching on the tensor cores or on the CUDA cores (default); same maps."""
+        """Unguided matching on the tensor cores (default) or on the CUDA cores; same maps."""
         check(lib().ct_bm_ncc_set_tensor_cores(self._h, 1 if enable else 0))
 
 
