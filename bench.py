@@ -64,12 +64,12 @@ def parse():
                     help="held-out 1080p pairs for the confidence-net AUC (default 4 in the census line, 24 in confnet1080)")
     ap.add_argument("--profile", default=None,
                     choices=["census_match", "census_fused", "confnet_infer", "pipelines", "sad640", "ncc1080",
-                             "aw1440", "batch64",
-                             "compat_ncc1080"],
+                             "ncc1080_cuda_cores", "aw1440", "batch64", "compat_ncc1080"],
                     help="for ncu captures, then exit: census_match or confnet_infer = that kernel twice on the "
                          "1080p D=128 pair; pipelines = the plain L-R pipeline 3x (one fused pass), 3x in two "
                          "passes, then the learned one 3x; a "
-                         "configuration name = its step twice (no autotuning, no CPU work)")
+                         "configuration name = its step twice (no autotuning, no CPU work); ncc1080_cuda_cores = "
+                         "the ncc1080 step with the window sums on the CUDA cores")
     ap.add_argument("--no-configs", action="store_true",
                     help="default run: measure the headline only, without the other configurations")
     return ap.parse_args()
@@ -632,7 +632,7 @@ def profile_config(args):
         step = lambda: m.process(pairs)
     else:
         W, H, D, kind = {"sad640": (640, 480, 64, 1), "ncc1080": (1920, 1080, 128, 2), "aw1440": (2560, 1440, 256, 3),
-                         "compat_ncc1080": (1920, 1080, 128, 2)}[wl]
+                         "compat_ncc1080": (1920, 1080, 128, 2), "ncc1080_cuda_cores": (1920, 1080, 128, 2)}[wl]
         L, R, _, _ = ct.synth_pair(kind, SEED, W, H, D - 1)
         dL, dR = up(L), up(R)
         if wl == "sad640":
@@ -640,9 +640,10 @@ def profile_config(args):
             m.configure(0, W, H, D, radius=4)
             out = ct.alloc_image(H, W, torch.uint8, dev)
             step = lambda: m.process(out, dL, dR)
-        elif wl == "ncc1080":
+        elif wl in ("ncc1080", "ncc1080_cuda_cores"):
             m = ct.BlockMatcherNCC()
             m.configure(0, W, H, D, radius=5)
+            m.set_tensor_cores(wl == "ncc1080")
             out = ct.alloc_image(H, W, torch.uint8, dev)
             score = ct.alloc_image(H, W, torch.float32, dev)
             step = lambda: m.process(out, dL, dR, score=score)
