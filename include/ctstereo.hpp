@@ -553,6 +553,12 @@ public:
     void Process(_CDeviceSurface& xImageDisp, const _CDeviceSurface& xImageL, const _CDeviceSurface& xImageR) {
         Process(xImageDisp, xImageL, xImageR, _CDeviceSurface(), _CDeviceSurface());
     }
+    /* Unguided plain matching with the window sums on the tensor cores (the
+     * default) or on the CUDA cores; the maps and scores are the same. */
+    void SetTensorCores(bool bEnable) {
+        if (!m_pHandle) throw CError(CT_ESTATE, "BlockMatcherNCC: configure a left-to-right matcher first");
+        Ensure(ct_bm_ncc_set_tensor_cores(m_pHandle, bEnable ? 1 : 0), "BlockMatcherNCC::SetTensorCores");
+    }
 
 private:
     SParameter m_xPars;

@@ -69,6 +69,7 @@ static int RunCpu() {
         BlockMatcherNCC::SParameter p;
         p.Set(dc, 0, 0.f, 0.f, 1, true, BlockMatcherNCC::EConfig::Patch_11x11);
         BlockMatcherNCC::CDriver d;
+        CHECK(ThrownCode([&] { d.SetTensorCores(false); }) == CT_ESTATE, "NCC SetTensorCores before Configure");
         p.iUseDispInput = 0;
         p.xDispConfig.Set(-1, 128);
         CHECK(ThrownCode([&] { d.Configure(dev, f, p); }) == CT_EINVAL, "NCC iMin < 0 must be rejected");
@@ -292,6 +293,16 @@ static int RunGpu(const char* weights) {
                     low += s[size_t(y) * W + x] < 0.9999f;
                 }
         CHECK(bad == 0 && low == 0, "NCC: %d interior pixels off, %d scores below 1", bad, low);
+        {  // the same map and scores with the window sums on the CUDA cores
+            d.SetTensorCores(false);
+            CDeviceSurface disp2(f16), score2(f32);
+            ProcessKernel(d, disp2, surfL, surfR, _CDeviceSurface(), score2);
+            d.SetTensorCores(true);
+            const auto v2 = disp2.CopyInto<uint16_t>();
+            const auto s2 = score2.CopyInto<float>();
+            CHECK(v2 == v && std::memcmp(s2.data(), s.data(), s.size() * sizeof(float)) == 0,
+                  "NCC: CUDA-core and tensor-core kernels differ");
+        }
 
         // visualisation of the map: interior pixels gray at t = K / 128,
         // border pixels (CannotEvaluate) in the default colour
