@@ -218,6 +218,7 @@ def test_aw_guided_matches_oracle(ct, oracle, cuda, W, H, D, s, holes, ctype):
     (129, 200, 128, 5, 0),   # one pixel past a 128-pixel tile, several strips
     (140, 33, 64, 5, 0),     # strips of 16, 16 and 1 rows
     (300, 50, 96, 4, 0),     # strips of 16, 16, 16 and 2 rows
+    (200, 70, 256, 2, 3),    # 5x5, two disparity blocks, odd minimum disparity
 ])
 def test_ncc_tensor_cores_equal_cuda_cores(ct, oracle, cuda, W, H, D, r, dmin):
     """Unguided NCC on the tensor cores gives the CUDA-core kernel's maps and
