@@ -17,22 +17,27 @@
 // row costs two MMAs. Operands are K-major, no swizzle: pixel row i of a
 // panel at i * 16 bytes, the second 8-element K chunk one panel column
 // (rows x 16 bytes) further. They are built in shared memory from two staged
-// image rows per step (bytes -> f16 through the exponent of 1024).
+// image rows per step (bytes -> f16 through the exponent of 1024); the
+// strip's first window is built at once and summed by one chain of 2R+1
+// MMAs.
 //
 // Epilogue: TMEM lane m = pixel x0 + m holds C(x, x') for all 256 columns;
 // its disparities d = m + 127 - n (column n) form a 128-wide band. 16 warps:
 // lane quarter q = warp % 4 (the lanes a warp may read), column slice h =
 // warp / 4 of the quarter's band (40 columns each: 32 q + 40 h ..), read with
 // one 32-column and one 8-column tcgen05.ld per row. Ranking as the CUDA-core
-// kernel, by the estimate num * rsqrt(vy), num = n C - Sx Sy, here from the
-// fp32 sum: est = C (n r) - Sx (Sy r), whose error is at most 240 r plus a
-// relative 1e-6 (the products n C and Sx Sy are below 2^30); every disparity
-// whose estimate lies within that margin of the thread's best is scored
+// kernel, by the estimate num * rsqrt(vy), num = n C - Sx Sy, here in fp32
+// with Sx Sy split into its rounded product and that product's exact error
+// (an fma), so that the estimate's error is relative only (~1e-6); every
+// disparity whose estimate lies within 4e-6 of the thread's best is scored
 // exactly (the IEEE score of the CUDA-core kernel, from the exact integer C),
 // so the exact argmax over the thread's disparities is always among them.
-// The 4 (column slices) x gridDim.z keys of a pixel merge by atomicMax, in
-// shared memory per row and, for D > 128, in global memory with the
-// last-arriver merge of the CUDA-core kernel.
+// The 4 column slices' keys of a pixel merge in shared memory per row; for
+// D > 128 the gridDim.z CTAs' keys merge by atomicMax in global memory with
+// the last-arriver merge of the CUDA-core kernel. After each row's barrier
+// warp 0 issues the window update, slices 1 and 2 build the operand panels
+// of the update after next, slice 3 the column records, slice 0 writes the
+// outputs and the pixel records.
 #pragma once
 
 #include <type_traits>
