@@ -30,56 +30,83 @@ __host__ __device__ constexpr size_t smem_bytes(int th, int R) {
     return strip_bytes(th, R) + size_t(th) * two_of(R) * 8 + 16;
 }
 
-// Box sum S and n*Q - S^2 for every pixel whose window is inside the image,
-// and (T non-null) the zero-score threshold of the left view: the smallest vy
-// with V * vy >= n^4, i.e. ceil(n^4 / V) (INT_MAX when V = 0), so that the
+// Box sum S and n*Q - S^2 of every pixel (the window zero-padded outside
+// the image; the matchers read them only where it is inside) for both views
+// in one launch (blockIdx.z: 0 the left view, which also gets T, 1 the right
+// view), and the zero-score threshold of the left view: the smallest vy with
+// V * vy >= n^4, i.e. ceil(n^4 / V) (INT_MAX when V = 0), so that the
 // matcher's test sigma_x sigma_y >= 1 is one 32-bit compare vy >= T.
-// Separable: a CTA stages a (32 + 2R) x (8 + 2R) tile, sums every staged row
-// horizontally (S and Q of 2R+1 pixels) into shared memory, then each thread
-// sums its column of 2R+1 row sums.
+// Separable: a CTA stages a (32 + 2R) x (64 + 2R) tile, sums every staged
+// row horizontally (running sums over 4 columns a thread) into shared
+// memory, then each thread runs a vertical sum down 8 rows of its column.
 template <int R>
-__global__ void __launch_bounds__(256) box_stats_kernel(const uint8_t* img, size_t pitch, int W, int H, int32_t* S,
-                                                        int32_t* V, int32_t* T) {
-    constexpr int TX = 32, TY = 8, SW = TX + 2 * R, SH = TY + 2 * R;
+__global__ void __launch_bounds__(256) box_stats_kernel(const uint8_t* imgL, size_t pitchL, const uint8_t* imgR,
+                                                        size_t pitchR, int W, int H, int32_t* SL, int32_t* VL,
+                                                        int32_t* TL, int32_t* SR, int32_t* VR) {
+    constexpr int TX = 32, TY = 64, K = 2 * R + 1, SW = TX + 2 * R, SH = TY + 2 * R;
     __shared__ uint8_t t[SH][SW];
     __shared__ int hs[SH][TX], hq[SH][TX];
+    const bool right = blockIdx.z != 0;
+    const uint8_t* img = right ? imgR : imgL;
+    const size_t pitch = right ? pitchR : pitchL;
+    int32_t* S = right ? SR : SL;
+    int32_t* V = right ? VR : VL;
+    int32_t* T = right ? nullptr : TL;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int tid = threadIdx.y * TX + threadIdx.x;
-    for (int i = tid; i < SW * SH; i += TX * TY) {
+    for (int i = tid; i < SW * SH; i += TX * 8) {
         const int yy = y0 - R + i / SW, xx = x0 - R + i % SW;
         t[i / SW][i % SW] = (xx >= 0 && xx < W && yy >= 0 && yy < H) ? img[(size_t)yy * pitch + xx] : 0;
     }
     __syncthreads();
-    for (int i = tid; i < SH * TX; i += TX * TY) {
-        const int r = i / TX, c = i % TX;
+    for (int i = tid; i < SH * (TX / 4); i += TX * 8) {
+        const int r = i / (TX / 4), c = 4 * (i % (TX / 4));
+        int v[K + 3];
+#pragma unroll
+        for (int k = 0; k < K + 3; ++k) v[k] = t[r][c + k];
         int s = 0, q = 0;
 #pragma unroll
-        for (int dx = 0; dx <= 2 * R; ++dx) {
-            const int v = t[r][c + dx];
-            s += v;
-            q += v * v;
+        for (int k = 0; k < K; ++k) {
+            s += v[k];
+            q += v[k] * v[k];
         }
         hs[r][c] = s;
         hq[r][c] = q;
+#pragma unroll
+        for (int j = 1; j < 4; ++j) {
+            s += v[j + K - 1] - v[j - 1];
+            q += v[j + K - 1] * v[j + K - 1] - v[j - 1] * v[j - 1];
+            hs[r][c + j] = s;
+            hq[r][c + j] = q;
+        }
     }
     __syncthreads();
-    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
-    if (x >= W || y >= H) return;
-    int s = 0, q = 0;
-#pragma unroll
-    for (int dy = 0; dy <= 2 * R; ++dy) {
-        s += hs[threadIdx.y + dy][threadIdx.x];
-        q += hq[threadIdx.y + dy][threadIdx.x];
-    }
-    constexpr int n = (2 * R + 1) * (2 * R + 1);
+    constexpr int n = K * K;
     constexpr long long n4 = (long long)n * n * n * n;
     static_assert(n4 < 0x7FFFFFFFll, "the threshold fits in int32");
     // n^4 + V - 1 < 2^32 (V <= n^2 255^2 / 4): one 32-bit division
     static_assert(n4 + (long long)n * n * 255 * 255 / 4 < 0xFFFFFFFFll, "32-bit threshold division");
-    const int v = n * q - s * s;
-    S[(size_t)y * W + x] = s;
-    V[(size_t)y * W + x] = v;
-    if (T) T[(size_t)y * W + x] = v > 0 ? int32_t((uint32_t(n4) + uint32_t(v) - 1u) / uint32_t(v)) : 0x7FFFFFFF;
+    const int x = x0 + threadIdx.x, r0 = 8 * threadIdx.y;
+    int s = 0, q = 0;
+#pragma unroll
+    for (int dy = 0; dy < K; ++dy) {
+        s += hs[r0 + dy][threadIdx.x];
+        q += hq[r0 + dy][threadIdx.x];
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        if (k > 0) {
+            s += hs[r0 + k + K - 1][threadIdx.x] - hs[r0 + k - 1][threadIdx.x];
+            q += hq[r0 + k + K - 1][threadIdx.x] - hq[r0 + k - 1][threadIdx.x];
+        }
+        const int y = y0 + r0 + k;
+        if (x < W && y < H) {
+            const int v = n * q - s * s;
+            S[(size_t)y * W + x] = s;
+            V[(size_t)y * W + x] = v;
+            if (T) T[(size_t)y * W + x] = v > 0 ? int32_t((uint32_t(n4) + uint32_t(v) - 1u) / uint32_t(v)) : 0x7FFFFFFF;
+        }
+    }
 }
 
 __device__ __forceinline__ uint32_t ordered(float f) {
@@ -455,11 +482,10 @@ int launch_ncc(NccHandle* h, const ct_image* disp, const ct_image* score, const 
         a.guide = h->guide;
         a.guide_gw = gw;
     }
-    dim3 sb(32, 8), sg((W + 31) / 32, (H + 7) / 8);
-    box_stats_kernel<R><<<sg, sb, 0, s>>>(static_cast<const uint8_t*>(L->ptr), L->pitch_bytes, W, H, h->stats,
-                                          h->stats + N, h->stats + 4 * N);
-    box_stats_kernel<R><<<sg, sb, 0, s>>>(static_cast<const uint8_t*>(Rr->ptr), Rr->pitch_bytes, W, H,
-                                          h->stats + 2 * N, h->stats + 3 * N, nullptr);
+    dim3 sb(32, 8), sg((W + 31) / 32, (H + 63) / 64, 2);
+    box_stats_kernel<R><<<sg, sb, 0, s>>>(static_cast<const uint8_t*>(L->ptr), L->pitch_bytes,
+                                          static_cast<const uint8_t*>(Rr->ptr), Rr->pitch_bytes, W, H, h->stats,
+                                          h->stats + N, h->stats + 4 * N, h->stats + 2 * N, h->stats + 3 * N);
     CT_LAUNCH_CHECK();
     if (!init && h->tensor_cores) {
         static bool attr_tc = false;
