@@ -36,15 +36,20 @@ __host__ __device__ constexpr size_t smem_bytes(int th, int R) {
 // view), and the zero-score threshold of the left view: the smallest vy with
 // V * vy >= n^4, i.e. ceil(n^4 / V) (INT_MAX when V = 0), so that the
 // matcher's test sigma_x sigma_y >= 1 is one 32-bit compare vy >= T.
-// Separable: a CTA stages a (32 + 2R) x (64 + 2R) tile, sums every staged
+// Separable: a CTA stages a (32 + 2R) x (64 + 2R) tile (aligned words), sums every staged
 // row horizontally (running sums over 4 columns a thread) into shared
 // memory, then each thread runs a vertical sum down 8 rows of its column.
 template <int R>
 __global__ void __launch_bounds__(256) box_stats_kernel(const uint8_t* imgL, size_t pitchL, const uint8_t* imgR,
                                                         size_t pitchR, int W, int H, int32_t* SL, int32_t* VL,
                                                         int32_t* TL, int32_t* SR, int32_t* VR) {
-    constexpr int TX = 32, TY = 64, K = 2 * R + 1, SW = TX + 2 * R, SH = TY + 2 * R;
-    __shared__ uint8_t t[SH][SW];
+    constexpr int TX = 32, TY = 64, K = 2 * R + 1, SH = TY + 2 * R;
+    // staged rows: 12 aligned words from x0 - 8 (x0 - R .. x0 + 31 + R at
+    // byte offset 8 - R); image pointers and pitches are 16-byte aligned, so
+    // a word starting inside a row lies inside the pitch
+    constexpr int NWd = 12;
+    static_assert(R <= 8 && TX + 2 * R + (8 - R) <= 4 * NWd, "staged words cover the tile");
+    __shared__ uint32_t tw[SH][NWd];
     __shared__ int hs[SH][TX], hq[SH][TX];
     const bool right = blockIdx.z != 0;
     const uint8_t* img = right ? imgR : imgL;
@@ -54,16 +59,22 @@ __global__ void __launch_bounds__(256) box_stats_kernel(const uint8_t* imgL, siz
     int32_t* T = right ? nullptr : TL;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int tid = threadIdx.y * TX + threadIdx.x;
-    for (int i = tid; i < SW * SH; i += TX * 8) {
-        const int yy = y0 - R + i / SW, xx = x0 - R + i % SW;
-        t[i / SW][i % SW] = (xx >= 0 && xx < W && yy >= 0 && yy < H) ? img[(size_t)yy * pitch + xx] : 0;
+    for (int i = tid; i < SH * NWd; i += TX * 8) {
+        const int r = i / NWd, wc = i % NWd;
+        const int yy = y0 - R + r, xw = x0 - 8 + 4 * wc;
+        uint32_t v = 0;
+        if (yy >= 0 && yy < H && xw >= 0 && xw < W) {
+            v = *reinterpret_cast<const uint32_t*>(img + (size_t)yy * pitch + xw);
+            if (xw + 4 > W) v &= 0xFFFFFFFFu >> (8 * (xw + 4 - W));  // bytes at x >= W read 0
+        }
+        tw[r][wc] = v;
     }
     __syncthreads();
     for (int i = tid; i < SH * (TX / 4); i += TX * 8) {
         const int r = i / (TX / 4), c = 4 * (i % (TX / 4));
         int v[K + 3];
 #pragma unroll
-        for (int k = 0; k < K + 3; ++k) v[k] = t[r][c + k];
+        for (int k = 0; k < K + 3; ++k) v[k] = reinterpret_cast<const uint8_t*>(tw[r])[8 - R + c + k];
         int s = 0, q = 0;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
