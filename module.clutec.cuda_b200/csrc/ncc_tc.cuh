@@ -54,7 +54,11 @@ constexpr int kCols = 40;  // accumulator columns a thread ranks per row
 constexpr int kPA = kM * 16 * 2, kPB = kN * 16 * 2;  // panel bytes (K = 16 f16)
 constexpr int kPanel = kPA + kPB;                    // one image row's A and B panels
 constexpr int kSet = 2 * kPanel;                     // entering + leaving row
-constexpr int kSL = kM + 16, kSR = kN + 16;          // staged bytes of one row (>= 128 + 2R, 256 + 2R)
+// staged bytes of one image row, as aligned words: the left view from x0 - 8
+// (x0 - R .. x0 + 127 + R at byte 8 - R), the right view from xb - R rounded
+// down to 4 bytes (xb - R .. xb + 255 + R at byte (xb - R) & 3)
+constexpr int kSL = kM + 24, kSR = kN + 20;
+static_assert(kSL % 4 == 0 && kSR % 4 == 0 && kSL >= kM + 8 + 2 * 7 && kSR >= kN + 3 + 2 * 7, "staged words");
 constexpr int kStage = 2 * (kSL + kSR);              // entering + leaving row
 // shared memory
 constexpr int kOffSet = 0;                        // 2 panel sets
@@ -211,19 +215,27 @@ __global__ void __launch_bounds__(tc::kNT, 1)
     uint32_t issued = 0;  // MMA commits issued (counted by every thread)
     bool failed = false;
 
-    // Byte b of a staging buffer: half s = b / kSB (0 the entering row, 1 the
-    // leaving row), index i = b % kSB: left view x0 - R + i (i < kSL), else
-    // right view xb - R + i - kSL; 0 outside the image.
-    auto fetch_byte = [&](int b, int r_in, int r_out) -> uint32_t {
-        const int s = b >= kSB, i = b - s * kSB, r = s ? r_out : r_in;
-        const bool left = i < kSL;
-        const int xx = left ? x0 - R + i : xb - R + (i - kSL);
+    // Word wi of a staging buffer: half s = wi / kWB (0 the entering row, 1
+    // the leaving row), word w = wi % kWB: the left view from x0 - 8 (w <
+    // kSL / 4), else the right view from xr; bytes outside the image read 0.
+    // Image pointers and pitches are 16-byte aligned and the starts are
+    // multiples of 4, so a word starting inside a row lies inside its pitch.
+    constexpr int kWB = kSB / 4;
+    const int xr = (xb - R) & ~3, oL = 8 - R, oR = (xb - R) - xr;
+    auto fetch_word = [&](int wi, int r_in, int r_out) -> uint32_t {
+        const int s = wi >= kWB, w = wi - s * kWB, r = s ? r_out : r_in;
+        const bool left = w < kSL / 4;
+        const int xx = left ? x0 - 8 + 4 * w : xr + 4 * (w - kSL / 4);
         if (r < 0 || r >= a.H || xx < 0 || xx >= a.W) return 0u;
-        return left ? __ldg(Limg + (size_t)r * pl + xx) : __ldg(Rimg + (size_t)r * pr + xx);
+        uint32_t v = left ? *reinterpret_cast<const uint32_t*>(Limg + (size_t)r * pl + xx)
+                          : *reinterpret_cast<const uint32_t*>(Rimg + (size_t)r * pr + xx);
+        if (xx + 4 > a.W) v &= 0xFFFFFFFFu >> (8 * (xx + 4 - a.W));  // bytes at x >= W read 0
+        return v;
     };
     // the whole staging buffer b (start of the strip)
     auto stage_rows = [&](int b, int r_in, int r_out) {
-        for (int i = tid; i < 2 * kSB; i += tc::kNT) smem[kOffStage + b * kStage + i] = uint8_t(fetch_byte(i, r_in, r_out));
+        uint32_t* st = reinterpret_cast<uint32_t*>(smem + kOffStage + b * kStage);
+        for (int i = tid; i < 2 * kWB; i += tc::kNT) st[i] = fetch_word(i, r_in, r_out);
     };
     // panel row k of panel set p (k < 2 (kM + kN): half k / (kM + kN), A rows
     // first) from staging buffer b
@@ -231,8 +243,8 @@ __global__ void __launch_bounds__(tc::kNT, 1)
         const int s = k >= kM + kN, i = k - s * (kM + kN);
         const uint8_t* src = smem + kOffStage + b * kStage + s * kSB;
         unsigned char* set = smem + kOffSet + p * kSet;
-        if (i < kM) tc::build_row<R>(src + i, set + s * kPA + i * 16, kM * 16);
-        else tc::build_row<R>(src + kSL + (i - kM), set + 2 * kPA + s * kPB + (i - kM) * 16, kN * 16);
+        if (i < kM) tc::build_row<R>(src + oL + i, set + s * kPA + i * 16, kM * 16);
+        else tc::build_row<R>(src + kSL + oR + (i - kM), set + 2 * kPA + s * kPB + (i - kM) * 16, kN * 16);
     };
     auto build_all = [&](int p, int b) {
         for (int k = tid; k < 2 * (kM + kN); k += tc::kNT) build_item(p, b, k);
@@ -293,9 +305,9 @@ __global__ void __launch_bounds__(tc::kNT, 1)
     {
         constexpr int NW = 2 * R + 1;
         uint8_t* istage = smem + kOffInit + NW * kPanel;
-        for (int i = tid; i < NW * kSB; i += tc::kNT) {
-            const int k = i / kSB;
-            istage[i] = uint8_t(fetch_byte(i - k * kSB, y0 - R + k, 0));
+        for (int i = tid; i < NW * kWB; i += tc::kNT) {
+            const int k = i / kWB;
+            reinterpret_cast<uint32_t*>(istage)[i] = fetch_word(i - k * kWB, y0 - R + k, 0);
         }
         stage_rows(1, y0 + R + 1, y0 - R);
         for (int cx = tid; cx < kN; cx += tc::kNT) {
@@ -310,8 +322,8 @@ __global__ void __launch_bounds__(tc::kNT, 1)
             const int k = i / (kM + kN), t = i - k * (kM + kN);
             const uint8_t* src = istage + k * kSB;
             unsigned char* pan = smem + kOffInit + k * kPanel;
-            if (t < kM) tc::build_row<R>(src + t, pan + t * 16, kM * 16);
-            else tc::build_row<R>(src + kSL + (t - kM), pan + kPA + (t - kM) * 16, kN * 16);
+            if (t < kM) tc::build_row<R>(src + oL + t, pan + t * 16, kM * 16);
+            else tc::build_row<R>(src + kSL + oR + (t - kM), pan + kPA + (t - kM) * 16, kN * 16);
         }
         build_all(1, 1);  // ends with the proxy fence
         tc::fence_before();
@@ -330,10 +342,10 @@ __global__ void __launch_bounds__(tc::kNT, 1)
         // y0 - R + 1 out)
         stage_rows(0, y0 + R + 2, y0 - R + 1);
     }
-    // loads in flight across a step: the staged bytes of the rows after next
-    // (bytes tid and tid + 512 of a buffer) and the column inputs of row y + 2
-    uint32_t pf0 = fetch_byte(tid, y0 + R + 3, y0 - R + 2);
-    uint32_t pf1 = tid + tc::kNT < 2 * kSB ? fetch_byte(tid + tc::kNT, y0 + R + 3, y0 - R + 2) : 0u;
+    // loads in flight across a step: the staged words of the rows after next
+    // (word tid of a buffer) and the column inputs of row y + 2
+    static_assert(2 * kWB <= tc::kNT, "one staged word a thread");
+    uint32_t pf0 = tid < 2 * kWB ? fetch_word(tid, y0 + R + 3, y0 - R + 2) : 0u;
     int pf_sy0 = 0, pf_vy0 = -1, pf_sy1 = 0, pf_vy1 = -1;
     if (colder) {
         fetch_col(cx0, y0 + 2, pf_sy0, pf_vy0);
@@ -511,11 +523,10 @@ __global__ void __launch_bounds__(tc::kNT, 1)
             fetch_col(cx0 + kM, y + 3, pf_sy1, pf_vy1);
         }
         if (oy + 3 < rows) {
-            unsigned char* st = smem + kOffStage + ((oy + 1) & 1) * kStage;
-            st[tid] = uint8_t(pf0);
-            if (tid + tc::kNT < 2 * kSB) st[tid + tc::kNT] = uint8_t(pf1);
-            pf0 = fetch_byte(tid, y + R + 4, y - R + 3);
-            pf1 = tid + tc::kNT < 2 * kSB ? fetch_byte(tid + tc::kNT, y + R + 4, y - R + 3) : 0u;
+            if (tid < 2 * kWB) {
+                reinterpret_cast<uint32_t*>(smem + kOffStage + ((oy + 1) & 1) * kStage)[tid] = pf0;
+                pf0 = fetch_word(tid, y + R + 4, y - R + 3);
+            }
         }
         if (oy + 2 < rows && h == 0) {
             pixrec[((oy + 2) % 3) * kM + m] = pf_pix;
